@@ -1,0 +1,280 @@
+/*
+ * ratbite_b200 — C ABI of the B200-native per-sample rendering path.
+ *
+ * This library is a drop-in for what sits below ratbite's OptiX launch:
+ * RenderingInterface keeps producing the same scene, material, light-tree,
+ * spectral and LUT data (src/core/rendering_interface.cpp) and hands it to
+ * these entry points instead of building OptiX acceleration structures and
+ * calling optixLaunch. Everything below is plain C: pointers, sizes and
+ * status codes. All functions return RB_OK (0) on success and a negative
+ * status otherwise; rb_last_error() gives the message. No call aborts, and
+ * device-side failures are reported through rb_status() (a status word the
+ * kernels set instead of trapping).
+ *
+ * Coordinates follow the reference's camera-relative convention: instance
+ * transforms, emissive triangles and light-tree node means are already offset
+ * by -cameraPosition by the caller (src/core/rendering_interface.cpp:986,
+ * 1449-1457, 1484-1486); camera rays start at the origin
+ * (src/device/dir_gen.h:29).
+ */
+#ifndef RATBITE_B200_H
+#define RATBITE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RB_ABI_VERSION 1
+
+/* Status codes. */
+#define RB_OK                  0
+#define RB_ERR_INVALID        -1  /* bad argument or inconsistent data */
+#define RB_ERR_CUDA           -2  /* a CUDA runtime call failed */
+#define RB_ERR_UNSUPPORTED    -3  /* a feature outside this build's scope */
+#define RB_ERR_NO_SCENE       -4  /* render called before geometry/launch set-up */
+#define RB_ERR_DEVICE         -5  /* a kernel set the device status word */
+#define RB_ERR_OOM            -6  /* device allocation failed */
+
+/* Device status bits (rb_device_status.flags). */
+#define RB_DEV_STACK_OVERFLOW   (1u << 0)  /* BVH traversal stack exhausted */
+#define RB_DEV_QUEUE_OVERFLOW   (1u << 1)  /* a wavefront queue overflowed */
+#define RB_DEV_NAN_RADIANCE     (1u << 2)  /* a path produced a non-finite sample */
+#define RB_DEV_ITERATION_LIMIT  (1u << 3)  /* a bounded wait gave up */
+#define RB_DEV_BAD_INDEX        (1u << 4)  /* an index read from scene data was out of range */
+
+/* Index buffer element types (IndexType, src/core/material.h:9-15). */
+#define RB_INDEX_U16 0
+#define RB_INDEX_U32 1
+
+/* BxDF callable indices (bxdfTypeToIndex, src/core/rendering_interface.cpp:1291-1309). */
+#define RB_BXDF_PURE_CONDUCTOR   0
+#define RB_BXDF_PURE_DIELECTRIC  1
+#define RB_BXDF_COMPLEX_SURFACE  2
+
+/* Bitfields of MaterialData (src/core/material.h:19-60), same bit values. */
+#define RB_ATTR_NORMAL       (1u << 0)
+#define RB_ATTR_FRAME        (1u << 1)
+#define RB_ATTR_COLOR        (1u << 2)
+#define RB_ATTR_TEX_COORD_1  (1u << 3)
+#define RB_ATTR_TEX_COORD_2  (1u << 4)
+#define RB_FACTOR_BASE_COLOR   (1u << 0)
+#define RB_FACTOR_METALNESS    (1u << 1)
+#define RB_FACTOR_ROUGHNESS    (1u << 2)
+#define RB_FACTOR_TRANSMISSION (1u << 3)
+#define RB_FACTOR_CUTOFF       (1u << 4)
+#define RB_FACTOR_BLEND        (1u << 5)
+#define RB_FACTOR_SHEEN_COLOR  (1u << 6)
+#define RB_FACTOR_SHEEN_ROUGH  (1u << 7)
+#define RB_FACTOR_EMISSION     (1u << 8)
+
+#define RB_SPECTRUM_BINS 471   /* 360..830 nm, src/core/spectral_settings.h:5-9 */
+#define RB_LUT_SIZE 32         /* LUT edge, src/core/rendering_interface.cpp:530-533 */
+
+typedef struct rb_ctx rb_ctx;
+
+typedef struct rb_config {
+    int32_t device;              /* CUDA device ordinal */
+    uint32_t max_paths_in_flight;/* wavefront capacity; 0 = choose from the device */
+    uint32_t reserved[6];
+} rb_config;
+
+/*
+ * One material record: MaterialData (src/core/material.h:17-107) field for
+ * field, minus OptiX and texture-object specifics. Textures are outside this
+ * build's scope: `textures` must be 0. The index and attribute buffers are the
+ * per-submesh vertex data the shading step reads
+ * (src/kernels/pathtrace.cu:1290-1431); they are copied at upload.
+ */
+typedef struct rb_material {
+    uint32_t bxdf;               /* RB_BXDF_* (bxdfIndexSBT) */
+    uint32_t double_sided;
+    uint32_t sheen_present;
+    uint32_t index_type;         /* RB_INDEX_U16 / RB_INDEX_U32 */
+    uint32_t attributes;         /* RB_ATTR_* bits */
+    uint32_t attribute_stride;   /* bytes per vertex in attribute_data */
+    uint32_t normal_offset, frame_offset, color_offset, texcoord1_offset, texcoord2_offset;
+    uint32_t ior_spectrum;       /* index into the extra spectra (indexOfRefractSpectrumDataIndex) */
+    uint32_t absorp_spectrum;    /* absorpCoefSpectrumDataIndex */
+    uint32_t emission_spectrum;  /* emissionSpectrumDataIndex (not read on the device) */
+    float mf_roughness;          /* mfRoughnessValue */
+    float ior;
+    float alpha_cutoff;
+    uint32_t textures;           /* must be 0 */
+    uint32_t factors;            /* RB_FACTOR_* bits */
+    float base_color[4];
+    float metalness;
+    float roughness;
+    float transmission;
+    float sheen_color[3];
+    float sheen_roughness;
+    float emissive[3];
+    uint32_t triangle_count;     /* triangles in `indices` */
+    const void* indices;         /* triangle_count * 3 indices of index_type */
+    uint32_t vertex_count;       /* vertices in attribute_data */
+    const void* attribute_data;  /* vertex_count * attribute_stride bytes, or NULL */
+} rb_material;
+
+/* Geometry: meshes of submeshes, placed by instances (SceneData::Mesh /
+ * Submesh / Instance, src/core/scene.h:85-152). */
+typedef struct rb_submesh {
+    uint32_t material;           /* index into the rb_set_materials table (hit-group data) */
+    uint32_t index_type;         /* RB_INDEX_U16 / RB_INDEX_U32 */
+    uint32_t triangle_count;
+    const void* indices;         /* triangle_count * 3 indices */
+    uint32_t vertex_count;
+    const float* vertices;       /* vertex_count * 4 floats: x, y, z, unused */
+    uint32_t discarded_count;    /* primitives made degenerate (emissive ones, cut out) */
+    const uint32_t* discarded;
+} rb_submesh;
+
+typedef struct rb_mesh {
+    uint32_t submesh_count;
+    const rb_submesh* submeshes;
+} rb_mesh;
+
+typedef struct rb_instance {
+    uint32_t mesh;
+    float transform[12];         /* object to camera-relative world, row-major 3x4 */
+} rb_instance;
+
+/* Emissive triangles are traced as their own instances, as the reference
+ * builds one GAS per emissive subset (src/core/rendering_interface.cpp:849-942);
+ * their primitive indices run over all subsets in order and index the
+ * light-tree triangle table. */
+typedef struct rb_emissive_subset {
+    float transform[12];         /* object to camera-relative world, row-major 3x4 */
+    uint32_t triangle_count;
+    const float* vertices;       /* triangle_count * 9 floats, object space */
+} rb_emissive_subset;
+
+typedef struct rb_geometry {
+    uint32_t mesh_count;
+    const rb_mesh* meshes;
+    uint32_t instance_count;
+    const rb_instance* instances;
+    uint32_t emissive_subset_count;
+    const rb_emissive_subset* emissive_subsets;
+} rb_geometry;
+
+/* Light tree in the reference's byte layouts: EmissiveTriangleLightData
+ * (68 B, src/core/light_tree_types.h:40-46), PackedNode (32 B, :119-163),
+ * LightPointer (4 B, :191-207) and the per-triangle 64-bit path bitmasks
+ * (src/core/light_tree.cpp:153-157). */
+typedef struct rb_light_tree {
+    uint32_t triangle_count;
+    const void* triangles;
+    uint32_t node_count;
+    const void* nodes;
+    uint32_t pointer_count;
+    const uint32_t* pointers;
+    const uint64_t* bitmasks;    /* triangle_count entries */
+} rb_light_tree;
+
+/* Launch parameters (LaunchParameters::ResolutionState / PathState /
+ * CameraState, src/core/launch_parameters.h:18-50). */
+typedef struct rb_launch {
+    uint32_t width, height;
+    float inv_width, inv_height;
+    float perspective_scale_w, perspective_scale_h;
+    uint32_t max_path_depth;
+    uint32_t max_reflected_depth;
+    uint32_t max_transmitted_depth;
+    float cam_u[3], cam_v[3], cam_w[3];
+    uint32_t dof_enabled;
+    float aperture;
+    float focus_distance;
+} rb_launch;
+
+typedef struct rb_device_status {
+    uint32_t flags;              /* RB_DEV_* bits accumulated since the last reset */
+    uint32_t first_code_detail;  /* implementation detail of the first failure */
+    uint64_t paths_traced;       /* paths finished since rb_create */
+    uint64_t rays_traced;        /* extension + shadow rays since rb_create */
+} rb_device_status;
+
+/* ---- context ---------------------------------------------------------- */
+int rb_create(const rb_config* config, rb_ctx** out);
+int rb_destroy(rb_ctx* ctx);
+const char* rb_last_error(const rb_ctx* ctx);
+int rb_abi_version(void);
+
+/* ---- scene upload (RenderingInterface data producers) ------------------ */
+/* Replaces loadLookUpTables' textures (src/core/rendering_interface.cpp:528-622):
+ * conductor 32x32, four dielectric 32x32x32 and sheen-LTC 32x32 float4, the
+ * layouts of bin/*.bin. */
+int rb_set_luts(rb_ctx* ctx, const float* conductor_albedo,
+                const float* dielectric_outer, const float* dielectric_inner,
+                const float* reflective_outer, const float* reflective_inner,
+                const float* sheen_ltc);
+/* Replaces fillSpectralCurvesData (:518) and the spectra table (:1198-1258):
+ * sensor curves X,Y,Z and RGB basis as 3 x 471 floats each, plus `extra`
+ * dense spectra (n_extra x 471) indexed by rb_material spectrum indices. */
+int rb_set_spectra(rb_ctx* ctx, const float* sensor_xyz, const float* basis_rgb,
+                   const float* extra, uint32_t n_extra);
+int rb_set_materials(rb_ctx* ctx, const rb_material* materials, uint32_t count);
+/* Replaces buildGeometryAccelerationStructures (:733), buildLightAccelerationStructure
+ * (:849) and updateInstanceAccelerationStructure (:943): builds the wide BVH. */
+int rb_set_geometry(rb_ctx* ctx, const rb_geometry* geometry);
+/* Replaces fillLightDataBuffer / fillLightTreeDataBuffers (:1433, :1470). */
+int rb_set_lights(rb_ctx* ctx, const rb_light_tree* tree);
+/* Host light-tree build (LightTree::Builder, src/core/light_tree.cpp:47-418,
+ * driven as RenderingInterface::buildLightTree, src/core/rendering_interface.cpp:
+ * 1065-1167): n emissive triangles with world-space vertices (9 floats each),
+ * flux (already scaled by the instance's flux correction), material and
+ * primitive indices, and the camera position. Writes the camera-relative
+ * EmissiveTriangleLightData records (n x 68 B), the PackedNode array
+ * (capacity 2n x 32 B), n light pointers and n path bitmasks, in the
+ * reference's layouts and order; *out_node_count receives the node count.
+ * Needs no device. */
+int rb_build_light_tree(uint32_t n, const float* world_vertices, const float* flux,
+                        const uint32_t* material, const uint32_t* primitive,
+                        const double* camera_position, void* out_triangles, void* out_nodes,
+                        uint32_t* out_pointers, uint64_t* out_bitmasks, uint32_t* out_node_count);
+/* Replaces loadEnvironmentMap's CDF launches (:1339-1432): rgba is w*h float4
+ * (w, h multiples of 4); the 2D CDF is built on the device. */
+int rb_set_envmap(rb_ctx* ctx, const float* rgba, uint32_t width, uint32_t height);
+int rb_clear_envmap(rb_ctx* ctx);
+int rb_set_launch(rb_ctx* ctx, const rb_launch* launch);
+
+/* ---- render (replaces optixLaunch, :1873-1879) ------------------------- */
+/* Renders samples [sample_offset, sample_offset + sample_count) of every pixel
+ * into the FP64 accumulation buffer. sample_offset == 0 restarts the
+ * accumulation (src/kernels/pathtrace.cu:1120). `stream` is a cudaStream_t or
+ * NULL for the library stream; the call is asynchronous with respect to the
+ * host. */
+int rb_render(rb_ctx* ctx, uint32_t sample_offset, uint32_t sample_count, void* stream);
+/* Copies the width*height*4 doubles (sum X, sum Y, sum Z, sample count) of
+ * the accumulation buffer (renderData) to host memory; synchronizes. */
+int rb_read_accum(rb_ctx* ctx, double* out);
+/* Device pointer of the accumulation buffer (width*height double4). */
+int rb_accum_device_ptr(rb_ctx* ctx, void** out);
+/* Stream-ordered copy of the accumulation buffer to `dst` (device or pinned
+ * host memory, width*height*4 doubles), on `stream` (NULL: context stream). */
+int rb_copy_accum_async(rb_ctx* ctx, void* dst, void* stream);
+int rb_status(rb_ctx* ctx, rb_device_status* out);
+int rb_clear_status(rb_ctx* ctx);
+int rb_synchronize(rb_ctx* ctx);
+
+/* ---- per-stage instrumentation (no counterpart in the reference, which has
+ * only -lineinfo; cudaEvent timers per stage) --------------------------- */
+#define RB_STATS_COUNT 1u   /* count traversal work: nodes and triangles visited (slower kernels) */
+#define RB_STATS_TIME  2u   /* time each kernel class with CUDA events on the render stream */
+typedef struct rb_render_stats {
+    uint64_t extend_rays, extend_nodes, extend_tris;
+    uint64_t shadow_rays, shadow_nodes, shadow_tris;
+    uint64_t waves;
+    double ms_generate, ms_extend, ms_shade, ms_shadow, ms_resolve;
+    uint32_t launches_generate, launches_extend, launches_shade, launches_shadow, launches_resolve;
+    uint32_t reserved;
+} rb_render_stats;
+int rb_set_stats(rb_ctx* ctx, uint32_t mode);
+/* Synchronizes, returns what was gathered since the last call, then resets. */
+int rb_get_stats(rb_ctx* ctx, rb_render_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RATBITE_B200_H */

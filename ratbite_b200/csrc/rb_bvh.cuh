@@ -1,0 +1,311 @@
+// Ray traversal of the 8-wide BVH (replaces OptiX's RT-core traversal behind
+// optixTrace / optixTraverse, src/kernels/pathtrace.cu:1162, 1708).
+//
+// One thread per ray. Nodes are 96 B with 8-bit quantized child boxes
+// (rb_scene.h); children that the ray enters are ordered near-to-far with a
+// sorting network held in registers, the nearest is descended directly and the
+// rest go on a short per-thread stack. Triangles use the watertight test of
+// Woop, Benthin and Wald (JCGT 2013) evaluated with explicitly rounded
+// operations (no FMA contraction) so distances and barycentrics are bitwise
+// reproducible on the CPU; closest-hit ties on t go to the smaller canonical
+// triangle id, which makes the result independent of traversal order.
+#pragma once
+
+#include "rb_math.cuh"
+#include "rb_scene.h"
+
+namespace rb
+{
+constexpr int kTraversalStack = 64;
+
+struct TraceRay
+{
+	f3 o, d;
+	float ix, iy, iz;         // safe reciprocal direction for box tests
+	int kx, ky, kz;
+	float sx, sy, sz;
+};
+
+RB_D float safeRcp(float d) { return 1.0f / (fabsf(d) < 1e-20f ? copysignf(1e-20f, d) : d); }
+
+RB_D float comp(f3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+RB_D TraceRay makeTraceRay(f3 o, f3 d)
+{
+	TraceRay r;
+	r.o = o; r.d = d;
+	r.ix = safeRcp(d.x); r.iy = safeRcp(d.y); r.iz = safeRcp(d.z);
+	const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+	r.kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+	r.kx = r.kz == 2 ? 0 : r.kz + 1;
+	r.ky = r.kx == 2 ? 0 : r.kx + 1;
+	if (comp(d, r.kz) < 0.0f) { const int t = r.kx; r.kx = r.ky; r.ky = t; }
+	const float dz = comp(d, r.kz);
+	r.sx = __fdiv_rn(comp(d, r.kx), dz);
+	r.sy = __fdiv_rn(comp(d, r.ky), dz);
+	r.sz = __fdiv_rn(1.0f, dz);
+	return r;
+}
+
+// Watertight ray/triangle test. Returns true for a hit with tmin < t < tmax
+// (t <= tmax when `inclusive`), writing t and the barycentrics of v1, v2.
+RB_D bool intersectTriangle(const TraceRay& r, f3 v0, f3 v1, f3 v2, float tmin, float tmax, bool inclusive,
+	float& t, float& b1, float& b2)
+{
+	const f3 A = mk(__fsub_rn(v0.x, r.o.x), __fsub_rn(v0.y, r.o.y), __fsub_rn(v0.z, r.o.z));
+	const f3 B = mk(__fsub_rn(v1.x, r.o.x), __fsub_rn(v1.y, r.o.y), __fsub_rn(v1.z, r.o.z));
+	const f3 C = mk(__fsub_rn(v2.x, r.o.x), __fsub_rn(v2.y, r.o.y), __fsub_rn(v2.z, r.o.z));
+	const float Akz = comp(A, r.kz), Bkz = comp(B, r.kz), Ckz = comp(C, r.kz);
+	const float Ax = __fsub_rn(comp(A, r.kx), __fmul_rn(r.sx, Akz));
+	const float Ay = __fsub_rn(comp(A, r.ky), __fmul_rn(r.sy, Akz));
+	const float Bx = __fsub_rn(comp(B, r.kx), __fmul_rn(r.sx, Bkz));
+	const float By = __fsub_rn(comp(B, r.ky), __fmul_rn(r.sy, Bkz));
+	const float Cx = __fsub_rn(comp(C, r.kx), __fmul_rn(r.sx, Ckz));
+	const float Cy = __fsub_rn(comp(C, r.ky), __fmul_rn(r.sy, Ckz));
+	float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+	float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+	float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+	if (U == 0.0f || V == 0.0f || W == 0.0f)
+	{
+		U = __double2float_rn(__dsub_rn(__dmul_rn(Cx, By), __dmul_rn(Cy, Bx)));
+		V = __double2float_rn(__dsub_rn(__dmul_rn(Ax, Cy), __dmul_rn(Ay, Cx)));
+		W = __double2float_rn(__dsub_rn(__dmul_rn(Bx, Ay), __dmul_rn(By, Ax)));
+	}
+	if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+	const float det = __fadd_rn(__fadd_rn(U, V), W);
+	if (det == 0.0f) return false;
+	const float Az = __fmul_rn(r.sz, Akz), Bz = __fmul_rn(r.sz, Bkz), Cz = __fmul_rn(r.sz, Ckz);
+	const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, Az), __fmul_rn(V, Bz)), __fmul_rn(W, Cz));
+	const float rcp = __fdiv_rn(1.0f, det);
+	const float tt = __fmul_rn(T, rcp);
+	if (!(tt > tmin && (inclusive ? tt <= tmax : tt < tmax))) return false;
+	t = tt;
+	b1 = __fmul_rn(V, rcp);
+	b2 = __fmul_rn(W, rcp);
+	return true;
+}
+
+struct NodeView
+{
+	float4 q[6];
+};
+RB_D NodeView loadNode(const BvhNode* nodes, uint32_t i)
+{
+	NodeView v;
+	const float4* p = reinterpret_cast<const float4*>(nodes + i);
+#pragma unroll
+	for (int k = 0; k < 6; ++k) v.q[k] = __ldg(p + k);
+	return v;
+}
+RB_D uint32_t nodeChild(const NodeView& v, int c)
+{
+	const float4& a = v.q[1 + c / 4];
+	const float w = (c & 3) == 0 ? a.x : ((c & 3) == 1 ? a.y : ((c & 3) == 2 ? a.z : a.w));
+	return __float_as_uint(w);
+}
+// Quantized byte of plane `k` (0..5: lo x,y,z, hi x,y,z) of child c.
+RB_D uint32_t nodeQ(const NodeView& v, int k, int c)
+{
+	const int byte = k * 8 + c;                 // offset inside the 48-byte box block
+	const float4& a = v.q[3 + byte / 16];
+	const int w = (byte % 16) / 4;
+	const uint32_t word = __float_as_uint(w == 0 ? a.x : (w == 1 ? a.y : (w == 2 ? a.z : a.w)));
+	return (word >> ((byte & 3) * 8)) & 0xFFu;
+}
+
+// Intersects the ray with the 8 child boxes; hitMask bit c set when child c
+// is entered within [tmin, tmax]; tnear[c] is its entry distance.
+RB_D uint32_t childBoxes(const TraceRay& r, const NodeView& v, float tmin, float tmax, float tnear[8])
+{
+	const float ox = v.q[0].x, oy = v.q[0].y, oz = v.q[0].z;
+	const uint32_t meta = __float_as_uint(v.q[0].w);
+	const float scx = __uint_as_float(((meta >> 0) & 0xFFu) << 23);
+	const float scy = __uint_as_float(((meta >> 8) & 0xFFu) << 23);
+	const float scz = __uint_as_float(((meta >> 16) & 0xFFu) << 23);
+	// Planes are rebuilt exactly (q * 2^e is exact, one rounding for the add)
+	// and intersected as (plane - o) / d, which keeps the error relative to
+	// the distance; the quantizer also pads every box by one step.
+	uint32_t mask = 0;
+#pragma unroll
+	for (int c = 0; c < 8; ++c)
+	{
+		const float lx = (__fmaf_rn(static_cast<float>(nodeQ(v, 0, c)), scx, ox) - r.o.x) * r.ix;
+		const float hx = (__fmaf_rn(static_cast<float>(nodeQ(v, 3, c)), scx, ox) - r.o.x) * r.ix;
+		const float ly = (__fmaf_rn(static_cast<float>(nodeQ(v, 1, c)), scy, oy) - r.o.y) * r.iy;
+		const float hy = (__fmaf_rn(static_cast<float>(nodeQ(v, 4, c)), scy, oy) - r.o.y) * r.iy;
+		const float lz = (__fmaf_rn(static_cast<float>(nodeQ(v, 2, c)), scz, oz) - r.o.z) * r.iz;
+		const float hz = (__fmaf_rn(static_cast<float>(nodeQ(v, 5, c)), scz, oz) - r.o.z) * r.iz;
+		const float n = fmaxf(fmaxf(fminf(lx, hx), fminf(ly, hy)), fmaxf(fminf(lz, hz), tmin));
+		const float f = fminf(fminf(fmaxf(lx, hx), fmaxf(ly, hy)), fminf(fmaxf(lz, hz), tmax)) * 1.0000004f;
+		tnear[c] = n;
+		if (n <= f && nodeChild(v, c) != kEmptyChild) mask |= 1u << c;
+	}
+	return mask;
+}
+
+RB_D void cswap(float& ka, uint32_t& va, float& kb, uint32_t& vb)
+{
+	if (kb < ka)
+	{
+		const float tk = ka; ka = kb; kb = tk;
+		const uint32_t tv = va; va = vb; vb = tv;
+	}
+}
+// Optimal 19-comparator sorting network for 8 keys.
+RB_D void sort8(float k[8], uint32_t v[8])
+{
+	cswap(k[0], v[0], k[2], v[2]); cswap(k[1], v[1], k[3], v[3]); cswap(k[4], v[4], k[6], v[6]); cswap(k[5], v[5], k[7], v[7]);
+	cswap(k[0], v[0], k[4], v[4]); cswap(k[1], v[1], k[5], v[5]); cswap(k[2], v[2], k[6], v[6]); cswap(k[3], v[3], k[7], v[7]);
+	cswap(k[0], v[0], k[1], v[1]); cswap(k[2], v[2], k[3], v[3]); cswap(k[4], v[4], k[5], v[5]); cswap(k[6], v[6], k[7], v[7]);
+	cswap(k[2], v[2], k[4], v[4]); cswap(k[3], v[3], k[5], v[5]);
+	cswap(k[1], v[1], k[4], v[4]); cswap(k[3], v[3], k[6], v[6]);
+	cswap(k[1], v[1], k[2], v[2]); cswap(k[3], v[3], k[4], v[4]); cswap(k[5], v[5], k[6], v[6]);
+}
+
+struct Hit
+{
+	int32_t tri;       // BVH-order triangle index, -1 on a miss
+	float t, b1, b2;
+};
+
+// Closest hit on (tmin, tmax). Sets RB_DEV_STACK_OVERFLOW in *status and
+// returns the best hit so far if the stack runs out. With COUNT, nNodes and
+// nTris count the wide nodes loaded and triangles tested.
+template<bool COUNT>
+RB_D Hit traceClosestT(const DevGeometry& g, f3 o, f3 d, float tmin, float tmax, uint32_t* status,
+	uint32_t& nNodes, uint32_t& nTris)
+{
+	Hit best{ -1, tmax, 0.0f, 0.0f };
+	if (g.triCount == 0) return best;
+	const TraceRay r = makeTraceRay(o, d);
+	uint32_t stackRef[kTraversalStack];
+	float stackT[kTraversalStack];
+	int sp = 0;
+	uint32_t bestId = 0xFFFFFFFFu;
+	uint32_t cur = g.rootIsLeaf ? (kLeafBit | (static_cast<uint32_t>(g.triCount - 1) << 28)) : 0u;
+	for (;;)
+	{
+		if (cur & kLeafBit)
+		{
+			const uint32_t first = cur & 0x0FFFFFFFu;
+			const uint32_t count = ((cur >> 28) & 0x7u) + 1u;
+			if (COUNT) nTris += count;
+			for (uint32_t i = first; i < first + count; ++i)
+			{
+				const float4 a = __ldg(g.triVerts + 3 * i);
+				const float4 b = __ldg(g.triVerts + 3 * i + 1);
+				const float4 c = __ldg(g.triVerts + 3 * i + 2);
+				float t, u, v;
+				if (intersectTriangle(r, f3_of(a), f3_of(b), f3_of(c), tmin, best.t, best.tri >= 0, t, u, v))
+				{
+					const uint32_t id = __float_as_uint(a.w);
+					if (best.tri < 0 || t < best.t || id < bestId)
+					{
+						best = Hit{ static_cast<int32_t>(i), t, u, v };
+						bestId = id;
+					}
+				}
+			}
+		}
+		else
+		{
+			if (COUNT) ++nNodes;
+			const NodeView nv = loadNode(g.nodes, cur);
+			float tn[8];
+			uint32_t mask = childBoxes(r, nv, tmin, best.t, tn);
+			if (mask)
+			{
+				float key[8];
+				uint32_t ref[8];
+#pragma unroll
+				for (int c = 0; c < 8; ++c)
+				{
+					key[c] = (mask >> c) & 1u ? tn[c] : INFINITY;
+					ref[c] = nodeChild(nv, c);
+				}
+				sort8(key, ref);
+				const int n = __popc(mask);
+				// push the far ones (n-1 .. 1), continue with the nearest
+#pragma unroll
+				for (int c = 7; c >= 1; --c)
+				{
+					if (c < n)
+					{
+						if (sp < kTraversalStack) { stackRef[sp] = ref[c]; stackT[sp] = key[c]; ++sp; }
+						else atomicOr(status, RB_DEV_STACK_OVERFLOW);
+					}
+				}
+				cur = ref[0];
+				continue;
+			}
+		}
+		// pop the next entry that may still hold a closer hit
+		bool found = false;
+		while (sp > 0)
+		{
+			--sp;
+			if (stackT[sp] <= best.t) { cur = stackRef[sp]; found = true; break; }
+		}
+		if (!found) break;
+	}
+	return best;
+}
+
+// Any hit on (tmin, tmax): occlusion test of a shadow ray.
+template<bool COUNT>
+RB_D bool traceAnyT(const DevGeometry& g, f3 o, f3 d, float tmin, float tmax, uint32_t* status,
+	uint32_t& nNodes, uint32_t& nTris)
+{
+	if (g.triCount == 0) return false;
+	const TraceRay r = makeTraceRay(o, d);
+	uint32_t stack[kTraversalStack];
+	int sp = 0;
+	uint32_t cur = g.rootIsLeaf ? (kLeafBit | (static_cast<uint32_t>(g.triCount - 1) << 28)) : 0u;
+	for (;;)
+	{
+		if (cur & kLeafBit)
+		{
+			const uint32_t first = cur & 0x0FFFFFFFu;
+			const uint32_t count = ((cur >> 28) & 0x7u) + 1u;
+			for (uint32_t i = first; i < first + count; ++i)
+			{
+				if (COUNT) ++nTris;
+				const float4 a = __ldg(g.triVerts + 3 * i);
+				const float4 b = __ldg(g.triVerts + 3 * i + 1);
+				const float4 c = __ldg(g.triVerts + 3 * i + 2);
+				float t, u, v;
+				if (intersectTriangle(r, f3_of(a), f3_of(b), f3_of(c), tmin, tmax, false, t, u, v)) return true;
+			}
+		}
+		else
+		{
+			if (COUNT) ++nNodes;
+			const NodeView nv = loadNode(g.nodes, cur);
+			float tn[8];
+			const uint32_t mask = childBoxes(r, nv, tmin, tmax, tn);
+#pragma unroll
+			for (int c = 0; c < 8; ++c)
+			{
+				if ((mask >> c) & 1u)
+				{
+					if (sp < kTraversalStack) stack[sp++] = nodeChild(nv, c);
+					else atomicOr(status, RB_DEV_STACK_OVERFLOW);
+				}
+			}
+		}
+		if (sp == 0) break;
+		cur = stack[--sp];
+	}
+	return false;
+}
+RB_D Hit traceClosest(const DevGeometry& g, f3 o, f3 d, float tmin, float tmax, uint32_t* status)
+{
+	uint32_t a = 0, b = 0;
+	return traceClosestT<false>(g, o, d, tmin, tmax, status, a, b);
+}
+RB_D bool traceAny(const DevGeometry& g, f3 o, f3 d, float tmin, float tmax, uint32_t* status)
+{
+	uint32_t a = 0, b = 0;
+	return traceAnyT<false>(g, o, d, tmin, tmax, status, a, b);
+}
+} // namespace rb

@@ -1,0 +1,20 @@
+// Host construction of the wide BVH (see rb_bvh_build.cpp).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "rb_scene.h"
+
+namespace rb
+{
+struct WideBvh
+{
+	std::vector<BvhNode> nodes;      // node 0 is the root unless rootIsLeaf
+	std::vector<uint32_t> triOrder;  // leaf order -> input triangle index
+	bool rootIsLeaf = false;         // <= kLeafMaxTris triangles: the root is one leaf
+};
+
+// worldVerts: 9 floats per triangle. Degenerate triangles must already be removed.
+WideBvh buildWideBvh(const std::vector<float>& worldVerts);
+} // namespace rb

@@ -1,0 +1,807 @@
+// C ABI of the renderer (include/ratbite_b200.h): context, scene upload,
+// geometry preparation, wavefront scheduling and readback.
+//
+// Compiled with -ffp-contract=off: the per-triangle values prepared here
+// (world-space vertices, encoded geometric normals, inverse transforms)
+// must be bitwise what the reference's closest-hit program computes from
+// the same inputs (src/kernels/pathtrace.cu:94-148).
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "ratbite_b200.h"
+#include "ratbite_b200_kernels.h"
+#include "rb_bvh_build.h"
+#include "rb_envmap.h"
+#include "rb_light.cuh"
+#include "rb_scene.h"
+#include "rb_wavefront.h"
+
+struct rb_ctx
+{
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	std::string error;
+	rb::DevScene scene{};
+	rb::LaunchShape shape{};
+	uint32_t* status = nullptr;          // [0] flags, [1] detail
+	// owned device buffers by role
+	std::vector<void*> lutBufs, spectraBufs, materialBufs, geoBufs, lightBufs, envBufs;
+	// wavefront state
+	rb::PathSoA soa{};
+	std::vector<void*> soaBufs;
+	uint32_t capacity = 0;
+	uint32_t requestedCapacity = 0;
+	double4* accum = nullptr;
+	size_t accumPixels = 0;
+	bool haveLaunch = false, haveGeometry = false;
+	uint64_t pathsTraced = 0;
+	// instrumentation (rb_set_stats)
+	uint32_t statsMode = 0;
+	unsigned long long* counters = nullptr;     // 6 device counters
+	struct Timed { int stage; cudaEvent_t a, b; };
+	std::vector<Timed> timed;
+	std::vector<cudaEvent_t> eventPool;
+	uint32_t launches[5] = {};
+	uint64_t waves = 0;
+};
+
+namespace
+{
+int fail(rb_ctx* ctx, int code, const std::string& msg)
+{
+	if (ctx) ctx->error = msg;
+	return code;
+}
+int cudaFail(rb_ctx* ctx, cudaError_t e, const char* what)
+{
+	return fail(ctx, e == cudaErrorMemoryAllocation ? RB_ERR_OOM : RB_ERR_CUDA,
+		std::string(what) + ": " + cudaGetErrorString(e));
+}
+void freeAll(std::vector<void*>& bufs)
+{
+	for (void* p : bufs) cudaFree(p);
+	bufs.clear();
+}
+// Allocates and uploads `bytes` from host `src` (may be null: zero fill).
+template<typename T>
+int upload(rb_ctx* ctx, std::vector<void*>& owner, const void* src, size_t bytes, T*& out)
+{
+	void* d = nullptr;
+	cudaError_t e = cudaMalloc(&d, std::max<size_t>(bytes, 16));
+	if (e != cudaSuccess) return cudaFail(ctx, e, "cudaMalloc");
+	owner.push_back(d);
+	e = src ? cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, ctx->stream)
+	        : cudaMemsetAsync(d, 0, std::max<size_t>(bytes, 16), ctx->stream);
+	if (e != cudaSuccess) return cudaFail(ctx, e, "upload");
+	out = static_cast<T*>(d);
+	return RB_OK;
+}
+cudaStream_t pick(rb_ctx* ctx, void* s) { return s ? static_cast<cudaStream_t>(s) : ctx->stream; }
+
+// Row-major 3x4 inverse in double, rounded once to float.
+void invert3x4(const float* m, float* out)
+{
+	const double a = m[0], b = m[1], c = m[2], d = m[4], e = m[5], f = m[6], g = m[8], h = m[9], i = m[10];
+	const double det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+	const double r = 1.0 / det;
+	const double inv[9] = {
+		(e * i - f * h) * r, (c * h - b * i) * r, (b * f - c * e) * r,
+		(f * g - d * i) * r, (a * i - c * g) * r, (c * d - a * f) * r,
+		(d * h - e * g) * r, (b * g - a * h) * r, (a * e - b * d) * r };
+	const double t[3] = { m[3], m[7], m[11] };
+	for (int row = 0; row < 3; ++row)
+	{
+		out[row * 4 + 0] = static_cast<float>(inv[row * 3 + 0]);
+		out[row * 4 + 1] = static_cast<float>(inv[row * 3 + 1]);
+		out[row * 4 + 2] = static_cast<float>(inv[row * 3 + 2]);
+		out[row * 4 + 3] = static_cast<float>(-(inv[row * 3 + 0] * t[0] + inv[row * 3 + 1] * t[1] + inv[row * 3 + 2] * t[2]));
+	}
+}
+// Object to world as the closest-hit program forms it: ((x*W0 + y*W1) + z*W2) + W3.
+void toWorld(const float* W, const float* p, float* o)
+{
+	o[0] = p[0] * W[0] + p[1] * W[1] + p[2] * W[2] + W[3];
+	o[1] = p[0] * W[4] + p[1] * W[5] + p[2] * W[6] + W[7];
+	o[2] = p[0] * W[8] + p[1] * W[9] + p[2] * W[10] + W[11];
+}
+// Encoded geometric normal of an object-space triangle under world-to-object
+// matrix Wi (pathtrace.cu:102-112): object-space cross product, transposed
+// inverse transform, correctly rounded reciprocal square root, octahedral code.
+uint32_t encodedNormal(const float* obj, const float* Wi)
+{
+	const float ux = obj[3] - obj[0], uy = obj[4] - obj[1], uz = obj[5] - obj[2];
+	const float vx = obj[6] - obj[0], vy = obj[7] - obj[1], vz = obj[8] - obj[2];
+	float gx = uy * vz - uz * vy, gy = uz * vx - ux * vz, gz = ux * vy - uy * vx;
+	const float nx = gx * Wi[0] + gy * Wi[4] + gz * Wi[8];
+	const float ny = gx * Wi[1] + gy * Wi[5] + gz * Wi[9];
+	const float nz = gx * Wi[2] + gy * Wi[6] + gz * Wi[10];
+	const float s = nx * nx + ny * ny + nz * nz;
+	const float r = static_cast<float>(1.0 / std::sqrt(static_cast<double>(s)));
+	return rb::octEncodeU32(rb::mk(nx * r, ny * r, nz * r));
+}
+uint32_t readIndex(const void* p, uint32_t type, size_t i)
+{
+	return type == RB_INDEX_U16 ? static_cast<const uint16_t*>(p)[i] : static_cast<const uint32_t*>(p)[i];
+}
+bool degenerate(const float* w)
+{
+	return (w[0] == w[3] && w[1] == w[4] && w[2] == w[5]) || (w[0] == w[6] && w[1] == w[7] && w[2] == w[8])
+		|| (w[3] == w[6] && w[4] == w[7] && w[5] == w[8]);
+}
+
+cudaEvent_t takeEvent(rb_ctx* ctx)
+{
+	if (!ctx->eventPool.empty())
+	{
+		cudaEvent_t e = ctx->eventPool.back();
+		ctx->eventPool.pop_back();
+		return e;
+	}
+	cudaEvent_t e = nullptr;
+	cudaEventCreate(&e);
+	return e;
+}
+// Runs `launch` bracketed by events when per-stage timing is on.
+template<typename F>
+void timedStage(rb_ctx* ctx, int stage, cudaStream_t st, F&& launch)
+{
+	++ctx->launches[stage];
+	if (!(ctx->statsMode & RB_STATS_TIME))
+	{
+		launch();
+		return;
+	}
+	rb_ctx::Timed t{ stage, takeEvent(ctx), takeEvent(ctx) };
+	cudaEventRecord(t.a, st);
+	launch();
+	cudaEventRecord(t.b, st);
+	ctx->timed.push_back(t);
+}
+
+void releaseWave(rb_ctx* ctx)
+{
+	freeAll(ctx->soaBufs);
+	ctx->soa = rb::PathSoA{};
+	ctx->capacity = 0;
+}
+int ensureWave(rb_ctx* ctx, uint32_t paths)
+{
+	if (ctx->capacity >= paths) return RB_OK;
+	releaseWave(ctx);
+	rb::PathSoA& s = ctx->soa;
+	int rc = RB_OK;
+	auto alloc = [&](auto*& p, size_t elem) {
+		if (rc != RB_OK) return;
+		rc = upload(ctx, ctx->soaBufs, nullptr, elem * paths, p);
+	};
+	alloc(s.rayO, sizeof(float4)); alloc(s.rayD, sizeof(float4)); alloc(s.lambda, sizeof(float4));
+	alloc(s.lpdf, sizeof(float4)); alloc(s.nrm, sizeof(float4)); alloc(s.L, sizeof(float4));
+	alloc(s.T, sizeof(float4)); alloc(s.fd, sizeof(uint2)); alloc(s.hit, sizeof(float4));
+	alloc(s.shO, sizeof(float4)); alloc(s.shD, sizeof(float4)); alloc(s.shC, sizeof(float4));
+	alloc(s.queue[0], sizeof(uint32_t)); alloc(s.queue[1], sizeof(uint32_t)); alloc(s.shadowQueue, sizeof(uint32_t));
+	if (rc == RB_OK)
+		rc = upload(ctx, ctx->soaBufs, nullptr, sizeof(uint32_t) * 2 * (rb::kMaxBounces + 1), s.counts);
+	if (rc != RB_OK) { releaseWave(ctx); return rc; }
+	s.capacity = paths;
+	ctx->capacity = paths;
+	return RB_OK;
+}
+} // namespace
+
+extern "C" {
+
+int rb_abi_version(void) { return RB_ABI_VERSION; }
+
+int rb_create(const rb_config* config, rb_ctx** out)
+{
+	if (!out) return RB_ERR_INVALID;
+	*out = nullptr;
+	rb_ctx* ctx = new (std::nothrow) rb_ctx();
+	if (!ctx) return RB_ERR_OOM;
+	ctx->device = config ? config->device : 0;
+	ctx->requestedCapacity = config ? config->max_paths_in_flight : 0u;
+	cudaError_t e = cudaSetDevice(ctx->device);
+	if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+	if (e == cudaSuccess) e = cudaMalloc(&ctx->status, 2 * sizeof(uint32_t));
+	if (e == cudaSuccess) e = cudaMemset(ctx->status, 0, 2 * sizeof(uint32_t));
+	if (e != cudaSuccess)
+	{
+		const int rc = e == cudaErrorMemoryAllocation ? RB_ERR_OOM : RB_ERR_CUDA;
+		if (ctx->stream) cudaStreamDestroy(ctx->stream);
+		delete ctx;
+		return rc;
+	}
+	ctx->scene.status = ctx->status;
+	ctx->shape = rb::queryLaunchShape();
+	*out = ctx;
+	return RB_OK;
+}
+
+int rb_destroy(rb_ctx* ctx)
+{
+	if (!ctx) return RB_ERR_INVALID;
+	cudaSetDevice(ctx->device);
+	cudaStreamSynchronize(ctx->stream);
+	for (auto* v : { &ctx->lutBufs, &ctx->spectraBufs, &ctx->materialBufs, &ctx->geoBufs, &ctx->lightBufs, &ctx->envBufs })
+		freeAll(*v);
+	releaseWave(ctx);
+	for (const auto& t : ctx->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+	for (cudaEvent_t e : ctx->eventPool) cudaEventDestroy(e);
+	if (ctx->counters) cudaFree(ctx->counters);
+	if (ctx->accum) cudaFree(ctx->accum);
+	if (ctx->status) cudaFree(ctx->status);
+	if (ctx->stream) cudaStreamDestroy(ctx->stream);
+	delete ctx;
+	return RB_OK;
+}
+
+const char* rb_last_error(const rb_ctx* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+
+int rb_set_luts(rb_ctx* ctx, const float* conductor, const float* dOuter, const float* dInner,
+	const float* rOuter, const float* rInner, const float* sheen)
+{
+	if (!ctx || !conductor || !dOuter || !dInner || !rOuter || !rInner || !sheen)
+		return fail(ctx, RB_ERR_INVALID, "rb_set_luts: null table");
+	cudaSetDevice(ctx->device);
+	cudaStreamSynchronize(ctx->stream);
+	freeAll(ctx->lutBufs);
+	const size_t n2 = rb::kLutN * rb::kLutN, n3 = n2 * rb::kLutN;
+	rb::DevLuts& L = ctx->scene.luts;
+	int rc = upload(ctx, ctx->lutBufs, conductor, n2 * 4, L.conductor);
+	if (rc == RB_OK) rc = upload(ctx, ctx->lutBufs, dOuter, n3 * 4, L.dielOuter);
+	if (rc == RB_OK) rc = upload(ctx, ctx->lutBufs, dInner, n3 * 4, L.dielInner);
+	if (rc == RB_OK) rc = upload(ctx, ctx->lutBufs, rOuter, n3 * 4, L.reflOuter);
+	if (rc == RB_OK) rc = upload(ctx, ctx->lutBufs, rInner, n3 * 4, L.reflInner);
+	if (rc == RB_OK) rc = upload(ctx, ctx->lutBufs, sheen, n2 * 16, L.sheen);
+	return rc;
+}
+
+int rb_set_spectra(rb_ctx* ctx, const float* sensor, const float* basis, const float* extra, uint32_t nExtra)
+{
+	if (!ctx || !sensor || !basis || (nExtra && !extra)) return fail(ctx, RB_ERR_INVALID, "rb_set_spectra: null table");
+	cudaSetDevice(ctx->device);
+	cudaStreamSynchronize(ctx->stream);
+	freeAll(ctx->spectraBufs);
+	const size_t b = sizeof(float) * rb::kSpectrumBins;
+	rb::DevSpectra& S = ctx->scene.spectra;
+	int rc = upload(ctx, ctx->spectraBufs, sensor, 3 * b, S.sensor);
+	if (rc == RB_OK) rc = upload(ctx, ctx->spectraBufs, basis, 3 * b, S.basis);
+	if (rc == RB_OK) rc = upload(ctx, ctx->spectraBufs, nExtra ? extra : nullptr, std::max<size_t>(nExtra, 1) * b, S.extra);
+	S.extraCount = nExtra;
+	return rc;
+}
+
+int rb_set_materials(rb_ctx* ctx, const rb_material* mats, uint32_t count)
+{
+	if (!ctx || (count && !mats)) return fail(ctx, RB_ERR_INVALID, "rb_set_materials: null materials");
+	cudaSetDevice(ctx->device);
+	cudaStreamSynchronize(ctx->stream);
+	freeAll(ctx->materialBufs);
+	std::vector<rb::DevMaterial> dm(std::max<uint32_t>(count, 1));
+	for (uint32_t i = 0; i < count; ++i)
+	{
+		const rb_material& m = mats[i];
+		if (m.textures != 0) return fail(ctx, RB_ERR_UNSUPPORTED, "rb_set_materials: textures are not supported");
+		if (m.bxdf > RB_BXDF_COMPLEX_SURFACE) return fail(ctx, RB_ERR_INVALID, "rb_set_materials: unknown bxdf");
+		if (m.index_type > RB_INDEX_U32) return fail(ctx, RB_ERR_INVALID, "rb_set_materials: unknown index type");
+		if ((m.attributes & (RB_ATTR_NORMAL | RB_ATTR_FRAME)) && (!m.attribute_data || m.attribute_stride == 0))
+			return fail(ctx, RB_ERR_INVALID, "rb_set_materials: attributes declared without attribute data");
+		rb::DevMaterial& d = dm[i];
+		d = rb::DevMaterial{};
+		d.bxdf = m.bxdf;
+		d.sheenPresent = m.sheen_present;
+		d.indexType = m.index_type;
+		d.attributes = m.attributes;
+		d.attributeStride = m.attribute_stride;
+		d.normalOffset = m.normal_offset;
+		d.frameOffset = m.frame_offset;
+		d.factors = m.factors;
+		d.iorSpectrum = m.ior_spectrum;
+		d.absorpSpectrum = m.absorp_spectrum;
+		d.mfRoughness = m.mf_roughness;
+		d.ior = m.ior;
+		d.alphaCutoff = m.alpha_cutoff;
+		d.metalness = m.metalness;
+		d.roughness = m.roughness;
+		d.transmission = m.transmission;
+		for (int k = 0; k < 4; ++k) d.baseColor[k] = m.base_color[k];
+		for (int k = 0; k < 3; ++k) { d.sheenColor[k] = m.sheen_color[k]; d.emissive[k] = m.emissive[k]; }
+		d.sheenRoughness = m.sheen_roughness;
+		d.triangleCount = m.triangle_count;
+		d.vertexCount = m.vertex_count;
+		const size_t ib = static_cast<size_t>(m.triangle_count) * 3 * (m.index_type == RB_INDEX_U16 ? 2 : 4);
+		if (m.triangle_count && !m.indices) return fail(ctx, RB_ERR_INVALID, "rb_set_materials: null indices");
+		uint8_t* dptr = nullptr;
+		int rc = upload(ctx, ctx->materialBufs, m.indices, ib, dptr);
+		if (rc != RB_OK) return rc;
+		d.indices = dptr;
+		const size_t ab = static_cast<size_t>(m.vertex_count) * m.attribute_stride;
+		rc = upload(ctx, ctx->materialBufs, m.attribute_data && ab ? m.attribute_data : nullptr, ab, dptr);
+		if (rc != RB_OK) return rc;
+		d.attributeData = dptr;
+	}
+	rb::DevMaterial* dptr = nullptr;
+	const int rc = upload(ctx, ctx->materialBufs, dm.data(), sizeof(rb::DevMaterial) * dm.size(), dptr);
+	if (rc != RB_OK) return rc;
+	ctx->scene.materials = dptr;
+	ctx->scene.materialCount = count;
+	return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? RB_OK : fail(ctx, RB_ERR_CUDA, "material upload");
+}
+
+int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
+{
+	if (!ctx || !g) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: null geometry");
+	if ((g->mesh_count && !g->meshes) || (g->instance_count && !g->instances) ||
+		(g->emissive_subset_count && !g->emissive_subsets))
+		return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: null array");
+	cudaSetDevice(ctx->device);
+	// Triangles in canonical order: emissive subsets, then instances x submeshes.
+	std::vector<float> world;          // 9 per kept triangle
+	std::vector<uint32_t> canon, inst, sbt, prim, enc;
+	std::vector<float> normalMatrix;   // 9 per instance
+	uint32_t instIndex = 0, canonical = 0, emissivePrim = 0;
+	auto addInstance = [&](const float* xf, float* wi) {
+		invert3x4(xf, wi);
+		const float nm[9] = { wi[0], wi[4], wi[8], wi[1], wi[5], wi[9], wi[2], wi[6], wi[10] };
+		normalMatrix.insert(normalMatrix.end(), nm, nm + 9);
+	};
+	auto addTriangle = [&](const float* obj, const float* xf, const float* wi, uint32_t instId, uint32_t sbtData, uint32_t primId) {
+		float w[9];
+		for (int k = 0; k < 3; ++k) toWorld(xf, obj + 3 * k, w + 3 * k);
+		const uint32_t id = canonical++;
+		for (float v : w) if (!std::isfinite(v)) return false;
+		if (degenerate(w) || degenerate(obj)) return true;
+		world.insert(world.end(), w, w + 9);
+		canon.push_back(id);
+		inst.push_back(instId);
+		sbt.push_back(sbtData);
+		prim.push_back(primId);
+		enc.push_back(encodedNormal(obj, wi));
+		return true;
+	};
+	for (uint32_t s = 0; s < g->emissive_subset_count; ++s)
+	{
+		const rb_emissive_subset& es = g->emissive_subsets[s];
+		if (es.triangle_count && !es.vertices) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: null emissive vertices");
+		float wi[12];
+		addInstance(es.transform, wi);
+		for (uint32_t t = 0; t < es.triangle_count; ++t)
+			if (!addTriangle(es.vertices + 9 * t, es.transform, wi, instIndex, 0xFFFFFFFFu, emissivePrim++))
+				return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: non-finite emissive vertex");
+		++instIndex;
+	}
+	for (uint32_t i = 0; i < g->instance_count; ++i)
+	{
+		const rb_instance& in = g->instances[i];
+		if (in.mesh >= g->mesh_count) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: instance mesh out of range");
+		float wi[12];
+		addInstance(in.transform, wi);
+		const rb_mesh& mesh = g->meshes[in.mesh];
+		if (mesh.submesh_count && !mesh.submeshes) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: null submeshes");
+		for (uint32_t s = 0; s < mesh.submesh_count; ++s)
+		{
+			const rb_submesh& sm = mesh.submeshes[s];
+			if (sm.triangle_count && (!sm.indices || !sm.vertices)) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: null submesh data");
+			if (sm.index_type > RB_INDEX_U32) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: unknown index type");
+			std::vector<uint8_t> discarded(sm.triangle_count, 0);
+			for (uint32_t k = 0; k < sm.discarded_count; ++k)
+				if (sm.discarded[k] < sm.triangle_count) discarded[sm.discarded[k]] = 1;
+			for (uint32_t t = 0; t < sm.triangle_count; ++t)
+			{
+				float obj[9];
+				for (int k = 0; k < 3; ++k)
+				{
+					const uint32_t vi = discarded[t] ? 0u : readIndex(sm.indices, sm.index_type, static_cast<size_t>(t) * 3 + k);
+					if (vi >= sm.vertex_count) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: vertex index out of range");
+					obj[3 * k + 0] = sm.vertices[4 * vi + 0];
+					obj[3 * k + 1] = sm.vertices[4 * vi + 1];
+					obj[3 * k + 2] = sm.vertices[4 * vi + 2];
+				}
+				if (!addTriangle(obj, in.transform, wi, instIndex, sm.material, t))
+					return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: non-finite vertex");
+			}
+		}
+		++instIndex;
+	}
+	const rb::WideBvh bvh = rb::buildWideBvh(world);
+	const size_t nt = canon.size();
+	std::vector<float4> triVerts(3 * std::max<size_t>(nt, 1));
+	std::vector<uint2> triAux(std::max<size_t>(nt, 1));
+	for (size_t j = 0; j < nt; ++j)
+	{
+		const uint32_t t = bvh.triOrder[j];
+		const float* w = world.data() + 9 * t;
+		float4 a, b, c;
+		a.x = w[0]; a.y = w[1]; a.z = w[2]; std::memcpy(&a.w, &canon[t], 4);
+		b.x = w[3]; b.y = w[4]; b.z = w[5]; std::memcpy(&b.w, &inst[t], 4);
+		c.x = w[6]; c.y = w[7]; c.z = w[8]; std::memcpy(&c.w, &sbt[t], 4);
+		triVerts[3 * j] = a; triVerts[3 * j + 1] = b; triVerts[3 * j + 2] = c;
+		triAux[j] = make_uint2(enc[t], prim[t]);
+	}
+	cudaStreamSynchronize(ctx->stream);
+	freeAll(ctx->geoBufs);
+	rb::DevGeometry& G = ctx->scene.geo;
+	G = rb::DevGeometry{};
+	int rc = upload(ctx, ctx->geoBufs, bvh.nodes.empty() ? nullptr : bvh.nodes.data(),
+		sizeof(rb::BvhNode) * std::max<size_t>(bvh.nodes.size(), 1), G.nodes);
+	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, triVerts.data(), sizeof(float4) * triVerts.size(), G.triVerts);
+	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, triAux.data(), sizeof(uint2) * triAux.size(), G.triAux);
+	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, normalMatrix.empty() ? nullptr : normalMatrix.data(),
+		sizeof(float) * std::max<size_t>(normalMatrix.size(), 9), G.normalMatrix);
+	if (rc != RB_OK) return rc;
+	G.nodeCount = static_cast<uint32_t>(bvh.nodes.size());
+	G.triCount = static_cast<uint32_t>(nt);
+	G.rootIsLeaf = bvh.rootIsLeaf ? 1u : 0u;
+	ctx->haveGeometry = true;
+	return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? RB_OK : fail(ctx, RB_ERR_CUDA, "geometry upload");
+}
+
+int rb_set_lights(rb_ctx* ctx, const rb_light_tree* t)
+{
+	if (!ctx || !t) return fail(ctx, RB_ERR_INVALID, "rb_set_lights: null tree");
+	if (t->triangle_count && (!t->triangles || !t->bitmasks)) return fail(ctx, RB_ERR_INVALID, "rb_set_lights: null triangles");
+	if (t->node_count && (!t->nodes || !t->pointers)) return fail(ctx, RB_ERR_INVALID, "rb_set_lights: null nodes");
+	cudaSetDevice(ctx->device);
+	// Validate the node graph so device code never indexes out of range.
+	const rb::PackedNode* nodes = static_cast<const rb::PackedNode*>(t->nodes);
+	for (uint32_t i = 0; i < t->node_count; ++i)
+	{
+		const uint32_t core = nodes[i].core;
+		if (core >> 31)
+		{
+			const uint32_t cnt = (core >> 27) & 0xFu, off = core & ((1u << 27) - 1u);
+			if (cnt == 0 || off + cnt > t->pointer_count) return fail(ctx, RB_ERR_INVALID, "rb_set_lights: leaf out of range");
+		}
+		else if (core >= t->node_count || i + 1 >= t->node_count)
+			return fail(ctx, RB_ERR_INVALID, "rb_set_lights: child index out of range");
+	}
+	for (uint32_t i = 0; i < t->pointer_count; ++i)
+	{
+		const uint32_t type = t->pointers[i] >> 30, idx = t->pointers[i] & ((1u << 30) - 1u);
+		if (type == rb::kLightTypeTriangle && idx >= t->triangle_count)
+			return fail(ctx, RB_ERR_INVALID, "rb_set_lights: light pointer out of range");
+	}
+	cudaStreamSynchronize(ctx->stream);
+	freeAll(ctx->lightBufs);
+	rb::DevLights& L = ctx->scene.lights;
+	L = rb::DevLights{};
+	int rc = upload(ctx, ctx->lightBufs, t->triangles, sizeof(rb::EmissiveTri) * t->triangle_count, L.triangles);
+	if (rc == RB_OK) rc = upload(ctx, ctx->lightBufs, t->bitmasks, sizeof(uint64_t) * t->triangle_count, L.bitmasks);
+	if (rc == RB_OK) rc = upload(ctx, ctx->lightBufs, t->pointers, sizeof(uint32_t) * t->pointer_count, L.pointers);
+	rb::PackedNode* dn = nullptr;
+	if (rc == RB_OK && t->node_count) rc = upload(ctx, ctx->lightBufs, t->nodes, sizeof(rb::PackedNode) * t->node_count, dn);
+	if (rc != RB_OK) return rc;
+	L.nodes = dn;
+	L.nodeCount = t->node_count;
+	L.triangleCount = t->triangle_count;
+	return RB_OK;
+}
+
+int rb_set_envmap(rb_ctx* ctx, const float* rgba, uint32_t w, uint32_t h)
+{
+	if (!ctx || !rgba) return fail(ctx, RB_ERR_INVALID, "rb_set_envmap: null image");
+	if (w < 4 || h < 4 || (w % 4) != 0 || (h % 4) != 0)
+		return fail(ctx, RB_ERR_INVALID, "rb_set_envmap: width and height must be multiples of 4");
+	if (w > 32768 || h > 32768) return fail(ctx, RB_ERR_INVALID, "rb_set_envmap: image larger than 32768");
+	cudaSetDevice(ctx->device);
+	cudaStreamSynchronize(ctx->stream);
+	freeAll(ctx->envBufs);
+	rb::DevEnvMap& E = ctx->scene.env;
+	E = rb::DevEnvMap{};
+	float4* tex = nullptr;
+	uint16_t *cond = nullptr, *marg = nullptr;
+	float* integral = nullptr;
+	void* scratch = nullptr;
+	int rc = upload(ctx, ctx->envBufs, rgba, sizeof(float4) * w * h, tex);
+	if (rc == RB_OK) rc = upload(ctx, ctx->envBufs, nullptr, sizeof(uint16_t) * w * h, cond);
+	if (rc == RB_OK) rc = upload(ctx, ctx->envBufs, nullptr, sizeof(uint16_t) * h, marg);
+	if (rc == RB_OK) rc = upload(ctx, ctx->envBufs, nullptr, sizeof(float), integral);
+	if (rc == RB_OK) rc = upload(ctx, ctx->envBufs, nullptr, rb_envmap_cdf_scratch_bytes(w, h), scratch);
+	if (rc != RB_OK) return rc;
+	rc = rb_envmap_cdf(w, h, reinterpret_cast<const float*>(tex), 1, scratch, cond, marg, integral, ctx->stream);
+	if (rc != RB_OK) return fail(ctx, rc, "rb_set_envmap: CDF build failed");
+	float hi = 0.0f;
+	cudaError_t e = cudaMemcpyAsync(&hi, integral, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+	if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+	if (e != cudaSuccess) return cudaFail(ctx, e, "rb_set_envmap");
+	E.enabled = 1;
+	E.w = w; E.h = h;
+	E.width = static_cast<float>(w); E.height = static_cast<float>(h);
+	E.integral = hi;
+	E.texels = tex;
+	E.conditional = cond;
+	E.marginal = marg;
+	return RB_OK;
+}
+
+int rb_clear_envmap(rb_ctx* ctx)
+{
+	if (!ctx) return RB_ERR_INVALID;
+	cudaSetDevice(ctx->device);
+	cudaStreamSynchronize(ctx->stream);
+	freeAll(ctx->envBufs);
+	ctx->scene.env = rb::DevEnvMap{};
+	return RB_OK;
+}
+
+int rb_set_launch(rb_ctx* ctx, const rb_launch* l)
+{
+	if (!ctx || !l) return fail(ctx, RB_ERR_INVALID, "rb_set_launch: null launch");
+	if (l->width == 0 || l->height == 0) return fail(ctx, RB_ERR_INVALID, "rb_set_launch: empty film");
+	if (static_cast<uint64_t>(l->width) * l->height > (1ull << 31)) return fail(ctx, RB_ERR_INVALID, "rb_set_launch: film too large");
+	if (l->max_path_depth == 0 || l->max_path_depth > rb::kMaxBounces || l->max_reflected_depth > rb::kMaxBounces ||
+		l->max_transmitted_depth > rb::kMaxBounces)
+		return fail(ctx, RB_ERR_INVALID, "rb_set_launch: path depth must be in [1, 64]");
+	cudaSetDevice(ctx->device);
+	rb::DevLaunch& D = ctx->scene.launch;
+	D.width = l->width; D.height = l->height;
+	D.invWidth = l->inv_width; D.invHeight = l->inv_height;
+	D.perspW = l->perspective_scale_w; D.perspH = l->perspective_scale_h;
+	D.maxDepth = l->max_path_depth; D.maxReflected = l->max_reflected_depth; D.maxTransmitted = l->max_transmitted_depth;
+	for (int k = 0; k < 3; ++k) { D.camU[k] = l->cam_u[k]; D.camV[k] = l->cam_v[k]; D.camW[k] = l->cam_w[k]; }
+	D.dof = l->dof_enabled; D.aperture = l->aperture; D.focusDistance = l->focus_distance;
+	const size_t pixels = static_cast<size_t>(l->width) * l->height;
+	if (pixels != ctx->accumPixels)
+	{
+		cudaStreamSynchronize(ctx->stream);
+		if (ctx->accum) cudaFree(ctx->accum);
+		ctx->accum = nullptr;
+		ctx->accumPixels = 0;
+		const cudaError_t e = cudaMalloc(&ctx->accum, sizeof(double4) * pixels);
+		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_set_launch: accumulation buffer");
+		cudaMemsetAsync(ctx->accum, 0, sizeof(double4) * pixels, ctx->stream);
+		ctx->accumPixels = pixels;
+	}
+	ctx->haveLaunch = true;
+	return RB_OK;
+}
+
+int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
+{
+	if (!ctx) return RB_ERR_INVALID;
+	if (!ctx->haveLaunch || !ctx->haveGeometry || !ctx->scene.materials || !ctx->scene.spectra.sensor || !ctx->scene.luts.conductor)
+		return fail(ctx, RB_ERR_NO_SCENE, "rb_render: launch, geometry, materials, spectra and LUTs must be set first");
+	if (count == 0) return RB_OK;
+	cudaSetDevice(ctx->device);
+	const cudaStream_t st = pick(ctx, stream);
+	const rb::DevScene& sc = ctx->scene;
+	const uint32_t pixels = sc.launch.width * sc.launch.height;
+	// Wave size: whole sample planes, up to the capacity (default 4M paths).
+	const uint64_t cap = ctx->requestedCapacity ? ctx->requestedCapacity : (4u << 20);
+	const uint32_t planesPerWave = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(count, cap / pixels)));
+	const uint32_t wavePaths = planesPerWave * pixels;
+	int rc = ensureWave(ctx, wavePaths);
+	if (rc != RB_OK) return rc;
+	const int bounces = static_cast<int>(std::min<uint32_t>(rb::kMaxBounces,
+		std::max({ sc.launch.maxDepth, sc.launch.maxReflected, sc.launch.maxTransmitted })));
+	for (uint32_t done = 0; done < count;)
+	{
+		const uint32_t planes = std::min(planesPerWave, count - done);
+		rb::WaveParams w{ planes * pixels, pixels, offset + done, (offset == 0 && done == 0) ? 1u : 0u };
+		unsigned long long* cnt = (ctx->statsMode & RB_STATS_COUNT) ? ctx->counters : nullptr;
+		cudaMemsetAsync(ctx->soa.counts, 0, sizeof(uint32_t) * 2 * (rb::kMaxBounces + 1), st);
+		timedStage(ctx, 0, st, [&] { rb::launchGenerate(sc, ctx->soa, w, ctx->shape, st); });
+		for (int b = 0; b < bounces; ++b)
+		{
+			timedStage(ctx, 1, st, [&] { rb::launchExtend(sc, ctx->soa, b, ctx->shape, st, cnt); });
+			timedStage(ctx, 2, st, [&] { rb::launchShade(sc, ctx->soa, w, b, ctx->shape, st); });
+			timedStage(ctx, 3, st, [&] { rb::launchShadow(sc, ctx->soa, b, ctx->shape, st, cnt); });
+		}
+		timedStage(ctx, 4, st, [&] { rb::launchResolve(sc, ctx->soa, w, ctx->accum, ctx->shape, st); });
+		done += planes;
+		ctx->pathsTraced += w.paths;
+		++ctx->waves;
+	}
+	const cudaError_t e = cudaGetLastError();
+	if (e != cudaSuccess) return cudaFail(ctx, e, "rb_render launch");
+	return RB_OK;
+}
+
+int rb_read_accum(rb_ctx* ctx, double* out)
+{
+	if (!ctx || !out) return RB_ERR_INVALID;
+	if (!ctx->accum) return fail(ctx, RB_ERR_NO_SCENE, "rb_read_accum: no accumulation buffer");
+	cudaSetDevice(ctx->device);
+	cudaError_t e = cudaStreamSynchronize(ctx->stream);
+	if (e == cudaSuccess) e = cudaDeviceSynchronize();
+	if (e == cudaSuccess) e = cudaMemcpy(out, ctx->accum, sizeof(double4) * ctx->accumPixels, cudaMemcpyDeviceToHost);
+	if (e != cudaSuccess) return cudaFail(ctx, e, "rb_read_accum");
+	return RB_OK;
+}
+
+int rb_accum_device_ptr(rb_ctx* ctx, void** out)
+{
+	if (!ctx || !out) return RB_ERR_INVALID;
+	*out = ctx->accum;
+	return ctx->accum ? RB_OK : fail(ctx, RB_ERR_NO_SCENE, "no accumulation buffer");
+}
+
+int rb_copy_accum_async(rb_ctx* ctx, void* dst, void* stream)
+{
+	if (!ctx || !dst) return RB_ERR_INVALID;
+	if (!ctx->accum) return fail(ctx, RB_ERR_NO_SCENE, "rb_copy_accum_async: no accumulation buffer");
+	cudaSetDevice(ctx->device);
+	const cudaError_t e = cudaMemcpyAsync(dst, ctx->accum, sizeof(double4) * ctx->accumPixels, cudaMemcpyDefault,
+		pick(ctx, stream));
+	return e == cudaSuccess ? RB_OK : cudaFail(ctx, e, "rb_copy_accum_async");
+}
+
+int rb_status(rb_ctx* ctx, rb_device_status* out)
+{
+	if (!ctx || !out) return RB_ERR_INVALID;
+	cudaSetDevice(ctx->device);
+	uint32_t h[2] = { 0, 0 };
+	cudaError_t e = cudaDeviceSynchronize();
+	if (e == cudaSuccess) e = cudaMemcpy(h, ctx->status, sizeof(h), cudaMemcpyDeviceToHost);
+	if (e != cudaSuccess) return cudaFail(ctx, e, "rb_status");
+	out->flags = h[0];
+	out->first_code_detail = h[1];
+	out->paths_traced = ctx->pathsTraced;
+	out->rays_traced = 0;
+	return RB_OK;
+}
+
+int rb_clear_status(rb_ctx* ctx)
+{
+	if (!ctx) return RB_ERR_INVALID;
+	cudaSetDevice(ctx->device);
+	return cudaMemset(ctx->status, 0, 2 * sizeof(uint32_t)) == cudaSuccess ? RB_OK : RB_ERR_CUDA;
+}
+
+int rb_synchronize(rb_ctx* ctx)
+{
+	if (!ctx) return RB_ERR_INVALID;
+	cudaSetDevice(ctx->device);
+	const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+	return e == cudaSuccess ? RB_OK : cudaFail(ctx, e, "rb_synchronize");
+}
+
+int rb_set_stats(rb_ctx* ctx, uint32_t mode)
+{
+	if (!ctx || (mode & ~(RB_STATS_COUNT | RB_STATS_TIME))) return fail(ctx, RB_ERR_INVALID, "rb_set_stats: bad mode");
+	cudaSetDevice(ctx->device);
+	if ((mode & RB_STATS_COUNT) && !ctx->counters)
+	{
+		const cudaError_t e = cudaMalloc(&ctx->counters, 6 * sizeof(unsigned long long));
+		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_set_stats");
+		cudaMemset(ctx->counters, 0, 6 * sizeof(unsigned long long));
+	}
+	ctx->statsMode = mode;
+	return RB_OK;
+}
+
+int rb_get_stats(rb_ctx* ctx, rb_render_stats* out)
+{
+	if (!ctx || !out) return RB_ERR_INVALID;
+	cudaSetDevice(ctx->device);
+	cudaError_t e = cudaStreamSynchronize(ctx->stream);
+	if (e == cudaSuccess) e = cudaDeviceSynchronize();
+	if (e != cudaSuccess) return cudaFail(ctx, e, "rb_get_stats");
+	*out = rb_render_stats{};
+	if (ctx->counters)
+	{
+		unsigned long long c[6] = {};
+		cudaMemcpy(c, ctx->counters, sizeof(c), cudaMemcpyDeviceToHost);
+		cudaMemset(ctx->counters, 0, sizeof(c));
+		out->extend_rays = c[0]; out->extend_nodes = c[1]; out->extend_tris = c[2];
+		out->shadow_rays = c[3]; out->shadow_nodes = c[4]; out->shadow_tris = c[5];
+	}
+	double ms[5] = {};
+	for (const auto& t : ctx->timed)
+	{
+		float v = 0.0f;
+		if (cudaEventElapsedTime(&v, t.a, t.b) == cudaSuccess) ms[t.stage] += v;
+		ctx->eventPool.push_back(t.a);
+		ctx->eventPool.push_back(t.b);
+	}
+	ctx->timed.clear();
+	out->ms_generate = ms[0]; out->ms_extend = ms[1]; out->ms_shade = ms[2]; out->ms_shadow = ms[3]; out->ms_resolve = ms[4];
+	out->launches_generate = ctx->launches[0]; out->launches_extend = ctx->launches[1];
+	out->launches_shade = ctx->launches[2]; out->launches_shadow = ctx->launches[3]; out->launches_resolve = ctx->launches[4];
+	out->waves = ctx->waves;
+	for (uint32_t& l : ctx->launches) l = 0;
+	ctx->waves = 0;
+	return RB_OK;
+}
+
+// ---- per-function entry points ----------------------------------------
+#define RB_K_CHECK(cond) do { if (!(cond)) return RB_ERR_INVALID; } while (0)
+static int lastLaunch()
+{
+	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
+}
+
+int rb_k_sobol(uint32_t n, uint32_t dims, const uint32_t* sample, const uint32_t* hash, const uint32_t* bounce,
+	const uint32_t* dim, float* out, void* stream)
+{
+	RB_K_CHECK(dims >= 1 && dims <= 3);
+	if (n == 0) return RB_OK;
+	RB_K_CHECK(sample && hash && bounce && dim && out);
+	rb::launchSobol(n, dims, sample, hash, bounce, dim, out, static_cast<cudaStream_t>(stream));
+	return lastLaunch();
+}
+int rb_k_pixel_hash(uint32_t n, const uint32_t* x, const uint32_t* y, uint32_t* out, void* stream)
+{
+	if (n == 0) return RB_OK;
+	RB_K_CHECK(x && y && out);
+	rb::launchPixelHash(n, x, y, out, static_cast<cudaStream_t>(stream));
+	return lastLaunch();
+}
+int rb_k_wavelengths(uint32_t n, const float* u, float* lambda, float* pdf, void* stream)
+{
+	if (n == 0) return RB_OK;
+	RB_K_CHECK(u && lambda && pdf);
+	rb::launchWavelengths(n, u, lambda, pdf, static_cast<cudaStream_t>(stream));
+	return lastLaunch();
+}
+int rb_k_camera_ray(rb_ctx* ctx, uint32_t n, const float* pixel, const float* fuv, const float* luv, float* out, void* stream)
+{
+	RB_K_CHECK(ctx && ctx->haveLaunch);
+	if (n == 0) return RB_OK;
+	RB_K_CHECK(pixel && fuv && luv && out);
+	rb::launchCameraRay(ctx->scene, n, pixel, fuv, luv, out, pick(ctx, stream));
+	return lastLaunch();
+}
+int rb_k_bxdf(rb_ctx* ctx, uint32_t n, rb_bxdf_case* cases, void* stream)
+{
+	RB_K_CHECK(ctx && ctx->scene.materials && ctx->scene.luts.conductor && ctx->scene.spectra.basis);
+	if (n == 0) return RB_OK;
+	RB_K_CHECK(cases);
+	rb::launchBxdfCases(ctx->scene, n, cases, pick(ctx, stream));
+	return lastLaunch();
+}
+int rb_k_light_tree(rb_ctx* ctx, uint32_t n, rb_light_case* cases, void* stream)
+{
+	RB_K_CHECK(ctx && (ctx->scene.lights.nodes || ctx->scene.env.enabled));
+	if (n == 0) return RB_OK;
+	RB_K_CHECK(cases);
+	rb::launchLightCases(ctx->scene, n, cases, pick(ctx, stream));
+	return lastLaunch();
+}
+int rb_k_offset_point(uint32_t n, const float* p, const float* nrm, float* out, void* stream)
+{
+	if (n == 0) return RB_OK;
+	RB_K_CHECK(p && nrm && out);
+	rb::launchOffsetPoint(n, p, nrm, out, static_cast<cudaStream_t>(stream));
+	return lastLaunch();
+}
+int rb_k_oct_encode(uint32_t n, const float* v, uint32_t* out, void* stream)
+{
+	if (n == 0) return RB_OK;
+	RB_K_CHECK(v && out);
+	rb::launchOctEncode(n, v, out, static_cast<cudaStream_t>(stream));
+	return lastLaunch();
+}
+int rb_k_oct_decode(uint32_t n, const uint32_t* code, float* out, void* stream)
+{
+	if (n == 0) return RB_OK;
+	RB_K_CHECK(code && out);
+	rb::launchOctDecode(n, code, out, static_cast<cudaStream_t>(stream));
+	return lastLaunch();
+}
+int rb_k_trace(rb_ctx* ctx, uint32_t n, const float* rays, uint32_t* payload, float* t, int32_t* tri, void* stream)
+{
+	RB_K_CHECK(ctx && ctx->haveGeometry);
+	if (n == 0) return RB_OK;
+	RB_K_CHECK(rays && payload && t && tri);
+	rb::launchTrace(ctx->scene, n, rays, payload, t, tri, pick(ctx, stream));
+	return lastLaunch();
+}
+int rb_k_occluded(rb_ctx* ctx, uint32_t n, const float* rays, const float* tmax, uint32_t* out, void* stream)
+{
+	RB_K_CHECK(ctx && ctx->haveGeometry);
+	if (n == 0) return RB_OK;
+	RB_K_CHECK(rays && tmax && out);
+	rb::launchOccluded(ctx->scene, n, rays, tmax, out, pick(ctx, stream));
+	return lastLaunch();
+}
+
+} // extern "C"

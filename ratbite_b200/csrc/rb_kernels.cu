@@ -1,0 +1,875 @@
+// Wavefront rendering kernels and per-function batch kernels.
+//
+// One wave renders whole sample planes of the image. Per bounce:
+//   extend  - closest hit of every active path (rb_bvh.cuh)
+//   shade   - the body of the reference's bounce loop
+//             (src/kernels/pathtrace.cu:1179-1785): hit emission with MIS,
+//             shading frame and material, light-tree / environment light
+//             sample, BxDF sample, Russian roulette, next ray; continuing
+//             paths go to the next queue, light samples to the shadow queue
+//   shadow  - any-hit test of the light samples; unoccluded ones add their
+//             contribution to L
+// and after the last bounce
+//   resolve - L / pdf -> XYZ, summed into the FP64 accumulation in sample
+//             order per pixel (pathtrace.cu:1789-1812), so the result does
+//             not depend on the order in which paths were processed.
+// Kernels are persistent: the grid is sized from the SM count and occupancy,
+// and each one reads its work count from device memory, so a whole wave is a
+// fixed launch sequence with no host round trip.
+
+#include <cfloat>
+
+#include "rb_bvh.cuh"
+#include "rb_bxdf.cuh"
+#include "rb_light.cuh"
+#include "rb_qrng.cuh"
+#include "rb_wavefront.h"
+#include "ratbite_b200_kernels.h"
+
+namespace rb
+{
+namespace
+{
+constexpr int kThreads = 128;
+
+RB_D uint32_t gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+RB_D uint32_t gstride() { return gridDim.x * blockDim.x; }
+
+// Warp-aggregated append: one atomic per warp for the lanes that push.
+RB_D uint32_t appendIndex(uint32_t* counter)
+{
+	const uint32_t active = __activemask();
+	const int leader = __ffs(active) - 1;
+	const uint32_t lane = threadIdx.x & 31u;
+	uint32_t base = 0;
+	if (lane == static_cast<uint32_t>(leader)) base = atomicAdd(counter, __popc(active));
+	base = __shfl_sync(active, base, leader);
+	return base + __popc(active & ((1u << lane) - 1u));
+}
+
+RB_D f3 mulMat(const float* m, f3 v)   // rows of 3
+{
+	return f3{ m[0] * v.x + m[1] * v.y + m[2] * v.z, m[3] * v.x + m[4] * v.y + m[5] * v.z,
+	           m[6] * v.x + m[7] * v.y + m[8] * v.z };
+}
+
+// Rotation matrix columns of a unit quaternion (glm::mat3_cast order of operations).
+RB_D void quatColumns(float4 q, f3& c0, f3& c2)
+{
+	const float qxx = q.x * q.x, qyy = q.y * q.y, qzz = q.z * q.z;
+	const float qxz = q.x * q.z, qxy = q.x * q.y, qyz = q.y * q.z;
+	const float qwx = q.w * q.x, qwy = q.w * q.y, qwz = q.w * q.z;
+	c0 = mk(1.0f - 2.0f * (qyy + qzz), 2.0f * (qxy + qwz), 2.0f * (qxz - qwy));
+	c2 = mk(2.0f * (qxz + qwy), 2.0f * (qyz - qwx), 1.0f - 2.0f * (qxx + qyy));
+}
+
+// Branchless orthonormal tangent of a unit normal (pathtrace.cu:1374-1377, 1408-1413).
+RB_D f3 tangentOf(f3 n)
+{
+	const float sign = copysignf(1.0f, n.z);
+	const float a = -1.0f / (sign + n.z);
+	const float b = n.x * n.y * a;
+	return mk(1.0f + sign * (n.x * n.x) * a, sign * b, -sign * n.x);
+}
+
+// Surface interaction reconstructed from a hit (unpackInteractionData,
+// pathtrace.cu:908-953, with the closest-hit program's payload, :86-149).
+struct Interaction
+{
+	f3 hitPos, hitPosInterp, gn;
+	f3 v0, v1, v2;
+	float b1, b2;
+	uint32_t lightType, lightIndex, material, prim;
+	uint32_t instance;
+	bool backHit;
+};
+
+RB_D void unpackHit(const DevScene& sc, float4 h, f3 rayD, Interaction& it)
+{
+	const int tri = __float_as_int(h.x);
+	if (tri < 0)
+	{
+		it.lightType = kLightTypeSky;
+		it.lightIndex = 0;
+		it.material = 0;
+		it.gn = octDecodeU32(0u);
+		it.backHit = dot(it.gn, rayD) > 0.0f;
+		return;
+	}
+	const float4 a = __ldg(sc.geo.triVerts + 3 * tri);
+	const float4 b = __ldg(sc.geo.triVerts + 3 * tri + 1);
+	const float4 c = __ldg(sc.geo.triVerts + 3 * tri + 2);
+	const uint2 aux = __ldg(sc.geo.triAux + tri);
+	it.v0 = f3_of(a); it.v1 = f3_of(b); it.v2 = f3_of(c);
+	it.instance = __float_as_uint(b.w);
+	const uint32_t sbt = __float_as_uint(c.w);
+	it.gn = octDecodeU32(aux.x);
+	it.prim = aux.y;
+	if (sbt == 0xFFFFFFFFu)
+	{
+		it.lightType = kLightTypeTriangle;
+		it.lightIndex = aux.y;
+		const EmissiveTri& et = sc.lights.triangles[aux.y];
+		it.prim = et.prim;
+		it.material = et.material;
+	}
+	else
+	{
+		it.lightType = kLightTypeNone;
+		it.lightIndex = 0;
+		it.material = sbt;
+	}
+	it.b1 = h.z; it.b2 = h.w;
+	const float w0 = 1.0f - it.b1 - it.b2;
+	it.hitPos = mk(it.v0.x * w0 + it.v1.x * it.b1 + it.v2.x * it.b2,
+	               it.v0.y * w0 + it.v1.y * it.b1 + it.v2.y * it.b2,
+	               it.v0.z * w0 + it.v1.z * it.b1 + it.v2.z * it.b2);
+	it.hitPosInterp = it.hitPos;
+	it.backHit = dot(it.gn, rayD) > 0.0f;
+}
+
+RB_D uint32_t readIndex(const DevMaterial& m, uint32_t i)
+{
+	return m.indexType == 0 ? static_cast<uint32_t>(reinterpret_cast<const uint16_t*>(m.indices)[i])
+	                        : reinterpret_cast<const uint32_t*>(m.indices)[i];
+}
+
+// Shading frame, shadow-terminator offset and surface description
+// (pathtrace.cu:1279-1567). Returns false if the interaction is skipped by
+// alpha testing.
+RB_D bool shadingSetup(const DevScene& sc, const DevMaterial& mat, Interaction& it, f3 rayD, const Qrng& q,
+	Frame& frame, Surface& surf, f3& lastNormal)
+{
+	const float w0 = 1.0f - it.b1 - it.b2, w1 = it.b1, w2 = it.b2;
+	const float* M = sc.geo.normalMatrix + 9u * it.instance;
+	f3 normal, tangent;
+	bool flipTangent = false;
+	const uint32_t idx0 = readIndex(mat, it.prim * 3 + 0);
+	const uint32_t idx1 = readIndex(mat, it.prim * 3 + 1);
+	const uint32_t idx2 = readIndex(mat, it.prim * 3 + 2);
+	if (mat.attributes & (RB_ATTR_NORMAL | RB_ATTR_FRAME))
+	{
+		f3 sn, st, n0, n1, n2;
+		const uint8_t* base = mat.attributeData;
+		const uint32_t stride = mat.attributeStride;
+		if (mat.attributes & RB_ATTR_FRAME)
+		{
+			const uint8_t* at = base + mat.frameOffset;
+			const float4 q0 = *reinterpret_cast<const float4*>(at + stride * idx0);
+			const float4 q1 = *reinterpret_cast<const float4*>(at + stride * idx1);
+			const float4 q2 = *reinterpret_cast<const float4*>(at + stride * idx2);
+			flipTangent = signbit(q0.w);
+			f3 t0, t1, t2;
+			quatColumns(q0, t0, n0);
+			quatColumns(q1, t1, n1);
+			quatColumns(q2, t2, n2);
+			sn = w0 * n0 + w1 * n1 + w2 * n2;
+			st = w0 * t0 + w1 * t1 + w2 * t2;
+		}
+		else
+		{
+			const uint8_t* at = base + mat.normalOffset;
+			const float2 e0 = *reinterpret_cast<const float2*>(at + stride * idx0);
+			const float2 e1 = *reinterpret_cast<const float2*>(at + stride * idx1);
+			const float2 e2 = *reinterpret_cast<const float2*>(at + stride * idx2);
+			n0 = octDecode(e0.x, e0.y);
+			n1 = octDecode(e1.x, e1.y);
+			n2 = octDecode(e2.x, e2.y);
+			sn = w0 * n0 + w1 * n1 + w2 * n2;
+			st = tangentOf(sn);
+		}
+		// Shadow-terminator offset (Hanika 2021), pathtrace.cu:1380-1399.
+		const f3 nA = normalize(mulMat(M, n0));
+		const f3 nB = normalize(mulMat(M, n1));
+		const f3 nC = normalize(mulMat(M, n2));
+		f3 tu = it.hitPos - it.v0, tv = it.hitPos - it.v1, tw = it.hitPos - it.v2;
+		const float du = fminf(0.0f, dot(tu, nA));
+		const float dv = fminf(0.0f, dot(tv, nB));
+		const float dw = fminf(0.0f, dot(tw, nC));
+		tu -= du * nA;
+		tv -= dv * nB;
+		tw -= dw * nC;
+		it.hitPosInterp = it.hitPos + w0 * tu + w1 * tv + w2 * tw;
+		normal = normalize(mulMat(M, sn));
+		// inverse(transpose(M)) with glm's cofactor formula; M is stored by rows.
+		const float m00 = M[0], m01 = M[3], m02 = M[6];   // column-major view m[c][r] of M
+		const float m10 = M[1], m11 = M[4], m12 = M[7];
+		const float m20 = M[2], m21 = M[5], m22 = M[8];
+		// T = transpose(M): T[c][r] = M[r][c]
+		const float t00 = m00, t01 = m10, t02 = m20, t10 = m01, t11 = m11, t12 = m21, t20 = m02, t21 = m12, t22 = m22;
+		const float inv = 1.0f / (+t00 * (t11 * t22 - t21 * t12) - t10 * (t01 * t22 - t21 * t02) + t20 * (t01 * t12 - t11 * t02));
+		const float i00 = +(t11 * t22 - t21 * t12) * inv, i10 = -(t10 * t22 - t20 * t12) * inv, i20 = +(t10 * t21 - t20 * t11) * inv;
+		const float i01 = -(t01 * t22 - t21 * t02) * inv, i11 = +(t00 * t22 - t20 * t02) * inv, i21 = -(t00 * t21 - t20 * t01) * inv;
+		const float i02 = +(t01 * t12 - t11 * t02) * inv, i12 = -(t00 * t12 - t10 * t02) * inv, i22 = +(t00 * t11 - t10 * t01) * inv;
+		const f3 vt = mk(i00 * st.x + i10 * st.y + i20 * st.z, i01 * st.x + i11 * st.y + i21 * st.z,
+		                 i02 * st.x + i12 * st.y + i22 * st.z);
+		tangent = normalize(vt);
+	}
+	else
+	{
+		normal = it.gn;
+		tangent = tangentOf(it.gn);
+	}
+	// Frame and shading-normal correction (pathtrace.cu:1434-1461).
+	const f3 bitangent = cross(normal, tangent) * (flipTangent ? -1.0f : 1.0f);
+	f3 n = mk(tangent.x * 0.0f + bitangent.x * 0.0f + normal.x * 1.0f,
+	          tangent.y * 0.0f + bitangent.y * 0.0f + normal.y * 1.0f,
+	          tangent.z * 0.0f + bitangent.z * 0.0f + normal.z * 1.0f);
+	const float dNs = dot(n, rayD), dNg = dot(it.gn, rayD);
+	const bool fromOutside = dNs > 0.0f && dNg < 0.0f;
+	const bool fromInside = dNs < 0.0f && dNg > 0.0f;
+	if (fromOutside || fromInside)
+		n = normalize(n - rayD * (dNs + (fromOutside ? 0.001f : -0.001f)));
+	f3 sb = normalize(cross(n, tangent));
+	const f3 stn = normalize(cross(sb, n));
+	sb *= flipTangent ? -1.0f : 1.0f;
+	frame = Frame{ stn, sb, n };
+	lastNormal = n;
+
+	// Material factors (pathtrace.cu:1463-1560); textures are not supported.
+	surf = defaultSurface();
+	float alpha = 0.0f;
+	if (mat.factors & RB_FACTOR_BASE_COLOR)
+	{
+		surf.baseColor = mk(mat.baseColor[0], mat.baseColor[1], mat.baseColor[2]);
+		alpha = mat.baseColor[3];
+	}
+	bool skipped = false;
+	if (mat.factors & RB_FACTOR_CUTOFF)
+	{
+		if (alpha < mat.alphaCutoff) skipped = true;
+	}
+	else if (mat.factors & RB_FACTOR_BLEND)
+	{
+		if (sample1D(q, DIM_ALPHA_BLEND) > alpha) skipped = true;
+	}
+	if (mat.factors & RB_FACTOR_METALNESS) surf.metalness = mat.metalness;
+	if (mat.factors & RB_FACTOR_ROUGHNESS) surf.roughness = mat.roughness;
+	if (mat.factors & RB_FACTOR_TRANSMISSION) surf.transmission = mat.transmission;
+	surf.ior = mat.ior;
+	if (mat.sheenPresent)
+	{
+		surf.layers |= 2u;
+		if (mat.factors & RB_FACTOR_SHEEN_COLOR) surf.sheenColor = mk(mat.sheenColor[0], mat.sheenColor[1], mat.sheenColor[2]);
+		if (mat.factors & RB_FACTOR_SHEEN_ROUGH) surf.sheenAlpha = mat.sheenRoughness;
+	}
+	return !skipped;
+}
+
+// ------------------------------------------------------------- kernels
+__global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, WaveParams w)
+{
+	const uint32_t W = sc.launch.width;
+	for (uint32_t p = gtid(); p < w.paths; p += gstride())
+	{
+		const uint32_t pix = p % w.pixels;
+		const uint32_t x = pix % W, y = pix / W;
+		const uint32_t sample = w.sampleBase + p / w.pixels;
+		const Qrng q = qrngAt(sample, pixelHash(x, y), 0);
+		const Wavelengths wl = sampleVisible(sample1D(q, DIM_WAVELENGTH));
+		float fu, fv, dx, dy, lu = 0.0f, lv = 0.0f;
+		sample2D(q, DIM_FILTER, fu, fv);
+		gaussianFilterSample(fu, fv, dx, dy);
+		if (sc.launch.dof) sample2D(q, DIM_LENS, lu, lv);
+		f3 o, d;
+		cameraRay(sc.launch, static_cast<float>(x) + dx, static_cast<float>(y) + dy, lu, lv, o, d);
+		s.rayO[p] = f4_of(o, 1.0f);
+		s.rayD[p] = f4_of(d, 1.0f);
+		s.lambda[p] = f4(wl.lambda);
+		s.lpdf[p] = f4(wl.pdf);
+		s.nrm[p] = make_float4(0.0f, 0.0f, 0.0f, wl.active);
+		s.L[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+		s.T[p] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+		s.fd[p] = make_uint2(0u, 0u);
+		s.queue[0][p] = p;
+	}
+	if (gtid() == 0) s.counts[0] = w.paths;
+}
+
+// Adds per-thread counts to a 64-bit counter with one atomic per warp.
+RB_D void warpAdd(unsigned long long* dst, uint32_t v)
+{
+	unsigned long long s = v;
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
+	if ((threadIdx.x & 31u) == 0 && s) atomicAdd(dst, s);
+}
+
+// counters (COUNT only): [0] rays, [1] nodes, [2] triangles.
+template<bool COUNT>
+__global__ void __launch_bounds__(kThreads) kExtend(DevScene sc, PathSoA s, int bounce, unsigned long long* counters)
+{
+	const uint32_t n = s.counts[bounce];
+	const uint32_t* q = s.queue[bounce & 1];
+	uint32_t rays = 0, nodes = 0, tris = 0;
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const uint32_t p = q[i];
+		const float4 o = s.rayO[p], d = s.rayD[p];
+		const Hit h = traceClosestT<COUNT>(sc.geo, f3_of(o), f3_of(d), 0.0f, FLT_MAX, sc.status, nodes, tris);
+		s.hit[p] = make_float4(__int_as_float(h.tri), h.t, h.b1, h.b2);
+		++rays;
+	}
+	if (COUNT)
+	{
+		warpAdd(counters + 0, rays);
+		warpAdd(counters + 1, nodes);
+		warpAdd(counters + 2, tris);
+	}
+}
+
+__global__ void __launch_bounds__(kThreads) kShade(DevScene sc, PathSoA s, WaveParams w, int bounce)
+{
+	const uint32_t n = s.counts[bounce];
+	const uint32_t* queue = s.queue[bounce & 1];
+	uint32_t* nextQueue = s.queue[(bounce + 1) & 1];
+	uint32_t* nextCount = s.counts + bounce + 1;
+	uint32_t* shadowCount = s.counts + (kMaxBounces + 1) + bounce;
+	const uint32_t W = sc.launch.width;
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const uint32_t p = queue[i];
+		const float4 ro = s.rayO[p], rd = s.rayD[p];
+		f3 rayO = f3_of(ro), rayD = f3_of(rd);
+		float refrScale = ro.w, bxdfPdf = rd.w;
+		const float4 nv = s.nrm[p];
+		f3 lastNormal = f3_of(nv);
+		Wavelengths wl{ s4(s.lambda[p]), s4(s.lpdf[p]), nv.w };
+		S4 L = s4(s.L[p]), T = s4(s.T[p]);
+		uint2 fd = s.fd[p];
+		uint32_t flags = fd.x, depth = fd.y;
+		const uint32_t pix = p % w.pixels;
+		const Qrng q = qrngAt(w.sampleBase + p / w.pixels, pixelHash(pix % W, pix / W), depth);
+
+		Interaction it;
+		unpackHit(sc, s.hit[p], rayD, it);
+		if (it.lightType == kLightTypeTriangle || it.lightType == kLightTypeNone) flags |= PF_TRIANGULAR_GEOMETRY;
+
+		// Hit emission with MIS (pathtrace.cu:1185-1274).
+		if (it.lightType != kLightTypeNone)
+		{
+			const bool prevNee = depth != 0 && !(flags & PF_PREVIOUS_HIT_SPECULAR);
+			const float treePdf = prevNee ? lightTreePdf(sc, it.lightType, it.lightIndex, rayO, lastNormal) : 1.0f;
+			float lightPdf = 0.0f;
+			S4 Le = s4(0.0f);
+			bool noEmission = false;
+			const f3 toHit = it.hitPos - rayO;
+			const float d2 = toHit.x * toHit.x + toHit.y * toHit.y + toHit.z * toHit.z;
+			if (it.lightType == kLightTypeTriangle)
+			{
+				const EmissiveTri& et = sc.lights.triangles[it.lightIndex];
+				const f3 a = mk(et.v[0], et.v[1], et.v[2]), b = mk(et.v[3], et.v[4], et.v[5]), c = mk(et.v[6], et.v[7], et.v[8]);
+				f3 nn = cross(b - a, c - a);
+				const float nl = length(nn);
+				nn = nn / nl;
+				const float area = nl / 2.0f;
+				const float lCos = -dot(rayD, nn);
+				noEmission = lCos <= 0.0f;
+				lightPdf = (1.0f / area) * d2 / lCos;
+				const DevMaterial& em = sc.materials[et.material];
+				Le = rgbToSpectrum(sc.spectra.basis, mk(em.emissive[0], em.emissive[1], em.emissive[2]), wl.lambda);
+			}
+			else
+			{
+				if (sc.env.enabled)
+					envEmission(sc, rayD, wl.lambda, Le, lightPdf);
+				else
+					noEmission = true;
+				flags |= PF_FINISHED;
+			}
+			if (!noEmission)
+			{
+				lightPdf *= treePdf;
+				const float wgt = prevNee ? powerHeuristic(bxdfPdf, lightPdf) : 1.0f;
+				L += T * Le * wgt;
+			}
+		}
+		bool done = (flags & PF_FINISHED) != 0;
+		bool hasShadow = false;
+		if (!done)
+		{
+			const DevMaterial& mat = sc.materials[it.material];
+			Frame frame;
+			Surface surf;
+			bool skipped = false;
+			if (flags & PF_TRIANGULAR_GEOMETRY)
+				skipped = !shadingSetup(sc, mat, it, rayD, q, frame, surf, lastNormal);
+			BxdfState st;
+			st.hasNee = false;
+			st.wl = wl; st.T = T; st.pdf = bxdfPdf; st.dir = rayD; st.flags = flags; st.refractionScale = refrScale;
+			if (!skipped)
+			{
+				// Light sample (pathtrace.cu:1572-1721).
+				LightSample dl;
+				dl.spectrum = s4(0.0f);
+				dl.dir = mk(0.0f);
+				dl.pdf = 0.0f;
+				dl.occluded = false;
+				f3 shadowO = mk(0.0f);
+				float dToL = 0.0f;
+				const bool envPresent = sc.env.enabled != 0;
+				const bool treePresent = sc.lights.nodes != nullptr;
+				if (!envPresent && !treePresent)
+				{
+					dl.occluded = true;
+				}
+				else
+				{
+					const f3 r = sample3D(q, DIM_LIGHT);
+					const bool tri = (flags & PF_TRIANGULAR_GEOMETRY) != 0;
+					const bool canTransmit = surf.transmission != 0.0f;
+					const f3 gn = it.gn, sn = lastNormal;
+					uint32_t type = 0, index = 0;
+					float treePdf = 0.0f, lightPdf = 0.0f;
+					lightTreeSample(sc, r.z, it.hitPos, sn, type, index, treePdf);
+					if (type == kLightTypeTriangle)
+					{
+						const EmissiveTri& et = sc.lights.triangles[index];
+						const f3 a = mk(et.v[0], et.v[1], et.v[2]), b = mk(et.v[3], et.v[4], et.v[5]), c = mk(et.v[6], et.v[7], et.v[8]);
+						f3 nn = cross(b - a, c - a);
+						const float nl = length(nn);
+						nn = nn / nl;
+						const float area = nl / 2.0f;
+						float u = r.x, v = r.y;
+						if (u + v > 1.0f) { u = 1.0f - u; v = 1.0f - v; }
+						const f3 lp = a + (b - a) * u + (c - a) * v;
+						const f3 sr = lp - it.hitPos;
+						const bool inSample = dot(sn, sr) < 0.0f;
+						if ((inSample && !canTransmit) || (inSample && dot(gn, sr) > 0.0f)) dl.occluded = true;
+						shadowO = offsetPoint(inSample || !tri ? it.hitPos : it.hitPosInterp, inSample ? -gn : gn);
+						const f3 rl = lp - shadowO;
+						const float d2 = rl.x * rl.x + rl.y * rl.y + rl.z * rl.z;
+						dToL = sqrtf(d2);
+						dl.dir = rl / dToL;
+						const float lCos = -dot(nn, dl.dir);
+						dl.occluded = lCos <= 0.0f;
+						lightPdf = (1.0f / area) * d2 / lCos;
+						const DevMaterial& em = sc.materials[et.material];
+						dl.spectrum = rgbToSpectrum(sc.spectra.basis, mk(em.emissive[0], em.emissive[1], em.emissive[2]), wl.lambda);
+					}
+					else if (type == kLightTypeSky)
+					{
+						envSample(sc, r.x, r.y, wl.lambda, dl.dir, dl.spectrum, lightPdf);
+						dToL = FLT_MAX;
+						shadowO = offsetPoint(!tri ? it.hitPos : it.hitPosInterp, it.backHit ? -it.gn : it.gn);
+					}
+					else
+					{
+						dl.occluded = true;
+					}
+					dl.pdf = lightPdf * treePdf;
+				}
+				evalBxdf(sc, mat, dl, q, frame, surf, st);
+				if (!dl.occluded && st.hasNee && !(st.flags & PF_PATH_TERMINATED))
+				{
+					hasShadow = true;
+					s.shO[p] = f4_of(shadowO, dToL - 0.1f);
+					s.shD[p] = f4_of(dl.dir, 0.0f);
+					s.shC[p] = f4(st.nee);
+				}
+			}
+			flags = st.flags;
+			T = st.T;
+			bxdfPdf = st.pdf;
+			rayD = st.dir;
+			refrScale = st.refractionScale;
+			wl = st.wl;
+			if (flags & PF_PATH_TERMINATED)
+			{
+				done = true;
+				hasShadow = false;
+			}
+			else
+			{
+				// Russian roulette (pathtrace.cu:1736-1744).
+				const float tMax = s4max(T) * refrScale;
+				bool killed = false;
+				if (tMax < 1.0f && depth > 0)
+				{
+					float qq = fmaxf(0.0f, 1.0f - tMax);
+					qq = qq * qq;
+					if (sample1D(q, DIM_ROULETTE) < qq) killed = true;
+					else T /= (1.0f - qq);
+				}
+				if (killed)
+				{
+					done = true;
+				}
+				else
+				{
+					// Next origin and direction fix-up (:1747-1766).
+					const bool refracted = (flags & PF_RAY_REFRACTED) != 0;
+					const bool triGeo = (flags & PF_TRIANGULAR_GEOMETRY) != 0;
+					const bool in = refracted || skipped;
+					const f3 origin = (in == it.backHit) && triGeo ? it.hitPosInterp : it.hitPos;
+					const f3 offset = in == it.backHit ? it.gn : -it.gn;
+					rayO = offsetPoint(origin, offset);
+					const float dNg = dot(it.gn, rayD);
+					if (dNg > 0.0f && (it.backHit != refracted) && !skipped)
+						rayD = normalize(rayD - (it.gn * (dNg + 0.001f)));
+					// Depth limits (:1769-1779).
+					++depth;
+					bool cont = depth < sc.launch.maxDepth;
+					if (!(flags & PF_CURRENT_HIT_SPECULAR) && !skipped)
+						cont = (flags & PF_REFRACTION_HAPPENED) ? depth < sc.launch.maxTransmitted : depth < sc.launch.maxReflected;
+					if (!cont) flags |= PF_FINISHED;
+					// updateStateFlags (:954-972).
+					uint32_t inc = 0;
+					if (flags & PF_CURRENT_HIT_SPECULAR) inc |= PF_PREVIOUS_HIT_SPECULAR; else inc |= PF_REGULARIZED;
+					if (flags & PF_RAY_REFRACTED) inc |= PF_REFRACTION_HAPPENED;
+					flags = (flags & ~(PF_CURRENT_HIT_SPECULAR | PF_PREVIOUS_HIT_SPECULAR | PF_TRIANGULAR_GEOMETRY
+						| PF_RIGHT_HANDED_FRAME | PF_RAY_REFRACTED)) | inc;
+					done = (flags & PF_FINISHED) != 0;
+				}
+			}
+		}
+		s.L[p] = f4(L);
+		s.T[p] = f4(T);
+		s.fd[p] = make_uint2(flags, depth);
+		s.nrm[p] = f4_of(lastNormal, wl.active);
+		s.lpdf[p] = f4(wl.pdf);
+		s.rayO[p] = f4_of(rayO, refrScale);
+		s.rayD[p] = f4_of(rayD, bxdfPdf);
+		if (hasShadow) s.shadowQueue[appendIndex(shadowCount)] = p;
+		if (!done) nextQueue[appendIndex(nextCount)] = p;
+	}
+}
+
+template<bool COUNT>
+__global__ void __launch_bounds__(kThreads) kShadow(DevScene sc, PathSoA s, int bounce, unsigned long long* counters)
+{
+	const uint32_t n = s.counts[(kMaxBounces + 1) + bounce];
+	uint32_t rays = 0, nodes = 0, tris = 0;
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const uint32_t p = s.shadowQueue[i];
+		const float4 o = s.shO[p], d = s.shD[p];
+		if (!traceAnyT<COUNT>(sc.geo, f3_of(o), f3_of(d), 0.0f, o.w, sc.status, nodes, tris))
+		{
+			S4 L = s4(s.L[p]);
+			L += s4(s.shC[p]);
+			s.L[p] = f4(L);
+		}
+		++rays;
+	}
+	if (COUNT)
+	{
+		warpAdd(counters + 3, rays);
+		warpAdd(counters + 4, nodes);
+		warpAdd(counters + 5, tris);
+	}
+}
+
+// Sample resolve and FP64 accumulation (pathtrace.cu:1789-1812, color::toRGB).
+__global__ void __launch_bounds__(kThreads) kResolve(DevScene sc, PathSoA s, WaveParams w, double4* accum)
+{
+	const uint32_t planes = w.paths / w.pixels;
+	const float* X = sc.spectra.sensor;
+	const float* Y = X + kSpectrumBins;
+	const float* Z = Y + kSpectrumBins;
+	for (uint32_t pix = gtid(); pix < w.pixels; pix += gstride())
+	{
+		double4 acc = w.fresh ? make_double4(0.0, 0.0, 0.0, 0.0) : accum[pix];
+		for (uint32_t k = 0; k < planes; ++k)
+		{
+			const uint32_t p = k * w.pixels + pix;
+			const uint32_t flags = s.fd[p].x;
+			if (!(flags & PF_PATH_TERMINATED))
+			{
+				S4 L = s4(s.L[p]);
+				const S4 pdf = s4(s.lpdf[p]);
+				const S4 lam = s4(s.lambda[p]);
+				for (int i = 0; i < 4; ++i) L.v[i] = pdf.v[i] != 0.0f ? L.v[i] / pdf.v[i] : 0.0f;
+				float cx = __fmul_rn(denseAt(X, lam.v[0]), L.v[0]);
+				float cy = __fmul_rn(denseAt(Y, lam.v[0]), L.v[0]);
+				float cz = __fmul_rn(denseAt(Z, lam.v[0]), L.v[0]);
+				for (int i = 1; i < 4; ++i)
+				{
+					cx = __fadd_rn(cx, __fmul_rn(denseAt(X, lam.v[i]), L.v[i]));
+					cy = __fadd_rn(cy, __fmul_rn(denseAt(Y, lam.v[i]), L.v[i]));
+					cz = __fadd_rn(cz, __fmul_rn(denseAt(Z, lam.v[i]), L.v[i]));
+				}
+				cx /= 4.0f; cy /= 4.0f; cz /= 4.0f;
+				if (!isfinite(cx) || !isfinite(cy) || !isfinite(cz)) atomicOr(sc.status, RB_DEV_NAN_RADIANCE);
+				acc.x += static_cast<double>(cx);
+				acc.y += static_cast<double>(cy);
+				acc.z += static_cast<double>(cz);
+				acc.w += 1.0;
+			}
+			else
+			{
+				acc.w += 1.0;
+			}
+		}
+		accum[pix] = acc;
+	}
+}
+
+// ------------------------------------------------ per-function kernels
+__global__ void kSobol(uint32_t n, uint32_t dims, const uint32_t* sample, const uint32_t* hash, const uint32_t* bounce,
+	const uint32_t* dim, float* out)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const Qrng q = qrngAt(sample[i], hash[i], bounce[i]);
+		if (dims == 1) out[i] = sample1D(q, dim[i]);
+		else if (dims == 2) sample2D(q, dim[i], out[2 * i], out[2 * i + 1]);
+		else
+		{
+			const f3 v = sample3D(q, dim[i]);
+			out[3 * i] = v.x; out[3 * i + 1] = v.y; out[3 * i + 2] = v.z;
+		}
+	}
+}
+__global__ void kPixelHash(uint32_t n, const uint32_t* x, const uint32_t* y, uint32_t* out)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride()) out[i] = pixelHash(x[i], y[i]);
+}
+__global__ void kWavelengths(uint32_t n, const float* u, float* lambda, float* pdf)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const Wavelengths w = sampleVisible(u[i]);
+		for (int k = 0; k < 4; ++k) { lambda[4 * i + k] = w.lambda.v[k]; pdf[4 * i + k] = w.pdf.v[k]; }
+	}
+}
+__global__ void kCameraRay(DevScene sc, uint32_t n, const float* pixel, const float* fuv, const float* luv, float* out)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		float dx, dy;
+		gaussianFilterSample(fuv[2 * i], fuv[2 * i + 1], dx, dy);
+		f3 o, d;
+		cameraRay(sc.launch, pixel[2 * i] + dx, pixel[2 * i + 1] + dy, luv[2 * i], luv[2 * i + 1], o, d);
+		out[6 * i] = o.x; out[6 * i + 1] = o.y; out[6 * i + 2] = o.z;
+		out[6 * i + 3] = d.x; out[6 * i + 4] = d.y; out[6 * i + 5] = d.z;
+	}
+}
+__global__ void kBxdfCases(DevScene sc, uint32_t n, rb_bxdf_case* cases)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		rb_bxdf_case c = cases[i];
+		const DevMaterial& mat = sc.materials[c.material];
+		LightSample dl;
+		for (int k = 0; k < 4; ++k) dl.spectrum.v[k] = c.light_spectrum[k];
+		dl.dir = mk(c.light_dir[0], c.light_dir[1], c.light_dir[2]);
+		dl.pdf = c.light_pdf;
+		dl.occluded = c.occluded != 0;
+		const Qrng q = qrngAt(c.sample, c.hash, c.bounce);
+		const Frame fr{ mk(c.frame_t[0], c.frame_t[1], c.frame_t[2]), mk(c.frame_b[0], c.frame_b[1], c.frame_b[2]),
+		                mk(c.frame_n[0], c.frame_n[1], c.frame_n[2]) };
+		Surface sf;
+		sf.layers = c.layers;
+		sf.baseColor = mk(c.base_color[0], c.base_color[1], c.base_color[2]);
+		sf.metalness = c.metalness;
+		sf.ior = c.ior;
+		sf.roughness = c.roughness;
+		sf.transmission = c.transmission;
+		sf.sheenColor = mk(c.sheen_color[0], c.sheen_color[1], c.sheen_color[2]);
+		sf.sheenAlpha = c.sheen_alpha;
+		BxdfState st;
+		st.hasNee = false;
+		for (int k = 0; k < 4; ++k)
+		{
+			st.wl.lambda.v[k] = c.lambda[k]; st.wl.pdf.v[k] = c.lambda_pdf[k]; st.T.v[k] = c.throughput[k];
+		}
+		st.wl.active = c.active_count;
+		st.pdf = c.bxdf_pdf;
+		st.dir = mk(c.dir[0], c.dir[1], c.dir[2]);
+		st.flags = c.flags;
+		st.refractionScale = c.refraction_scale;
+		evalBxdf(sc, mat, dl, q, fr, sf, st);
+		S4 L;
+		for (int k = 0; k < 4; ++k) L.v[k] = c.L[k];
+		if (st.hasNee) L += st.nee;
+		for (int k = 0; k < 4; ++k)
+		{
+			c.L[k] = L.v[k]; c.throughput[k] = st.T.v[k]; c.lambda[k] = st.wl.lambda.v[k]; c.lambda_pdf[k] = st.wl.pdf.v[k];
+		}
+		c.active_count = st.wl.active;
+		c.bxdf_pdf = st.pdf;
+		c.dir[0] = st.dir.x; c.dir[1] = st.dir.y; c.dir[2] = st.dir.z;
+		c.flags = st.flags;
+		c.refraction_scale = st.refractionScale;
+		cases[i] = c;
+	}
+}
+__global__ void kLightCases(DevScene sc, uint32_t n, rb_light_case* cases)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		rb_light_case c = cases[i];
+		const f3 p = mk(c.position[0], c.position[1], c.position[2]);
+		const f3 nn = mk(c.normal[0], c.normal[1], c.normal[2]);
+		lightTreeSample(sc, c.rand, p, nn, c.type, c.index, c.pdf);
+		c.q_pdf = lightTreePdf(sc, c.q_type, c.q_index, p, nn);
+		cases[i] = c;
+	}
+}
+__global__ void kOffsetPoint(uint32_t n, const float* p, const float* nrm, float* out)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const f3 r = offsetPoint(mk(p[3 * i], p[3 * i + 1], p[3 * i + 2]), mk(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]));
+		out[3 * i] = r.x; out[3 * i + 1] = r.y; out[3 * i + 2] = r.z;
+	}
+}
+__global__ void kOctEncode(uint32_t n, const float* v, uint32_t* out)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride()) out[i] = octEncodeU32(mk(v[3 * i], v[3 * i + 1], v[3 * i + 2]));
+}
+__global__ void kOctDecode(uint32_t n, const uint32_t* code, float* out)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const f3 r = octDecodeU32(code[i]);
+		out[3 * i] = r.x; out[3 * i + 1] = r.y; out[3 * i + 2] = r.z;
+	}
+}
+// Closest hit returned in the reference's 24-word payload layout.
+__global__ void kTrace(DevScene sc, uint32_t n, const float* rays, uint32_t* payload, float* tOut, int32_t* triOut)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const f3 o = mk(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
+		const f3 d = mk(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
+		const Hit h = traceClosest(sc.geo, o, d, 0.0f, FLT_MAX, sc.status);
+		uint32_t* pl = payload + 24 * static_cast<size_t>(i);
+		for (int k = 0; k < 24; ++k) pl[k] = 0u;
+		if (h.tri < 0)
+		{
+			pl[8] = kLightTypeSky << 30;
+			tOut[i] = INFINITY;
+			triOut[i] = -1;
+			continue;
+		}
+		const float4 a = sc.geo.triVerts[3 * h.tri], b = sc.geo.triVerts[3 * h.tri + 1], c = sc.geo.triVerts[3 * h.tri + 2];
+		const uint2 aux = sc.geo.triAux[h.tri];
+		const uint32_t sbt = __float_as_uint(c.w);
+		uint32_t prim = aux.y, mat = sbt, lptr = kLightTypeNone << 30;
+		if (sbt == 0xFFFFFFFFu)
+		{
+			lptr = (kLightTypeTriangle << 30) | (aux.y & ((1u << 30) - 1u));
+			prim = sc.lights.triangles[aux.y].prim;
+			mat = sc.lights.triangles[aux.y].material;
+		}
+		pl[0] = __float_as_uint(a.x); pl[1] = __float_as_uint(a.y); pl[2] = __float_as_uint(a.z);
+		pl[3] = aux.x; pl[4] = prim; pl[5] = __float_as_uint(h.b1); pl[6] = __float_as_uint(h.b2);
+		pl[7] = mat; pl[8] = lptr;
+		const float* M = sc.geo.normalMatrix + 9u * __float_as_uint(b.w);
+		for (int k = 0; k < 9; ++k) pl[9 + k] = __float_as_uint(M[k]);
+		pl[18] = __float_as_uint(b.x); pl[19] = __float_as_uint(b.y); pl[20] = __float_as_uint(b.z);
+		pl[21] = __float_as_uint(c.x); pl[22] = __float_as_uint(c.y); pl[23] = __float_as_uint(c.z);
+		tOut[i] = h.t;
+		triOut[i] = static_cast<int32_t>(__float_as_uint(a.w));
+	}
+}
+__global__ void kOccluded(DevScene sc, uint32_t n, const float* rays, const float* tmax, uint32_t* out)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const f3 o = mk(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
+		const f3 d = mk(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
+		out[i] = traceAny(sc.geo, o, d, 0.0f, tmax[i], sc.status) ? 1u : 0u;
+	}
+}
+
+int gridFor(uint32_t n)
+{
+	const uint32_t b = (n + kThreads - 1) / kThreads;
+	return static_cast<int>(b < 1 ? 1 : (b > 65535u * 4 ? 65535u * 4 : b));
+}
+} // namespace
+
+LaunchShape queryLaunchShape()
+{
+	LaunchShape ls{};
+	int dev = 0;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&ls.smCount, cudaDevAttrMultiProcessorCount, dev);
+	auto occ = [&](const void* fn) {
+		int b = 0;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, 0);
+		return (b < 1 ? 1 : b) * ls.smCount;
+	};
+	ls.threads = kThreads;
+	ls.blocksGenerate = occ(reinterpret_cast<const void*>(kGenerate));
+	ls.blocksExtend = occ(reinterpret_cast<const void*>(kExtend<false>));
+	ls.blocksShade = occ(reinterpret_cast<const void*>(kShade));
+	ls.blocksShadow = occ(reinterpret_cast<const void*>(kShadow<false>));
+	ls.blocksResolve = occ(reinterpret_cast<const void*>(kResolve));
+	return ls;
+}
+
+void launchGenerate(const DevScene& sc, const PathSoA& s, const WaveParams& w, const LaunchShape& ls, cudaStream_t st)
+{
+	kGenerate<<<ls.blocksGenerate, kThreads, 0, st>>>(sc, s, w);
+}
+void launchExtend(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
+	unsigned long long* counters)
+{
+	if (counters) kExtend<true><<<ls.blocksExtend, kThreads, 0, st>>>(sc, s, bounce, counters);
+	else kExtend<false><<<ls.blocksExtend, kThreads, 0, st>>>(sc, s, bounce, nullptr);
+}
+void launchShade(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
+{
+	kShade<<<ls.blocksShade, kThreads, 0, st>>>(sc, s, w, bounce);
+}
+void launchShadow(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
+	unsigned long long* counters)
+{
+	if (counters) kShadow<true><<<ls.blocksShadow, kThreads, 0, st>>>(sc, s, bounce, counters);
+	else kShadow<false><<<ls.blocksShadow, kThreads, 0, st>>>(sc, s, bounce, nullptr);
+}
+void launchResolve(const DevScene& sc, const PathSoA& s, const WaveParams& w, double4* accum, const LaunchShape& ls, cudaStream_t st)
+{
+	kResolve<<<ls.blocksResolve, kThreads, 0, st>>>(sc, s, w, accum);
+}
+
+void launchSobol(uint32_t n, uint32_t dims, const uint32_t* sample, const uint32_t* hash, const uint32_t* bounce,
+	const uint32_t* dim, float* out, cudaStream_t st)
+{
+	kSobol<<<gridFor(n), kThreads, 0, st>>>(n, dims, sample, hash, bounce, dim, out);
+}
+void launchPixelHash(uint32_t n, const uint32_t* x, const uint32_t* y, uint32_t* out, cudaStream_t st)
+{
+	kPixelHash<<<gridFor(n), kThreads, 0, st>>>(n, x, y, out);
+}
+void launchWavelengths(uint32_t n, const float* u, float* lambda, float* pdf, cudaStream_t st)
+{
+	kWavelengths<<<gridFor(n), kThreads, 0, st>>>(n, u, lambda, pdf);
+}
+void launchCameraRay(const DevScene& sc, uint32_t n, const float* pixel, const float* fuv, const float* luv, float* out, cudaStream_t st)
+{
+	kCameraRay<<<gridFor(n), kThreads, 0, st>>>(sc, n, pixel, fuv, luv, out);
+}
+void launchBxdfCases(const DevScene& sc, uint32_t n, void* cases, cudaStream_t st)
+{
+	kBxdfCases<<<gridFor(n), kThreads, 0, st>>>(sc, n, static_cast<rb_bxdf_case*>(cases));
+}
+void launchLightCases(const DevScene& sc, uint32_t n, void* cases, cudaStream_t st)
+{
+	kLightCases<<<gridFor(n), kThreads, 0, st>>>(sc, n, static_cast<rb_light_case*>(cases));
+}
+void launchOffsetPoint(uint32_t n, const float* p, const float* nrm, float* out, cudaStream_t st)
+{
+	kOffsetPoint<<<gridFor(n), kThreads, 0, st>>>(n, p, nrm, out);
+}
+void launchOctEncode(uint32_t n, const float* v, uint32_t* out, cudaStream_t st)
+{
+	kOctEncode<<<gridFor(n), kThreads, 0, st>>>(n, v, out);
+}
+void launchOctDecode(uint32_t n, const uint32_t* code, float* out, cudaStream_t st)
+{
+	kOctDecode<<<gridFor(n), kThreads, 0, st>>>(n, code, out);
+}
+void launchTrace(const DevScene& sc, uint32_t n, const float* rays, uint32_t* payload, float* t, int32_t* tri, cudaStream_t st)
+{
+	kTrace<<<gridFor(n), kThreads, 0, st>>>(sc, n, rays, payload, t, tri);
+}
+void launchOccluded(const DevScene& sc, uint32_t n, const float* rays, const float* tmax, uint32_t* out, cudaStream_t st)
+{
+	kOccluded<<<gridFor(n), kThreads, 0, st>>>(sc, n, rays, tmax, out);
+}
+} // namespace rb

@@ -1,0 +1,75 @@
+// Wavefront path state and the host-side launchers of the rendering kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "rb_scene.h"
+
+namespace rb
+{
+// Structure-of-arrays state of the paths of one wave, one slot per path.
+// A wave holds `samplesPerWave` whole sample planes of the image, so slot p
+// renders pixel p % (W*H), sample sampleBase + p / (W*H). Every array is
+// 16-byte aligned and read/written with vector accesses.
+struct PathSoA
+{
+	float4* rayO;      // origin, w: refraction scale
+	float4* rayD;      // direction, w: BxDF pdf of the last bounce
+	float4* lambda;    // hero wavelengths
+	float4* lpdf;      // wavelength pdfs
+	float4* nrm;       // last shading normal, w: active wavelength count
+	float4* L;         // radiance
+	float4* T;         // throughput
+	uint2* fd;         // flags, depth
+	float4* hit;       // closest hit: triangle (bits, -1 miss), t, b1, b2
+	float4* shO;       // shadow ray origin, w: tmax
+	float4* shD;       // shadow ray direction
+	float4* shC;       // pending light-sample contribution
+	uint32_t* queue[2];// active path slots, ping-pong by bounce parity
+	uint32_t* shadowQueue;
+	uint32_t* counts;  // [bounce] active counts (kMaxBounces+1), then [kMaxBounces+1 + bounce] shadow counts
+	uint32_t capacity;
+};
+constexpr int kMaxBounces = 64;
+
+struct WaveParams
+{
+	uint32_t paths;        // slots in this wave
+	uint32_t pixels;       // W*H
+	uint32_t sampleBase;   // absolute sample index of plane 0 of the wave
+	uint32_t fresh;        // 1: accumulation starts from zero (first wave of a launch at offset 0)
+};
+
+struct LaunchShape
+{
+	int smCount;
+	int blocksGenerate, blocksExtend, blocksShade, blocksShadow, blocksResolve;
+	int threads;
+};
+
+LaunchShape queryLaunchShape();
+void launchGenerate(const DevScene& sc, const PathSoA& s, const WaveParams& w, const LaunchShape& ls, cudaStream_t st);
+// counters: nullptr, or 6 device uint64 (extend rays/nodes/tris, shadow rays/nodes/tris)
+// to run the counting variants.
+void launchExtend(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
+	unsigned long long* counters);
+void launchShade(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st);
+void launchShadow(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
+	unsigned long long* counters);
+void launchResolve(const DevScene& sc, const PathSoA& s, const WaveParams& w, double4* accum, const LaunchShape& ls, cudaStream_t st);
+
+// Per-function batch kernels (include/ratbite_b200_kernels.h).
+void launchSobol(uint32_t n, uint32_t dims, const uint32_t* sample, const uint32_t* hash, const uint32_t* bounce,
+	const uint32_t* dim, float* out, cudaStream_t st);
+void launchPixelHash(uint32_t n, const uint32_t* x, const uint32_t* y, uint32_t* out, cudaStream_t st);
+void launchWavelengths(uint32_t n, const float* u, float* lambda, float* pdf, cudaStream_t st);
+void launchCameraRay(const DevScene& sc, uint32_t n, const float* pixel, const float* fuv, const float* luv, float* out, cudaStream_t st);
+void launchBxdfCases(const DevScene& sc, uint32_t n, void* cases, cudaStream_t st);
+void launchLightCases(const DevScene& sc, uint32_t n, void* cases, cudaStream_t st);
+void launchOffsetPoint(uint32_t n, const float* p, const float* nrm, float* out, cudaStream_t st);
+void launchOctEncode(uint32_t n, const float* v, uint32_t* out, cudaStream_t st);
+void launchOctDecode(uint32_t n, const uint32_t* code, float* out, cudaStream_t st);
+void launchTrace(const DevScene& sc, uint32_t n, const float* rays, uint32_t* payload, float* t, int32_t* tri, cudaStream_t st);
+void launchOccluded(const DevScene& sc, uint32_t n, const float* rays, const float* tmax, uint32_t* out, cudaStream_t st);
+} // namespace rb

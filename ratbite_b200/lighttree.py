@@ -1,0 +1,54 @@
+"""Light-tree construction through the C ABI (rb_build_light_tree): the
+host restatement of ratbite's LightTree::Builder, producing the records
+rb_set_lights uploads."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from ._native import NativeError, load
+
+
+def build(world: np.ndarray, flux: np.ndarray, material: np.ndarray, primitive: np.ndarray,
+          camera=(0.0, 0.0, 0.0)):
+    """Returns (triangles, nodes, pointers, bitmasks) numpy arrays."""
+    n = len(flux)
+    world = np.ascontiguousarray(world, np.float32).reshape(n, 9)
+    flux = np.ascontiguousarray(flux, np.float32)
+    material = np.ascontiguousarray(material, np.uint32)
+    primitive = np.ascontiguousarray(primitive, np.uint32)
+    cam = np.ascontiguousarray(camera, np.float64)
+    tris = np.zeros(n, abi.emissive_triangle_dtype())
+    nodes = np.zeros(max(2 * n, 1), abi.packed_node_dtype())
+    ptrs = np.zeros(n, np.uint32)
+    masks = np.zeros(n, np.uint64)
+    count = C.c_uint32(0)
+    p = lambda a: C.c_void_p(a.ctypes.data)
+    rc = load().rb_build_light_tree(n, p(world), p(flux), p(material), p(primitive), p(cam), p(tris), p(nodes),
+                                    p(ptrs), p(masks), C.byref(count))
+    if rc != 0:
+        raise NativeError(f"rb_build_light_tree failed with status {rc}")
+    return tris, nodes[:count.value].copy(), ptrs, masks
+
+
+def record(tris, nodes, ptrs, masks) -> abi.rb_light_tree:
+    """rb_light_tree record pointing into the arrays (kept alive on it)."""
+    lt = abi.rb_light_tree()
+    lt.triangle_count = len(tris)
+    lt.triangles = tris.ctypes.data
+    lt.node_count = len(nodes)
+    lt.nodes = nodes.ctypes.data if len(nodes) else None
+    lt.pointer_count = len(ptrs)
+    lt.pointers = ptrs.ctypes.data
+    lt.bitmasks = masks.ctypes.data
+    lt._arrays = (tris, nodes, ptrs, masks)
+    return lt
+
+
+def build_for_scene(scene, camera=(0.0, 0.0, 0.0)) -> abi.rb_light_tree | None:
+    world, flux, mat, prim = scene.emissive_arrays()
+    if len(flux) == 0:
+        return None
+    return record(*build(world, flux, mat, prim, camera))

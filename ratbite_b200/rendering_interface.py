@@ -1,0 +1,148 @@
+"""Host-side mirror of ratbite's RenderingInterface
+(src/core/rendering_interface.h:19-226) over the B200 C ABI.
+
+Method names follow the reference where they have a counterpart:
+loadLookUpTables / fillSpectralCurvesData / fillModelMaterials /
+loadModel (geometry) / loadLights / loadEnvironmentMap / prepareDataForRendering
+/ render. The object owns one rb_ctx; all device memory belongs to it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from ._native import check, load
+
+
+def _ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
+
+class RenderingInterface:
+    def __init__(self, device: int = 0, max_paths_in_flight: int = 0):
+        self.lib = load()
+        cfg = abi.rb_config()
+        cfg.device = device
+        cfg.max_paths_in_flight = max_paths_in_flight
+        h = C.c_void_p()
+        check(self.lib.rb_create(C.byref(cfg), C.byref(h)), None, "rb_create")
+        self.ctx = h
+        self.width = self.height = 0
+        self._keep = []
+
+    # ---- lifetime ----------------------------------------------------------
+    def cleanup(self):
+        if self.ctx:
+            self.lib.rb_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.cleanup()
+
+    def __del__(self):
+        try:
+            self.cleanup()
+        except Exception:
+            pass
+
+    # ---- uploads -----------------------------------------------------------
+    def load_look_up_tables(self, luts: dict):
+        arrs = [np.ascontiguousarray(luts[k], np.float32) for k in
+                ("conductor", "dielectric_outer", "dielectric_inner", "reflective_outer",
+                 "reflective_inner", "sheen")]
+        sizes = [32 * 32, 32 ** 3, 32 ** 3, 32 ** 3, 32 ** 3, 32 * 32 * 4]
+        for a, s in zip(arrs, sizes):
+            if a.size != s:
+                raise ValueError(f"LUT has {a.size} values, expected {s}")
+        check(self.lib.rb_set_luts(self.ctx, *[_ptr(a) for a in arrs]), self.ctx, "rb_set_luts")
+
+    def fill_spectral_curves_data(self, sensor_xyz: np.ndarray, basis_rgb: np.ndarray,
+                                  extra: np.ndarray | None = None):
+        s = np.ascontiguousarray(sensor_xyz, np.float32).reshape(3, abi.RB_SPECTRUM_BINS)
+        b = np.ascontiguousarray(basis_rgb, np.float32).reshape(3, abi.RB_SPECTRUM_BINS)
+        e = (np.zeros((0, abi.RB_SPECTRUM_BINS), np.float32) if extra is None
+             else np.ascontiguousarray(extra, np.float32).reshape(-1, abi.RB_SPECTRUM_BINS))
+        check(self.lib.rb_set_spectra(self.ctx, _ptr(s), _ptr(b), _ptr(e) if len(e) else None, len(e)),
+              self.ctx, "rb_set_spectra")
+
+    def fill_model_materials(self, records):
+        check(self.lib.rb_set_materials(self.ctx, C.cast(records, C.c_void_p), len(records)),
+              self.ctx, "rb_set_materials")
+
+    def load_geometry(self, geometry: abi.rb_geometry):
+        check(self.lib.rb_set_geometry(self.ctx, C.byref(geometry)), self.ctx, "rb_set_geometry")
+
+    def load_lights(self, light_tree: abi.rb_light_tree):
+        check(self.lib.rb_set_lights(self.ctx, C.byref(light_tree)), self.ctx, "rb_set_lights")
+
+    def load_environment_map(self, rgba: np.ndarray):
+        img = np.ascontiguousarray(rgba, np.float32)
+        h, w = img.shape[:2]
+        check(self.lib.rb_set_envmap(self.ctx, _ptr(img), w, h), self.ctx, "rb_set_envmap")
+
+    def clear_environment_map(self):
+        check(self.lib.rb_clear_envmap(self.ctx), self.ctx, "rb_clear_envmap")
+
+    def prepare_data_for_rendering(self, launch: abi.rb_launch):
+        check(self.lib.rb_set_launch(self.ctx, C.byref(launch)), self.ctx, "rb_set_launch")
+        self.width, self.height = launch.width, launch.height
+
+    def load_scene(self, scene, luts: dict, sensor_xyz, basis_rgb, light_tree=None, extra=None,
+                   width=None, height=None, max_depth=None):
+        """Uploads a ratbite_b200.scenes.Scene (and its light tree records)."""
+        self.load_look_up_tables(luts)
+        self.fill_spectral_curves_data(sensor_xyz, basis_rgb, extra)
+        mats = scene.material_records()
+        self._keep.append(mats)
+        self.fill_model_materials(mats)
+        g = scene.geometry_record()
+        self._keep.append(g)
+        self.load_geometry(g)
+        if light_tree is not None:
+            self._keep.append(light_tree)
+            self.load_lights(light_tree)
+        launch = scene.launch_record(width, height, max_depth)
+        self._keep.append(launch)
+        self.prepare_data_for_rendering(launch)
+
+    # ---- rendering -----------------------------------------------------------
+    def render(self, sample_offset: int, sample_count: int, stream=None):
+        """Asynchronous: renders samples [offset, offset+count) of every pixel."""
+        s = None if stream is None else C.c_void_p(stream)
+        check(self.lib.rb_render(self.ctx, sample_offset, sample_count, s), self.ctx, "rb_render")
+
+    def synchronize(self):
+        check(self.lib.rb_synchronize(self.ctx), self.ctx, "rb_synchronize")
+
+    def read_accumulation(self) -> np.ndarray:
+        out = np.zeros((self.height, self.width, 4), np.float64)
+        check(self.lib.rb_read_accum(self.ctx, _ptr(out)), self.ctx, "rb_read_accum")
+        return out
+
+    def copy_accumulation_async(self, dst_ptr: int, stream=None):
+        """Stream-ordered copy into device or pinned host memory at dst_ptr."""
+        s = None if stream is None else C.c_void_p(stream)
+        check(self.lib.rb_copy_accum_async(self.ctx, C.c_void_p(dst_ptr), s), self.ctx, "rb_copy_accum_async")
+
+    def accumulation_device_ptr(self) -> int:
+        p = C.c_void_p()
+        check(self.lib.rb_accum_device_ptr(self.ctx, C.byref(p)), self.ctx, "rb_accum_device_ptr")
+        return p.value
+
+    def set_stats(self, mode: int):
+        check(self.lib.rb_set_stats(self.ctx, mode), self.ctx, "rb_set_stats")
+
+    def get_stats(self) -> abi.rb_render_stats:
+        st = abi.rb_render_stats()
+        check(self.lib.rb_get_stats(self.ctx, C.byref(st)), self.ctx, "rb_get_stats")
+        return st
+
+    def status(self) -> abi.rb_device_status:
+        st = abi.rb_device_status()
+        check(self.lib.rb_status(self.ctx, C.byref(st)), self.ctx, "rb_status")
+        return st

@@ -1,0 +1,370 @@
+"""Seeded synthetic scenes in the renderer's upload format.
+
+A scene here is the data ratbite's RenderingInterface would hand to the
+drop-in: meshes of submeshes placed by instances, one material record per
+submesh (MaterialData carries its submesh's index and attribute buffers,
+src/core/rendering_interface.cpp:47-290), emissive triangles cut out of their
+submesh into emissive subsets (src/core/scene.cpp:485-631), and the camera /
+launch parameters (src/core/rendering_interface.cpp:623-668). Everything is
+camera-relative with the camera at the origin.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+
+
+class PCG32:
+    """PCG-XSH-RR 32-bit generator (O'Neill 2014); the seed is recorded with
+    each scene so the same scene can be regenerated anywhere."""
+
+    MULT = 6364136223846793005
+    MASK = (1 << 64) - 1
+
+    def __init__(self, seed: int, stream: int = 54):
+        self.state = 0
+        self.inc = ((stream << 1) | 1) & self.MASK
+        self.next_u32()
+        self.state = (self.state + seed) & self.MASK
+        self.next_u32()
+
+    def next_u32(self) -> int:
+        old = self.state
+        self.state = (old * self.MULT + self.inc) & self.MASK
+        xorshifted = (((old >> 18) ^ old) >> 27) & 0xFFFFFFFF
+        rot = old >> 59
+        return ((xorshifted >> rot) | (xorshifted << ((-rot) & 31))) & 0xFFFFFFFF
+
+    def uniform(self, lo=0.0, hi=1.0) -> float:
+        return lo + (hi - lo) * (self.next_u32() / 4294967296.0)
+
+
+def oct_encode(n: np.ndarray) -> np.ndarray:
+    """Octahedral encoding of unit vectors to float2, the encoding the
+    reference uses for the NORMAL vertex attribute
+    (src/core/rendering_interface.cpp:217-229). float32 throughout."""
+    n = n.astype(np.float32)
+    s = (np.abs(n[:, 0]) + np.abs(n[:, 1]) + np.abs(n[:, 2])).astype(np.float32)
+    p = (n[:, :2] * (np.float32(1.0) / s)[:, None]).astype(np.float32)
+    sign = np.where(p >= 0, np.float32(1.0), np.float32(-1.0)).astype(np.float32)
+    folded = ((np.float32(1.0) - np.abs(p[:, ::-1])) * sign).astype(np.float32)
+    return np.where((n[:, 2] <= 0)[:, None], folded, p).astype(np.float32)
+
+
+def icosphere(subdiv: int):
+    """Unit icosphere: subdivision s gives 20*4^s triangles."""
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t),
+             (0, -1, -t), (0, 1, -t), (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    verts = [np.array(v, dtype=np.float64) / np.linalg.norm(v) for v in verts]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4),
+             (11, 10, 2), (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8),
+             (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdiv):
+        cache = {}
+        new_faces = []
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            new_faces += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = new_faces
+    return np.array(verts), np.array(faces, dtype=np.int64)
+
+
+@dataclass
+class Submesh:
+    vertices: np.ndarray          # (V, 4) float32
+    indices: np.ndarray           # (T, 3) uint16/uint32
+    material: int
+    normals: np.ndarray | None = None   # (V, 3) float32 shading normals
+    discarded: list = field(default_factory=list)
+
+
+@dataclass
+class Material:
+    base_color: tuple = (1.0, 1.0, 1.0)
+    metalness: float = 0.0
+    roughness: float = 1.0
+    transmission: float = 0.0
+    ior: float = 1.5
+    sheen_color: tuple | None = None
+    sheen_roughness: float = 0.0
+    emissive: tuple | None = None
+    bxdf: int = abi.RB_BXDF_COMPLEX_SURFACE
+    ior_spectrum: int = 0
+    absorp_spectrum: int = 0
+    mf_roughness: float = 0.0
+
+
+@dataclass
+class Scene:
+    """Upload-ready scene; keeps every numpy buffer alive for the ctypes
+    records that point into them."""
+    name: str
+    seed: int
+    meshes: list            # list[list[Submesh]]
+    instances: list         # list[(mesh, transform (3,4))]
+    materials: list         # list[Material]; index = submesh material
+    emissive: list          # list[dict(transform, tris (n,9) object space, world (n,9), prim, flux, material)]
+    width: int = 256
+    height: int = 256
+    spp: int = 64
+    max_depth: int = 8
+    fov_deg: float = 70.0
+    cam_u: tuple = (1.0, 0.0, 0.0)
+    cam_v: tuple = (0.0, 0.0, -1.0)
+    cam_w: tuple = (0.0, 1.0, 0.0)
+    _keep: list = field(default_factory=list)
+
+    # ---- counts ---------------------------------------------------------
+    def triangle_count(self) -> int:
+        n = sum(len(e["prim"]) for e in self.emissive)
+        for mesh_idx, _ in self.instances:
+            n += sum(len(sm.indices) for sm in self.meshes[mesh_idx])
+        return n
+
+    # ---- ABI records ----------------------------------------------------
+    def _attr_buffer(self, sm: Submesh):
+        if sm.normals is None:
+            return None, 0, 0
+        enc = oct_encode(sm.normals)
+        return np.ascontiguousarray(enc, dtype=np.float32), 8, abi.RB_ATTR_NORMAL
+
+    def material_records(self):
+        """One rb_material per submesh material slot."""
+        owner = {}
+        for mesh in self.meshes:
+            for sm in mesh:
+                owner.setdefault(sm.material, sm)
+        recs = (abi.rb_material * len(self.materials))()
+        for i, m in enumerate(self.materials):
+            r = recs[i]
+            sm = owner.get(i)
+            r.bxdf = m.bxdf
+            r.double_sided = 0
+            r.sheen_present = 1 if m.sheen_color is not None else 0
+            r.ior = m.ior
+            r.mf_roughness = m.mf_roughness
+            r.ior_spectrum = m.ior_spectrum
+            r.absorp_spectrum = m.absorp_spectrum
+            factors = abi.RB_FACTOR_BASE_COLOR | abi.RB_FACTOR_METALNESS | abi.RB_FACTOR_ROUGHNESS
+            r.base_color = abi.F4(*m.base_color, 1.0)
+            r.metalness = m.metalness
+            r.roughness = m.roughness
+            if m.transmission != 0.0:
+                factors |= abi.RB_FACTOR_TRANSMISSION
+                r.transmission = m.transmission
+            if m.sheen_color is not None:
+                factors |= abi.RB_FACTOR_SHEEN_COLOR | abi.RB_FACTOR_SHEEN_ROUGH
+                r.sheen_color = abi.F3(*m.sheen_color)
+                r.sheen_roughness = m.sheen_roughness
+            if m.emissive is not None:
+                factors |= abi.RB_FACTOR_EMISSION
+                r.emissive = abi.F3(*m.emissive)
+            r.factors = factors
+            if sm is not None:
+                idx = np.ascontiguousarray(sm.indices)
+                self._keep.append(idx)
+                r.index_type = abi.RB_INDEX_U16 if idx.dtype == np.uint16 else abi.RB_INDEX_U32
+                r.triangle_count = len(idx)
+                r.indices = idx.ctypes.data
+                attr, stride, bits = self._attr_buffer(sm)
+                r.attributes = bits
+                r.attribute_stride = stride
+                r.normal_offset = 0
+                r.vertex_count = len(sm.vertices)
+                if attr is not None:
+                    self._keep.append(attr)
+                    r.attribute_data = attr.ctypes.data
+        self._keep.append(recs)
+        return recs
+
+    def geometry_record(self):
+        mesh_recs = (abi.rb_mesh * len(self.meshes))()
+        for mi, mesh in enumerate(self.meshes):
+            subs = (abi.rb_submesh * len(mesh))()
+            for si, sm in enumerate(mesh):
+                v = np.ascontiguousarray(sm.vertices, dtype=np.float32)
+                idx = np.ascontiguousarray(sm.indices)
+                disc = np.ascontiguousarray(np.array(sm.discarded, dtype=np.uint32))
+                self._keep += [v, idx, disc]
+                s = subs[si]
+                s.material = sm.material
+                s.index_type = abi.RB_INDEX_U16 if idx.dtype == np.uint16 else abi.RB_INDEX_U32
+                s.triangle_count = len(idx)
+                s.indices = idx.ctypes.data
+                s.vertex_count = len(v)
+                s.vertices = v.ctypes.data
+                s.discarded_count = len(disc)
+                s.discarded = disc.ctypes.data if len(disc) else None
+            self._keep.append(subs)
+            mesh_recs[mi].submesh_count = len(mesh)
+            mesh_recs[mi].submeshes = subs
+        inst = (abi.rb_instance * len(self.instances))()
+        for i, (m, xf) in enumerate(self.instances):
+            inst[i].mesh = m
+            inst[i].transform = abi.F12(*np.asarray(xf, dtype=np.float32).reshape(12))
+        em = (abi.rb_emissive_subset * len(self.emissive))()
+        for i, e in enumerate(self.emissive):
+            tri = np.ascontiguousarray(e["tris"], dtype=np.float32)
+            self._keep.append(tri)
+            em[i].transform = abi.F12(*np.asarray(e["transform"], dtype=np.float32).reshape(12))
+            em[i].triangle_count = len(tri)
+            em[i].vertices = tri.ctypes.data
+        g = abi.rb_geometry()
+        g.mesh_count = len(self.meshes)
+        g.meshes = mesh_recs
+        g.instance_count = len(self.instances)
+        g.instances = inst
+        g.emissive_subset_count = len(self.emissive)
+        g.emissive_subsets = em
+        self._keep += [mesh_recs, inst, em, g]
+        return g
+
+    def emissive_arrays(self):
+        """Flat emissive-triangle inputs of the light-tree builder, in the
+        reference's enumeration order (src/core/rendering_interface.cpp:1084-1160):
+        world-space vertices, flux, material index, primitive index."""
+        if not self.emissive:
+            z = np.zeros((0,), np.float32)
+            return z.reshape(0, 9), z, np.zeros(0, np.uint32), np.zeros(0, np.uint32)
+        world = np.concatenate([e["world"] for e in self.emissive]).astype(np.float32)
+        flux = np.concatenate([e["flux"] for e in self.emissive]).astype(np.float32)
+        mat = np.concatenate([np.full(len(e["prim"]), e["material"], np.uint32) for e in self.emissive])
+        prim = np.concatenate([np.asarray(e["prim"], np.uint32) for e in self.emissive])
+        return (np.ascontiguousarray(world), np.ascontiguousarray(flux),
+                np.ascontiguousarray(mat), np.ascontiguousarray(prim))
+
+    def launch_record(self, width=None, height=None, max_depth=None):
+        w = width or self.width
+        h = height or self.height
+        d = max_depth or self.max_depth
+        l = abi.rb_launch()
+        l.width, l.height = w, h
+        # RenderContext inverse sizes and prepareDataForRendering's scales
+        # (src/core/render_context.h:35, src/core/rendering_interface.cpp:638-640).
+        l.inv_width = float(np.float32(1.0) / np.float32(w))
+        l.inv_height = float(np.float32(1.0) / np.float32(h))
+        t = math.tan(math.radians(self.fov_deg) * 0.5)
+        l.perspective_scale_w = float(np.float32(t) * (np.float32(w) / np.float32(h)))
+        l.perspective_scale_h = float(np.float32(t))
+        l.max_path_depth = d
+        l.max_reflected_depth = d
+        l.max_transmitted_depth = d
+        l.cam_u = abi.F3(*self.cam_u)
+        l.cam_v = abi.F3(*self.cam_v)
+        l.cam_w = abi.F3(*self.cam_w)
+        l.dof_enabled = 0
+        l.aperture = 0.01
+        l.focus_distance = 1.0
+        return l
+
+
+IDENTITY = np.array([[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 1, 0]], dtype=np.float32)
+
+
+def _quad(p0, p1, p2, p3):
+    """Two triangles (p0,p1,p2), (p0,p2,p3); normal = (p1-p0)x(p2-p0)."""
+    v = np.array([p0, p1, p2, p3], dtype=np.float32)
+    v4 = np.concatenate([v, np.zeros((4, 1), np.float32)], axis=1)
+    return v4, np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint16)
+
+
+def blackbody_rgb(temperature_k: float, cie_xyz: np.ndarray) -> np.ndarray:
+    """Linear sRGB of a blackbody at `temperature_k`, normalised to max 1,
+    from Planck's law and the given 471-bin CIE 1931 tables. Used as the
+    emitter's RGB factor: the reference has only RGB emission
+    (src/kernels/pathtrace.cu:1216-1231)."""
+    lam = np.arange(360, 831, dtype=np.float64) * 1e-9
+    h, c, k = 6.62607015e-34, 2.99792458e8, 1.380649e-23
+    spd = 1.0 / (lam ** 5 * (np.exp(h * c / (lam * k * temperature_k)) - 1.0))
+    xyz = cie_xyz.astype(np.float64) @ spd
+    m = np.array([[3.2404542, -1.5371385, -0.4985314],
+                  [-0.9692660, 1.8760108, 0.0415560],
+                  [0.0556434, -0.2040259, 1.0572252]])
+    rgb = np.maximum(m @ xyz, 0.0)
+    return rgb / rgb.max()
+
+
+def cornell_box(seed: int = 1, cie_xyz: np.ndarray | None = None, light_scale: float = 12.0,
+                subdiv: int = 3, width: int = 256, height: int = 256, spp: int = 64,
+                max_depth: int = 8) -> Scene:
+    """The small plain-method workload: procedural Cornell box, 5 walls (10
+    triangles, albedo U[0.2,0.8]^3 from PCG32(seed)), one 0.25 m^2 emissive
+    quad (6500 K blackbody as RGB), a metal icosphere (roughness 0.3, F0 from
+    PCG32) and a dielectric icosphere (IOR 1.5, roughness 0.05), 1280
+    triangles each at subdivision 3. Camera at the origin looking down -z."""
+    rng = PCG32(seed)
+    cz = -3.2          # box centre depth
+    x0, x1, y0, y1, z0, z1 = -1.0, 1.0, -1.0, 1.0, cz - 1.0, cz + 1.0
+    materials: list[Material] = []
+    walls: list[Submesh] = []
+    quads = [
+        ((x0, y0, z1), (x1, y0, z1), (x1, y0, z0), (x0, y0, z0)),   # floor, normal +y
+        ((x0, y1, z0), (x1, y1, z0), (x1, y1, z1), (x0, y1, z1)),   # ceiling, normal -y
+        ((x0, y0, z0), (x1, y0, z0), (x1, y1, z0), (x0, y1, z0)),   # back, normal +z
+        ((x0, y0, z1), (x0, y0, z0), (x0, y1, z0), (x0, y1, z1)),   # left, normal +x
+        ((x1, y0, z0), (x1, y0, z1), (x1, y1, z1), (x1, y1, z0)),   # right, normal -x
+    ]
+    for q in quads:
+        albedo = tuple(rng.uniform(0.2, 0.8) for _ in range(3))
+        materials.append(Material(base_color=albedo, metalness=0.0, roughness=1.0))
+        v, i = _quad(*q)
+        walls.append(Submesh(v, i, len(materials) - 1))
+    # Emissive quad, 0.5 m x 0.5 m just below the ceiling, facing down.
+    if cie_xyz is None:
+        rgb = np.array([1.0, 0.97, 0.93])
+    else:
+        rgb = blackbody_rgb(6500.0, cie_xyz)
+    emissive_rgb = tuple(float(np.float32(c * light_scale)) for c in rgb)
+    ly = y1 - 1e-3
+    lq = ((-0.25, ly, cz - 0.25), (0.25, ly, cz - 0.25), (0.25, ly, cz + 0.25), (-0.25, ly, cz + 0.25))
+    materials.append(Material(base_color=(0.78, 0.78, 0.78), metalness=0.0, roughness=1.0, emissive=emissive_rgb))
+    lv, li = _quad(*lq)
+    light_sub = Submesh(lv, li, len(materials) - 1, discarded=[0, 1])
+    walls.append(light_sub)
+
+    sv, sf = icosphere(subdiv)
+    spheres = []
+    for (cx, cy, czz, r), kind in (((-0.45, -0.6, cz - 0.3, 0.4), "metal"), ((0.45, -0.6, cz + 0.35, 0.4), "glass")):
+        if kind == "metal":
+            f0 = tuple(rng.uniform(0.5, 1.0) for _ in range(3))
+            materials.append(Material(base_color=f0, metalness=1.0, roughness=0.3))
+        else:
+            materials.append(Material(base_color=(1.0, 1.0, 1.0), metalness=0.0, roughness=0.05,
+                                      transmission=1.0, ior=1.5))
+        pos = (sv * r + np.array([cx, cy, czz])).astype(np.float32)
+        v4 = np.concatenate([pos, np.zeros((len(pos), 1), np.float32)], axis=1)
+        spheres.append([Submesh(v4, sf.astype(np.uint16), len(materials) - 1,
+                                normals=sv.astype(np.float32))])
+
+    # Emissive subset: the light quad's triangles cut out of the wall mesh.
+    tris_obj = np.stack([lv[li[k], :3].reshape(9) for k in range(2)]).astype(np.float32)
+    flux = []
+    for k in range(2):
+        a, b, c = tris_obj[k, 0:3], tris_obj[k, 3:6], tris_obj[k, 6:9]
+        area2 = np.linalg.norm(np.cross((b - a).astype(np.float32), (c - a).astype(np.float32)).astype(np.float32))
+        # scene.cpp:518-523,607: average factor * area * pi, in float32.
+        f = np.float32((np.float32(emissive_rgb[0]) + np.float32(emissive_rgb[1]) + np.float32(emissive_rgb[2])) / np.float32(3.0))
+        f = np.float32(f * (np.float32(area2) * np.float32(0.5) * np.float32(math.pi)))
+        flux.append(f)
+    emissive = [dict(transform=IDENTITY, tris=tris_obj, world=tris_obj.copy(), prim=[0, 1],
+                     flux=np.array(flux, np.float32), material=light_sub.material)]
+
+    meshes = [walls, spheres[0], spheres[1]]
+    instances = [(0, IDENTITY), (1, IDENTITY), (2, IDENTITY)]
+    return Scene(name="cornell_box", seed=seed, meshes=meshes, instances=instances,
+                 materials=materials, emissive=emissive, width=width, height=height,
+                 spp=spp, max_depth=max_depth)

@@ -1,0 +1,305 @@
+"""GPU parity: every stage of the per-sample path on the B200, through the C
+ABI, against the reference's own code run by the oracle on the same inputs.
+
+Tolerances: integer work (QRNG, hashes, hit ids, payload words, ray-origin
+offsets) is bit-exact. Float stages are compared at 1e-5 relative (plus an
+absolute floor for values near zero): the device uses fused multiply-add and
+CUDA's libm, the oracle strict IEEE and glibc. A stage whose result is a
+discrete choice made by comparing floats (BxDF lobe, light-tree child) can
+flip when a probability lands within rounding of the random number; those
+cases are counted and bounded (<= 0.5 %), not ignored.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import cases
+from gpu_util import dev, empty, host, ptr, run_bxdf, run_light, torch
+from oracle_lib import RefLib, light_tree_record, load_scene_into_ref, ref_render, reference_luts, _np_ptr
+from ratbite_b200 import abi, scenes
+from ratbite_b200._native import check, load
+from ratbite_b200.rendering_interface import RenderingInterface
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-5
+
+
+def close(a, b, rtol=RTOL, atol=1e-6):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a - b) <= atol + rtol * np.abs(b)
+
+
+@pytest.fixture(scope="module")
+def ref():
+    return RefLib()
+
+
+@pytest.fixture(scope="module")
+def tables(ref):
+    return dict(cie=ref.cie_xyz(), basis=ref.basis_rgb(), luts=reference_luts())
+
+
+@pytest.fixture(scope="module")
+def cornell(ref, tables):
+    """Cornell box loaded identically into the oracle and the product."""
+    sc = scenes.cornell_box(seed=1, cie_xyz=tables["cie"], width=48, height=48, spp=8)
+    keep = load_scene_into_ref(ref, sc, tables["luts"], tables["cie"], tables["basis"])
+    world, flux, mat, prim = sc.emissive_arrays()
+    tris, nodes, ptrs, masks = ref.build_light_tree(world, flux, mat, prim)
+    lt = light_tree_record(tris, nodes, ptrs, masks, keep)
+    ri = RenderingInterface(device=0)
+    ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lt)
+    yield sc, ri, keep
+    ri.cleanup()
+
+
+def reload_ref(ref, sc, tables, extra=None):
+    return load_scene_into_ref(ref, sc, tables["luts"], tables["cie"], tables["basis"], extra=extra)
+
+
+# ---------------------------------------------------------------- QRNG
+@pytest.mark.parametrize("dims", [1, 2, 3])
+def test_sobol_bit_exact(ref, dims):
+    s, h, b, d = cases.sobol_inputs()
+    n = len(s)
+    want = np.zeros(n * dims, np.float32)
+    ref.lib.rbref_sobol(n, dims, _np_ptr(s), _np_ptr(h), _np_ptr(b), _np_ptr(d), _np_ptr(want))
+    ts, th, tb, td = dev(s), dev(h), dev(b), dev(d)
+    out = empty(n * dims, torch().float32)
+    check(load().rb_k_sobol(n, dims, ptr(ts), ptr(th), ptr(tb), ptr(td), ptr(out), None), None, "rb_k_sobol")
+    got = host(out)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_pixel_hash_exact(ref):
+    rng = np.random.default_rng(1)
+    x = rng.integers(0, 8192, 5000, dtype=np.uint32)
+    y = rng.integers(0, 8192, 5000, dtype=np.uint32)
+    want = np.zeros(5000, np.uint32)
+    ref.lib.rbref_pixel_hash(5000, _np_ptr(x), _np_ptr(y), _np_ptr(want))
+    out = empty(5000, torch().int32)
+    check(load().rb_k_pixel_hash(5000, ptr(dev(x)), ptr(dev(y)), ptr(out), None), None, "pixel hash")
+    assert np.array_equal(host(out).view(np.uint32), want)
+
+
+def test_wavelengths(ref):
+    u = np.random.default_rng(2).random(4096).astype(np.float32)
+    u[:3] = [0.0, 0.5, 0.99999994]
+    lam = np.zeros(4096 * 4, np.float32)
+    pdf = np.zeros(4096 * 4, np.float32)
+    ref.lib.rbref_wavelengths(4096, _np_ptr(u), _np_ptr(lam), _np_ptr(pdf))
+    gl, gp = empty(4096 * 4, torch().float32), empty(4096 * 4, torch().float32)
+    check(load().rb_k_wavelengths(4096, ptr(dev(u)), ptr(gl), ptr(gp), None), None, "wavelengths")
+    assert close(host(gl), lam).all()
+    assert close(host(gp), pdf).all()
+
+
+def test_camera_rays(ref, cornell, tables):
+    sc, ri, _ = cornell
+    reload_ref(ref, sc, tables, )
+    pix, fuv, luv = cases.camera_rays(w=48, h=48)
+    n = len(pix)
+    want = np.zeros(n * 6, np.float32)
+    ref.lib.rbref_camera_ray(n, _np_ptr(pix), _np_ptr(fuv), _np_ptr(luv), _np_ptr(want))
+    out = empty(n * 6, torch().float32)
+    check(load().rb_k_camera_ray(ri.ctx, n, ptr(dev(pix)), ptr(dev(fuv)), ptr(dev(luv)), ptr(out), None), ri.ctx, "camera")
+    assert close(host(out), want, atol=1e-6).all()
+
+
+def test_offset_point_exact(ref):
+    rng = np.random.default_rng(4)
+    p = (rng.normal(size=(4000, 3)) * np.array([[0.01], [1.0], [100.0], [1e-4]] * 1000)).astype(np.float32)
+    nrm = cases.unit_vectors(rng, 4000)
+    want = np.zeros(12000, np.float32)
+    ref.lib.rbref_offset_point(4000, _np_ptr(p), _np_ptr(nrm), _np_ptr(want))
+    out = empty(12000, torch().float32)
+    check(load().rb_k_offset_point(4000, ptr(dev(p)), ptr(dev(nrm)), ptr(out), None), None, "offset")
+    got = host(out)
+    # integer-offset branch is exact; the near-origin branch is a + s*n (FMA on device)
+    assert close(got, want, rtol=2e-7, atol=1e-12).all()
+
+
+def test_octahedral(ref):
+    rng = np.random.default_rng(6)
+    v = cases.unit_vectors(rng, 5000)
+    want = np.zeros(5000, np.uint32)
+    ref.lib.rbref_oct_encode(5000, _np_ptr(v), _np_ptr(want))
+    out = empty(5000, torch().int32)
+    check(load().rb_k_oct_encode(5000, ptr(dev(v)), ptr(out), None), None, "oct encode")
+    got = host(out).view(np.uint32)
+    dx = np.abs((got & 0xFFFF).astype(np.int64) - (want & 0xFFFF).astype(np.int64))
+    dy = np.abs((got >> 16).astype(np.int64) - (want >> 16).astype(np.int64))
+    assert dx.max() <= 1 and dy.max() <= 1            # quantisation boundary under FMA
+    assert (got == want).mean() > 0.999
+    dec = np.zeros(15000, np.float32)
+    ref.lib.rbref_oct_decode(5000, _np_ptr(want), _np_ptr(dec))
+    out3 = empty(15000, torch().float32)
+    check(load().rb_k_oct_decode(5000, ptr(dev(want)), ptr(out3), None), None, "oct decode")
+    assert close(host(out3), dec, atol=1e-6).all()
+
+
+# ------------------------------------------------------------ traversal
+def test_trace_payload_exact(ref, cornell, tables):
+    sc, ri, _ = cornell
+    reload_ref(ref, sc, tables)
+    rays = cases.scene_rays()
+    n = len(rays)
+    pl = np.zeros(n * 24, np.uint32)
+    t = np.zeros(n, np.float32)
+    tri = np.zeros(n, np.int32)
+    ref.lib.rbref_trace(n, _np_ptr(rays), _np_ptr(pl), _np_ptr(t), _np_ptr(tri))
+    gpl, gt, gtri = empty(n * 24, torch().int32), empty(n, torch().float32), empty(n, torch().int32)
+    check(load().rb_k_trace(ri.ctx, n, ptr(dev(rays)), ptr(gpl), ptr(gt), ptr(gtri), None), ri.ctx, "trace")
+    gtri, gt, gpl = host(gtri), host(gt), host(gpl).view(np.uint32).reshape(n, 24)
+    pl = pl.reshape(n, 24)
+    assert (tri >= 0).mean() > 0.9
+    assert np.array_equal(gtri, tri)
+    hit = tri >= 0
+    assert np.array_equal(gt[hit].view(np.uint32), t[hit].view(np.uint32))
+    # every payload word the closest-hit / miss programs write
+    assert np.array_equal(gpl[hit], pl[hit])
+    assert np.array_equal(gpl[~hit][:, 8], pl[~hit][:, 8])
+
+
+def test_occlusion_exact(ref, cornell, tables):
+    sc, ri, _ = cornell
+    reload_ref(ref, sc, tables)
+    rays = cases.scene_rays(seed=23)
+    n = len(rays)
+    tmax = np.random.default_rng(5).uniform(0.01, 4.0, n).astype(np.float32)
+    want = np.zeros(n, np.uint32)
+    ref.lib.rbref_occluded(n, _np_ptr(rays), _np_ptr(tmax), _np_ptr(want))
+    out = empty(n, torch().int32)
+    check(load().rb_k_occluded(ri.ctx, n, ptr(dev(rays)), ptr(dev(tmax)), ptr(out), None), ri.ctx, "occluded")
+    assert np.array_equal(host(out).view(np.uint32), want)
+
+
+# ------------------------------------------------------------------ BxDF
+def _bxdf_setup(ref, tables):
+    mats = cases.material_table()
+    recs = cases.bxdf_material_records(mats)
+    extra = np.stack([ref.named_spectrum(cases.SPEC_AU_IOR), ref.named_spectrum(cases.SPEC_AU_AC),
+                      ref.named_spectrum(cases.SPEC_CU_IOR), ref.named_spectrum(cases.SPEC_CU_AC)])
+    L = ref.lib
+    L.rbref_reset()
+    L.rbref_set_spectra(_np_ptr(tables["cie"]), _np_ptr(tables["basis"]), _np_ptr(extra), len(extra))
+    lut_arrays = [np.ascontiguousarray(tables["luts"][k], np.float32) for k in
+                  ("conductor", "dielectric_outer", "dielectric_inner", "reflective_outer", "reflective_inner", "sheen")]
+    L.rbref_set_luts(*[_np_ptr(a) for a in lut_arrays])
+    assert L.rbref_set_materials(C.cast(recs, C.c_void_p), len(recs)) == 0
+    ri = RenderingInterface(device=0)
+    ri.load_look_up_tables(tables["luts"])
+    ri.fill_spectral_curves_data(tables["cie"], tables["basis"], extra)
+    ri.fill_model_materials(recs)
+    return ri, (recs, extra, lut_arrays)
+
+
+def test_bxdf_parity(ref, tables):
+    ri, keep = _bxdf_setup(ref, tables)
+    cs = cases.bxdf_cases()
+    n = len(cs)
+    want = (abi.rb_bxdf_case * n).from_buffer_copy(bytes(cs))
+    ref.lib.rbref_bxdf(n, C.cast(want, C.c_void_p))
+    got = run_bxdf(ri, cs)
+    ri.cleanup()
+
+    def arr(cs_, f, k=None):
+        return np.array([getattr(c, f)[:] if k else getattr(c, f) for c in cs_], np.float64)
+    flags_eq = np.array([a.flags == b.flags for a, b in zip(got, want)])
+    dirs_ok = close(arr(got, "dir", 1), arr(want, "dir", 1), rtol=1e-4, atol=2e-5).all(axis=1)
+    pdf_ok = close(arr(got, "bxdf_pdf"), arr(want, "bxdf_pdf"), rtol=1e-4, atol=1e-6)
+    thr_ok = close(arr(got, "throughput", 1), arr(want, "throughput", 1), rtol=1e-4, atol=1e-6).all(axis=1)
+    L_ok = close(arr(got, "L", 1), arr(want, "L", 1), rtol=1e-4, atol=1e-6).all(axis=1)
+    ok = flags_eq & dirs_ok & pdf_ok & thr_ok & L_ok
+    frac_bad = 1.0 - ok.mean()
+    print(f"bxdf cases {n}: mismatch fraction {frac_bad:.4%} (flags {1 - flags_eq.mean():.4%}, "
+          f"dir {1 - dirs_ok.mean():.4%}, pdf {1 - pdf_ok.mean():.4%}, T {1 - thr_ok.mean():.4%}, L {1 - L_ok.mean():.4%})")
+    assert frac_bad <= 0.005
+    # the typical case is far tighter than the bound
+    good = ok & (arr(want, "bxdf_pdf") > 0)
+    rel = np.abs(arr(got, "bxdf_pdf")[good] - arr(want, "bxdf_pdf")[good]) / np.abs(arr(want, "bxdf_pdf")[good])
+    assert np.median(rel) < 1e-6
+
+
+# ------------------------------------------------------------- light tree
+def test_light_tree_parity(ref, tables):
+    sc = cases.many_lights_scene()
+    keep = reload_ref(ref, sc, tables)
+    world, flux, mat, prim = sc.emissive_arrays()
+    tris, nodes, ptrs, masks = ref.build_light_tree(world, flux, mat, prim)
+    assert len(nodes) > 20
+    lt = light_tree_record(tris, nodes, ptrs, masks, keep)
+    ri = RenderingInterface(device=0)
+    ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lt)
+    cs = cases.light_cases()
+    n = len(cs)
+    want = (abi.rb_light_case * n).from_buffer_copy(bytes(cs))
+    ref.lib.rbref_light_tree(n, C.cast(want, C.c_void_p))
+    got = run_light(ri, cs)
+    ri.cleanup()
+    same_pick = np.array([(a.type, a.index) == (b.type, b.index) for a, b in zip(got, want)])
+    print(f"light picks identical: {same_pick.mean():.4%}")
+    assert same_pick.mean() >= 0.995
+    gp = np.array([c.pdf for c in got]); wp = np.array([c.pdf for c in want])
+    assert close(gp[same_pick], wp[same_pick], rtol=1e-4, atol=1e-9).mean() >= 0.999
+    gq = np.array([c.q_pdf for c in got]); wq = np.array([c.q_pdf for c in want])
+    assert close(gq, wq, rtol=1e-4, atol=1e-9).mean() >= 0.999
+
+
+# ----------------------------------------------------------------- render
+def _image_stats(got, want):
+    g = got[..., :3] / np.maximum(got[..., 3:4], 1)
+    w = want[..., :3] / np.maximum(want[..., 3:4], 1)
+    rel_mean = abs(g.sum() - w.sum()) / abs(w.sum())
+    l1 = np.abs(g - w).sum() / np.abs(w).sum()
+    return rel_mean, l1
+
+
+def test_render_parity_cornell(ref, tables, cornell):
+    sc, ri, _ = cornell
+    reload_ref(ref, sc, tables)
+    W, H, spp = 48, 48, 8
+    want = ref_render(ref, W, H, 0, spp)
+    ri.render(0, spp)
+    got = ri.read_accumulation()
+    st = ri.status()
+    assert st.flags == 0
+    assert np.array_equal(got[..., 3], want[..., 3])
+    rel_mean, l1 = _image_stats(got, want)
+    print(f"cornell {W}x{H}x{spp}: image-mean rel diff {rel_mean:.3e}, per-pixel L1 {l1:.3e}")
+    assert rel_mean < 5e-3
+    assert l1 < 5e-2
+
+
+def test_render_progressive_offsets(ref, tables, cornell):
+    """Sample ranges accumulate like one launch: [0,3) + [3,8) == [0,8)."""
+    sc, ri, _ = cornell
+    ri.render(0, 8)
+    full = ri.read_accumulation()
+    ri.render(0, 3)
+    ri.render(3, 5)
+    split = ri.read_accumulation()
+    assert np.array_equal(full, split)
+
+
+def test_render_many_lights(ref, tables):
+    sc = cases.many_lights_scene()
+    W, H, spp = 32, 32, 8
+    keep = load_scene_into_ref(ref, sc, tables["luts"], tables["cie"], tables["basis"], width=W, height=H)
+    world, flux, mat, prim = sc.emissive_arrays()
+    tris, nodes, ptrs, masks = ref.build_light_tree(world, flux, mat, prim)
+    lt = light_tree_record(tris, nodes, ptrs, masks, keep)
+    want = ref_render(ref, W, H, 0, spp)
+    with RenderingInterface(device=0) as ri:
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lt, width=W, height=H)
+        ri.render(0, spp)
+        got = ri.read_accumulation()
+    rel_mean, l1 = _image_stats(got, want)
+    print(f"many lights {W}x{H}x{spp}: image-mean rel diff {rel_mean:.3e}, per-pixel L1 {l1:.3e}")
+    assert rel_mean < 1e-2
+    assert l1 < 1e-1
