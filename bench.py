@@ -1,25 +1,28 @@
 """Benchmark of the per-sample rendering path on B200.
 
-Workload (the small plain-method configuration): seeded Cornell box, 2,574
-triangles, 256x256 pixels, 64 samples per pixel, max depth 8, 4 hero
-wavelengths. One step renders the whole 64-spp frame (4,194,304 paths);
-metric = paths per second (higher is better).
+Default workload (the plain method at scale): seeded scene of ~2.03M
+triangles from 128 instances of noise-displaced spheres, tori and boxes,
+256 materials, 4,096 emissive triangles with lognormal(0, 1.5) radiance in a
+Gaussian light tree, a 1024x512 sky + sun environment map whose 2D CDF is
+rebuilt every frame; 1920x1080, 256 samples per pixel, depth 12. One step =
+one frame: CDF rebuild + 530,841,600 paths. Metric: paths per second.
+`--workload cornell` selects the small configuration (Cornell box, 256x256,
+64 spp, depth 8).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 ours       renders through the C ABI (libratbite_b200.so). `value` is device
            time (CUDA events on the render stream, max over ranks); `e2e` is
-           the same metric through the public API with the per-step launch
-           parameters uploaded and the FP64 accumulation buffer read back to
-           host memory inside the timed region.
+           the same metric through the public API with the launch parameters
+           uploaded and the FP64 accumulation buffer read back to host memory
+           inside the timed region, every step.
 reference  the reference's own per-sample code compiled host-side
            (oracle/_ref) rendering the same scene on all host cores; each step
-           renders a bounded number of samples of the same frame.
+           is a bounded sample (a band of rows at a few samples per pixel).
 
-With N GPUs (torchrun) each rank renders its own 64-spp sample range of the
-frame (weak scaling; Sobol indices are disjoint) and the FP64 images are
-summed with one NCCL all-reduce per step, the combine step of progressive
-rendering across devices.
+With N GPUs (torchrun) each rank renders its own sample range of the frame
+(weak scaling; disjoint Sobol indices) and the FP64 images are summed by one
+NCCL all-reduce per step, the combine step of progressive rendering.
 """
 from __future__ import annotations
 
@@ -29,7 +32,6 @@ import json
 import os
 import subprocess
 import sys
-import threading
 import time
 from pathlib import Path
 
@@ -38,9 +40,23 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-W, H, SPP, DEPTH = 256, 256, 64, 8
 METRIC = "paths/s"
-WORKLOAD = "cornell_box_256x256_64spp_depth8"
+
+WORKLOADS = {
+    "scale": dict(name="scale_2M_tris_1920x1080_256spp_depth12_envcdf_per_frame", width=1920, height=1080,
+                  spp=256, depth=12),
+    "cornell": dict(name="cornell_box_256x256_64spp_depth8", width=256, height=256, spp=64, depth=8),
+}
+
+# Algorithmic bytes of one shading step (kShade) per path vertex: path state
+# read and written (ray o/d, wavelengths, pdfs, normal, L, T: 7 x 16 B,
+# twice), flags, the hit record, the hit triangle (3 x 16 B + 8 B), the
+# material record (128 B), the vertex indices and 3 attribute reads
+# (6 + 24 B), LUT taps (two 3D tables x 8 taps + one 2D x 4 taps, 4 B
+# each), spectral basis / sensor lookups (12 x 4 B), the emitter record
+# (68 B) and the shadow request written (48 B). Light-tree node reads grow
+# with tree depth and are not counted.
+SHADE_BYTES_PER_PATH = 2 * 7 * 16 + 2 * 8 + 16 + 56 + 128 + 30 + 20 * 4 + 12 * 4 + 68 + 48
 
 
 def peaks():
@@ -61,6 +77,7 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.lines = []
 
     def __enter__(self):
         try:
@@ -72,7 +89,6 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
         if self.proc is not None:
             time.sleep(0.25)
             self.proc.terminate()
@@ -86,7 +102,7 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
+        for l in self.lines:
             f = [x.strip() for x in l.split(",")]
             if len(f) < 9:
                 continue
@@ -103,72 +119,82 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_scene():
+def make_scene(wl: dict):
     from ratbite_b200 import assets, scenes
     cie = assets.cie_xyz()
     basis = assets.basis_rgb()
     luts = assets.luts()
-    scene = scenes.cornell_box(seed=1, cie_xyz=cie, width=W, height=H, spp=SPP, max_depth=DEPTH)
+    if wl["width"] == 256:
+        scene = scenes.cornell_box(seed=1, cie_xyz=cie, width=wl["width"], height=wl["height"], spp=wl["spp"],
+                                   max_depth=wl["depth"])
+    else:
+        scene = scenes.scale_scene(seed=3, width=wl["width"], height=wl["height"], spp=wl["spp"],
+                                   max_depth=wl["depth"])
     return scene, cie, basis, luts
 
 
-def build_light_tree(scene):
-    from ratbite_b200 import lighttree
-    return lighttree.build_for_scene(scene)
-
-
 # ------------------------------------------------------------- CPU baseline
-def cpu_render(scene, cie, basis, luts, target_s: float, threads: int = 0):
-    """Times the reference's code (oracle/_ref) on the host cores on a
-    bounded sample of the frame; returns (paths/s, cores, sample text)."""
+def _ref_setup(scene, cie, basis, luts):
     sys.path.insert(0, str(ROOT / "tests"))
     from oracle_lib import RefLib, load_scene_into_ref
     ref = RefLib()
     keep = load_scene_into_ref(ref, scene, luts, cie, basis)
-    cores = threads or os.cpu_count() or 1
+    return ref, keep
+
+
+def _calibrate(ref, wl, cores, target_s):
+    """Rows x spp of a band that takes about target_s on `cores` threads."""
+    W, H = wl["width"], wl["height"]
+    rows = min(H, 8)
     t0 = time.perf_counter()
-    ref.lib.rbref_render(0, 1, cores)
-    dt1 = max(time.perf_counter() - t0, 1e-3)
-    spp = int(max(1, min(SPP, round(target_s / dt1))))
+    ref.lib.rbref_render_rows(0, 1, cores, 0, rows)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    per_row_spp = dt / rows
+    budget_rows_spp = max(1.0, target_s / per_row_spp)
+    spp = int(min(wl["spp"], max(1, budget_rows_spp // H)))
+    rows = int(min(H, max(1, budget_rows_spp // spp)))
+    return rows, spp
+
+
+def cpu_baseline(scene, cie, basis, luts, wl, target_s):
+    ref, keep = _ref_setup(scene, cie, basis, luts)
+    cores = os.cpu_count() or 1
+    rows, spp = _calibrate(ref, wl, cores, target_s)
+    r0 = (wl["height"] - rows) // 2
     t0 = time.perf_counter()
-    ref.lib.rbref_render(0, spp, cores)
+    ref.lib.rbref_render_rows(0, spp, cores, r0, r0 + rows)
     dt = time.perf_counter() - t0
-    paths = W * H * spp
+    paths = wl["width"] * rows * spp
     del keep
-    return paths / dt, cores, f"{W}x{H} at {spp} spp ({paths} paths, {dt:.2f} s)"
+    return paths / dt, cores, f"{wl['width']}x{rows} rows (centre band) at {spp} spp: {paths} paths in {dt:.2f} s"
 
 
 # ----------------------------------------------------------- reference arm
-def run_reference(args, rank: int, world: int):
+def run_reference(args, rank: int, world: int, wl: dict):
     if rank != 0:
         return
-    scene, cie, basis, luts = make_scene()
-    sys.path.insert(0, str(ROOT / "tests"))
-    from oracle_lib import RefLib, load_scene_into_ref
-    ref = RefLib()
-    keep = load_scene_into_ref(ref, scene, luts, cie, basis)
+    scene, cie, basis, luts = make_scene(wl)
+    ref, keep = _ref_setup(scene, cie, basis, luts)
     cores = os.cpu_count() or 1
+    rows, spp = _calibrate(ref, wl, cores, args.ref_step_s)
+    r0 = (wl["height"] - rows) // 2
+    for _ in range(args.warmup):
+        ref.lib.rbref_render_rows(0, spp, cores, r0, r0 + rows)
     t0 = time.perf_counter()
-    ref.lib.rbref_render(0, 1, cores)
-    dt1 = max(time.perf_counter() - t0, 1e-3)
-    spp = int(max(1, min(SPP, round(args.ref_step_s / dt1))))
-    for i in range(args.warmup):
-        ref.lib.rbref_render(0, spp, cores)
-    t0 = time.perf_counter()
-    for i in range(args.steps):
-        ref.lib.rbref_render(0, spp, cores)
+    for _ in range(args.steps):
+        ref.lib.rbref_render_rows(0, spp, cores, r0, r0 + rows)
     dt = time.perf_counter() - t0
-    paths = W * H * spp * args.steps
+    paths = wl["width"] * rows * spp * args.steps
     v = paths / dt
+    sample = f"{wl['width']}x{rows} rows (centre band) at {spp} spp per step, {args.steps} steps"
     line = {
         "metric": METRIC, "value": v, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
         "impl": "reference",
-        "config": {"workload": WORKLOAD, "width": W, "height": H, "spp_per_step": spp,
-                   "max_depth": DEPTH, "triangles": scene.triangle_count()},
-        "cpu_baseline": {"value": v, "unit": "paths/s", "cores": cores, "kind": "reference",
-                         "sample": f"{W}x{H} at {spp} spp per step, {args.steps} steps"},
+        "config": {"workload": wl["name"], "width": wl["width"], "height": wl["height"], "spp": wl["spp"],
+                   "max_depth": wl["depth"], "triangles": scene.triangle_count(), "sample_per_step": sample},
+        "cpu_baseline": {"value": v, "unit": "paths/s", "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     del keep
@@ -176,34 +202,41 @@ def run_reference(args, rank: int, world: int):
 
 
 # ---------------------------------------------------------------- our arm
-def run_ours(args, rank: int, world: int):
+def run_ours(args, rank: int, world: int, wl: dict):
     import torch
-    from ratbite_b200 import abi
+    from ratbite_b200 import abi, lighttree
     from ratbite_b200.rendering_interface import RenderingInterface
 
+    W, H, SPP = wl["width"], wl["height"], wl["spp"]
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
-    scene, cie, basis, luts = make_scene()
-    lt = build_light_tree(scene)
+    t_setup = time.perf_counter()
+    scene, cie, basis, luts = make_scene(wl)
+    lt = lighttree.build_for_scene(scene)
     ri = RenderingInterface(device=local)
     ri.load_scene(scene, luts, cie, basis, light_tree=lt)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t_setup
+    has_env = getattr(scene, "envmap", None) is not None
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
     launch = scene.launch_record()
-    accum_dev = torch.zeros((H, W, 4), dtype=torch.float64, device="cuda")
+    accum_dev = torch.zeros((H, W, 4), dtype=torch.float64, device="cuda") if world > 1 else None
     offset = rank * SPP                     # disjoint Sobol sample range per rank
 
-    def step():
-        ri.render(offset, SPP, stream=sp)
+    def step(s=sp):
+        if has_env:
+            ri.rebuild_environment_cdf(stream=s)
+        ri.render(offset, SPP, stream=s)
         if world > 1:
-            ri.copy_accumulation_async(accum_dev.data_ptr(), stream=sp)
+            ri.copy_accumulation_async(accum_dev.data_ptr(), stream=s)
             with torch.cuda.stream(stream):
                 dist.all_reduce(accum_dev)
 
@@ -216,7 +249,7 @@ def run_ours(args, rank: int, world: int):
         step()
     torch.cuda.synchronize()
 
-    # ---- device-timed region (per-stage events on the render stream)
+    # ---- device-timed region (per-stage CUDA events on the render stream)
     ri.set_stats(abi.RB_STATS_TIME)
     ri.get_stats()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -240,13 +273,15 @@ def run_ours(args, rank: int, world: int):
     value = paths_per_step * args.steps / (ms / 1e3)
 
     # ---- end to end through the public API (host copies inside the region)
-    host = np.zeros((H, W, 4), np.float64)
+    e2e_steps = max(1, args.steps // 2)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(e2e_steps):
         ri.prepare_data_for_rendering(launch)            # H2D: launch parameters
+        if has_env:
+            ri.rebuild_environment_cdf()
         ri.render(offset, SPP)
         host = ri.read_accumulation()                    # D2H: FP64 accumulation
     torch.cuda.synchronize()
@@ -255,56 +290,60 @@ def run_ours(args, rank: int, world: int):
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = paths_per_step * args.steps / e2e_s
+    e2e_value = paths_per_step * e2e_steps / e2e_s
     st = ri.status()
 
     if rank == 0:
-        # Roofline of the dominant stage (HBM-bound model; bytes per unit in DESIGN.md).
         hbm, peak_kind = peaks()
         shares = {"extend": stages.ms_extend, "shade": stages.ms_shade, "shadow": stages.ms_shadow,
                   "generate": stages.ms_generate, "resolve": stages.ms_resolve}
         total_ms = sum(shares.values())
         dom = max(("extend", "shade", "shadow"), key=lambda k: shares[k])
-        per_step = lambda x: x / max(1, counts.waves)          # counts were gathered over one step
-        ext_rays = per_step(counts.extend_rays)
-        sh_rays = per_step(counts.shadow_rays)
+        # counts were gathered over one step
+        ext_rays, sh_rays = counts.extend_rays, counts.shadow_rays
         if dom == "extend":
-            bytes_step = ext_rays * (32 + 16) + per_step(counts.extend_nodes) * 96 + per_step(counts.extend_tris) * 48
+            bytes_step = ext_rays * (32 + 16) + counts.extend_nodes * 96 + counts.extend_tris * 48
             launches = stages.launches_extend
         elif dom == "shadow":
-            bytes_step = sh_rays * (32 + 4) + per_step(counts.shadow_nodes) * 96 + per_step(counts.shadow_tris) * 48
+            bytes_step = sh_rays * (32 + 4) + counts.shadow_nodes * 96 + counts.shadow_tris * 48
             launches = stages.launches_shadow
         else:
             bytes_step = ext_rays * SHADE_BYTES_PER_PATH
             launches = stages.launches_shade
-        stage_ms = shares[dom]
-        achieved = bytes_step * args.steps / (stage_ms / 1e3) / 1e9
-        launches_per_step = (stages.launches_generate + stages.launches_extend + stages.launches_shade
-                             + stages.launches_shadow + stages.launches_resolve) / args.steps
+        achieved = bytes_step * args.steps / (shares[dom] / 1e3) / 1e9
+        launches_total = (stages.launches_generate + stages.launches_extend + stages.launches_shade
+                          + stages.launches_shadow + stages.launches_resolve)
         traffic = None
         tp = ROOT / "profiles" / "traffic.json"
         if tp.exists():
-            traffic = json.loads(tp.read_text()).get(dom)
-        cpu_v, cores, sample = cpu_render(scene, cie, basis, luts, args.cpu_seconds) if args.cpu_seconds > 0 else (None, 0, "skipped")
+            traffic = json.loads(tp.read_text()).get(wl["name"], {}).get(dom)
+        if args.cpu_seconds > 0:
+            cpu_v, cores, sample = cpu_baseline(scene, cie, basis, luts, wl, args.cpu_seconds)
+        else:
+            cpu_v, cores, sample = None, 0, "skipped"
         line = {
             "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "max_depth": DEPTH,
-                       "triangles": scene.triangle_count(), "paths_per_step": paths_per_step,
-                       "parallelism": f"sample-range x{world}",
-                       "l2": "inputs larger than L2 (wavefront path state ~800 MB per wave)"},
+            "config": {"workload": wl["name"], "width": W, "height": H, "spp": SPP, "max_depth": wl["depth"],
+                       "triangles": scene.triangle_count(), "emitters": int(sum(len(e["prim"]) for e in scene.emissive)),
+                       "materials": len(scene.materials), "envmap": list(scene.envmap.shape[1::-1]) if has_env else None,
+                       "paths_per_step": paths_per_step, "parallelism": f"sample-range x{world}",
+                       "l2": "inputs larger than L2 (wavefront path state ~3.2 GB per wave)",
+                       "setup_s": setup_s},
             "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": C.sizeof(launch),
-                    "d2h_bytes_per_step": W * H * 32},
-            "gpu_launches": int(round(launches_per_step * args.steps)),
+                    "d2h_bytes_per_step": W * H * 32, "steps": e2e_steps},
+            "gpu_launches": int(launches_total),
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "bytes_per_launch": bytes_step / max(1, launches / args.steps)},
             "stages_ms_per_step": {k: v / args.steps for k, v in shares.items()},
             "stage_share": {k: (v / total_ms if total_ms else None) for k, v in shares.items()},
             "rays_per_step": {"extend": ext_rays, "shadow": sh_rays,
-                              "nodes_per_extend_ray": counts.extend_nodes / max(1, counts.extend_rays),
-                              "tris_per_extend_ray": counts.extend_tris / max(1, counts.extend_rays)},
+                              "nodes_per_extend_ray": counts.extend_nodes / max(1, ext_rays),
+                              "tris_per_extend_ray": counts.extend_tris / max(1, ext_rays),
+                              "nodes_per_shadow_ray": counts.shadow_nodes / max(1, sh_rays),
+                              "tris_per_shadow_ray": counts.shadow_tris / max(1, sh_rays)},
             "device_status_flags": st.flags,
             "clocks": clocks.summary(),
             "cpu_baseline": {"value": cpu_v, "unit": "paths/s", "cores": cores, "kind": "reference",
@@ -317,33 +356,24 @@ def run_ours(args, rank: int, world: int):
         dist.destroy_process_group()
 
 
-# Algorithmic bytes of one shading step (kShade) per path: path state read and
-# written (ray o/d, wavelengths, pdfs, normal, L, T: 7 x 16 B, twice), flags,
-# the hit record, the hit triangle (3 x 16 B + 8 B), the material record
-# (128 B), the vertex indices and 3 attribute reads (6 + 24 B), LUT taps (two
-# 3D tables x 8 taps + one 2D x 4 taps, 4 B each), spectral basis and sensor
-# lookups (12 x 4 B), the emitter record (68 B) and the shadow request written
-# (48 B). Light-tree node reads grow with tree depth and are not counted.
-SHADE_BYTES_PER_PATH = 2 * 7 * 16 + 2 * 8 + 16 + 56 + 128 + 30 + 20 * 4 + 12 * 4 + 68 + 48
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="scale")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample length (0 = skip)")
     ap.add_argument("--ref-step-s", type=float, default=4.0, help="reference arm: seconds per step")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
-    if args.warmup < 3:
-        args.warmup = 3
+    args.warmup = max(args.warmup, 3)
+    wl = WORKLOADS[args.workload]
     if args.impl == "reference":
-        run_reference(args, rank, world)
+        run_reference(args, rank, world, wl)
     else:
-        run_ours(args, rank, world)
+        run_ours(args, rank, world, wl)
 
 
 if __name__ == "__main__":

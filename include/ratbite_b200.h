@@ -77,9 +77,12 @@ typedef struct rb_ctx rb_ctx;
 
 typedef struct rb_config {
     int32_t device;              /* CUDA device ordinal */
-    uint32_t max_paths_in_flight;/* wavefront capacity; 0 = choose from the device */
-    uint32_t reserved[6];
+    uint32_t max_paths_in_flight;/* wavefront capacity; 0 = default (16M paths) */
+    uint32_t envmap_cdf_mode;    /* RB_CDF_FP64 (default, 0) or RB_CDF_REFERENCE */
+    uint32_t reserved[5];
 } rb_config;
+#define RB_CDF_FP64       0u     /* float64 row/column sums */
+#define RB_CDF_REFERENCE  1u     /* float32 in the reference's scan order: bit-identical tables */
 
 /*
  * One material record: MaterialData (src/core/material.h:17-107) field for
@@ -236,6 +239,9 @@ int rb_build_light_tree(uint32_t n, const float* world_vertices, const float* fl
 /* Replaces loadEnvironmentMap's CDF launches (:1339-1432): rgba is w*h float4
  * (w, h multiples of 4); the 2D CDF is built on the device. */
 int rb_set_envmap(rb_ctx* ctx, const float* rgba, uint32_t width, uint32_t height);
+/* Rebuilds the CDF of the resident map on `stream` (the per-frame rebuild of
+ * the at-scale workload); stream-ordered, no host synchronisation. */
+int rb_rebuild_envmap_cdf(rb_ctx* ctx, void* stream);
 int rb_clear_envmap(rb_ctx* ctx);
 int rb_set_launch(rb_ctx* ctx, const rb_launch* launch);
 

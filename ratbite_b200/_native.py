@@ -31,6 +31,7 @@ SIGNATURES = {
     "rb_build_light_tree": (C.c_int, [_U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "rb_set_envmap": (C.c_int, [_P, _P, _U32, _U32]),
     "rb_clear_envmap": (C.c_int, [_P]),
+    "rb_rebuild_envmap_cdf": (C.c_int, [_P, _P]),
     "rb_set_launch": (C.c_int, [_P, _P]),
     "rb_render": (C.c_int, [_P, _U32, _U32, _P]),
     "rb_read_accum": (C.c_int, [_P, _P]),

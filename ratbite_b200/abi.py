@@ -79,9 +79,13 @@ F4 = C.c_float * 4
 F12 = C.c_float * 12
 
 
+RB_CDF_FP64 = 0
+RB_CDF_REFERENCE = 1
+
+
 class rb_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_paths_in_flight", C.c_uint32),
-                ("reserved", C.c_uint32 * 6)]
+                ("envmap_cdf_mode", C.c_uint32), ("reserved", C.c_uint32 * 5)]
 
 
 class rb_material(C.Structure):

@@ -39,10 +39,17 @@ struct rb_ctx
 	std::vector<void*> soaBufs;
 	uint32_t capacity = 0;
 	uint32_t requestedCapacity = 0;
+	uint32_t cdfMode = RB_CDF_FP64;
+	void* envScratch = nullptr;                 // CDF scratch of the current map (in envBufs)
+	float* envIntegral = nullptr;               // device scalar (in envBufs)
 	double4* accum = nullptr;
 	size_t accumPixels = 0;
 	bool haveLaunch = false, haveGeometry = false;
 	uint64_t pathsTraced = 0;
+	// cross-table references checked before any kernel reads them
+	uint32_t geoEmissive = 0;                   // emissive triangles traced by the geometry
+	uint32_t geoMaxMaterial = 0;                // 1 + largest material index of the geometry
+	uint32_t lightMaxMaterial = 0;              // 1 + largest material index of the light records
 	// instrumentation (rb_set_stats)
 	uint32_t statsMode = 0;
 	unsigned long long* counters = nullptr;     // 6 device counters
@@ -166,6 +173,16 @@ void timedStage(rb_ctx* ctx, int stage, cudaStream_t st, F&& launch)
 	ctx->timed.push_back(t);
 }
 
+// Every index a kernel will follow must land inside its table.
+int checkReferences(rb_ctx* ctx)
+{
+	if (ctx->geoMaxMaterial > ctx->scene.materialCount || ctx->lightMaxMaterial > ctx->scene.materialCount)
+		return fail(ctx, RB_ERR_INVALID, "material index out of range of the material table");
+	if (ctx->geoEmissive > ctx->scene.lights.triangleCount)
+		return fail(ctx, RB_ERR_INVALID, "geometry traces more emissive triangles than the light data holds");
+	return RB_OK;
+}
+
 void releaseWave(rb_ctx* ctx)
 {
 	freeAll(ctx->soaBufs);
@@ -208,6 +225,8 @@ int rb_create(const rb_config* config, rb_ctx** out)
 	if (!ctx) return RB_ERR_OOM;
 	ctx->device = config ? config->device : 0;
 	ctx->requestedCapacity = config ? config->max_paths_in_flight : 0u;
+	if (config && config->envmap_cdf_mode > RB_CDF_REFERENCE) { delete ctx; return RB_ERR_INVALID; }
+	ctx->cdfMode = config ? config->envmap_cdf_mode : RB_CDF_FP64;
 	cudaError_t e = cudaSetDevice(ctx->device);
 	if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
 	if (e == cudaSuccess) e = cudaMalloc(&ctx->status, 2 * sizeof(uint32_t));
@@ -440,6 +459,10 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 	G.nodeCount = static_cast<uint32_t>(bvh.nodes.size());
 	G.triCount = static_cast<uint32_t>(nt);
 	G.rootIsLeaf = bvh.rootIsLeaf ? 1u : 0u;
+	ctx->geoEmissive = emissivePrim;
+	ctx->geoMaxMaterial = 0;
+	for (uint32_t s : sbt)
+		if (s != 0xFFFFFFFFu) ctx->geoMaxMaterial = std::max(ctx->geoMaxMaterial, s + 1);
 	ctx->haveGeometry = true;
 	return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? RB_OK : fail(ctx, RB_ERR_CUDA, "geometry upload");
 }
@@ -482,6 +505,9 @@ int rb_set_lights(rb_ctx* ctx, const rb_light_tree* t)
 	L.nodes = dn;
 	L.nodeCount = t->node_count;
 	L.triangleCount = t->triangle_count;
+	ctx->lightMaxMaterial = 0;
+	const rb::EmissiveTri* lt = static_cast<const rb::EmissiveTri*>(t->triangles);
+	for (uint32_t i = 0; i < t->triangle_count; ++i) ctx->lightMaxMaterial = std::max(ctx->lightMaxMaterial, lt[i].material + 1);
 	return RB_OK;
 }
 
@@ -506,20 +532,34 @@ int rb_set_envmap(rb_ctx* ctx, const float* rgba, uint32_t w, uint32_t h)
 	if (rc == RB_OK) rc = upload(ctx, ctx->envBufs, nullptr, sizeof(float), integral);
 	if (rc == RB_OK) rc = upload(ctx, ctx->envBufs, nullptr, rb_envmap_cdf_scratch_bytes(w, h), scratch);
 	if (rc != RB_OK) return rc;
-	rc = rb_envmap_cdf(w, h, reinterpret_cast<const float*>(tex), 1, scratch, cond, marg, integral, ctx->stream);
+	// kernel mode 0 is the reference order, 1 the float64 sums
+	const int kmode = ctx->cdfMode == RB_CDF_REFERENCE ? 0 : 1;
+	rc = rb_envmap_cdf(w, h, reinterpret_cast<const float*>(tex), kmode, scratch, cond, marg, integral, ctx->stream);
 	if (rc != RB_OK) return fail(ctx, rc, "rb_set_envmap: CDF build failed");
-	float hi = 0.0f;
-	cudaError_t e = cudaMemcpyAsync(&hi, integral, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
-	if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+	const cudaError_t e = cudaStreamSynchronize(ctx->stream);
 	if (e != cudaSuccess) return cudaFail(ctx, e, "rb_set_envmap");
 	E.enabled = 1;
 	E.w = w; E.h = h;
 	E.width = static_cast<float>(w); E.height = static_cast<float>(h);
-	E.integral = hi;
+	E.integral = integral;
 	E.texels = tex;
 	E.conditional = cond;
 	E.marginal = marg;
+	ctx->envScratch = scratch;
+	ctx->envIntegral = integral;
 	return RB_OK;
+}
+
+int rb_rebuild_envmap_cdf(rb_ctx* ctx, void* stream)
+{
+	if (!ctx) return RB_ERR_INVALID;
+	if (!ctx->scene.env.enabled) return fail(ctx, RB_ERR_NO_SCENE, "rb_rebuild_envmap_cdf: no environment map");
+	cudaSetDevice(ctx->device);
+	rb::DevEnvMap& E = ctx->scene.env;
+	const int kmode = ctx->cdfMode == RB_CDF_REFERENCE ? 0 : 1;
+	const int rc = rb_envmap_cdf(E.w, E.h, reinterpret_cast<const float*>(E.texels), kmode, ctx->envScratch,
+		const_cast<uint16_t*>(E.conditional), const_cast<uint16_t*>(E.marginal), ctx->envIntegral, pick(ctx, stream));
+	return rc == RB_OK ? RB_OK : fail(ctx, rc, "rb_rebuild_envmap_cdf");
 }
 
 int rb_clear_envmap(rb_ctx* ctx)
@@ -570,12 +610,15 @@ int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 	if (!ctx->haveLaunch || !ctx->haveGeometry || !ctx->scene.materials || !ctx->scene.spectra.sensor || !ctx->scene.luts.conductor)
 		return fail(ctx, RB_ERR_NO_SCENE, "rb_render: launch, geometry, materials, spectra and LUTs must be set first");
 	if (count == 0) return RB_OK;
+	const int rc0 = checkReferences(ctx);
+	if (rc0 != RB_OK) return rc0;
 	cudaSetDevice(ctx->device);
 	const cudaStream_t st = pick(ctx, stream);
 	const rb::DevScene& sc = ctx->scene;
 	const uint32_t pixels = sc.launch.width * sc.launch.height;
-	// Wave size: whole sample planes, up to the capacity (default 4M paths).
-	const uint64_t cap = ctx->requestedCapacity ? ctx->requestedCapacity : (4u << 20);
+	// Wave size: whole sample planes, up to the capacity (default 16M paths,
+	// about 3.2 GB of path state).
+	const uint64_t cap = ctx->requestedCapacity ? ctx->requestedCapacity : (16u << 20);
 	const uint32_t planesPerWave = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(count, cap / pixels)));
 	const uint32_t wavePaths = planesPerWave * pixels;
 	int rc = ensureWave(ctx, wavePaths);
@@ -790,6 +833,7 @@ int rb_k_oct_decode(uint32_t n, const uint32_t* code, float* out, void* stream)
 int rb_k_trace(rb_ctx* ctx, uint32_t n, const float* rays, uint32_t* payload, float* t, int32_t* tri, void* stream)
 {
 	RB_K_CHECK(ctx && ctx->haveGeometry);
+	if (checkReferences(ctx) != RB_OK) return RB_ERR_INVALID;
 	if (n == 0) return RB_OK;
 	RB_K_CHECK(rays && payload && t && tri);
 	rb::launchTrace(ctx->scene, n, rays, payload, t, tri, pick(ctx, stream));

@@ -117,7 +117,9 @@ RB_D Lobe product(f3 a1, float s1, f3 a2, float s2)
 {
 	const f3 axis = a1 * s1 + a2 * s2;
 	const float sharp = length(axis);
-	const float cosine = clampf(dot(a1, a2), -1.0f, 1.0f);
+	// (cosine - 1) below cancels for nearly aligned lobes: keep the dot
+	// product uncontracted so it rounds as the reference's does.
+	const float cosine = clampf(dotRn(a1, a2), -1.0f, 1.0f);
 	const float sMin = fminf(s1, s2);
 	const float ratio = sMin / fmaxf(fmaxf(s1, s2), FLT_MIN);
 	const float logAmp = 2.0f * sMin * (cosine - 1.0f) / (sqrtf(2.0f * ratio * cosine + ratio * ratio + 1.0f) + ratio + 1.0f);
@@ -200,8 +202,8 @@ RB_D TreeNode unpackNode(const PackedNode* nodes, uint32_t i)
 RB_D float nodeImportance(const TreeNode& n, f3 p, f3 nrm)
 {
 	f3 ld = n.mean - p;
-	const float d2 = dot(ld, ld);
-	ld *= rsqrtf(d2);
+	const float d2 = dotRn(ld, ld);
+	ld *= __frsqrt_rn(d2);
 	const float var = fmaxf(n.variance, 0x1.0p-31f * d2);
 	const float sharp = d2 / var;
 	const sg::Lobe lobe = sg::product(n.direction, n.sharpness, ld, sharp);
@@ -308,7 +310,7 @@ RB_D void envEmission(const DevScene& sc, f3 d, const S4& lambda, S4& Le, float&
 	const float theta = acosf(d.z);
 	const float4 c = envFetch(sc.env, 0.5f - phi / (2.0f * kPi), theta / kPi);
 	const float surfacePdf = 1.0f / (4.0f * kPi);
-	lightPdf = surfacePdf * ((c.x + c.y + c.z) / 3.0f) * sinf(theta) / sc.env.integral;
+	lightPdf = surfacePdf * ((c.x + c.y + c.z) / 3.0f) * sinf(theta) / __ldg(sc.env.integral);
 	Le = rgbToSpectrum(sc.spectra.basis, mk(c.x, c.y, c.z), lambda);
 }
 // Importance sample of the map from interpolated inverted-CDF indices (pathtrace.cu:1657-1689).
@@ -333,6 +335,6 @@ RB_D void envSample(const DevScene& sc, float rx, float ry, const S4& lambda, f3
 	const float4 c = envFetch(e, sx, sy);
 	spectrum = rgbToSpectrum(sc.spectra.basis, mk(c.x, c.y, c.z), lambda);
 	const float surfacePdf = 1.0f / (4.0f * kPi);
-	lightPdf = surfacePdf * ((c.x + c.y + c.z) / 3.0f) * sinf(theta) / e.integral;
+	lightPdf = surfacePdf * ((c.x + c.y + c.z) / 3.0f) * sinf(theta) / __ldg(e.integral);
 }
 } // namespace rb

@@ -32,6 +32,12 @@ RB_HD f3& operator+=(f3& a, f3 b) { a = a + b; return a; }
 RB_HD f3& operator-=(f3& a, f3 b) { a = a - b; return a; }
 RB_HD f3& operator*=(f3& a, float s) { a = a * s; return a; }
 RB_HD float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// Dot product with every operation rounded separately (no FMA contraction),
+// for the few places where cancellation makes the last bit matter.
+RB_D float dotRn(f3 a, f3 b)
+{
+	return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
 RB_HD f3 cross(f3 a, f3 b)
 {
 	return f3{ a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y };

@@ -129,7 +129,7 @@ struct DevEnvMap
 	uint32_t enabled;
 	uint32_t w, h;
 	float width, height;         // as floats, as LaunchParameters stores them
-	float integral;              // divided by w*h
+	const float* integral;       // device scalar: integral divided by w*h (rebuilt on the device)
 	const float4* texels;
 	const uint16_t* conditional;
 	const uint16_t* marginal;

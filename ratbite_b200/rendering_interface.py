@@ -21,11 +21,12 @@ def _ptr(a: np.ndarray):
 
 
 class RenderingInterface:
-    def __init__(self, device: int = 0, max_paths_in_flight: int = 0):
+    def __init__(self, device: int = 0, max_paths_in_flight: int = 0, envmap_cdf_mode: int = abi.RB_CDF_FP64):
         self.lib = load()
         cfg = abi.rb_config()
         cfg.device = device
         cfg.max_paths_in_flight = max_paths_in_flight
+        cfg.envmap_cdf_mode = envmap_cdf_mode
         h = C.c_void_p()
         check(self.lib.rb_create(C.byref(cfg), C.byref(h)), None, "rb_create")
         self.ctx = h
@@ -85,6 +86,10 @@ class RenderingInterface:
         h, w = img.shape[:2]
         check(self.lib.rb_set_envmap(self.ctx, _ptr(img), w, h), self.ctx, "rb_set_envmap")
 
+    def rebuild_environment_cdf(self, stream=None):
+        s = None if stream is None else C.c_void_p(stream)
+        check(self.lib.rb_rebuild_envmap_cdf(self.ctx, s), self.ctx, "rb_rebuild_envmap_cdf")
+
     def clear_environment_map(self):
         check(self.lib.rb_clear_envmap(self.ctx), self.ctx, "rb_clear_envmap")
 
@@ -106,6 +111,9 @@ class RenderingInterface:
         if light_tree is not None:
             self._keep.append(light_tree)
             self.load_lights(light_tree)
+        env = getattr(scene, "envmap", None)
+        if env is not None:
+            self.load_environment_map(env)
         launch = scene.launch_record(width, height, max_depth)
         self._keep.append(launch)
         self.prepare_data_for_rendering(launch)

@@ -275,6 +275,218 @@ class Scene:
 IDENTITY = np.array([[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 1, 0]], dtype=np.float32)
 
 
+# ------------------------------------------------------------ at-scale scene
+def _smooth_noise(p: np.ndarray, rng: np.random.Generator, octaves: int = 4) -> np.ndarray:
+    """Seeded smooth noise: a sum of random-direction sinusoids per octave."""
+    out = np.zeros(len(p))
+    amp, freq = 1.0, 2.0
+    for _ in range(octaves):
+        for _ in range(3):
+            k = rng.normal(size=3)
+            k /= np.linalg.norm(k)
+            out += amp * np.sin(freq * (p @ k) + rng.uniform(0, 2 * np.pi))
+        amp *= 0.5
+        freq *= 2.0
+    return out / 3.0
+
+
+def _torus(major: float, minor: float, nu: int, nv: int):
+    u = np.linspace(0, 2 * np.pi, nu, endpoint=False)
+    v = np.linspace(0, 2 * np.pi, nv, endpoint=False)
+    uu, vv = np.meshgrid(u, v, indexing="ij")
+    pos = np.stack([(major + minor * np.cos(vv)) * np.cos(uu), minor * np.sin(vv),
+                    (major + minor * np.cos(vv)) * np.sin(uu)], -1).reshape(-1, 3)
+    nrm = np.stack([np.cos(vv) * np.cos(uu), np.sin(vv), np.cos(vv) * np.sin(uu)], -1).reshape(-1, 3)
+    i, j = np.meshgrid(np.arange(nu), np.arange(nv), indexing="ij")
+    a = i * nv + j
+    b = ((i + 1) % nu) * nv + j
+    c = ((i + 1) % nu) * nv + (j + 1) % nv
+    d = i * nv + (j + 1) % nv
+    faces = np.concatenate([np.stack([a, b, c], -1).reshape(-1, 3), np.stack([a, c, d], -1).reshape(-1, 3)])
+    return pos, nrm, faces
+
+
+def _box(n: int):
+    """Unit box [-1,1]^3 with each face split into n x n quads."""
+    verts, faces, normals = [], [], []
+    t = np.linspace(-1, 1, n + 1)
+    for axis in range(3):
+        for sign in (-1.0, 1.0):
+            a, b = [k for k in range(3) if k != axis]
+            uu, vv = np.meshgrid(t, t, indexing="ij")
+            p = np.zeros((n + 1, n + 1, 3))
+            p[..., axis] = sign
+            p[..., a] = uu
+            p[..., b] = vv
+            base = sum(len(x) for x in verts)
+            verts.append(p.reshape(-1, 3))
+            nn = np.zeros(3)
+            nn[axis] = sign
+            normals.append(np.repeat(nn[None], (n + 1) ** 2, 0))
+            i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+            q0 = base + i * (n + 1) + j
+            q1 = q0 + (n + 1)
+            q2 = q1 + 1
+            q3 = q0 + 1
+            f = np.concatenate([np.stack([q0, q1, q2], -1).reshape(-1, 3), np.stack([q0, q2, q3], -1).reshape(-1, 3)])
+            if sign < 0:
+                f = f[:, ::-1]
+            faces.append(f)
+    return np.concatenate(verts), np.concatenate(normals), np.concatenate(faces)
+
+
+def _vertex_normals(pos, faces):
+    n = np.zeros_like(pos)
+    fn = np.cross(pos[faces[:, 1]] - pos[faces[:, 0]], pos[faces[:, 2]] - pos[faces[:, 0]])
+    for k in range(3):
+        np.add.at(n, faces[:, k], fn)
+    return n / np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-20)
+
+
+def sky_envmap(width: int = 1024, height: int = 512, seed: int = 7, sun_deg: float = 0.5,
+               dynamic_range: float = 1e4) -> np.ndarray:
+    """Lat-long RGBA float32 map (theta = pi * v, phi = 2 pi u): a vertical
+    sky gradient plus a Gaussian sun lobe of `sun_deg` angular size whose peak
+    is `dynamic_range` times the darkest sky texel."""
+    rng = np.random.default_rng(seed)
+    v = (np.arange(height) + 0.5) / height
+    u = (np.arange(width) + 0.5) / width
+    theta = np.pi * v[:, None]
+    phi = 2 * np.pi * u[None, :]
+    up = np.cos(theta)                                  # z-up lat-long
+    horizon = np.array([0.9, 0.85, 0.8])
+    zenith = np.array([0.25, 0.45, 0.9])
+    ground = np.array([0.12, 0.1, 0.08])
+    t = np.clip(up, 0, 1)[..., None]
+    sky = np.where(up[..., None] > 0, horizon * (1 - t) + zenith * t, ground * np.ones_like(t))
+    sky = sky * np.ones((height, width, 1))
+    sun_t, sun_p = np.deg2rad(rng.uniform(25, 60)), rng.uniform(0, 2 * np.pi)
+    d = np.stack([np.sin(theta) * np.cos(phi), np.sin(theta) * np.sin(phi), np.cos(theta) * np.ones_like(phi)], -1)
+    s = np.array([np.sin(sun_t) * np.cos(sun_p), np.sin(sun_t) * np.sin(sun_p), np.cos(sun_t)])
+    ang = np.arccos(np.clip(d @ s, -1, 1))
+    sigma = np.deg2rad(sun_deg) / 2.0
+    lo = sky.mean(-1).min()
+    sun = dynamic_range * lo * np.exp(-0.5 * (ang / sigma) ** 2)
+    img = np.zeros((height, width, 4), np.float32)
+    img[..., :3] = (sky + sun[..., None] * np.array([1.0, 0.95, 0.85])).astype(np.float32)
+    img[..., 3] = 1.0
+    return img
+
+
+def scale_scene(seed: int = 3, target_tris: int = 2_000_000, n_emitters: int = 4096, width: int = 1920,
+                height: int = 1080, spp: int = 256, max_depth: int = 12, envmap_size=(1024, 512)) -> Scene:
+    """The plain-method workload at scale: ~target_tris triangles from seeded
+    instanced procedural meshes (noise-displaced spheres, boxes, tori, 16
+    submeshes each), n_emitters emissive triangles with lognormal(0, 1.5)
+    grey radiance, 256 materials with OpenPBR-style parameters (base_weight
+    U[0.5,1] scaling the base colour, metalness Bernoulli(0.3), roughness
+    U[0.02,1], transmission Bernoulli(0.15), fuzz_weight U[0,0.5] as the sheen
+    colour scale; coat Bernoulli(0.2) is drawn but has no counterpart in the
+    reference BxDF), and a sky + sun environment map. Camera at the origin
+    looking down -z."""
+    rng = np.random.default_rng(seed)
+    n_sub = 16
+    materials: list[Material] = []
+
+    def surface_material():
+        base_weight = rng.uniform(0.5, 1.0)
+        color = tuple(float(np.float32(c * base_weight)) for c in rng.uniform(0.05, 0.95, 3))
+        metal = 1.0 if rng.random() < 0.3 else 0.0
+        trans = 1.0 if rng.random() < 0.15 else 0.0
+        fuzz = rng.uniform(0.0, 0.5)
+        _coat = rng.random() < 0.2
+        return Material(base_color=color, metalness=metal, roughness=float(np.float32(rng.uniform(0.02, 1.0))),
+                        transmission=trans, ior=1.5,
+                        sheen_color=tuple(float(np.float32(fuzz)) for _ in range(3)) if fuzz > 0.05 else None,
+                        sheen_roughness=float(np.float32(rng.uniform(0.2, 0.8))))
+
+    # Base meshes: 5 displaced spheres, 4 displaced tori, 3 boxes; 16
+    # submeshes each. A material record belongs to one submesh (it carries
+    # that submesh's index and attribute buffers), so 12 x 16 = 192 surface
+    # materials, + 1 ground + 63 emitter groups = 256.
+    bases = []
+    sv, sf = icosphere(5)                                # 20,480 triangles
+    for k in range(5):
+        disp = 1.0 + 0.12 * _smooth_noise(sv, rng)
+        pos = sv * disp[:, None]
+        bases.append((pos, _vertex_normals(pos, sf), sf))
+    for k in range(4):
+        tp, tn, tf = _torus(1.0, 0.35, 128, 64)           # 16,384 triangles
+        disp = 0.06 * _smooth_noise(tp, rng)
+        pos = tp + tn * disp[:, None]
+        bases.append((pos, _vertex_normals(pos, tf), tf))
+    for k in range(3):
+        bp, bn, bf = _box(24)                             # 6,912 triangles
+        disp = 0.03 * _smooth_noise(bp, rng)
+        pos = bp + bn * disp[:, None]
+        bases.append((pos, bn, bf))
+    meshes = []
+    for mi, (pos, nrm, faces) in enumerate(bases):
+        parts = np.array_split(np.arange(len(faces)), n_sub)
+        subs = []
+        for si, part in enumerate(parts):
+            used, inv = np.unique(faces[part].reshape(-1), return_inverse=True)
+            v4 = np.concatenate([pos[used], np.zeros((len(used), 1))], 1).astype(np.float32)
+            idx = inv.reshape(-1, 3).astype(np.uint32 if len(used) > 65535 else np.uint16)
+            materials.append(surface_material())
+            subs.append(Submesh(v4, idx, len(materials) - 1, normals=nrm[used].astype(np.float32)))
+        meshes.append(subs)
+    tri_per_mesh = [len(f) for _, _, f in bases]
+    instances = []
+    total = 0
+    k = 0
+    while total < target_tris:
+        m = k % len(bases)
+        k += 1
+        scale = rng.uniform(0.3, 1.2)
+        ang = rng.uniform(0, 2 * np.pi, 3)
+        cx, cy, cz = np.cos(ang)
+        sx, sy, sz = np.sin(ang)
+        rot = (np.array([[1, 0, 0], [0, cx, -sx], [0, sx, cx]]) @ np.array([[cy, 0, sy], [0, 1, 0], [-sy, 0, cy]])
+               @ np.array([[cz, -sz, 0], [sz, cz, 0], [0, 0, 1]]))
+        pos = np.array([rng.uniform(-14, 14), rng.uniform(-3, 5), rng.uniform(-40, -6)])
+        xf = np.concatenate([rot * scale, pos[:, None]], 1).astype(np.float32)
+        instances.append((m, xf))
+        total += tri_per_mesh[m]
+    # Ground: a large subdivided box slab.
+    gp, gn, gf = _box(32)
+    gpos = gp * np.array([40.0, 0.5, 40.0]) + np.array([0.0, -4.5, -25.0])
+    gmat = len(materials)
+    materials.append(Material(base_color=(0.35, 0.33, 0.3), metalness=0.0, roughness=0.8))
+    gv = np.concatenate([gpos, np.zeros((len(gpos), 1))], 1).astype(np.float32)
+    meshes.append([Submesh(gv, gf.astype(np.uint16), gmat)])
+    instances.append((len(meshes) - 1, IDENTITY))
+    # Emitters: 63 emissive submeshes sharing n_emitters small triangles,
+    # radiance ~ lognormal(0, 1.5) grey per submesh.
+    groups = np.array_split(np.arange(n_emitters), 63)
+    emissive = []
+    em_subs = []
+    for e, grp in enumerate(groups):
+        per = len(grp)
+        rad = float(np.exp(rng.normal(0.0, 1.5)))
+        materials.append(Material(base_color=(0.8, 0.8, 0.8), emissive=(rad, rad, rad)))
+        mat = len(materials) - 1
+        c = np.stack([rng.uniform(-16, 16, per), rng.uniform(5.0, 9.0, per), rng.uniform(-42, -4, per)], 1)
+        s = rng.uniform(0.1, 0.4, (per, 1))
+        a = c
+        b = c + s * np.array([1.0, 0.0, 0.0])
+        d = c + s * np.array([0.3, 0.0, 1.0])
+        tris = np.concatenate([a, d, b], 1).astype(np.float32)     # normal points down (-y)
+        v4 = np.concatenate([tris.reshape(-1, 3), np.zeros((3 * per, 1))], 1).astype(np.float32)
+        idx = np.arange(3 * per, dtype=np.uint16).reshape(per, 3)
+        em_subs.append(Submesh(v4, idx, mat, discarded=list(range(per))))
+        area = 0.5 * np.linalg.norm(np.cross(tris[:, 3:6] - tris[:, :3], tris[:, 6:9] - tris[:, :3]).astype(np.float32), axis=1)
+        flux = (np.float32(rad) * area.astype(np.float32) * np.float32(math.pi)).astype(np.float32)
+        emissive.append(dict(transform=IDENTITY, tris=tris, world=tris.copy(), prim=list(range(per)),
+                             flux=flux, material=mat, submesh=e))
+    meshes.append(em_subs)
+    instances.append((len(meshes) - 1, IDENTITY))
+    sc = Scene(name="scale_scene", seed=seed, meshes=meshes, instances=instances, materials=materials,
+               emissive=emissive, width=width, height=height, spp=spp, max_depth=max_depth)
+    sc.envmap = sky_envmap(*envmap_size, seed=seed)
+    return sc
+
+
 def _quad(p0, p1, p2, p3):
     """Two triangles (p0,p1,p2), (p0,p2,p3); normal = (p1-p0)x(p2-p0)."""
     v = np.array([p0, p1, p2, p3], dtype=np.float32)

