@@ -37,6 +37,7 @@ extern "C" {
 #define RB_ERR_NO_SCENE       -4  /* render called before geometry/launch set-up */
 #define RB_ERR_DEVICE         -5  /* a kernel set the device status word */
 #define RB_ERR_OOM            -6  /* device allocation failed */
+#define RB_ERR_TOO_LARGE      -7  /* input larger than a fixed-size entry point supports */
 
 /* Device status bits (rb_device_status.flags). */
 #define RB_DEV_STACK_OVERFLOW   (1u << 0)  /* BVH traversal stack exhausted */

@@ -117,6 +117,23 @@ int rb_envmap_cdf(uint32_t width, uint32_t height, const float* rgba, int mode,
                   void* scratch, uint16_t* conditional_idx, uint16_t* marginal_idx,
                   float* integral, void* stream);
 
+/* The same CDF build without any device allocation: it has no counterpart
+ * in the reference. It is for callers that must not allocate device memory
+ * once they are running, for example a host application or plugin host that
+ * owns a fixed device-memory budget, or a per-frame loop that cannot afford
+ * cudaMalloc / cudaFree (both may synchronise the whole device). The caller
+ * still passes the image and the output tables; the scratch is a fixed
+ * static device array inside this library, sized for images up to 8192
+ * rows (about 100 KB), held by every GPU that loads the library until the
+ * process exits. Taller images return RB_ERR_TOO_LARGE. The first call on a
+ * device looks the array's device address up (cudaGetSymbolAddress), so make
+ * that first call before any stream capture. All calls share the one array:
+ * calls that overlap on the GPU (on different streams, or from different
+ * threads) race, so serialise them. */
+int rb_envmap_cdf_noalloc(uint32_t width, uint32_t height, const float* rgba, int mode,
+                          uint16_t* conditional_idx, uint16_t* marginal_idx, float* integral,
+                          void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,6 +15,7 @@ RB_ERR_UNSUPPORTED = -3
 RB_ERR_NO_SCENE = -4
 RB_ERR_DEVICE = -5
 RB_ERR_OOM = -6
+RB_ERR_TOO_LARGE = -7
 
 RB_DEV_STACK_OVERFLOW = 1 << 0
 RB_DEV_QUEUE_OVERFLOW = 1 << 1

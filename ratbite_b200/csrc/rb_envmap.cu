@@ -20,6 +20,7 @@
 //      values rounded to float once, sin weights in double.
 
 #include <cstdint>
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include "ratbite_b200_kernels.h"
@@ -327,6 +328,54 @@ int envCdfLaunch(uint32_t w, uint32_t h, const float* rgba, int mode, void* scra
 extern "C" size_t rb_envmap_cdf_scratch_bytes(uint32_t width, uint32_t height)
 {
 	return rb::envCdfScratchBytes(width, height);
+}
+
+// ---- no-allocation variant ---------------------------------------------
+// The CDF build needs a small scratch area (completion ticket, per-row
+// totals, marginal). For callers that may not allocate device memory it
+// lives in a fixed file-scope device array sized for the largest supported
+// image height; every GPU that loads this library holds it until exit.
+namespace
+{
+constexpr uint32_t kNoAllocMaxHeight = 8192;
+constexpr size_t kNoAllocScratchBytes = 256 + ((sizeof(double) * kNoAllocMaxHeight + 255) / 256) * 256
+	+ ((sizeof(float) * kNoAllocMaxHeight + 255) / 256) * 256;
+__device__ __align__(256) unsigned char g_envCdfScratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratchMutex;
+void* g_scratchAddress[kMaxDevices] = {};
+
+// Device address of g_envCdfScratch on the current device, looked up once
+// per device. In host code the array's name is only a host-side handle, so
+// the address has to come from cudaGetSymbolAddress.
+int scratchAddress(void** out)
+{
+	int dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return RB_ERR_CUDA;
+	std::lock_guard<std::mutex> lock(g_scratchMutex);
+	if (!g_scratchAddress[dev])
+	{
+		void* p = nullptr;
+		if (cudaGetSymbolAddress(&p, g_envCdfScratch) != cudaSuccess || !p) return RB_ERR_CUDA;
+		g_scratchAddress[dev] = p;
+	}
+	*out = g_scratchAddress[dev];
+	return RB_OK;
+}
+} // namespace
+
+extern "C" int rb_envmap_cdf_noalloc(uint32_t width, uint32_t height, const float* rgba, int mode,
+	uint16_t* conditional_idx, uint16_t* marginal_idx, float* integral, void* stream)
+{
+	if (height > kNoAllocMaxHeight) return RB_ERR_TOO_LARGE;
+	void* scratch = nullptr;
+	const int rc = scratchAddress(&scratch);
+	if (rc != RB_OK) return rc;
+	const cudaStream_t st = static_cast<cudaStream_t>(stream);
+	// The ticket must start at zero; the rest of the scratch is written before it is read.
+	if (cudaMemsetAsync(scratch, 0, sizeof(uint32_t), st) != cudaSuccess) return RB_ERR_CUDA;
+	return rb::envCdfLaunch(width, height, rgba, mode, scratch, conditional_idx, marginal_idx, integral, st);
 }
 
 extern "C" int rb_envmap_cdf(uint32_t width, uint32_t height, const float* rgba, int mode, void* scratch,
