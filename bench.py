@@ -48,15 +48,31 @@ WORKLOADS = {
     "cornell": dict(name="cornell_box_256x256_64spp_depth8", width=256, height=256, spp=64, depth=8),
 }
 
-# Algorithmic bytes of one shading step (kShade) per path vertex: path state
-# read and written (ray o/d, wavelengths, pdfs, normal, L, T: 7 x 16 B,
-# twice), flags, the hit record, the hit triangle (3 x 16 B + 8 B), the
-# material record (128 B), the vertex indices and 3 attribute reads
-# (6 + 24 B), LUT taps (two 3D tables x 8 taps + one 2D x 4 taps, 4 B
-# each), spectral basis / sensor lookups (12 x 4 B), the emitter record
-# (68 B) and the shadow request written (48 B). Light-tree node reads grow
-# with tree depth and are not counted.
-SHADE_BYTES_PER_PATH = 2 * 7 * 16 + 2 * 8 + 16 + 56 + 128 + 30 + 20 * 4 + 12 * 4 + 68 + 48
+# Algorithmic HBM bytes per work unit of each wavefront kernel: the path
+# state it must stream in and out, plus the per-unit gathers from tables
+# larger than L2. Tables that stay cache-resident (materials, LUTs, spectra,
+# light-tree nodes, emitter records, the env-map CDF) are not counted.
+#   extend  per ray: queue slot 4, ray o/d 32, hit written 16; nodes (96 B)
+#           and triangles (48 B) per visit, counted from the traversal counters
+#   shadow  per ray: queue 4, shadow o/d 32, L read+write 32 when unoccluded
+#           (counted as always), pending contribution 16, plus visits as extend
+#   surface per path entering the bounce: queue 4, ray o/d 32, normal 16,
+#           flags 8, hit 16 read; the hit triangle 48 + 8; vertex indices 12
+#           and three 16-B attribute reads 48; surface record 80 + normal 16 +
+#           flags 8 + queue 4 written (for surface records)
+#   nee     per surface record: queue 4, record 48, normal 16, flags 8,
+#           wavelengths 16 read; record word 16 and the light sample 48 written
+#   bsdf    per surface record: queue 4, record 80, ray o/d 32, normal 16,
+#           flags 8, wavelengths + pdfs + throughput 48, light sample 32 read;
+#           throughput, flags, normal, pdfs, ray o/d 88, contribution 16 and
+#           two queue slots 8 written
+EXTEND_BYTES_PER_RAY = 4 + 32 + 16
+SHADOW_BYTES_PER_RAY = 4 + 32 + 32 + 16
+SURFACE_BYTES_PER_PATH = 4 + 32 + 16 + 8 + 16 + 56
+SURFACE_BYTES_PER_RECORD = 12 + 48 + 80 + 16 + 8 + 4
+NEE_BYTES_PER_RECORD = 4 + 48 + 16 + 8 + 16 + 16 + 48
+BSDF_BYTES_PER_RECORD = 4 + 80 + 32 + 16 + 8 + 48 + 32 + 88 + 16 + 8
+NODE_BYTES, TRI_BYTES = 96, 48
 
 
 def peaks():
@@ -295,28 +311,39 @@ def run_ours(args, rank: int, world: int, wl: dict):
 
     if rank == 0:
         hbm, peak_kind = peaks()
-        shares = {"extend": stages.ms_extend, "shade": stages.ms_shade, "shadow": stages.ms_shadow,
+        shares = {"extend": stages.ms_extend, "surface": stages.ms_surface, "nee": stages.ms_nee,
+                  "bsdf": stages.ms_bsdf, "shadow": stages.ms_shadow,
                   "generate": stages.ms_generate, "resolve": stages.ms_resolve}
         total_ms = sum(shares.values())
-        dom = max(("extend", "shade", "shadow"), key=lambda k: shares[k])
+        dom = max(("extend", "surface", "nee", "bsdf", "shadow"), key=lambda k: shares[k])
         # counts were gathered over one step
-        ext_rays, sh_rays = counts.extend_rays, counts.shadow_rays
-        if dom == "extend":
-            bytes_step = ext_rays * (32 + 16) + counts.extend_nodes * 96 + counts.extend_tris * 48
-            launches = stages.launches_extend
-        elif dom == "shadow":
-            bytes_step = sh_rays * (32 + 4) + counts.shadow_nodes * 96 + counts.shadow_tris * 48
-            launches = stages.launches_shadow
-        else:
-            bytes_step = ext_rays * SHADE_BYTES_PER_PATH
-            launches = stages.launches_shade
+        ext_rays, sh_rays, recs = counts.extend_rays, counts.shadow_rays, counts.surface_records
+        step_bytes = {
+            "extend": ext_rays * EXTEND_BYTES_PER_RAY + counts.extend_nodes * NODE_BYTES
+            + counts.extend_tris * TRI_BYTES,
+            "shadow": sh_rays * SHADOW_BYTES_PER_RAY + counts.shadow_nodes * NODE_BYTES
+            + counts.shadow_tris * TRI_BYTES,
+            "surface": ext_rays * SURFACE_BYTES_PER_PATH + recs * SURFACE_BYTES_PER_RECORD,
+            "nee": recs * NEE_BYTES_PER_RECORD,
+            "bsdf": recs * BSDF_BYTES_PER_RECORD,
+        }
+        kernel_launches = {"extend": stages.launches_extend, "shadow": stages.launches_shadow,
+                           "surface": stages.launches_shade, "nee": stages.launches_nee,
+                           "bsdf": stages.launches_bsdf}
+        kernel_names = {"extend": "kExtend", "shadow": "kShadow", "surface": "kSurface", "nee": "kNee",
+                        "bsdf": "kBsdf"}
+        bytes_step = step_bytes[dom]
+        launches = kernel_launches[dom]
         achieved = bytes_step * args.steps / (shares[dom] / 1e3) / 1e9
+        # every kernel of ours in the timed region: the wavefront kernels and
+        # one env-map CDF build per step
         launches_total = (stages.launches_generate + stages.launches_extend + stages.launches_shade
-                          + stages.launches_shadow + stages.launches_resolve)
+                          + stages.launches_nee + stages.launches_bsdf + stages.launches_shadow
+                          + stages.launches_resolve + (args.steps if has_env else 0))
         traffic = None
         tp = ROOT / "profiles" / "traffic.json"
         if tp.exists():
-            traffic = json.loads(tp.read_text()).get(wl["name"], {}).get(dom)
+            traffic = json.loads(tp.read_text()).get(wl["name"], {}).get(kernel_names[dom])
         if args.cpu_seconds > 0:
             cpu_v, cores, sample = cpu_baseline(scene, cie, basis, luts, wl, args.cpu_seconds)
         else:
@@ -334,12 +361,14 @@ def run_ours(args, rank: int, world: int, wl: dict):
             "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": C.sizeof(launch),
                     "d2h_bytes_per_step": W * H * 32, "steps": e2e_steps},
             "gpu_launches": int(launches_total),
-            "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm,
+            "roofline": {"kernel": kernel_names[dom], "bound": "hbm", "achieved": achieved, "peak": hbm,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "bytes_per_launch": bytes_step / max(1, launches / args.steps)},
             "stages_ms_per_step": {k: v / args.steps for k, v in shares.items()},
             "stage_share": {k: (v / total_ms if total_ms else None) for k, v in shares.items()},
-            "rays_per_step": {"extend": ext_rays, "shadow": sh_rays,
+            "kernel_gbs": {k: (step_bytes[k] * args.steps / (shares[k] / 1e3) / 1e9 if shares[k] else None)
+                           for k in step_bytes},
+            "rays_per_step": {"extend": ext_rays, "shadow": sh_rays, "surface_records": recs,
                               "nodes_per_extend_ray": counts.extend_nodes / max(1, ext_rays),
                               "tris_per_extend_ray": counts.extend_tris / max(1, ext_rays),
                               "nodes_per_shadow_ray": counts.shadow_nodes / max(1, sh_rays),

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define RB_ABI_VERSION 1
+#define RB_ABI_VERSION 2
 
 /* Status codes. */
 #define RB_OK                  0
@@ -276,6 +276,11 @@ typedef struct rb_render_stats {
     double ms_generate, ms_extend, ms_shade, ms_shadow, ms_resolve;
     uint32_t launches_generate, launches_extend, launches_shade, launches_shadow, launches_resolve;
     uint32_t reserved;
+    /* the shading stage per kernel: ms_shade = ms_surface + ms_nee + ms_bsdf
+     * (hit record, emission and frame; light sample; BxDF and next ray) */
+    double ms_surface, ms_nee, ms_bsdf;
+    uint32_t launches_nee, launches_bsdf;   /* launches_shade counts the surface kernel */
+    uint64_t surface_records;               /* path vertices shaded (RB_STATS_COUNT) */
 } rb_render_stats;
 int rb_set_stats(rb_ctx* ctx, uint32_t mode);
 /* Synchronizes, returns what was gathered since the last call, then resets. */

@@ -6,7 +6,7 @@ the sizes against the compiled library.
 """
 import ctypes as C
 
-RB_ABI_VERSION = 1
+RB_ABI_VERSION = 2
 
 RB_OK = 0
 RB_ERR_INVALID = -1
@@ -173,6 +173,9 @@ class rb_render_stats(C.Structure):
         ("ms_shadow", C.c_double), ("ms_resolve", C.c_double),
         ("launches_generate", C.c_uint32), ("launches_extend", C.c_uint32), ("launches_shade", C.c_uint32),
         ("launches_shadow", C.c_uint32), ("launches_resolve", C.c_uint32), ("reserved", C.c_uint32),
+        ("ms_surface", C.c_double), ("ms_nee", C.c_double), ("ms_bsdf", C.c_double),
+        ("launches_nee", C.c_uint32), ("launches_bsdf", C.c_uint32),
+        ("surface_records", C.c_uint64),
     ]
 
 

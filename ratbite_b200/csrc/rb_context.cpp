@@ -52,11 +52,11 @@ struct rb_ctx
 	uint32_t lightMaxMaterial = 0;              // 1 + largest material index of the light records
 	// instrumentation (rb_set_stats)
 	uint32_t statsMode = 0;
-	unsigned long long* counters = nullptr;     // 6 device counters
+	unsigned long long* counters = nullptr;     // 7 device counters
 	struct Timed { int stage; cudaEvent_t a, b; };
 	std::vector<Timed> timed;
 	std::vector<cudaEvent_t> eventPool;
-	uint32_t launches[5] = {};
+	uint32_t launches[7] = {};   // generate, extend, surface, shadow, resolve, nee, bsdf
 	uint64_t waves = 0;
 };
 
@@ -203,9 +203,12 @@ int ensureWave(rb_ctx* ctx, uint32_t paths)
 	alloc(s.lpdf, sizeof(float4)); alloc(s.nrm, sizeof(float4)); alloc(s.L, sizeof(float4));
 	alloc(s.T, sizeof(float4)); alloc(s.fd, sizeof(uint2)); alloc(s.hit, sizeof(float4));
 	alloc(s.shO, sizeof(float4)); alloc(s.shD, sizeof(float4)); alloc(s.shC, sizeof(float4));
+	alloc(s.sfP, sizeof(float4)); alloc(s.sfPi, sizeof(float4)); alloc(s.sfGn, sizeof(float4));
+	alloc(s.sfT, sizeof(float4)); alloc(s.sfB, sizeof(float4));
 	alloc(s.queue[0], sizeof(uint32_t)); alloc(s.queue[1], sizeof(uint32_t)); alloc(s.shadowQueue, sizeof(uint32_t));
+	alloc(s.surfQueue, sizeof(uint32_t));
 	if (rc == RB_OK)
-		rc = upload(ctx, ctx->soaBufs, nullptr, sizeof(uint32_t) * 2 * (rb::kMaxBounces + 1), s.counts);
+		rc = upload(ctx, ctx->soaBufs, nullptr, sizeof(uint32_t) * rb::kCountSlots, s.counts);
 	if (rc != RB_OK) { releaseWave(ctx); return rc; }
 	s.capacity = paths;
 	ctx->capacity = paths;
@@ -500,9 +503,18 @@ int rb_set_lights(rb_ctx* ctx, const rb_light_tree* t)
 	if (rc == RB_OK) rc = upload(ctx, ctx->lightBufs, t->bitmasks, sizeof(uint64_t) * t->triangle_count, L.bitmasks);
 	if (rc == RB_OK) rc = upload(ctx, ctx->lightBufs, t->pointers, sizeof(uint32_t) * t->pointer_count, L.pointers);
 	rb::PackedNode* dn = nullptr;
+	rb::TreeNodeU* du = nullptr;
 	if (rc == RB_OK && t->node_count) rc = upload(ctx, ctx->lightBufs, t->nodes, sizeof(rb::PackedNode) * t->node_count, dn);
+	if (rc == RB_OK && t->node_count) rc = upload(ctx, ctx->lightBufs, nullptr, sizeof(rb::TreeNodeU) * t->node_count, du);
 	if (rc != RB_OK) return rc;
+	if (t->node_count)
+	{
+		rb::launchUnpackLightTree(dn, du, t->node_count, ctx->stream);
+		const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_set_lights: unpack");
+	}
 	L.nodes = dn;
+	L.unpacked = du;
 	L.nodeCount = t->node_count;
 	L.triangleCount = t->triangle_count;
 	ctx->lightMaxMaterial = 0;
@@ -630,12 +642,14 @@ int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 		const uint32_t planes = std::min(planesPerWave, count - done);
 		rb::WaveParams w{ planes * pixels, pixels, offset + done, (offset == 0 && done == 0) ? 1u : 0u };
 		unsigned long long* cnt = (ctx->statsMode & RB_STATS_COUNT) ? ctx->counters : nullptr;
-		cudaMemsetAsync(ctx->soa.counts, 0, sizeof(uint32_t) * 2 * (rb::kMaxBounces + 1), st);
+		cudaMemsetAsync(ctx->soa.counts, 0, sizeof(uint32_t) * rb::kCountSlots, st);
 		timedStage(ctx, 0, st, [&] { rb::launchGenerate(sc, ctx->soa, w, ctx->shape, st); });
 		for (int b = 0; b < bounces; ++b)
 		{
 			timedStage(ctx, 1, st, [&] { rb::launchExtend(sc, ctx->soa, b, ctx->shape, st, cnt); });
-			timedStage(ctx, 2, st, [&] { rb::launchShade(sc, ctx->soa, w, b, ctx->shape, st); });
+			timedStage(ctx, 2, st, [&] { rb::launchSurface(sc, ctx->soa, w, b, ctx->shape, st, cnt); });
+			timedStage(ctx, 5, st, [&] { rb::launchNee(sc, ctx->soa, w, b, ctx->shape, st); });
+			timedStage(ctx, 6, st, [&] { rb::launchBsdf(sc, ctx->soa, w, b, ctx->shape, st); });
 			timedStage(ctx, 3, st, [&] { rb::launchShadow(sc, ctx->soa, b, ctx->shape, st, cnt); });
 		}
 		timedStage(ctx, 4, st, [&] { rb::launchResolve(sc, ctx->soa, w, ctx->accum, ctx->shape, st); });
@@ -713,9 +727,9 @@ int rb_set_stats(rb_ctx* ctx, uint32_t mode)
 	cudaSetDevice(ctx->device);
 	if ((mode & RB_STATS_COUNT) && !ctx->counters)
 	{
-		const cudaError_t e = cudaMalloc(&ctx->counters, 6 * sizeof(unsigned long long));
+		const cudaError_t e = cudaMalloc(&ctx->counters, 7 * sizeof(unsigned long long));
 		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_set_stats");
-		cudaMemset(ctx->counters, 0, 6 * sizeof(unsigned long long));
+		cudaMemset(ctx->counters, 0, 7 * sizeof(unsigned long long));
 	}
 	ctx->statsMode = mode;
 	return RB_OK;
@@ -731,13 +745,14 @@ int rb_get_stats(rb_ctx* ctx, rb_render_stats* out)
 	*out = rb_render_stats{};
 	if (ctx->counters)
 	{
-		unsigned long long c[6] = {};
+		unsigned long long c[7] = {};
 		cudaMemcpy(c, ctx->counters, sizeof(c), cudaMemcpyDeviceToHost);
 		cudaMemset(ctx->counters, 0, sizeof(c));
 		out->extend_rays = c[0]; out->extend_nodes = c[1]; out->extend_tris = c[2];
 		out->shadow_rays = c[3]; out->shadow_nodes = c[4]; out->shadow_tris = c[5];
+		out->surface_records = c[6];
 	}
-	double ms[5] = {};
+	double ms[7] = {};
 	for (const auto& t : ctx->timed)
 	{
 		float v = 0.0f;
@@ -746,9 +761,12 @@ int rb_get_stats(rb_ctx* ctx, rb_render_stats* out)
 		ctx->eventPool.push_back(t.b);
 	}
 	ctx->timed.clear();
-	out->ms_generate = ms[0]; out->ms_extend = ms[1]; out->ms_shade = ms[2]; out->ms_shadow = ms[3]; out->ms_resolve = ms[4];
+	out->ms_generate = ms[0]; out->ms_extend = ms[1]; out->ms_shade = ms[2] + ms[5] + ms[6];
+	out->ms_shadow = ms[3]; out->ms_resolve = ms[4];
+	out->ms_surface = ms[2]; out->ms_nee = ms[5]; out->ms_bsdf = ms[6];
 	out->launches_generate = ctx->launches[0]; out->launches_extend = ctx->launches[1];
 	out->launches_shade = ctx->launches[2]; out->launches_shadow = ctx->launches[3]; out->launches_resolve = ctx->launches[4];
+	out->launches_nee = ctx->launches[5]; out->launches_bsdf = ctx->launches[6];
 	out->waves = ctx->waves;
 	for (uint32_t& l : ctx->launches) l = 0;
 	ctx->waves = 0;

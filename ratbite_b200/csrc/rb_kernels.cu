@@ -22,6 +22,7 @@
 #include "rb_bvh.cuh"
 #include "rb_bxdf.cuh"
 #include "rb_light.cuh"
+#include "rb_launch.cuh"
 #include "rb_qrng.cuh"
 #include "rb_wavefront.h"
 #include "ratbite_b200_kernels.h"
@@ -30,23 +31,6 @@ namespace rb
 {
 namespace
 {
-constexpr int kThreads = 128;
-
-RB_D uint32_t gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
-RB_D uint32_t gstride() { return gridDim.x * blockDim.x; }
-
-// Warp-aggregated append: one atomic per warp for the lanes that push.
-RB_D uint32_t appendIndex(uint32_t* counter)
-{
-	const uint32_t active = __activemask();
-	const int leader = __ffs(active) - 1;
-	const uint32_t lane = threadIdx.x & 31u;
-	uint32_t base = 0;
-	if (lane == static_cast<uint32_t>(leader)) base = atomicAdd(counter, __popc(active));
-	base = __shfl_sync(active, base, leader);
-	return base + __popc(active & ((1u << lane) - 1u));
-}
-
 RB_D f3 mulMat(const float* m, f3 v)   // rows of 3
 {
 	return f3{ m[0] * v.x + m[1] * v.y + m[2] * v.z, m[3] * v.x + m[4] * v.y + m[5] * v.z,
@@ -134,11 +118,9 @@ RB_D uint32_t readIndex(const DevMaterial& m, uint32_t i)
 	                        : reinterpret_cast<const uint32_t*>(m.indices)[i];
 }
 
-// Shading frame, shadow-terminator offset and surface description
-// (pathtrace.cu:1279-1567). Returns false if the interaction is skipped by
-// alpha testing.
-RB_D bool shadingSetup(const DevScene& sc, const DevMaterial& mat, Interaction& it, f3 rayD, const Qrng& q,
-	Frame& frame, Surface& surf, f3& lastNormal)
+// Shading frame and shadow-terminator offset (pathtrace.cu:1279-1461).
+RB_D void shadingFrame(const DevScene& sc, const DevMaterial& mat, Interaction& it, f3 rayD, Frame& frame,
+	f3& lastNormal)
 {
 	const float w0 = 1.0f - it.b1 - it.b2, w1 = it.b1, w2 = it.b2;
 	const float* M = sc.geo.normalMatrix + 9u * it.instance;
@@ -225,24 +207,14 @@ RB_D bool shadingSetup(const DevScene& sc, const DevMaterial& mat, Interaction& 
 	sb *= flipTangent ? -1.0f : 1.0f;
 	frame = Frame{ stn, sb, n };
 	lastNormal = n;
+}
 
-	// Material factors (pathtrace.cu:1463-1560); textures are not supported.
-	surf = defaultSurface();
-	float alpha = 0.0f;
-	if (mat.factors & RB_FACTOR_BASE_COLOR)
-	{
-		surf.baseColor = mk(mat.baseColor[0], mat.baseColor[1], mat.baseColor[2]);
-		alpha = mat.baseColor[3];
-	}
-	bool skipped = false;
-	if (mat.factors & RB_FACTOR_CUTOFF)
-	{
-		if (alpha < mat.alphaCutoff) skipped = true;
-	}
-	else if (mat.factors & RB_FACTOR_BLEND)
-	{
-		if (sample1D(q, DIM_ALPHA_BLEND) > alpha) skipped = true;
-	}
+// Surface description from the material factors (pathtrace.cu:1463-1560);
+// textures are not supported.
+RB_D Surface surfaceOf(const DevMaterial& mat)
+{
+	Surface surf = defaultSurface();
+	if (mat.factors & RB_FACTOR_BASE_COLOR) surf.baseColor = mk(mat.baseColor[0], mat.baseColor[1], mat.baseColor[2]);
 	if (mat.factors & RB_FACTOR_METALNESS) surf.metalness = mat.metalness;
 	if (mat.factors & RB_FACTOR_ROUGHNESS) surf.roughness = mat.roughness;
 	if (mat.factors & RB_FACTOR_TRANSMISSION) surf.transmission = mat.transmission;
@@ -253,7 +225,17 @@ RB_D bool shadingSetup(const DevScene& sc, const DevMaterial& mat, Interaction& 
 		if (mat.factors & RB_FACTOR_SHEEN_COLOR) surf.sheenColor = mk(mat.sheenColor[0], mat.sheenColor[1], mat.sheenColor[2]);
 		if (mat.factors & RB_FACTOR_SHEEN_ROUGH) surf.sheenAlpha = mat.sheenRoughness;
 	}
-	return !skipped;
+	return surf;
+}
+
+// Alpha cutoff or stochastic alpha blending (pathtrace.cu:1485-1496): true
+// if the interaction is skipped and the path continues through the surface.
+RB_D bool alphaSkipped(const DevMaterial& mat, const Qrng& q)
+{
+	const float alpha = (mat.factors & RB_FACTOR_BASE_COLOR) ? mat.baseColor[3] : 0.0f;
+	if (mat.factors & RB_FACTOR_CUTOFF) return alpha < mat.alphaCutoff;
+	if (mat.factors & RB_FACTOR_BLEND) return sample1D(q, DIM_ALPHA_BLEND) > alpha;
+	return false;
 }
 
 // ------------------------------------------------------------- kernels
@@ -286,68 +268,49 @@ __global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, Wa
 	if (gtid() == 0) s.counts[0] = w.paths;
 }
 
-// Adds per-thread counts to a 64-bit counter with one atomic per warp.
-RB_D void warpAdd(unsigned long long* dst, uint32_t v)
+// Surface-record bits (PathSoA::sfPi.w).
+constexpr uint32_t kSfBackHit = 1u << 0;
+constexpr uint32_t kSfSkipped = 1u << 1;
+constexpr uint32_t kSfTriangle = 1u << 2;
+constexpr uint32_t kSfOccluded = 1u << 3;
+
+RB_D Qrng pathQrng(const DevScene& sc, const WaveParams& w, uint32_t p, uint32_t depth)
 {
-	unsigned long long s = v;
-#pragma unroll
-	for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
-	if ((threadIdx.x & 31u) == 0 && s) atomicAdd(dst, s);
+	const uint32_t pix = p % w.pixels;
+	return qrngAt(w.sampleBase + p / w.pixels, pixelHash(pix % sc.launch.width, pix / sc.launch.width), depth);
 }
 
-// counters (COUNT only): [0] rays, [1] nodes, [2] triangles.
-template<bool COUNT>
-__global__ void __launch_bounds__(kThreads) kExtend(DevScene sc, PathSoA s, int bounce, unsigned long long* counters)
-{
-	const uint32_t n = s.counts[bounce];
-	const uint32_t* q = s.queue[bounce & 1];
-	uint32_t rays = 0, nodes = 0, tris = 0;
-	for (uint32_t i = gtid(); i < n; i += gstride())
-	{
-		const uint32_t p = q[i];
-		const float4 o = s.rayO[p], d = s.rayD[p];
-		const Hit h = traceClosestT<COUNT>(sc.geo, f3_of(o), f3_of(d), 0.0f, FLT_MAX, sc.status, nodes, tris);
-		s.hit[p] = make_float4(__int_as_float(h.tri), h.t, h.b1, h.b2);
-		++rays;
-	}
-	if (COUNT)
-	{
-		warpAdd(counters + 0, rays);
-		warpAdd(counters + 1, nodes);
-		warpAdd(counters + 2, tris);
-	}
-}
-
-__global__ void __launch_bounds__(kThreads) kShade(DevScene sc, PathSoA s, WaveParams w, int bounce)
+// Stage 1 of shading: the hit record, hit emission with MIS
+// (pathtrace.cu:1185-1274), the shading frame and the alpha test. Paths that
+// continue get a surface record and join the surface queue, which the light
+// sampling and BxDF stages read.
+// counters (optional): [6] surface records.
+__global__ void __launch_bounds__(kThreads) kSurface(DevScene sc, PathSoA s, WaveParams w, int bounce,
+	unsigned long long* counters)
 {
 	const uint32_t n = s.counts[bounce];
 	const uint32_t* queue = s.queue[bounce & 1];
-	uint32_t* nextQueue = s.queue[(bounce + 1) & 1];
-	uint32_t* nextCount = s.counts + bounce + 1;
-	uint32_t* shadowCount = s.counts + (kMaxBounces + 1) + bounce;
-	const uint32_t W = sc.launch.width;
+	uint32_t* surfCount = s.counts + kSurfaceCounts + bounce;
+	uint32_t records = 0;
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
 		const uint32_t p = queue[i];
 		const float4 ro = s.rayO[p], rd = s.rayD[p];
-		f3 rayO = f3_of(ro), rayD = f3_of(rd);
-		float refrScale = ro.w, bxdfPdf = rd.w;
+		const f3 rayO = f3_of(ro), rayD = f3_of(rd);
+		const float bxdfPdf = rd.w;
 		const float4 nv = s.nrm[p];
 		f3 lastNormal = f3_of(nv);
-		Wavelengths wl{ s4(s.lambda[p]), s4(s.lpdf[p]), nv.w };
-		S4 L = s4(s.L[p]), T = s4(s.T[p]);
 		uint2 fd = s.fd[p];
-		uint32_t flags = fd.x, depth = fd.y;
-		const uint32_t pix = p % w.pixels;
-		const Qrng q = qrngAt(w.sampleBase + p / w.pixels, pixelHash(pix % W, pix / W), depth);
+		uint32_t flags = fd.x;
+		const uint32_t depth = fd.y;
 
 		Interaction it;
 		unpackHit(sc, s.hit[p], rayD, it);
 		if (it.lightType == kLightTypeTriangle || it.lightType == kLightTypeNone) flags |= PF_TRIANGULAR_GEOMETRY;
 
-		// Hit emission with MIS (pathtrace.cu:1185-1274).
 		if (it.lightType != kLightTypeNone)
 		{
+			const S4 lambda = s4(s.lambda[p]);
 			const bool prevNee = depth != 0 && !(flags & PF_PREVIOUS_HIT_SPECULAR);
 			const float treePdf = prevNee ? lightTreePdf(sc, it.lightType, it.lightIndex, rayO, lastNormal) : 1.0f;
 			float lightPdf = 0.0f;
@@ -367,12 +330,12 @@ __global__ void __launch_bounds__(kThreads) kShade(DevScene sc, PathSoA s, WaveP
 				noEmission = lCos <= 0.0f;
 				lightPdf = (1.0f / area) * d2 / lCos;
 				const DevMaterial& em = sc.materials[et.material];
-				Le = rgbToSpectrum(sc.spectra.basis, mk(em.emissive[0], em.emissive[1], em.emissive[2]), wl.lambda);
+				Le = rgbToSpectrum(sc.spectra.basis, mk(em.emissive[0], em.emissive[1], em.emissive[2]), lambda);
 			}
 			else
 			{
 				if (sc.env.enabled)
-					envEmission(sc, rayD, wl.lambda, Le, lightPdf);
+					envEmission(sc, rayD, lambda, Le, lightPdf);
 				else
 					noEmission = true;
 				flags |= PF_FINISHED;
@@ -381,183 +344,233 @@ __global__ void __launch_bounds__(kThreads) kShade(DevScene sc, PathSoA s, WaveP
 			{
 				lightPdf *= treePdf;
 				const float wgt = prevNee ? powerHeuristic(bxdfPdf, lightPdf) : 1.0f;
-				L += T * Le * wgt;
+				S4 L = s4(s.L[p]);
+				L += s4(s.T[p]) * Le * wgt;
+				s.L[p] = f4(L);
 			}
 		}
-		bool done = (flags & PF_FINISHED) != 0;
-		bool hasShadow = false;
-		if (!done)
+		if (!(flags & PF_FINISHED))
 		{
 			const DevMaterial& mat = sc.materials[it.material];
-			Frame frame;
-			Surface surf;
+			Frame frame{};
 			bool skipped = false;
 			if (flags & PF_TRIANGULAR_GEOMETRY)
-				skipped = !shadingSetup(sc, mat, it, rayD, q, frame, surf, lastNormal);
-			BxdfState st;
-			st.hasNee = false;
-			st.wl = wl; st.T = T; st.pdf = bxdfPdf; st.dir = rayD; st.flags = flags; st.refractionScale = refrScale;
-			if (!skipped)
 			{
-				// Light sample (pathtrace.cu:1572-1721).
-				LightSample dl;
-				dl.spectrum = s4(0.0f);
-				dl.dir = mk(0.0f);
-				dl.pdf = 0.0f;
-				dl.occluded = false;
-				f3 shadowO = mk(0.0f);
-				float dToL = 0.0f;
-				const bool envPresent = sc.env.enabled != 0;
-				const bool treePresent = sc.lights.nodes != nullptr;
-				if (!envPresent && !treePresent)
-				{
-					dl.occluded = true;
-				}
-				else
-				{
-					const f3 r = sample3D(q, DIM_LIGHT);
-					const bool tri = (flags & PF_TRIANGULAR_GEOMETRY) != 0;
-					const bool canTransmit = surf.transmission != 0.0f;
-					const f3 gn = it.gn, sn = lastNormal;
-					uint32_t type = 0, index = 0;
-					float treePdf = 0.0f, lightPdf = 0.0f;
-					lightTreeSample(sc, r.z, it.hitPos, sn, type, index, treePdf);
-					if (type == kLightTypeTriangle)
-					{
-						const EmissiveTri& et = sc.lights.triangles[index];
-						const f3 a = mk(et.v[0], et.v[1], et.v[2]), b = mk(et.v[3], et.v[4], et.v[5]), c = mk(et.v[6], et.v[7], et.v[8]);
-						f3 nn = cross(b - a, c - a);
-						const float nl = length(nn);
-						nn = nn / nl;
-						const float area = nl / 2.0f;
-						float u = r.x, v = r.y;
-						if (u + v > 1.0f) { u = 1.0f - u; v = 1.0f - v; }
-						const f3 lp = a + (b - a) * u + (c - a) * v;
-						const f3 sr = lp - it.hitPos;
-						const bool inSample = dot(sn, sr) < 0.0f;
-						if ((inSample && !canTransmit) || (inSample && dot(gn, sr) > 0.0f)) dl.occluded = true;
-						shadowO = offsetPoint(inSample || !tri ? it.hitPos : it.hitPosInterp, inSample ? -gn : gn);
-						const f3 rl = lp - shadowO;
-						const float d2 = rl.x * rl.x + rl.y * rl.y + rl.z * rl.z;
-						dToL = sqrtf(d2);
-						dl.dir = rl / dToL;
-						const float lCos = -dot(nn, dl.dir);
-						dl.occluded = lCos <= 0.0f;
-						lightPdf = (1.0f / area) * d2 / lCos;
-						const DevMaterial& em = sc.materials[et.material];
-						dl.spectrum = rgbToSpectrum(sc.spectra.basis, mk(em.emissive[0], em.emissive[1], em.emissive[2]), wl.lambda);
-					}
-					else if (type == kLightTypeSky)
-					{
-						envSample(sc, r.x, r.y, wl.lambda, dl.dir, dl.spectrum, lightPdf);
-						dToL = FLT_MAX;
-						shadowO = offsetPoint(!tri ? it.hitPos : it.hitPosInterp, it.backHit ? -it.gn : it.gn);
-					}
-					else
-					{
-						dl.occluded = true;
-					}
-					dl.pdf = lightPdf * treePdf;
-				}
-				evalBxdf(sc, mat, dl, q, frame, surf, st);
-				if (!dl.occluded && st.hasNee && !(st.flags & PF_PATH_TERMINATED))
-				{
-					hasShadow = true;
-					s.shO[p] = f4_of(shadowO, dToL - 0.1f);
-					s.shD[p] = f4_of(dl.dir, 0.0f);
-					s.shC[p] = f4(st.nee);
-				}
+				shadingFrame(sc, mat, it, rayD, frame, lastNormal);
+				skipped = alphaSkipped(mat, pathQrng(sc, w, p, depth));
 			}
-			flags = st.flags;
-			T = st.T;
-			bxdfPdf = st.pdf;
-			rayD = st.dir;
-			refrScale = st.refractionScale;
-			wl = st.wl;
-			if (flags & PF_PATH_TERMINATED)
+			const uint32_t bits = (it.backHit ? kSfBackHit : 0u) | (skipped ? kSfSkipped : 0u)
+				| ((flags & PF_TRIANGULAR_GEOMETRY) ? kSfTriangle : 0u);
+			s.sfP[p] = f4_of(it.hitPos, __uint_as_float(it.material));
+			s.sfPi[p] = f4_of(it.hitPosInterp, __uint_as_float(bits));
+			s.sfGn[p] = f4_of(it.gn, 0.0f);
+			s.sfT[p] = f4_of(frame.t, 0.0f);
+			s.sfB[p] = f4_of(frame.b, 0.0f);
+			s.nrm[p] = f4_of(lastNormal, nv.w);
+			s.surfQueue[appendIndex(surfCount)] = p;
+			++records;
+		}
+		s.fd[p] = make_uint2(flags, depth);
+	}
+	if (counters) warpAdd(counters + 6, records);
+}
+
+// Stage 2 of shading: the light sample (pathtrace.cu:1572-1721) for every
+// surface that is not skipped: pick a light from the light tree (held in the
+// read-only cache: it is read by every thread) or the environment, sample a
+// point on it and write the shadow ray and the light sample.
+__global__ void __launch_bounds__(kThreads) kNee(DevScene sc, PathSoA s, WaveParams w, int bounce)
+{
+	const uint32_t n = s.counts[kSurfaceCounts + bounce];
+	const TreeNodeU* nodes = sc.lights.unpacked;
+	const bool envPresent = sc.env.enabled != 0;
+	const bool treePresent = sc.lights.nodes != nullptr;
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const uint32_t p = s.surfQueue[i];
+		const float4 pi = s.sfPi[p];
+		uint32_t bits = __float_as_uint(pi.w);
+		if (bits & kSfSkipped) continue;
+		const float4 hp = s.sfP[p];
+		const f3 hitPos = f3_of(hp), hitPosInterp = f3_of(pi), gn = f3_of(s.sfGn[p]), sn = f3_of(s.nrm[p]);
+		f3 dir = mk(0.0f), shadowO = mk(0.0f);
+		S4 spectrum = s4(0.0f);
+		float pdf = 0.0f, dToL = 0.0f;
+		bool occluded = false;
+		if (!envPresent && !treePresent)
+		{
+			occluded = true;
+		}
+		else
+		{
+			const DevMaterial& mat = sc.materials[__float_as_uint(hp.w)];
+			const bool canTransmit = surfaceOf(mat).transmission != 0.0f;
+			const Qrng q = pathQrng(sc, w, p, s.fd[p].y);
+			const f3 r = sample3D(q, DIM_LIGHT);
+			const bool tri = (bits & kSfTriangle) != 0;
+			const S4 lambda = s4(s.lambda[p]);
+			uint32_t type = 0, index = 0;
+			float treePdf = 0.0f, lightPdf = 0.0f;
+			lightTreeSample(sc, nodes, r.z, hitPos, sn, type, index, treePdf);
+			if (type == kLightTypeTriangle)
 			{
-				done = true;
-				hasShadow = false;
+				const EmissiveTri& et = sc.lights.triangles[index];
+				const f3 a = mk(et.v[0], et.v[1], et.v[2]), b = mk(et.v[3], et.v[4], et.v[5]), c = mk(et.v[6], et.v[7], et.v[8]);
+				f3 nn = cross(b - a, c - a);
+				const float nl = length(nn);
+				nn = nn / nl;
+				const float area = nl / 2.0f;
+				float u = r.x, v = r.y;
+				if (u + v > 1.0f) { u = 1.0f - u; v = 1.0f - v; }
+				const f3 lp = a + (b - a) * u + (c - a) * v;
+				const f3 sr = lp - hitPos;
+				const bool inSample = dot(sn, sr) < 0.0f;
+				if ((inSample && !canTransmit) || (inSample && dot(gn, sr) > 0.0f)) occluded = true;
+				shadowO = offsetPoint(inSample || !tri ? hitPos : hitPosInterp, inSample ? -gn : gn);
+				const f3 rl = lp - shadowO;
+				const float d2 = rl.x * rl.x + rl.y * rl.y + rl.z * rl.z;
+				dToL = sqrtf(d2);
+				dir = rl / dToL;
+				const float lCos = -dot(nn, dir);
+				// the reference overwrites the flag set above here (pathtrace.cu:1633)
+				occluded = lCos <= 0.0f;
+				lightPdf = (1.0f / area) * d2 / lCos;
+				const DevMaterial& em = sc.materials[et.material];
+				spectrum = rgbToSpectrum(sc.spectra.basis, mk(em.emissive[0], em.emissive[1], em.emissive[2]), lambda);
+			}
+			else if (type == kLightTypeSky)
+			{
+				envSample(sc, r.x, r.y, lambda, dir, spectrum, lightPdf);
+				dToL = FLT_MAX;
+				shadowO = offsetPoint(!tri ? hitPos : hitPosInterp, (bits & kSfBackHit) ? -gn : gn);
 			}
 			else
 			{
-				// Russian roulette (pathtrace.cu:1736-1744).
-				const float tMax = s4max(T) * refrScale;
-				bool killed = false;
-				if (tMax < 1.0f && depth > 0)
-				{
-					float qq = fmaxf(0.0f, 1.0f - tMax);
-					qq = qq * qq;
-					if (sample1D(q, DIM_ROULETTE) < qq) killed = true;
-					else T /= (1.0f - qq);
-				}
-				if (killed)
-				{
-					done = true;
-				}
-				else
-				{
-					// Next origin and direction fix-up (:1747-1766).
-					const bool refracted = (flags & PF_RAY_REFRACTED) != 0;
-					const bool triGeo = (flags & PF_TRIANGULAR_GEOMETRY) != 0;
-					const bool in = refracted || skipped;
-					const f3 origin = (in == it.backHit) && triGeo ? it.hitPosInterp : it.hitPos;
-					const f3 offset = in == it.backHit ? it.gn : -it.gn;
-					rayO = offsetPoint(origin, offset);
-					const float dNg = dot(it.gn, rayD);
-					if (dNg > 0.0f && (it.backHit != refracted) && !skipped)
-						rayD = normalize(rayD - (it.gn * (dNg + 0.001f)));
-					// Depth limits (:1769-1779).
-					++depth;
-					bool cont = depth < sc.launch.maxDepth;
-					if (!(flags & PF_CURRENT_HIT_SPECULAR) && !skipped)
-						cont = (flags & PF_REFRACTION_HAPPENED) ? depth < sc.launch.maxTransmitted : depth < sc.launch.maxReflected;
-					if (!cont) flags |= PF_FINISHED;
-					// updateStateFlags (:954-972).
-					uint32_t inc = 0;
-					if (flags & PF_CURRENT_HIT_SPECULAR) inc |= PF_PREVIOUS_HIT_SPECULAR; else inc |= PF_REGULARIZED;
-					if (flags & PF_RAY_REFRACTED) inc |= PF_REFRACTION_HAPPENED;
-					flags = (flags & ~(PF_CURRENT_HIT_SPECULAR | PF_PREVIOUS_HIT_SPECULAR | PF_TRIANGULAR_GEOMETRY
-						| PF_RIGHT_HANDED_FRAME | PF_RAY_REFRACTED)) | inc;
-					done = (flags & PF_FINISHED) != 0;
-				}
+				occluded = true;
+			}
+			pdf = lightPdf * treePdf;
+		}
+		if (occluded) bits |= kSfOccluded;
+		s.sfPi[p] = f4_of(hitPosInterp, __uint_as_float(bits));
+		s.shO[p] = f4_of(shadowO, dToL - 0.1f);
+		s.shD[p] = f4_of(dir, pdf);
+		s.shC[p] = f4(spectrum);
+	}
+}
+
+// Stage 3 of shading: the BxDF call with the light sample
+// (pathtrace.cu:1724-1733), Russian roulette, the next ray and the depth
+// limits (:1736-1785). Continuing paths go to the next extend queue, light
+// samples that passed to the shadow queue.
+__global__ void __launch_bounds__(kThreads) kBsdf(DevScene sc, PathSoA s, WaveParams w, int bounce)
+{
+	const uint32_t n = s.counts[kSurfaceCounts + bounce];
+	uint32_t* nextQueue = s.queue[(bounce + 1) & 1];
+	uint32_t* nextCount = s.counts + bounce + 1;
+	uint32_t* shadowCount = s.counts + kShadowCounts + bounce;
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const uint32_t p = s.surfQueue[i];
+		const float4 hp = s.sfP[p], pi = s.sfPi[p], gv = s.sfGn[p];
+		const uint32_t bits = __float_as_uint(pi.w);
+		const bool skipped = (bits & kSfSkipped) != 0, backHit = (bits & kSfBackHit) != 0;
+		const f3 hitPos = f3_of(hp), hitPosInterp = f3_of(pi), gn = f3_of(gv);
+		const float4 ro = s.rayO[p], rd = s.rayD[p], nv = s.nrm[p];
+		const uint2 fd = s.fd[p];
+		uint32_t flags = fd.x, depth = fd.y;
+		const Qrng q = pathQrng(sc, w, p, depth);
+		const DevMaterial& mat = sc.materials[__float_as_uint(hp.w)];
+
+		BxdfState st;
+		st.hasNee = false;
+		st.wl = Wavelengths{ s4(s.lambda[p]), s4(s.lpdf[p]), nv.w };
+		st.T = s4(s.T[p]);
+		st.pdf = rd.w;
+		st.dir = f3_of(rd);
+		st.flags = flags;
+		st.refractionScale = ro.w;
+		bool hasShadow = false;
+		if (!skipped)
+		{
+			const float4 dd = s.shD[p];
+			LightSample dl;
+			dl.spectrum = s4(s.shC[p]);
+			dl.dir = f3_of(dd);
+			dl.pdf = dd.w;
+			dl.occluded = (bits & kSfOccluded) != 0;
+			const Frame frame{ f3_of(s.sfT[p]), f3_of(s.sfB[p]), f3_of(nv) };
+			evalBxdf(sc, mat, dl, q, frame, surfaceOf(mat), st);
+			hasShadow = !dl.occluded && st.hasNee && !(st.flags & PF_PATH_TERMINATED);
+		}
+		flags = st.flags;
+		S4 T = st.T;
+		f3 rayO = f3_of(ro), rayD = st.dir;
+		const float refrScale = st.refractionScale;
+		bool done = false;
+		if (flags & PF_PATH_TERMINATED)
+		{
+			done = true;
+			hasShadow = false;
+		}
+		else
+		{
+			// Russian roulette (pathtrace.cu:1736-1744).
+			const float tMax = s4max(T) * refrScale;
+			bool killed = false;
+			if (tMax < 1.0f && depth > 0)
+			{
+				float qq = fmaxf(0.0f, 1.0f - tMax);
+				qq = qq * qq;
+				if (sample1D(q, DIM_ROULETTE) < qq) killed = true;
+				else T /= (1.0f - qq);
+			}
+			if (killed)
+			{
+				done = true;
+			}
+			else
+			{
+				// Next origin and direction fix-up (:1747-1766).
+				const bool refracted = (flags & PF_RAY_REFRACTED) != 0;
+				const bool triGeo = (flags & PF_TRIANGULAR_GEOMETRY) != 0;
+				const bool in = refracted || skipped;
+				const f3 origin = (in == backHit) && triGeo ? hitPosInterp : hitPos;
+				const f3 offset = in == backHit ? gn : -gn;
+				rayO = offsetPoint(origin, offset);
+				const float dNg = dot(gn, rayD);
+				if (dNg > 0.0f && (backHit != refracted) && !skipped)
+					rayD = normalize(rayD - (gn * (dNg + 0.001f)));
+				// Depth limits (:1769-1779).
+				++depth;
+				bool cont = depth < sc.launch.maxDepth;
+				if (!(flags & PF_CURRENT_HIT_SPECULAR) && !skipped)
+					cont = (flags & PF_REFRACTION_HAPPENED) ? depth < sc.launch.maxTransmitted : depth < sc.launch.maxReflected;
+				if (!cont) flags |= PF_FINISHED;
+				// updateStateFlags (:954-972).
+				uint32_t inc = 0;
+				if (flags & PF_CURRENT_HIT_SPECULAR) inc |= PF_PREVIOUS_HIT_SPECULAR; else inc |= PF_REGULARIZED;
+				if (flags & PF_RAY_REFRACTED) inc |= PF_REFRACTION_HAPPENED;
+				flags = (flags & ~(PF_CURRENT_HIT_SPECULAR | PF_PREVIOUS_HIT_SPECULAR | PF_TRIANGULAR_GEOMETRY
+					| PF_RIGHT_HANDED_FRAME | PF_RAY_REFRACTED)) | inc;
+				done = (flags & PF_FINISHED) != 0;
 			}
 		}
-		s.L[p] = f4(L);
+		if (hasShadow) s.shC[p] = f4(st.nee);
 		s.T[p] = f4(T);
 		s.fd[p] = make_uint2(flags, depth);
-		s.nrm[p] = f4_of(lastNormal, wl.active);
-		s.lpdf[p] = f4(wl.pdf);
+		s.nrm[p] = make_float4(nv.x, nv.y, nv.z, st.wl.active);
+		s.lpdf[p] = f4(st.wl.pdf);
 		s.rayO[p] = f4_of(rayO, refrScale);
-		s.rayD[p] = f4_of(rayD, bxdfPdf);
+		s.rayD[p] = f4_of(rayD, st.pdf);
 		if (hasShadow) s.shadowQueue[appendIndex(shadowCount)] = p;
 		if (!done) nextQueue[appendIndex(nextCount)] = p;
 	}
 }
 
-template<bool COUNT>
-__global__ void __launch_bounds__(kThreads) kShadow(DevScene sc, PathSoA s, int bounce, unsigned long long* counters)
+// Unpacks the light tree once per upload (TreeNodeU).
+__global__ void kUnpackLightTree(const PackedNode* in, TreeNodeU* out, uint32_t n)
 {
-	const uint32_t n = s.counts[(kMaxBounces + 1) + bounce];
-	uint32_t rays = 0, nodes = 0, tris = 0;
-	for (uint32_t i = gtid(); i < n; i += gstride())
-	{
-		const uint32_t p = s.shadowQueue[i];
-		const float4 o = s.shO[p], d = s.shD[p];
-		if (!traceAnyT<COUNT>(sc.geo, f3_of(o), f3_of(d), 0.0f, o.w, sc.status, nodes, tris))
-		{
-			S4 L = s4(s.L[p]);
-			L += s4(s.shC[p]);
-			s.L[p] = f4(L);
-		}
-		++rays;
-	}
-	if (COUNT)
-	{
-		warpAdd(counters + 3, rays);
-		warpAdd(counters + 4, nodes);
-		warpAdd(counters + 5, tris);
-	}
+	for (uint32_t i = gtid(); i < n; i += gstride()) out[i] = makeNodeU(in, i);
 }
 
 // Sample resolve and FP64 accumulation (pathtrace.cu:1789-1812, color::toRGB).
@@ -702,7 +715,7 @@ __global__ void kLightCases(DevScene sc, uint32_t n, rb_light_case* cases)
 		rb_light_case c = cases[i];
 		const f3 p = mk(c.position[0], c.position[1], c.position[2]);
 		const f3 nn = mk(c.normal[0], c.normal[1], c.normal[2]);
-		lightTreeSample(sc, c.rand, p, nn, c.type, c.index, c.pdf);
+		lightTreeSample(sc, sc.lights.unpacked, c.rand, p, nn, c.type, c.index, c.pdf);
 		c.q_pdf = lightTreePdf(sc, c.q_type, c.q_index, p, nn);
 		cases[i] = c;
 	}
@@ -727,59 +740,6 @@ __global__ void kOctDecode(uint32_t n, const uint32_t* code, float* out)
 		out[3 * i] = r.x; out[3 * i + 1] = r.y; out[3 * i + 2] = r.z;
 	}
 }
-// Closest hit returned in the reference's 24-word payload layout.
-__global__ void kTrace(DevScene sc, uint32_t n, const float* rays, uint32_t* payload, float* tOut, int32_t* triOut)
-{
-	for (uint32_t i = gtid(); i < n; i += gstride())
-	{
-		const f3 o = mk(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
-		const f3 d = mk(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
-		const Hit h = traceClosest(sc.geo, o, d, 0.0f, FLT_MAX, sc.status);
-		uint32_t* pl = payload + 24 * static_cast<size_t>(i);
-		for (int k = 0; k < 24; ++k) pl[k] = 0u;
-		if (h.tri < 0)
-		{
-			pl[8] = kLightTypeSky << 30;
-			tOut[i] = INFINITY;
-			triOut[i] = -1;
-			continue;
-		}
-		const float4 a = sc.geo.triVerts[3 * h.tri], b = sc.geo.triVerts[3 * h.tri + 1], c = sc.geo.triVerts[3 * h.tri + 2];
-		const uint2 aux = sc.geo.triAux[h.tri];
-		const uint32_t sbt = __float_as_uint(c.w);
-		uint32_t prim = aux.y, mat = sbt, lptr = kLightTypeNone << 30;
-		if (sbt == 0xFFFFFFFFu)
-		{
-			lptr = (kLightTypeTriangle << 30) | (aux.y & ((1u << 30) - 1u));
-			prim = sc.lights.triangles[aux.y].prim;
-			mat = sc.lights.triangles[aux.y].material;
-		}
-		pl[0] = __float_as_uint(a.x); pl[1] = __float_as_uint(a.y); pl[2] = __float_as_uint(a.z);
-		pl[3] = aux.x; pl[4] = prim; pl[5] = __float_as_uint(h.b1); pl[6] = __float_as_uint(h.b2);
-		pl[7] = mat; pl[8] = lptr;
-		const float* M = sc.geo.normalMatrix + 9u * __float_as_uint(b.w);
-		for (int k = 0; k < 9; ++k) pl[9 + k] = __float_as_uint(M[k]);
-		pl[18] = __float_as_uint(b.x); pl[19] = __float_as_uint(b.y); pl[20] = __float_as_uint(b.z);
-		pl[21] = __float_as_uint(c.x); pl[22] = __float_as_uint(c.y); pl[23] = __float_as_uint(c.z);
-		tOut[i] = h.t;
-		triOut[i] = static_cast<int32_t>(__float_as_uint(a.w));
-	}
-}
-__global__ void kOccluded(DevScene sc, uint32_t n, const float* rays, const float* tmax, uint32_t* out)
-{
-	for (uint32_t i = gtid(); i < n; i += gstride())
-	{
-		const f3 o = mk(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
-		const f3 d = mk(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
-		out[i] = traceAny(sc.geo, o, d, 0.0f, tmax[i], sc.status) ? 1u : 0u;
-	}
-}
-
-int gridFor(uint32_t n)
-{
-	const uint32_t b = (n + kThreads - 1) / kThreads;
-	return static_cast<int>(b < 1 ? 1 : (b > 65535u * 4 ? 65535u * 4 : b));
-}
 } // namespace
 
 LaunchShape queryLaunchShape()
@@ -795,10 +755,11 @@ LaunchShape queryLaunchShape()
 	};
 	ls.threads = kThreads;
 	ls.blocksGenerate = occ(reinterpret_cast<const void*>(kGenerate));
-	ls.blocksExtend = occ(reinterpret_cast<const void*>(kExtend<false>));
-	ls.blocksShade = occ(reinterpret_cast<const void*>(kShade));
-	ls.blocksShadow = occ(reinterpret_cast<const void*>(kShadow<false>));
+	ls.blocksSurface = occ(reinterpret_cast<const void*>(kSurface));
+	ls.blocksNee = occ(reinterpret_cast<const void*>(kNee));
+	ls.blocksBsdf = occ(reinterpret_cast<const void*>(kBsdf));
 	ls.blocksResolve = occ(reinterpret_cast<const void*>(kResolve));
+	queryTraceShape(ls);
 	return ls;
 }
 
@@ -806,21 +767,22 @@ void launchGenerate(const DevScene& sc, const PathSoA& s, const WaveParams& w, c
 {
 	kGenerate<<<ls.blocksGenerate, kThreads, 0, st>>>(sc, s, w);
 }
-void launchExtend(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
+void launchSurface(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st,
 	unsigned long long* counters)
 {
-	if (counters) kExtend<true><<<ls.blocksExtend, kThreads, 0, st>>>(sc, s, bounce, counters);
-	else kExtend<false><<<ls.blocksExtend, kThreads, 0, st>>>(sc, s, bounce, nullptr);
+	kSurface<<<ls.blocksSurface, kThreads, 0, st>>>(sc, s, w, bounce, counters);
 }
-void launchShade(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
+void launchNee(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
 {
-	kShade<<<ls.blocksShade, kThreads, 0, st>>>(sc, s, w, bounce);
+	kNee<<<ls.blocksNee, kThreads, 0, st>>>(sc, s, w, bounce);
 }
-void launchShadow(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
-	unsigned long long* counters)
+void launchBsdf(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
 {
-	if (counters) kShadow<true><<<ls.blocksShadow, kThreads, 0, st>>>(sc, s, bounce, counters);
-	else kShadow<false><<<ls.blocksShadow, kThreads, 0, st>>>(sc, s, bounce, nullptr);
+	kBsdf<<<ls.blocksBsdf, kThreads, 0, st>>>(sc, s, w, bounce);
+}
+void launchUnpackLightTree(const PackedNode* in, TreeNodeU* out, uint32_t n, cudaStream_t st)
+{
+	kUnpackLightTree<<<gridFor(n), kThreads, 0, st>>>(in, out, n);
 }
 void launchResolve(const DevScene& sc, const PathSoA& s, const WaveParams& w, double4* accum, const LaunchShape& ls, cudaStream_t st)
 {
@@ -863,13 +825,5 @@ void launchOctEncode(uint32_t n, const float* v, uint32_t* out, cudaStream_t st)
 void launchOctDecode(uint32_t n, const uint32_t* code, float* out, cudaStream_t st)
 {
 	kOctDecode<<<gridFor(n), kThreads, 0, st>>>(n, code, out);
-}
-void launchTrace(const DevScene& sc, uint32_t n, const float* rays, uint32_t* payload, float* t, int32_t* tri, cudaStream_t st)
-{
-	kTrace<<<gridFor(n), kThreads, 0, st>>>(sc, n, rays, payload, t, tri);
-}
-void launchOccluded(const DevScene& sc, uint32_t n, const float* rays, const float* tmax, uint32_t* out, cudaStream_t st)
-{
-	kOccluded<<<gridFor(n), kThreads, 0, st>>>(sc, n, rays, tmax, out);
 }
 } // namespace rb

@@ -1,0 +1,42 @@
+// Grid helpers shared by the kernel translation units.
+#pragma once
+
+#include <cstdint>
+
+#include "rb_math.cuh"
+
+namespace rb
+{
+constexpr int kThreads = 128;
+
+RB_D uint32_t gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+RB_D uint32_t gstride() { return gridDim.x * blockDim.x; }
+
+// Warp-aggregated append: one atomic per warp for the lanes that push.
+RB_D uint32_t appendIndex(uint32_t* counter)
+{
+	const uint32_t active = __activemask();
+	const int leader = __ffs(active) - 1;
+	const uint32_t lane = threadIdx.x & 31u;
+	uint32_t base = 0;
+	if (lane == static_cast<uint32_t>(leader)) base = atomicAdd(counter, __popc(active));
+	base = __shfl_sync(active, base, leader);
+	return base + __popc(active & ((1u << lane) - 1u));
+}
+
+// Adds per-thread counts to a 64-bit counter with one atomic per warp.
+RB_D void warpAdd(unsigned long long* dst, uint32_t v)
+{
+	unsigned long long s = v;
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
+	if ((threadIdx.x & 31u) == 0 && s) atomicAdd(dst, s);
+}
+
+// Grid for a one-thread-per-item batch kernel (grid-stride loops cover the rest).
+inline int gridFor(uint32_t n)
+{
+	const uint32_t b = (n + kThreads - 1) / kThreads;
+	return static_cast<int>(b < 1 ? 1 : (b > 65535u * 4 ? 65535u * 4 : b));
+}
+} // namespace rb

@@ -212,6 +212,45 @@ RB_D float nodeImportance(const TreeNode& n, f3 p, f3 nrm)
 	return (n.flux / (var * sg::integral(n.sharpness))) * amp * sg::clampedCosineProductOverPi2024(cosine, lobe.sharpness);
 }
 
+// Light-tree node unpacked once per tree on the device (kUnpackLightTree,
+// TreeNodeU in rb_scene.h): the decoded average direction and the SG integral
+// of the node's sharpness are stored, so the per-sample descent does only the
+// point-dependent part, with three 16-B loads per node.
+RB_D TreeNodeU makeNodeU(const PackedNode* nodes, uint32_t i)
+{
+	const TreeNode n = unpackNode(nodes, i);
+	TreeNodeU u;
+	u.meanVar = make_float4(n.mean.x, n.mean.y, n.mean.z, n.variance);
+	u.dirSharp = make_float4(n.direction.x, n.direction.y, n.direction.z, n.sharpness);
+	u.fluxInt = make_float4(n.flux, sg::integral(n.sharpness), __uint_as_float(n.a),
+		__uint_as_float(n.b | (n.leaf ? 0x80000000u : 0u)));
+	return u;
+}
+RB_D bool nodeLeaf(const TreeNodeU& u) { return (__float_as_uint(u.fluxInt.w) >> 31) != 0u; }
+RB_D uint32_t nodeA(const TreeNodeU& u) { return __float_as_uint(u.fluxInt.z); }
+RB_D uint32_t nodeB(const TreeNodeU& u) { return __float_as_uint(u.fluxInt.w) & 0x7FFFFFFFu; }
+RB_D TreeNodeU loadNodeU(const TreeNodeU* nodes, uint32_t i)
+{
+	TreeNodeU u;
+	u.meanVar = __ldg(&nodes[i].meanVar);
+	u.dirSharp = __ldg(&nodes[i].dirSharp);
+	u.fluxInt = __ldg(&nodes[i].fluxInt);
+	return u;
+}
+// nodeImportance on an unpacked node: the same float operations in the same order.
+RB_D float nodeImportanceU(const TreeNodeU& n, f3 p, f3 nrm)
+{
+	f3 ld = f3_of(n.meanVar) - p;
+	const float d2 = dotRn(ld, ld);
+	ld *= __frsqrt_rn(d2);
+	const float var = fmaxf(n.meanVar.w, 0x1.0p-31f * d2);
+	const float sharp = d2 / var;
+	const sg::Lobe lobe = sg::product(f3_of(n.dirSharp), n.dirSharp.w, ld, sharp);
+	const float amp = expf(lobe.logAmplitude);
+	const float cosine = clampf(dot(lobe.axis, nrm), -1.0f, 1.0f);
+	return (n.fluxInt.x / (var * n.fluxInt.y)) * amp * sg::clampedCosineProductOverPi2024(cosine, lobe.sharpness);
+}
+
 // traverseLightTree: pdf of picking light (type, index) from p with normal n.
 RB_D float lightTreePdf(const DevScene& sc, uint32_t type, uint32_t index, f3 p, f3 nrm)
 {
@@ -219,27 +258,30 @@ RB_D float lightTreePdf(const DevScene& sc, uint32_t type, uint32_t index, f3 p,
 	if (type == kLightTypeSky) return envImp;
 	float pdf = 1.0f - envImp;
 	const uint64_t mask = sc.lights.bitmasks[index];
+	const TreeNodeU* nodes = sc.lights.unpacked;
 	uint32_t cur = 0;
-	TreeNode node = unpackNode(sc.lights.nodes, 0);
+	TreeNodeU node = loadNodeU(nodes, 0);
 	for (int depth = 0; depth < 64; ++depth)
 	{
-		if (node.leaf) break;
-		const TreeNode l = unpackNode(sc.lights.nodes, cur + 1);
-		const float li = nodeImportance(l, p, nrm);
-		const TreeNode r = unpackNode(sc.lights.nodes, node.a);
-		const float ri = nodeImportance(r, p, nrm);
+		if (nodeLeaf(node)) break;
+		const TreeNodeU l = loadNodeU(nodes, cur + 1);
+		const float li = nodeImportanceU(l, p, nrm);
+		const TreeNodeU r = loadNodeU(nodes, nodeA(node));
+		const float ri = nodeImportanceU(r, p, nrm);
 		const bool right = (mask >> depth) & 1ull;
-		cur = right ? node.a : cur + 1;
+		cur = right ? nodeA(node) : cur + 1;
 		node = right ? r : l;
 		pdf *= right ? ri / (li + ri) : li / (li + ri);
 	}
-	pdf *= 1.0f / static_cast<float>(node.a);
+	pdf *= 1.0f / static_cast<float>(nodeA(node));
 	return pdf;
 }
 
 // sampleLightTree: pick the environment (0.3 when both exist) or descend the
-// tree choosing children by importance with rescaled `rand`.
-RB_D void lightTreeSample(const DevScene& sc, float rand, f3 p, f3 nrm, uint32_t& type, uint32_t& index, float& pdf)
+// tree choosing children by importance with rescaled `rand`. `nodes` is the
+// unpacked tree in shared or global memory.
+RB_D void lightTreeSample(const DevScene& sc, const TreeNodeU* nodes, float rand, f3 p, f3 nrm, uint32_t& type,
+	uint32_t& index, float& pdf)
 {
 	const bool envPresent = sc.env.enabled != 0;
 	const bool treePresent = sc.lights.nodes != nullptr;
@@ -252,23 +294,24 @@ RB_D void lightTreeSample(const DevScene& sc, float rand, f3 p, f3 nrm, uint32_t
 	rand = clampf((rand - envImp) / (1.0f - envImp), 0.0f, 1.0f);
 	pdf = 1.0f - envImp;
 	uint32_t cur = 0;
-	TreeNode node = unpackNode(sc.lights.nodes, 0);
-	while (!node.leaf)
+	TreeNodeU node = loadNodeU(nodes, 0);
+	while (!nodeLeaf(node))
 	{
-		const TreeNode l = unpackNode(sc.lights.nodes, cur + 1);
-		const TreeNode r = unpackNode(sc.lights.nodes, node.a);
-		const float li = nodeImportance(l, p, nrm);
-		const float ri = nodeImportance(r, p, nrm);
+		const TreeNodeU l = loadNodeU(nodes, cur + 1);
+		const TreeNodeU r = loadNodeU(nodes, nodeA(node));
+		const float li = nodeImportanceU(l, p, nrm);
+		const float ri = nodeImportanceU(r, p, nrm);
 		const float sep = li / (li + ri);
 		const bool right = rand > sep;
-		cur = right ? node.a : cur + 1;
+		cur = right ? nodeA(node) : cur + 1;
 		node = right ? r : l;
 		pdf *= right ? 1.0f - sep : sep;
 		rand = right ? clampf((rand - sep) / (1.0f - sep), 0.0f, 1.0f) : clampf(rand / sep, 0.0f, 1.0f);
 	}
-	const uint32_t k = static_cast<uint32_t>(static_cast<float>(node.a) * rand);
-	const uint32_t slot = node.b + (k == node.a ? node.a - 1u : k);
-	pdf *= 1.0f / static_cast<float>(node.a);
+	const uint32_t count = nodeA(node);
+	const uint32_t k = static_cast<uint32_t>(static_cast<float>(count) * rand);
+	const uint32_t slot = nodeB(node) + (k == count ? count - 1u : k);
+	pdf *= 1.0f / static_cast<float>(count);
 	const uint32_t ptr = __ldg(sc.lights.pointers + slot);
 	type = ptr >> 30;
 	index = ptr & ((1u << 30) - 1u);

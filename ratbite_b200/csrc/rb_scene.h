@@ -114,9 +114,20 @@ struct DevGeometry
 	uint32_t pad;
 };
 
+// A light-tree node unpacked for the descent (48 B): mean and variance,
+// decoded average direction and sharpness, then flux, the SG integral of the
+// sharpness, and the child / leaf words (a; b with the leaf bit in bit 31).
+struct alignas(16) TreeNodeU
+{
+	float4 meanVar;
+	float4 dirSharp;
+	float4 fluxInt;
+};
+
 struct DevLights
 {
 	const PackedNode* nodes;     // nullptr when there is no light tree
+	const TreeNodeU* unpacked;   // nodes unpacked on the device (same indexing)
 	const uint32_t* pointers;
 	const EmissiveTri* triangles;
 	const uint64_t* bitmasks;

@@ -1,0 +1,148 @@
+// Ray-traversal kernels: the extend (closest hit) and shadow (any hit)
+// stages of the wavefront loop, and the batched trace / occlusion entry
+// points. This translation unit keeps the compiler's default multiply-add
+// contraction: the box tests are conservative by construction (outward
+// rounding and padding of the quantized boxes), and the triangle test, which
+// decides the reported hit, is written with explicitly rounded operations.
+
+#include <cfloat>
+
+#include "rb_bvh.cuh"
+#include "rb_launch.cuh"
+#include "rb_wavefront.h"
+
+namespace rb
+{
+namespace
+{
+// counters (COUNT only): [0] rays, [1] nodes, [2] triangles.
+template<bool COUNT>
+__global__ void __launch_bounds__(kThreads) kExtend(DevScene sc, PathSoA s, int bounce, unsigned long long* counters)
+{
+	const uint32_t n = s.counts[bounce];
+	const uint32_t* q = s.queue[bounce & 1];
+	uint32_t rays = 0, nodes = 0, tris = 0;
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const uint32_t p = q[i];
+		const float4 o = s.rayO[p], d = s.rayD[p];
+		const Hit h = traceClosestT<COUNT>(sc.geo, f3_of(o), f3_of(d), 0.0f, FLT_MAX, sc.status, nodes, tris);
+		s.hit[p] = make_float4(__int_as_float(h.tri), h.t, h.b1, h.b2);
+		++rays;
+	}
+	if (COUNT)
+	{
+		warpAdd(counters + 0, rays);
+		warpAdd(counters + 1, nodes);
+		warpAdd(counters + 2, tris);
+	}
+}
+
+
+template<bool COUNT>
+__global__ void __launch_bounds__(kThreads) kShadow(DevScene sc, PathSoA s, int bounce, unsigned long long* counters)
+{
+	const uint32_t n = s.counts[kShadowCounts + bounce];
+	uint32_t rays = 0, nodes = 0, tris = 0;
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const uint32_t p = s.shadowQueue[i];
+		const float4 o = s.shO[p], d = s.shD[p];
+		if (!traceAnyT<COUNT>(sc.geo, f3_of(o), f3_of(d), 0.0f, o.w, sc.status, nodes, tris))
+		{
+			S4 L = s4(s.L[p]);
+			L += s4(s.shC[p]);
+			s.L[p] = f4(L);
+		}
+		++rays;
+	}
+	if (COUNT)
+	{
+		warpAdd(counters + 3, rays);
+		warpAdd(counters + 4, nodes);
+		warpAdd(counters + 5, tris);
+	}
+}
+
+
+// Closest hit returned in the reference's 24-word payload layout.
+__global__ void kTrace(DevScene sc, uint32_t n, const float* rays, uint32_t* payload, float* tOut, int32_t* triOut)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const f3 o = mk(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
+		const f3 d = mk(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
+		const Hit h = traceClosest(sc.geo, o, d, 0.0f, FLT_MAX, sc.status);
+		uint32_t* pl = payload + 24 * static_cast<size_t>(i);
+		for (int k = 0; k < 24; ++k) pl[k] = 0u;
+		if (h.tri < 0)
+		{
+			pl[8] = kLightTypeSky << 30;
+			tOut[i] = INFINITY;
+			triOut[i] = -1;
+			continue;
+		}
+		const float4 a = sc.geo.triVerts[3 * h.tri], b = sc.geo.triVerts[3 * h.tri + 1], c = sc.geo.triVerts[3 * h.tri + 2];
+		const uint2 aux = sc.geo.triAux[h.tri];
+		const uint32_t sbt = __float_as_uint(c.w);
+		uint32_t prim = aux.y, mat = sbt, lptr = kLightTypeNone << 30;
+		if (sbt == 0xFFFFFFFFu)
+		{
+			lptr = (kLightTypeTriangle << 30) | (aux.y & ((1u << 30) - 1u));
+			prim = sc.lights.triangles[aux.y].prim;
+			mat = sc.lights.triangles[aux.y].material;
+		}
+		pl[0] = __float_as_uint(a.x); pl[1] = __float_as_uint(a.y); pl[2] = __float_as_uint(a.z);
+		pl[3] = aux.x; pl[4] = prim; pl[5] = __float_as_uint(h.b1); pl[6] = __float_as_uint(h.b2);
+		pl[7] = mat; pl[8] = lptr;
+		const float* M = sc.geo.normalMatrix + 9u * __float_as_uint(b.w);
+		for (int k = 0; k < 9; ++k) pl[9 + k] = __float_as_uint(M[k]);
+		pl[18] = __float_as_uint(b.x); pl[19] = __float_as_uint(b.y); pl[20] = __float_as_uint(b.z);
+		pl[21] = __float_as_uint(c.x); pl[22] = __float_as_uint(c.y); pl[23] = __float_as_uint(c.z);
+		tOut[i] = h.t;
+		triOut[i] = static_cast<int32_t>(__float_as_uint(a.w));
+	}
+}
+__global__ void kOccluded(DevScene sc, uint32_t n, const float* rays, const float* tmax, uint32_t* out)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const f3 o = mk(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
+		const f3 d = mk(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
+		out[i] = traceAny(sc.geo, o, d, 0.0f, tmax[i], sc.status) ? 1u : 0u;
+	}
+}
+} // namespace
+
+void queryTraceShape(LaunchShape& ls)
+{
+	auto occ = [&](const void* fn) {
+		int b = 0;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, 0);
+		return (b < 1 ? 1 : b) * ls.smCount;
+	};
+	ls.blocksExtend = occ(reinterpret_cast<const void*>(kExtend<false>));
+	ls.blocksShadow = occ(reinterpret_cast<const void*>(kShadow<false>));
+}
+
+void launchExtend(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
+	unsigned long long* counters)
+{
+	if (counters) kExtend<true><<<ls.blocksExtend, kThreads, 0, st>>>(sc, s, bounce, counters);
+	else kExtend<false><<<ls.blocksExtend, kThreads, 0, st>>>(sc, s, bounce, nullptr);
+}
+void launchShadow(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
+	unsigned long long* counters)
+{
+	if (counters) kShadow<true><<<ls.blocksShadow, kThreads, 0, st>>>(sc, s, bounce, counters);
+	else kShadow<false><<<ls.blocksShadow, kThreads, 0, st>>>(sc, s, bounce, nullptr);
+}
+void launchTrace(const DevScene& sc, uint32_t n, const float* rays, uint32_t* payload, float* t, int32_t* tri, cudaStream_t st)
+{
+	kTrace<<<gridFor(n), kThreads, 0, st>>>(sc, n, rays, payload, t, tri);
+}
+void launchOccluded(const DevScene& sc, uint32_t n, const float* rays, const float* tmax, uint32_t* out, cudaStream_t st)
+{
+	kOccluded<<<gridFor(n), kThreads, 0, st>>>(sc, n, rays, tmax, out);
+}
+} // namespace rb

@@ -25,13 +25,25 @@ struct PathSoA
 	float4* hit;       // closest hit: triangle (bits, -1 miss), t, b1, b2
 	float4* shO;       // shadow ray origin, w: tmax
 	float4* shD;       // shadow ray direction
-	float4* shC;       // pending light-sample contribution
+	float4* shC;       // light sample spectrum, then the pending light-sample contribution
+	// surface record of the current bounce (written by kSurface)
+	float4* sfP;       // hit position, w: material index (bits)
+	float4* sfPi;      // shadow-terminator-offset position, w: surface bits (kSf*)
+	float4* sfGn;      // geometric normal
+	float4* sfT;       // shading frame tangent (the normal is nrm)
+	float4* sfB;       // shading frame bitangent
 	uint32_t* queue[2];// active path slots, ping-pong by bounce parity
+	uint32_t* surfQueue;   // paths with a surface record this bounce
 	uint32_t* shadowQueue;
-	uint32_t* counts;  // [bounce] active counts (kMaxBounces+1), then [kMaxBounces+1 + bounce] shadow counts
+	uint32_t* counts;  // kCountSlots words: see kShadowCounts, kSurfaceCounts
 	uint32_t capacity;
 };
 constexpr int kMaxBounces = 64;
+// counts[b]: paths entering bounce b; counts[kShadowCounts + b]: shadow rays
+// of bounce b; counts[kSurfaceCounts + b]: surface records of bounce b.
+constexpr uint32_t kShadowCounts = kMaxBounces + 1;
+constexpr uint32_t kSurfaceCounts = 2 * (kMaxBounces + 1);
+constexpr uint32_t kCountSlots = 3 * (kMaxBounces + 1);
 
 struct WaveParams
 {
@@ -44,17 +56,23 @@ struct WaveParams
 struct LaunchShape
 {
 	int smCount;
-	int blocksGenerate, blocksExtend, blocksShade, blocksShadow, blocksResolve;
+	int blocksGenerate, blocksExtend, blocksSurface, blocksNee, blocksBsdf, blocksShadow, blocksResolve;
 	int threads;
 };
 
 LaunchShape queryLaunchShape();
 void launchGenerate(const DevScene& sc, const PathSoA& s, const WaveParams& w, const LaunchShape& ls, cudaStream_t st);
-// counters: nullptr, or 6 device uint64 (extend rays/nodes/tris, shadow rays/nodes/tris)
-// to run the counting variants.
+// counters: nullptr, or 7 device uint64 (extend rays/nodes/tris, shadow rays/nodes/tris,
+// surface records) to run the counting variants.
 void launchExtend(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
 	unsigned long long* counters);
-void launchShade(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st);
+// The shading stage as three kernels: surface record, light sample, BxDF.
+void launchSurface(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st,
+	unsigned long long* counters);
+void launchNee(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st);
+void launchBsdf(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st);
+void launchUnpackLightTree(const PackedNode* in, TreeNodeU* out, uint32_t n, cudaStream_t st);
+void queryTraceShape(LaunchShape& ls);   // fills blocksExtend, blocksShadow (rb_trace.cu)
 void launchShadow(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
 	unsigned long long* counters);
 void launchResolve(const DevScene& sc, const PathSoA& s, const WaveParams& w, double4* accum, const LaunchShape& ls, cudaStream_t st);

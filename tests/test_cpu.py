@@ -57,20 +57,20 @@ def test_library_loads_without_gpu():
     assert rc != 0 and not h.value
 
 
-def test_abi_record_sizes():
+def test_abi_record_sizes(tmp_path):
     # sizes of the C records (x86-64 SysV): computed by the C compiler
-    src = ROOT / "_work" / "abi_sizes.c"
-    src.parent.mkdir(exist_ok=True)
-    src.write_text('#include <stdio.h>\n#include "ratbite_b200_kernels.h"\nint main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n",'
+    src = tmp_path / "abi_sizes.c"
+    src.write_text('#include <stdio.h>\n#include "ratbite_b200_kernels.h"\nint main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n",'
                    'sizeof(rb_config),sizeof(rb_material),sizeof(rb_submesh),sizeof(rb_mesh),sizeof(rb_instance),'
                    'sizeof(rb_emissive_subset),sizeof(rb_geometry),sizeof(rb_light_tree),sizeof(rb_launch),'
-                   'sizeof(rb_bxdf_case),sizeof(rb_light_case));}\n')
+                   'sizeof(rb_bxdf_case),sizeof(rb_light_case),sizeof(rb_device_status),sizeof(rb_render_stats));}\n')
     exe = src.with_suffix("")
     subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
     sizes = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     ours = [C.sizeof(t) for t in (abi.rb_config, abi.rb_material, abi.rb_submesh, abi.rb_mesh, abi.rb_instance,
                                   abi.rb_emissive_subset, abi.rb_geometry, abi.rb_light_tree, abi.rb_launch,
-                                  abi.rb_bxdf_case, abi.rb_light_case)]
+                                  abi.rb_bxdf_case, abi.rb_light_case, abi.rb_device_status,
+                                  abi.rb_render_stats)]
     assert sizes == ours
 
 

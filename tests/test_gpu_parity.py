@@ -112,7 +112,15 @@ def test_wavelengths(ref):
     report("wavelength", gl, lam)
     report("wavelength pdf", gp, pdf)
     assert close(gl, lam).all()
-    assert close(gp, pdf, atol=1e-9).all()
+    # visibleWavelengthsPDF is 0 outside [360, 830] nm and u = 0 maps to
+    # 360.0 nm up to one ulp of the atanh warp, so a one-ulp difference of
+    # atanhf between CUDA and the host libm could put a wavelength on the other
+    # side of the range end than the oracle's: such entries alone are exempt,
+    # and only when they sit within 1e-3 nm of an end (none did on B200).
+    pdf_ok = close(gp, pdf, atol=1e-9)
+    at_end = (np.abs(lam - 360.0) < 1e-3) | (np.abs(lam - 830.0) < 1e-3)
+    assert (pdf_ok | at_end).all()
+    assert (~pdf_ok).sum() <= 8
 
 
 def test_camera_rays(ref, cornell, tables):
@@ -278,12 +286,22 @@ def test_light_tree_parity(ref, tables):
     gq = np.array([c.q_pdf for c in got]); wq = np.array([c.q_pdf for c in want])
     report("light sample pdf", gp[same_pick], wp[same_pick])
     report("light pdf replay", gq, wq)
-    # The SG importance has (cos - 1) cancellations for distant, sharp nodes:
-    # an ulp of input moves the pdf by ~1e-5..1e-4 relative in rare cases.
-    assert close(gp[same_pick], wp[same_pick], rtol=1e-5, atol=1e-9).mean() >= 0.99
-    assert close(gp[same_pick], wp[same_pick], rtol=1e-3, atol=1e-9).all()
-    assert close(gq, wq, rtol=1e-5, atol=1e-9).mean() >= 0.99
-    assert close(gq, wq, rtol=1e-3, atol=1e-9).all()
+    # Tolerance. A pick's pdf is a product of one importance ratio per tree
+    # level, and each importance goes through exp(logAmplitude) with
+    # logAmplitude = 2 s (cos - 1) / (...) of magnitude up to ~1e2 for sharp,
+    # distant nodes, so a one-ulp difference of expf between CUDA and the host
+    # libm is up to ~1e2 ulps in the pdf. The shading kernels round every
+    # operation as the oracle does (no FMA contraction), so that is the only
+    # source: the 1e-5 relative bound holds for all but the worst-conditioned
+    # cases, and the tail stays below 2e-4 (measured on B200: sample pdf max
+    # 7.0e-5, replayed pdf max 5.8e-5, 99.9% within 1e-5). Picks must agree.
+    ok_s = close(gp[same_pick], wp[same_pick], rtol=1e-5, atol=1e-9)
+    ok_q = close(gq, wq, rtol=1e-5, atol=1e-9)
+    print(f"within 1e-5: sample pdf {ok_s.mean():.4%}, replayed pdf {ok_q.mean():.4%}")
+    assert ok_s.mean() >= 0.995
+    assert ok_q.mean() >= 0.995
+    assert close(gp[same_pick], wp[same_pick], rtol=2e-4, atol=1e-9).all()
+    assert close(gq, wq, rtol=2e-4, atol=1e-9).all()
 
 
 # ----------------------------------------------------------------- render
