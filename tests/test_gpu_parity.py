@@ -3,8 +3,9 @@ ABI, against the reference's own code run by the oracle on the same inputs.
 
 Tolerances: integer work (QRNG, hashes, hit ids, payload words, ray-origin
 offsets) is bit-exact. Float stages are compared at 1e-5 relative (plus an
-absolute floor for values near zero): the device uses fused multiply-add and
-CUDA's libm, the oracle strict IEEE and glibc. A stage whose result is a
+absolute floor for values near zero): the shading kernels round every
+operation as the oracle does (no multiply-add contraction), so what remains
+is CUDA's libm against glibc (expf, sinf, atanhf, powf ...). A stage whose result is a
 discrete choice made by comparing floats (BxDF lobe, light-tree child) can
 flip when a probability lands within rounding of the random number; those
 cases are counted and bounded (<= 0.5 %), not ignored.
