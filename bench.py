@@ -236,7 +236,7 @@ def run_ours(args, rank: int, world: int, wl: dict):
     t_setup = time.perf_counter()
     scene, cie, basis, luts = make_scene(wl)
     lt = lighttree.build_for_scene(scene)
-    ri = RenderingInterface(device=local)
+    ri = RenderingInterface(device=local, max_paths_in_flight=args.max_paths)
     ri.load_scene(scene, luts, cie, basis, light_tree=lt)
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t_setup
@@ -356,7 +356,8 @@ def run_ours(args, rank: int, world: int, wl: dict):
                        "triangles": scene.triangle_count(), "emitters": int(sum(len(e["prim"]) for e in scene.emissive)),
                        "materials": len(scene.materials), "envmap": list(scene.envmap.shape[1::-1]) if has_env else None,
                        "paths_per_step": paths_per_step, "parallelism": f"sample-range x{world}",
-                       "l2": "inputs larger than L2 (wavefront path state ~3.2 GB per wave)",
+                       "l2": "inputs larger than L2 (wavefront path state 280 B per path in flight, "
+                             "~4.7 GB at the default 16M paths per wave)",
                        "setup_s": setup_s},
             "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": C.sizeof(launch),
                     "d2h_bytes_per_step": W * H * 32, "steps": e2e_steps},
@@ -394,11 +395,18 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="scale")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample length (0 = skip)")
     ap.add_argument("--ref-step-s", type=float, default=4.0, help="reference arm: seconds per step")
+    ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0 = the workload's)")
+    ap.add_argument("--max-paths", type=int, default=0,
+                    help="paths in flight per wave (0 = the library default, 16M); small values make profiling "
+                         "captures small")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     args.warmup = max(args.warmup, 3)
-    wl = WORKLOADS[args.workload]
+    wl = dict(WORKLOADS[args.workload])
+    if args.spp:
+        wl["spp"] = args.spp
+        wl["name"] = wl["name"].replace(f"{WORKLOADS[args.workload]['spp']}spp", f"{args.spp}spp")
     if args.impl == "reference":
         run_reference(args, rank, world, wl)
     else:

@@ -103,14 +103,18 @@ RB_D uint32_t nodeChild(const NodeView& v, int c)
 	const float w = (c & 3) == 0 ? a.x : ((c & 3) == 1 ? a.y : ((c & 3) == 2 ? a.z : a.w));
 	return __float_as_uint(w);
 }
-// Quantized byte of plane `k` (0..5: lo x,y,z, hi x,y,z) of child c.
-RB_D uint32_t nodeQ(const NodeView& v, int k, int c)
+// Quantized byte of plane `k` (0..5: lo x,y,z, hi x,y,z) of child c, as a
+// float. The byte is placed in the mantissa of 2^23 with one byte permute and
+// 2^23 subtracted (exact), which keeps the conversion off the slower
+// conversion pipe.
+RB_D float nodeQf(const NodeView& v, int k, int c)
 {
 	const int byte = k * 8 + c;                 // offset inside the 48-byte box block
 	const float4& a = v.q[3 + byte / 16];
 	const int w = (byte % 16) / 4;
 	const uint32_t word = __float_as_uint(w == 0 ? a.x : (w == 1 ? a.y : (w == 2 ? a.z : a.w)));
-	return (word >> ((byte & 3) * 8)) & 0xFFu;
+	const uint32_t bits = __byte_perm(word, 0x4B000000u, static_cast<uint32_t>(byte & 3) | 0x7540u);
+	return __fsub_rn(__uint_as_float(bits), 8388608.0f);
 }
 
 // Intersects the ray with the 8 child boxes; hitMask bit c set when child c
@@ -129,12 +133,12 @@ RB_D uint32_t childBoxes(const TraceRay& r, const NodeView& v, float tmin, float
 #pragma unroll
 	for (int c = 0; c < 8; ++c)
 	{
-		const float lx = (__fmaf_rn(static_cast<float>(nodeQ(v, 0, c)), scx, ox) - r.o.x) * r.ix;
-		const float hx = (__fmaf_rn(static_cast<float>(nodeQ(v, 3, c)), scx, ox) - r.o.x) * r.ix;
-		const float ly = (__fmaf_rn(static_cast<float>(nodeQ(v, 1, c)), scy, oy) - r.o.y) * r.iy;
-		const float hy = (__fmaf_rn(static_cast<float>(nodeQ(v, 4, c)), scy, oy) - r.o.y) * r.iy;
-		const float lz = (__fmaf_rn(static_cast<float>(nodeQ(v, 2, c)), scz, oz) - r.o.z) * r.iz;
-		const float hz = (__fmaf_rn(static_cast<float>(nodeQ(v, 5, c)), scz, oz) - r.o.z) * r.iz;
+		const float lx = (__fmaf_rn(nodeQf(v, 0, c), scx, ox) - r.o.x) * r.ix;
+		const float hx = (__fmaf_rn(nodeQf(v, 3, c), scx, ox) - r.o.x) * r.ix;
+		const float ly = (__fmaf_rn(nodeQf(v, 1, c), scy, oy) - r.o.y) * r.iy;
+		const float hy = (__fmaf_rn(nodeQf(v, 4, c), scy, oy) - r.o.y) * r.iy;
+		const float lz = (__fmaf_rn(nodeQf(v, 2, c), scz, oz) - r.o.z) * r.iz;
+		const float hz = (__fmaf_rn(nodeQf(v, 5, c), scz, oz) - r.o.z) * r.iz;
 		const float n = fmaxf(fmaxf(fminf(lx, hx), fminf(ly, hy)), fmaxf(fminf(lz, hz), tmin));
 		const float f = fminf(fminf(fmaxf(lx, hx), fmaxf(ly, hy)), fminf(fmaxf(lz, hz), tmax)) * 1.0000004f;
 		tnear[c] = n;
@@ -168,135 +172,199 @@ struct Hit
 	float t, b1, b2;
 };
 
-// Closest hit on (tmin, tmax). Sets RB_DEV_STACK_OVERFLOW in *status and
-// returns the best hit so far if the stack runs out. With COUNT, nNodes and
-// nTris count the wide nodes loaded and triangles tested.
+// Closest-hit traversal on (tmin, tmax) as a resumable state: run() visits
+// at most `budget` nodes or leaves and returns true once the traversal has
+// ended, so a persistent warp can hand an idle lane a new ray between calls.
+// Sets RB_DEV_STACK_OVERFLOW in *status and keeps the best hit so far if the
+// stack runs out. With COUNT, nNodes and nTris count the wide nodes loaded and
+// triangles tested.
+struct ClosestTraversal
+{
+	TraceRay r;
+	float tmin;
+	Hit best;
+	uint32_t bestId;
+	uint32_t cur;
+	int sp;
+	bool done;
+
+	RB_D void init(const DevGeometry& g, f3 o, f3 d, float tmin_, float tmax)
+	{
+		best = Hit{ -1, tmax, 0.0f, 0.0f };
+		bestId = 0xFFFFFFFFu;
+		tmin = tmin_;
+		sp = 0;
+		done = g.triCount == 0;
+		r = makeTraceRay(o, d);
+		cur = g.rootIsLeaf ? (kLeafBit | (static_cast<uint32_t>(g.triCount - 1) << 28)) : 0u;
+	}
+
+	// The stack lives outside the state (separate local arrays) so that the
+	// scalar state can stay in registers.
+	template<bool COUNT>
+	RB_D bool run(const DevGeometry& g, int budget, uint32_t* status, uint32_t& nNodes, uint32_t& nTris,
+		uint32_t (&stackRef)[kTraversalStack], float (&stackT)[kTraversalStack])
+	{
+		for (int it = 0; it < budget && !done; ++it)
+		{
+			if (cur & kLeafBit)
+			{
+				const uint32_t first = cur & 0x0FFFFFFFu;
+				const uint32_t count = ((cur >> 28) & 0x7u) + 1u;
+				if (COUNT) nTris += count;
+				for (uint32_t i = first; i < first + count; ++i)
+				{
+					const float4 a = __ldg(g.triVerts + 3 * i);
+					const float4 b = __ldg(g.triVerts + 3 * i + 1);
+					const float4 c = __ldg(g.triVerts + 3 * i + 2);
+					float t, u, v;
+					if (intersectTriangle(r, f3_of(a), f3_of(b), f3_of(c), tmin, best.t, best.tri >= 0, t, u, v))
+					{
+						const uint32_t id = __float_as_uint(a.w);
+						if (best.tri < 0 || t < best.t || id < bestId)
+						{
+							best = Hit{ static_cast<int32_t>(i), t, u, v };
+							bestId = id;
+						}
+					}
+				}
+			}
+			else
+			{
+				if (COUNT) ++nNodes;
+				const NodeView nv = loadNode(g.nodes, cur);
+				float tn[8];
+				const uint32_t mask = childBoxes(r, nv, tmin, best.t, tn);
+				if (mask)
+				{
+					float key[8];
+					uint32_t ref[8];
+#pragma unroll
+					for (int c = 0; c < 8; ++c)
+					{
+						key[c] = (mask >> c) & 1u ? tn[c] : INFINITY;
+						ref[c] = nodeChild(nv, c);
+					}
+					sort8(key, ref);
+					const int n = __popc(mask);
+					// push the far ones (n-1 .. 1), continue with the nearest
+#pragma unroll
+					for (int c = 7; c >= 1; --c)
+					{
+						if (c < n)
+						{
+							if (sp < kTraversalStack) { stackRef[sp] = ref[c]; stackT[sp] = key[c]; ++sp; }
+							else atomicOr(status, RB_DEV_STACK_OVERFLOW);
+						}
+					}
+					cur = ref[0];
+					continue;
+				}
+			}
+			// pop the next entry that may still hold a closer hit
+			bool found = false;
+			while (sp > 0)
+			{
+				--sp;
+				if (stackT[sp] <= best.t) { cur = stackRef[sp]; found = true; break; }
+			}
+			if (!found) done = true;
+		}
+		return done;
+	}
+};
+
+// Any-hit traversal on (tmin, tmax), resumable like ClosestTraversal:
+// occlusion test of a shadow ray.
+struct AnyTraversal
+{
+	TraceRay r;
+	float tmin, tmax;
+	uint32_t cur;
+	int sp;
+	bool done, hit;
+
+	RB_D void init(const DevGeometry& g, f3 o, f3 d, float tmin_, float tmax_)
+	{
+		tmin = tmin_;
+		tmax = tmax_;
+		sp = 0;
+		hit = false;
+		done = g.triCount == 0;
+		r = makeTraceRay(o, d);
+		cur = g.rootIsLeaf ? (kLeafBit | (static_cast<uint32_t>(g.triCount - 1) << 28)) : 0u;
+	}
+
+	template<bool COUNT>
+	RB_D bool run(const DevGeometry& g, int budget, uint32_t* status, uint32_t& nNodes, uint32_t& nTris,
+		uint32_t (&stack)[kTraversalStack])
+	{
+		for (int it = 0; it < budget && !done; ++it)
+		{
+			if (cur & kLeafBit)
+			{
+				const uint32_t first = cur & 0x0FFFFFFFu;
+				const uint32_t count = ((cur >> 28) & 0x7u) + 1u;
+				for (uint32_t i = first; i < first + count; ++i)
+				{
+					if (COUNT) ++nTris;
+					const float4 a = __ldg(g.triVerts + 3 * i);
+					const float4 b = __ldg(g.triVerts + 3 * i + 1);
+					const float4 c = __ldg(g.triVerts + 3 * i + 2);
+					float t, u, v;
+					if (intersectTriangle(r, f3_of(a), f3_of(b), f3_of(c), tmin, tmax, false, t, u, v))
+					{
+						hit = true;
+						done = true;
+						break;
+					}
+				}
+				if (done) break;
+			}
+			else
+			{
+				if (COUNT) ++nNodes;
+				const NodeView nv = loadNode(g.nodes, cur);
+				float tn[8];
+				const uint32_t mask = childBoxes(r, nv, tmin, tmax, tn);
+#pragma unroll
+				for (int c = 0; c < 8; ++c)
+				{
+					if ((mask >> c) & 1u)
+					{
+						if (sp < kTraversalStack) stack[sp++] = nodeChild(nv, c);
+						else atomicOr(status, RB_DEV_STACK_OVERFLOW);
+					}
+				}
+			}
+			if (sp == 0) { done = true; break; }
+			cur = stack[--sp];
+		}
+		return done;
+	}
+};
+
 template<bool COUNT>
 RB_D Hit traceClosestT(const DevGeometry& g, f3 o, f3 d, float tmin, float tmax, uint32_t* status,
 	uint32_t& nNodes, uint32_t& nTris)
 {
-	Hit best{ -1, tmax, 0.0f, 0.0f };
-	if (g.triCount == 0) return best;
-	const TraceRay r = makeTraceRay(o, d);
+	ClosestTraversal tr;
 	uint32_t stackRef[kTraversalStack];
 	float stackT[kTraversalStack];
-	int sp = 0;
-	uint32_t bestId = 0xFFFFFFFFu;
-	uint32_t cur = g.rootIsLeaf ? (kLeafBit | (static_cast<uint32_t>(g.triCount - 1) << 28)) : 0u;
-	for (;;)
-	{
-		if (cur & kLeafBit)
-		{
-			const uint32_t first = cur & 0x0FFFFFFFu;
-			const uint32_t count = ((cur >> 28) & 0x7u) + 1u;
-			if (COUNT) nTris += count;
-			for (uint32_t i = first; i < first + count; ++i)
-			{
-				const float4 a = __ldg(g.triVerts + 3 * i);
-				const float4 b = __ldg(g.triVerts + 3 * i + 1);
-				const float4 c = __ldg(g.triVerts + 3 * i + 2);
-				float t, u, v;
-				if (intersectTriangle(r, f3_of(a), f3_of(b), f3_of(c), tmin, best.t, best.tri >= 0, t, u, v))
-				{
-					const uint32_t id = __float_as_uint(a.w);
-					if (best.tri < 0 || t < best.t || id < bestId)
-					{
-						best = Hit{ static_cast<int32_t>(i), t, u, v };
-						bestId = id;
-					}
-				}
-			}
-		}
-		else
-		{
-			if (COUNT) ++nNodes;
-			const NodeView nv = loadNode(g.nodes, cur);
-			float tn[8];
-			uint32_t mask = childBoxes(r, nv, tmin, best.t, tn);
-			if (mask)
-			{
-				float key[8];
-				uint32_t ref[8];
-#pragma unroll
-				for (int c = 0; c < 8; ++c)
-				{
-					key[c] = (mask >> c) & 1u ? tn[c] : INFINITY;
-					ref[c] = nodeChild(nv, c);
-				}
-				sort8(key, ref);
-				const int n = __popc(mask);
-				// push the far ones (n-1 .. 1), continue with the nearest
-#pragma unroll
-				for (int c = 7; c >= 1; --c)
-				{
-					if (c < n)
-					{
-						if (sp < kTraversalStack) { stackRef[sp] = ref[c]; stackT[sp] = key[c]; ++sp; }
-						else atomicOr(status, RB_DEV_STACK_OVERFLOW);
-					}
-				}
-				cur = ref[0];
-				continue;
-			}
-		}
-		// pop the next entry that may still hold a closer hit
-		bool found = false;
-		while (sp > 0)
-		{
-			--sp;
-			if (stackT[sp] <= best.t) { cur = stackRef[sp]; found = true; break; }
-		}
-		if (!found) break;
-	}
-	return best;
+	tr.init(g, o, d, tmin, tmax);
+	while (!tr.run<COUNT>(g, 1 << 30, status, nNodes, nTris, stackRef, stackT)) {}
+	return tr.best;
 }
 
-// Any hit on (tmin, tmax): occlusion test of a shadow ray.
 template<bool COUNT>
 RB_D bool traceAnyT(const DevGeometry& g, f3 o, f3 d, float tmin, float tmax, uint32_t* status,
 	uint32_t& nNodes, uint32_t& nTris)
 {
-	if (g.triCount == 0) return false;
-	const TraceRay r = makeTraceRay(o, d);
+	AnyTraversal tr;
 	uint32_t stack[kTraversalStack];
-	int sp = 0;
-	uint32_t cur = g.rootIsLeaf ? (kLeafBit | (static_cast<uint32_t>(g.triCount - 1) << 28)) : 0u;
-	for (;;)
-	{
-		if (cur & kLeafBit)
-		{
-			const uint32_t first = cur & 0x0FFFFFFFu;
-			const uint32_t count = ((cur >> 28) & 0x7u) + 1u;
-			for (uint32_t i = first; i < first + count; ++i)
-			{
-				if (COUNT) ++nTris;
-				const float4 a = __ldg(g.triVerts + 3 * i);
-				const float4 b = __ldg(g.triVerts + 3 * i + 1);
-				const float4 c = __ldg(g.triVerts + 3 * i + 2);
-				float t, u, v;
-				if (intersectTriangle(r, f3_of(a), f3_of(b), f3_of(c), tmin, tmax, false, t, u, v)) return true;
-			}
-		}
-		else
-		{
-			if (COUNT) ++nNodes;
-			const NodeView nv = loadNode(g.nodes, cur);
-			float tn[8];
-			const uint32_t mask = childBoxes(r, nv, tmin, tmax, tn);
-#pragma unroll
-			for (int c = 0; c < 8; ++c)
-			{
-				if ((mask >> c) & 1u)
-				{
-					if (sp < kTraversalStack) stack[sp++] = nodeChild(nv, c);
-					else atomicOr(status, RB_DEV_STACK_OVERFLOW);
-				}
-			}
-		}
-		if (sp == 0) break;
-		cur = stack[--sp];
-	}
-	return false;
+	tr.init(g, o, d, tmin, tmax);
+	while (!tr.run<COUNT>(g, 1 << 30, status, nNodes, nTris, stack)) {}
+	return tr.hit;
 }
 RB_D Hit traceClosest(const DevGeometry& g, f3 o, f3 d, float tmin, float tmax, uint32_t* status)
 {

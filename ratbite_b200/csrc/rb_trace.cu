@@ -15,6 +15,44 @@ namespace rb
 {
 namespace
 {
+// Node / leaf visits a lane makes before its warp hands idle lanes new rays.
+constexpr int kStepBudget = 16;
+
+// Persistent traversal warps with dynamic ray fetch: a lane whose ray has
+// ended takes the next one from the stage's work counter (one atomic per warp
+// for all idle lanes) after at most kStepBudget visits of the other lanes, so
+// lanes do not idle until the warp's longest ray ends. The loop exits are
+// warp-uniform, so the full-mask warp votes are safe.
+template<typename Traversal, typename Begin, typename Step>
+RB_D void persistentTraversal(uint32_t n, uint32_t* workCounter, Begin&& begin, Step&& step)
+{
+	const uint32_t lane = threadIdx.x & 31u;
+	bool active = false, exhausted = false;
+	for (;;)
+	{
+		const uint32_t idle = __ballot_sync(0xFFFFFFFFu, !active);
+		if (idle && !exhausted)
+		{
+			const int leader = __ffs(idle) - 1;
+			uint32_t base = 0;
+			if (lane == static_cast<uint32_t>(leader)) base = atomicAdd(workCounter, __popc(idle));
+			base = __shfl_sync(0xFFFFFFFFu, base, leader);
+			if (base + __popc(idle) >= n) exhausted = true;
+			if (!active)
+			{
+				const uint32_t idx = base + __popc(idle & ((1u << lane) - 1u));
+				if (idx < n)
+				{
+					begin(idx);
+					active = true;
+				}
+			}
+		}
+		if (__all_sync(0xFFFFFFFFu, !active)) break;
+		if (active && step()) active = false;
+	}
+}
+
 // counters (COUNT only): [0] rays, [1] nodes, [2] triangles.
 template<bool COUNT>
 __global__ void __launch_bounds__(kThreads) kExtend(DevScene sc, PathSoA s, int bounce, unsigned long long* counters)
@@ -22,14 +60,22 @@ __global__ void __launch_bounds__(kThreads) kExtend(DevScene sc, PathSoA s, int 
 	const uint32_t n = s.counts[bounce];
 	const uint32_t* q = s.queue[bounce & 1];
 	uint32_t rays = 0, nodes = 0, tris = 0;
-	for (uint32_t i = gtid(); i < n; i += gstride())
-	{
-		const uint32_t p = q[i];
-		const float4 o = s.rayO[p], d = s.rayD[p];
-		const Hit h = traceClosestT<COUNT>(sc.geo, f3_of(o), f3_of(d), 0.0f, FLT_MAX, sc.status, nodes, tris);
-		s.hit[p] = make_float4(__int_as_float(h.tri), h.t, h.b1, h.b2);
-		++rays;
-	}
+	uint32_t p = 0;
+	ClosestTraversal tr;
+	uint32_t stackRef[kTraversalStack];
+	float stackT[kTraversalStack];
+	persistentTraversal<ClosestTraversal>(n, s.counts + kExtendFetch + bounce,
+		[&](uint32_t idx) {
+			p = q[idx];
+			const float4 o = s.rayO[p], d = s.rayD[p];
+			tr.init(sc.geo, f3_of(o), f3_of(d), 0.0f, FLT_MAX);
+			++rays;
+		},
+		[&]() {
+			if (!tr.template run<COUNT>(sc.geo, kStepBudget, sc.status, nodes, tris, stackRef, stackT)) return false;
+			s.hit[p] = make_float4(__int_as_float(tr.best.tri), tr.best.t, tr.best.b1, tr.best.b2);
+			return true;
+		});
 	if (COUNT)
 	{
 		warpAdd(counters + 0, rays);
@@ -38,24 +84,31 @@ __global__ void __launch_bounds__(kThreads) kExtend(DevScene sc, PathSoA s, int 
 	}
 }
 
-
 template<bool COUNT>
 __global__ void __launch_bounds__(kThreads) kShadow(DevScene sc, PathSoA s, int bounce, unsigned long long* counters)
 {
 	const uint32_t n = s.counts[kShadowCounts + bounce];
 	uint32_t rays = 0, nodes = 0, tris = 0;
-	for (uint32_t i = gtid(); i < n; i += gstride())
-	{
-		const uint32_t p = s.shadowQueue[i];
-		const float4 o = s.shO[p], d = s.shD[p];
-		if (!traceAnyT<COUNT>(sc.geo, f3_of(o), f3_of(d), 0.0f, o.w, sc.status, nodes, tris))
-		{
-			S4 L = s4(s.L[p]);
-			L += s4(s.shC[p]);
-			s.L[p] = f4(L);
-		}
-		++rays;
-	}
+	uint32_t p = 0;
+	AnyTraversal tr;
+	uint32_t stack[kTraversalStack];
+	persistentTraversal<AnyTraversal>(n, s.counts + kShadowFetch + bounce,
+		[&](uint32_t idx) {
+			p = s.shadowQueue[idx];
+			const float4 o = s.shO[p], d = s.shD[p];
+			tr.init(sc.geo, f3_of(o), f3_of(d), 0.0f, o.w);
+			++rays;
+		},
+		[&]() {
+			if (!tr.template run<COUNT>(sc.geo, kStepBudget, sc.status, nodes, tris, stack)) return false;
+			if (!tr.hit)
+			{
+				S4 L = s4(s.L[p]);
+				L += s4(s.shC[p]);
+				s.L[p] = f4(L);
+			}
+			return true;
+		});
 	if (COUNT)
 	{
 		warpAdd(counters + 3, rays);
@@ -63,7 +116,6 @@ __global__ void __launch_bounds__(kThreads) kShadow(DevScene sc, PathSoA s, int 
 		warpAdd(counters + 5, tris);
 	}
 }
-
 
 // Closest hit returned in the reference's 24-word payload layout.
 __global__ void kTrace(DevScene sc, uint32_t n, const float* rays, uint32_t* payload, float* tOut, int32_t* triOut)

@@ -40,10 +40,14 @@ struct PathSoA
 };
 constexpr int kMaxBounces = 64;
 // counts[b]: paths entering bounce b; counts[kShadowCounts + b]: shadow rays
-// of bounce b; counts[kSurfaceCounts + b]: surface records of bounce b.
+// of bounce b; counts[kSurfaceCounts + b]: surface records of bounce b;
+// counts[kExtendFetch + b], counts[kShadowFetch + b]: work counters from
+// which the persistent traversal warps take their next rays.
 constexpr uint32_t kShadowCounts = kMaxBounces + 1;
 constexpr uint32_t kSurfaceCounts = 2 * (kMaxBounces + 1);
-constexpr uint32_t kCountSlots = 3 * (kMaxBounces + 1);
+constexpr uint32_t kExtendFetch = 3 * (kMaxBounces + 1);
+constexpr uint32_t kShadowFetch = 4 * (kMaxBounces + 1);
+constexpr uint32_t kCountSlots = 5 * (kMaxBounces + 1);
 
 struct WaveParams
 {
