@@ -268,6 +268,21 @@ __global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, Wa
 	if (gtid() == 0) s.counts[0] = w.paths;
 }
 
+// Minimum resident blocks per SM requested for the shading kernels, which
+// caps their registers per thread (65536 / (128 x blocks)): 85, 64 and 102.
+// These kernels are latency-bound, and on B200 (at-scale frame) the extra
+// warps outweigh the few spilled bytes: surface -8%, light sample -6%,
+// BxDF -10% against the compiler's own choice.
+#ifndef RB_SURFACE_MIN_BLOCKS
+#define RB_SURFACE_MIN_BLOCKS 6
+#endif
+#ifndef RB_NEE_MIN_BLOCKS
+#define RB_NEE_MIN_BLOCKS 8
+#endif
+#ifndef RB_BSDF_MIN_BLOCKS
+#define RB_BSDF_MIN_BLOCKS 5
+#endif
+
 // Surface-record bits (PathSoA::sfPi.w).
 constexpr uint32_t kSfBackHit = 1u << 0;
 constexpr uint32_t kSfSkipped = 1u << 1;
@@ -285,7 +300,7 @@ RB_D Qrng pathQrng(const DevScene& sc, const WaveParams& w, uint32_t p, uint32_t
 // continue get a surface record and join the surface queue, which the light
 // sampling and BxDF stages read.
 // counters (optional): [6] surface records.
-__global__ void __launch_bounds__(kThreads) kSurface(DevScene sc, PathSoA s, WaveParams w, int bounce,
+__global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevScene sc, PathSoA s, WaveParams w, int bounce,
 	unsigned long long* counters)
 {
 	const uint32_t n = s.counts[bounce];
@@ -379,7 +394,7 @@ __global__ void __launch_bounds__(kThreads) kSurface(DevScene sc, PathSoA s, Wav
 // surface that is not skipped: pick a light from the light tree (held in the
 // read-only cache: it is read by every thread) or the environment, sample a
 // point on it and write the shadow ray and the light sample.
-__global__ void __launch_bounds__(kThreads) kNee(DevScene sc, PathSoA s, WaveParams w, int bounce)
+__global__ void __launch_bounds__(kThreads, RB_NEE_MIN_BLOCKS) kNee(DevScene sc, PathSoA s, WaveParams w, int bounce)
 {
 	const uint32_t n = s.counts[kSurfaceCounts + bounce];
 	const TreeNodeU* nodes = sc.lights.unpacked;
@@ -462,7 +477,7 @@ __global__ void __launch_bounds__(kThreads) kNee(DevScene sc, PathSoA s, WavePar
 // (pathtrace.cu:1724-1733), Russian roulette, the next ray and the depth
 // limits (:1736-1785). Continuing paths go to the next extend queue, light
 // samples that passed to the shadow queue.
-__global__ void __launch_bounds__(kThreads) kBsdf(DevScene sc, PathSoA s, WaveParams w, int bounce)
+__global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(DevScene sc, PathSoA s, WaveParams w, int bounce)
 {
 	const uint32_t n = s.counts[kSurfaceCounts + bounce];
 	uint32_t* nextQueue = s.queue[(bounce + 1) & 1];

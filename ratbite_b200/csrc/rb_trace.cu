@@ -15,8 +15,12 @@ namespace rb
 {
 namespace
 {
-// Node / leaf visits a lane makes before its warp hands idle lanes new rays.
-constexpr int kStepBudget = 16;
+// Node / leaf visits a lane makes before its warp hands idle lanes new rays
+// (on B200, at-scale frame: 16 beats 8 and 32).
+#ifndef RB_STEP_BUDGET
+#define RB_STEP_BUDGET 16
+#endif
+constexpr int kStepBudget = RB_STEP_BUDGET;
 
 // Persistent traversal warps with dynamic ray fetch: a lane whose ray has
 // ended takes the next one from the stage's work counter (one atomic per warp
