@@ -269,10 +269,10 @@ __global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, Wa
 }
 
 // Minimum resident blocks per SM requested for the shading kernels, which
-// caps their registers per thread (65536 / (128 x blocks)): 85, 64 and 102.
+// caps their registers per thread (65536 / (128 x blocks)): 85, 64 and 85.
 // These kernels are latency-bound, and on B200 (at-scale frame) the extra
 // warps outweigh the few spilled bytes: surface -8%, light sample -6%,
-// BxDF -10% against the compiler's own choice.
+// BxDF -18% against the compiler's own choice.
 #ifndef RB_SURFACE_MIN_BLOCKS
 #define RB_SURFACE_MIN_BLOCKS 6
 #endif
@@ -280,8 +280,16 @@ __global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, Wa
 #define RB_NEE_MIN_BLOCKS 8
 #endif
 #ifndef RB_BSDF_MIN_BLOCKS
-#define RB_BSDF_MIN_BLOCKS 5
+#define RB_BSDF_MIN_BLOCKS 6
 #endif
+
+// Block size of the shared-memory light-sample kernel: two blocks of 512
+// per SM hold two copies of a tree of up to kNeeSharedMaxBytes.
+#ifndef RB_NEE_SHARED_MAX_BYTES
+#define RB_NEE_SHARED_MAX_BYTES (100u * 1024u)
+#endif
+constexpr int kNeeSharedThreads = 512;
+constexpr uint32_t kNeeSharedMaxBytes = RB_NEE_SHARED_MAX_BYTES;
 
 // Surface-record bits (PathSoA::sfPi.w).
 constexpr uint32_t kSfBackHit = 1u << 0;
@@ -394,10 +402,23 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 // surface that is not skipped: pick a light from the light tree (held in the
 // read-only cache: it is read by every thread) or the environment, sample a
 // point on it and write the shadow ray and the light sample.
-__global__ void __launch_bounds__(kThreads, RB_NEE_MIN_BLOCKS) kNee(DevScene sc, PathSoA s, WaveParams w, int bounce)
+// SHARED: the block first copies the unpacked tree into shared memory
+// (dynamic, nodeCount x 48 B) and descends it there; used when the tree fits.
+template<bool SHARED>
+__global__ void __launch_bounds__(SHARED ? kNeeSharedThreads : kThreads, SHARED ? 2 : RB_NEE_MIN_BLOCKS)
+kNee(DevScene sc, PathSoA s, WaveParams w, int bounce)
 {
+	extern __shared__ float4 sharedTree[];
 	const uint32_t n = s.counts[kSurfaceCounts + bounce];
 	const TreeNodeU* nodes = sc.lights.unpacked;
+	if (SHARED)
+	{
+		const float4* src = reinterpret_cast<const float4*>(sc.lights.unpacked);
+		const uint32_t words = 3u * sc.lights.nodeCount;
+		for (uint32_t k = threadIdx.x; k < words; k += blockDim.x) sharedTree[k] = __ldg(src + k);
+		__syncthreads();
+		nodes = reinterpret_cast<const TreeNodeU*>(sharedTree);
+	}
 	const bool envPresent = sc.env.enabled != 0;
 	const bool treePresent = sc.lights.nodes != nullptr;
 	for (uint32_t i = gtid(); i < n; i += gstride())
@@ -426,7 +447,7 @@ __global__ void __launch_bounds__(kThreads, RB_NEE_MIN_BLOCKS) kNee(DevScene sc,
 			const S4 lambda = s4(s.lambda[p]);
 			uint32_t type = 0, index = 0;
 			float treePdf = 0.0f, lightPdf = 0.0f;
-			lightTreeSample(sc, nodes, r.z, hitPos, sn, type, index, treePdf);
+			lightTreeSample<SHARED>(sc, nodes, r.z, hitPos, sn, type, index, treePdf);
 			if (type == kLightTypeTriangle)
 			{
 				const EmissiveTri& et = sc.lights.triangles[index];
@@ -771,7 +792,9 @@ LaunchShape queryLaunchShape()
 	ls.threads = kThreads;
 	ls.blocksGenerate = occ(reinterpret_cast<const void*>(kGenerate));
 	ls.blocksSurface = occ(reinterpret_cast<const void*>(kSurface));
-	ls.blocksNee = occ(reinterpret_cast<const void*>(kNee));
+	ls.blocksNee = occ(reinterpret_cast<const void*>(kNee<false>));
+	cudaFuncSetAttribute(reinterpret_cast<const void*>(kNee<true>), cudaFuncAttributeMaxDynamicSharedMemorySize,
+		static_cast<int>(kNeeSharedMaxBytes));
 	ls.blocksBsdf = occ(reinterpret_cast<const void*>(kBsdf));
 	ls.blocksResolve = occ(reinterpret_cast<const void*>(kResolve));
 	queryTraceShape(ls);
@@ -789,7 +812,18 @@ void launchSurface(const DevScene& sc, const PathSoA& s, const WaveParams& w, in
 }
 void launchNee(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
 {
-	kNee<<<ls.blocksNee, kThreads, 0, st>>>(sc, s, w, bounce);
+	const size_t treeBytes = sizeof(TreeNodeU) * sc.lights.nodeCount;
+	if (sc.lights.unpacked && treeBytes <= kNeeSharedMaxBytes)
+	{
+		int b = 0;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, reinterpret_cast<const void*>(kNee<true>), kNeeSharedThreads,
+			treeBytes);
+		kNee<true><<<(b < 1 ? 1 : b) * ls.smCount, kNeeSharedThreads, treeBytes, st>>>(sc, s, w, bounce);
+	}
+	else
+	{
+		kNee<false><<<ls.blocksNee, kThreads, 0, st>>>(sc, s, w, bounce);
+	}
 }
 void launchBsdf(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
 {

@@ -229,8 +229,12 @@ RB_D TreeNodeU makeNodeU(const PackedNode* nodes, uint32_t i)
 RB_D bool nodeLeaf(const TreeNodeU& u) { return (__float_as_uint(u.fluxInt.w) >> 31) != 0u; }
 RB_D uint32_t nodeA(const TreeNodeU& u) { return __float_as_uint(u.fluxInt.z); }
 RB_D uint32_t nodeB(const TreeNodeU& u) { return __float_as_uint(u.fluxInt.w) & 0x7FFFFFFFu; }
+// Node load from global memory through the read-only cache, or (SHARED)
+// from a copy of the tree in shared memory.
+template<bool SHARED = false>
 RB_D TreeNodeU loadNodeU(const TreeNodeU* nodes, uint32_t i)
 {
+	if (SHARED) return nodes[i];
 	TreeNodeU u;
 	u.meanVar = __ldg(&nodes[i].meanVar);
 	u.dirSharp = __ldg(&nodes[i].dirSharp);
@@ -280,6 +284,7 @@ RB_D float lightTreePdf(const DevScene& sc, uint32_t type, uint32_t index, f3 p,
 // sampleLightTree: pick the environment (0.3 when both exist) or descend the
 // tree choosing children by importance with rescaled `rand`. `nodes` is the
 // unpacked tree in shared or global memory.
+template<bool SHARED = false>
 RB_D void lightTreeSample(const DevScene& sc, const TreeNodeU* nodes, float rand, f3 p, f3 nrm, uint32_t& type,
 	uint32_t& index, float& pdf)
 {
@@ -294,11 +299,11 @@ RB_D void lightTreeSample(const DevScene& sc, const TreeNodeU* nodes, float rand
 	rand = clampf((rand - envImp) / (1.0f - envImp), 0.0f, 1.0f);
 	pdf = 1.0f - envImp;
 	uint32_t cur = 0;
-	TreeNodeU node = loadNodeU(nodes, 0);
+	TreeNodeU node = loadNodeU<SHARED>(nodes, 0);
 	while (!nodeLeaf(node))
 	{
-		const TreeNodeU l = loadNodeU(nodes, cur + 1);
-		const TreeNodeU r = loadNodeU(nodes, nodeA(node));
+		const TreeNodeU l = loadNodeU<SHARED>(nodes, cur + 1);
+		const TreeNodeU r = loadNodeU<SHARED>(nodes, nodeA(node));
 		const float li = nodeImportanceU(l, p, nrm);
 		const float ri = nodeImportanceU(r, p, nrm);
 		const float sep = li / (li + ri);
