@@ -220,7 +220,7 @@ def run_reference(args, rank: int, world: int, wl: dict):
 # ---------------------------------------------------------------- our arm
 def run_ours(args, rank: int, world: int, wl: dict):
     import torch
-    from ratbite_b200 import abi, lighttree
+    from ratbite_b200 import abi, lighttree, multigpu
     from ratbite_b200.rendering_interface import RenderingInterface
 
     W, H, SPP = wl["width"], wl["height"], wl["spp"]
@@ -245,16 +245,15 @@ def run_ours(args, rank: int, world: int, wl: dict):
     sp = stream.cuda_stream
     launch = scene.launch_record()
     accum_dev = torch.zeros((H, W, 4), dtype=torch.float64, device="cuda") if world > 1 else None
-    offset = rank * SPP                     # disjoint Sobol sample range per rank
+    offset, _ = multigpu.weak_sample_range(SPP, rank)   # disjoint Sobol sample range per rank
 
-    def step(s=sp):
+    def step():
         if has_env:
-            ri.rebuild_environment_cdf(stream=s)
-        ri.render(offset, SPP, stream=s)
+            ri.rebuild_environment_cdf(stream=sp)
         if world > 1:
-            ri.copy_accumulation_async(accum_dev.data_ptr(), stream=s)
-            with torch.cuda.stream(stream):
-                dist.all_reduce(accum_dev)
+            multigpu.render_frame(ri, accum_dev, offset, SPP, stream=stream)
+        else:
+            ri.render(offset, SPP, stream=sp)
 
     # traversal work counts (untimed): nodes / triangles per extension and shadow ray
     ri.set_stats(abi.RB_STATS_COUNT)
@@ -298,7 +297,7 @@ def run_ours(args, rank: int, world: int, wl: dict):
         ri.prepare_data_for_rendering(launch)            # H2D: launch parameters
         if has_env:
             ri.rebuild_environment_cdf()
-        ri.render(offset, SPP)
+        multigpu.render_range(ri, offset, SPP)
         host = ri.read_accumulation()                    # D2H: FP64 accumulation
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0

@@ -261,6 +261,11 @@ int rb_accum_device_ptr(rb_ctx* ctx, void** out);
 /* Stream-ordered copy of the accumulation buffer to `dst` (device or pinned
  * host memory, width*height*4 doubles), on `stream` (NULL: context stream). */
 int rb_copy_accum_async(rb_ctx* ctx, void* dst, void* stream);
+/* Zeroes the accumulation buffer, stream-ordered. No reference counterpart
+ * (the reference restarts only through sample_offset == 0): a rank that
+ * renders its own sample range [offset, offset + count) of a frame with
+ * offset > 0 starts its frame with this call. */
+int rb_clear_accum(rb_ctx* ctx, void* stream);
 int rb_status(rb_ctx* ctx, rb_device_status* out);
 int rb_clear_status(rb_ctx* ctx);
 int rb_synchronize(rb_ctx* ctx);

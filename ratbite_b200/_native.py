@@ -37,6 +37,7 @@ SIGNATURES = {
     "rb_read_accum": (C.c_int, [_P, _P]),
     "rb_accum_device_ptr": (C.c_int, [_P, C.POINTER(_P)]),
     "rb_copy_accum_async": (C.c_int, [_P, _P, _P]),
+    "rb_clear_accum": (C.c_int, [_P, _P]),
     "rb_status": (C.c_int, [_P, C.POINTER(abi.rb_device_status)]),
     "rb_clear_status": (C.c_int, [_P]),
     "rb_synchronize": (C.c_int, [_P]),

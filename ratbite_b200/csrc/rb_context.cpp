@@ -691,6 +691,15 @@ int rb_copy_accum_async(rb_ctx* ctx, void* dst, void* stream)
 	return e == cudaSuccess ? RB_OK : cudaFail(ctx, e, "rb_copy_accum_async");
 }
 
+int rb_clear_accum(rb_ctx* ctx, void* stream)
+{
+	if (!ctx) return RB_ERR_INVALID;
+	if (!ctx->accum) return fail(ctx, RB_ERR_NO_SCENE, "rb_clear_accum: no accumulation buffer");
+	cudaSetDevice(ctx->device);
+	const cudaError_t e = cudaMemsetAsync(ctx->accum, 0, sizeof(double4) * ctx->accumPixels, pick(ctx, stream));
+	return e == cudaSuccess ? RB_OK : cudaFail(ctx, e, "rb_clear_accum");
+}
+
 int rb_status(rb_ctx* ctx, rb_device_status* out)
 {
 	if (!ctx || !out) return RB_ERR_INVALID;

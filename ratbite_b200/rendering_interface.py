@@ -137,6 +137,11 @@ class RenderingInterface:
         s = None if stream is None else C.c_void_p(stream)
         check(self.lib.rb_copy_accum_async(self.ctx, C.c_void_p(dst_ptr), s), self.ctx, "rb_copy_accum_async")
 
+    def clear_accumulation(self, stream=None):
+        """Zeroes the FP64 accumulation (stream-ordered)."""
+        s = None if stream is None else C.c_void_p(stream)
+        check(self.lib.rb_clear_accum(self.ctx, s), self.ctx, "rb_clear_accum")
+
     def accumulation_device_ptr(self) -> int:
         p = C.c_void_p()
         check(self.lib.rb_accum_device_ptr(self.ctx, C.byref(p)), self.ctx, "rb_accum_device_ptr")
