@@ -261,6 +261,21 @@ int rb_accum_device_ptr(rb_ctx* ctx, void** out);
 /* Stream-ordered copy of the accumulation buffer to `dst` (device or pinned
  * host memory, width*height*4 doubles), on `stream` (NULL: context stream). */
 int rb_copy_accum_async(rb_ctx* ctx, void* dst, void* stream);
+/* ---- resolve (replaces resolveRender, src/core/rendering_interface.cpp
+ * :1512-1532, and the GL image it writes) -------------------------------- */
+/* Resolves the accumulation into the context's headless image: per pixel
+ * sum/count, max(., 0) * exposure_scale, the XYZ -> RGB `colorspace` matrix
+ * (9 floats, column-major as glm::mat3; Color::generateColorspaceConversionMatrix,
+ * src/core/color.h:60-99), the AgX tonemap and 8-bit quantisation
+ * (renderResolve + tonemap, src/kernels/image.cu:16-121). The reference passes
+ * exposure_scale = 2^(exposure - 7). The image is width*height RGBA8, row-major,
+ * owned by the context; stream-ordered on `stream` (NULL: context stream). */
+int rb_resolve(rb_ctx* ctx, const float colorspace[9], float exposure_scale, void* stream);
+/* Copies the width*height*4 bytes of the resolved image to host memory;
+ * synchronizes. */
+int rb_read_image(rb_ctx* ctx, uint8_t* out);
+/* Device pointer of the resolved image (width*height RGBA8 words). */
+int rb_image_device_ptr(rb_ctx* ctx, void** out);
 /* Zeroes the accumulation buffer, stream-ordered. No reference counterpart
  * (the reference restarts only through sample_offset == 0): a rank that
  * renders its own sample range [offset, offset + count) of a frame with

@@ -105,6 +105,13 @@ int rb_k_trace(rb_ctx* ctx, uint32_t n, const float* rays, uint32_t* payload24,
 int rb_k_occluded(rb_ctx* ctx, uint32_t n, const float* rays, const float* tmax,
                   uint32_t* out, void* stream);
 
+/* renderResolve + AgX tonemap (src/kernels/image.cu:16-121) over a caller
+ * buffer: render_data is width*height double4 (sum X, Y, Z, count) in device
+ * memory, out_rgba width*height RGBA8 in device memory (row-major), colorspace
+ * 9 floats in host memory (column-major XYZ -> RGB). */
+int rb_k_resolve(uint32_t width, uint32_t height, const float* colorspace, float exposure_scale,
+                 const double* render_data, uint8_t* out_rgba, void* stream);
+
 /* Environment-map 2D CDF (src/kernels/cdf.cu:332-535), in device memory:
  * rgba is w*h float4; outputs the inverted conditional (w*h) and marginal
  * (h) uint16 index tables and the integral divided by w*h, as

@@ -19,6 +19,7 @@
 #include "_ref/src/core/light_tree.h"
 #include "_ref/src/core/scene.h"
 #include "_ref/src/core/spectral.h"
+#include "_ref/src/core/color.h"
 
 #include "../include/ratbite_b200.h"
 #include "../include/ratbite_b200_kernels.h"
@@ -748,6 +749,17 @@ int rbref_build_light_tree(uint32_t n, const float* worldVerts, const float* flu
 	const int count = tree.nodeCount;
 	tree.clear();
 	return count;
+}
+
+// Color::generateColorspaceConversionMatrix (src/core/color.h:60-99): the
+// XYZ -> RGB matrix of colorspace `cs` (0 sRGB, 1 DCI-P3, 2 Rec.2020) with the
+// D65 white point from the reference's own illuminant spectrum; out is
+// column-major (glm::mat3).
+void rbref_colorspace_matrix(int cs, float* out)
+{
+	const glm::mat3 m = Color::generateColorspaceConversionMatrix(static_cast<Color::RGBColorspace>(cs));
+	for (int c = 0; c < 3; ++c)
+		for (int r = 0; r < 3; ++r) out[3 * c + r] = m[c][r];
 }
 
 uint32_t rbref_sizeof_material_data() { return sizeof(MaterialData); }

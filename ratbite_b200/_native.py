@@ -38,6 +38,9 @@ SIGNATURES = {
     "rb_accum_device_ptr": (C.c_int, [_P, C.POINTER(_P)]),
     "rb_copy_accum_async": (C.c_int, [_P, _P, _P]),
     "rb_clear_accum": (C.c_int, [_P, _P]),
+    "rb_resolve": (C.c_int, [_P, _P, C.c_float, _P]),
+    "rb_read_image": (C.c_int, [_P, _P]),
+    "rb_image_device_ptr": (C.c_int, [_P, C.POINTER(_P)]),
     "rb_status": (C.c_int, [_P, C.POINTER(abi.rb_device_status)]),
     "rb_clear_status": (C.c_int, [_P]),
     "rb_synchronize": (C.c_int, [_P]),
@@ -54,6 +57,7 @@ SIGNATURES = {
     "rb_k_oct_decode": (C.c_int, [_U32, _P, _P, _P]),
     "rb_k_trace": (C.c_int, [_P, _U32, _P, _P, _P, _P, _P]),
     "rb_k_occluded": (C.c_int, [_P, _U32, _P, _P, _P, _P]),
+    "rb_k_resolve": (C.c_int, [_U32, _U32, _P, C.c_float, _P, _P, _P]),
     "rb_envmap_cdf_scratch_bytes": (C.c_size_t, [_U32, _U32]),
     "rb_envmap_cdf": (C.c_int, [_U32, _U32, _P, C.c_int, _P, _P, _P, _P, _P]),
     "rb_envmap_cdf_noalloc": (C.c_int, [_U32, _U32, _P, C.c_int, _P, _P, _P, _P]),

@@ -44,6 +44,8 @@ struct rb_ctx
 	float* envIntegral = nullptr;               // device scalar (in envBufs)
 	double4* accum = nullptr;
 	size_t accumPixels = 0;
+	uint32_t* image = nullptr;                  // resolved RGBA8 (rb_resolve)
+	size_t imagePixels = 0;
 	bool haveLaunch = false, haveGeometry = false;
 	uint64_t pathsTraced = 0;
 	// cross-table references checked before any kernel reads them
@@ -259,6 +261,7 @@ int rb_destroy(rb_ctx* ctx)
 	for (cudaEvent_t e : ctx->eventPool) cudaEventDestroy(e);
 	if (ctx->counters) cudaFree(ctx->counters);
 	if (ctx->accum) cudaFree(ctx->accum);
+	if (ctx->image) cudaFree(ctx->image);
 	if (ctx->status) cudaFree(ctx->status);
 	if (ctx->stream) cudaStreamDestroy(ctx->stream);
 	delete ctx;
@@ -691,6 +694,46 @@ int rb_copy_accum_async(rb_ctx* ctx, void* dst, void* stream)
 	return e == cudaSuccess ? RB_OK : cudaFail(ctx, e, "rb_copy_accum_async");
 }
 
+int rb_resolve(rb_ctx* ctx, const float colorspace[9], float exposure_scale, void* stream)
+{
+	if (!ctx || !colorspace) return RB_ERR_INVALID;
+	if (!ctx->accum || !ctx->haveLaunch) return fail(ctx, RB_ERR_NO_SCENE, "rb_resolve: nothing rendered");
+	cudaSetDevice(ctx->device);
+	const cudaStream_t st = pick(ctx, stream);
+	if (ctx->imagePixels != ctx->accumPixels)
+	{
+		cudaStreamSynchronize(st);
+		cudaStreamSynchronize(ctx->stream);
+		if (ctx->image) cudaFree(ctx->image);
+		ctx->image = nullptr;
+		ctx->imagePixels = 0;
+		const cudaError_t e = cudaMalloc(&ctx->image, sizeof(uint32_t) * ctx->accumPixels);
+		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_resolve: image buffer");
+		ctx->imagePixels = ctx->accumPixels;
+	}
+	rb::launchResolveImage(ctx->scene.launch.width, ctx->scene.launch.height, colorspace, exposure_scale, ctx->accum,
+		ctx->image, ctx->shape.smCount, st);
+	const cudaError_t e = cudaGetLastError();
+	return e == cudaSuccess ? RB_OK : cudaFail(ctx, e, "rb_resolve");
+}
+
+int rb_read_image(rb_ctx* ctx, uint8_t* out)
+{
+	if (!ctx || !out) return RB_ERR_INVALID;
+	if (!ctx->image) return fail(ctx, RB_ERR_NO_SCENE, "rb_read_image: nothing resolved");
+	cudaSetDevice(ctx->device);
+	cudaError_t e = cudaDeviceSynchronize();
+	if (e == cudaSuccess) e = cudaMemcpy(out, ctx->image, sizeof(uint32_t) * ctx->imagePixels, cudaMemcpyDeviceToHost);
+	return e == cudaSuccess ? RB_OK : cudaFail(ctx, e, "rb_read_image");
+}
+
+int rb_image_device_ptr(rb_ctx* ctx, void** out)
+{
+	if (!ctx || !out) return RB_ERR_INVALID;
+	*out = ctx->image;
+	return ctx->image ? RB_OK : fail(ctx, RB_ERR_NO_SCENE, "no resolved image");
+}
+
 int rb_clear_accum(rb_ctx* ctx, void* stream)
 {
 	if (!ctx) return RB_ERR_INVALID;
@@ -834,6 +877,19 @@ int rb_k_light_tree(rb_ctx* ctx, uint32_t n, rb_light_case* cases, void* stream)
 	if (n == 0) return RB_OK;
 	RB_K_CHECK(cases);
 	rb::launchLightCases(ctx->scene, n, cases, pick(ctx, stream));
+	return lastLaunch();
+}
+int rb_k_resolve(uint32_t width, uint32_t height, const float* colorspace, float exposure_scale,
+	const double* render_data, uint8_t* out_rgba, void* stream)
+{
+	if (width == 0 || height == 0) return RB_OK;
+	RB_K_CHECK(colorspace && render_data && out_rgba);
+	RB_K_CHECK(static_cast<uint64_t>(width) * height <= (1ull << 31));
+	int dev = 0, sms = 0;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	rb::launchResolveImage(width, height, colorspace, exposure_scale, reinterpret_cast<const double4*>(render_data),
+		reinterpret_cast<uint32_t*>(out_rgba), sms, static_cast<cudaStream_t>(stream));
 	return lastLaunch();
 }
 int rb_k_offset_point(uint32_t n, const float* p, const float* nrm, float* out, void* stream)

@@ -75,6 +75,10 @@ void launchSurface(const DevScene& sc, const PathSoA& s, const WaveParams& w, in
 	unsigned long long* counters);
 void launchNee(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st);
 void launchBsdf(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st);
+// Resolve + AgX tonemap of the accumulation into width*height RGBA8 words
+// (rb_image.cu); colorspace: 9 floats, column-major XYZ -> RGB.
+void launchResolveImage(uint32_t width, uint32_t height, const float* colorspace, float exposureScale,
+	const double4* data, uint32_t* out, int smCount, cudaStream_t st);
 void launchUnpackLightTree(const PackedNode* in, TreeNodeU* out, uint32_t n, cudaStream_t st);
 void queryTraceShape(LaunchShape& ls);   // fills blocksExtend, blocksShadow (rb_trace.cu)
 void launchShadow(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,

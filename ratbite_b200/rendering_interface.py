@@ -137,6 +137,23 @@ class RenderingInterface:
         s = None if stream is None else C.c_void_p(stream)
         check(self.lib.rb_copy_accum_async(self.ctx, C.c_void_p(dst_ptr), s), self.ctx, "rb_copy_accum_async")
 
+    def resolve(self, exposure: float = 0.0, colorspace=None, stream=None):
+        """Resolves the accumulation into the headless RGBA8 image (stream-ordered):
+        AgX tonemap with exposure scale 2^(exposure - 7), as the reference's
+        resolveRender. `colorspace`: 9 floats, column-major XYZ -> RGB (default sRGB)."""
+        from .color import colorspace_matrix
+        cs = colorspace_matrix("sRGB") if colorspace is None else np.ascontiguousarray(colorspace, np.float32)
+        if cs.size != 9:
+            raise ValueError("colorspace must hold 9 floats")
+        s = None if stream is None else C.c_void_p(stream)
+        check(self.lib.rb_resolve(self.ctx, _ptr(cs), float(2.0 ** (exposure - 7.0)), s), self.ctx, "rb_resolve")
+
+    def read_image(self) -> np.ndarray:
+        """The resolved image as an (H, W, 4) uint8 array (synchronizes)."""
+        out = np.zeros((self.height, self.width, 4), np.uint8)
+        check(self.lib.rb_read_image(self.ctx, _ptr(out)), self.ctx, "rb_read_image")
+        return out
+
     def clear_accumulation(self, stream=None):
         """Zeroes the FP64 accumulation (stream-ordered)."""
         s = None if stream is None else C.c_void_p(stream)

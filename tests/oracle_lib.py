@@ -67,6 +67,7 @@ class RefLib:
             ("rbref_trace", None, [_U32, _P, _P, _P, _P]),
             ("rbref_occluded", None, [_U32, _P, _P, _P]),
             ("rbref_build_light_tree", C.c_int, [_U32, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+            ("rbref_colorspace_matrix", None, [C.c_int, _P]),
             ("rbref_sizeof_material_data", _U32, []),
             ("rbref_sizeof_launch_parameters", _U32, []),
         ]:
@@ -196,3 +197,22 @@ def ref_render(ref: RefLib, width: int, height: int, offset: int, count: int, th
     out = np.zeros((height, width, 4), np.float64)
     ref.lib.rbref_read_accum(_np_ptr(out))
     return out
+
+
+class RefImageGpu:
+    """The reference's resolve kernel (src/kernels/image.cu) on the GPU,
+    through oracle/ref_image_harness.cpp (checker only)."""
+
+    def __init__(self):
+        self.cubin = str(REF_DIR / "image.cubin").encode()
+        self.lib = C.CDLL(str(REF_DIR / "libratbite_ref_image.so"))
+        self.lib.rbrefgpu_resolve.argtypes = [C.c_char_p, _U32, _U32, _P, C.c_float, _P, _P]
+        self.lib.rbrefgpu_resolve.restype = C.c_int
+
+    def resolve(self, width: int, height: int, colorspace: np.ndarray, exposure_scale: float, d_render: int):
+        out = np.zeros((height, width, 4), np.uint8)
+        cs = np.ascontiguousarray(colorspace, np.float32)
+        rc = self.lib.rbrefgpu_resolve(self.cubin, width, height, _np_ptr(cs), exposure_scale, d_render,
+                                       _np_ptr(out))
+        assert rc == 0, rc
+        return out

@@ -247,3 +247,25 @@ def test_light_tree_builder_rejects_bad_input():
     flux[1] = 0.0
     with pytest.raises(NativeError):
         lighttree.build(world, flux, mat, prim)
+
+
+# --------------------------------------------------------------- resolve
+@pytest.mark.parametrize("cs,name", [(0, "sRGB"), (1, "DCI_P3"), (2, "Rec2020")])
+def test_colorspace_matrix_matches_reference(ref, cs, name):
+    from ratbite_b200 import color
+    want = np.zeros(9, np.float32)
+    ref.lib.rbref_colorspace_matrix(cs, want.ctypes.data)
+    # with the reference's white point (from its D65 spectrum) the restatement agrees to float rounding
+    got = color.colorspace_matrix(name, white_xyz=color.white_of(want))
+    np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-6)
+    # the default white point (CIE D65 chromaticity) is within 2e-3
+    np.testing.assert_allclose(color.colorspace_matrix(name), want, rtol=2e-3, atol=2e-3)
+
+
+def test_png_round_trip(tmp_path):
+    from ratbite_b200 import image_io
+    img = (np.random.default_rng(3).random((9, 13, 4)) * 256).astype(np.uint8)
+    image_io.write_png(tmp_path / "x.png", img)
+    assert np.array_equal(image_io.read_png(tmp_path / "x.png"), img)
+    with pytest.raises(ValueError):
+        image_io.write_png(tmp_path / "y.png", img[..., :3])
