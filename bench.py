@@ -339,10 +339,16 @@ def run_ours(args, rank: int, world: int, wl: dict):
         launches_total = (stages.launches_generate + stages.launches_extend + stages.launches_shade
                           + stages.launches_nee + stages.launches_bsdf + stages.launches_shadow
                           + stages.launches_resolve + (args.steps if has_env else 0))
+        # DRAM traffic of the dominant kernel per launch: ncu's dram bytes per
+        # work unit (measured on a reduced case of this workload, see
+        # profiles/traffic.json) times the units one launch processes here
+        units_step = {"extend": ext_rays, "shadow": sh_rays, "surface": ext_rays, "nee": recs, "bsdf": recs}
         traffic = None
         tp = ROOT / "profiles" / "traffic.json"
         if tp.exists():
-            traffic = json.loads(tp.read_text()).get(wl["name"], {}).get(kernel_names[dom])
+            t = json.loads(tp.read_text()).get(WORKLOADS[args.workload]["name"], {}).get(kernel_names[dom])
+            if t:
+                traffic = t["dram_bytes_per_unit"] * units_step[dom] / max(1.0, launches / args.steps)
         if args.cpu_seconds > 0:
             cpu_v, cores, sample = cpu_baseline(scene, cie, basis, luts, wl, args.cpu_seconds)
         else:

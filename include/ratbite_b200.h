@@ -45,6 +45,7 @@ extern "C" {
 #define RB_DEV_NAN_RADIANCE     (1u << 2)  /* a path produced a non-finite sample */
 #define RB_DEV_ITERATION_LIMIT  (1u << 3)  /* a bounded wait gave up */
 #define RB_DEV_BAD_INDEX        (1u << 4)  /* an index read from scene data was out of range */
+#define RB_DEV_BAD_GEOMETRY     (1u << 5)  /* a moved vertex is not finite (rb_update_instances) */
 
 /* Index buffer element types (IndexType, src/core/material.h:9-15). */
 #define RB_INDEX_U16 0
@@ -223,6 +224,19 @@ int rb_set_materials(rb_ctx* ctx, const rb_material* materials, uint32_t count);
  * (:849) and updateInstanceAccelerationStructure (:943): builds the wide BVH. */
 int rb_set_geometry(rb_ctx* ctx, const rb_geometry* geometry);
 /* Replaces fillLightDataBuffer / fillLightTreeDataBuffers (:1433, :1470). */
+/* Moves the instances of the last rb_set_geometry (replaces
+ * updateInstanceAccelerationStructure, src/core/rendering_interface.cpp
+ * :943-1063, run by the reference on every camera move): new camera-relative
+ * 3x4 transforms, instance_transforms[12 * instance_count] in the order of
+ * rb_geometry.instances and subset_transforms[12 * emissive_subset_count] in
+ * the order of rb_geometry.emissive_subsets. World vertices, geometric normals
+ * and the BVH boxes are recomputed on the device (the tree topology is kept),
+ * stream-ordered on `stream`; the results equal those of rb_set_geometry with
+ * the same transforms. The light data (camera-relative emissive triangles and
+ * light-tree means) is refreshed by the caller through rb_set_lights, as the
+ * reference refills it. */
+int rb_update_instances(rb_ctx* ctx, const float* instance_transforms, const float* subset_transforms,
+                        void* stream);
 int rb_set_lights(rb_ctx* ctx, const rb_light_tree* tree);
 /* Host light-tree build (LightTree::Builder, src/core/light_tree.cpp:47-418,
  * driven as RenderingInterface::buildLightTree, src/core/rendering_interface.cpp:

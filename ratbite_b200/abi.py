@@ -22,6 +22,7 @@ RB_DEV_QUEUE_OVERFLOW = 1 << 1
 RB_DEV_NAN_RADIANCE = 1 << 2
 RB_DEV_ITERATION_LIMIT = 1 << 3
 RB_DEV_BAD_INDEX = 1 << 4
+RB_DEV_BAD_GEOMETRY = 1 << 5
 
 RB_INDEX_U16 = 0
 RB_INDEX_U32 = 1

@@ -103,22 +103,28 @@ RB_D uint32_t nodeChild(const NodeView& v, int c)
 	const float w = (c & 3) == 0 ? a.x : ((c & 3) == 1 ? a.y : ((c & 3) == 2 ? a.z : a.w));
 	return __float_as_uint(w);
 }
-// Quantized byte of plane `k` (0..5: lo x,y,z, hi x,y,z) of child c, as a
-// float. The byte is placed in the mantissa of 2^23 with one byte permute and
-// 2^23 subtracted (exact), which keeps the conversion off the slower
-// conversion pipe.
-RB_D float nodeQf(const NodeView& v, int k, int c)
+// Byte c (0..7) of a child plane row held in two words, as a float: the
+// byte is placed in the mantissa of 2^23 with one byte permute and 2^23
+// subtracted (exact), which keeps the conversion off the slower conversion
+// pipe.
+RB_D float planeQ(uint32_t w0, uint32_t w1, int c)
 {
-	const int byte = k * 8 + c;                 // offset inside the 48-byte box block
-	const float4& a = v.q[3 + byte / 16];
-	const int w = (byte % 16) / 4;
-	const uint32_t word = __float_as_uint(w == 0 ? a.x : (w == 1 ? a.y : (w == 2 ? a.z : a.w)));
-	const uint32_t bits = __byte_perm(word, 0x4B000000u, static_cast<uint32_t>(byte & 3) | 0x7540u);
+	const uint32_t word = c < 4 ? w0 : w1;
+	const uint32_t bits = __byte_perm(word, 0x4B000000u, static_cast<uint32_t>(c & 3) | 0x7540u);
 	return __fsub_rn(__uint_as_float(bits), 8388608.0f);
+}
+// Word w (0..11) of the 48-byte plane block: rows of 8 bytes, lo x,y,z then hi x,y,z.
+RB_D uint32_t planeWord(const NodeView& v, int w)
+{
+	const float4& a = v.q[3 + w / 4];
+	return __float_as_uint((w & 3) == 0 ? a.x : ((w & 3) == 1 ? a.y : ((w & 3) == 2 ? a.z : a.w)));
 }
 
 // Intersects the ray with the 8 child boxes; hitMask bit c set when child c
-// is entered within [tmin, tmax]; tnear[c] is its entry distance.
+// is entered within [tmin, tmax]; tnear[c] is its entry distance. Per axis the
+// near and far plane rows are chosen once from the sign of the reciprocal
+// direction, which gives the same distances as taking the min and max of the
+// two planes per child (the rounding is monotonic).
 RB_D uint32_t childBoxes(const TraceRay& r, const NodeView& v, float tmin, float tmax, float tnear[8])
 {
 	const float ox = v.q[0].x, oy = v.q[0].y, oz = v.q[0].z;
@@ -126,6 +132,14 @@ RB_D uint32_t childBoxes(const TraceRay& r, const NodeView& v, float tmin, float
 	const float scx = __uint_as_float(((meta >> 0) & 0xFFu) << 23);
 	const float scy = __uint_as_float(((meta >> 8) & 0xFFu) << 23);
 	const float scz = __uint_as_float(((meta >> 16) & 0xFFu) << 23);
+	// rows: lo x = words 0,1; lo y = 2,3; lo z = 4,5; hi x = 6,7; hi y = 8,9; hi z = 10,11
+	const bool nx = signbit(r.ix), ny = signbit(r.iy), nz = signbit(r.iz);
+	const uint32_t lo0 = planeWord(v, 0), lo1 = planeWord(v, 1), lo2 = planeWord(v, 2), lo3 = planeWord(v, 3);
+	const uint32_t lo4 = planeWord(v, 4), lo5 = planeWord(v, 5), hi0 = planeWord(v, 6), hi1 = planeWord(v, 7);
+	const uint32_t hi2 = planeWord(v, 8), hi3 = planeWord(v, 9), hi4 = planeWord(v, 10), hi5 = planeWord(v, 11);
+	const uint32_t nx0 = nx ? hi0 : lo0, nx1 = nx ? hi1 : lo1, fx0 = nx ? lo0 : hi0, fx1 = nx ? lo1 : hi1;
+	const uint32_t ny0 = ny ? hi2 : lo2, ny1 = ny ? hi3 : lo3, fy0 = ny ? lo2 : hi2, fy1 = ny ? lo3 : hi3;
+	const uint32_t nz0 = nz ? hi4 : lo4, nz1 = nz ? hi5 : lo5, fz0 = nz ? lo4 : hi4, fz1 = nz ? lo5 : hi5;
 	// Planes are rebuilt exactly (q * 2^e is exact, one rounding for the add)
 	// and intersected as (plane - o) / d, which keeps the error relative to
 	// the distance; the quantizer also pads every box by one step.
@@ -133,14 +147,14 @@ RB_D uint32_t childBoxes(const TraceRay& r, const NodeView& v, float tmin, float
 #pragma unroll
 	for (int c = 0; c < 8; ++c)
 	{
-		const float lx = (__fmaf_rn(nodeQf(v, 0, c), scx, ox) - r.o.x) * r.ix;
-		const float hx = (__fmaf_rn(nodeQf(v, 3, c), scx, ox) - r.o.x) * r.ix;
-		const float ly = (__fmaf_rn(nodeQf(v, 1, c), scy, oy) - r.o.y) * r.iy;
-		const float hy = (__fmaf_rn(nodeQf(v, 4, c), scy, oy) - r.o.y) * r.iy;
-		const float lz = (__fmaf_rn(nodeQf(v, 2, c), scz, oz) - r.o.z) * r.iz;
-		const float hz = (__fmaf_rn(nodeQf(v, 5, c), scz, oz) - r.o.z) * r.iz;
-		const float n = fmaxf(fmaxf(fminf(lx, hx), fminf(ly, hy)), fmaxf(fminf(lz, hz), tmin));
-		const float f = fminf(fminf(fmaxf(lx, hx), fmaxf(ly, hy)), fminf(fmaxf(lz, hz), tmax)) * 1.0000004f;
+		const float tnx = (__fmaf_rn(planeQ(nx0, nx1, c), scx, ox) - r.o.x) * r.ix;
+		const float tfx = (__fmaf_rn(planeQ(fx0, fx1, c), scx, ox) - r.o.x) * r.ix;
+		const float tny = (__fmaf_rn(planeQ(ny0, ny1, c), scy, oy) - r.o.y) * r.iy;
+		const float tfy = (__fmaf_rn(planeQ(fy0, fy1, c), scy, oy) - r.o.y) * r.iy;
+		const float tnz = (__fmaf_rn(planeQ(nz0, nz1, c), scz, oz) - r.o.z) * r.iz;
+		const float tfz = (__fmaf_rn(planeQ(fz0, fz1, c), scz, oz) - r.o.z) * r.iz;
+		const float n = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+		const float f = fminf(fminf(tfx, tfy), fminf(tfz, tmax)) * 1.0000004f;
 		tnear[c] = n;
 		if (n <= f && nodeChild(v, c) != kEmptyChild) mask |= 1u << c;
 	}

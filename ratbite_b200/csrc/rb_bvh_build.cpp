@@ -12,6 +12,7 @@
 //    plane origin + q*scale is exact in float; boxes are rounded outward and
 //    padded by one step, so the quantized box always contains the exact one.
 #include "rb_bvh_build.h"
+#include "rb_bvh_quant.h"
 
 #include <algorithm>
 #include <cmath>
@@ -163,17 +164,6 @@ private:
 
 bool isLeaf(const BinNode& n) { return n.left < 0; }
 
-// Exponent e (scale 2^e) covering `extent` in 250 steps and at least two ulps of `mag`.
-int scaleExponent(double extent, double mag)
-{
-	double need = extent / 250.0;
-	const double ulp2 = mag > 0.0 ? std::ldexp(1.0, std::ilogb(mag) - 22) : std::ldexp(1.0, -126);
-	need = std::max(need, ulp2);
-	int e = static_cast<int>(std::ceil(std::log2(need)));
-	while (std::ldexp(1.0, e) < need) ++e;
-	return std::max(std::min(e, 127), -126);
-}
-
 class WideBuilder
 {
 public:
@@ -207,36 +197,11 @@ public:
 		const uint32_t me = static_cast<uint32_t>(nodes.size());
 		nodes.emplace_back();
 		BvhNode node{};
-		// Quantization frame.
-		Box all;
-		for (int i = 0; i < n; ++i) all.grow(m_bin[kids[i]].box);
-		double origin[3], scale[3];
-		for (int a = 0; a < 3; ++a)
-		{
-			const double mag = std::max(std::fabs(all.lo[a]), std::fabs(all.hi[a]));
-			const int e = scaleExponent(all.hi[a] - all.lo[a], mag);
-			scale[a] = std::ldexp(1.0, e);
-			origin[a] = std::floor(all.lo[a] / scale[a]) * scale[a] - scale[a];
-			node.origin[a] = static_cast<float>(origin[a]);
-			node.exponent[a] = static_cast<uint8_t>(e + 127);
-		}
-		node.childCount = static_cast<uint8_t>(n);
-		for (int c = 0; c < 8; ++c)
-		{
-			node.child[c] = kEmptyChild;
-			for (int a = 0; a < 3; ++a) { node.qlo[a][c] = 0; node.qhi[a][c] = 0; }
-		}
+		double lo[8][3], hi[8][3];
 		for (int c = 0; c < n; ++c)
-		{
-			const BinNode& k = m_bin[kids[c]];
-			for (int a = 0; a < 3; ++a)
-			{
-				const double ql = std::floor((k.box.lo[a] - origin[a]) / scale[a]) - 1.0;
-				const double qh = std::ceil((k.box.hi[a] - origin[a]) / scale[a]) + 1.0;
-				node.qlo[a][c] = static_cast<uint8_t>(std::min(std::max(ql, 0.0), 255.0));
-				node.qhi[a][c] = static_cast<uint8_t>(std::min(std::max(qh, 0.0), 255.0));
-			}
-		}
+			for (int a = 0; a < 3; ++a) { lo[c][a] = m_bin[kids[c]].box.lo[a]; hi[c][a] = m_bin[kids[c]].box.hi[a]; }
+		quantizeChildren(n, lo, hi, node);
+		for (int c = 0; c < 8; ++c) node.child[c] = kEmptyChild;
 		// Children: leaves reference their (re-emitted) triangle range, interior
 		// nodes recurse.
 		for (int c = 0; c < n; ++c)
@@ -292,6 +257,26 @@ WideBvh buildWideBvh(const std::vector<float>& worldVerts)
 	WideBuilder wb(bb.nodes);
 	wb.emit(0, out.triOrder, bb.m_order);
 	out.nodes = std::move(wb.nodes);
+	// Refit order: nodes grouped by depth, deepest level first.
+	std::vector<uint32_t> depth(out.nodes.size(), 0);
+	uint32_t maxDepth = 0;
+	for (uint32_t i = 0; i < out.nodes.size(); ++i)          // pre-order: parents come first
+		for (int c = 0; c < out.nodes[i].childCount; ++c)
+		{
+			const uint32_t ref = out.nodes[i].child[c];
+			if (ref != kEmptyChild && !(ref & kLeafBit))
+			{
+				depth[ref] = depth[i] + 1;
+				maxDepth = std::max(maxDepth, depth[ref]);
+			}
+		}
+	out.levelStart.assign(1, 0);
+	for (int d = static_cast<int>(maxDepth); d >= 0; --d)
+	{
+		for (uint32_t i = 0; i < out.nodes.size(); ++i)
+			if (depth[i] == static_cast<uint32_t>(d)) out.refitOrder.push_back(i);
+		out.levelStart.push_back(static_cast<uint32_t>(out.refitOrder.size()));
+	}
 	return out;
 }
 } // namespace rb

@@ -13,6 +13,10 @@ struct WideBvh
 	std::vector<BvhNode> nodes;      // node 0 is the root unless rootIsLeaf
 	std::vector<uint32_t> triOrder;  // leaf order -> input triangle index
 	bool rootIsLeaf = false;         // <= kLeafMaxTris triangles: the root is one leaf
+	// Bottom-up refit schedule: node indices grouped by depth, deepest first;
+	// level k is refitOrder[levelStart[k] .. levelStart[k+1]).
+	std::vector<uint32_t> refitOrder;
+	std::vector<uint32_t> levelStart;
 };
 
 // worldVerts: 9 floats per triangle. Degenerate triangles must already be removed.

@@ -21,6 +21,7 @@
 #include "rb_bvh_build.h"
 #include "rb_envmap.h"
 #include "rb_light.cuh"
+#include "rb_refit.h"
 #include "rb_scene.h"
 #include "rb_wavefront.h"
 
@@ -49,6 +50,11 @@ struct rb_ctx
 	bool haveLaunch = false, haveGeometry = false;
 	uint64_t pathsTraced = 0;
 	// cross-table references checked before any kernel reads them
+	// refit of moved instances (rb_update_instances)
+	rb::RefitData refit;
+	uint32_t geoInstances = 0, geoSubsets = 0;
+	float* xfDev = nullptr;                     // 12 floats per flattened instance (in geoBufs)
+	float* wiDev = nullptr;
 	uint32_t geoEmissive = 0;                   // emissive triangles traced by the geometry
 	uint32_t geoMaxMaterial = 0;                // 1 + largest material index of the geometry
 	uint32_t lightMaxMaterial = 0;              // 1 + largest material index of the light records
@@ -370,6 +376,7 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 	cudaSetDevice(ctx->device);
 	// Triangles in canonical order: emissive subsets, then instances x submeshes.
 	std::vector<float> world;          // 9 per kept triangle
+	std::vector<float> objAll;         // 9 object-space floats per kept triangle
 	std::vector<uint32_t> canon, inst, sbt, prim, enc;
 	std::vector<float> normalMatrix;   // 9 per instance
 	uint32_t instIndex = 0, canonical = 0, emissivePrim = 0;
@@ -385,6 +392,7 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 		for (float v : w) if (!std::isfinite(v)) return false;
 		if (degenerate(w) || degenerate(obj)) return true;
 		world.insert(world.end(), w, w + 9);
+		objAll.insert(objAll.end(), obj, obj + 9);
 		canon.push_back(id);
 		inst.push_back(instId);
 		sbt.push_back(sbtData);
@@ -438,7 +446,7 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 	}
 	const rb::WideBvh bvh = rb::buildWideBvh(world);
 	const size_t nt = canon.size();
-	std::vector<float4> triVerts(3 * std::max<size_t>(nt, 1));
+	std::vector<float4> triVerts(3 * std::max<size_t>(nt, 1)), objVerts(3 * std::max<size_t>(nt, 1));
 	std::vector<uint2> triAux(std::max<size_t>(nt, 1));
 	for (size_t j = 0; j < nt; ++j)
 	{
@@ -449,6 +457,8 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 		b.x = w[3]; b.y = w[4]; b.z = w[5]; std::memcpy(&b.w, &inst[t], 4);
 		c.x = w[6]; c.y = w[7]; c.z = w[8]; std::memcpy(&c.w, &sbt[t], 4);
 		triVerts[3 * j] = a; triVerts[3 * j + 1] = b; triVerts[3 * j + 2] = c;
+		const float* ob = objAll.data() + 9 * t;
+		for (int k = 0; k < 3; ++k) objVerts[3 * j + k] = make_float4(ob[3 * k], ob[3 * k + 1], ob[3 * k + 2], 0.0f);
 		triAux[j] = make_uint2(enc[t], prim[t]);
 	}
 	cudaStreamSynchronize(ctx->stream);
@@ -461,7 +471,26 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, triAux.data(), sizeof(uint2) * triAux.size(), G.triAux);
 	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, normalMatrix.empty() ? nullptr : normalMatrix.data(),
 		sizeof(float) * std::max<size_t>(normalMatrix.size(), 9), G.normalMatrix);
+	// refit data: object-space vertices, the bottom-up schedule, box scratch
+	// and room for the flattened instances' transforms and inverses
+	ctx->refit = rb::RefitData{};
+	float4* objDev = nullptr;
+	uint32_t* orderDev = nullptr;
+	double* boxDev = nullptr;
+	const size_t nInst = std::max<size_t>(instIndex, 1);
+	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, objVerts.data(), sizeof(float4) * objVerts.size(), objDev);
+	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, bvh.refitOrder.empty() ? nullptr : bvh.refitOrder.data(),
+		sizeof(uint32_t) * std::max<size_t>(bvh.refitOrder.size(), 1), orderDev);
+	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, nullptr, sizeof(double) * 6 * std::max<size_t>(bvh.nodes.size(), 1), boxDev);
+	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, nullptr, sizeof(float) * 12 * nInst, ctx->xfDev);
+	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, nullptr, sizeof(float) * 12 * nInst, ctx->wiDev);
 	if (rc != RB_OK) return rc;
+	ctx->refit.objVerts = objDev;
+	ctx->refit.order = orderDev;
+	ctx->refit.nodeBox = boxDev;
+	ctx->refit.levelStart = bvh.levelStart;
+	ctx->geoInstances = g->instance_count;
+	ctx->geoSubsets = g->emissive_subset_count;
 	G.nodeCount = static_cast<uint32_t>(bvh.nodes.size());
 	G.triCount = static_cast<uint32_t>(nt);
 	G.rootIsLeaf = bvh.rootIsLeaf ? 1u : 0u;
@@ -471,6 +500,40 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 		if (s != 0xFFFFFFFFu) ctx->geoMaxMaterial = std::max(ctx->geoMaxMaterial, s + 1);
 	ctx->haveGeometry = true;
 	return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? RB_OK : fail(ctx, RB_ERR_CUDA, "geometry upload");
+}
+
+int rb_update_instances(rb_ctx* ctx, const float* instXf, const float* subsetXf, void* stream)
+{
+	if (!ctx) return RB_ERR_INVALID;
+	if (!ctx->haveGeometry) return fail(ctx, RB_ERR_NO_SCENE, "rb_update_instances: no geometry");
+	if ((ctx->geoInstances && !instXf) || (ctx->geoSubsets && !subsetXf))
+		return fail(ctx, RB_ERR_INVALID, "rb_update_instances: null transforms");
+	const uint32_t n = ctx->geoSubsets + ctx->geoInstances;
+	std::vector<float> xf(12 * std::max<uint32_t>(n, 1), 0.0f), wi(12 * std::max<uint32_t>(n, 1), 0.0f),
+		nm(9 * std::max<uint32_t>(n, 1), 0.0f);
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		const float* src = i < ctx->geoSubsets ? subsetXf + 12 * i : instXf + 12 * (i - ctx->geoSubsets);
+		for (int k = 0; k < 12; ++k)
+			if (!std::isfinite(src[k])) return fail(ctx, RB_ERR_INVALID, "rb_update_instances: non-finite transform");
+		std::memcpy(xf.data() + 12 * i, src, sizeof(float) * 12);
+		float* w = wi.data() + 12 * i;
+		invert3x4(src, w);
+		const float m[9] = { w[0], w[4], w[8], w[1], w[5], w[9], w[2], w[6], w[10] };
+		std::memcpy(nm.data() + 9 * i, m, sizeof(m));
+	}
+	cudaSetDevice(ctx->device);
+	const cudaStream_t st = pick(ctx, stream);
+	cudaError_t e = cudaMemcpyAsync(ctx->xfDev, xf.data(), sizeof(float) * 12 * n, cudaMemcpyHostToDevice, st);
+	if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->wiDev, wi.data(), sizeof(float) * 12 * n, cudaMemcpyHostToDevice, st);
+	if (e == cudaSuccess)
+		e = cudaMemcpyAsync(const_cast<float*>(ctx->scene.geo.normalMatrix), nm.data(), sizeof(float) * 9 * n,
+			cudaMemcpyHostToDevice, st);
+	if (e != cudaSuccess) return cudaFail(ctx, e, "rb_update_instances: upload");
+	rb::launchRefit(ctx->refit, ctx->scene.geo, ctx->xfDev, ctx->wiDev, ctx->status, ctx->shape.smCount, st);
+	// the host copies above read pageable memory that goes away on return
+	e = cudaStreamSynchronize(st);
+	return e == cudaSuccess ? RB_OK : cudaFail(ctx, e, "rb_update_instances");
 }
 
 int rb_set_lights(rb_ctx* ctx, const rb_light_tree* t)

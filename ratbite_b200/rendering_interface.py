@@ -118,6 +118,18 @@ class RenderingInterface:
         self._keep.append(launch)
         self.prepare_data_for_rendering(launch)
 
+    def update_instances(self, instance_transforms, subset_transforms=None, stream=None):
+        """Moves the instances of the loaded geometry (the reference's
+        updateInstanceAccelerationStructure on a camera move): (n, 3, 4)
+        camera-relative transforms in the order of the scene's instances and
+        emissive subsets; the BVH is refit on the device."""
+        inst = np.ascontiguousarray(instance_transforms, np.float32).reshape(-1)
+        sub = np.ascontiguousarray(np.zeros(0, np.float32) if subset_transforms is None else subset_transforms,
+                                   np.float32).reshape(-1)
+        s = None if stream is None else C.c_void_p(stream)
+        check(self.lib.rb_update_instances(self.ctx, _ptr(inst) if inst.size else None,
+                                           _ptr(sub) if sub.size else None, s), self.ctx, "rb_update_instances")
+
     # ---- rendering -----------------------------------------------------------
     def render(self, sample_offset: int, sample_count: int, stream=None):
         """Asynchronous: renders samples [offset, offset+count) of every pixel."""
