@@ -275,6 +275,31 @@ int rb_accum_device_ptr(rb_ctx* ctx, void** out);
 /* Stream-ordered copy of the accumulation buffer to `dst` (device or pinned
  * host memory, width*height*4 doubles), on `stream` (NULL: context stream). */
 int rb_copy_accum_async(rb_ctx* ctx, void* dst, void* stream);
+/* ---- progressive rendering (RenderingInterface::render,
+ * updateSubLaunchData, updateSamplingState and the restart of
+ * processCommands, src/core/rendering_interface.cpp:1830-1839, 1846-1872,
+ * 1980-2013) ---------------------------------------------------------------- */
+#define RB_MODE_IMMEDIATE 0   /* one sample per sub-launch (RenderContext::Mode) */
+#define RB_MODE_GRADUAL   1   /* sub-launches grow as min(int(max(3, n)^1.5), 64) */
+typedef struct rb_progress {
+    uint32_t launched_offset;  /* first sample of the sub-launch this step started */
+    uint32_t launched_count;   /* its sample count (0: nothing left to render) */
+    uint32_t processed;        /* samples per pixel complete before it (m_processedSampleCount) */
+    uint32_t total;            /* target samples per pixel */
+    uint32_t finished;         /* 1 once every sample has been launched */
+    uint32_t reserved;
+} rb_progress;
+/* Restarts the progressive render: the next step renders sample 0 alone and
+ * restarts the accumulation, as a scene or camera change does. */
+int rb_progressive_restart(rb_ctx* ctx, uint32_t total_samples, int mode);
+/* Launches the current sub-launch (rb_render, asynchronous on `stream`) and
+ * advances the schedule; a step after the last sample reports finished. */
+int rb_progressive_step(rb_ctx* ctx, void* stream, rb_progress* out);
+/* The schedule alone: writes up to `capacity` (offset, count) pairs of the
+ * sub-launches of a render of total_samples in `mode`; returns their number
+ * (negative on bad arguments). No device needed. */
+int rb_progressive_plan(uint32_t total_samples, int mode, uint32_t* offsets, uint32_t* counts, uint32_t capacity);
+
 /* ---- resolve (replaces resolveRender, src/core/rendering_interface.cpp
  * :1512-1532, and the GL image it writes) -------------------------------- */
 /* Resolves the accumulation into the context's headless image: per pixel

@@ -39,6 +39,9 @@ SIGNATURES = {
     "rb_accum_device_ptr": (C.c_int, [_P, C.POINTER(_P)]),
     "rb_copy_accum_async": (C.c_int, [_P, _P, _P]),
     "rb_clear_accum": (C.c_int, [_P, _P]),
+    "rb_progressive_restart": (C.c_int, [_P, _U32, C.c_int]),
+    "rb_progressive_step": (C.c_int, [_P, _P, C.POINTER(abi.rb_progress)]),
+    "rb_progressive_plan": (C.c_int, [_U32, C.c_int, _P, _P, _U32]),
     "rb_resolve": (C.c_int, [_P, _P, C.c_float, _P]),
     "rb_read_image": (C.c_int, [_P, _P]),
     "rb_image_device_ptr": (C.c_int, [_P, C.POINTER(_P)]),

@@ -161,6 +161,15 @@ class rb_device_status(C.Structure):
                 ("paths_traced", C.c_uint64), ("rays_traced", C.c_uint64)]
 
 
+RB_MODE_IMMEDIATE = 0
+RB_MODE_GRADUAL = 1
+
+
+class rb_progress(C.Structure):
+    _fields_ = [("launched_offset", C.c_uint32), ("launched_count", C.c_uint32), ("processed", C.c_uint32),
+                ("total", C.c_uint32), ("finished", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 RB_STATS_COUNT = 1
 RB_STATS_TIME = 2
 

@@ -58,6 +58,9 @@ struct rb_ctx
 	uint32_t geoEmissive = 0;                   // emissive triangles traced by the geometry
 	uint32_t geoMaxMaterial = 0;                // 1 + largest material index of the geometry
 	uint32_t lightMaxMaterial = 0;              // 1 + largest material index of the light records
+	// progressive schedule (rb_progressive_*)
+	uint32_t progOffset = 0, progCount = 0, progTotal = 0;
+	int progMode = RB_MODE_IMMEDIATE;
 	// instrumentation (rb_set_stats)
 	uint32_t statsMode = 0;
 	unsigned long long* counters = nullptr;     // 7 device counters
@@ -755,6 +758,68 @@ int rb_copy_accum_async(rb_ctx* ctx, void* dst, void* stream)
 	const cudaError_t e = cudaMemcpyAsync(dst, ctx->accum, sizeof(double4) * ctx->accumPixels, cudaMemcpyDefault,
 		pick(ctx, stream));
 	return e == cudaSuccess ? RB_OK : cudaFail(ctx, e, "rb_copy_accum_async");
+}
+
+namespace
+{
+// updateSamplingState (src/core/rendering_interface.cpp:1859-1872): the
+// sub-launch after (offset, count).
+void advance(uint32_t total, int mode, uint32_t& offset, uint32_t& count)
+{
+	offset += count;
+	int size = 1;
+	if (mode == RB_MODE_GRADUAL)
+		size = std::min(static_cast<int>(std::pow(std::max(3, static_cast<int>(count)), 1.5)), 64);
+	const int left = std::max(0, static_cast<int>(total) - static_cast<int>(offset));
+	count = static_cast<uint32_t>(std::min(left, size));
+}
+} // namespace
+
+int rb_progressive_plan(uint32_t total, int mode, uint32_t* offsets, uint32_t* counts, uint32_t capacity)
+{
+	if ((mode != RB_MODE_IMMEDIATE && mode != RB_MODE_GRADUAL) || total > (1u << 30)) return RB_ERR_INVALID;
+	if (capacity && (!offsets || !counts)) return RB_ERR_INVALID;
+	uint32_t offset = 0, count = total ? 1u : 0u, n = 0;
+	while (count)
+	{
+		if (n < capacity) { offsets[n] = offset; counts[n] = count; }
+		++n;
+		advance(total, mode, offset, count);
+	}
+	return static_cast<int>(n);
+}
+
+int rb_progressive_restart(rb_ctx* ctx, uint32_t total, int mode)
+{
+	if (!ctx) return RB_ERR_INVALID;
+	if ((mode != RB_MODE_IMMEDIATE && mode != RB_MODE_GRADUAL) || total > (1u << 30))
+		return fail(ctx, RB_ERR_INVALID, "rb_progressive_restart: bad mode or sample count");
+	ctx->progOffset = 0;
+	ctx->progCount = total ? 1u : 0u;
+	ctx->progTotal = total;
+	ctx->progMode = mode;
+	return RB_OK;
+}
+
+int rb_progressive_step(rb_ctx* ctx, void* stream, rb_progress* out)
+{
+	if (!ctx || !out) return RB_ERR_INVALID;
+	*out = rb_progress{};
+	out->total = ctx->progTotal;
+	out->processed = ctx->progOffset;
+	if (ctx->progCount == 0)
+	{
+		out->finished = 1;
+		return RB_OK;
+	}
+	const uint32_t offset = ctx->progOffset, count = ctx->progCount;
+	const int rc = rb_render(ctx, offset, count, stream);
+	if (rc != RB_OK) return rc;
+	advance(ctx->progTotal, ctx->progMode, ctx->progOffset, ctx->progCount);
+	out->launched_offset = offset;
+	out->launched_count = count;
+	out->finished = ctx->progCount == 0 ? 1u : 0u;
+	return RB_OK;
 }
 
 int rb_resolve(rb_ctx* ctx, const float colorspace[9], float exposure_scale, void* stream)

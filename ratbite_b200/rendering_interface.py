@@ -136,6 +136,17 @@ class RenderingInterface:
         s = None if stream is None else C.c_void_p(stream)
         check(self.lib.rb_render(self.ctx, sample_offset, sample_count, s), self.ctx, "rb_render")
 
+    def progressive_restart(self, total_samples: int, mode: int = abi.RB_MODE_GRADUAL):
+        """Restarts the progressive render (the next step renders sample 0 alone)."""
+        check(self.lib.rb_progressive_restart(self.ctx, total_samples, mode), self.ctx, "rb_progressive_restart")
+
+    def progressive_step(self, stream=None) -> abi.rb_progress:
+        """Launches the next sub-launch of the progressive render (asynchronous)."""
+        out = abi.rb_progress()
+        s = None if stream is None else C.c_void_p(stream)
+        check(self.lib.rb_progressive_step(self.ctx, s, C.byref(out)), self.ctx, "rb_progressive_step")
+        return out
+
     def synchronize(self):
         check(self.lib.rb_synchronize(self.ctx), self.ctx, "rb_synchronize")
 

@@ -269,3 +269,36 @@ def test_png_round_trip(tmp_path):
     assert np.array_equal(image_io.read_png(tmp_path / "x.png"), img)
     with pytest.raises(ValueError):
         image_io.write_png(tmp_path / "y.png", img[..., :3])
+
+
+# ------------------------------------------------------- progressive schedule
+def _reference_schedule(total, gradual):
+    """updateSamplingState (src/core/rendering_interface.cpp:1859-1872) after a
+    restart (offset 0, count 1, :1830-1839), restated."""
+    out, offset, count = [], 0, (1 if total else 0)
+    while count:
+        out.append((offset, count))
+        offset += count
+        size = min(int(max(3, count) ** 1.5), 64) if gradual else 1
+        count = min(max(0, total - offset), size)
+    return out
+
+
+@pytest.mark.parametrize("total", [0, 1, 2, 3, 5, 64, 100, 1000, 4096])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_progressive_plan_matches_reference_schedule(total, mode):
+    lib = _native.load()
+    offs = np.zeros(5000, np.uint32)
+    cnts = np.zeros(5000, np.uint32)
+    n = lib.rb_progressive_plan(total, mode, offs.ctypes.data, cnts.ctypes.data, 5000)
+    want = _reference_schedule(total, mode == 1)
+    assert n == len(want)
+    assert list(zip(offs[:n].tolist(), cnts[:n].tolist())) == want
+    assert int(cnts[:n].sum()) == total
+
+
+def test_progressive_plan_rejects_bad_input():
+    lib = _native.load()
+    assert lib.rb_progressive_plan(10, 2, None, None, 0) < 0
+    assert lib.rb_progressive_plan(10, 1, None, None, 4) < 0
+    assert lib.rb_progressive_plan(10, 1, None, None, 0) == len(_reference_schedule(10, True))
