@@ -10,6 +10,8 @@ cp -r "$REF/src" "$OUT/src"
 cp -r "$REF/bin" "$OUT/bin"
 mkdir -p "$OUT/dependencies/include"
 cp -r "$REF/dependencies/include/glm" "$OUT/dependencies/include/glm"
+cp -r "$REF/dependencies/include/cgltf" "$OUT/dependencies/include/cgltf"
+cp -r "$REF/dependencies/include/stb" "$OUT/dependencies/include/stb"
 chmod -R u+w "$OUT"
 # src/core/util.h:60-105 — `-> typename enable_if_t<...>` is accepted only by MSVC.
 sed -i 's/-> typename enable_if_t</-> enable_if_t</' "$OUT/src/core/util.h"

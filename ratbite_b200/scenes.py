@@ -106,6 +106,12 @@ class Material:
     ior_spectrum: int = 0
     absorp_spectrum: int = 0
     mf_roughness: float = 0.0
+    # explicit MaterialData factor bits (e.g. from a glTF descriptor); None:
+    # base colour, metalness and roughness always present, the rest by value
+    factors: int | None = None
+    alpha: float = 1.0
+    alpha_cutoff: float = 0.0
+    double_sided: bool = False
 
 
 @dataclass
@@ -153,7 +159,7 @@ class Scene:
             r = recs[i]
             sm = owner.get(i)
             r.bxdf = m.bxdf
-            r.double_sided = 0
+            r.double_sided = 1 if m.double_sided else 0
             r.sheen_present = 1 if m.sheen_color is not None else 0
             r.ior = m.ior
             r.mf_roughness = m.mf_roughness
@@ -173,6 +179,10 @@ class Scene:
             if m.emissive is not None:
                 factors |= abi.RB_FACTOR_EMISSION
                 r.emissive = abi.F3(*m.emissive)
+            if m.factors is not None:
+                factors = m.factors
+                r.base_color = abi.F4(*m.base_color, m.alpha)
+                r.alpha_cutoff = m.alpha_cutoff
             r.factors = factors
             if sm is not None:
                 idx = np.ascontiguousarray(sm.indices)
