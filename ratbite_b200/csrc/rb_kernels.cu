@@ -269,10 +269,11 @@ __global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, Wa
 }
 
 // Minimum resident blocks per SM requested for the shading kernels, which
-// caps their registers per thread (65536 / (128 x blocks)): 85, 64 and 85.
+// caps their registers per thread (65536 / (128 x blocks)): 85, 64 and 64.
 // These kernels are latency-bound, and on B200 (at-scale frame) the extra
-// warps outweigh the few spilled bytes: surface -8%, light sample -6%,
-// BxDF -18% against the compiler's own choice.
+// warps outweigh the spilled bytes: surface -8%, light sample -6%, BxDF -29%
+// against the compiler's own choice (BxDF at 5 / 6 / 7 / 8 blocks: 339 /
+// 306 / 283 / 265 ms per frame).
 #ifndef RB_SURFACE_MIN_BLOCKS
 #define RB_SURFACE_MIN_BLOCKS 6
 #endif
@@ -280,7 +281,7 @@ __global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, Wa
 #define RB_NEE_MIN_BLOCKS 8
 #endif
 #ifndef RB_BSDF_MIN_BLOCKS
-#define RB_BSDF_MIN_BLOCKS 6
+#define RB_BSDF_MIN_BLOCKS 8
 #endif
 
 // Block size of the shared-memory light-sample kernel: two blocks of 512
