@@ -269,11 +269,12 @@ __global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, Wa
 }
 
 // Minimum resident blocks per SM requested for the shading kernels, which
-// caps their registers per thread (65536 / (128 x blocks)): 85, 64 and 64.
+// caps their registers per thread (65536 / (128 x blocks)): 85, 64 and 32.
 // These kernels are latency-bound, and on B200 (at-scale frame) the extra
-// warps outweigh the spilled bytes: surface -8%, light sample -6%, BxDF -29%
-// against the compiler's own choice (BxDF at 5 / 6 / 7 / 8 blocks: 339 /
-// 306 / 283 / 265 ms per frame).
+// warps outweigh the spilled bytes, which stay in L1: surface -8%, light
+// sample -6%, BxDF -38% against the compiler's own choice (BxDF at 5 / 6 /
+// 8 / 12 / 16 blocks: 339 / 306 / 265 / 236 / 232 ms per frame, with 100 B
+// to 1.2 KB of spills per thread).
 #ifndef RB_SURFACE_MIN_BLOCKS
 #define RB_SURFACE_MIN_BLOCKS 6
 #endif
@@ -281,7 +282,7 @@ __global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, Wa
 #define RB_NEE_MIN_BLOCKS 8
 #endif
 #ifndef RB_BSDF_MIN_BLOCKS
-#define RB_BSDF_MIN_BLOCKS 8
+#define RB_BSDF_MIN_BLOCKS 16
 #endif
 
 // Block size of the shared-memory light-sample kernel: two blocks of 512
