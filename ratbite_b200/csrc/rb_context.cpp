@@ -104,6 +104,28 @@ int upload(rb_ctx* ctx, std::vector<void*>& owner, const void* src, size_t bytes
 }
 cudaStream_t pick(rb_ctx* ctx, void* s) { return s ? static_cast<cudaStream_t>(s) : ctx->stream; }
 
+// Setters are transactional: new tables are uploaded into `fresh` first, and
+// only when every upload succeeded does the context switch to them, after
+// all queued work (renders may run on caller streams) has finished with the
+// old ones. A rejected or failed call leaves the context exactly as it was.
+int commit(rb_ctx* ctx, std::vector<void*>& owned, std::vector<void*>& fresh, int rc)
+{
+	if (rc != RB_OK)
+	{
+		freeAll(fresh);
+		return rc;
+	}
+	const cudaError_t e = cudaDeviceSynchronize();
+	if (e != cudaSuccess)
+	{
+		freeAll(fresh);
+		return cudaFail(ctx, e, "synchronize before replacing scene data");
+	}
+	freeAll(owned);
+	owned.swap(fresh);
+	return RB_OK;
+}
+
 // Row-major 3x4 inverse in double, rounded once to float.
 void invert3x4(const float* m, float* out)
 {
@@ -285,16 +307,17 @@ int rb_set_luts(rb_ctx* ctx, const float* conductor, const float* dOuter, const 
 	if (!ctx || !conductor || !dOuter || !dInner || !rOuter || !rInner || !sheen)
 		return fail(ctx, RB_ERR_INVALID, "rb_set_luts: null table");
 	cudaSetDevice(ctx->device);
-	cudaStreamSynchronize(ctx->stream);
-	freeAll(ctx->lutBufs);
 	const size_t n2 = rb::kLutN * rb::kLutN, n3 = n2 * rb::kLutN;
-	rb::DevLuts& L = ctx->scene.luts;
-	int rc = upload(ctx, ctx->lutBufs, conductor, n2 * 4, L.conductor);
-	if (rc == RB_OK) rc = upload(ctx, ctx->lutBufs, dOuter, n3 * 4, L.dielOuter);
-	if (rc == RB_OK) rc = upload(ctx, ctx->lutBufs, dInner, n3 * 4, L.dielInner);
-	if (rc == RB_OK) rc = upload(ctx, ctx->lutBufs, rOuter, n3 * 4, L.reflOuter);
-	if (rc == RB_OK) rc = upload(ctx, ctx->lutBufs, rInner, n3 * 4, L.reflInner);
-	if (rc == RB_OK) rc = upload(ctx, ctx->lutBufs, sheen, n2 * 16, L.sheen);
+	std::vector<void*> fresh;
+	rb::DevLuts L{};
+	int rc = upload(ctx, fresh, conductor, n2 * 4, L.conductor);
+	if (rc == RB_OK) rc = upload(ctx, fresh, dOuter, n3 * 4, L.dielOuter);
+	if (rc == RB_OK) rc = upload(ctx, fresh, dInner, n3 * 4, L.dielInner);
+	if (rc == RB_OK) rc = upload(ctx, fresh, rOuter, n3 * 4, L.reflOuter);
+	if (rc == RB_OK) rc = upload(ctx, fresh, rInner, n3 * 4, L.reflInner);
+	if (rc == RB_OK) rc = upload(ctx, fresh, sheen, n2 * 16, L.sheen);
+	rc = commit(ctx, ctx->lutBufs, fresh, rc);
+	if (rc == RB_OK) ctx->scene.luts = L;
 	return rc;
 }
 
@@ -302,24 +325,21 @@ int rb_set_spectra(rb_ctx* ctx, const float* sensor, const float* basis, const f
 {
 	if (!ctx || !sensor || !basis || (nExtra && !extra)) return fail(ctx, RB_ERR_INVALID, "rb_set_spectra: null table");
 	cudaSetDevice(ctx->device);
-	cudaStreamSynchronize(ctx->stream);
-	freeAll(ctx->spectraBufs);
 	const size_t b = sizeof(float) * rb::kSpectrumBins;
-	rb::DevSpectra& S = ctx->scene.spectra;
-	int rc = upload(ctx, ctx->spectraBufs, sensor, 3 * b, S.sensor);
-	if (rc == RB_OK) rc = upload(ctx, ctx->spectraBufs, basis, 3 * b, S.basis);
-	if (rc == RB_OK) rc = upload(ctx, ctx->spectraBufs, nExtra ? extra : nullptr, std::max<size_t>(nExtra, 1) * b, S.extra);
+	std::vector<void*> fresh;
+	rb::DevSpectra S{};
+	int rc = upload(ctx, fresh, sensor, 3 * b, S.sensor);
+	if (rc == RB_OK) rc = upload(ctx, fresh, basis, 3 * b, S.basis);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nExtra ? extra : nullptr, std::max<size_t>(nExtra, 1) * b, S.extra);
 	S.extraCount = nExtra;
+	rc = commit(ctx, ctx->spectraBufs, fresh, rc);
+	if (rc == RB_OK) ctx->scene.spectra = S;
 	return rc;
 }
 
 int rb_set_materials(rb_ctx* ctx, const rb_material* mats, uint32_t count)
 {
 	if (!ctx || (count && !mats)) return fail(ctx, RB_ERR_INVALID, "rb_set_materials: null materials");
-	cudaSetDevice(ctx->device);
-	cudaStreamSynchronize(ctx->stream);
-	freeAll(ctx->materialBufs);
-	std::vector<rb::DevMaterial> dm(std::max<uint32_t>(count, 1));
 	for (uint32_t i = 0; i < count; ++i)
 	{
 		const rb_material& m = mats[i];
@@ -328,6 +348,14 @@ int rb_set_materials(rb_ctx* ctx, const rb_material* mats, uint32_t count)
 		if (m.index_type > RB_INDEX_U32) return fail(ctx, RB_ERR_INVALID, "rb_set_materials: unknown index type");
 		if ((m.attributes & (RB_ATTR_NORMAL | RB_ATTR_FRAME)) && (!m.attribute_data || m.attribute_stride == 0))
 			return fail(ctx, RB_ERR_INVALID, "rb_set_materials: attributes declared without attribute data");
+		if (m.triangle_count && !m.indices) return fail(ctx, RB_ERR_INVALID, "rb_set_materials: null indices");
+	}
+	cudaSetDevice(ctx->device);
+	std::vector<void*> fresh;
+	std::vector<rb::DevMaterial> dm(std::max<uint32_t>(count, 1));
+	for (uint32_t i = 0; i < count; ++i)
+	{
+		const rb_material& m = mats[i];
 		rb::DevMaterial& d = dm[i];
 		d = rb::DevMaterial{};
 		d.bxdf = m.bxdf;
@@ -352,22 +380,23 @@ int rb_set_materials(rb_ctx* ctx, const rb_material* mats, uint32_t count)
 		d.triangleCount = m.triangle_count;
 		d.vertexCount = m.vertex_count;
 		const size_t ib = static_cast<size_t>(m.triangle_count) * 3 * (m.index_type == RB_INDEX_U16 ? 2 : 4);
-		if (m.triangle_count && !m.indices) return fail(ctx, RB_ERR_INVALID, "rb_set_materials: null indices");
 		uint8_t* dptr = nullptr;
-		int rc = upload(ctx, ctx->materialBufs, m.indices, ib, dptr);
-		if (rc != RB_OK) return rc;
+		int rc = upload(ctx, fresh, m.indices, ib, dptr);
+		if (rc != RB_OK) return commit(ctx, ctx->materialBufs, fresh, rc);
 		d.indices = dptr;
 		const size_t ab = static_cast<size_t>(m.vertex_count) * m.attribute_stride;
-		rc = upload(ctx, ctx->materialBufs, m.attribute_data && ab ? m.attribute_data : nullptr, ab, dptr);
-		if (rc != RB_OK) return rc;
+		rc = upload(ctx, fresh, m.attribute_data && ab ? m.attribute_data : nullptr, ab, dptr);
+		if (rc != RB_OK) return commit(ctx, ctx->materialBufs, fresh, rc);
 		d.attributeData = dptr;
 	}
 	rb::DevMaterial* dptr = nullptr;
-	const int rc = upload(ctx, ctx->materialBufs, dm.data(), sizeof(rb::DevMaterial) * dm.size(), dptr);
+	int rc = upload(ctx, fresh, dm.data(), sizeof(rb::DevMaterial) * dm.size(), dptr);
+	if (rc == RB_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = fail(ctx, RB_ERR_CUDA, "material upload");
+	rc = commit(ctx, ctx->materialBufs, fresh, rc);
 	if (rc != RB_OK) return rc;
 	ctx->scene.materials = dptr;
 	ctx->scene.materialCount = count;
-	return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? RB_OK : fail(ctx, RB_ERR_CUDA, "material upload");
+	return RB_OK;
 }
 
 int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
@@ -464,45 +493,50 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 		for (int k = 0; k < 3; ++k) objVerts[3 * j + k] = make_float4(ob[3 * k], ob[3 * k + 1], ob[3 * k + 2], 0.0f);
 		triAux[j] = make_uint2(enc[t], prim[t]);
 	}
-	cudaStreamSynchronize(ctx->stream);
-	freeAll(ctx->geoBufs);
-	rb::DevGeometry& G = ctx->scene.geo;
-	G = rb::DevGeometry{};
-	int rc = upload(ctx, ctx->geoBufs, bvh.nodes.empty() ? nullptr : bvh.nodes.data(),
+	std::vector<void*> fresh;
+	rb::DevGeometry G{};
+	int rc = upload(ctx, fresh, bvh.nodes.empty() ? nullptr : bvh.nodes.data(),
 		sizeof(rb::BvhNode) * std::max<size_t>(bvh.nodes.size(), 1), G.nodes);
-	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, triVerts.data(), sizeof(float4) * triVerts.size(), G.triVerts);
-	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, triAux.data(), sizeof(uint2) * triAux.size(), G.triAux);
-	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, normalMatrix.empty() ? nullptr : normalMatrix.data(),
+	if (rc == RB_OK) rc = upload(ctx, fresh, triVerts.data(), sizeof(float4) * triVerts.size(), G.triVerts);
+	if (rc == RB_OK) rc = upload(ctx, fresh, triAux.data(), sizeof(uint2) * triAux.size(), G.triAux);
+	if (rc == RB_OK) rc = upload(ctx, fresh, normalMatrix.empty() ? nullptr : normalMatrix.data(),
 		sizeof(float) * std::max<size_t>(normalMatrix.size(), 9), G.normalMatrix);
 	// refit data: object-space vertices, the bottom-up schedule, box scratch
 	// and room for the flattened instances' transforms and inverses
-	ctx->refit = rb::RefitData{};
+	rb::RefitData refit{};
 	float4* objDev = nullptr;
 	uint32_t* orderDev = nullptr;
 	double* boxDev = nullptr;
+	float *xfDev = nullptr, *wiDev = nullptr;
 	const size_t nInst = std::max<size_t>(instIndex, 1);
-	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, objVerts.data(), sizeof(float4) * objVerts.size(), objDev);
-	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, bvh.refitOrder.empty() ? nullptr : bvh.refitOrder.data(),
+	if (rc == RB_OK) rc = upload(ctx, fresh, objVerts.data(), sizeof(float4) * objVerts.size(), objDev);
+	if (rc == RB_OK) rc = upload(ctx, fresh, bvh.refitOrder.empty() ? nullptr : bvh.refitOrder.data(),
 		sizeof(uint32_t) * std::max<size_t>(bvh.refitOrder.size(), 1), orderDev);
-	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, nullptr, sizeof(double) * 6 * std::max<size_t>(bvh.nodes.size(), 1), boxDev);
-	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, nullptr, sizeof(float) * 12 * nInst, ctx->xfDev);
-	if (rc == RB_OK) rc = upload(ctx, ctx->geoBufs, nullptr, sizeof(float) * 12 * nInst, ctx->wiDev);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(double) * 6 * std::max<size_t>(bvh.nodes.size(), 1), boxDev);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(float) * 12 * nInst, xfDev);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(float) * 12 * nInst, wiDev);
+	if (rc == RB_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = fail(ctx, RB_ERR_CUDA, "geometry upload");
+	rc = commit(ctx, ctx->geoBufs, fresh, rc);
 	if (rc != RB_OK) return rc;
-	ctx->refit.objVerts = objDev;
-	ctx->refit.order = orderDev;
-	ctx->refit.nodeBox = boxDev;
-	ctx->refit.levelStart = bvh.levelStart;
+	refit.objVerts = objDev;
+	refit.order = orderDev;
+	refit.nodeBox = boxDev;
+	refit.levelStart = bvh.levelStart;
+	ctx->refit = refit;
+	ctx->xfDev = xfDev;
+	ctx->wiDev = wiDev;
 	ctx->geoInstances = g->instance_count;
 	ctx->geoSubsets = g->emissive_subset_count;
 	G.nodeCount = static_cast<uint32_t>(bvh.nodes.size());
 	G.triCount = static_cast<uint32_t>(nt);
 	G.rootIsLeaf = bvh.rootIsLeaf ? 1u : 0u;
+	ctx->scene.geo = G;
 	ctx->geoEmissive = emissivePrim;
 	ctx->geoMaxMaterial = 0;
 	for (uint32_t s : sbt)
 		if (s != 0xFFFFFFFFu) ctx->geoMaxMaterial = std::max(ctx->geoMaxMaterial, s + 1);
 	ctx->haveGeometry = true;
-	return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? RB_OK : fail(ctx, RB_ERR_CUDA, "geometry upload");
+	return RB_OK;
 }
 
 int rb_update_instances(rb_ctx* ctx, const float* instXf, const float* subsetXf, void* stream)
@@ -564,28 +598,28 @@ int rb_set_lights(rb_ctx* ctx, const rb_light_tree* t)
 		if (type == rb::kLightTypeTriangle && idx >= t->triangle_count)
 			return fail(ctx, RB_ERR_INVALID, "rb_set_lights: light pointer out of range");
 	}
-	cudaStreamSynchronize(ctx->stream);
-	freeAll(ctx->lightBufs);
-	rb::DevLights& L = ctx->scene.lights;
-	L = rb::DevLights{};
-	int rc = upload(ctx, ctx->lightBufs, t->triangles, sizeof(rb::EmissiveTri) * t->triangle_count, L.triangles);
-	if (rc == RB_OK) rc = upload(ctx, ctx->lightBufs, t->bitmasks, sizeof(uint64_t) * t->triangle_count, L.bitmasks);
-	if (rc == RB_OK) rc = upload(ctx, ctx->lightBufs, t->pointers, sizeof(uint32_t) * t->pointer_count, L.pointers);
+	std::vector<void*> fresh;
+	rb::DevLights L{};
+	int rc = upload(ctx, fresh, t->triangles, sizeof(rb::EmissiveTri) * t->triangle_count, L.triangles);
+	if (rc == RB_OK) rc = upload(ctx, fresh, t->bitmasks, sizeof(uint64_t) * t->triangle_count, L.bitmasks);
+	if (rc == RB_OK) rc = upload(ctx, fresh, t->pointers, sizeof(uint32_t) * t->pointer_count, L.pointers);
 	rb::PackedNode* dn = nullptr;
 	rb::TreeNodeU* du = nullptr;
-	if (rc == RB_OK && t->node_count) rc = upload(ctx, ctx->lightBufs, t->nodes, sizeof(rb::PackedNode) * t->node_count, dn);
-	if (rc == RB_OK && t->node_count) rc = upload(ctx, ctx->lightBufs, nullptr, sizeof(rb::TreeNodeU) * t->node_count, du);
-	if (rc != RB_OK) return rc;
-	if (t->node_count)
+	if (rc == RB_OK && t->node_count) rc = upload(ctx, fresh, t->nodes, sizeof(rb::PackedNode) * t->node_count, dn);
+	if (rc == RB_OK && t->node_count) rc = upload(ctx, fresh, nullptr, sizeof(rb::TreeNodeU) * t->node_count, du);
+	if (rc == RB_OK && t->node_count) rb::launchUnpackLightTree(dn, du, t->node_count, ctx->stream);
+	if (rc == RB_OK)
 	{
-		rb::launchUnpackLightTree(dn, du, t->node_count, ctx->stream);
 		const cudaError_t e = cudaStreamSynchronize(ctx->stream);
-		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_set_lights: unpack");
+		if (e != cudaSuccess) rc = cudaFail(ctx, e, "rb_set_lights: upload");
 	}
+	rc = commit(ctx, ctx->lightBufs, fresh, rc);
+	if (rc != RB_OK) return rc;
 	L.nodes = dn;
 	L.unpacked = du;
 	L.nodeCount = t->node_count;
 	L.triangleCount = t->triangle_count;
+	ctx->scene.lights = L;
 	ctx->lightMaxMaterial = 0;
 	const rb::EmissiveTri* lt = static_cast<const rb::EmissiveTri*>(t->triangles);
 	for (uint32_t i = 0; i < t->triangle_count; ++i) ctx->lightMaxMaterial = std::max(ctx->lightMaxMaterial, lt[i].material + 1);
@@ -599,26 +633,31 @@ int rb_set_envmap(rb_ctx* ctx, const float* rgba, uint32_t w, uint32_t h)
 		return fail(ctx, RB_ERR_INVALID, "rb_set_envmap: width and height must be multiples of 4");
 	if (w > 32768 || h > 32768) return fail(ctx, RB_ERR_INVALID, "rb_set_envmap: image larger than 32768");
 	cudaSetDevice(ctx->device);
-	cudaStreamSynchronize(ctx->stream);
-	freeAll(ctx->envBufs);
-	rb::DevEnvMap& E = ctx->scene.env;
-	E = rb::DevEnvMap{};
+	std::vector<void*> fresh;
+	rb::DevEnvMap E{};
 	float4* tex = nullptr;
 	uint16_t *cond = nullptr, *marg = nullptr;
 	float* integral = nullptr;
 	void* scratch = nullptr;
-	int rc = upload(ctx, ctx->envBufs, rgba, sizeof(float4) * w * h, tex);
-	if (rc == RB_OK) rc = upload(ctx, ctx->envBufs, nullptr, sizeof(uint16_t) * w * h, cond);
-	if (rc == RB_OK) rc = upload(ctx, ctx->envBufs, nullptr, sizeof(uint16_t) * h, marg);
-	if (rc == RB_OK) rc = upload(ctx, ctx->envBufs, nullptr, sizeof(float), integral);
-	if (rc == RB_OK) rc = upload(ctx, ctx->envBufs, nullptr, rb_envmap_cdf_scratch_bytes(w, h), scratch);
-	if (rc != RB_OK) return rc;
+	int rc = upload(ctx, fresh, rgba, sizeof(float4) * w * h, tex);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(uint16_t) * w * h, cond);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(uint16_t) * h, marg);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(float), integral);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, rb_envmap_cdf_scratch_bytes(w, h), scratch);
 	// kernel mode 0 is the reference order, 1 the float64 sums
 	const int kmode = ctx->cdfMode == RB_CDF_REFERENCE ? 0 : 1;
-	rc = rb_envmap_cdf(w, h, reinterpret_cast<const float*>(tex), kmode, scratch, cond, marg, integral, ctx->stream);
-	if (rc != RB_OK) return fail(ctx, rc, "rb_set_envmap: CDF build failed");
-	const cudaError_t e = cudaStreamSynchronize(ctx->stream);
-	if (e != cudaSuccess) return cudaFail(ctx, e, "rb_set_envmap");
+	if (rc == RB_OK)
+	{
+		rc = rb_envmap_cdf(w, h, reinterpret_cast<const float*>(tex), kmode, scratch, cond, marg, integral, ctx->stream);
+		if (rc != RB_OK) rc = fail(ctx, rc, "rb_set_envmap: CDF build failed");
+	}
+	if (rc == RB_OK)
+	{
+		const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+		if (e != cudaSuccess) rc = cudaFail(ctx, e, "rb_set_envmap");
+	}
+	rc = commit(ctx, ctx->envBufs, fresh, rc);
+	if (rc != RB_OK) return rc;
 	E.enabled = 1;
 	E.w = w; E.h = h;
 	E.width = static_cast<float>(w); E.height = static_cast<float>(h);
@@ -626,6 +665,7 @@ int rb_set_envmap(rb_ctx* ctx, const float* rgba, uint32_t w, uint32_t h)
 	E.texels = tex;
 	E.conditional = cond;
 	E.marginal = marg;
+	ctx->scene.env = E;
 	ctx->envScratch = scratch;
 	ctx->envIntegral = integral;
 	return RB_OK;

@@ -1,0 +1,168 @@
+"""Edge cases of the rendering path on the GPU, through the C ABI: scenes
+without geometry, lights or environment; a one-pixel film; depth 1;
+degenerate triangles; and the host-side rejections that keep invalid input
+away from the kernels (every rejected call returns a status and leaves the
+context usable). Renders that have an oracle counterpart are compared with
+it like the other render tests."""
+from __future__ import annotations
+
+import copy
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle_lib import RefLib, light_tree_record, load_scene_into_ref, ref_render, reference_luts
+from ratbite_b200 import abi, lighttree, scenes
+from ratbite_b200._native import load
+from ratbite_b200.rendering_interface import RenderingInterface
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def tables():
+    ref = RefLib()
+    return dict(ref=ref, cie=ref.cie_xyz(), basis=ref.basis_rgb(), luts=reference_luts())
+
+
+def _compare(tables, sc, W, H, spp, depth=None):
+    ref = tables["ref"]
+    keep = load_scene_into_ref(ref, sc, tables["luts"], tables["cie"], tables["basis"], width=W, height=H,
+                               max_depth=depth)
+    world, flux, mat, prim = sc.emissive_arrays()
+    lt = None
+    if len(flux):
+        tris, nodes, ptrs, masks = ref.build_light_tree(world, flux, mat, prim)
+        lt = light_tree_record(tris, nodes, ptrs, masks, keep)
+    want = ref_render(ref, W, H, 0, spp)
+    with RenderingInterface(device=0) as ri:
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lt, width=W, height=H,
+                      max_depth=depth)
+        ri.render(0, spp)
+        got = ri.read_accumulation()
+        st = ri.status()
+    assert st.flags == 0
+    assert np.array_equal(got[..., 3], want[..., 3])
+    g = got[..., :3] / np.maximum(got[..., 3:4], 1)
+    w = want[..., :3] / np.maximum(want[..., 3:4], 1)
+    denom = max(np.abs(w).sum(), 1e-30)
+    return g, w, np.abs(g - w).sum() / denom
+
+
+def _no_geometry_scene(with_env=True):
+    sc = scenes.cornell_box(seed=1, width=16, height=16, spp=2)
+    sc.meshes, sc.instances, sc.emissive, sc.materials = [], [], [], [scenes.Material()]
+    if with_env:
+        sc.envmap = scenes.sky_envmap(64, 32, seed=2)
+    return sc
+
+
+def test_environment_only_scene(tables):
+    g, w, l1 = _compare(tables, _no_geometry_scene(), 16, 16, 2)
+    assert w.sum() > 0 and l1 < 1e-5
+
+
+def test_dark_scene_without_lights(tables):
+    sc = scenes.cornell_box(seed=1, width=16, height=16, spp=2)
+    # drop the emitter: no light tree, no environment, nothing emits
+    sc.emissive = []
+    for m in sc.materials:
+        m.emissive = None
+    with RenderingInterface(device=0) as ri:
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"])
+        ri.render(0, 3)
+        got = ri.read_accumulation()
+        assert ri.status().flags == 0
+    assert np.all(got[..., :3] == 0.0) and np.all(got[..., 3] == 3.0)
+
+
+def test_one_pixel_film_and_depth_one(tables):
+    sc = scenes.cornell_box(seed=1, width=1, height=1, spp=16)
+    g, w, l1 = _compare(tables, sc, 1, 1, 16)
+    assert l1 < 1e-4
+    sc = scenes.cornell_box(seed=1, width=24, height=24, spp=4, max_depth=1)
+    g, w, l1 = _compare(tables, sc, 24, 24, 4, depth=1)
+    assert l1 < 1e-4
+
+
+def test_degenerate_triangles_are_skipped(tables):
+    sc = scenes.cornell_box(seed=1, width=24, height=24, spp=4)
+    sc = copy.copy(sc)
+    sm = sc.meshes[0][0]
+    v = np.concatenate([sm.vertices, sm.vertices[:1], sm.vertices[:1]]).astype(np.float32)
+    n = len(sm.vertices)
+    idx = np.concatenate([sm.indices, np.array([[0, n, n + 1], [1, 1, 2]], sm.indices.dtype)])
+    sc.meshes = [list(m) for m in sc.meshes]
+    sc.meshes[0][0] = scenes.Submesh(v, idx, sm.material, sm.normals, list(sm.discarded))
+    sc._keep = []
+    g, w, l1 = _compare(tables, sc, 24, 24, 4)
+    assert l1 < 1e-4
+
+
+# ------------------------------------------------------ host-side rejections
+def _context(tables):
+    sc = scenes.cornell_box(seed=1, width=16, height=16, spp=1)
+    ri = RenderingInterface(device=0)
+    ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(sc))
+    return sc, ri
+
+
+def test_rejections_leave_the_context_usable(tables):
+    lib = load()
+    sc, ri = _context(tables)
+    ctx = ri.ctx
+    # render before anything is set
+    empty = C.c_void_p()
+    assert lib.rb_create(None, C.byref(empty)) == 0
+    assert lib.rb_render(empty, 0, 1, None) == abi.RB_ERR_NO_SCENE
+    assert lib.rb_resolve(empty, np.zeros(9, np.float32).ctypes.data, 1.0, None) == abi.RB_ERR_NO_SCENE
+    lib.rb_destroy(empty)
+    # launch parameters: empty film, depth above 64
+    bad = sc.launch_record()
+    bad.width = 0
+    assert lib.rb_set_launch(ctx, C.byref(bad)) == abi.RB_ERR_INVALID
+    bad = sc.launch_record()
+    bad.max_path_depth = 65
+    assert lib.rb_set_launch(ctx, C.byref(bad)) == abi.RB_ERR_INVALID
+    # material table smaller than the geometry's references: rb_render refuses
+    mats = sc.material_records()
+    assert lib.rb_set_materials(ctx, C.cast(mats, C.c_void_p), 2) == 0
+    assert lib.rb_render(ctx, 0, 1, None) == abi.RB_ERR_INVALID
+    assert lib.rb_set_materials(ctx, C.cast(mats, C.c_void_p), len(mats)) == 0
+    # textured material, unknown BxDF
+    m1 = (abi.rb_material * 1).from_buffer_copy(bytes(mats)[:C.sizeof(abi.rb_material)])
+    m1[0].textures = 1
+    assert lib.rb_set_materials(ctx, C.cast(m1, C.c_void_p), 1) == abi.RB_ERR_UNSUPPORTED
+    m1[0].textures = 0
+    m1[0].bxdf = 7
+    assert lib.rb_set_materials(ctx, C.cast(m1, C.c_void_p), 1) == abi.RB_ERR_INVALID
+    # light tree whose child index points outside the node array
+    world, flux, mat, prim = sc.emissive_arrays()
+    tris, nodes, ptrs, masks = lighttree.build(world, flux, mat, prim)
+    keep = []
+    nodes = nodes.copy()
+    if len(nodes) > 1:
+        nodes["core"][0] = len(nodes) + 5
+    else:
+        nodes["core"][0] = (1 << 31) | (15 << 27)
+    lt = light_tree_record(tris, nodes, ptrs, masks, keep)
+    assert lib.rb_set_lights(ctx, C.byref(lt)) == abi.RB_ERR_INVALID
+    # non-finite vertex
+    g = copy.copy(sc)
+    sm = g.meshes[0][0]
+    v = sm.vertices.copy()
+    v[0, 0] = np.inf
+    g.meshes = [list(m) for m in g.meshes]
+    g.meshes[0][0] = scenes.Submesh(v, sm.indices, sm.material, sm.normals, list(sm.discarded))
+    g._keep = []
+    assert lib.rb_set_geometry(ctx, C.byref(g.geometry_record())) == abi.RB_ERR_INVALID
+    # environment map sizes
+    img = np.ones((6, 6, 4), np.float32)
+    assert lib.rb_set_envmap(ctx, img.ctypes.data, 6, 6) == abi.RB_ERR_INVALID
+    # the context still renders the original scene
+    ri.render(0, 2)
+    acc = ri.read_accumulation()
+    assert np.all(acc[..., 3] == 2.0) and acc[..., :3].sum() > 0
+    assert ri.status().flags == 0
+    ri.cleanup()
