@@ -338,7 +338,7 @@ typedef struct rb_render_stats {
     /* the shading stage per kernel: ms_shade = ms_surface + ms_nee + ms_bsdf
      * (hit record, emission and frame; light sample; BxDF and next ray) */
     double ms_surface, ms_nee, ms_bsdf;
-    uint32_t launches_nee, launches_bsdf;   /* launches_shade counts the surface kernel */
+    uint32_t launches_nee, launches_bsdf;   /* launches_shade counts the surface and deferred-emission kernels */
     uint64_t surface_records;               /* path vertices shaded (RB_STATS_COUNT) */
 } rb_render_stats;
 int rb_set_stats(rb_ctx* ctx, uint32_t mode);

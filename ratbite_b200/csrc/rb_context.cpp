@@ -240,6 +240,8 @@ int ensureWave(rb_ctx* ctx, uint32_t paths)
 	alloc(s.sfT, sizeof(float4)); alloc(s.sfB, sizeof(float4));
 	alloc(s.queue[0], sizeof(uint32_t)); alloc(s.queue[1], sizeof(uint32_t)); alloc(s.shadowQueue, sizeof(uint32_t));
 	alloc(s.surfQueue, sizeof(uint32_t));
+	alloc(s.emQueue, sizeof(uint32_t)); alloc(s.emA, sizeof(float4)); alloc(s.emB, sizeof(float4));
+	alloc(s.emC, sizeof(float4)); alloc(s.emLight, sizeof(uint32_t));
 	if (rc == RB_OK)
 		rc = upload(ctx, ctx->soaBufs, nullptr, sizeof(uint32_t) * rb::kCountSlots, s.counts);
 	if (rc != RB_OK) { releaseWave(ctx); return rc; }
@@ -757,6 +759,7 @@ int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 		{
 			timedStage(ctx, 1, st, [&] { rb::launchExtend(sc, ctx->soa, b, ctx->shape, st, cnt); });
 			timedStage(ctx, 2, st, [&] { rb::launchSurface(sc, ctx->soa, w, b, ctx->shape, st, cnt); });
+			timedStage(ctx, 2, st, [&] { rb::launchEmission(sc, ctx->soa, b, ctx->shape, st); });
 			timedStage(ctx, 5, st, [&] { rb::launchNee(sc, ctx->soa, w, b, ctx->shape, st); });
 			timedStage(ctx, 6, st, [&] { rb::launchBsdf(sc, ctx->soa, w, b, ctx->shape, st); });
 			timedStage(ctx, 3, st, [&] { rb::launchShadow(sc, ctx->soa, b, ctx->shape, st, cnt); });

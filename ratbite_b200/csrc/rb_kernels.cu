@@ -337,7 +337,12 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 		{
 			const S4 lambda = s4(s.lambda[p]);
 			const bool prevNee = depth != 0 && !(flags & PF_PREVIOUS_HIT_SPECULAR);
-			const float treePdf = prevNee ? lightTreePdf(sc, it.lightType, it.lightIndex, rayO, lastNormal) : 1.0f;
+			// The light-tree pdf of an emitter hit replays ~2 SG importances
+			// per tree level; few lanes need it, so it is deferred to kEmission
+			// over a compacted queue. The sky's tree pdf is a constant.
+			const bool deferTree = prevNee && it.lightType == kLightTypeTriangle;
+			const float treePdf = prevNee && !deferTree ? lightTreePdf(sc, it.lightType, it.lightIndex, rayO, lastNormal)
+				: 1.0f;
 			float lightPdf = 0.0f;
 			S4 Le = s4(0.0f);
 			bool noEmission = false;
@@ -365,7 +370,16 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 					noEmission = true;
 				flags |= PF_FINISHED;
 			}
-			if (!noEmission)
+			if (!noEmission && deferTree)
+			{
+				const uint32_t slot = appendIndex(s.counts + kEmissionCounts + bounce);
+				s.emQueue[slot] = p;
+				s.emA[slot] = f4_of(rayO, bxdfPdf);
+				s.emB[slot] = f4_of(lastNormal, lightPdf);
+				s.emC[slot] = f4(Le);
+				s.emLight[slot] = it.lightIndex;
+			}
+			else if (!noEmission)
 			{
 				lightPdf *= treePdf;
 				const float wgt = prevNee ? powerHeuristic(bxdfPdf, lightPdf) : 1.0f;
@@ -398,6 +412,27 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 		s.fd[p] = make_uint2(flags, depth);
 	}
 	if (counters) warpAdd(counters + 6, records);
+}
+
+// Emission MIS of emitter hits whose previous vertex sampled a light
+// (pathtrace.cu:1185-1274): the light-tree pdf of the hit light replayed from
+// the previous vertex, the power heuristic, and the contribution, with the
+// values kSurface queued for it; the same arithmetic as the inline case.
+__global__ void __launch_bounds__(kThreads) kEmission(DevScene sc, PathSoA s, int bounce)
+{
+	const uint32_t n = s.counts[kEmissionCounts + bounce];
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const uint32_t p = s.emQueue[i];
+		const float4 a = s.emA[i], b = s.emB[i];
+		const float treePdf = lightTreePdf(sc, kLightTypeTriangle, s.emLight[i], f3_of(a), f3_of(b));
+		float lightPdf = b.w;
+		lightPdf *= treePdf;
+		const float wgt = powerHeuristic(a.w, lightPdf);
+		S4 L = s4(s.L[p]);
+		L += s4(s.T[p]) * s4(s.emC[i]) * wgt;
+		s.L[p] = f4(L);
+	}
 }
 
 // Stage 2 of shading: the light sample (pathtrace.cu:1572-1721) for every
@@ -795,6 +830,7 @@ LaunchShape queryLaunchShape()
 	ls.blocksGenerate = occ(reinterpret_cast<const void*>(kGenerate));
 	ls.blocksSurface = occ(reinterpret_cast<const void*>(kSurface));
 	ls.blocksNee = occ(reinterpret_cast<const void*>(kNee<false>));
+	ls.blocksEmission = occ(reinterpret_cast<const void*>(kEmission));
 	cudaFuncSetAttribute(reinterpret_cast<const void*>(kNee<true>), cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(kNeeSharedMaxBytes));
 	ls.blocksBsdf = occ(reinterpret_cast<const void*>(kBsdf));
@@ -811,6 +847,10 @@ void launchSurface(const DevScene& sc, const PathSoA& s, const WaveParams& w, in
 	unsigned long long* counters)
 {
 	kSurface<<<ls.blocksSurface, kThreads, 0, st>>>(sc, s, w, bounce, counters);
+}
+void launchEmission(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st)
+{
+	kEmission<<<ls.blocksEmission, kThreads, 0, st>>>(sc, s, bounce);
 }
 void launchNee(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
 {

@@ -34,6 +34,14 @@ struct PathSoA
 	float4* sfB;       // shading frame bitangent
 	uint32_t* queue[2];// active path slots, ping-pong by bounce parity
 	uint32_t* surfQueue;   // paths with a surface record this bounce
+	// emitter hits whose MIS weight needs the light-tree pdf (kEmission),
+	// indexed by queue position: path, (previous origin, BxDF pdf),
+	// (previous normal, area pdf), emitted spectrum, light index
+	uint32_t* emQueue;
+	float4* emA;
+	float4* emB;
+	float4* emC;
+	uint32_t* emLight;
 	uint32_t* shadowQueue;
 	uint32_t* counts;  // kCountSlots words: see kShadowCounts, kSurfaceCounts
 	uint32_t capacity;
@@ -42,12 +50,14 @@ constexpr int kMaxBounces = 64;
 // counts[b]: paths entering bounce b; counts[kShadowCounts + b]: shadow rays
 // of bounce b; counts[kSurfaceCounts + b]: surface records of bounce b;
 // counts[kExtendFetch + b], counts[kShadowFetch + b]: work counters from
-// which the persistent traversal warps take their next rays.
+// which the persistent traversal warps take their next rays;
+// counts[kEmissionCounts + b]: deferred emission-MIS records of bounce b.
 constexpr uint32_t kShadowCounts = kMaxBounces + 1;
 constexpr uint32_t kSurfaceCounts = 2 * (kMaxBounces + 1);
 constexpr uint32_t kExtendFetch = 3 * (kMaxBounces + 1);
 constexpr uint32_t kShadowFetch = 4 * (kMaxBounces + 1);
-constexpr uint32_t kCountSlots = 5 * (kMaxBounces + 1);
+constexpr uint32_t kEmissionCounts = 5 * (kMaxBounces + 1);
+constexpr uint32_t kCountSlots = 6 * (kMaxBounces + 1);
 
 struct WaveParams
 {
@@ -60,7 +70,7 @@ struct WaveParams
 struct LaunchShape
 {
 	int smCount;
-	int blocksGenerate, blocksExtend, blocksSurface, blocksNee, blocksBsdf, blocksShadow, blocksResolve;
+	int blocksGenerate, blocksExtend, blocksSurface, blocksEmission, blocksNee, blocksBsdf, blocksShadow, blocksResolve;
 	int threads;
 };
 
@@ -73,6 +83,7 @@ void launchExtend(const DevScene& sc, const PathSoA& s, int bounce, const Launch
 // The shading stage as three kernels: surface record, light sample, BxDF.
 void launchSurface(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st,
 	unsigned long long* counters);
+void launchEmission(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st);
 void launchNee(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st);
 void launchBsdf(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st);
 // Resolve + AgX tonemap of the accumulation into width*height RGBA8 words
