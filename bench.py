@@ -361,8 +361,8 @@ def run_ours(args, rank: int, world: int, wl: dict):
                        "triangles": scene.triangle_count(), "emitters": int(sum(len(e["prim"]) for e in scene.emissive)),
                        "materials": len(scene.materials), "envmap": list(scene.envmap.shape[1::-1]) if has_env else None,
                        "paths_per_step": paths_per_step, "parallelism": f"sample-range x{world}",
-                       "l2": "inputs larger than L2 (wavefront path state 336 B per path in flight, "
-                             "~5.6 GB at the default 16M paths per wave)",
+                       "l2": "inputs larger than L2 (wavefront path state 344 B per path in flight, "
+                             "~5.8 GB at the default 16M paths per wave)",
                        "setup_s": setup_s},
             "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": C.sizeof(launch),
                     "d2h_bytes_per_step": W * H * 32, "steps": e2e_steps},

@@ -240,6 +240,7 @@ int ensureWave(rb_ctx* ctx, uint32_t paths)
 	alloc(s.sfT, sizeof(float4)); alloc(s.sfB, sizeof(float4));
 	alloc(s.queue[0], sizeof(uint32_t)); alloc(s.queue[1], sizeof(uint32_t)); alloc(s.shadowQueue, sizeof(uint32_t));
 	alloc(s.surfQueue, sizeof(uint32_t));
+	alloc(s.neeQueue[0], sizeof(uint32_t)); alloc(s.neeQueue[1], sizeof(uint32_t));
 	alloc(s.emQueue, sizeof(uint32_t)); alloc(s.emA, sizeof(float4)); alloc(s.emB, sizeof(float4));
 	alloc(s.emC, sizeof(float4)); alloc(s.emLight, sizeof(uint32_t));
 	if (rc == RB_OK)
@@ -761,6 +762,7 @@ int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 			timedStage(ctx, 2, st, [&] { rb::launchSurface(sc, ctx->soa, w, b, ctx->shape, st, cnt); });
 			timedStage(ctx, 2, st, [&] { rb::launchEmission(sc, ctx->soa, b, ctx->shape, st); });
 			timedStage(ctx, 5, st, [&] { rb::launchNee(sc, ctx->soa, w, b, ctx->shape, st); });
+			ctx->launches[5] += 2;   // launchNee runs the pick kernel and two light-sample kernels
 			timedStage(ctx, 6, st, [&] { rb::launchBsdf(sc, ctx->soa, w, b, ctx->shape, st); });
 			timedStage(ctx, 3, st, [&] { rb::launchShadow(sc, ctx->soa, b, ctx->shape, st, cnt); });
 		}

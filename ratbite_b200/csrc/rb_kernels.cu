@@ -435,18 +435,49 @@ __global__ void __launch_bounds__(kThreads) kEmission(DevScene sc, PathSoA s, in
 	}
 }
 
+// Sorts the surface records that need a light sample by the light choice
+// of sampleLightTree (pathtrace.cu:1064-1076): records that pick the
+// environment (and all records when neither the tree nor the environment
+// exists) go to queue 1, tree picks to queue 0. The choice uses the same
+// sample dimension and comparison as the light-sample body that follows.
+__global__ void __launch_bounds__(kThreads) kNeePick(DevScene sc, PathSoA s, WaveParams w, int bounce)
+{
+	const uint32_t n = s.counts[kSurfaceCounts + bounce];
+	const bool envPresent = sc.env.enabled != 0;
+	const bool treePresent = sc.lights.nodes != nullptr;
+	const float envImp = envPresent ? (treePresent ? kEnvMapImportance : 1.0f) : 0.0f;
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const uint32_t p = s.surfQueue[i];
+		if (__float_as_uint(s.sfPi[p].w) & kSfSkipped) continue;
+		bool sky = true;
+		if (envPresent || treePresent)
+		{
+			const Qrng q = pathQrng(sc, w, p, s.fd[p].y);
+			sky = sample3D(q, DIM_LIGHT).z < envImp;
+		}
+		// one counter per branch: appendIndex aggregates over the lanes active at the call
+		if (sky) s.neeQueue[1][appendIndex(s.counts + kNeeSkyCounts + bounce)] = p;
+		else s.neeQueue[0][appendIndex(s.counts + kNeeTreeCounts + bounce)] = p;
+	}
+}
+
 // Stage 2 of shading: the light sample (pathtrace.cu:1572-1721) for every
 // surface that is not skipped: pick a light from the light tree (held in the
 // read-only cache: it is read by every thread) or the environment, sample a
 // point on it and write the shadow ray and the light sample.
 // SHARED: the block first copies the unpacked tree into shared memory
 // (dynamic, nodeCount x 48 B) and descends it there; used when the tree fits.
+// The records come from one of kNeePick's queues (`which`: 0 tree picks,
+// 1 environment picks), so a warp's lanes take the same branch of the light
+// choice; the body is the same for both.
 template<bool SHARED>
 __global__ void __launch_bounds__(SHARED ? kNeeSharedThreads : kThreads, SHARED ? 2 : RB_NEE_MIN_BLOCKS)
-kNee(DevScene sc, PathSoA s, WaveParams w, int bounce)
+kNee(DevScene sc, PathSoA s, WaveParams w, int bounce, int which)
 {
 	extern __shared__ float4 sharedTree[];
-	const uint32_t n = s.counts[kSurfaceCounts + bounce];
+	const uint32_t n = s.counts[(which ? kNeeSkyCounts : kNeeTreeCounts) + bounce];
+	const uint32_t* queue = s.neeQueue[which];
 	const TreeNodeU* nodes = sc.lights.unpacked;
 	if (SHARED)
 	{
@@ -460,10 +491,9 @@ kNee(DevScene sc, PathSoA s, WaveParams w, int bounce)
 	const bool treePresent = sc.lights.nodes != nullptr;
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
-		const uint32_t p = s.surfQueue[i];
+		const uint32_t p = queue[i];
 		const float4 pi = s.sfPi[p];
 		uint32_t bits = __float_as_uint(pi.w);
-		if (bits & kSfSkipped) continue;
 		const float4 hp = s.sfP[p];
 		const f3 hitPos = f3_of(hp), hitPosInterp = f3_of(pi), gn = f3_of(s.sfGn[p]), sn = f3_of(s.nrm[p]);
 		f3 dir = mk(0.0f), shadowO = mk(0.0f);
@@ -831,6 +861,7 @@ LaunchShape queryLaunchShape()
 	ls.blocksSurface = occ(reinterpret_cast<const void*>(kSurface));
 	ls.blocksNee = occ(reinterpret_cast<const void*>(kNee<false>));
 	ls.blocksEmission = occ(reinterpret_cast<const void*>(kEmission));
+	ls.blocksNeePick = occ(reinterpret_cast<const void*>(kNeePick));
 	cudaFuncSetAttribute(reinterpret_cast<const void*>(kNee<true>), cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(kNeeSharedMaxBytes));
 	ls.blocksBsdf = occ(reinterpret_cast<const void*>(kBsdf));
@@ -854,18 +885,20 @@ void launchEmission(const DevScene& sc, const PathSoA& s, int bounce, const Laun
 }
 void launchNee(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
 {
+	kNeePick<<<ls.blocksNeePick, kThreads, 0, st>>>(sc, s, w, bounce);
 	const size_t treeBytes = sizeof(TreeNodeU) * sc.lights.nodeCount;
 	if (sc.lights.unpacked && treeBytes <= kNeeSharedMaxBytes)
 	{
 		int b = 0;
 		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, reinterpret_cast<const void*>(kNee<true>), kNeeSharedThreads,
 			treeBytes);
-		kNee<true><<<(b < 1 ? 1 : b) * ls.smCount, kNeeSharedThreads, treeBytes, st>>>(sc, s, w, bounce);
+		kNee<true><<<(b < 1 ? 1 : b) * ls.smCount, kNeeSharedThreads, treeBytes, st>>>(sc, s, w, bounce, 0);
 	}
 	else
 	{
-		kNee<false><<<ls.blocksNee, kThreads, 0, st>>>(sc, s, w, bounce);
+		kNee<false><<<ls.blocksNee, kThreads, 0, st>>>(sc, s, w, bounce, 0);
 	}
+	kNee<false><<<ls.blocksNee, kThreads, 0, st>>>(sc, s, w, bounce, 1);
 }
 void launchBsdf(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
 {

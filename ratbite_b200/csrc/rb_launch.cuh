@@ -12,7 +12,9 @@ constexpr int kThreads = 128;
 RB_D uint32_t gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 RB_D uint32_t gstride() { return gridDim.x * blockDim.x; }
 
-// Warp-aggregated append: one atomic per warp for the lanes that push.
+// Warp-aggregated append: one atomic per warp for the lanes that push. Every
+// lane active at the call must append to the same counter (call it inside
+// the branch that selects the counter).
 RB_D uint32_t appendIndex(uint32_t* counter)
 {
 	const uint32_t active = __activemask();

@@ -37,6 +37,7 @@ struct PathSoA
 	// emitter hits whose MIS weight needs the light-tree pdf (kEmission),
 	// indexed by queue position: path, (previous origin, BxDF pdf),
 	// (previous normal, area pdf), emitted spectrum, light index
+	uint32_t* neeQueue[2]; // light-sample records by light choice: tree picks, environment picks
 	uint32_t* emQueue;
 	float4* emA;
 	float4* emB;
@@ -51,13 +52,17 @@ constexpr int kMaxBounces = 64;
 // of bounce b; counts[kSurfaceCounts + b]: surface records of bounce b;
 // counts[kExtendFetch + b], counts[kShadowFetch + b]: work counters from
 // which the persistent traversal warps take their next rays;
-// counts[kEmissionCounts + b]: deferred emission-MIS records of bounce b.
+// counts[kEmissionCounts + b]: deferred emission-MIS records of bounce b;
+// counts[kNeeTreeCounts + b], counts[kNeeSkyCounts + b]: light-sample records
+// by light choice.
 constexpr uint32_t kShadowCounts = kMaxBounces + 1;
 constexpr uint32_t kSurfaceCounts = 2 * (kMaxBounces + 1);
 constexpr uint32_t kExtendFetch = 3 * (kMaxBounces + 1);
 constexpr uint32_t kShadowFetch = 4 * (kMaxBounces + 1);
 constexpr uint32_t kEmissionCounts = 5 * (kMaxBounces + 1);
-constexpr uint32_t kCountSlots = 6 * (kMaxBounces + 1);
+constexpr uint32_t kNeeTreeCounts = 6 * (kMaxBounces + 1);
+constexpr uint32_t kNeeSkyCounts = 7 * (kMaxBounces + 1);
+constexpr uint32_t kCountSlots = 8 * (kMaxBounces + 1);
 
 struct WaveParams
 {
@@ -70,7 +75,8 @@ struct WaveParams
 struct LaunchShape
 {
 	int smCount;
-	int blocksGenerate, blocksExtend, blocksSurface, blocksEmission, blocksNee, blocksBsdf, blocksShadow, blocksResolve;
+	int blocksGenerate, blocksExtend, blocksSurface, blocksEmission, blocksNeePick, blocksNee, blocksBsdf, blocksShadow,
+		blocksResolve;
 	int threads;
 };
 
