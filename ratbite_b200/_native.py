@@ -65,6 +65,15 @@ SIGNATURES = {
     "rb_envmap_cdf_scratch_bytes": (C.c_size_t, [_U32, _U32]),
     "rb_envmap_cdf": (C.c_int, [_U32, _U32, _P, C.c_int, _P, _P, _P, _P, _P]),
     "rb_envmap_cdf_noalloc": (C.c_int, [_U32, _U32, _P, C.c_int, _P, _P, _P, _P]),
+    "rb_nrc_create": (C.c_int, [C.POINTER(abi.rb_nrc_config), C.POINTER(_P)]),
+    "rb_nrc_destroy": (C.c_int, [_P]),
+    "rb_nrc_grid_size": (C.c_size_t, []),
+    "rb_nrc_weight_count": (C.c_size_t, []),
+    "rb_nrc_set_parameters": (C.c_int, [_P, _P, _P]),
+    "rb_nrc_get_parameters": (C.c_int, [_P, _P, _P]),
+    "rb_nrc_infer": (C.c_int, [_P, _U32, _P, _P, _P]),
+    "rb_nrc_train": (C.c_int, [_P, _U32, _P, _P, _P, _P]),
+    "rb_nrc_gradients": (C.c_int, [_P, _U32, _P, _P, _P, _P]),
 }
 
 _lib = None

@@ -222,3 +222,11 @@ def packed_node_dtype():
     import numpy as np
     return np.dtype([("mean", "<f4", 3), ("variance", "<f4"), ("direction", "<u4"),
                      ("sharpness", "<f4"), ("flux", "<f4"), ("core", "<u4")])
+
+
+NRC_INPUTS = 10
+
+
+class rb_nrc_config(C.Structure):
+    _fields_ = [("device", C.c_int32), ("seed", C.c_uint32), ("learning_rate", C.c_float), ("beta1", C.c_float),
+                ("beta2", C.c_float), ("epsilon", C.c_float), ("reserved", C.c_uint32 * 2)]

@@ -1,0 +1,677 @@
+// Neural radiance cache: multiresolution hash-grid encoding and a 4 x 64
+// MLP, trained online on radiance estimates the renderer produces.
+//
+// Encoding (Mueller et al. 2022): 16 levels, 2 features per level, 2^19
+// entries per level (FP16 table, FP32 master copy for the optimiser);
+// resolutions grow geometrically from 16 to 2048; a level whose dense grid
+// fits the table is indexed densely, the others by the spatial hash
+// x * 1 ^ y * 2654435761 ^ z * 805459861. Features are trilinear in the cell.
+// Network input (64): 32 grid features, direction and normal mapped to
+// [0, 1], the normalised hero wavelength, a constant 1, zero padding. Four
+// hidden layers of 64 with ReLU, a linear output of 4 (radiance at the four
+// hero wavelengths). No biases except through the constant input.
+//
+// Tensor cores: the fused forward kernel keeps a 16-row tile of activations
+// in registers as mma.sync m16n8k16 BF16 fragments (FP32 accumulation); an
+// accumulator fragment of one layer is repacked in registers into the A
+// fragment of the next. The fused backward kernel chains dX = dY W the same
+// way with the transposed weights; the weight gradients dW = dY^T X over the
+// batch are plain GEMMs (cuBLAS). Adam runs in FP32 on the master copies.
+
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include <cublas_v2.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "rb_launch.cuh"
+#include "ratbite_b200_nrc.h"
+
+namespace rb
+{
+namespace nrc
+{
+constexpr int kLevels = 16, kFeat = 2, kLog2T = 19, kTable = 1 << kLog2T;
+constexpr int kIn = 64, kH = 64, kOutPad = 16;
+constexpr int kGridFeatures = kLevels * kFeat;          // 32
+// offset of W_l in the packed weights: W0..W3 are 64 x 64, W4 is 16 x 64
+__host__ __device__ constexpr int wOffset(int l) { return l < 5 ? l * kH * kH : 4 * kH * kH + kOutPad * kH; }
+constexpr int kWTotal = wOffset(5);                     // 17408 weights
+constexpr int kWStride = 72;                            // smem row stride (bf16), conflict-free fragment loads
+constexpr int kTile = 16;                               // rows per warp tile
+
+struct Resolutions { float s[kLevels]; uint32_t dense[kLevels]; uint32_t side[kLevels]; };
+
+RB_D uint32_t cellIndex(const Resolutions& R, int l, uint32_t x, uint32_t y, uint32_t z)
+{
+	if (R.dense[l]) return x + R.side[l] * (y + R.side[l] * z);
+	return (x * 1u ^ y * 2654435761u ^ z * 805459861u) & (kTable - 1u);
+}
+
+// ---------------------------------------------------------------- encoding
+__global__ void kEncode(uint32_t n, const float* __restrict__ in, const __half2* __restrict__ grid, Resolutions R,
+	__nv_bfloat16* __restrict__ X)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const float* v = in + static_cast<size_t>(kNrcInputs) * i;
+		__nv_bfloat16* row = X + static_cast<size_t>(kIn) * i;
+		const float px = fminf(fmaxf(v[0], 0.0f), 1.0f), py = fminf(fmaxf(v[1], 0.0f), 1.0f),
+			pz = fminf(fmaxf(v[2], 0.0f), 1.0f);
+		for (int l = 0; l < kLevels; ++l)
+		{
+			const float sx = px * R.s[l], sy = py * R.s[l], sz = pz * R.s[l];
+			const float fx = floorf(sx), fy = floorf(sy), fz = floorf(sz);
+			const float wx = sx - fx, wy = sy - fy, wz = sz - fz;
+			const uint32_t cx = static_cast<uint32_t>(fx), cy = static_cast<uint32_t>(fy), cz = static_cast<uint32_t>(fz);
+			float f0 = 0.0f, f1 = 0.0f;
+			for (int c = 0; c < 8; ++c)
+			{
+				const uint32_t dx = c & 1u, dy = (c >> 1) & 1u, dz = (c >> 2) & 1u;
+				const float w = (dx ? wx : 1.0f - wx) * (dy ? wy : 1.0f - wy) * (dz ? wz : 1.0f - wz);
+				const float2 e = __half22float2(grid[static_cast<size_t>(l) * kTable + cellIndex(R, l, cx + dx, cy + dy, cz + dz)]);
+				f0 += w * e.x;
+				f1 += w * e.y;
+			}
+			row[2 * l] = __float2bfloat16_rn(f0);
+			row[2 * l + 1] = __float2bfloat16_rn(f1);
+		}
+		row[32] = __float2bfloat16_rn(v[3] * 0.5f + 0.5f);
+		row[33] = __float2bfloat16_rn(v[4] * 0.5f + 0.5f);
+		row[34] = __float2bfloat16_rn(v[5] * 0.5f + 0.5f);
+		row[35] = __float2bfloat16_rn(v[6] * 0.5f + 0.5f);
+		row[36] = __float2bfloat16_rn(v[7] * 0.5f + 0.5f);
+		row[37] = __float2bfloat16_rn(v[8] * 0.5f + 0.5f);
+		row[38] = __float2bfloat16_rn(v[9]);
+		row[39] = __float2bfloat16_rn(1.0f);
+		for (int k = 40; k < kIn; ++k) row[k] = __float2bfloat16_rn(0.0f);
+	}
+}
+
+// Scatters the gradient of the 32 grid features into the FP32 gradient table.
+__global__ void kEncodeBackward(uint32_t n, const float* __restrict__ in, const float* __restrict__ dX0, Resolutions R,
+	float* __restrict__ gridGrad)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const float* v = in + static_cast<size_t>(kNrcInputs) * i;
+		const float* g = dX0 + static_cast<size_t>(kGridFeatures) * i;
+		const float px = fminf(fmaxf(v[0], 0.0f), 1.0f), py = fminf(fmaxf(v[1], 0.0f), 1.0f),
+			pz = fminf(fmaxf(v[2], 0.0f), 1.0f);
+		for (int l = 0; l < kLevels; ++l)
+		{
+			const float g0 = g[2 * l], g1 = g[2 * l + 1];
+			if (g0 == 0.0f && g1 == 0.0f) continue;
+			const float sx = px * R.s[l], sy = py * R.s[l], sz = pz * R.s[l];
+			const float fx = floorf(sx), fy = floorf(sy), fz = floorf(sz);
+			const float wx = sx - fx, wy = sy - fy, wz = sz - fz;
+			const uint32_t cx = static_cast<uint32_t>(fx), cy = static_cast<uint32_t>(fy), cz = static_cast<uint32_t>(fz);
+			for (int c = 0; c < 8; ++c)
+			{
+				const uint32_t dx = c & 1u, dy = (c >> 1) & 1u, dz = (c >> 2) & 1u;
+				const float w = (dx ? wx : 1.0f - wx) * (dy ? wy : 1.0f - wy) * (dz ? wz : 1.0f - wz);
+				float* e = gridGrad + 2 * (static_cast<size_t>(l) * kTable + cellIndex(R, l, cx + dx, cy + dy, cz + dz));
+				atomicAdd(e, w * g0);
+				atomicAdd(e + 1, w * g1);
+			}
+		}
+	}
+}
+
+// ---------------------------------------------------------------- MLP tiles
+RB_D uint32_t pack2(float lo, float hi)
+{
+	const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+	return *reinterpret_cast<const uint32_t*>(&h);
+}
+RB_D float2 unpack2(uint32_t v)
+{
+	const __nv_bfloat162 h = *reinterpret_cast<const __nv_bfloat162*>(&v);
+	return __bfloat1622float2(h);
+}
+RB_D void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+{
+	asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+		"{%0,%1,%2,%3};\n"
+		: "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+		: "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// One layer on a 16-row tile: C[16 x 8*NT] = A[16 x 64] x W^T, W in smem as
+// [out][in] rows of kWStride bf16. A: 4 k-tiles of fragments.
+template<int NT>
+RB_D void layer(const uint32_t (&A)[4][4], const __nv_bfloat16* W, float (&C)[NT][4])
+{
+	const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, c = lane & 3u;
+#pragma unroll
+	for (int j = 0; j < NT; ++j)
+	{
+		C[j][0] = C[j][1] = C[j][2] = C[j][3] = 0.0f;
+		const __nv_bfloat16* wr = W + (8 * j + g) * kWStride;
+#pragma unroll
+		for (int t = 0; t < 4; ++t)
+		{
+			const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wr + 16 * t + 2 * c);
+			const uint32_t b1 = *reinterpret_cast<const uint32_t*>(wr + 16 * t + 8 + 2 * c);
+			mma16816(C[j], A[t], b0, b1);
+		}
+	}
+}
+// Accumulator fragments of 8 n-tiles -> A fragments of the next layer, with ReLU.
+RB_D void toA(const float (&C)[8][4], uint32_t (&A)[4][4], bool relu)
+{
+#pragma unroll
+	for (int t = 0; t < 4; ++t)
+	{
+		const float* a = C[2 * t];
+		const float* b = C[2 * t + 1];
+		auto r = [relu](float x) { return relu ? fmaxf(x, 0.0f) : x; };
+		A[t][0] = pack2(r(a[0]), r(a[1]));
+		A[t][1] = pack2(r(a[2]), r(a[3]));
+		A[t][2] = pack2(r(b[0]), r(b[1]));
+		A[t][3] = pack2(r(b[2]), r(b[3]));
+	}
+}
+// A fragments of rows r0..r0+15 of a row-major [rows][64] bf16 array.
+RB_D void loadA(const __nv_bfloat16* X, uint32_t r0, uint32_t rows, uint32_t (&A)[4][4])
+{
+	const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, c = lane & 3u;
+	const uint32_t ra = r0 + g, rb = r0 + g + 8;
+#pragma unroll
+	for (int t = 0; t < 4; ++t)
+	{
+		const uint32_t k0 = 16 * t + 2 * c;
+		A[t][0] = ra < rows ? *reinterpret_cast<const uint32_t*>(X + static_cast<size_t>(ra) * kIn + k0) : 0u;
+		A[t][1] = rb < rows ? *reinterpret_cast<const uint32_t*>(X + static_cast<size_t>(rb) * kIn + k0) : 0u;
+		A[t][2] = ra < rows ? *reinterpret_cast<const uint32_t*>(X + static_cast<size_t>(ra) * kIn + k0 + 8) : 0u;
+		A[t][3] = rb < rows ? *reinterpret_cast<const uint32_t*>(X + static_cast<size_t>(rb) * kIn + k0 + 8) : 0u;
+	}
+}
+RB_D void storeA(__nv_bfloat16* Y, uint32_t r0, uint32_t rows, const uint32_t (&A)[4][4])
+{
+	const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, c = lane & 3u;
+	const uint32_t ra = r0 + g, rb = r0 + g + 8;
+#pragma unroll
+	for (int t = 0; t < 4; ++t)
+	{
+		const uint32_t k0 = 16 * t + 2 * c;
+		if (ra < rows)
+		{
+			*reinterpret_cast<uint32_t*>(Y + static_cast<size_t>(ra) * kIn + k0) = A[t][0];
+			*reinterpret_cast<uint32_t*>(Y + static_cast<size_t>(ra) * kIn + k0 + 8) = A[t][2];
+		}
+		if (rb < rows)
+		{
+			*reinterpret_cast<uint32_t*>(Y + static_cast<size_t>(rb) * kIn + k0) = A[t][1];
+			*reinterpret_cast<uint32_t*>(Y + static_cast<size_t>(rb) * kIn + k0 + 8) = A[t][3];
+		}
+	}
+}
+
+// Copies the 5 weight matrices (global, [out][in] bf16, dense) into shared
+// memory with the padded stride.
+RB_D void stageWeights(const __nv_bfloat16* __restrict__ w, __nv_bfloat16* sw)
+{
+	for (int i = threadIdx.x; i < kWTotal / 2; i += blockDim.x)
+	{
+		const int e = 2 * i, row = e / kH, col = e % kH;
+		*reinterpret_cast<uint32_t*>(sw + row * kWStride + col) = *reinterpret_cast<const uint32_t*>(w + e);
+	}
+	__syncthreads();
+}
+constexpr int kWRowsTotal = kWTotal / kH;   // 272 rows of 64
+constexpr size_t kSmemWeights = sizeof(__nv_bfloat16) * kWRowsTotal * kWStride;
+// backward: W4^T as 64 rows (16 used columns) + W3^T..W0^T as 4 x 64 rows
+constexpr int kWtRows = 64 + 4 * 64;
+constexpr size_t kSmemBackward = sizeof(__nv_bfloat16) * kWtRows * kWStride;
+
+// Forward: out[n][4] (FP32). With acts, the post-ReLU hidden activations of
+// layers 1..4 are stored ([4][n][64] bf16) for the backward pass.
+__global__ void __launch_bounds__(128) kMlpForward(uint32_t n, const __nv_bfloat16* __restrict__ X,
+	const __nv_bfloat16* __restrict__ w, float* __restrict__ out, __nv_bfloat16* __restrict__ acts)
+{
+	extern __shared__ __nv_bfloat16 sw[];
+	stageWeights(w, sw);
+	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
+	const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, c = lane & 3u;
+	for (uint32_t r0 = warp * kTile; r0 < n; r0 += warps * kTile)
+	{
+		uint32_t A[4][4];
+		loadA(X, r0, n, A);
+		float C[8][4];
+#pragma unroll
+		for (int l = 0; l < 4; ++l)
+		{
+			layer<8>(A, sw + wOffset(l) / kH * kWStride, C);
+			toA(C, A, true);
+			if (acts) storeA(acts + static_cast<size_t>(l) * n * kIn, r0, n, A);
+		}
+		float O[1][4];
+		layer<1>(A, sw + wOffset(4) / kH * kWStride, O);
+		// O: rows g, g+8; cols 2c, 2c+1 -> outputs 0..3 live in lanes with c < 2
+		if (c < 2)
+		{
+			const uint32_t ra = r0 + g, rb = r0 + g + 8;
+			if (ra < n) { out[4 * ra + 2 * c] = O[0][0]; out[4 * ra + 2 * c + 1] = O[0][1]; }
+			if (rb < n) { out[4 * rb + 2 * c] = O[0][2]; out[4 * rb + 2 * c + 1] = O[0][3]; }
+		}
+	}
+}
+
+// Relative L2 loss (Mueller et al. 2021): sum over outputs of
+// (y - t)^2 / (sg(y)^2 + 0.01), averaged over the batch; dY is written as
+// bf16 rows of 16 (4 used) and the loss sum accumulated.
+__global__ void kLoss(uint32_t n, const float* __restrict__ y, const float* __restrict__ t,
+	__nv_bfloat16* __restrict__ dY, float* __restrict__ lossSum)
+{
+	float local = 0.0f;
+	const float scale = 1.0f / static_cast<float>(n);
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		for (int k = 0; k < kOutPad; ++k)
+		{
+			float gk = 0.0f;
+			if (k < 4)
+			{
+				const float yy = y[4 * i + k], tt = t[4 * i + k];
+				const float den = yy * yy + 0.01f;
+				const float d = yy - tt;
+				local += d * d / den;
+				gk = 2.0f * d / den * scale;
+			}
+			dY[static_cast<size_t>(kOutPad) * i + k] = __float2bfloat16_rn(gk);
+		}
+	}
+	for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xFFFFFFFFu, local, o);
+	if ((threadIdx.x & 31u) == 0) atomicAdd(lossSum, local * scale);
+}
+
+// Backward through the layers on 16-row tiles: with the transposed weights
+// wt ([in][out] per layer, the output layer padded to 16 columns), dH4 = dY W4
+// masked by ReLU', ..., dX0 = dH1 W0. Writes the masked gradients of the
+// hidden layers ([4][n][64] bf16, for the weight gradients) and the
+// gradient of the 32 grid features (FP32).
+__global__ void __launch_bounds__(128) kMlpBackward(uint32_t n, const __nv_bfloat16* __restrict__ dY,
+	const __nv_bfloat16* __restrict__ wt, const __nv_bfloat16* __restrict__ acts, __nv_bfloat16* __restrict__ dH,
+	float* __restrict__ dX0)
+{
+	extern __shared__ __nv_bfloat16 sw[];
+	// wt layout: W4^T [64][16] first (as 64 rows of 16), then W3^T..W0^T [64][64]
+	for (int i = threadIdx.x; i < (64 * 16) / 2; i += blockDim.x)
+	{
+		const int e = 2 * i, row = e / 16, col = e % 16;
+		*reinterpret_cast<uint32_t*>(sw + row * kWStride + col) = *reinterpret_cast<const uint32_t*>(wt + e);
+	}
+	for (int i = threadIdx.x; i < (4 * 64 * 64) / 2; i += blockDim.x)
+	{
+		const int e = 2 * i, row = e / 64, col = e % 64;
+		*reinterpret_cast<uint32_t*>(sw + (64 + row) * kWStride + col) = *reinterpret_cast<const uint32_t*>(wt + 64 * 16 + e);
+	}
+	__syncthreads();
+	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
+	const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, c = lane & 3u;
+	for (uint32_t r0 = warp * kTile; r0 < n; r0 += warps * kTile)
+	{
+		// dY tile as one k-tile (16 columns, 4 used)
+		uint32_t A[4][4];
+		const uint32_t ra = r0 + g, rb = r0 + g + 8;
+		{
+			const __nv_bfloat16* base = dY;
+			A[0][0] = ra < n ? *reinterpret_cast<const uint32_t*>(base + static_cast<size_t>(ra) * kOutPad + 2 * c) : 0u;
+			A[0][1] = rb < n ? *reinterpret_cast<const uint32_t*>(base + static_cast<size_t>(rb) * kOutPad + 2 * c) : 0u;
+			A[0][2] = ra < n ? *reinterpret_cast<const uint32_t*>(base + static_cast<size_t>(ra) * kOutPad + 8 + 2 * c) : 0u;
+			A[0][3] = rb < n ? *reinterpret_cast<const uint32_t*>(base + static_cast<size_t>(rb) * kOutPad + 8 + 2 * c) : 0u;
+		}
+		float C[8][4];
+		// dH4 = dY[16 x 16] x W4 (B(k = out, n = in) = W4^T[in][out])
+#pragma unroll
+		for (int j = 0; j < 8; ++j)
+		{
+			C[j][0] = C[j][1] = C[j][2] = C[j][3] = 0.0f;
+			const __nv_bfloat16* wr = sw + (8 * j + g) * kWStride;
+			const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wr + 2 * c);
+			const uint32_t b1 = *reinterpret_cast<const uint32_t*>(wr + 8 + 2 * c);
+			mma16816(C[j], A[0], b0, b1);
+		}
+		for (int l = 3; l >= 0; --l)
+		{
+			// mask by ReLU' of the stored activation of layer l (post-ReLU > 0)
+			uint32_t H[4][4];
+			loadA(acts + static_cast<size_t>(l) * n * kIn, r0, n, H);
+#pragma unroll
+			for (int t = 0; t < 4; ++t)
+			{
+				const float2 h00 = unpack2(H[t][0]), h10 = unpack2(H[t][1]), h01 = unpack2(H[t][2]), h11 = unpack2(H[t][3]);
+				float* a = C[2 * t];
+				float* b = C[2 * t + 1];
+				a[0] = h00.x > 0.0f ? a[0] : 0.0f; a[1] = h00.y > 0.0f ? a[1] : 0.0f;
+				a[2] = h10.x > 0.0f ? a[2] : 0.0f; a[3] = h10.y > 0.0f ? a[3] : 0.0f;
+				b[0] = h01.x > 0.0f ? b[0] : 0.0f; b[1] = h01.y > 0.0f ? b[1] : 0.0f;
+				b[2] = h11.x > 0.0f ? b[2] : 0.0f; b[3] = h11.y > 0.0f ? b[3] : 0.0f;
+			}
+			toA(C, A, false);
+			storeA(dH + static_cast<size_t>(l) * n * kIn, r0, n, A);
+			// next: dH_{l} x W_l  (W_l^T at row block 64 + (3 - l) * 64)
+			layer<8>(A, sw + (64 + (3 - l) * 64) * kWStride, C);
+		}
+		// C = dX0 (64 columns); the first 32 are the grid features
+#pragma unroll
+		for (int j = 0; j < 4; ++j)
+		{
+			if (ra < n) { dX0[32 * ra + 8 * j + 2 * c] = C[j][0]; dX0[32 * ra + 8 * j + 2 * c + 1] = C[j][1]; }
+			if (rb < n) { dX0[32 * rb + 8 * j + 2 * c] = C[j][2]; dX0[32 * rb + 8 * j + 2 * c + 1] = C[j][3]; }
+		}
+	}
+}
+
+// ---------------------------------------------------------------- optimiser
+__global__ void kAdam(uint32_t n, float* __restrict__ p, float* __restrict__ grad, float* __restrict__ m,
+	float* __restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2, __nv_bfloat16* outBf16,
+	__half* outF16)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const float gr = grad[i];
+		const float mm = b1 * m[i] + (1.0f - b1) * gr;
+		const float vv = b2 * v[i] + (1.0f - b2) * gr * gr;
+		m[i] = mm;
+		v[i] = vv;
+		const float w = p[i] - lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+		p[i] = w;
+		grad[i] = 0.0f;
+		if (outBf16) outBf16[i] = __float2bfloat16_rn(w);
+		if (outF16) outF16[i] = __float2half_rn(w);
+	}
+}
+
+// transposed bf16 copies of the weights for the backward kernel
+__global__ void kTransposeWeights(const float* __restrict__ w, __nv_bfloat16* __restrict__ wt)
+{
+	for (uint32_t i = gtid(); i < static_cast<uint32_t>(kWTotal); i += gstride())
+	{
+		if (i < 64u * 16u)
+		{
+			const uint32_t in = i / 16, out = i % 16;                     // W4^T [64][16]
+			wt[i] = __float2bfloat16_rn(w[wOffset(4) + out * kH + in]);
+		}
+		else
+		{
+			const uint32_t j = i - 64u * 16u, blk = j / 4096u, e = j % 4096u;   // blocks: W3^T, W2^T, W1^T, W0^T
+			const uint32_t l = 3u - blk, in = e / 64u, out = e % 64u;
+			wt[i] = __float2bfloat16_rn(w[wOffset(l) + out * kH + in]);
+		}
+	}
+}
+} // namespace nrc
+} // namespace rb
+
+// ------------------------------------------------------------------ C ABI
+using namespace rb::nrc;
+using rb::gridFor;
+using rb::kThreads;
+
+struct rb_nrc
+{
+	int device = 0;
+	rb_nrc_config cfg{};
+	Resolutions R{};
+	float *gridF32 = nullptr, *gridGrad = nullptr, *gridM = nullptr, *gridV = nullptr;
+	__half* grid = nullptr;
+	float *wF32 = nullptr, *wGrad = nullptr, *wM = nullptr, *wV = nullptr;
+	__nv_bfloat16 *w = nullptr, *wt = nullptr;
+	// training scratch, grown on demand
+	uint32_t cap = 0;
+	__nv_bfloat16 *X = nullptr, *acts = nullptr, *dY = nullptr, *dH = nullptr;
+	float *out = nullptr, *dX0 = nullptr, *loss = nullptr;
+	cublasHandle_t blas = nullptr;
+	uint32_t step = 0;
+	int smCount = 148;
+};
+
+namespace
+{
+int nrcFail(cudaError_t e) { return e == cudaErrorMemoryAllocation ? RB_ERR_OOM : RB_ERR_CUDA; }
+
+// Deterministic uniform init (SplitMix64), as floats in [-a, a].
+void initUniform(std::vector<float>& v, uint64_t seed, float a)
+{
+	uint64_t s = seed;
+	for (float& x : v)
+	{
+		s += 0x9E3779B97F4A7C15ull;
+		uint64_t z = s;
+		z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+		z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+		z ^= z >> 31;
+		x = (static_cast<float>(z >> 40) / 16777216.0f * 2.0f - 1.0f) * a;
+	}
+}
+
+int growScratch(rb_nrc* h, uint32_t n)
+{
+	if (n <= h->cap) return RB_OK;
+	cudaFree(h->X); cudaFree(h->acts); cudaFree(h->dY); cudaFree(h->dH); cudaFree(h->out); cudaFree(h->dX0);
+	h->X = h->acts = h->dY = h->dH = nullptr;
+	h->out = h->dX0 = nullptr;
+	h->cap = 0;
+	cudaError_t e = cudaMalloc(&h->X, sizeof(__nv_bfloat16) * kIn * n);
+	if (e == cudaSuccess) e = cudaMalloc(&h->acts, sizeof(__nv_bfloat16) * 4 * kIn * n);
+	if (e == cudaSuccess) e = cudaMalloc(&h->dY, sizeof(__nv_bfloat16) * kOutPad * n);
+	if (e == cudaSuccess) e = cudaMalloc(&h->dH, sizeof(__nv_bfloat16) * 4 * kIn * n);
+	if (e == cudaSuccess) e = cudaMalloc(&h->out, sizeof(float) * 4 * n);
+	if (e == cudaSuccess) e = cudaMalloc(&h->dX0, sizeof(float) * kGridFeatures * n);
+	if (e != cudaSuccess) return nrcFail(e);
+	h->cap = n;
+	return RB_OK;
+}
+
+int blocksFor(const rb_nrc* h, uint32_t rows)
+{
+	const uint32_t tiles = (rows + kTile - 1) / kTile, perBlock = 4;   // 4 warps, one tile each
+	const uint32_t need = (tiles + perBlock - 1) / perBlock;
+	const uint32_t cap = static_cast<uint32_t>(h->smCount) * 4;
+	return static_cast<int>(need < 1 ? 1 : (need < cap ? need : cap));
+}
+} // namespace
+
+extern "C" {
+
+int rb_nrc_create(const rb_nrc_config* config, rb_nrc** out)
+{
+	if (!out) return RB_ERR_INVALID;
+	*out = nullptr;
+	rb_nrc* h = new (std::nothrow) rb_nrc();
+	if (!h) return RB_ERR_OOM;
+	h->cfg = config ? *config : rb_nrc_config{};
+	if (h->cfg.learning_rate <= 0.0f) h->cfg.learning_rate = 1e-2f;
+	if (h->cfg.beta1 <= 0.0f) h->cfg.beta1 = 0.9f;
+	if (h->cfg.beta2 <= 0.0f) h->cfg.beta2 = 0.99f;
+	if (h->cfg.epsilon <= 0.0f) h->cfg.epsilon = 1e-15f;
+	h->device = h->cfg.device;
+	cudaSetDevice(h->device);
+	cudaDeviceGetAttribute(&h->smCount, cudaDevAttrMultiProcessorCount, h->device);
+	// resolutions 16 .. 2048, geometric
+	const double growth = std::exp((std::log(2048.0) - std::log(16.0)) / (kLevels - 1));
+	for (int l = 0; l < kLevels; ++l)
+	{
+		const double res = std::floor(16.0 * std::pow(growth, l));
+		h->R.s[l] = static_cast<float>(res);
+		const double side = res + 2.0;
+		h->R.dense[l] = side * side * side <= static_cast<double>(kTable) ? 1u : 0u;
+		h->R.side[l] = static_cast<uint32_t>(side);
+	}
+	const size_t gridN = static_cast<size_t>(kLevels) * kTable * kFeat;
+	cudaError_t e = cudaMalloc(&h->gridF32, sizeof(float) * gridN);
+	if (e == cudaSuccess) e = cudaMalloc(&h->gridGrad, sizeof(float) * gridN);
+	if (e == cudaSuccess) e = cudaMalloc(&h->gridM, sizeof(float) * gridN);
+	if (e == cudaSuccess) e = cudaMalloc(&h->gridV, sizeof(float) * gridN);
+	if (e == cudaSuccess) e = cudaMalloc(&h->grid, sizeof(__half) * gridN);
+	if (e == cudaSuccess) e = cudaMalloc(&h->wF32, sizeof(float) * kWTotal);
+	if (e == cudaSuccess) e = cudaMalloc(&h->wGrad, sizeof(float) * kWTotal);
+	if (e == cudaSuccess) e = cudaMalloc(&h->wM, sizeof(float) * kWTotal);
+	if (e == cudaSuccess) e = cudaMalloc(&h->wV, sizeof(float) * kWTotal);
+	if (e == cudaSuccess) e = cudaMalloc(&h->w, sizeof(__nv_bfloat16) * kWTotal);
+	if (e == cudaSuccess) e = cudaMalloc(&h->wt, sizeof(__nv_bfloat16) * kWTotal);
+	if (e == cudaSuccess) e = cudaMalloc(&h->loss, sizeof(float));
+	if (e != cudaSuccess) { rb_nrc_destroy(h); return nrcFail(e); }
+	cudaMemset(h->gridGrad, 0, sizeof(float) * gridN);
+	cudaMemset(h->gridM, 0, sizeof(float) * gridN);
+	cudaMemset(h->gridV, 0, sizeof(float) * gridN);
+	cudaMemset(h->wGrad, 0, sizeof(float) * kWTotal);
+	cudaMemset(h->wM, 0, sizeof(float) * kWTotal);
+	cudaMemset(h->wV, 0, sizeof(float) * kWTotal);
+	// initial parameters: grid U(-1e-4, 1e-4), weights U(-sqrt(6/fan_in), ...); padded output rows zero
+	std::vector<float> g(gridN), w(kWTotal, 0.0f);
+	initUniform(g, h->cfg.seed * 2 + 1, 1e-4f);
+	std::vector<float> wl(4096);
+	for (int l = 0; l < 4; ++l)
+	{
+		initUniform(wl, h->cfg.seed * 2 + 2 + l, std::sqrt(6.0f / kIn));
+		std::memcpy(w.data() + wOffset(l), wl.data(), sizeof(float) * 4096);
+	}
+	std::vector<float> wo(4 * kH);
+	initUniform(wo, h->cfg.seed * 2 + 7, std::sqrt(6.0f / kH));
+	std::memcpy(w.data() + wOffset(4), wo.data(), sizeof(float) * wo.size());
+	const int rc = rb_nrc_set_parameters(h, g.data(), w.data());
+	if (rc != RB_OK) { rb_nrc_destroy(h); return rc; }
+	if (cublasCreate(&h->blas) != CUBLAS_STATUS_SUCCESS) { rb_nrc_destroy(h); return RB_ERR_CUDA; }
+	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpForward), cudaFuncAttributeMaxDynamicSharedMemorySize,
+		static_cast<int>(kSmemWeights));
+	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpBackward), cudaFuncAttributeMaxDynamicSharedMemorySize,
+		static_cast<int>(kSmemBackward));
+	*out = h;
+	return RB_OK;
+}
+
+int rb_nrc_destroy(rb_nrc* h)
+{
+	if (!h) return RB_ERR_INVALID;
+	cudaSetDevice(h->device);
+	cudaDeviceSynchronize();
+	for (void* p : { (void*)h->gridF32, (void*)h->gridGrad, (void*)h->gridM, (void*)h->gridV, (void*)h->grid,
+			(void*)h->wF32, (void*)h->wGrad, (void*)h->wM, (void*)h->wV, (void*)h->w, (void*)h->wt, (void*)h->X,
+			(void*)h->acts, (void*)h->dY, (void*)h->dH, (void*)h->out, (void*)h->dX0, (void*)h->loss })
+		if (p) cudaFree(p);
+	if (h->blas) cublasDestroy(h->blas);
+	delete h;
+	return RB_OK;
+}
+
+size_t rb_nrc_grid_size(void) { return static_cast<size_t>(kLevels) * kTable * kFeat; }
+size_t rb_nrc_weight_count(void) { return kWTotal; }
+
+int rb_nrc_set_parameters(rb_nrc* h, const float* grid, const float* weights)
+{
+	if (!h || !grid || !weights) return RB_ERR_INVALID;
+	cudaSetDevice(h->device);
+	const size_t gridN = rb_nrc_grid_size();
+	cudaError_t e = cudaMemcpy(h->gridF32, grid, sizeof(float) * gridN, cudaMemcpyHostToDevice);
+	if (e == cudaSuccess) e = cudaMemcpy(h->wF32, weights, sizeof(float) * kWTotal, cudaMemcpyHostToDevice);
+	if (e != cudaSuccess) return nrcFail(e);
+	// refresh the low-precision copies with a zero-gradient, zero-rate Adam pass
+	kAdam<<<4 * h->smCount, 256>>>(static_cast<uint32_t>(gridN), h->gridF32, h->gridGrad, h->gridM, h->gridV, 0.0f,
+		0.0f, 0.0f, 1.0f, 1.0f, 1.0f, nullptr, h->grid);
+	kAdam<<<64, 256>>>(kWTotal, h->wF32, h->wGrad, h->wM, h->wV, 0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f, h->w, nullptr);
+	kTransposeWeights<<<64, 256>>>(h->wF32, h->wt);
+	e = cudaDeviceSynchronize();
+	return e == cudaSuccess ? RB_OK : nrcFail(e);
+}
+
+int rb_nrc_get_parameters(rb_nrc* h, float* grid, float* weights)
+{
+	if (!h || !grid || !weights) return RB_ERR_INVALID;
+	cudaSetDevice(h->device);
+	cudaError_t e = cudaDeviceSynchronize();
+	if (e == cudaSuccess) e = cudaMemcpy(grid, h->gridF32, sizeof(float) * rb_nrc_grid_size(), cudaMemcpyDeviceToHost);
+	if (e == cudaSuccess) e = cudaMemcpy(weights, h->wF32, sizeof(float) * kWTotal, cudaMemcpyDeviceToHost);
+	return e == cudaSuccess ? RB_OK : nrcFail(e);
+}
+
+int rb_nrc_infer(rb_nrc* h, uint32_t n, const float* inputs, float* outputs, void* stream)
+{
+	if (!h || (n && (!inputs || !outputs))) return RB_ERR_INVALID;
+	if (n == 0) return RB_OK;
+	cudaSetDevice(h->device);
+	const int rc = growScratch(h, n);
+	if (rc != RB_OK) return rc;
+	const cudaStream_t st = static_cast<cudaStream_t>(stream);
+	kEncode<<<gridFor(n), kThreads, 0, st>>>(n, inputs, reinterpret_cast<const __half2*>(h->grid), h->R, h->X);
+	kMlpForward<<<blocksFor(h, n), 128, kSmemWeights, st>>>(n, h->X, h->w, outputs, nullptr);
+	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
+}
+
+namespace
+{
+// Forward, loss, backward: accumulates the batch's gradients into wGrad and
+// gridGrad (which the optimiser step or rb_nrc_gradients consume).
+int computeGradients(rb_nrc* h, uint32_t n, const float* inputs, const float* targets, cudaStream_t st)
+{
+	int rc = growScratch(h, n);
+	if (rc != RB_OK) return rc;
+	cudaMemsetAsync(h->loss, 0, sizeof(float), st);
+	kEncode<<<gridFor(n), kThreads, 0, st>>>(n, inputs, reinterpret_cast<const __half2*>(h->grid), h->R, h->X);
+	kMlpForward<<<blocksFor(h, n), 128, kSmemWeights, st>>>(n, h->X, h->w, h->out, h->acts);
+	kLoss<<<gridFor(n), kThreads, 0, st>>>(n, h->out, targets, h->dY, h->loss);
+	kMlpBackward<<<blocksFor(h, n), 128, kSmemBackward, st>>>(n, h->dY, h->wt, h->acts, h->dH, h->dX0);
+	// weight gradients: dW_l[out][in] = sum over rows dY_l[r][out] X_l[r][in]
+	// (column-major view: dW^T = X^T dY with X [n][64] row-major = X^T column-major)
+	cublasSetStream(h->blas, st);
+	const float one = 1.0f;
+	const __nv_bfloat16* inputsOf[5] = { h->X, h->acts, h->acts + static_cast<size_t>(n) * kIn,
+		h->acts + 2 * static_cast<size_t>(n) * kIn, h->acts + 3 * static_cast<size_t>(n) * kIn };
+	for (int l = 0; l < 5; ++l)
+	{
+		const int outDim = l < 4 ? kH : kOutPad;
+		const __nv_bfloat16* dOut = l < 4 ? h->dH + static_cast<size_t>(l) * n * kIn : h->dY;
+		const int ldd = l < 4 ? kIn : kOutPad;
+		// C (col-major, in x out) = A (in x n) * B^T... written as C[in][out] += sum_r X[r][in] dOut[r][out]:
+		// A = X viewed col-major (in x n, lda = 64), B = dOut viewed col-major (out x n, ldb = ldd), op(B) = T.
+		if (cublasGemmEx(h->blas, CUBLAS_OP_N, CUBLAS_OP_T, kIn, outDim, static_cast<int>(n), &one, inputsOf[l],
+				CUDA_R_16BF, kIn, dOut, CUDA_R_16BF, ldd, &one, h->wGrad + wOffset(l), CUDA_R_32F, kIn,
+				CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT) != CUBLAS_STATUS_SUCCESS)
+			return RB_ERR_CUDA;
+	}
+	kEncodeBackward<<<gridFor(n), kThreads, 0, st>>>(n, inputs, h->dX0, h->R, h->gridGrad);
+	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
+}
+} // namespace
+
+int rb_nrc_gradients(rb_nrc* h, uint32_t n, const float* inputs, const float* targets, float* grid_grad,
+	float* weight_grad)
+{
+	if (!h || n == 0 || !inputs || !targets || !grid_grad || !weight_grad) return RB_ERR_INVALID;
+	cudaSetDevice(h->device);
+	int rc = computeGradients(h, n, inputs, targets, nullptr);
+	if (rc != RB_OK) return rc;
+	const size_t gridN = rb_nrc_grid_size();
+	cudaError_t e = cudaDeviceSynchronize();
+	if (e == cudaSuccess) e = cudaMemcpy(grid_grad, h->gridGrad, sizeof(float) * gridN, cudaMemcpyDeviceToHost);
+	if (e == cudaSuccess) e = cudaMemcpy(weight_grad, h->wGrad, sizeof(float) * kWTotal, cudaMemcpyDeviceToHost);
+	if (e == cudaSuccess) e = cudaMemset(h->gridGrad, 0, sizeof(float) * gridN);
+	if (e == cudaSuccess) e = cudaMemset(h->wGrad, 0, sizeof(float) * kWTotal);
+	return e == cudaSuccess ? RB_OK : nrcFail(e);
+}
+
+int rb_nrc_train(rb_nrc* h, uint32_t n, const float* inputs, const float* targets, float* loss_out, void* stream)
+{
+	if (!h || n == 0 || !inputs || !targets) return RB_ERR_INVALID;
+	cudaSetDevice(h->device);
+	const cudaStream_t st = static_cast<cudaStream_t>(stream);
+	const int rc = computeGradients(h, n, inputs, targets, st);
+	if (rc != RB_OK) return rc;
+	++h->step;
+	const float b1 = h->cfg.beta1, b2 = h->cfg.beta2;
+	const float c1 = 1.0f - std::pow(b1, static_cast<float>(h->step)), c2 = 1.0f - std::pow(b2, static_cast<float>(h->step));
+	kAdam<<<4 * h->smCount, 256, 0, st>>>(static_cast<uint32_t>(rb_nrc_grid_size()), h->gridF32, h->gridGrad, h->gridM,
+		h->gridV, h->cfg.learning_rate, b1, b2, h->cfg.epsilon, c1, c2, nullptr, h->grid);
+	kAdam<<<64, 256, 0, st>>>(kWTotal, h->wF32, h->wGrad, h->wM, h->wV, h->cfg.learning_rate, b1, b2, h->cfg.epsilon,
+		c1, c2, h->w, nullptr);
+	kTransposeWeights<<<64, 256, 0, st>>>(h->wF32, h->wt);
+	if (loss_out) cudaMemcpyAsync(loss_out, h->loss, sizeof(float), cudaMemcpyDefault, st);
+	const cudaError_t e = cudaGetLastError();
+	return e == cudaSuccess ? RB_OK : RB_ERR_CUDA;
+}
+
+} // extern "C"

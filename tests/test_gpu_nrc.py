@@ -1,0 +1,187 @@
+"""The radiance cache's own kernels (hash-grid encoding, fused BF16 MLP
+forward and backward, Adam) against a plain PyTorch fp32 reference of the
+same model, and a training run that must fit a target.
+
+Tolerances. The forward reference rounds where the kernels round (grid
+entries to fp16, encoded inputs and hidden activations to bf16) and
+multiplies in fp32 without TF32: outputs agree to 2e-2 relative (measured
+9e-3). The gradient reference is fp32 autograd at the rounded parameter
+values; the kernels also round the loss gradient and each layer's input
+gradient to bf16 on the way back, which perturbs the grid gradient most
+(measured cosine 0.997, norm within 0.1 %) and the weight gradients least
+(cosine 0.999999): the bounds are cosine > 0.99 and > 0.999, norms within 2 %.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+L, T, H = 16, 1 << 19, 64
+
+
+def _resolutions():
+    growth = math.exp((math.log(2048.0) - math.log(16.0)) / (L - 1))
+    res, dense, side = [], [], []
+    for l in range(L):
+        r = math.floor(16.0 * math.pow(growth, l))
+        s = r + 2
+        res.append(float(np.float32(r)))
+        dense.append(s * s * s <= T)
+        side.append(int(s))
+    return res, dense, side
+
+
+def _encode(torch, inputs, grid, round_bf16=True):
+    """inputs [n,10] fp32, grid [L,T,2] (fp16-rounded values) -> X [n,64]."""
+    res, dense, side = _resolutions()
+    p = inputs[:, :3].clamp(0.0, 1.0)
+    feats = []
+    for l in range(L):
+        sp = p * res[l]
+        f = torch.floor(sp)
+        w = sp - f
+        c = f.to(torch.int64)
+        acc = torch.zeros(inputs.shape[0], 2, device=inputs.device)
+        for k in range(8):
+            d = torch.tensor([k & 1, (k >> 1) & 1, (k >> 2) & 1], device=inputs.device)
+            cc = c + d
+            ww = torch.where(d.bool(), w, 1.0 - w).prod(dim=1)
+            if dense[l]:
+                idx = cc[:, 0] + side[l] * (cc[:, 1] + side[l] * cc[:, 2])
+            else:
+                x = cc[:, 0] & 0xFFFFFFFF
+                y = (cc[:, 1] * 2654435761) & 0xFFFFFFFF
+                z = (cc[:, 2] * 805459861) & 0xFFFFFFFF
+                idx = (x ^ y ^ z) & (T - 1)
+            acc = acc + ww[:, None] * grid[l][idx]
+        feats.append(acc)
+    n = inputs.shape[0]
+    rest = torch.zeros(n, 32, device=inputs.device)
+    rest[:, 0:6] = inputs[:, 3:9] * 0.5 + 0.5
+    rest[:, 6] = inputs[:, 9]
+    rest[:, 7] = 1.0
+    X = torch.cat([torch.cat(feats, dim=1), rest], dim=1)
+    return X.to(torch.bfloat16).to(torch.float32) if round_bf16 else X
+
+
+def _mlp(torch, X, W):
+    h = X
+    for l in range(4):
+        h = torch.relu(h @ W[l].T).to(torch.bfloat16).to(torch.float32)
+    return h @ W[4][:4].T
+
+
+def _split(torch, w):
+    W = [w[l * 4096:(l + 1) * 4096].view(64, 64) for l in range(4)]
+    W.append(w[4 * 4096:].view(16, 64))
+    return [x.to(torch.bfloat16).to(torch.float32) for x in W]
+
+
+def _inputs(torch, n, seed):
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    pos = torch.rand(n, 3, device="cuda", generator=g)
+    d = torch.nn.functional.normalize(torch.randn(n, 3, device="cuda", generator=g), dim=1)
+    nn = torch.nn.functional.normalize(torch.randn(n, 3, device="cuda", generator=g), dim=1)
+    lam = torch.rand(n, 1, device="cuda", generator=g)
+    return torch.cat([pos, d, nn, lam], dim=1).contiguous()
+
+
+def _target(torch, x):
+    p, d, lam = x[:, :3], x[:, 3:6], x[:, 9:10]
+    base = 0.5 + 0.4 * torch.sin(6.0 * p[:, :1]) * torch.cos(4.0 * p[:, 1:2]) + 0.3 * p[:, 2:3]
+    spec = torch.stack([base[:, 0] * (1.0 + 0.3 * k * lam[:, 0]) * (1.0 + 0.2 * d[:, 1]) for k in range(4)], dim=1)
+    return spec.contiguous()
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    t.backends.cuda.matmul.allow_tf32 = False
+    t.backends.cudnn.allow_tf32 = False
+    return t
+
+
+def _cache_with_random_grid(torch, seed=3):
+    from ratbite_b200.nrc import RadianceCache
+    cache = RadianceCache(seed=seed)
+    g, w = cache.parameters()
+    g = (np.random.default_rng(seed).random(g.shape, dtype=np.float32) - 0.5) * 0.2   # visible features
+    cache.set_parameters(g, w)
+    return cache
+
+
+def test_forward_matches_torch(torch):
+    cache = _cache_with_random_grid(torch)
+    g, w = cache.parameters()
+    n = 5000
+    x = _inputs(torch, n, 1)
+    out = torch.zeros(n, 4, device="cuda")
+    cache.infer(n, x.data_ptr(), out.data_ptr())
+    torch.cuda.synchronize()
+    grid = torch.from_numpy(g).cuda().view(L, T, 2).half().float()
+    ref = _mlp(torch, _encode(torch, x, grid), _split(torch, torch.from_numpy(w).cuda()))
+    err = ((out - ref).abs() / (ref.abs() + 1e-2)).max().item()
+    print(f"nrc forward: max rel err {err:.2e}, mean |y| {ref.abs().mean().item():.3e}")
+    assert err < 2e-2
+    cache.close()
+
+
+def test_gradients_match_torch_autograd(torch):
+    cache = _cache_with_random_grid(torch, seed=5)
+    g, w = cache.parameters()
+    n = 4096
+    x = _inputs(torch, n, 2)
+    t = _target(torch, x)
+    gg, wg = cache.gradients(n, x.data_ptr(), t.data_ptr())
+    # fp32 autograd of the same model at the rounded parameter values
+    grid = torch.from_numpy(g).cuda().view(L, T, 2).half().float().requires_grad_(True)
+    W = [m.detach().clone().requires_grad_(True) for m in _split(torch, torch.from_numpy(w).cuda())]
+    h = _encode(torch, x, grid, round_bf16=False)
+    for l in range(4):
+        h = torch.relu(h @ W[l].T)
+    y = h @ W[4][:4].T
+    loss = (((y - t) ** 2) / (y.detach() ** 2 + 0.01)).sum(dim=1).mean()
+    loss.backward()
+    rw = torch.cat([m.grad.reshape(-1) for m in W]).cpu().numpy()
+    rg = grid.grad.reshape(-1).cpu().numpy()
+
+    def cos(a, b):
+        return float(np.dot(a, b) / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30))
+    cw, cg = cos(wg, rw), cos(gg, rg)
+    print(f"nrc gradients: weights cos {cw:.6f} norm ratio {np.linalg.norm(wg) / np.linalg.norm(rw):.4f}, "
+          f"grid cos {cg:.6f} norm ratio {np.linalg.norm(gg) / np.linalg.norm(rg):.4f}")
+    assert cw > 0.999 and cg > 0.99
+    assert abs(np.linalg.norm(wg) / np.linalg.norm(rw) - 1.0) < 2e-2
+    assert abs(np.linalg.norm(gg) / np.linalg.norm(rg) - 1.0) < 2e-2
+    cache.close()
+
+
+def test_training_fits_a_target(torch):
+    from ratbite_b200.nrc import RadianceCache
+    cache = RadianceCache(seed=7, learning_rate=1e-2)
+    n = 1 << 14
+    loss = torch.zeros(1, device="cuda")
+    first = last = None
+    for step in range(400):
+        x = _inputs(torch, n, 100 + step)
+        t = _target(torch, x)
+        cache.train(n, x.data_ptr(), t.data_ptr(), loss.data_ptr())
+        if step == 0:
+            torch.cuda.synchronize()
+            first = loss.item()
+    torch.cuda.synchronize()
+    x = _inputs(torch, n, 9999)
+    t = _target(torch, x)
+    out = torch.zeros(n, 4, device="cuda")
+    cache.infer(n, x.data_ptr(), out.data_ptr())
+    torch.cuda.synchronize()
+    rel = ((out - t).abs() / t.abs().clamp_min(1e-2)).mean().item()
+    last = loss.item()
+    print(f"nrc training: loss {first:.3e} -> {last:.3e}, held-out mean rel err {rel:.3e}")
+    assert last < 0.05 * first
+    assert rel < 0.1
+    cache.close()
