@@ -391,6 +391,98 @@ def run_ours(args, rank: int, world: int, wl: dict):
         dist.destroy_process_group()
 
 
+def time_to_rmse(device: int = 0, width: int = 1920, height: int = 1080, depth: int = 12, ref_spp: int = 4096,
+                 plain_spp: int = 1024, chunk: int = 32, failed_mode: int = 0, cache_kw: dict | None = None,
+                 time_factor: float = 2.0):
+    """The cached form against the plain tracer on the Cornell box at
+    width x height, depth `depth`: device seconds until each reaches the
+    plain tracer's plain_spp RMSE against a ref_spp plain oracle (FP64
+    accumulation, sample indices disjoint from both runs). RMSE is taken on
+    the linear XYZ mean image, relative to the oracle's mean, between chunks
+    and outside the timed spans. Both runs get one untimed warm-up chunk
+    (first-launch costs and buffer allocation); the cached form then starts
+    from an untrained cache and stops at the target or at time_factor x the
+    plain tracer's time."""
+    import torch
+    from ratbite_b200 import assets, lighttree, scenes
+    from ratbite_b200.nrc import RadianceCache
+    from ratbite_b200.rendering_interface import RenderingInterface
+
+    cie, basis, luts = assets.cie_xyz(), assets.basis_rgb(), assets.luts()
+    scene = scenes.cornell_box(seed=1, cie_xyz=cie, width=width, height=height, spp=plain_spp, max_depth=depth)
+    lt = lighttree.build_for_scene(scene)
+    ri = RenderingInterface(device=device, failed_sample_mode=failed_mode)
+    ri.load_scene(scene, luts, cie, basis, light_tree=lt)
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    n = width * height
+
+    def mean_image():
+        ri.synchronize()
+        acc = torch.from_numpy(ri.read_accumulation().reshape(n, 4)).cuda()
+        return acc[:, :3] / acc[:, 3:4].clamp_min(1.0)
+
+    ri.render(1 << 20, ref_spp, stream=sp)
+    ref = mean_image()
+    ref_mean = float(ref.mean())
+
+    def rel_rmse(img):
+        return float(torch.sqrt(((img - ref) ** 2).mean()) / ref_mean)
+
+    def timed(offset, count):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ri.render(offset, count, stream=sp)
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / 1e3
+
+    ri.render(0, chunk, stream=sp)
+    plain_curve, t = [], 0.0
+    for k in range(plain_spp // chunk):
+        t += timed(k * chunk, chunk)
+        plain_curve.append(((k + 1) * chunk, t, rel_rmse(mean_image())))
+    target, t_plain = plain_curve[-1][2], plain_curve[-1][1]
+
+    kw = dict(cache_kw or {})
+    scratch = RadianceCache(device=device, seed=99)
+    ri.attach_radiance_cache(scratch, **kw)
+    ri.render(1 << 22, chunk, stream=sp)          # warm-up: sizes the cache's wave buffers
+    cache = RadianceCache(device=device, seed=2)
+    ri.attach_radiance_cache(cache, **kw)
+    ri.cache_stats()
+    cached_curve, t, done, reached = [], 0.0, 0, None
+    while t < time_factor * t_plain:
+        t += timed(done, chunk)
+        done += chunk
+        r = rel_rmse(mean_image())
+        cached_curve.append((done, t, r))
+        if r <= target:
+            reached = t
+            break
+    st = ri.cache_stats()
+    ri.cleanup()
+    cache.close()
+    scratch.close()
+    best = min(cached_curve, key=lambda c: c[2])
+    at_plain_time = min((c for c in cached_curve if c[1] <= t_plain), key=lambda c: c[2], default=None)
+    return {
+        "workload": f"cornell_box_{width}x{height}_depth{depth}",
+        "rmse": f"relative RMSE of the XYZ mean image vs a {ref_spp}-spp FP64-accumulated plain render",
+        "failed_sample_mode": "keep" if failed_mode else "drop (reference)",
+        "plain": {"spp": plain_spp, "s": t_plain, "rel_rmse": target, "paths_per_s": n * plain_spp / t_plain},
+        "cached": {"s_to_target": reached, "spp_to_target": done if reached else None,
+                   "best_rel_rmse": best[2], "best_at_spp": best[0],
+                   "rel_rmse_at_plain_time": at_plain_time[2] if at_plain_time else None,
+                   "spp_rendered": done, "s_rendered": t, "paths_per_s": n * done / t,
+                   "queries_per_sample": st.queries / max(1, done), "records_per_sample": st.records / max(1, done),
+                   "train_steps": st.steps, "last_loss": st.last_loss, "params": kw or "library defaults"},
+        "time_ratio": (reached / t_plain) if reached else None,
+        "plain_curve": [(a, round(b, 4), round(c, 5)) for a, b, c in plain_curve[::max(1, len(plain_curve) // 8)]],
+        "cached_curve": [(a, round(b, 4), round(c, 5)) for a, b, c in cached_curve[::max(1, len(cached_curve) // 8)]],
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)

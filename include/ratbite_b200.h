@@ -81,8 +81,16 @@ typedef struct rb_config {
     int32_t device;              /* CUDA device ordinal */
     uint32_t max_paths_in_flight;/* wavefront capacity; 0 = default (16M paths) */
     uint32_t envmap_cdf_mode;    /* RB_CDF_FP64 (default, 0) or RB_CDF_REFERENCE */
-    uint32_t reserved[5];
+    uint32_t failed_sample_mode; /* RB_FAILED_DROP (default, 0) or RB_FAILED_KEEP */
+    uint32_t reserved[4];
 } rb_config;
+/* A BxDF sample that fails (a direction on the wrong side of the shading
+ * hemisphere, a zero or infinite pdf) sets the path's terminated flag. The
+ * reference then drops the whole sample, radiance gathered before included
+ * (src/kernels/pathtrace.cu:1789-1812): RB_FAILED_DROP, the default. With
+ * RB_FAILED_KEEP the path ends there and keeps what it gathered. */
+#define RB_FAILED_DROP    0u
+#define RB_FAILED_KEEP    1u
 #define RB_CDF_FP64       0u     /* float64 row/column sums */
 #define RB_CDF_REFERENCE  1u     /* float32 in the reference's scan order: bit-identical tables */
 

@@ -74,6 +74,8 @@ SIGNATURES = {
     "rb_nrc_infer": (C.c_int, [_P, _U32, _P, _P, _P]),
     "rb_nrc_train": (C.c_int, [_P, _U32, _P, _P, _P, _P]),
     "rb_nrc_gradients": (C.c_int, [_P, _U32, _P, _P, _P, _P]),
+    "rb_attach_radiance_cache": (C.c_int, [_P, _P, C.POINTER(abi.rb_cache_params)]),
+    "rb_get_cache_stats": (C.c_int, [_P, C.POINTER(abi.rb_cache_stats)]),
 }
 
 _lib = None

@@ -87,7 +87,11 @@ RB_CDF_REFERENCE = 1
 
 class rb_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_paths_in_flight", C.c_uint32),
-                ("envmap_cdf_mode", C.c_uint32), ("reserved", C.c_uint32 * 5)]
+                ("envmap_cdf_mode", C.c_uint32), ("failed_sample_mode", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+
+
+RB_FAILED_DROP = 0
+RB_FAILED_KEEP = 1
 
 
 class rb_material(C.Structure):
@@ -230,3 +234,15 @@ NRC_INPUTS = 10
 class rb_nrc_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("seed", C.c_uint32), ("learning_rate", C.c_float), ("beta1", C.c_float),
                 ("beta2", C.c_float), ("epsilon", C.c_float), ("reserved", C.c_uint32 * 2)]
+
+
+class rb_cache_params(C.Structure):
+    _fields_ = [("spread_threshold", C.c_float), ("train_one_in", C.c_uint32), ("targets_per_sample", C.c_uint32),
+                ("batch", C.c_uint32), ("frozen", C.c_uint32), ("samples_per_wave", C.c_uint32),
+                ("scene_min", C.c_float * 3), ("scene_max", C.c_float * 3), ("min_roughness", C.c_float),
+                ("reserved", C.c_uint32 * 3)]
+
+
+class rb_cache_stats(C.Structure):
+    _fields_ = [("queries", C.c_uint64), ("records", C.c_uint64), ("steps", C.c_uint64), ("last_loss", C.c_float),
+                ("launches", C.c_uint32), ("ms_infer", C.c_double), ("ms_train", C.c_double)]

@@ -18,9 +18,12 @@
 
 #include "ratbite_b200.h"
 #include "ratbite_b200_kernels.h"
+#include "ratbite_b200_nrc.h"
 #include "rb_bvh_build.h"
 #include "rb_envmap.h"
+#include "rb_launch.cuh"
 #include "rb_light.cuh"
+#include "rb_nrc_internal.h"
 #include "rb_refit.h"
 #include "rb_scene.h"
 #include "rb_wavefront.h"
@@ -41,6 +44,7 @@ struct rb_ctx
 	uint32_t capacity = 0;
 	uint32_t requestedCapacity = 0;
 	uint32_t cdfMode = RB_CDF_FP64;
+	uint32_t failedMode = RB_FAILED_DROP;
 	void* envScratch = nullptr;                 // CDF scratch of the current map (in envBufs)
 	float* envIntegral = nullptr;               // device scalar (in envBufs)
 	double4* accum = nullptr;
@@ -67,8 +71,23 @@ struct rb_ctx
 	struct Timed { int stage; cudaEvent_t a, b; };
 	std::vector<Timed> timed;
 	std::vector<cudaEvent_t> eventPool;
-	uint32_t launches[7] = {};   // generate, extend, surface, shadow, resolve, nee, bsdf
+	uint32_t launches[9] = {};   // generate, extend, surface, shadow, resolve, nee, bsdf, cache queries, cache training
+	double stageMs[9] = {};      // device time drained from `timed`
 	uint64_t waves = 0;
+	// geometry bounds at upload (radiance-cache position normalisation)
+	float geoMin[3] = {}, geoMax[3] = {};
+	// radiance-cache form (rb_attach_radiance_cache)
+	rb_nrc* cache = nullptr;
+	rb_cache_params cacheParams{};
+	rb::PathSoA cacheArrays{};           // only the cache fields are used
+	std::vector<void*> cacheBufs;
+	uint32_t cacheCapacity = 0;          // paths the per-path arrays hold
+	uint32_t cacheBatchRows = 0;         // rows of the training batch buffers
+	float* batchIn = nullptr;
+	float* batchTarget = nullptr;
+	uint32_t* batchValid = nullptr;
+	unsigned long long* cacheTally = nullptr;   // device: queries, records
+	uint64_t cacheWaves = 0, cacheSteps = 0, cacheStepsReported = 0;
 };
 
 namespace
@@ -206,6 +225,19 @@ void timedStage(rb_ctx* ctx, int stage, cudaStream_t st, F&& launch)
 	ctx->timed.push_back(t);
 }
 
+// Adds the device time of the finished timed launches to stageMs (synchronized by the caller).
+void drainTimed(rb_ctx* ctx)
+{
+	for (const auto& t : ctx->timed)
+	{
+		float v = 0.0f;
+		if (cudaEventElapsedTime(&v, t.a, t.b) == cudaSuccess) ctx->stageMs[t.stage] += v;
+		ctx->eventPool.push_back(t.a);
+		ctx->eventPool.push_back(t.b);
+	}
+	ctx->timed.clear();
+}
+
 // Every index a kernel will follow must land inside its table.
 int checkReferences(rb_ctx* ctx)
 {
@@ -250,11 +282,131 @@ int ensureWave(rb_ctx* ctx, uint32_t paths)
 	ctx->capacity = paths;
 	return RB_OK;
 }
+// Radiance-cache arrays for waves of `paths` paths and up to `depth` vertices.
+int ensureCache(rb_ctx* ctx, uint32_t paths, uint32_t depth)
+{
+	const rb_cache_params& P = ctx->cacheParams;
+	const uint64_t oneIn = P.frozen ? 0 : P.train_one_in;
+	const uint32_t want = oneIn ? static_cast<uint32_t>(std::min<uint64_t>((paths / oneIn + 1) * (depth + 1), 64u << 20)) : 1u;
+	if (ctx->cacheCapacity >= paths && ctx->cacheArrays.trainCapacity >= want && ctx->cacheBatchRows >= P.batch)
+		return RB_OK;
+	cudaStreamSynchronize(ctx->stream);
+	freeAll(ctx->cacheBufs);
+	ctx->cacheArrays = rb::PathSoA{};
+	ctx->cacheCapacity = ctx->cacheBatchRows = 0;
+	rb::PathSoA& c = ctx->cacheArrays;
+	int rc = RB_OK;
+	auto alloc = [&](auto*& ptr, size_t bytes) {
+		if (rc == RB_OK) rc = upload(ctx, ctx->cacheBufs, nullptr, bytes, ptr);
+	};
+	alloc(c.spread, sizeof(float2) * paths);
+	alloc(c.trainRec, sizeof(uint32_t) * paths);
+	alloc(c.cPath, sizeof(uint32_t) * paths);
+	alloc(c.cIn, sizeof(float) * kNrcInputs * static_cast<size_t>(paths));
+	alloc(c.tPath, sizeof(uint32_t) * want);
+	alloc(c.tIn, sizeof(float) * kNrcInputs * static_cast<size_t>(want));
+	alloc(c.tL, sizeof(float4) * want);
+	alloc(c.tT, sizeof(float4) * want);
+	alloc(ctx->batchIn, sizeof(float) * kNrcInputs * static_cast<size_t>(P.batch));
+	alloc(ctx->batchTarget, 2 * sizeof(float4) * P.batch);   // radiance, drop (+3 unused)
+	alloc(ctx->batchValid, sizeof(uint32_t));
+	if (rc != RB_OK)
+	{
+		freeAll(ctx->cacheBufs);
+		ctx->cacheArrays = rb::PathSoA{};
+		return rc;
+	}
+	c.trainCapacity = want;
+	ctx->cacheCapacity = paths;
+	ctx->cacheBatchRows = P.batch;
+	return RB_OK;
+}
+
+void releaseCache(rb_ctx* ctx)
+{
+	cudaStreamSynchronize(ctx->stream);
+	freeAll(ctx->cacheBufs);
+	ctx->cacheArrays = rb::PathSoA{};
+	ctx->cacheCapacity = ctx->cacheBatchRows = 0;
+	ctx->batchIn = ctx->batchTarget = nullptr;
+	ctx->batchValid = nullptr;
+}
 } // namespace
 
 extern "C" {
 
 int rb_abi_version(void) { return RB_ABI_VERSION; }
+
+int rb_attach_radiance_cache(rb_ctx* ctx, rb_nrc* cache, const rb_cache_params* params)
+{
+	if (!ctx) return RB_ERR_INVALID;
+	cudaSetDevice(ctx->device);
+	if (!cache)
+	{
+		releaseCache(ctx);
+		ctx->cache = nullptr;
+		return RB_OK;
+	}
+	if (rb::nrc::deviceOf(cache) != ctx->device)
+		return fail(ctx, RB_ERR_INVALID, "rb_attach_radiance_cache: the cache lives on another device");
+	rb_cache_params P = params ? *params : rb_cache_params{};
+	if (!std::isfinite(P.spread_threshold) || P.spread_threshold < 0.0f)
+		return fail(ctx, RB_ERR_INVALID, "rb_attach_radiance_cache: spread threshold must be finite and >= 0");
+	for (int k = 0; k < 3; ++k)
+		if (!std::isfinite(P.scene_min[k]) || !std::isfinite(P.scene_max[k]))
+			return fail(ctx, RB_ERR_INVALID, "rb_attach_radiance_cache: non-finite bounds");
+	if (!std::isfinite(P.min_roughness)) return fail(ctx, RB_ERR_INVALID, "rb_attach_radiance_cache: non-finite roughness");
+	if (P.spread_threshold == 0.0f) P.spread_threshold = 0.01f;
+	if (P.train_one_in == 0) P.train_one_in = 16;
+	if (P.targets_per_sample == 0) P.targets_per_sample = 65536;
+	if (P.batch == 0) P.batch = 65536;
+	if (P.samples_per_wave == 0) P.samples_per_wave = 8;
+	if (P.min_roughness == 0.0f) P.min_roughness = 0.25f;
+	if (P.batch > (1u << 22)) return fail(ctx, RB_ERR_INVALID, "rb_attach_radiance_cache: batch above 2^22 rows");
+	if (!ctx->cacheTally)
+	{
+		cudaError_t e = cudaMalloc(&ctx->cacheTally, 2 * sizeof(unsigned long long));
+		if (e == cudaSuccess) e = cudaMemset(ctx->cacheTally, 0, 2 * sizeof(unsigned long long));
+		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_attach_radiance_cache");
+	}
+	// per-path arrays are sized by the next render; batch buffers follow the new parameters
+	ctx->cache = cache;
+	ctx->cacheParams = P;
+	return RB_OK;
+}
+
+int rb_get_cache_stats(rb_ctx* ctx, rb_cache_stats* out)
+{
+	if (!ctx || !out) return RB_ERR_INVALID;
+	cudaSetDevice(ctx->device);
+	cudaError_t e = cudaStreamSynchronize(ctx->stream);
+	if (e == cudaSuccess) e = cudaDeviceSynchronize();
+	if (e != cudaSuccess) return cudaFail(ctx, e, "rb_get_cache_stats");
+	drainTimed(ctx);
+	*out = rb_cache_stats{};
+	if (ctx->cacheTally)
+	{
+		unsigned long long t[2] = {};
+		e = cudaMemcpy(t, ctx->cacheTally, sizeof(t), cudaMemcpyDeviceToHost);
+		if (e == cudaSuccess) e = cudaMemset(ctx->cacheTally, 0, sizeof(t));
+		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_get_cache_stats");
+		out->queries = t[0];
+		out->records = t[1];
+	}
+	if (ctx->cache)
+	{
+		e = cudaMemcpy(&out->last_loss, rb::nrc::lossDevice(ctx->cache), sizeof(float), cudaMemcpyDeviceToHost);
+		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_get_cache_stats");
+	}
+	out->steps = ctx->cacheSteps - ctx->cacheStepsReported;
+	ctx->cacheStepsReported = ctx->cacheSteps;
+	out->launches = ctx->launches[7] + ctx->launches[8];
+	out->ms_infer = ctx->stageMs[7];
+	out->ms_train = ctx->stageMs[8];
+	ctx->launches[7] = ctx->launches[8] = 0;
+	ctx->stageMs[7] = ctx->stageMs[8] = 0.0;
+	return RB_OK;
+}
 
 int rb_create(const rb_config* config, rb_ctx** out)
 {
@@ -266,6 +418,8 @@ int rb_create(const rb_config* config, rb_ctx** out)
 	ctx->requestedCapacity = config ? config->max_paths_in_flight : 0u;
 	if (config && config->envmap_cdf_mode > RB_CDF_REFERENCE) { delete ctx; return RB_ERR_INVALID; }
 	ctx->cdfMode = config ? config->envmap_cdf_mode : RB_CDF_FP64;
+	if (config && config->failed_sample_mode > RB_FAILED_KEEP) { delete ctx; return RB_ERR_INVALID; }
+	ctx->failedMode = config ? config->failed_sample_mode : RB_FAILED_DROP;
 	cudaError_t e = cudaSetDevice(ctx->device);
 	if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
 	if (e == cudaSuccess) e = cudaMalloc(&ctx->status, 2 * sizeof(uint32_t));
@@ -291,6 +445,8 @@ int rb_destroy(rb_ctx* ctx)
 	for (auto* v : { &ctx->lutBufs, &ctx->spectraBufs, &ctx->materialBufs, &ctx->geoBufs, &ctx->lightBufs, &ctx->envBufs })
 		freeAll(*v);
 	releaseWave(ctx);
+	freeAll(ctx->cacheBufs);
+	if (ctx->cacheTally) cudaFree(ctx->cacheTally);
 	for (const auto& t : ctx->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
 	for (cudaEvent_t e : ctx->eventPool) cudaEventDestroy(e);
 	if (ctx->counters) cudaFree(ctx->counters);
@@ -481,6 +637,13 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 	}
 	const rb::WideBvh bvh = rb::buildWideBvh(world);
 	const size_t nt = canon.size();
+	float lo[3] = { 0.0f, 0.0f, 0.0f }, hi[3] = { 0.0f, 0.0f, 0.0f };
+	for (size_t j = 0; j < world.size(); j += 3)
+		for (int k = 0; k < 3; ++k)
+		{
+			lo[k] = j ? std::min(lo[k], world[j + k]) : world[j + k];
+			hi[k] = j ? std::max(hi[k], world[j + k]) : world[j + k];
+		}
 	std::vector<float4> triVerts(3 * std::max<size_t>(nt, 1)), objVerts(3 * std::max<size_t>(nt, 1));
 	std::vector<uint2> triAux(std::max<size_t>(nt, 1));
 	for (size_t j = 0; j < nt; ++j)
@@ -535,6 +698,7 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 	G.rootIsLeaf = bvh.rootIsLeaf ? 1u : 0u;
 	ctx->scene.geo = G;
 	ctx->geoEmissive = emissivePrim;
+	for (int k = 0; k < 3; ++k) { ctx->geoMin[k] = lo[k]; ctx->geoMax[k] = hi[k]; }
 	ctx->geoMaxMaterial = 0;
 	for (uint32_t s : sbt)
 		if (s != 0xFFFFFFFFu) ctx->geoMaxMaterial = std::max(ctx->geoMaxMaterial, s + 1);
@@ -743,30 +907,100 @@ int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 	// Wave size: whole sample planes, up to the capacity (default 16M paths,
 	// about 3.2 GB of path state).
 	const uint64_t cap = ctx->requestedCapacity ? ctx->requestedCapacity : (16u << 20);
-	const uint32_t planesPerWave = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(count, cap / pixels)));
+	const bool cached = ctx->cache != nullptr;
+	const rb_cache_params& CP = ctx->cacheParams;
+	uint32_t planesPerWave = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(count, cap / pixels)));
+	if (cached) planesPerWave = std::min(planesPerWave, CP.samples_per_wave);
 	const uint32_t wavePaths = planesPerWave * pixels;
 	int rc = ensureWave(ctx, wavePaths);
 	if (rc != RB_OK) return rc;
 	const int bounces = static_cast<int>(std::min<uint32_t>(rb::kMaxBounces,
 		std::max({ sc.launch.maxDepth, sc.launch.maxReflected, sc.launch.maxTransmitted })));
+	rb::PathSoA soa = ctx->soa;
+	float posMin[3] = {}, posScale[3] = {};
+	if (cached)
+	{
+		rc = ensureCache(ctx, wavePaths, static_cast<uint32_t>(bounces));
+		if (rc != RB_OK) return rc;
+		const rb::PathSoA& c = ctx->cacheArrays;
+		soa.spread = c.spread; soa.trainRec = c.trainRec; soa.cPath = c.cPath; soa.cIn = c.cIn;
+		soa.tPath = c.tPath; soa.tIn = c.tIn; soa.tL = c.tL; soa.tT = c.tT; soa.trainCapacity = c.trainCapacity;
+		// the given box, or the geometry's bounds grown by 1 %
+		const bool given = CP.scene_min[0] < CP.scene_max[0] && CP.scene_min[1] < CP.scene_max[1] &&
+			CP.scene_min[2] < CP.scene_max[2];
+		for (int k = 0; k < 3; ++k)
+		{
+			float lo = given ? CP.scene_min[k] : ctx->geoMin[k], hi = given ? CP.scene_max[k] : ctx->geoMax[k];
+			if (!given)
+			{
+				const float pad = 0.005f * std::max(hi - lo, 1e-6f);
+				lo -= pad;
+				hi += pad;
+			}
+			posMin[k] = lo;
+			posScale[k] = hi > lo ? 1.0f / (hi - lo) : 1.0f;
+		}
+	}
 	for (uint32_t done = 0; done < count;)
 	{
 		const uint32_t planes = std::min(planesPerWave, count - done);
-		rb::WaveParams w{ planes * pixels, pixels, offset + done, (offset == 0 && done == 0) ? 1u : 0u };
+		rb::WaveParams w{};
+		w.paths = planes * pixels;
+		w.pixels = pixels;
+		w.sampleBase = offset + done;
+		w.fresh = (offset == 0 && done == 0) ? 1u : 0u;
+		w.keepFailed = ctx->failedMode == RB_FAILED_KEEP ? 1u : 0u;
+		if (cached)
+		{
+			w.cached = 1;
+			w.trainOneIn = CP.frozen ? 0u : CP.train_one_in;
+			w.trainSeed = rb::mix32(static_cast<uint32_t>(ctx->cacheWaves++) * 0x9E3779B9u + 1u);
+			w.spreadC = CP.spread_threshold;
+			w.minRoughness = CP.min_roughness;
+			for (int k = 0; k < 3; ++k) { w.posMin[k] = posMin[k]; w.posScale[k] = posScale[k]; }
+		}
 		unsigned long long* cnt = (ctx->statsMode & RB_STATS_COUNT) ? ctx->counters : nullptr;
-		cudaMemsetAsync(ctx->soa.counts, 0, sizeof(uint32_t) * rb::kCountSlots, st);
-		timedStage(ctx, 0, st, [&] { rb::launchGenerate(sc, ctx->soa, w, ctx->shape, st); });
+		cudaMemsetAsync(soa.counts, 0, sizeof(uint32_t) * rb::kCountSlots, st);
+		timedStage(ctx, 0, st, [&] { rb::launchGenerate(sc, soa, w, ctx->shape, st); });
 		for (int b = 0; b < bounces; ++b)
 		{
-			timedStage(ctx, 1, st, [&] { rb::launchExtend(sc, ctx->soa, b, ctx->shape, st, cnt); });
-			timedStage(ctx, 2, st, [&] { rb::launchSurface(sc, ctx->soa, w, b, ctx->shape, st, cnt); });
-			timedStage(ctx, 2, st, [&] { rb::launchEmission(sc, ctx->soa, b, ctx->shape, st); });
-			timedStage(ctx, 5, st, [&] { rb::launchNee(sc, ctx->soa, w, b, ctx->shape, st); });
+			timedStage(ctx, 1, st, [&] { rb::launchExtend(sc, soa, b, ctx->shape, st, cnt); });
+			timedStage(ctx, 2, st, [&] { rb::launchSurface(sc, soa, w, b, ctx->shape, st, cnt); });
+			timedStage(ctx, 2, st, [&] { rb::launchEmission(sc, soa, b, ctx->shape, st); });
+			timedStage(ctx, 5, st, [&] { rb::launchNee(sc, soa, w, b, ctx->shape, st); });
 			ctx->launches[5] += 2;   // launchNee runs the pick kernel and two light-sample kernels
-			timedStage(ctx, 6, st, [&] { rb::launchBsdf(sc, ctx->soa, w, b, ctx->shape, st); });
-			timedStage(ctx, 3, st, [&] { rb::launchShadow(sc, ctx->soa, b, ctx->shape, st, cnt); });
+			timedStage(ctx, 6, st, [&] { rb::launchBsdf(sc, soa, w, b, ctx->shape, st); });
+			timedStage(ctx, 3, st, [&] { rb::launchShadow(sc, soa, b, ctx->shape, st, cnt); });
 		}
-		timedStage(ctx, 4, st, [&] { rb::launchResolve(sc, ctx->soa, w, ctx->accum, ctx->shape, st); });
+		if (cached)
+		{
+			// answer the wave's cache queries, then train on its records
+			timedStage(ctx, 7, st, [&] {
+				rc = rb::nrc::applyQueries(ctx->cache, w.paths, soa.counts + rb::kCacheQueryCount, soa.cIn, soa.cPath,
+					soa.L, soa.T, st);
+			});
+			if (rc != RB_OK) return fail(ctx, rc, "rb_render: cache queries");
+			if (!CP.frozen)
+			{
+				const uint64_t rows = static_cast<uint64_t>(CP.targets_per_sample) * planes;
+				const uint32_t steps = static_cast<uint32_t>((rows + CP.batch - 1) / CP.batch);
+				timedStage(ctx, 8, st, [&] {
+					rb::launchTrainTargets(soa, w.keepFailed, ctx->shape.smCount, st);
+					for (uint32_t k = 0; k < steps && rc == RB_OK; ++k)
+					{
+						rb::launchTrainGather(soa, w.keepFailed, CP.batch, static_cast<uint32_t>(ctx->cacheSteps++),
+							ctx->batchIn, ctx->batchTarget, ctx->batchValid, st);
+						rc = rb::nrc::trainRows(ctx->cache, CP.batch, ctx->batchValid, ctx->batchIn, ctx->batchTarget, st,
+							true);
+					}
+				});
+				if (rc != RB_OK) return fail(ctx, rc, "rb_render: cache training");
+				ctx->launches[8] += 9 * steps;   // per step: gather + 8 network kernels (cuBLAS GEMMs not counted)
+			}
+			rb::launchCacheTally(soa, ctx->cacheTally, st);
+			++ctx->launches[8];
+		}
+		timedStage(ctx, 4, st, [&] { rb::launchResolve(sc, soa, w, ctx->accum, ctx->shape, st); });
 		done += planes;
 		ctx->pathsTraced += w.paths;
 		++ctx->waves;
@@ -977,15 +1211,8 @@ int rb_get_stats(rb_ctx* ctx, rb_render_stats* out)
 		out->shadow_rays = c[3]; out->shadow_nodes = c[4]; out->shadow_tris = c[5];
 		out->surface_records = c[6];
 	}
-	double ms[7] = {};
-	for (const auto& t : ctx->timed)
-	{
-		float v = 0.0f;
-		if (cudaEventElapsedTime(&v, t.a, t.b) == cudaSuccess) ms[t.stage] += v;
-		ctx->eventPool.push_back(t.a);
-		ctx->eventPool.push_back(t.b);
-	}
-	ctx->timed.clear();
+	drainTimed(ctx);
+	const double* ms = ctx->stageMs;
 	out->ms_generate = ms[0]; out->ms_extend = ms[1]; out->ms_shade = ms[2] + ms[5] + ms[6];
 	out->ms_shadow = ms[3]; out->ms_resolve = ms[4];
 	out->ms_surface = ms[2]; out->ms_nee = ms[5]; out->ms_bsdf = ms[6];
@@ -993,7 +1220,7 @@ int rb_get_stats(rb_ctx* ctx, rb_render_stats* out)
 	out->launches_shade = ctx->launches[2]; out->launches_shadow = ctx->launches[3]; out->launches_resolve = ctx->launches[4];
 	out->launches_nee = ctx->launches[5]; out->launches_bsdf = ctx->launches[6];
 	out->waves = ctx->waves;
-	for (uint32_t& l : ctx->launches) l = 0;
+	for (int k = 0; k < 7; ++k) { ctx->launches[k] = 0; ctx->stageMs[k] = 0.0; }
 	ctx->waves = 0;
 	return RB_OK;
 }

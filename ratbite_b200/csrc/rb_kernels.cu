@@ -26,6 +26,7 @@
 #include "rb_qrng.cuh"
 #include "rb_wavefront.h"
 #include "ratbite_b200_kernels.h"
+#include "ratbite_b200_nrc.h"
 
 namespace rb
 {
@@ -264,6 +265,11 @@ __global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, Wa
 		s.T[p] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
 		s.fd[p] = make_uint2(0u, 0u);
 		s.queue[0][p] = p;
+		if (w.cached)
+		{
+			s.spread[p] = make_float2(0.0f, 0.0f);
+			s.trainRec[p] = w.trainOneIn && mix32(p ^ w.trainSeed) % w.trainOneIn == 0 ? kNoRecord : kNotTraining;
+		}
 	}
 	if (gtid() == 0) s.counts[0] = w.paths;
 }
@@ -303,6 +309,56 @@ RB_D Qrng pathQrng(const DevScene& sc, const WaveParams& w, uint32_t p, uint32_t
 {
 	const uint32_t pix = p % w.pixels;
 	return qrngAt(w.sampleBase + p / w.pixels, pixelHash(pix % sc.launch.width, pix / sc.launch.width), depth);
+}
+
+// wavelength range of the hero sampling, for the cache's normalised input
+constexpr float kLambdaMin = 360.0f, kLambdaMax = 830.0f;
+
+// Radiance-cache form at a shaded vertex (Mueller et al. 2021, sec. 4):
+// the path spread of eq. 3 -- the first shaded vertex sets the footprint
+// a0 = d^2 / (4 pi cos), each later vertex adds sqrt(d^2 / (pdf cos)) for
+// the direction that reached it (nothing after a specular vertex). A path
+// that is not a training path terminates into the cache once
+// (summed spread)^2 > c a0 at a surface rough enough to cache (queued as a
+// query; returns true); a training path records the vertex (inputs,
+// radiance so far, throughput) instead.
+RB_D bool cacheVertex(const PathSoA& s, const WaveParams& w, uint32_t p, uint32_t flags, const f3& rayO,
+	const f3& rayD, float bxdfPdf, const f3& hitPos, const f3& gn, const f3& nrm, float lambda0, bool rough)
+{
+	const f3 toHit = hitPos - rayO;
+	const float d2 = dot(toHit, toHit);
+	const float cosHit = fmaxf(fabsf(dot(rayD, gn)), 1e-4f);
+	float2 sp = s.spread[p];
+	if (sp.x == 0.0f) sp.x = d2 / (4.0f * kPi * cosHit);   // first shaded vertex
+	else if (!(flags & PF_PREVIOUS_HIT_SPECULAR) && bxdfPdf > 0.0f) sp.y += sqrtf(d2 / (bxdfPdf * cosHit));
+	s.spread[p] = sp;
+	const uint32_t tr = s.trainRec[p];
+	const bool terminate = tr == kNotTraining && rough && sp.y > 0.0f && sp.y * sp.y > w.spreadC * sp.x;
+	if (tr == kNotTraining && !terminate) return false;
+	float in[kNrcInputs];
+	in[0] = (hitPos.x - w.posMin[0]) * w.posScale[0];
+	in[1] = (hitPos.y - w.posMin[1]) * w.posScale[1];
+	in[2] = (hitPos.z - w.posMin[2]) * w.posScale[2];
+	in[3] = -rayD.x; in[4] = -rayD.y; in[5] = -rayD.z;
+	in[6] = nrm.x; in[7] = nrm.y; in[8] = nrm.z;
+	in[9] = (lambda0 - kLambdaMin) / (kLambdaMax - kLambdaMin);
+	if (terminate)
+	{
+		const uint32_t q = appendIndex(s.counts + kCacheQueryCount);
+		s.cPath[q] = p;
+		for (int k = 0; k < kNrcInputs; ++k) s.cIn[static_cast<size_t>(kNrcInputs) * q + k] = in[k];
+		return true;
+	}
+	const uint32_t r = appendIndex(s.counts + kTrainRecordCount);
+	if (r < s.trainCapacity)
+	{
+		s.tPath[r] = p;
+		for (int k = 0; k < kNrcInputs; ++k) s.tIn[static_cast<size_t>(kNrcInputs) * r + k] = in[k];
+		s.tL[r] = s.L[p];
+		s.tT[r] = s.T[p];
+	}
+	s.trainRec[p] = r < s.trainCapacity ? r : kNoRecord;
+	return false;
 }
 
 // Stage 1 of shading: the hit record, hit emission with MIS
@@ -398,6 +454,24 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 				shadingFrame(sc, mat, it, rayD, frame, lastNormal);
 				skipped = alphaSkipped(mat, pathQrng(sc, w, p, depth));
 			}
+			if (w.cached)
+			{
+				if (!skipped && (flags & PF_TRIANGULAR_GEOMETRY))
+				{
+					const Surface sf = surfaceOf(mat);
+					const bool rough = (sf.metalness == 0.0f && sf.transmission == 0.0f) || sf.roughness >= w.minRoughness;
+					if (cacheVertex(s, w, p, flags, rayO, rayD, bxdfPdf, it.hitPos, it.gn, lastNormal,
+							s.lambda[p].x, rough))
+					{
+						s.fd[p] = make_uint2(flags | PF_FINISHED, depth);
+						continue;
+					}
+				}
+				else if (s.trainRec[p] != kNotTraining)
+				{
+					s.trainRec[p] = kNoRecord;
+				}
+			}
 			const uint32_t bits = (it.backHit ? kSfBackHit : 0u) | (skipped ? kSfSkipped : 0u)
 				| ((flags & PF_TRIANGULAR_GEOMETRY) ? kSfTriangle : 0u);
 			s.sfP[p] = f4_of(it.hitPos, __uint_as_float(it.material));
@@ -408,6 +482,10 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 			s.nrm[p] = f4_of(lastNormal, nv.w);
 			s.surfQueue[appendIndex(surfCount)] = p;
 			++records;
+		}
+		else if (w.cached && s.trainRec[p] != kNotTraining)
+		{
+			s.trainRec[p] = kNoRecord;
 		}
 		s.fd[p] = make_uint2(flags, depth);
 	}
@@ -429,9 +507,21 @@ __global__ void __launch_bounds__(kThreads) kEmission(DevScene sc, PathSoA s, in
 		float lightPdf = b.w;
 		lightPdf *= treePdf;
 		const float wgt = powerHeuristic(a.w, lightPdf);
+		const S4 c = s4(s.T[p]) * s4(s.emC[i]) * wgt;
 		S4 L = s4(s.L[p]);
-		L += s4(s.T[p]) * s4(s.emC[i]) * wgt;
+		L += c;
 		s.L[p] = f4(L);
+		if (s.trainRec)
+		{
+			// a training record of this vertex counts the emission on arrival
+			const uint32_t r = s.trainRec[p];
+			if (r < kNoRecord)
+			{
+				S4 R = s4(s.tL[r]);
+				R += c;
+				s.tL[r] = f4(R);
+			}
+		}
 	}
 }
 
@@ -690,7 +780,7 @@ __global__ void __launch_bounds__(kThreads) kResolve(DevScene sc, PathSoA s, Wav
 		{
 			const uint32_t p = k * w.pixels + pix;
 			const uint32_t flags = s.fd[p].x;
-			if (!(flags & PF_PATH_TERMINATED))
+			if (!(flags & PF_PATH_TERMINATED) || w.keepFailed)
 			{
 				S4 L = s4(s.L[p]);
 				const S4 pdf = s4(s.lpdf[p]);

@@ -35,6 +35,17 @@ RB_D void warpAdd(unsigned long long* dst, uint32_t v)
 	if ((threadIdx.x & 31u) == 0 && s) atomicAdd(dst, s);
 }
 
+// 32-bit integer hash (the "lowbias32" finaliser: xorshift-multiply rounds).
+RB_HD uint32_t mix32(uint32_t x)
+{
+	x ^= x >> 16;
+	x *= 0x7feb352du;
+	x ^= x >> 15;
+	x *= 0x846ca68bu;
+	x ^= x >> 16;
+	return x;
+}
+
 // Grid for a one-thread-per-item batch kernel (grid-stride loops cover the rest).
 inline int gridFor(uint32_t n)
 {

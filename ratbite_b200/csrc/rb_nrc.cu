@@ -9,7 +9,9 @@
 // Network input (64): 32 grid features, direction and normal mapped to
 // [0, 1], the normalised hero wavelength, a constant 1, zero padding. Four
 // hidden layers of 64 with ReLU, a linear output of 4 (radiance at the four
-// hero wavelengths). No biases except through the constant input.
+// hero wavelengths) plus a fifth, the probability that the plain estimator
+// would drop the sample, which only the renderer's cached form trains. No
+// biases except through the constant input.
 //
 // Tensor cores: the fused forward kernel keeps a 16-row tile of activations
 // in registers as mma.sync m16n8k16 BF16 fragments (FP32 accumulation); an
@@ -28,6 +30,7 @@
 
 #include "rb_launch.cuh"
 #include "ratbite_b200_nrc.h"
+#include "rb_nrc_internal.h"
 
 namespace rb
 {
@@ -41,6 +44,8 @@ __host__ __device__ constexpr int wOffset(int l) { return l < 5 ? l * kH * kH : 
 constexpr int kWTotal = wOffset(5);                     // 17408 weights
 constexpr int kWStride = 72;                            // smem row stride (bf16), conflict-free fragment loads
 constexpr int kTile = 16;                               // rows per warp tile
+constexpr int kOutStride = 8;                           // forward outputs per row in the training scratch
+constexpr int kDropOutput = 4;                          // output trained by the renderer: drop probability
 
 struct Resolutions { float s[kLevels]; uint32_t dense[kLevels]; uint32_t side[kLevels]; };
 
@@ -51,6 +56,35 @@ RB_D uint32_t cellIndex(const Resolutions& R, int l, uint32_t x, uint32_t y, uin
 }
 
 // ---------------------------------------------------------------- encoding
+// The two features of level l at a position in [0,1]^3: trilinear in the cell.
+RB_D void levelFeatures(const Resolutions& R, const __half2* __restrict__ grid, int l, float px, float py, float pz,
+	float& f0, float& f1)
+{
+	const float sx = px * R.s[l], sy = py * R.s[l], sz = pz * R.s[l];
+	const float fx = floorf(sx), fy = floorf(sy), fz = floorf(sz);
+	const float wx = sx - fx, wy = sy - fy, wz = sz - fz;
+	const uint32_t cx = static_cast<uint32_t>(fx), cy = static_cast<uint32_t>(fy), cz = static_cast<uint32_t>(fz);
+	f0 = 0.0f;
+	f1 = 0.0f;
+	for (int c = 0; c < 8; ++c)
+	{
+		const uint32_t dx = c & 1u, dy = (c >> 1) & 1u, dz = (c >> 2) & 1u;
+		const float w = (dx ? wx : 1.0f - wx) * (dy ? wy : 1.0f - wy) * (dz ? wz : 1.0f - wz);
+		const float2 e = __half22float2(grid[static_cast<size_t>(l) * kTable + cellIndex(R, l, cx + dx, cy + dy, cz + dz)]);
+		f0 += w * e.x;
+		f1 += w * e.y;
+	}
+}
+RB_D float clamp01(float v) { return fminf(fmaxf(v, 0.0f), 1.0f); }
+// Columns 32..63 of an input row: direction and normal mapped to [0,1], the
+// wavelength, a constant 1, zeros.
+RB_D float restColumn(const float* v, int k)
+{
+	if (k < 6) return v[3 + k] * 0.5f + 0.5f;
+	if (k == 6) return v[9];
+	return k == 7 ? 1.0f : 0.0f;
+}
+
 __global__ void kEncode(uint32_t n, const float* __restrict__ in, const __half2* __restrict__ grid, Resolutions R,
 	__nv_bfloat16* __restrict__ X)
 {
@@ -58,35 +92,15 @@ __global__ void kEncode(uint32_t n, const float* __restrict__ in, const __half2*
 	{
 		const float* v = in + static_cast<size_t>(kNrcInputs) * i;
 		__nv_bfloat16* row = X + static_cast<size_t>(kIn) * i;
-		const float px = fminf(fmaxf(v[0], 0.0f), 1.0f), py = fminf(fmaxf(v[1], 0.0f), 1.0f),
-			pz = fminf(fmaxf(v[2], 0.0f), 1.0f);
+		const float px = clamp01(v[0]), py = clamp01(v[1]), pz = clamp01(v[2]);
 		for (int l = 0; l < kLevels; ++l)
 		{
-			const float sx = px * R.s[l], sy = py * R.s[l], sz = pz * R.s[l];
-			const float fx = floorf(sx), fy = floorf(sy), fz = floorf(sz);
-			const float wx = sx - fx, wy = sy - fy, wz = sz - fz;
-			const uint32_t cx = static_cast<uint32_t>(fx), cy = static_cast<uint32_t>(fy), cz = static_cast<uint32_t>(fz);
-			float f0 = 0.0f, f1 = 0.0f;
-			for (int c = 0; c < 8; ++c)
-			{
-				const uint32_t dx = c & 1u, dy = (c >> 1) & 1u, dz = (c >> 2) & 1u;
-				const float w = (dx ? wx : 1.0f - wx) * (dy ? wy : 1.0f - wy) * (dz ? wz : 1.0f - wz);
-				const float2 e = __half22float2(grid[static_cast<size_t>(l) * kTable + cellIndex(R, l, cx + dx, cy + dy, cz + dz)]);
-				f0 += w * e.x;
-				f1 += w * e.y;
-			}
+			float f0, f1;
+			levelFeatures(R, grid, l, px, py, pz, f0, f1);
 			row[2 * l] = __float2bfloat16_rn(f0);
 			row[2 * l + 1] = __float2bfloat16_rn(f1);
 		}
-		row[32] = __float2bfloat16_rn(v[3] * 0.5f + 0.5f);
-		row[33] = __float2bfloat16_rn(v[4] * 0.5f + 0.5f);
-		row[34] = __float2bfloat16_rn(v[5] * 0.5f + 0.5f);
-		row[35] = __float2bfloat16_rn(v[6] * 0.5f + 0.5f);
-		row[36] = __float2bfloat16_rn(v[7] * 0.5f + 0.5f);
-		row[37] = __float2bfloat16_rn(v[8] * 0.5f + 0.5f);
-		row[38] = __float2bfloat16_rn(v[9]);
-		row[39] = __float2bfloat16_rn(1.0f);
-		for (int k = 40; k < kIn; ++k) row[k] = __float2bfloat16_rn(0.0f);
+		for (int k = 0; k < 32; ++k) row[32 + k] = __float2bfloat16_rn(restColumn(v, k));
 	}
 }
 
@@ -98,8 +112,7 @@ __global__ void kEncodeBackward(uint32_t n, const float* __restrict__ in, const 
 	{
 		const float* v = in + static_cast<size_t>(kNrcInputs) * i;
 		const float* g = dX0 + static_cast<size_t>(kGridFeatures) * i;
-		const float px = fminf(fmaxf(v[0], 0.0f), 1.0f), py = fminf(fmaxf(v[1], 0.0f), 1.0f),
-			pz = fminf(fmaxf(v[2], 0.0f), 1.0f);
+		const float px = clamp01(v[0]), py = clamp01(v[1]), pz = clamp01(v[2]);
 		for (int l = 0; l < kLevels; ++l)
 		{
 			const float g0 = g[2 * l], g1 = g[2 * l + 1];
@@ -112,9 +125,9 @@ __global__ void kEncodeBackward(uint32_t n, const float* __restrict__ in, const 
 			{
 				const uint32_t dx = c & 1u, dy = (c >> 1) & 1u, dz = (c >> 2) & 1u;
 				const float w = (dx ? wx : 1.0f - wx) * (dy ? wy : 1.0f - wy) * (dz ? wz : 1.0f - wz);
-				float* e = gridGrad + 2 * (static_cast<size_t>(l) * kTable + cellIndex(R, l, cx + dx, cy + dy, cz + dz));
-				atomicAdd(e, w * g0);
-				atomicAdd(e + 1, w * g1);
+				float2* e = reinterpret_cast<float2*>(gridGrad) + static_cast<size_t>(l) * kTable
+					+ cellIndex(R, l, cx + dx, cy + dy, cz + dz);
+				atomicAdd(e, make_float2(w * g0, w * g1));
 			}
 		}
 	}
@@ -227,7 +240,8 @@ constexpr size_t kSmemWeights = sizeof(__nv_bfloat16) * kWRowsTotal * kWStride;
 constexpr int kWtRows = 64 + 4 * 64;
 constexpr size_t kSmemBackward = sizeof(__nv_bfloat16) * kWtRows * kWStride;
 
-// Forward: out[n][4] (FP32). With acts, the post-ReLU hidden activations of
+// Forward: out[n][kOutStride] (FP32; outputs 0..3 radiance, 4 the drop
+// probability the renderer trains, 5..7 unused). With acts, the post-ReLU hidden activations of
 // layers 1..4 are stored ([4][n][64] bf16) for the backward pass.
 __global__ void __launch_bounds__(128) kMlpForward(uint32_t n, const __nv_bfloat16* __restrict__ X,
 	const __nv_bfloat16* __restrict__ w, float* __restrict__ out, __nv_bfloat16* __restrict__ acts)
@@ -250,32 +264,133 @@ __global__ void __launch_bounds__(128) kMlpForward(uint32_t n, const __nv_bfloat
 		}
 		float O[1][4];
 		layer<1>(A, sw + wOffset(4) / kH * kWStride, O);
-		// O: rows g, g+8; cols 2c, 2c+1 -> outputs 0..3 live in lanes with c < 2
-		if (c < 2)
+		// O: rows g, g+8; cols 2c, 2c+1: the first 8 output rows of W4
+		const uint32_t ra = r0 + g, rb = r0 + g + 8;
+		if (ra < n) { out[kOutStride * ra + 2 * c] = O[0][0]; out[kOutStride * ra + 2 * c + 1] = O[0][1]; }
+		if (rb < n) { out[kOutStride * rb + 2 * c] = O[0][2]; out[kOutStride * rb + 2 * c + 1] = O[0][3]; }
+	}
+}
+
+// Inference with the encoding fused in: each warp encodes its 16-row tile
+// into a shared-memory tile (lanes split the 16 rows x 16 levels of grid
+// lookups, then the 32 remaining columns), reads the A fragments from it and
+// runs the layers as kMlpForward. Rows: min(*count, cap) when count is given,
+// else cap. Outputs 0..3 go to out[rows][4] and/or, with path, are applied
+// as L[p] = L[p] (1 - q) + T[p] max(y, 0), p = path[r], q = output 4
+// clamped to [0, 1] (radiance-cache queries).
+constexpr size_t kSmemInfer = kSmemWeights + sizeof(__nv_bfloat16) * 4 * kTile * kWStride;
+__global__ void __launch_bounds__(128) kMlpInfer(uint32_t cap, const uint32_t* __restrict__ count,
+	const float* __restrict__ in, const __half2* __restrict__ grid, Resolutions R, const __nv_bfloat16* __restrict__ w,
+	float* __restrict__ out, const uint32_t* __restrict__ path, float4* __restrict__ L, const float4* __restrict__ T)
+{
+	extern __shared__ __nv_bfloat16 sw[];
+	stageWeights(w, sw);
+	const uint32_t n = count ? min(*count, cap) : cap;
+	__nv_bfloat16* tile = sw + kWRowsTotal * kWStride + (threadIdx.x >> 5) * kTile * kWStride;
+	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
+	const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, c = lane & 3u;
+	for (uint32_t r0 = warp * kTile; r0 < n; r0 += warps * kTile)
+	{
+		// grid features: lane handles (row k / 16, level k % 16) for k = lane + 32 i
+#pragma unroll 2
+		for (uint32_t k = lane; k < kTile * kLevels; k += 32)
 		{
-			const uint32_t ra = r0 + g, rb = r0 + g + 8;
-			if (ra < n) { out[4 * ra + 2 * c] = O[0][0]; out[4 * ra + 2 * c + 1] = O[0][1]; }
-			if (rb < n) { out[4 * rb + 2 * c] = O[0][2]; out[4 * rb + 2 * c + 1] = O[0][3]; }
+			const uint32_t row = k >> 4, l = k & 15u, r = r0 + row;
+			float f0 = 0.0f, f1 = 0.0f;
+			if (r < n)
+			{
+				const float* v = in + static_cast<size_t>(kNrcInputs) * r;
+				levelFeatures(R, grid, static_cast<int>(l), clamp01(v[0]), clamp01(v[1]), clamp01(v[2]), f0, f1);
+			}
+			*reinterpret_cast<uint32_t*>(tile + row * kWStride + 2 * l) = pack2(f0, f1);
+		}
+		// columns 32..63: lane handles 16 columns of row lane / 2
+		{
+			const uint32_t row = lane >> 1, r = r0 + row, k0 = 16 * (lane & 1u);
+			const float* v = in + static_cast<size_t>(kNrcInputs) * r;
+#pragma unroll
+			for (uint32_t k = 0; k < 16; k += 2)
+			{
+				const float a = r < n ? restColumn(v, static_cast<int>(k0 + k)) : 0.0f;
+				const float b = r < n ? restColumn(v, static_cast<int>(k0 + k + 1)) : 0.0f;
+				*reinterpret_cast<uint32_t*>(tile + row * kWStride + 32 + k0 + k) = pack2(a, b);
+			}
+		}
+		__syncwarp();
+		uint32_t A[4][4];
+#pragma unroll
+		for (int t = 0; t < 4; ++t)
+		{
+			const uint32_t k0 = 16 * t + 2 * c;
+			A[t][0] = *reinterpret_cast<const uint32_t*>(tile + g * kWStride + k0);
+			A[t][1] = *reinterpret_cast<const uint32_t*>(tile + (g + 8) * kWStride + k0);
+			A[t][2] = *reinterpret_cast<const uint32_t*>(tile + g * kWStride + k0 + 8);
+			A[t][3] = *reinterpret_cast<const uint32_t*>(tile + (g + 8) * kWStride + k0 + 8);
+		}
+		__syncwarp();
+		float C[8][4];
+#pragma unroll
+		for (int l = 0; l < 4; ++l)
+		{
+			layer<8>(A, sw + wOffset(l) / kH * kWStride, C);
+			toA(C, A, true);
+		}
+		float O[1][4];
+		layer<1>(A, sw + wOffset(4) / kH * kWStride, O);
+		// lanes c = 0 hold outputs 0, 1, lanes c = 1 outputs 2, 3 and lanes
+		// c = 2 output 4 (drop probability) of rows g and g + 8
+		const float a2 = __shfl_down_sync(0xFFFFFFFFu, O[0][0], 1), a3 = __shfl_down_sync(0xFFFFFFFFu, O[0][1], 1);
+		const float b2 = __shfl_down_sync(0xFFFFFFFFu, O[0][2], 1), b3 = __shfl_down_sync(0xFFFFFFFFu, O[0][3], 1);
+		const float aq = __shfl_down_sync(0xFFFFFFFFu, O[0][0], 2), bq = __shfl_down_sync(0xFFFFFFFFu, O[0][2], 2);
+		if (c == 0)
+		{
+			const uint32_t rows[2] = { r0 + g, r0 + g + 8 };
+			const float4 y[2] = { make_float4(O[0][0], O[0][1], a2, a3), make_float4(O[0][2], O[0][3], b2, b3) };
+			const float q[2] = { aq, bq };
+#pragma unroll
+			for (int h = 0; h < 2; ++h)
+			{
+				if (rows[h] >= n) continue;
+				if (out) reinterpret_cast<float4*>(out)[rows[h]] = y[h];
+				if (path)
+				{
+					// the plain estimator drops a whole sample whose later BxDF
+					// sample fails: the prefix survives with 1 - q
+					const uint32_t p = path[rows[h]];
+					const float4 t = T[p];
+					const float keep = fminf(fmaxf(1.0f - q[h], 0.0f), 1.0f);
+					float4 l = L[p];
+					l.x = l.x * keep + t.x * fmaxf(y[h].x, 0.0f);
+					l.y = l.y * keep + t.y * fmaxf(y[h].y, 0.0f);
+					l.z = l.z * keep + t.z * fmaxf(y[h].z, 0.0f);
+					l.w = l.w * keep + t.w * fmaxf(y[h].w, 0.0f);
+					L[p] = l;
+				}
+			}
 		}
 	}
 }
 
-// Relative L2 loss (Mueller et al. 2021): sum over outputs of
-// (y - t)^2 / (sg(y)^2 + 0.01), averaged over the batch; dY is written as
-// bf16 rows of 16 (4 used) and the loss sum accumulated.
+// Relative L2 loss (Mueller et al. 2021): sum over the first `outs` outputs
+// of (y - t)^2 / (sg(y)^2 + 0.01), averaged over the batch; targets are rows
+// of tStride floats; dY is written as bf16 rows of 16 and the loss sum
+// accumulated. With valid, only the first min(*valid, n) rows count (the
+// others get a zero gradient).
 __global__ void kLoss(uint32_t n, const float* __restrict__ y, const float* __restrict__ t,
-	__nv_bfloat16* __restrict__ dY, float* __restrict__ lossSum)
+	__nv_bfloat16* __restrict__ dY, float* __restrict__ lossSum, const uint32_t* __restrict__ valid, int outs,
+	int tStride)
 {
 	float local = 0.0f;
-	const float scale = 1.0f / static_cast<float>(n);
+	const uint32_t nv = valid ? min(*valid, n) : n;
+	const float scale = nv ? 1.0f / static_cast<float>(nv) : 0.0f;
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
 		for (int k = 0; k < kOutPad; ++k)
 		{
 			float gk = 0.0f;
-			if (k < 4)
+			if (k < outs && i < nv)
 			{
-				const float yy = y[4 * i + k], tt = t[4 * i + k];
+				const float yy = y[kOutStride * i + k], tt = t[static_cast<size_t>(tStride) * i + k];
 				const float den = yy * yy + 0.01f;
 				const float d = yy - tt;
 				local += d * d / den;
@@ -367,24 +482,49 @@ __global__ void __launch_bounds__(128) kMlpBackward(uint32_t n, const __nv_bfloa
 }
 
 // ---------------------------------------------------------------- optimiser
+// Adam on float4 groups (n must be a multiple of 4: both parameter tables
+// are); the gradient is cleared, and the bf16 / fp16 copies refreshed.
+RB_D void adam1(float& p, float g, float& m, float& v, float lr, float b1, float b2, float eps, float c1, float c2)
+{
+	m = b1 * m + (1.0f - b1) * g;
+	v = b2 * v + (1.0f - b2) * g * g;
+	p = p - lr * (m / c1) / (sqrtf(v / c2) + eps);
+}
 __global__ void kAdam(uint32_t n, float* __restrict__ p, float* __restrict__ grad, float* __restrict__ m,
 	float* __restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2, __nv_bfloat16* outBf16,
 	__half* outF16)
 {
-	for (uint32_t i = gtid(); i < n; i += gstride())
+	float4* P = reinterpret_cast<float4*>(p);
+	float4* G = reinterpret_cast<float4*>(grad);
+	float4* M = reinterpret_cast<float4*>(m);
+	float4* V = reinterpret_cast<float4*>(v);
+	for (uint32_t i = gtid(); i < n / 4; i += gstride())
 	{
-		const float gr = grad[i];
-		const float mm = b1 * m[i] + (1.0f - b1) * gr;
-		const float vv = b2 * v[i] + (1.0f - b2) * gr * gr;
-		m[i] = mm;
-		v[i] = vv;
-		const float w = p[i] - lr * (mm / c1) / (sqrtf(vv / c2) + eps);
-		p[i] = w;
-		grad[i] = 0.0f;
-		if (outBf16) outBf16[i] = __float2bfloat16_rn(w);
-		if (outF16) outF16[i] = __float2half_rn(w);
+		float4 pp = P[i], mm = M[i], vv = V[i];
+		const float4 gg = G[i];
+		adam1(pp.x, gg.x, mm.x, vv.x, lr, b1, b2, eps, c1, c2);
+		adam1(pp.y, gg.y, mm.y, vv.y, lr, b1, b2, eps, c1, c2);
+		adam1(pp.z, gg.z, mm.z, vv.z, lr, b1, b2, eps, c1, c2);
+		adam1(pp.w, gg.w, mm.w, vv.w, lr, b1, b2, eps, c1, c2);
+		P[i] = pp;
+		M[i] = mm;
+		V[i] = vv;
+		G[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+		if (outBf16)
+		{
+			__nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(outBf16) + 2 * i;
+			o[0] = __floats2bfloat162_rn(pp.x, pp.y);
+			o[1] = __floats2bfloat162_rn(pp.z, pp.w);
+		}
+		if (outF16)
+		{
+			__half2* o = reinterpret_cast<__half2*>(outF16) + 2 * i;
+			o[0] = __floats2half2_rn(pp.x, pp.y);
+			o[1] = __floats2half2_rn(pp.z, pp.w);
+		}
 	}
 }
+static_assert(kWTotal % 4 == 0 && (kLevels * kTable * kFeat) % 4 == 0, "kAdam works on float4 groups");
 
 // transposed bf16 copies of the weights for the backward kernel
 __global__ void kTransposeWeights(const float* __restrict__ w, __nv_bfloat16* __restrict__ wt)
@@ -460,7 +600,7 @@ int growScratch(rb_nrc* h, uint32_t n)
 	if (e == cudaSuccess) e = cudaMalloc(&h->acts, sizeof(__nv_bfloat16) * 4 * kIn * n);
 	if (e == cudaSuccess) e = cudaMalloc(&h->dY, sizeof(__nv_bfloat16) * kOutPad * n);
 	if (e == cudaSuccess) e = cudaMalloc(&h->dH, sizeof(__nv_bfloat16) * 4 * kIn * n);
-	if (e == cudaSuccess) e = cudaMalloc(&h->out, sizeof(float) * 4 * n);
+	if (e == cudaSuccess) e = cudaMalloc(&h->out, sizeof(float) * kOutStride * n);
 	if (e == cudaSuccess) e = cudaMalloc(&h->dX0, sizeof(float) * kGridFeatures * n);
 	if (e != cudaSuccess) return nrcFail(e);
 	h->cap = n;
@@ -541,6 +681,8 @@ int rb_nrc_create(const rb_nrc_config* config, rb_nrc** out)
 		static_cast<int>(kSmemWeights));
 	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpBackward), cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(kSmemBackward));
+	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpInfer), cudaFuncAttributeMaxDynamicSharedMemorySize,
+		static_cast<int>(kSmemInfer));
 	*out = h;
 	return RB_OK;
 }
@@ -592,13 +734,12 @@ int rb_nrc_get_parameters(rb_nrc* h, float* grid, float* weights)
 int rb_nrc_infer(rb_nrc* h, uint32_t n, const float* inputs, float* outputs, void* stream)
 {
 	if (!h || (n && (!inputs || !outputs))) return RB_ERR_INVALID;
+	if (reinterpret_cast<uintptr_t>(outputs) & 15u) return RB_ERR_INVALID;
 	if (n == 0) return RB_OK;
 	cudaSetDevice(h->device);
-	const int rc = growScratch(h, n);
-	if (rc != RB_OK) return rc;
 	const cudaStream_t st = static_cast<cudaStream_t>(stream);
-	kEncode<<<gridFor(n), kThreads, 0, st>>>(n, inputs, reinterpret_cast<const __half2*>(h->grid), h->R, h->X);
-	kMlpForward<<<blocksFor(h, n), 128, kSmemWeights, st>>>(n, h->X, h->w, outputs, nullptr);
+	kMlpInfer<<<blocksFor(h, n), 128, kSmemInfer, st>>>(n, nullptr, inputs, reinterpret_cast<const __half2*>(h->grid),
+		h->R, h->w, outputs, nullptr, nullptr, nullptr);
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
 
@@ -606,14 +747,15 @@ namespace
 {
 // Forward, loss, backward: accumulates the batch's gradients into wGrad and
 // gridGrad (which the optimiser step or rb_nrc_gradients consume).
-int computeGradients(rb_nrc* h, uint32_t n, const float* inputs, const float* targets, cudaStream_t st)
+int computeGradients(rb_nrc* h, uint32_t n, const float* inputs, const float* targets, cudaStream_t st,
+	const uint32_t* valid = nullptr, int outs = 4, int tStride = 4)
 {
 	int rc = growScratch(h, n);
 	if (rc != RB_OK) return rc;
 	cudaMemsetAsync(h->loss, 0, sizeof(float), st);
 	kEncode<<<gridFor(n), kThreads, 0, st>>>(n, inputs, reinterpret_cast<const __half2*>(h->grid), h->R, h->X);
 	kMlpForward<<<blocksFor(h, n), 128, kSmemWeights, st>>>(n, h->X, h->w, h->out, h->acts);
-	kLoss<<<gridFor(n), kThreads, 0, st>>>(n, h->out, targets, h->dY, h->loss);
+	kLoss<<<gridFor(n), kThreads, 0, st>>>(n, h->out, targets, h->dY, h->loss, valid, outs, tStride);
 	kMlpBackward<<<blocksFor(h, n), 128, kSmemBackward, st>>>(n, h->dY, h->wt, h->acts, h->dH, h->dX0);
 	// weight gradients: dW_l[out][in] = sum over rows dY_l[r][out] X_l[r][in]
 	// (column-major view: dW^T = X^T dY with X [n][64] row-major = X^T column-major)
@@ -659,7 +801,36 @@ int rb_nrc_train(rb_nrc* h, uint32_t n, const float* inputs, const float* target
 	if (!h || n == 0 || !inputs || !targets) return RB_ERR_INVALID;
 	cudaSetDevice(h->device);
 	const cudaStream_t st = static_cast<cudaStream_t>(stream);
-	const int rc = computeGradients(h, n, inputs, targets, st);
+	const int rc = rb::nrc::trainRows(h, n, nullptr, inputs, targets, st, false);
+	if (rc != RB_OK) return rc;
+	if (loss_out) cudaMemcpyAsync(loss_out, h->loss, sizeof(float), cudaMemcpyDefault, st);
+	const cudaError_t e = cudaGetLastError();
+	return e == cudaSuccess ? RB_OK : RB_ERR_CUDA;
+}
+
+} // extern "C"
+
+namespace rb
+{
+namespace nrc
+{
+int applyQueries(rb_nrc* h, uint32_t cap, const uint32_t* count, const float* inputs, const uint32_t* path, float4* L,
+	const float4* T, cudaStream_t st)
+{
+	if (cap == 0) return RB_OK;
+	kMlpInfer<<<blocksFor(h, cap), 128, kSmemInfer, st>>>(cap, count, inputs, reinterpret_cast<const __half2*>(h->grid),
+		h->R, h->w, nullptr, path, L, T);
+	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
+}
+
+const float* lossDevice(const rb_nrc* h) { return h->loss; }
+int deviceOf(const rb_nrc* h) { return h->device; }
+
+int trainRows(rb_nrc* h, uint32_t n, const uint32_t* valid, const float* inputs, const float* targets, cudaStream_t st,
+	bool withDrop)
+{
+	const int rc = withDrop ? computeGradients(h, n, inputs, targets, st, valid, kDropOutput + 1, 8)
+		: computeGradients(h, n, inputs, targets, st, valid);
 	if (rc != RB_OK) return rc;
 	++h->step;
 	const float b1 = h->cfg.beta1, b2 = h->cfg.beta2;
@@ -669,9 +840,7 @@ int rb_nrc_train(rb_nrc* h, uint32_t n, const float* inputs, const float* target
 	kAdam<<<64, 256, 0, st>>>(kWTotal, h->wF32, h->wGrad, h->wM, h->wV, h->cfg.learning_rate, b1, b2, h->cfg.epsilon,
 		c1, c2, h->w, nullptr);
 	kTransposeWeights<<<64, 256, 0, st>>>(h->wF32, h->wt);
-	if (loss_out) cudaMemcpyAsync(loss_out, h->loss, sizeof(float), cudaMemcpyDefault, st);
-	const cudaError_t e = cudaGetLastError();
-	return e == cudaSuccess ? RB_OK : RB_ERR_CUDA;
+	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
-
-} // extern "C"
+} // namespace nrc
+} // namespace rb

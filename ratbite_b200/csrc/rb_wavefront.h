@@ -46,7 +46,24 @@ struct PathSoA
 	uint32_t* shadowQueue;
 	uint32_t* counts;  // kCountSlots words: see kShadowCounts, kSurfaceCounts
 	uint32_t capacity;
+	// radiance-cache form (all null without a cache): per path, the spread
+	// (primary footprint a0, summed spread) and, for training paths, the
+	// record of the current vertex (kNoRecord: none this vertex; kNotTraining
+	// for the other paths); cache queries (path, kNrcInputs floats); training
+	// records (path, inputs, radiance at the vertex then the target,
+	// throughput at the vertex)
+	float2* spread;
+	uint32_t* trainRec;
+	uint32_t* cPath;
+	float* cIn;
+	uint32_t* tPath;
+	float* tIn;
+	float4* tL;
+	float4* tT;
+	uint32_t trainCapacity;
 };
+constexpr uint32_t kNotTraining = 0xFFFFFFFFu;
+constexpr uint32_t kNoRecord = 0xFFFFFFFEu;
 constexpr int kMaxBounces = 64;
 // counts[b]: paths entering bounce b; counts[kShadowCounts + b]: shadow rays
 // of bounce b; counts[kSurfaceCounts + b]: surface records of bounce b;
@@ -54,7 +71,8 @@ constexpr int kMaxBounces = 64;
 // which the persistent traversal warps take their next rays;
 // counts[kEmissionCounts + b]: deferred emission-MIS records of bounce b;
 // counts[kNeeTreeCounts + b], counts[kNeeSkyCounts + b]: light-sample records
-// by light choice.
+// by light choice; counts[kCacheQueryCount], counts[kTrainRecordCount]:
+// radiance-cache queries and training records of the wave (all bounces).
 constexpr uint32_t kShadowCounts = kMaxBounces + 1;
 constexpr uint32_t kSurfaceCounts = 2 * (kMaxBounces + 1);
 constexpr uint32_t kExtendFetch = 3 * (kMaxBounces + 1);
@@ -62,7 +80,9 @@ constexpr uint32_t kShadowFetch = 4 * (kMaxBounces + 1);
 constexpr uint32_t kEmissionCounts = 5 * (kMaxBounces + 1);
 constexpr uint32_t kNeeTreeCounts = 6 * (kMaxBounces + 1);
 constexpr uint32_t kNeeSkyCounts = 7 * (kMaxBounces + 1);
-constexpr uint32_t kCountSlots = 8 * (kMaxBounces + 1);
+constexpr uint32_t kCacheQueryCount = 8 * (kMaxBounces + 1);
+constexpr uint32_t kTrainRecordCount = kCacheQueryCount + 1;
+constexpr uint32_t kCountSlots = kCacheQueryCount + 2;
 
 struct WaveParams
 {
@@ -70,6 +90,14 @@ struct WaveParams
 	uint32_t pixels;       // W*H
 	uint32_t sampleBase;   // absolute sample index of plane 0 of the wave
 	uint32_t fresh;        // 1: accumulation starts from zero (first wave of a launch at offset 0)
+	uint32_t keepFailed;   // 1: a path with the terminated flag keeps its radiance (RB_FAILED_KEEP)
+	// radiance-cache form
+	uint32_t cached;       // 1: paths terminate into the cache (PathSoA cache arrays are set)
+	uint32_t trainOneIn;   // one path in trainOneIn is a training path (0: none)
+	uint32_t trainSeed;    // varies the training paths from wave to wave
+	float spreadC;         // terminate once (summed spread)^2 > spreadC * a0
+	float minRoughness;    // ... at a surface that is not metallic or transmissive, or at least this rough
+	float posMin[3], posScale[3];  // hit position -> [0,1]^3
 };
 
 struct LaunchShape
@@ -101,6 +129,17 @@ void queryTraceShape(LaunchShape& ls);   // fills blocksExtend, blocksShadow (rb
 void launchShadow(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
 	unsigned long long* counters);
 void launchResolve(const DevScene& sc, const PathSoA& s, const WaveParams& w, double4* accum, const LaunchShape& ls, cudaStream_t st);
+// Radiance-cache form, after the last bounce of a wave: training targets
+// (L_final - L_vertex) / T_vertex in place of the records' radiance (0 for a
+// dropped path), then n training rows drawn from them (step: varies the
+// draw) into in (kNrcInputs floats) and target (8 floats: radiance, drop
+// flag, unused) with valid = n (or 0 without records). keepFailed:
+// RB_FAILED_KEEP (a path with the terminated flag is not dropped).
+void launchTrainTargets(const PathSoA& s, uint32_t keepFailed, int smCount, cudaStream_t st);
+void launchTrainGather(const PathSoA& s, uint32_t keepFailed, uint32_t n, uint32_t step, float* in, float* target,
+	uint32_t* valid, cudaStream_t st);
+// tally[0] += queries, tally[1] += training records of the wave.
+void launchCacheTally(const PathSoA& s, unsigned long long* tally, cudaStream_t st);
 
 // Per-function batch kernels (include/ratbite_b200_kernels.h).
 void launchSobol(uint32_t n, uint32_t dims, const uint32_t* sample, const uint32_t* hash, const uint32_t* bounce,

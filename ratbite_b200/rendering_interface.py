@@ -21,12 +21,14 @@ def _ptr(a: np.ndarray):
 
 
 class RenderingInterface:
-    def __init__(self, device: int = 0, max_paths_in_flight: int = 0, envmap_cdf_mode: int = abi.RB_CDF_FP64):
+    def __init__(self, device: int = 0, max_paths_in_flight: int = 0, envmap_cdf_mode: int = abi.RB_CDF_FP64,
+                 failed_sample_mode: int = abi.RB_FAILED_DROP):
         self.lib = load()
         cfg = abi.rb_config()
         cfg.device = device
         cfg.max_paths_in_flight = max_paths_in_flight
         cfg.envmap_cdf_mode = envmap_cdf_mode
+        cfg.failed_sample_mode = failed_sample_mode
         h = C.c_void_p()
         check(self.lib.rb_create(C.byref(cfg), C.byref(h)), None, "rb_create")
         self.ctx = h
@@ -198,4 +200,35 @@ class RenderingInterface:
     def status(self) -> abi.rb_device_status:
         st = abi.rb_device_status()
         check(self.lib.rb_status(self.ctx, C.byref(st)), self.ctx, "rb_status")
+        return st
+
+    # ---- radiance-cache form (include/ratbite_b200_nrc.h) -------------------
+    def attach_radiance_cache(self, cache, spread_threshold: float = 0.0, train_one_in: int = 0,
+                              targets_per_sample: int = 0, batch: int = 0, frozen: bool = False,
+                              samples_per_wave: int = 0, scene_bounds=None, min_roughness: float = 0.0):
+        """Renders through `cache` (a RadianceCache, or None to detach);
+        zero arguments take the library's defaults."""
+        if cache is None:
+            check(self.lib.rb_attach_radiance_cache(self.ctx, None, None), self.ctx, "rb_attach_radiance_cache")
+            self._cache = None
+            return
+        p = abi.rb_cache_params()
+        p.spread_threshold = spread_threshold
+        p.train_one_in = train_one_in
+        p.targets_per_sample = targets_per_sample
+        p.batch = batch
+        p.frozen = 1 if frozen else 0
+        p.samples_per_wave = samples_per_wave
+        p.min_roughness = min_roughness
+        if scene_bounds is not None:
+            lo, hi = scene_bounds
+            p.scene_min[:] = [float(v) for v in lo]
+            p.scene_max[:] = [float(v) for v in hi]
+        check(self.lib.rb_attach_radiance_cache(self.ctx, cache.h, C.byref(p)), self.ctx,
+              "rb_attach_radiance_cache")
+        self._cache = cache   # the cache must outlive the attachment
+
+    def cache_stats(self) -> abi.rb_cache_stats:
+        st = abi.rb_cache_stats()
+        check(self.lib.rb_get_cache_stats(self.ctx, C.byref(st)), self.ctx, "rb_get_cache_stats")
         return st
