@@ -9,6 +9,12 @@ one frame: CDF rebuild + 530,841,600 paths. Metric: paths per second.
 `--workload cornell` selects the small configuration (Cornell box, 256x256,
 64 spp, depth 8).
 
+On one GPU the line also carries `time_to_rmse`: the radiance-cached form
+against the plain tracer on the Cornell box at 1920x1080, depth 12 -- device
+seconds until each reaches the plain tracer's 1024-spp RMSE against a
+4096-spp FP64-accumulated plain render (time_to_rmse() below; --no-ttr skips
+it).
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 ours       renders through the C ABI (libratbite_b200.so). `value` is device
@@ -40,12 +46,19 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "paths/s"
+# The headline: paths/s of the plain tracer (`value`), and the cached form's
+# time to the plain tracer's 1024-spp RMSE against the FP64 oracle
+# (`time_to_rmse`, one B200).
+METRIC = "paths/s and time-to-RMSE vs FP64 oracle: guided/cached vs plain, 1 B200"
 
 WORKLOADS = {
     "scale": dict(name="scale_2M_tris_1920x1080_256spp_depth12_envcdf_per_frame", width=1920, height=1080,
                   spp=256, depth=12),
     "cornell": dict(name="cornell_box_256x256_64spp_depth8", width=256, height=256, spp=64, depth=8),
+    # throughput of the radiance-cached form (queries, training paths and optimiser steps inside the
+    # timed frames; the cache keeps training from frame to frame)
+    "cached": dict(name="cornell_box_1920x1080_64spp_depth12_radiance_cache", width=1920, height=1080, spp=64,
+                   depth=12, cached=True),
 }
 
 # Algorithmic HBM bytes per work unit of each wavefront kernel: the path
@@ -140,7 +153,7 @@ def make_scene(wl: dict):
     cie = assets.cie_xyz()
     basis = assets.basis_rgb()
     luts = assets.luts()
-    if wl["width"] == 256:
+    if wl["name"].startswith("cornell"):
         scene = scenes.cornell_box(seed=1, cie_xyz=cie, width=wl["width"], height=wl["height"], spp=wl["spp"],
                                    max_depth=wl["depth"])
     else:
@@ -238,6 +251,11 @@ def run_ours(args, rank: int, world: int, wl: dict):
     lt = lighttree.build_for_scene(scene)
     ri = RenderingInterface(device=local, max_paths_in_flight=args.max_paths)
     ri.load_scene(scene, luts, cie, basis, light_tree=lt)
+    cache = None
+    if wl.get("cached"):
+        from ratbite_b200.nrc import RadianceCache
+        cache = RadianceCache(device=local, seed=2)
+        ri.attach_radiance_cache(cache)
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t_setup
     has_env = getattr(scene, "envmap", None) is not None
@@ -267,6 +285,8 @@ def run_ours(args, rank: int, world: int, wl: dict):
     # ---- device-timed region (per-stage CUDA events on the render stream)
     ri.set_stats(abi.RB_STATS_TIME)
     ri.get_stats()
+    if cache:
+        ri.cache_stats()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if dist:
         dist.barrier()
@@ -279,6 +299,7 @@ def run_ours(args, rank: int, world: int, wl: dict):
         torch.cuda.synchronize()
     ms = start.elapsed_time(end)
     stages = ri.get_stats()
+    cst = ri.cache_stats() if cache else None
     ri.set_stats(0)
     if dist:
         t = torch.tensor([ms], device="cuda")
@@ -313,6 +334,8 @@ def run_ours(args, rank: int, world: int, wl: dict):
         shares = {"extend": stages.ms_extend, "surface": stages.ms_surface, "nee": stages.ms_nee,
                   "bsdf": stages.ms_bsdf, "shadow": stages.ms_shadow,
                   "generate": stages.ms_generate, "resolve": stages.ms_resolve}
+        if cst:
+            shares.update({"cache_infer": cst.ms_infer, "cache_train": cst.ms_train})
         total_ms = sum(shares.values())
         dom = max(("extend", "surface", "nee", "bsdf", "shadow"), key=lambda k: shares[k])
         # counts were gathered over one step
@@ -338,7 +361,8 @@ def run_ours(args, rank: int, world: int, wl: dict):
         # one env-map CDF build per step
         launches_total = (stages.launches_generate + stages.launches_extend + stages.launches_shade
                           + stages.launches_nee + stages.launches_bsdf + stages.launches_shadow
-                          + stages.launches_resolve + (args.steps if has_env else 0))
+                          + stages.launches_resolve + (args.steps if has_env else 0)
+                          + (cst.launches if cst else 0))
         # DRAM traffic of the dominant kernel per launch: ncu's dram bytes per
         # work unit (measured on a reduced case of this workload, see
         # profiles/traffic.json) times the units one launch processes here
@@ -353,6 +377,10 @@ def run_ours(args, rank: int, world: int, wl: dict):
             cpu_v, cores, sample = cpu_baseline(scene, cie, basis, luts, wl, args.cpu_seconds)
         else:
             cpu_v, cores, sample = None, 0, "skipped"
+        ttr = None
+        if args.ttr and world == 1 and args.workload == "scale":
+            ri.cleanup()                     # free this workload's wave before the second one
+            ttr = time_to_rmse(device=local)
         line = {
             "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -380,12 +408,18 @@ def run_ours(args, rank: int, world: int, wl: dict):
                               "nodes_per_shadow_ray": counts.shadow_nodes / max(1, sh_rays),
                               "tris_per_shadow_ray": counts.shadow_tris / max(1, sh_rays)},
             "device_status_flags": st.flags,
+            "radiance_cache": ({"queries_per_step": cst.queries / args.steps, "records_per_step": cst.records / args.steps,
+                                "train_steps_per_step": cst.steps / args.steps, "last_loss": cst.last_loss}
+                               if cst else None),
             "clocks": clocks.summary(),
             "cpu_baseline": {"value": cpu_v, "unit": "paths/s", "cores": cores, "kind": "reference",
                              "sample": sample},
+            "time_to_rmse": ttr,
         }
         print(json.dumps(line), flush=True)
     ri.cleanup()
+    if cache:
+        cache.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -493,6 +527,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample length (0 = skip)")
     ap.add_argument("--ref-step-s", type=float, default=4.0, help="reference arm: seconds per step")
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0 = the workload's)")
+    ap.add_argument("--no-ttr", dest="ttr", action="store_false",
+                    help="skip the time-to-RMSE measurement of the cached form (1920x1080 Cornell box, ~30 s)")
     ap.add_argument("--max-paths", type=int, default=0,
                     help="paths in flight per wave (0 = the library default, 16M); small values make profiling "
                          "captures small")

@@ -49,7 +49,7 @@ int rb_nrc_get_parameters(rb_nrc* nrc, float* grid_host, float* weights_host);
 /* outputs[n][4] = network(inputs[n][kNrcInputs]), stream-ordered; outputs
  * 16-byte aligned. */
 int rb_nrc_infer(rb_nrc* nrc, uint32_t n, const float* inputs, float* outputs, void* stream);
-/* One optimisation step on n (input, target[4]) pairs; loss_out (host or
+/* One optimisation step on n (input, target[4]) pairs, n <= 2^24; loss_out (host or
  * device, may be NULL) receives the batch's mean relative L2 loss before the
  * step, stream-ordered. */
 int rb_nrc_train(rb_nrc* nrc, uint32_t n, const float* inputs, const float* targets, float* loss_out,
@@ -84,7 +84,7 @@ typedef struct rb_cache_params {
     float spread_threshold;        /* c above; 0: 0.01 */
     uint32_t train_one_in;         /* 0: 16; 1: every path trains (none terminates) */
     uint32_t targets_per_sample;   /* 0: 65536 */
-    uint32_t batch;                /* rows per optimisation step; 0: 65536 */
+    uint32_t batch;                /* rows per optimisation step; 0: 131072 */
     uint32_t frozen;               /* 1: query only (no training paths, no optimisation steps) */
     uint32_t samples_per_wave;     /* sample planes per wave (the cache trains after each wave),
                                       bounded by the wavefront capacity; 0: 8 */

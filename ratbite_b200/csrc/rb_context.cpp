@@ -359,7 +359,7 @@ int rb_attach_radiance_cache(rb_ctx* ctx, rb_nrc* cache, const rb_cache_params* 
 	if (P.spread_threshold == 0.0f) P.spread_threshold = 0.01f;
 	if (P.train_one_in == 0) P.train_one_in = 16;
 	if (P.targets_per_sample == 0) P.targets_per_sample = 65536;
-	if (P.batch == 0) P.batch = 65536;
+	if (P.batch == 0) P.batch = 131072;
 	if (P.samples_per_wave == 0) P.samples_per_wave = 8;
 	if (P.min_roughness == 0.0f) P.min_roughness = 0.25f;
 	if (P.batch > (1u << 22)) return fail(ctx, RB_ERR_INVALID, "rb_attach_radiance_cache: batch above 2^22 rows");

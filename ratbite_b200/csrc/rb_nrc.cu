@@ -44,6 +44,7 @@ __host__ __device__ constexpr int wOffset(int l) { return l < 5 ? l * kH * kH : 
 constexpr int kWTotal = wOffset(5);                     // 17408 weights
 constexpr int kWStride = 72;                            // smem row stride (bf16), conflict-free fragment loads
 constexpr int kTile = 16;                               // rows per warp tile
+constexpr uint32_t kMaxTrainRows = 1u << 24;          // rows per training batch (encode kernels index rows x levels)
 constexpr int kOutStride = 8;                           // forward outputs per row in the training scratch
 constexpr int kDropOutput = 4;                          // output trained by the renderer: drop probability
 
@@ -85,50 +86,49 @@ RB_D float restColumn(const float* v, int k)
 	return k == 7 ? 1.0f : 0.0f;
 }
 
+// One thread per (row, level): the level's two features, and for levels
+// 0..7 four of the 32 remaining columns of the row.
 __global__ void kEncode(uint32_t n, const float* __restrict__ in, const __half2* __restrict__ grid, Resolutions R,
 	__nv_bfloat16* __restrict__ X)
 {
-	for (uint32_t i = gtid(); i < n; i += gstride())
+	for (uint32_t i = gtid(); i < n * kLevels; i += gstride())
 	{
-		const float* v = in + static_cast<size_t>(kNrcInputs) * i;
-		__nv_bfloat16* row = X + static_cast<size_t>(kIn) * i;
-		const float px = clamp01(v[0]), py = clamp01(v[1]), pz = clamp01(v[2]);
-		for (int l = 0; l < kLevels; ++l)
-		{
-			float f0, f1;
-			levelFeatures(R, grid, l, px, py, pz, f0, f1);
-			row[2 * l] = __float2bfloat16_rn(f0);
-			row[2 * l + 1] = __float2bfloat16_rn(f1);
-		}
-		for (int k = 0; k < 32; ++k) row[32 + k] = __float2bfloat16_rn(restColumn(v, k));
+		const uint32_t r = i / kLevels, l = i % kLevels;
+		const float* v = in + static_cast<size_t>(kNrcInputs) * r;
+		__nv_bfloat16* row = X + static_cast<size_t>(kIn) * r;
+		float f0, f1;
+		levelFeatures(R, grid, static_cast<int>(l), clamp01(v[0]), clamp01(v[1]), clamp01(v[2]), f0, f1);
+		row[2 * l] = __float2bfloat16_rn(f0);
+		row[2 * l + 1] = __float2bfloat16_rn(f1);
+		if (l < 8)
+			for (int k = 4 * static_cast<int>(l); k < 4 * static_cast<int>(l) + 4; ++k)
+				row[32 + k] = __float2bfloat16_rn(restColumn(v, k));
 	}
 }
 
-// Scatters the gradient of the 32 grid features into the FP32 gradient table.
+// Scatters the gradient of the 32 grid features into the FP32 gradient
+// table, one thread per (row, level).
 __global__ void kEncodeBackward(uint32_t n, const float* __restrict__ in, const float* __restrict__ dX0, Resolutions R,
 	float* __restrict__ gridGrad)
 {
-	for (uint32_t i = gtid(); i < n; i += gstride())
+	for (uint32_t i = gtid(); i < n * kLevels; i += gstride())
 	{
-		const float* v = in + static_cast<size_t>(kNrcInputs) * i;
-		const float* g = dX0 + static_cast<size_t>(kGridFeatures) * i;
-		const float px = clamp01(v[0]), py = clamp01(v[1]), pz = clamp01(v[2]);
-		for (int l = 0; l < kLevels; ++l)
+		const uint32_t r = i / kLevels, l = i % kLevels;
+		const float g0 = dX0[static_cast<size_t>(kGridFeatures) * r + 2 * l];
+		const float g1 = dX0[static_cast<size_t>(kGridFeatures) * r + 2 * l + 1];
+		if (g0 == 0.0f && g1 == 0.0f) continue;
+		const float* v = in + static_cast<size_t>(kNrcInputs) * r;
+		const float sx = clamp01(v[0]) * R.s[l], sy = clamp01(v[1]) * R.s[l], sz = clamp01(v[2]) * R.s[l];
+		const float fx = floorf(sx), fy = floorf(sy), fz = floorf(sz);
+		const float wx = sx - fx, wy = sy - fy, wz = sz - fz;
+		const uint32_t cx = static_cast<uint32_t>(fx), cy = static_cast<uint32_t>(fy), cz = static_cast<uint32_t>(fz);
+		for (int c = 0; c < 8; ++c)
 		{
-			const float g0 = g[2 * l], g1 = g[2 * l + 1];
-			if (g0 == 0.0f && g1 == 0.0f) continue;
-			const float sx = px * R.s[l], sy = py * R.s[l], sz = pz * R.s[l];
-			const float fx = floorf(sx), fy = floorf(sy), fz = floorf(sz);
-			const float wx = sx - fx, wy = sy - fy, wz = sz - fz;
-			const uint32_t cx = static_cast<uint32_t>(fx), cy = static_cast<uint32_t>(fy), cz = static_cast<uint32_t>(fz);
-			for (int c = 0; c < 8; ++c)
-			{
-				const uint32_t dx = c & 1u, dy = (c >> 1) & 1u, dz = (c >> 2) & 1u;
-				const float w = (dx ? wx : 1.0f - wx) * (dy ? wy : 1.0f - wy) * (dz ? wz : 1.0f - wz);
-				float2* e = reinterpret_cast<float2*>(gridGrad) + static_cast<size_t>(l) * kTable
-					+ cellIndex(R, l, cx + dx, cy + dy, cz + dz);
-				atomicAdd(e, make_float2(w * g0, w * g1));
-			}
+			const uint32_t dx = c & 1u, dy = (c >> 1) & 1u, dz = (c >> 2) & 1u;
+			const float w = (dx ? wx : 1.0f - wx) * (dy ? wy : 1.0f - wy) * (dz ? wz : 1.0f - wz);
+			float2* e = reinterpret_cast<float2*>(gridGrad) + static_cast<size_t>(l) * kTable
+				+ cellIndex(R, static_cast<int>(l), cx + dx, cy + dy, cz + dz);
+			atomicAdd(e, make_float2(w * g0, w * g1));
 		}
 	}
 }
@@ -278,8 +278,11 @@ __global__ void __launch_bounds__(128) kMlpForward(uint32_t n, const __nv_bfloat
 // else cap. Outputs 0..3 go to out[rows][4] and/or, with path, are applied
 // as L[p] = L[p] (1 - q) + T[p] max(y, 0), p = path[r], q = output 4
 // clamped to [0, 1] (radiance-cache queries).
-constexpr size_t kSmemInfer = kSmemWeights + sizeof(__nv_bfloat16) * 4 * kTile * kWStride;
-__global__ void __launch_bounds__(128) kMlpInfer(uint32_t cap, const uint32_t* __restrict__ count,
+// 512 threads (16 warps) share one copy of the weights: 2 blocks, 32 warps
+// per SM hide the grid gathers' latency.
+constexpr int kInferThreads = 512;
+constexpr size_t kSmemInfer = kSmemWeights + sizeof(__nv_bfloat16) * (kInferThreads / 32) * kTile * kWStride;
+__global__ void __launch_bounds__(kInferThreads, 2) kMlpInfer(uint32_t cap, const uint32_t* __restrict__ count,
 	const float* __restrict__ in, const __half2* __restrict__ grid, Resolutions R, const __nv_bfloat16* __restrict__ w,
 	float* __restrict__ out, const uint32_t* __restrict__ path, float4* __restrict__ L, const float4* __restrict__ T)
 {
@@ -614,6 +617,19 @@ int blocksFor(const rb_nrc* h, uint32_t rows)
 	const uint32_t cap = static_cast<uint32_t>(h->smCount) * 4;
 	return static_cast<int>(need < 1 ? 1 : (need < cap ? need : cap));
 }
+
+int inferBlocks(const rb_nrc* h, uint32_t rows)
+{
+	const uint32_t tiles = (rows + kTile - 1) / kTile, perBlock = kInferThreads / 32;
+	const uint32_t need = (tiles + perBlock - 1) / perBlock;
+	const uint32_t cap = static_cast<uint32_t>(h->smCount) * 2;
+	return static_cast<int>(need < 1 ? 1 : (need < cap ? need : cap));
+}
+
+int encodeBlocks(uint32_t rows)
+{
+	return gridFor(rows * static_cast<uint32_t>(kLevels));
+}
 } // namespace
 
 extern "C" {
@@ -738,7 +754,7 @@ int rb_nrc_infer(rb_nrc* h, uint32_t n, const float* inputs, float* outputs, voi
 	if (n == 0) return RB_OK;
 	cudaSetDevice(h->device);
 	const cudaStream_t st = static_cast<cudaStream_t>(stream);
-	kMlpInfer<<<blocksFor(h, n), 128, kSmemInfer, st>>>(n, nullptr, inputs, reinterpret_cast<const __half2*>(h->grid),
+	kMlpInfer<<<inferBlocks(h, n), kInferThreads, kSmemInfer, st>>>(n, nullptr, inputs, reinterpret_cast<const __half2*>(h->grid),
 		h->R, h->w, outputs, nullptr, nullptr, nullptr);
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
@@ -753,7 +769,7 @@ int computeGradients(rb_nrc* h, uint32_t n, const float* inputs, const float* ta
 	int rc = growScratch(h, n);
 	if (rc != RB_OK) return rc;
 	cudaMemsetAsync(h->loss, 0, sizeof(float), st);
-	kEncode<<<gridFor(n), kThreads, 0, st>>>(n, inputs, reinterpret_cast<const __half2*>(h->grid), h->R, h->X);
+	kEncode<<<encodeBlocks(n), kThreads, 0, st>>>(n, inputs, reinterpret_cast<const __half2*>(h->grid), h->R, h->X);
 	kMlpForward<<<blocksFor(h, n), 128, kSmemWeights, st>>>(n, h->X, h->w, h->out, h->acts);
 	kLoss<<<gridFor(n), kThreads, 0, st>>>(n, h->out, targets, h->dY, h->loss, valid, outs, tStride);
 	kMlpBackward<<<blocksFor(h, n), 128, kSmemBackward, st>>>(n, h->dY, h->wt, h->acts, h->dH, h->dX0);
@@ -775,7 +791,7 @@ int computeGradients(rb_nrc* h, uint32_t n, const float* inputs, const float* ta
 				CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT) != CUBLAS_STATUS_SUCCESS)
 			return RB_ERR_CUDA;
 	}
-	kEncodeBackward<<<gridFor(n), kThreads, 0, st>>>(n, inputs, h->dX0, h->R, h->gridGrad);
+	kEncodeBackward<<<encodeBlocks(n), kThreads, 0, st>>>(n, inputs, h->dX0, h->R, h->gridGrad);
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
 } // namespace
@@ -783,7 +799,7 @@ int computeGradients(rb_nrc* h, uint32_t n, const float* inputs, const float* ta
 int rb_nrc_gradients(rb_nrc* h, uint32_t n, const float* inputs, const float* targets, float* grid_grad,
 	float* weight_grad)
 {
-	if (!h || n == 0 || !inputs || !targets || !grid_grad || !weight_grad) return RB_ERR_INVALID;
+	if (!h || n == 0 || n > kMaxTrainRows || !inputs || !targets || !grid_grad || !weight_grad) return RB_ERR_INVALID;
 	cudaSetDevice(h->device);
 	int rc = computeGradients(h, n, inputs, targets, nullptr);
 	if (rc != RB_OK) return rc;
@@ -798,7 +814,7 @@ int rb_nrc_gradients(rb_nrc* h, uint32_t n, const float* inputs, const float* ta
 
 int rb_nrc_train(rb_nrc* h, uint32_t n, const float* inputs, const float* targets, float* loss_out, void* stream)
 {
-	if (!h || n == 0 || !inputs || !targets) return RB_ERR_INVALID;
+	if (!h || n == 0 || n > kMaxTrainRows || !inputs || !targets) return RB_ERR_INVALID;
 	cudaSetDevice(h->device);
 	const cudaStream_t st = static_cast<cudaStream_t>(stream);
 	const int rc = rb::nrc::trainRows(h, n, nullptr, inputs, targets, st, false);
@@ -818,7 +834,7 @@ int applyQueries(rb_nrc* h, uint32_t cap, const uint32_t* count, const float* in
 	const float4* T, cudaStream_t st)
 {
 	if (cap == 0) return RB_OK;
-	kMlpInfer<<<blocksFor(h, cap), 128, kSmemInfer, st>>>(cap, count, inputs, reinterpret_cast<const __half2*>(h->grid),
+	kMlpInfer<<<inferBlocks(h, cap), kInferThreads, kSmemInfer, st>>>(cap, count, inputs, reinterpret_cast<const __half2*>(h->grid),
 		h->R, h->w, nullptr, path, L, T);
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
