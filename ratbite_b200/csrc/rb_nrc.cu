@@ -152,24 +152,36 @@ RB_D void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t 
 		: "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// Four 8x8 b16 matrices from shared memory (ldmatrix.x4): lanes 8m..8m+7
+// give the row addresses of matrix m; register m receives matrix m's
+// fragment (row lane / 4, columns 2 (lane % 4), +1).
+RB_D void ldsm4(uint32_t (&r)[4], const __nv_bfloat16* p)
+{
+	const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
+	asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+		: "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
+}
+
 // One layer on a 16-row tile: C[16 x 8*NT] = A[16 x 64] x W^T, W in smem as
-// [out][in] rows of kWStride bf16. A: 4 k-tiles of fragments.
+// [out][in] rows of kWStride bf16. A: 4 k-tiles of fragments. The B
+// fragments of two k-tiles come from one ldmatrix.x4 (matrices at k offsets
+// 0, 8, 16, 24 of the lane's weight row).
 template<int NT>
 RB_D void layer(const uint32_t (&A)[4][4], const __nv_bfloat16* W, float (&C)[NT][4])
 {
-	const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, c = lane & 3u;
+	const uint32_t lane = threadIdx.x & 31u, r = lane & 7u, m = lane >> 3;
 #pragma unroll
 	for (int j = 0; j < NT; ++j)
 	{
 		C[j][0] = C[j][1] = C[j][2] = C[j][3] = 0.0f;
-		const __nv_bfloat16* wr = W + (8 * j + g) * kWStride;
-#pragma unroll
-		for (int t = 0; t < 4; ++t)
-		{
-			const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wr + 16 * t + 2 * c);
-			const uint32_t b1 = *reinterpret_cast<const uint32_t*>(wr + 16 * t + 8 + 2 * c);
-			mma16816(C[j], A[t], b0, b1);
-		}
+		const __nv_bfloat16* wr = W + (8 * j + r) * kWStride + 8 * m;
+		uint32_t b[4];
+		ldsm4(b, wr);
+		mma16816(C[j], A[0], b[0], b[1]);
+		mma16816(C[j], A[1], b[2], b[3]);
+		ldsm4(b, wr + 32);
+		mma16816(C[j], A[2], b[0], b[1]);
+		mma16816(C[j], A[3], b[2], b[3]);
 	}
 }
 // Accumulator fragments of 8 n-tiles -> A fragments of the next layer, with ReLU.
@@ -278,11 +290,25 @@ __global__ void __launch_bounds__(128) kMlpForward(uint32_t n, const __nv_bfloat
 // else cap. Outputs 0..3 go to out[rows][4] and/or, with path, are applied
 // as L[p] = L[p] (1 - q) + T[p] max(y, 0), p = path[r], q = output 4
 // clamped to [0, 1] (radiance-cache queries).
-// 512 threads (16 warps) share one copy of the weights: 2 blocks, 32 warps
-// per SM hide the grid gathers' latency.
-constexpr int kInferThreads = 512;
+// RB_INFER_THREADS threads share one copy of the weights; as many blocks per
+// SM as fit (3 at 256 threads: 56 KB of shared memory each, registers capped
+// for 3). Measured on the cached Cornell frame (1920x1080, 64 spp): 256
+// threads 8.06 ms of inference, 384: 8.14, 512: 8.71 (spills at the
+// 64-register cap).
+#ifndef RB_INFER_THREADS
+#define RB_INFER_THREADS 256
+#endif
+#ifndef RB_INFER_GATHER_UNROLL
+#define RB_INFER_GATHER_UNROLL 2
+#endif
+constexpr int kInferThreads = RB_INFER_THREADS;
+constexpr int kGatherUnroll = RB_INFER_GATHER_UNROLL;
+#ifndef RB_INFER_MIN_BLOCKS
+#define RB_INFER_MIN_BLOCKS 3
+#endif
+constexpr int kInferMinBlocks = RB_INFER_MIN_BLOCKS;
 constexpr size_t kSmemInfer = kSmemWeights + sizeof(__nv_bfloat16) * (kInferThreads / 32) * kTile * kWStride;
-__global__ void __launch_bounds__(kInferThreads, 2) kMlpInfer(uint32_t cap, const uint32_t* __restrict__ count,
+__global__ void __launch_bounds__(kInferThreads, kInferMinBlocks) kMlpInfer(uint32_t cap, const uint32_t* __restrict__ count,
 	const float* __restrict__ in, const __half2* __restrict__ grid, Resolutions R, const __nv_bfloat16* __restrict__ w,
 	float* __restrict__ out, const uint32_t* __restrict__ path, float4* __restrict__ L, const float4* __restrict__ T)
 {
@@ -295,7 +321,7 @@ __global__ void __launch_bounds__(kInferThreads, 2) kMlpInfer(uint32_t cap, cons
 	for (uint32_t r0 = warp * kTile; r0 < n; r0 += warps * kTile)
 	{
 		// grid features: lane handles (row k / 16, level k % 16) for k = lane + 32 i
-#pragma unroll 2
+#pragma unroll kGatherUnroll
 		for (uint32_t k = lane; k < kTile * kLevels; k += 32)
 		{
 			const uint32_t row = k >> 4, l = k & 15u, r = r0 + row;
@@ -320,15 +346,12 @@ __global__ void __launch_bounds__(kInferThreads, 2) kMlpInfer(uint32_t cap, cons
 			}
 		}
 		__syncwarp();
+		// A fragments (ldmatrix.x4 per k-tile: rows 0-7 / 8-15 x columns 0-7 / 8-15 of the tile)
 		uint32_t A[4][4];
-#pragma unroll
-		for (int t = 0; t < 4; ++t)
 		{
-			const uint32_t k0 = 16 * t + 2 * c;
-			A[t][0] = *reinterpret_cast<const uint32_t*>(tile + g * kWStride + k0);
-			A[t][1] = *reinterpret_cast<const uint32_t*>(tile + (g + 8) * kWStride + k0);
-			A[t][2] = *reinterpret_cast<const uint32_t*>(tile + g * kWStride + k0 + 8);
-			A[t][3] = *reinterpret_cast<const uint32_t*>(tile + (g + 8) * kWStride + k0 + 8);
+			const uint32_t m = lane >> 3, rr = (lane & 7u) + 8u * (m & 1u);
+#pragma unroll
+			for (int t = 0; t < 4; ++t) ldsm4(A[t], tile + rr * kWStride + 16 * t + 8 * (m >> 1));
 		}
 		__syncwarp();
 		float C[8][4];
@@ -571,6 +594,7 @@ struct rb_nrc
 	cublasHandle_t blas = nullptr;
 	uint32_t step = 0;
 	int smCount = 148;
+	uint32_t inferBlocksPerSm = 2;
 };
 
 namespace
@@ -622,7 +646,7 @@ int inferBlocks(const rb_nrc* h, uint32_t rows)
 {
 	const uint32_t tiles = (rows + kTile - 1) / kTile, perBlock = kInferThreads / 32;
 	const uint32_t need = (tiles + perBlock - 1) / perBlock;
-	const uint32_t cap = static_cast<uint32_t>(h->smCount) * 2;
+	const uint32_t cap = static_cast<uint32_t>(h->smCount) * h->inferBlocksPerSm;
 	return static_cast<int>(need < 1 ? 1 : (need < cap ? need : cap));
 }
 
@@ -699,6 +723,9 @@ int rb_nrc_create(const rb_nrc_config* config, rb_nrc** out)
 		static_cast<int>(kSmemBackward));
 	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpInfer), cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(kSmemInfer));
+	int perSm = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMlpInfer, kInferThreads, kSmemInfer) == cudaSuccess && perSm > 0)
+		h->inferBlocksPerSm = static_cast<uint32_t>(perSm);
 	*out = h;
 	return RB_OK;
 }

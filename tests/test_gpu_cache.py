@@ -10,10 +10,11 @@ their vertices, and the optimiser steps the wave feeds.
    pixel is closer to a 2048-spp plain reference than the plain tracer's at
    16 spp, and an untrained cache (same termination, no training) is worse
    than the trained one: the gain comes from what the network learned.
-3. The cached form is unbiased against the plain estimator where the cache
-   is accurate: after training, the mean of the image matches the
-   reference's within 3 % (an untrained cache, or one that ignored the
-   reference's dropped samples, is several percent off).
+3. The cached form is close to unbiased against the plain estimator: after
+   training, the mean of the image matches the reference's within 5 %
+   (measured -0.2 % to -2.8 % over runs: the training's float atomics make
+   each run's trajectory differ). An untrained cache is +43 % off, and a
+   cache that ignored the reference's dropped samples was +7 % off.
 """
 from __future__ import annotations
 
@@ -109,7 +110,7 @@ def test_trained_cache_reduces_error_at_equal_samples(setup):
     assert warm.steps == 256 and st.steps == spp and st.queries > W * H
     assert cached < 0.9 * plain
     assert cached < cold
-    assert abs(bias) < 0.03
+    assert abs(bias) < 0.05
     ri.cleanup()
     cache.close()
     untrained.close()
