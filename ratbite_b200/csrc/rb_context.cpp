@@ -917,7 +917,6 @@ int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 	const int bounces = static_cast<int>(std::min<uint32_t>(rb::kMaxBounces,
 		std::max({ sc.launch.maxDepth, sc.launch.maxReflected, sc.launch.maxTransmitted })));
 	rb::PathSoA soa = ctx->soa;
-	float posMin[3] = {}, posScale[3] = {};
 	if (cached)
 	{
 		rc = ensureCache(ctx, wavePaths, static_cast<uint32_t>(bounces));
@@ -925,21 +924,23 @@ int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 		const rb::PathSoA& c = ctx->cacheArrays;
 		soa.spread = c.spread; soa.trainRec = c.trainRec; soa.cPath = c.cPath; soa.cIn = c.cIn;
 		soa.tPath = c.tPath; soa.tIn = c.tIn; soa.tL = c.tL; soa.tT = c.tT; soa.trainCapacity = c.trainCapacity;
-		// the given box, or the geometry's bounds grown by 1 %
-		const bool given = CP.scene_min[0] < CP.scene_max[0] && CP.scene_min[1] < CP.scene_max[1] &&
-			CP.scene_min[2] < CP.scene_max[2];
-		for (int k = 0; k < 3; ++k)
+	}
+	// scene box -> [0,1]^3 (cache inputs): the cache's
+	// given box, or the geometry's bounds grown by 1 %
+	float posMin[3] = {}, posScale[3] = {};
+	const bool given = cached && CP.scene_min[0] < CP.scene_max[0] && CP.scene_min[1] < CP.scene_max[1] &&
+		CP.scene_min[2] < CP.scene_max[2];
+	for (int k = 0; k < 3; ++k)
+	{
+		float lo = given ? CP.scene_min[k] : ctx->geoMin[k], hi = given ? CP.scene_max[k] : ctx->geoMax[k];
+		if (!given)
 		{
-			float lo = given ? CP.scene_min[k] : ctx->geoMin[k], hi = given ? CP.scene_max[k] : ctx->geoMax[k];
-			if (!given)
-			{
-				const float pad = 0.005f * std::max(hi - lo, 1e-6f);
-				lo -= pad;
-				hi += pad;
-			}
-			posMin[k] = lo;
-			posScale[k] = hi > lo ? 1.0f / (hi - lo) : 1.0f;
+			const float pad = 0.005f * std::max(hi - lo, 1e-6f);
+			lo -= pad;
+			hi += pad;
 		}
+		posMin[k] = lo;
+		posScale[k] = hi > lo ? 1.0f / (hi - lo) : 1.0f;
 	}
 	for (uint32_t done = 0; done < count;)
 	{
@@ -957,8 +958,8 @@ int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 			w.trainSeed = rb::mix32(static_cast<uint32_t>(ctx->cacheWaves++) * 0x9E3779B9u + 1u);
 			w.spreadC = CP.spread_threshold;
 			w.minRoughness = CP.min_roughness;
-			for (int k = 0; k < 3; ++k) { w.posMin[k] = posMin[k]; w.posScale[k] = posScale[k]; }
 		}
+		for (int k = 0; k < 3; ++k) { w.posMin[k] = posMin[k]; w.posScale[k] = posScale[k]; }
 		unsigned long long* cnt = (ctx->statsMode & RB_STATS_COUNT) ? ctx->counters : nullptr;
 		cudaMemsetAsync(soa.counts, 0, sizeof(uint32_t) * rb::kCountSlots, st);
 		timedStage(ctx, 0, st, [&] { rb::launchGenerate(sc, soa, w, ctx->shape, st); });
