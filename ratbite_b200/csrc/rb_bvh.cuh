@@ -153,19 +153,24 @@ RB_D uint32_t childBoxes(const TraceRay& r, const NodeView& v, float tmin, float
 	const uint32_t nx0 = nx ? hi0 : lo0, nx1 = nx ? hi1 : lo1, fx0 = nx ? lo0 : hi0, fx1 = nx ? lo1 : hi1;
 	const uint32_t ny0 = ny ? hi2 : lo2, ny1 = ny ? hi3 : lo3, fy0 = ny ? lo2 : hi2, fy1 = ny ? lo3 : hi3;
 	const uint32_t nz0 = nz ? hi4 : lo4, nz1 = nz ? hi5 : lo5, fz0 = nz ? lo4 : hi4, fz1 = nz ? lo5 : hi5;
-	// Planes are rebuilt exactly (q * 2^e is exact, one rounding for the add)
-	// and intersected as (plane - o) / d, which keeps the error relative to
-	// the distance; the quantizer also pads every box by one step.
+	// Plane distance t = (q 2^e + origin - o) / d as one FMA per plane,
+	// fma(q, 2^e / d, (origin - o) / d): 2^e / d is exact (power of two), so
+	// the error is the rounding of (origin - o) / d, a world-space error of
+	// about |origin - o| 2^-24; the quantizer pads every box by one step
+	// (at least 1/256 of the node's extent), far more than that for rays
+	// inside the scene, so the test stays conservative.
+	const float ax = scx * r.ix, ay = scy * r.iy, az = scz * r.iz;
+	const float bx = (ox - r.o.x) * r.ix, by = (oy - r.o.y) * r.iy, bz = (oz - r.o.z) * r.iz;
 	uint32_t mask = 0;
 #pragma unroll
 	for (int c = 0; c < 8; ++c)
 	{
-		const float tnx = (__fmaf_rn(planeQ(nx0, nx1, c), scx, ox) - r.o.x) * r.ix;
-		const float tfx = (__fmaf_rn(planeQ(fx0, fx1, c), scx, ox) - r.o.x) * r.ix;
-		const float tny = (__fmaf_rn(planeQ(ny0, ny1, c), scy, oy) - r.o.y) * r.iy;
-		const float tfy = (__fmaf_rn(planeQ(fy0, fy1, c), scy, oy) - r.o.y) * r.iy;
-		const float tnz = (__fmaf_rn(planeQ(nz0, nz1, c), scz, oz) - r.o.z) * r.iz;
-		const float tfz = (__fmaf_rn(planeQ(fz0, fz1, c), scz, oz) - r.o.z) * r.iz;
+		const float tnx = __fmaf_rn(planeQ(nx0, nx1, c), ax, bx);
+		const float tfx = __fmaf_rn(planeQ(fx0, fx1, c), ax, bx);
+		const float tny = __fmaf_rn(planeQ(ny0, ny1, c), ay, by);
+		const float tfy = __fmaf_rn(planeQ(fy0, fy1, c), ay, by);
+		const float tnz = __fmaf_rn(planeQ(nz0, nz1, c), az, bz);
+		const float tfz = __fmaf_rn(planeQ(fz0, fz1, c), az, bz);
 		const float n = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
 		const float f = fminf(fminf(tfx, tfy), fminf(tfz, tmax)) * 1.0000004f;
 		tnear[c] = n;
