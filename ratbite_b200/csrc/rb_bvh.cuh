@@ -179,23 +179,31 @@ RB_D uint32_t childBoxes(const TraceRay& r, const NodeView& v, float tmin, float
 	return mask;
 }
 
-RB_D void cswap(float& ka, uint32_t& va, float& kb, uint32_t& vb)
+// Integer-key form for the near-to-far order: key = entry distance bits
+// with the low 3 mantissa bits replaced by the child slot (entry distances
+// are >= 0, so their bit patterns order like the values), 0xFFFFFFF8 | slot
+// for a child that is not entered. One min and one max per comparator.
+RB_D void cswapU(uint32_t& a, uint32_t& b)
 {
-	if (kb < ka)
-	{
-		const float tk = ka; ka = kb; kb = tk;
-		const uint32_t tv = va; va = vb; vb = tv;
-	}
+	const uint32_t lo = min(a, b), hi = max(a, b);
+	a = lo;
+	b = hi;
 }
-// Optimal 19-comparator sorting network for 8 keys.
-RB_D void sort8(float k[8], uint32_t v[8])
+RB_D void sort8u(uint32_t k[8])
 {
-	cswap(k[0], v[0], k[2], v[2]); cswap(k[1], v[1], k[3], v[3]); cswap(k[4], v[4], k[6], v[6]); cswap(k[5], v[5], k[7], v[7]);
-	cswap(k[0], v[0], k[4], v[4]); cswap(k[1], v[1], k[5], v[5]); cswap(k[2], v[2], k[6], v[6]); cswap(k[3], v[3], k[7], v[7]);
-	cswap(k[0], v[0], k[1], v[1]); cswap(k[2], v[2], k[3], v[3]); cswap(k[4], v[4], k[5], v[5]); cswap(k[6], v[6], k[7], v[7]);
-	cswap(k[2], v[2], k[4], v[4]); cswap(k[3], v[3], k[5], v[5]);
-	cswap(k[1], v[1], k[4], v[4]); cswap(k[3], v[3], k[6], v[6]);
-	cswap(k[1], v[1], k[2], v[2]); cswap(k[3], v[3], k[4], v[4]); cswap(k[5], v[5], k[6], v[6]);
+	cswapU(k[0], k[2]); cswapU(k[1], k[3]); cswapU(k[4], k[6]); cswapU(k[5], k[7]);
+	cswapU(k[0], k[4]); cswapU(k[1], k[5]); cswapU(k[2], k[6]); cswapU(k[3], k[7]);
+	cswapU(k[0], k[1]); cswapU(k[2], k[3]); cswapU(k[4], k[5]); cswapU(k[6], k[7]);
+	cswapU(k[2], k[4]); cswapU(k[3], k[5]);
+	cswapU(k[1], k[4]); cswapU(k[3], k[6]);
+	cswapU(k[1], k[2]); cswapU(k[3], k[4]); cswapU(k[5], k[6]);
+}
+// Child reference of slot s (0..7) chosen at run time.
+RB_D uint32_t nodeChildAt(const NodeView& v, uint32_t s)
+{
+	const float4 a = s < 4u ? v.q[1] : v.q[2];
+	const uint32_t k = s & 3u;
+	return __float_as_uint(k == 0u ? a.x : (k == 1u ? a.y : (k == 2u ? a.z : a.w)));
 }
 
 struct Hit
@@ -259,9 +267,11 @@ struct ClosestTraversal
 	// Tests the children of the interior node `cur`; descends into the
 	// nearest one entered (returns true) after pushing the others, farthest
 	// first. Returns false when no child is entered.
+	// Stack entries: (child reference, entry-distance bits, truncated down:
+	// popping compares a value <= the true distance, so culling stays
+	// conservative).
 	template<bool COUNT>
-	RB_D bool nodeStep(const DevGeometry& g, uint32_t* status, uint32_t& nNodes, uint32_t (&stackRef)[kTraversalStack],
-		float (&stackT)[kTraversalStack])
+	RB_D bool nodeStep(const DevGeometry& g, uint32_t* status, uint32_t& nNodes, uint2 (&stack)[kTraversalStack])
 	{
 		if (COUNT) ++nNodes;
 		const NodeView nv = loadNode(g.nodes, cur);
@@ -269,26 +279,23 @@ struct ClosestTraversal
 		const uint32_t mask = childBoxes(r, nv, tmin, best.t, tn);
 		if (!mask) return false;
 #if RB_TRAV_SORT
-		float key[8];
-		uint32_t ref[8];
+		uint32_t key[8];
 #pragma unroll
 		for (int c = 0; c < 8; ++c)
-		{
-			key[c] = (mask >> c) & 1u ? tn[c] : INFINITY;
-			ref[c] = nodeChild(nv, c);
-		}
-		sort8(key, ref);
+			key[c] = ((mask >> c) & 1u) ? ((__float_as_uint(tn[c]) & 0x7FFFFFF8u) | static_cast<uint32_t>(c))
+				: (0xFFFFFFF8u | static_cast<uint32_t>(c));
+		sort8u(key);
 		const int n = __popc(mask);
 #pragma unroll
 		for (int c = 7; c >= 1; --c)
 		{
 			if (c < n)
 			{
-				if (sp < kTraversalStack) { stackRef[sp] = ref[c]; stackT[sp] = key[c]; ++sp; }
+				if (sp < kTraversalStack) { stack[sp] = make_uint2(nodeChildAt(nv, key[c] & 7u), key[c] & ~7u); ++sp; }
 				else atomicOr(status, RB_DEV_STACK_OVERFLOW);
 			}
 		}
-		cur = ref[0];
+		cur = nodeChildAt(nv, key[0] & 7u);
 #else
 		int nearest = 0;
 		float nk = INFINITY;
@@ -300,7 +307,7 @@ struct ClosestTraversal
 		{
 			if (((mask >> c) & 1u) && c != nearest)
 			{
-				if (sp < kTraversalStack) { stackRef[sp] = nodeChild(nv, c); stackT[sp] = tn[c]; ++sp; }
+				if (sp < kTraversalStack) { stack[sp] = make_uint2(nodeChild(nv, c), __float_as_uint(tn[c])); ++sp; }
 				else atomicOr(status, RB_DEV_STACK_OVERFLOW);
 			}
 		}
@@ -310,12 +317,13 @@ struct ClosestTraversal
 	}
 
 	// Pops the next entry that may still hold a closer hit; false when none is left.
-	RB_D bool pop(const uint32_t (&stackRef)[kTraversalStack], const float (&stackT)[kTraversalStack])
+	RB_D bool pop(const uint2 (&stack)[kTraversalStack])
 	{
 		while (sp > 0)
 		{
 			--sp;
-			if (stackT[sp] <= best.t) { cur = stackRef[sp]; return true; }
+			const uint2 e = stack[sp];
+			if (__uint_as_float(e.y) <= best.t) { cur = e.x; return true; }
 		}
 		return false;
 	}
@@ -324,7 +332,7 @@ struct ClosestTraversal
 	// scalar state can stay in registers.
 	template<bool COUNT>
 	RB_D bool run(const DevGeometry& g, int budget, uint32_t* status, uint32_t& nNodes, uint32_t& nTris,
-		uint32_t (&stackRef)[kTraversalStack], float (&stackT)[kTraversalStack])
+		uint2 (&stack)[kTraversalStack])
 	{
 #if RB_TRAV_WHILE_WHILE
 		// interior nodes until a leaf, then the leaf: lanes of a warp meet at
@@ -335,7 +343,7 @@ struct ClosestTraversal
 			while (!(cur & kLeafBit) && it < budget)
 			{
 				++it;
-				if (!nodeStep<COUNT>(g, status, nNodes, stackRef, stackT) && !pop(stackRef, stackT))
+				if (!nodeStep<COUNT>(g, status, nNodes, stack) && !pop(stack))
 				{
 					done = true;
 					break;
@@ -344,7 +352,7 @@ struct ClosestTraversal
 			if (done || it >= budget) break;
 			++it;
 			leafStep<COUNT>(g, nTris);
-			if (!pop(stackRef, stackT)) done = true;
+			if (!pop(stack)) done = true;
 		}
 #else
 		for (int it = 0; it < budget && !done; ++it)
@@ -352,9 +360,9 @@ struct ClosestTraversal
 			if (cur & kLeafBit)
 			{
 				leafStep<COUNT>(g, nTris);
-				if (!pop(stackRef, stackT)) done = true;
+				if (!pop(stack)) done = true;
 			}
-			else if (!nodeStep<COUNT>(g, status, nNodes, stackRef, stackT) && !pop(stackRef, stackT))
+			else if (!nodeStep<COUNT>(g, status, nNodes, stack) && !pop(stack))
 			{
 				done = true;
 			}
@@ -439,10 +447,9 @@ RB_D Hit traceClosestT(const DevGeometry& g, f3 o, f3 d, float tmin, float tmax,
 	uint32_t& nNodes, uint32_t& nTris)
 {
 	ClosestTraversal tr;
-	uint32_t stackRef[kTraversalStack];
-	float stackT[kTraversalStack];
+	uint2 stack[kTraversalStack];
 	tr.init(g, o, d, tmin, tmax);
-	while (!tr.run<COUNT>(g, 1 << 30, status, nNodes, nTris, stackRef, stackT)) {}
+	while (!tr.run<COUNT>(g, 1 << 30, status, nNodes, nTris, stack)) {}
 	return tr.best;
 }
 

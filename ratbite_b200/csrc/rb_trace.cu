@@ -66,8 +66,7 @@ __global__ void __launch_bounds__(kThreads) kExtend(DevScene sc, PathSoA s, int 
 	uint32_t rays = 0, nodes = 0, tris = 0;
 	uint32_t p = 0;
 	ClosestTraversal tr;
-	uint32_t stackRef[kTraversalStack];
-	float stackT[kTraversalStack];
+	uint2 stack[kTraversalStack];
 	persistentTraversal<ClosestTraversal>(n, s.counts + kExtendFetch + bounce,
 		[&](uint32_t idx) {
 			p = q[idx];
@@ -76,7 +75,7 @@ __global__ void __launch_bounds__(kThreads) kExtend(DevScene sc, PathSoA s, int 
 			++rays;
 		},
 		[&]() {
-			if (!tr.template run<COUNT>(sc.geo, kStepBudget, sc.status, nodes, tris, stackRef, stackT)) return false;
+			if (!tr.template run<COUNT>(sc.geo, kStepBudget, sc.status, nodes, tris, stack)) return false;
 			s.hit[p] = make_float4(__int_as_float(tr.best.tri), tr.best.t, tr.best.b1, tr.best.b2);
 			return true;
 		});
