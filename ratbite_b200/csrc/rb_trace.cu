@@ -15,18 +15,24 @@ namespace rb
 {
 namespace
 {
-// Node / leaf visits a lane makes before its warp hands idle lanes new rays
-// (on B200, at-scale frame: 16 beats 8 and 32).
+// Node / leaf visits per step of the persistent loop, and the number of idle
+// lanes at which the warp fetches new rays (all lanes idle always fetches).
+// On B200, at-scale frame (extension ms): 16 / 1 (the default) 442; 2 / 8
+// 433 (but shadow 75 -> 86); 1 / 8 448; 4 / 8 709; 8 / 8 1185.
 #ifndef RB_STEP_BUDGET
 #define RB_STEP_BUDGET 16
 #endif
+#ifndef RB_REFILL_LANES
+#define RB_REFILL_LANES 1
+#endif
 constexpr int kStepBudget = RB_STEP_BUDGET;
+constexpr int kRefillLanes = RB_REFILL_LANES;
 
-// Persistent traversal warps with dynamic ray fetch: a lane whose ray has
-// ended takes the next one from the stage's work counter (one atomic per warp
-// for all idle lanes) after at most kStepBudget visits of the other lanes, so
-// lanes do not idle until the warp's longest ray ends. The loop exits are
-// warp-uniform, so the full-mask warp votes are safe.
+// Persistent traversal warps with dynamic ray fetch: lanes whose rays have
+// ended take the next ones from the stage's work counter (one atomic per warp
+// for all idle lanes) once kRefillLanes of them are idle, between steps of
+// kStepBudget visits, so lanes do not idle until the warp's longest ray ends.
+// The loop exits are warp-uniform, so the full-mask warp votes are safe.
 template<typename Traversal, typename Begin, typename Step>
 RB_D void persistentTraversal(uint32_t n, uint32_t* workCounter, Begin&& begin, Step&& step)
 {
@@ -35,7 +41,7 @@ RB_D void persistentTraversal(uint32_t n, uint32_t* workCounter, Begin&& begin, 
 	for (;;)
 	{
 		const uint32_t idle = __ballot_sync(0xFFFFFFFFu, !active);
-		if (idle && !exhausted)
+		if (!exhausted && idle && (idle == 0xFFFFFFFFu || __popc(idle) >= kRefillLanes))
 		{
 			const int leader = __ffs(idle) - 1;
 			uint32_t base = 0;
