@@ -275,6 +275,14 @@ int rb_set_launch(rb_ctx* ctx, const rb_launch* launch);
  * NULL for the library stream; the call is asynchronous with respect to the
  * host. */
 int rb_render(rb_ctx* ctx, uint32_t sample_offset, uint32_t sample_count, void* stream);
+/* rb_render with the call's wave sequence captured once as a CUDA graph and
+ * replayed (no reference counterpart: the reference launches one OptiX
+ * pipeline per sub-launch): the same accumulation bit for bit, one kernel
+ * launch plus one graph launch per call instead of ~8 launches per bounce.
+ * A graph is kept per sample_count (up to 8) for the current scene state;
+ * any setter, a new launch size or a new wave capacity captures anew. With a
+ * radiance cache attached or statistics on, it is rb_render. */
+int rb_render_graph(rb_ctx* ctx, uint32_t sample_offset, uint32_t sample_count, void* stream);
 /* Copies the width*height*4 doubles (sum X, sum Y, sum Z, sample count) of
  * the accumulation buffer (renderData) to host memory; synchronizes. */
 int rb_read_accum(rb_ctx* ctx, double* out);

@@ -88,6 +88,24 @@ struct rb_ctx
 	uint32_t* batchValid = nullptr;
 	unsigned long long* cacheTally = nullptr;   // device: queries, records
 	uint64_t cacheWaves = 0, cacheSteps = 0, cacheStepsReported = 0;
+	// replayed wave sequences (rb_render_graph): one per call shape and scene
+	// state; dyn holds the replayed call's offset and fresh flag
+	struct GraphKey
+	{
+		rb::DevScene scene;
+		rb::PathSoA soa;
+		double4* accum;
+		uint32_t count;
+	};
+	struct Graph
+	{
+		GraphKey key;
+		cudaGraphExec_t exec;
+		uint32_t launches[9];
+		uint64_t paths, waves;
+	};
+	std::vector<Graph> graphs;
+	uint32_t* dyn = nullptr;
 };
 
 namespace
@@ -424,10 +442,13 @@ int rb_create(const rb_config* config, rb_ctx** out)
 	if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
 	if (e == cudaSuccess) e = cudaMalloc(&ctx->status, 2 * sizeof(uint32_t));
 	if (e == cudaSuccess) e = cudaMemset(ctx->status, 0, 2 * sizeof(uint32_t));
+	if (e == cudaSuccess) e = cudaMalloc(&ctx->dyn, 2 * sizeof(uint32_t));
 	if (e != cudaSuccess)
 	{
 		const int rc = e == cudaErrorMemoryAllocation ? RB_ERR_OOM : RB_ERR_CUDA;
 		if (ctx->stream) cudaStreamDestroy(ctx->stream);
+		if (ctx->status) cudaFree(ctx->status);
+		if (ctx->dyn) cudaFree(ctx->dyn);
 		delete ctx;
 		return rc;
 	}
@@ -453,6 +474,8 @@ int rb_destroy(rb_ctx* ctx)
 	if (ctx->accum) cudaFree(ctx->accum);
 	if (ctx->image) cudaFree(ctx->image);
 	if (ctx->status) cudaFree(ctx->status);
+	if (ctx->dyn) cudaFree(ctx->dyn);
+	for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.exec);
 	if (ctx->stream) cudaStreamDestroy(ctx->stream);
 	delete ctx;
 	return RB_OK;
@@ -892,25 +915,40 @@ int rb_set_launch(rb_ctx* ctx, const rb_launch* l)
 	return RB_OK;
 }
 
-int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
+} // extern "C"
+
+namespace
 {
-	if (!ctx) return RB_ERR_INVALID;
+// Checks shared by the render entry points.
+int renderReady(rb_ctx* ctx)
+{
 	if (!ctx->haveLaunch || !ctx->haveGeometry || !ctx->scene.materials || !ctx->scene.spectra.sensor || !ctx->scene.luts.conductor)
 		return fail(ctx, RB_ERR_NO_SCENE, "rb_render: launch, geometry, materials, spectra and LUTs must be set first");
-	if (count == 0) return RB_OK;
-	const int rc0 = checkReferences(ctx);
-	if (rc0 != RB_OK) return rc0;
-	cudaSetDevice(ctx->device);
-	const cudaStream_t st = pick(ctx, stream);
+	return RB_OK;
+}
+
+// Sample planes per wave of a call rendering `count` planes.
+uint32_t planesPerWaveFor(const rb_ctx* ctx, uint32_t count)
+{
+	const uint32_t pixels = ctx->scene.launch.width * ctx->scene.launch.height;
+	const uint64_t cap = ctx->requestedCapacity ? ctx->requestedCapacity : (16u << 20);
+	uint32_t planes = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(count, cap / pixels)));
+	if (ctx->cache) planes = std::min(planes, ctx->cacheParams.samples_per_wave);
+	return planes;
+}
+
+// The wave sequence of one render call, launched on st. With dyn (replayed
+// waves), the call's offset and fresh flag are read from dyn at run time and
+// `offset` is ignored.
+int renderWaves(rb_ctx* ctx, uint32_t offset, uint32_t count, cudaStream_t st, const uint32_t* dyn)
+{
 	const rb::DevScene& sc = ctx->scene;
 	const uint32_t pixels = sc.launch.width * sc.launch.height;
 	// Wave size: whole sample planes, up to the capacity (default 16M paths,
-	// about 3.2 GB of path state).
-	const uint64_t cap = ctx->requestedCapacity ? ctx->requestedCapacity : (16u << 20);
+	// about 5.8 GB of path state).
 	const bool cached = ctx->cache != nullptr;
 	const rb_cache_params& CP = ctx->cacheParams;
-	uint32_t planesPerWave = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(count, cap / pixels)));
-	if (cached) planesPerWave = std::min(planesPerWave, CP.samples_per_wave);
+	const uint32_t planesPerWave = planesPerWaveFor(ctx, count);
 	const uint32_t wavePaths = planesPerWave * pixels;
 	int rc = ensureWave(ctx, wavePaths);
 	if (rc != RB_OK) return rc;
@@ -948,8 +986,9 @@ int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 		rb::WaveParams w{};
 		w.paths = planes * pixels;
 		w.pixels = pixels;
-		w.sampleBase = offset + done;
-		w.fresh = (offset == 0 && done == 0) ? 1u : 0u;
+		w.dyn = dyn;
+		w.sampleBase = dyn ? done : offset + done;
+		w.fresh = dyn ? (done == 0 ? 1u : 0u) : ((offset == 0 && done == 0) ? 1u : 0u);
 		w.keepFailed = ctx->failedMode == RB_FAILED_KEEP ? 1u : 0u;
 		if (cached)
 		{
@@ -961,17 +1000,19 @@ int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 		}
 		for (int k = 0; k < 3; ++k) { w.posMin[k] = posMin[k]; w.posScale[k] = posScale[k]; }
 		unsigned long long* cnt = (ctx->statsMode & RB_STATS_COUNT) ? ctx->counters : nullptr;
+		rb::LaunchShape shape = ctx->shape;
+		shape.items = w.paths;
 		cudaMemsetAsync(soa.counts, 0, sizeof(uint32_t) * rb::kCountSlots, st);
-		timedStage(ctx, 0, st, [&] { rb::launchGenerate(sc, soa, w, ctx->shape, st); });
+		timedStage(ctx, 0, st, [&] { rb::launchGenerate(sc, soa, w, shape, st); });
 		for (int b = 0; b < bounces; ++b)
 		{
-			timedStage(ctx, 1, st, [&] { rb::launchExtend(sc, soa, b, ctx->shape, st, cnt); });
-			timedStage(ctx, 2, st, [&] { rb::launchSurface(sc, soa, w, b, ctx->shape, st, cnt); });
-			timedStage(ctx, 2, st, [&] { rb::launchEmission(sc, soa, b, ctx->shape, st); });
-			timedStage(ctx, 5, st, [&] { rb::launchNee(sc, soa, w, b, ctx->shape, st); });
+			timedStage(ctx, 1, st, [&] { rb::launchExtend(sc, soa, b, shape, st, cnt); });
+			timedStage(ctx, 2, st, [&] { rb::launchSurface(sc, soa, w, b, shape, st, cnt); });
+			timedStage(ctx, 2, st, [&] { rb::launchEmission(sc, soa, b, shape, st); });
+			timedStage(ctx, 5, st, [&] { rb::launchNee(sc, soa, w, b, shape, st); });
 			ctx->launches[5] += 2;   // launchNee runs the pick kernel and two light-sample kernels
-			timedStage(ctx, 6, st, [&] { rb::launchBsdf(sc, soa, w, b, ctx->shape, st); });
-			timedStage(ctx, 3, st, [&] { rb::launchShadow(sc, soa, b, ctx->shape, st, cnt); });
+			timedStage(ctx, 6, st, [&] { rb::launchBsdf(sc, soa, w, b, shape, st); });
+			timedStage(ctx, 3, st, [&] { rb::launchShadow(sc, soa, b, shape, st, cnt); });
 		}
 		if (cached)
 		{
@@ -1001,13 +1042,101 @@ int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 			rb::launchCacheTally(soa, ctx->cacheTally, st);
 			++ctx->launches[8];
 		}
-		timedStage(ctx, 4, st, [&] { rb::launchResolve(sc, soa, w, ctx->accum, ctx->shape, st); });
+		timedStage(ctx, 4, st, [&] { rb::launchResolve(sc, soa, w, ctx->accum, shape, st); });
 		done += planes;
 		ctx->pathsTraced += w.paths;
 		++ctx->waves;
 	}
 	const cudaError_t e = cudaGetLastError();
 	if (e != cudaSuccess) return cudaFail(ctx, e, "rb_render launch");
+	return RB_OK;
+}
+} // namespace
+
+extern "C" {
+
+int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
+{
+	if (!ctx) return RB_ERR_INVALID;
+	int rc = renderReady(ctx);
+	if (rc != RB_OK) return rc;
+	if (count == 0) return RB_OK;
+	rc = checkReferences(ctx);
+	if (rc != RB_OK) return rc;
+	cudaSetDevice(ctx->device);
+	return renderWaves(ctx, offset, count, pick(ctx, stream), nullptr);
+}
+
+int rb_render_graph(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
+{
+	if (!ctx) return RB_ERR_INVALID;
+	int rc = renderReady(ctx);
+	if (rc != RB_OK) return rc;
+	if (count == 0) return RB_OK;
+	rc = checkReferences(ctx);
+	if (rc != RB_OK) return rc;
+	if (ctx->cache || ctx->statsMode) return rb_render(ctx, offset, count, stream);
+	cudaSetDevice(ctx->device);
+	const cudaStream_t st = pick(ctx, stream);
+	// buffers first: the capture must not allocate
+	const uint32_t pixels = ctx->scene.launch.width * ctx->scene.launch.height;
+	rc = ensureWave(ctx, planesPerWaveFor(ctx, count) * pixels);
+	if (rc != RB_OK) return rc;
+	rb_ctx::GraphKey key{};
+	key.scene = ctx->scene;
+	key.soa = ctx->soa;
+	key.accum = ctx->accum;
+	key.count = count;
+	rb_ctx::Graph* g = nullptr;
+	for (auto& c : ctx->graphs)
+		if (std::memcmp(&c.key, &key, sizeof(key)) == 0) { g = &c; break; }
+	if (!g)
+	{
+		// capture the wave sequence once for this call shape and scene state
+		uint32_t launches[9];
+		std::memcpy(launches, ctx->launches, sizeof(launches));
+		const uint64_t paths0 = ctx->pathsTraced, waves0 = ctx->waves;
+		cudaGraph_t graph = nullptr;
+		cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_render_graph: begin capture");
+		rc = renderWaves(ctx, 0, count, st, ctx->dyn);
+		e = cudaStreamEndCapture(st, &graph);
+		if (rc != RB_OK || e != cudaSuccess)
+		{
+			if (graph) cudaGraphDestroy(graph);
+			return rc != RB_OK ? rc : cudaFail(ctx, e, "rb_render_graph: capture");
+		}
+		rb_ctx::Graph ng{};
+		ng.key = key;
+		e = cudaGraphInstantiate(&ng.exec, graph, 0);
+		cudaGraphDestroy(graph);
+		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_render_graph: instantiate");
+		for (int k = 0; k < 9; ++k) ng.launches[k] = ctx->launches[k] - launches[k];
+		ng.paths = ctx->pathsTraced - paths0;
+		ng.waves = ctx->waves - waves0;
+		std::memcpy(ctx->launches, launches, sizeof(launches));
+		ctx->pathsTraced = paths0;
+		ctx->waves = waves0;
+		// graphs of an older scene state are not replayed again; up to 8
+		// call shapes of the current one are kept
+		std::vector<rb_ctx::Graph> keep;
+		for (auto& c : ctx->graphs)
+		{
+			rb_ctx::GraphKey k = c.key;
+			k.count = count;
+			if (keep.size() < 7 && std::memcmp(&k, &key, sizeof(key)) == 0) keep.push_back(c);
+			else cudaGraphExecDestroy(c.exec);
+		}
+		keep.push_back(ng);
+		ctx->graphs.swap(keep);
+		g = &ctx->graphs.back();
+	}
+	rb::launchSetWaveDyn(ctx->dyn, offset, offset == 0 ? 1u : 0u, st);
+	const cudaError_t e = cudaGraphLaunch(g->exec, st);
+	if (e != cudaSuccess) return cudaFail(ctx, e, "rb_render_graph: launch");
+	for (int k = 0; k < 9; ++k) ctx->launches[k] += g->launches[k];
+	ctx->pathsTraced += g->paths;
+	ctx->waves += g->waves;
 	return RB_OK;
 }
 

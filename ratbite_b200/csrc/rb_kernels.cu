@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, Wa
 	{
 		const uint32_t pix = p % w.pixels;
 		const uint32_t x = pix % W, y = pix / W;
-		const uint32_t sample = w.sampleBase + p / w.pixels;
+		const uint32_t sample = waveSampleBase(w) + p / w.pixels;
 		const Qrng q = qrngAt(sample, pixelHash(x, y), 0);
 		const Wavelengths wl = sampleVisible(sample1D(q, DIM_WAVELENGTH));
 		float fu, fv, dx, dy, lu = 0.0f, lv = 0.0f;
@@ -308,7 +308,7 @@ constexpr uint32_t kSfOccluded = 1u << 3;
 RB_D Qrng pathQrng(const DevScene& sc, const WaveParams& w, uint32_t p, uint32_t depth)
 {
 	const uint32_t pix = p % w.pixels;
-	return qrngAt(w.sampleBase + p / w.pixels, pixelHash(pix % sc.launch.width, pix / sc.launch.width), depth);
+	return qrngAt(waveSampleBase(w) + p / w.pixels, pixelHash(pix % sc.launch.width, pix / sc.launch.width), depth);
 }
 
 // wavelength range of the hero sampling, for the cache's normalised input
@@ -760,6 +760,12 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(DevScene s
 	}
 }
 
+__global__ void kSetWaveDyn(uint32_t* dyn, uint32_t offset, uint32_t fresh)
+{
+	dyn[0] = offset;
+	dyn[1] = fresh;
+}
+
 // Unpacks the light tree once per upload (TreeNodeU).
 __global__ void kUnpackLightTree(const PackedNode* in, TreeNodeU* out, uint32_t n)
 {
@@ -775,7 +781,7 @@ __global__ void __launch_bounds__(kThreads) kResolve(DevScene sc, PathSoA s, Wav
 	const float* Z = Y + kSpectrumBins;
 	for (uint32_t pix = gtid(); pix < w.pixels; pix += gstride())
 	{
-		double4 acc = w.fresh ? make_double4(0.0, 0.0, 0.0, 0.0) : accum[pix];
+		double4 acc = waveFresh(w) ? make_double4(0.0, 0.0, 0.0, 0.0) : accum[pix];
 		for (uint32_t k = 0; k < planes; ++k)
 		{
 			const uint32_t p = k * w.pixels + pix;
@@ -962,37 +968,41 @@ LaunchShape queryLaunchShape()
 
 void launchGenerate(const DevScene& sc, const PathSoA& s, const WaveParams& w, const LaunchShape& ls, cudaStream_t st)
 {
-	kGenerate<<<ls.blocksGenerate, kThreads, 0, st>>>(sc, s, w);
+	kGenerate<<<capBlocks(ls.blocksGenerate, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w);
 }
 void launchSurface(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st,
 	unsigned long long* counters)
 {
-	kSurface<<<ls.blocksSurface, kThreads, 0, st>>>(sc, s, w, bounce, counters);
+	kSurface<<<capBlocks(ls.blocksSurface, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce, counters);
 }
 void launchEmission(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st)
 {
-	kEmission<<<ls.blocksEmission, kThreads, 0, st>>>(sc, s, bounce);
+	kEmission<<<capBlocks(ls.blocksEmission, ls.items, kThreads), kThreads, 0, st>>>(sc, s, bounce);
 }
 void launchNee(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
 {
-	kNeePick<<<ls.blocksNeePick, kThreads, 0, st>>>(sc, s, w, bounce);
+	kNeePick<<<capBlocks(ls.blocksNeePick, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce);
 	const size_t treeBytes = sizeof(TreeNodeU) * sc.lights.nodeCount;
 	if (sc.lights.unpacked && treeBytes <= kNeeSharedMaxBytes)
 	{
 		int b = 0;
 		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, reinterpret_cast<const void*>(kNee<true>), kNeeSharedThreads,
 			treeBytes);
-		kNee<true><<<(b < 1 ? 1 : b) * ls.smCount, kNeeSharedThreads, treeBytes, st>>>(sc, s, w, bounce, 0);
+		kNee<true><<<capBlocks((b < 1 ? 1 : b) * ls.smCount, ls.items, kNeeSharedThreads), kNeeSharedThreads, treeBytes, st>>>(sc, s, w, bounce, 0);
 	}
 	else
 	{
-		kNee<false><<<ls.blocksNee, kThreads, 0, st>>>(sc, s, w, bounce, 0);
+		kNee<false><<<capBlocks(ls.blocksNee, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce, 0);
 	}
-	kNee<false><<<ls.blocksNee, kThreads, 0, st>>>(sc, s, w, bounce, 1);
+	kNee<false><<<capBlocks(ls.blocksNee, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce, 1);
 }
 void launchBsdf(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
 {
-	kBsdf<<<ls.blocksBsdf, kThreads, 0, st>>>(sc, s, w, bounce);
+	kBsdf<<<capBlocks(ls.blocksBsdf, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce);
+}
+void launchSetWaveDyn(uint32_t* dyn, uint32_t offset, uint32_t fresh, cudaStream_t st)
+{
+	kSetWaveDyn<<<1, 1, 0, st>>>(dyn, offset, fresh);
 }
 void launchUnpackLightTree(const PackedNode* in, TreeNodeU* out, uint32_t n, cudaStream_t st)
 {
@@ -1000,7 +1010,7 @@ void launchUnpackLightTree(const PackedNode* in, TreeNodeU* out, uint32_t n, cud
 }
 void launchResolve(const DevScene& sc, const PathSoA& s, const WaveParams& w, double4* accum, const LaunchShape& ls, cudaStream_t st)
 {
-	kResolve<<<ls.blocksResolve, kThreads, 0, st>>>(sc, s, w, accum);
+	kResolve<<<capBlocks(ls.blocksResolve, w.pixels, kThreads), kThreads, 0, st>>>(sc, s, w, accum);
 }
 
 void launchSobol(uint32_t n, uint32_t dims, const uint32_t* sample, const uint32_t* hash, const uint32_t* bounce,

@@ -46,6 +46,16 @@ RB_HD uint32_t mix32(uint32_t x)
 	return x;
 }
 
+// A persistent grid of `blocks`, capped at the blocks of `threads` that
+// `items` work items need (items 0: no cap): small waves then launch small
+// grids.
+inline int capBlocks(int blocks, uint32_t items, int threads)
+{
+	if (items == 0) return blocks;
+	const uint32_t need = (items + static_cast<uint32_t>(threads) - 1) / static_cast<uint32_t>(threads);
+	return need < static_cast<uint32_t>(blocks) ? static_cast<int>(need < 1 ? 1 : need) : blocks;
+}
+
 // Grid for a one-thread-per-item batch kernel (grid-stride loops cover the rest).
 inline int gridFor(uint32_t n)
 {

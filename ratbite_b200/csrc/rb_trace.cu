@@ -189,14 +189,14 @@ void queryTraceShape(LaunchShape& ls)
 void launchExtend(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
 	unsigned long long* counters)
 {
-	if (counters) kExtend<true><<<ls.blocksExtend, kThreads, 0, st>>>(sc, s, bounce, counters);
-	else kExtend<false><<<ls.blocksExtend, kThreads, 0, st>>>(sc, s, bounce, nullptr);
+	if (counters) kExtend<true><<<capBlocks(ls.blocksExtend, ls.items, kThreads), kThreads, 0, st>>>(sc, s, bounce, counters);
+	else kExtend<false><<<capBlocks(ls.blocksExtend, ls.items, kThreads), kThreads, 0, st>>>(sc, s, bounce, nullptr);
 }
 void launchShadow(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
 	unsigned long long* counters)
 {
-	if (counters) kShadow<true><<<ls.blocksShadow, kThreads, 0, st>>>(sc, s, bounce, counters);
-	else kShadow<false><<<ls.blocksShadow, kThreads, 0, st>>>(sc, s, bounce, nullptr);
+	if (counters) kShadow<true><<<capBlocks(ls.blocksShadow, ls.items, kThreads), kThreads, 0, st>>>(sc, s, bounce, counters);
+	else kShadow<false><<<capBlocks(ls.blocksShadow, ls.items, kThreads), kThreads, 0, st>>>(sc, s, bounce, nullptr);
 }
 void launchTrace(const DevScene& sc, uint32_t n, const float* rays, uint32_t* payload, float* t, int32_t* tri, cudaStream_t st)
 {

@@ -91,6 +91,10 @@ struct WaveParams
 	uint32_t sampleBase;   // absolute sample index of plane 0 of the wave
 	uint32_t fresh;        // 1: accumulation starts from zero (first wave of a launch at offset 0)
 	uint32_t keepFailed;   // 1: a path with the terminated flag keeps its radiance (RB_FAILED_KEEP)
+	// replayed waves (rb_render_graph): dyn[0] is the call's first sample
+	// index, added to sampleBase, and dyn[1] is 1 when the call starts at
+	// sample 0 (fresh then also needs it); null for directly launched waves
+	const uint32_t* dyn;
 	// radiance-cache form
 	uint32_t cached;       // 1: paths terminate into the cache (PathSoA cache arrays are set)
 	uint32_t trainOneIn;   // one path in trainOneIn is a training path (0: none)
@@ -106,9 +110,24 @@ struct LaunchShape
 	int blocksGenerate, blocksExtend, blocksSurface, blocksEmission, blocksNeePick, blocksNee, blocksBsdf, blocksShadow,
 		blocksResolve;
 	int threads;
+	uint32_t items;   // paths of the wave (0: no limit): grids are capped at the blocks those need
 };
 
+// First sample index and fresh flag of a wave, reading dyn when set.
+#ifdef __CUDACC__
+__device__ __forceinline__ uint32_t waveSampleBase(const WaveParams& w)
+{
+	return w.dyn ? __ldg(w.dyn) + w.sampleBase : w.sampleBase;
+}
+__device__ __forceinline__ bool waveFresh(const WaveParams& w)
+{
+	return w.fresh && (!w.dyn || __ldg(w.dyn + 1) != 0u);
+}
+#endif
+
 LaunchShape queryLaunchShape();
+// dyn[0] = offset, dyn[1] = fresh, stream-ordered (one thread).
+void launchSetWaveDyn(uint32_t* dyn, uint32_t offset, uint32_t fresh, cudaStream_t st);
 void launchGenerate(const DevScene& sc, const PathSoA& s, const WaveParams& w, const LaunchShape& ls, cudaStream_t st);
 // counters: nullptr, or 7 device uint64 (extend rays/nodes/tris, shadow rays/nodes/tris,
 // surface records) to run the counting variants.

@@ -138,6 +138,12 @@ class RenderingInterface:
         s = None if stream is None else C.c_void_p(stream)
         check(self.lib.rb_render(self.ctx, sample_offset, sample_count, s), self.ctx, "rb_render")
 
+    def render_graph(self, sample_offset: int, sample_count: int, stream=None):
+        """render() through a captured CUDA graph of the call's waves (same
+        accumulation); the first call of a sample count captures it."""
+        s = None if stream is None else C.c_void_p(stream)
+        check(self.lib.rb_render_graph(self.ctx, sample_offset, sample_count, s), self.ctx, "rb_render_graph")
+
     def progressive_restart(self, total_samples: int, mode: int = abi.RB_MODE_GRADUAL):
         """Restarts the progressive render (the next step renders sample 0 alone)."""
         check(self.lib.rb_progressive_restart(self.ctx, total_samples, mode), self.ctx, "rb_progressive_restart")
