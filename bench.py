@@ -425,6 +425,44 @@ def run_ours(args, rank: int, world: int, wl: dict):
         dist.destroy_process_group()
 
 
+def run_batched(args):
+    """Batched jobs: 64 render jobs drawn from a seed (ratbite_b200.batch),
+    schedule chosen by the autotuner, aggregate paths/s and p50 / p99 job
+    completion latency (device events)."""
+    import torch
+    from ratbite_b200 import batch
+
+    t0 = time.perf_counter()
+    jobs = batch.draw_jobs(seed=5, n=args.jobs)
+    br = batch.BatchRenderer(jobs, device=0)
+    setup_s = time.perf_counter() - t0
+    best, trials = br.autotune()
+    runs = []
+    with ClockSampler(0) as clocks:
+        for _ in range(max(1, args.steps)):
+            runs.append(br.run(best))
+    r = min(runs, key=lambda x: x.seconds)
+    line = {
+        "metric": METRIC, "value": r.paths_per_s, "unit": "paths/s", "n_gpus": 1, "steps": len(runs),
+        "warmup": 1, "ms_per_step": r.seconds * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scenes)",
+        "config": {"workload": f"batched_{len(jobs)}_jobs", "jobs": len(jobs),
+                   "sides": sorted({j.side for j in jobs}), "spp_range": [min(j.spp for j in jobs), max(j.spp for j in jobs)],
+                   "triangles_range": [min(j.triangles for j in jobs), max(j.triangles for j in jobs)],
+                   "forms": {f: sum(j.form == f for j in jobs) for f in ("plain", "cached")},
+                   "total_paths": r.total_paths, "setup_s": setup_s,
+                   "schedule": {"streams": best.streams, "samples_per_call": best.chunk, "paths_in_flight_per_job": best.max_paths},
+                   "autotune": [{"streams": c.streams, "samples_per_call": c.chunk, "paths_in_flight_per_job": c.max_paths,
+                                 "paths_per_s": v} for c, v in trials],
+                   "l2": "inputs larger than L2 (path state of every job's wave)"},
+        "latency_s": {"p50": r.percentile(50), "p99": r.percentile(99), "max": max(r.latencies)},
+        "host_enqueue_s": r.host_seconds,
+        "gpu_launches": None,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def time_to_rmse(device: int = 0, width: int = 1920, height: int = 1080, depth: int = 12, ref_spp: int = 4096,
                  plain_spp: int = 1024, chunk: int = 32, failed_mode: int = 0, cache_kw: dict | None = None,
                  time_factor: float = 2.0):
@@ -523,7 +561,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="scale")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched"], default="scale")
+    ap.add_argument("--jobs", type=int, default=64, help="batched workload: number of jobs")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample length (0 = skip)")
     ap.add_argument("--ref-step-s", type=float, default=4.0, help="reference arm: seconds per step")
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0 = the workload's)")
@@ -536,10 +575,17 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     args.warmup = max(args.warmup, 3)
-    wl = dict(WORKLOADS[args.workload])
+    wl = dict(WORKLOADS.get(args.workload, WORKLOADS["scale"]))
     if args.spp:
         wl["spp"] = args.spp
         wl["name"] = wl["name"].replace(f"{WORKLOADS[args.workload]['spp']}spp", f"{args.spp}spp")
+    if args.workload == "batched":
+        if rank == 0 and args.impl == "ours":
+            run_batched(args)
+        elif rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference renders one scene at a time; "
+                              "batched jobs have no reference counterpart"}), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world, wl)
     else:
