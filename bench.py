@@ -457,7 +457,7 @@ def run_batched(args):
                    "l2": "inputs larger than L2 (path state of every job's wave)"},
         "latency_s": {"p50": r.percentile(50), "p99": r.percentile(99), "max": max(r.latencies)},
         "host_enqueue_s": r.host_seconds,
-        "gpu_launches": None,
+        "gpu_launches": r.gpu_launches,
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)

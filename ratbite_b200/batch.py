@@ -143,6 +143,9 @@ class BatchRenderer:
                 for c in sizes:
                     self._call(ctxs[j.index], j, 1 << 24, c, streams[k])
         torch.cuda.synchronize()
+        for ri in ctxs.values():                      # launch counters start here
+            ri.get_stats()
+            ri.cache_stats() if ri._cache is not None else None
         start = torch.cuda.Event(enable_timing=True)
         start.record(torch.cuda.current_stream())
         for s in streams:
@@ -161,6 +164,13 @@ class BatchRenderer:
         host_s = time.perf_counter() - t0
         lat = [start.elapsed_time(ends[j.index]) / 1e3 for j in jobs]
         images = {j.index: ctxs[j.index].read_accumulation() for j in jobs} if keep_images else None
+        launches = 0
+        for ri in ctxs.values():
+            st = ri.get_stats()
+            launches += (st.launches_generate + st.launches_extend + st.launches_shade + st.launches_nee
+                         + st.launches_bsdf + st.launches_shadow + st.launches_resolve)
+            if ri._cache is not None:
+                launches += ri.cache_stats().launches
         for j in jobs:
             assert ctxs[j.index].status().flags == 0
             ctxs[j.index].cleanup()
@@ -169,6 +179,7 @@ class BatchRenderer:
         res = Result(schedule, sum(j.side * j.side * spp_of[j.index] for j in jobs), max(lat), lat)
         res.host_seconds = host_s
         res.images = images
+        res.gpu_launches = launches
         return res
 
     @staticmethod

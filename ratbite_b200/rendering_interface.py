@@ -34,6 +34,7 @@ class RenderingInterface:
         self.ctx = h
         self.width = self.height = 0
         self._keep = []
+        self._cache = None
 
     # ---- lifetime ----------------------------------------------------------
     def cleanup(self):
