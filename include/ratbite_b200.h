@@ -240,12 +240,21 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* geometry);
  * the order of rb_geometry.emissive_subsets. World vertices, geometric normals
  * and the BVH boxes are recomputed on the device (the tree topology is kept),
  * stream-ordered on `stream`; the results equal those of rb_set_geometry with
- * the same transforms. The light data (camera-relative emissive triangles and
- * light-tree means) is refreshed by the caller through rb_set_lights, as the
- * reference refills it. */
+ * the same transforms. The light data follows with rb_set_light_origin. */
 int rb_update_instances(rb_ctx* ctx, const float* instance_transforms, const float* subset_transforms,
                         void* stream);
+/* Light data: emissive triangles, light-tree nodes, light pointers, path
+ * bitmasks. The triangle vertices and node means are taken relative to the
+ * light origin (rb_set_light_origin; 0 until set, which uses them as given). */
 int rb_set_lights(rb_ctx* ctx, const rb_light_tree* tree);
+/* The camera-move refresh of the light data on the device (the reference's
+ * fillLightDataBuffer and fillLightTreeDataBuffers,
+ * src/core/rendering_interface.cpp:1433-1510, run on CHANGE_CAMERA_POS
+ * :1615-1622, 1810-1820): every emissive-triangle vertex and light-tree mean
+ * becomes (value given to rb_set_lights) - origin, one float subtraction per
+ * coordinate as the reference computes it on the host, and the tree is
+ * unpacked again; stream-ordered on `stream`. */
+int rb_set_light_origin(rb_ctx* ctx, const float origin[3], void* stream);
 /* Host light-tree build (LightTree::Builder, src/core/light_tree.cpp:47-418,
  * driven as RenderingInterface::buildLightTree, src/core/rendering_interface.cpp:
  * 1065-1167): n emissive triangles with world-space vertices (9 floats each),

@@ -28,6 +28,7 @@ SIGNATURES = {
     "rb_set_materials": (C.c_int, [_P, _P, _U32]),
     "rb_set_geometry": (C.c_int, [_P, _P]),
     "rb_set_lights": (C.c_int, [_P, _P]),
+    "rb_set_light_origin": (C.c_int, [_P, _P, _P]),
     "rb_update_instances": (C.c_int, [_P, _P, _P, _P]),
     "rb_build_light_tree": (C.c_int, [_U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "rb_set_envmap": (C.c_int, [_P, _P, _U32, _U32]),

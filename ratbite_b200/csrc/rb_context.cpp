@@ -74,6 +74,10 @@ struct rb_ctx
 	uint32_t launches[9] = {};   // generate, extend, surface, shadow, resolve, nee, bsdf, cache queries, cache training
 	double stageMs[9] = {};      // device time drained from `timed`
 	uint64_t waves = 0;
+	// light data as given to rb_set_lights (in lightBufs), and the light origin
+	const rb::EmissiveTri* lightWorldTris = nullptr;
+	const rb::PackedNode* lightWorldNodes = nullptr;
+	float lightOrigin[3] = { 0.0f, 0.0f, 0.0f };
 	// geometry bounds at upload (radiance-cache position normalisation)
 	float geoMin[3] = {}, geoMax[3] = {};
 	// radiance-cache form (rb_attach_radiance_cache)
@@ -790,13 +794,21 @@ int rb_set_lights(rb_ctx* ctx, const rb_light_tree* t)
 	}
 	std::vector<void*> fresh;
 	rb::DevLights L{};
-	int rc = upload(ctx, fresh, t->triangles, sizeof(rb::EmissiveTri) * t->triangle_count, L.triangles);
+	// the given (origin-independent) triangles and nodes, and their
+	// camera-relative working copies: given - light origin
+	rb::EmissiveTri *worldTris = nullptr, *tris = nullptr;
+	rb::PackedNode *worldNodes = nullptr, *dn = nullptr;
+	rb::TreeNodeU* du = nullptr;
+	int rc = upload(ctx, fresh, t->triangles, sizeof(rb::EmissiveTri) * t->triangle_count, worldTris);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(rb::EmissiveTri) * std::max<uint32_t>(t->triangle_count, 1), tris);
 	if (rc == RB_OK) rc = upload(ctx, fresh, t->bitmasks, sizeof(uint64_t) * t->triangle_count, L.bitmasks);
 	if (rc == RB_OK) rc = upload(ctx, fresh, t->pointers, sizeof(uint32_t) * t->pointer_count, L.pointers);
-	rb::PackedNode* dn = nullptr;
-	rb::TreeNodeU* du = nullptr;
-	if (rc == RB_OK && t->node_count) rc = upload(ctx, fresh, t->nodes, sizeof(rb::PackedNode) * t->node_count, dn);
+	if (rc == RB_OK && t->node_count) rc = upload(ctx, fresh, t->nodes, sizeof(rb::PackedNode) * t->node_count, worldNodes);
+	if (rc == RB_OK && t->node_count) rc = upload(ctx, fresh, nullptr, sizeof(rb::PackedNode) * t->node_count, dn);
 	if (rc == RB_OK && t->node_count) rc = upload(ctx, fresh, nullptr, sizeof(rb::TreeNodeU) * t->node_count, du);
+	if (rc == RB_OK)
+		rb::launchLightOrigin(worldTris, tris, t->triangle_count, worldNodes, dn, t->node_count, ctx->lightOrigin[0],
+			ctx->lightOrigin[1], ctx->lightOrigin[2], ctx->stream);
 	if (rc == RB_OK && t->node_count) rb::launchUnpackLightTree(dn, du, t->node_count, ctx->stream);
 	if (rc == RB_OK)
 	{
@@ -805,15 +817,36 @@ int rb_set_lights(rb_ctx* ctx, const rb_light_tree* t)
 	}
 	rc = commit(ctx, ctx->lightBufs, fresh, rc);
 	if (rc != RB_OK) return rc;
+	L.triangles = t->triangle_count ? tris : nullptr;
 	L.nodes = dn;
 	L.unpacked = du;
 	L.nodeCount = t->node_count;
 	L.triangleCount = t->triangle_count;
 	ctx->scene.lights = L;
+	ctx->lightWorldTris = worldTris;
+	ctx->lightWorldNodes = worldNodes;
 	ctx->lightMaxMaterial = 0;
 	const rb::EmissiveTri* lt = static_cast<const rb::EmissiveTri*>(t->triangles);
 	for (uint32_t i = 0; i < t->triangle_count; ++i) ctx->lightMaxMaterial = std::max(ctx->lightMaxMaterial, lt[i].material + 1);
 	return RB_OK;
+}
+
+int rb_set_light_origin(rb_ctx* ctx, const float origin[3], void* stream)
+{
+	if (!ctx || !origin) return RB_ERR_INVALID;
+	for (int k = 0; k < 3; ++k)
+		if (!std::isfinite(origin[k])) return fail(ctx, RB_ERR_INVALID, "rb_set_light_origin: non-finite origin");
+	cudaSetDevice(ctx->device);
+	for (int k = 0; k < 3; ++k) ctx->lightOrigin[k] = origin[k];
+	const rb::DevLights& L = ctx->scene.lights;
+	if (L.triangleCount + L.nodeCount == 0) return RB_OK;
+	const cudaStream_t st = pick(ctx, stream);
+	rb::launchLightOrigin(ctx->lightWorldTris, const_cast<rb::EmissiveTri*>(L.triangles), L.triangleCount,
+		ctx->lightWorldNodes, const_cast<rb::PackedNode*>(L.nodes), L.nodeCount, origin[0], origin[1], origin[2], st);
+	if (L.nodeCount)
+		rb::launchUnpackLightTree(L.nodes, const_cast<rb::TreeNodeU*>(L.unpacked), L.nodeCount, st);
+	const cudaError_t e = cudaGetLastError();
+	return e == cudaSuccess ? RB_OK : cudaFail(ctx, e, "rb_set_light_origin");
 }
 
 int rb_set_envmap(rb_ctx* ctx, const float* rgba, uint32_t w, uint32_t h)

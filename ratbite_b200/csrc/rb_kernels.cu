@@ -766,6 +766,36 @@ __global__ void kSetWaveDyn(uint32_t* dyn, uint32_t offset, uint32_t fresh)
 	dyn[1] = fresh;
 }
 
+// Camera-relative light data (the reference's fillLightDataBuffer /
+// fillLightTreeDataBuffers): one float subtraction per coordinate.
+__global__ void kLightOrigin(const EmissiveTri* __restrict__ worldTris, EmissiveTri* __restrict__ tris, uint32_t nTris,
+	const PackedNode* __restrict__ worldNodes, PackedNode* __restrict__ nodes, uint32_t nNodes, float ox, float oy,
+	float oz)
+{
+	for (uint32_t i = gtid(); i < nTris + nNodes; i += gstride())
+	{
+		if (i < nTris)
+		{
+			EmissiveTri t = worldTris[i];
+			for (int k = 0; k < 3; ++k)
+			{
+				t.v[3 * k] = __fsub_rn(t.v[3 * k], ox);
+				t.v[3 * k + 1] = __fsub_rn(t.v[3 * k + 1], oy);
+				t.v[3 * k + 2] = __fsub_rn(t.v[3 * k + 2], oz);
+			}
+			tris[i] = t;
+		}
+		else
+		{
+			PackedNode n = worldNodes[i - nTris];
+			n.mean[0] = __fsub_rn(n.mean[0], ox);
+			n.mean[1] = __fsub_rn(n.mean[1], oy);
+			n.mean[2] = __fsub_rn(n.mean[2], oz);
+			nodes[i - nTris] = n;
+		}
+	}
+}
+
 // Unpacks the light tree once per upload (TreeNodeU).
 __global__ void kUnpackLightTree(const PackedNode* in, TreeNodeU* out, uint32_t n)
 {
@@ -1003,6 +1033,12 @@ void launchBsdf(const DevScene& sc, const PathSoA& s, const WaveParams& w, int b
 void launchSetWaveDyn(uint32_t* dyn, uint32_t offset, uint32_t fresh, cudaStream_t st)
 {
 	kSetWaveDyn<<<1, 1, 0, st>>>(dyn, offset, fresh);
+}
+void launchLightOrigin(const EmissiveTri* worldTris, EmissiveTri* tris, uint32_t nTris, const PackedNode* worldNodes,
+	PackedNode* nodes, uint32_t nNodes, float ox, float oy, float oz, cudaStream_t st)
+{
+	if (nTris + nNodes == 0) return;
+	kLightOrigin<<<gridFor(nTris + nNodes), kThreads, 0, st>>>(worldTris, tris, nTris, worldNodes, nodes, nNodes, ox, oy, oz);
 }
 void launchUnpackLightTree(const PackedNode* in, TreeNodeU* out, uint32_t n, cudaStream_t st)
 {

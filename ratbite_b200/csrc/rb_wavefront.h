@@ -144,6 +144,10 @@ void launchBsdf(const DevScene& sc, const PathSoA& s, const WaveParams& w, int b
 void launchResolveImage(uint32_t width, uint32_t height, const float* colorspace, float exposureScale,
 	const double4* data, uint32_t* out, int smCount, cudaStream_t st);
 void launchUnpackLightTree(const PackedNode* in, TreeNodeU* out, uint32_t n, cudaStream_t st);
+// Camera-relative light data: tris[i].v = worldTris[i].v - origin, nodes[i].mean =
+// worldNodes[i].mean - origin (all other fields copied).
+void launchLightOrigin(const EmissiveTri* worldTris, EmissiveTri* tris, uint32_t nTris, const PackedNode* worldNodes,
+	PackedNode* nodes, uint32_t nNodes, float ox, float oy, float oz, cudaStream_t st);
 void queryTraceShape(LaunchShape& ls);   // fills blocksExtend, blocksShadow (rb_trace.cu)
 void launchShadow(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
 	unsigned long long* counters);

@@ -133,6 +133,13 @@ class RenderingInterface:
         check(self.lib.rb_update_instances(self.ctx, _ptr(inst) if inst.size else None,
                                            _ptr(sub) if sub.size else None, s), self.ctx, "rb_update_instances")
 
+    def set_light_origin(self, origin, stream=None):
+        """Camera-move refresh of the light data on the device: emissive
+        triangle vertices and light-tree means become (as loaded) - origin."""
+        o = np.ascontiguousarray(origin, np.float32).reshape(3)
+        s = None if stream is None else C.c_void_p(stream)
+        check(self.lib.rb_set_light_origin(self.ctx, _ptr(o), s), self.ctx, "rb_set_light_origin")
+
     # ---- rendering -----------------------------------------------------------
     def render(self, sample_offset: int, sample_count: int, stream=None):
         """Asynchronous: renders samples [offset, offset+count) of every pixel."""

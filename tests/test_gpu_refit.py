@@ -103,6 +103,48 @@ def test_refit_equals_fresh_upload(delta):
         ri.cleanup()
 
 
+@pytest.mark.parametrize("delta", [(0.37, -0.21, 1.3), (-25.0, 3.5, 60.0)])
+def test_camera_move_on_device_equals_host_refresh(delta):
+    """The whole camera-move refresh on the device -- rb_update_instances for
+    the transforms and rb_set_light_origin for the light data -- against a
+    fresh context given the moved transforms and the light records refreshed
+    on the host as the reference does (fillLightDataBuffer /
+    fillLightTreeDataBuffers: float32 world value - camera position): the
+    renders must be bit-identical."""
+    ref = RefLib()
+    tables = dict(cie=ref.cie_xyz(), basis=ref.basis_rgb(), luts=reference_luts())
+    sc = scenes.scale_scene(seed=5, target_tris=60_000, n_emitters=48, width=64, height=36, spp=4, max_depth=6,
+                            envmap_size=(64, 32))
+    lt = lighttree.build_for_scene(sc)
+    moved = _moved(sc, delta)
+    a = _context(sc, tables, lt)
+    a.update_instances(np.stack([x for _, x in moved.instances]),
+                       np.stack([e["transform"] for e in moved.emissive]) if moved.emissive else None)
+    a.set_light_origin(delta)
+    tris, nodes, ptrs, masks = lt._arrays
+    cam = np.asarray(delta, np.float32)
+    t2, n2 = tris.copy(), nodes.copy()
+    t2["vertices"] = (t2["vertices"].reshape(-1, 3, 3) - cam).reshape(-1, 9)
+    n2["mean"] = n2["mean"] - cam
+    b = _context(moved, tables, lighttree.record(t2, n2, ptrs.copy(), masks.copy()))
+    a.render(0, 4)
+    b.render(0, 4)
+    ga, gb = a.read_accumulation(), b.read_accumulation()
+    assert ga[..., :3].sum() > 0
+    assert np.array_equal(ga, gb)
+    # and back: origin 0 restores the light data as loaded
+    a.set_light_origin((0.0, 0.0, 0.0))
+    a.update_instances(np.stack([x for _, x in sc.instances]),
+                       np.stack([e["transform"] for e in sc.emissive]) if sc.emissive else None)
+    c = _context(sc, tables, lt)
+    a.render(0, 4)
+    c.render(0, 4)
+    assert np.array_equal(a.read_accumulation(), c.read_accumulation())
+    for ri in (a, b, c):
+        assert ri.status().flags == 0
+        ri.cleanup()
+
+
 def test_refit_rejects_bad_transforms():
     ref = RefLib()
     tables = dict(cie=ref.cie_xyz(), basis=ref.basis_rgb(), luts=reference_luts())
