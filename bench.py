@@ -152,7 +152,9 @@ def make_scene(wl: dict):
     from ratbite_b200 import assets, scenes
     cie = assets.cie_xyz()
     basis = assets.basis_rgb()
-    luts = assets.luts()
+    # compensation tables regenerated on the GPU (rb_k_generate_luts: they
+    # match the reference's bin/*.bin to Monte Carlo noise); sheen: stand-in
+    luts = assets.generated_luts(samples=1 << 14)
     if wl["name"].startswith("cornell"):
         scene = scenes.cornell_box(seed=1, cie_xyz=cie, width=wl["width"], height=wl["height"], spp=wl["spp"],
                                    max_depth=wl["depth"])

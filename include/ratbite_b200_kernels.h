@@ -141,6 +141,16 @@ int rb_envmap_cdf_noalloc(uint32_t width, uint32_t height, const float* rgba, in
                           uint16_t* conditional_idx, uint16_t* marginal_idx, float* integral,
                           void* stream);
 
+/* Regenerates the multiple-scattering compensation tables (no counterpart in
+ * the reference, which ships them as bin/*.bin without a generator) by Monte
+ * Carlo integration of the BxDF lobes: `samples` visible-normal samples per
+ * texel, on the reference's grids (i / 31 per axis). Outputs (device, 32x32
+ * and 32^3 floats, the layouts rb_set_luts takes): conductor albedo;
+ * dielectric albedo, eta > 1 and eta < 1; reflective share, eta > 1 and
+ * eta < 1 (definitions in rb_lut.cu). */
+int rb_k_generate_luts(uint32_t samples, float* conductor, float* dielectric_outer, float* dielectric_inner,
+                       float* reflective_outer, float* reflective_inner, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

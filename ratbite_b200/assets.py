@@ -112,3 +112,26 @@ def luts(n_mc: int = 256) -> dict:
     sheen[..., 2] = (0.15 * alpha[:, None] * (1.0 - 0.5 * mu[None, :])).astype(np.float32)
     return dict(conductor=cond.reshape(-1), dielectric_outer=diel.reshape(-1), dielectric_inner=diel.reshape(-1),
                 reflective_outer=refl.reshape(-1), reflective_inner=refl.reshape(-1), sheen=sheen.reshape(-1))
+
+
+def generated_luts(samples: int = 1 << 14, device: int = 0) -> dict:
+    """The multiple-scattering tables regenerated on the GPU by Monte Carlo
+    integration of the BxDF lobes (rb_k_generate_luts); the sheen table is
+    the stand-in of luts() (an LTC fit, not an albedo)."""
+    import ctypes as C
+
+    import torch
+
+    from ._native import check, load
+    lib = load()
+    with torch.cuda.device(device):
+        cond = torch.zeros(32 * 32, dtype=torch.float32, device="cuda")
+        t3 = [torch.zeros(32 ** 3, dtype=torch.float32, device="cuda") for _ in range(4)]
+        check(lib.rb_k_generate_luts(samples, C.c_void_p(cond.data_ptr()), *[C.c_void_p(t.data_ptr()) for t in t3],
+                                     None), None, "rb_k_generate_luts")
+        torch.cuda.synchronize()
+    out = luts(n_mc=1)
+    out.update(conductor=cond.cpu().numpy(), dielectric_outer=t3[0].cpu().numpy(),
+               dielectric_inner=t3[1].cpu().numpy(), reflective_outer=t3[2].cpu().numpy(),
+               reflective_inner=t3[3].cpu().numpy())
+    return out
