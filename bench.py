@@ -482,7 +482,7 @@ def time_to_rmse(device: int = 0, width: int = 1920, height: int = 1080, depth: 
     from ratbite_b200.nrc import RadianceCache
     from ratbite_b200.rendering_interface import RenderingInterface
 
-    cie, basis, luts = assets.cie_xyz(), assets.basis_rgb(), assets.luts()
+    cie, basis, luts = assets.cie_xyz(), assets.basis_rgb(), assets.generated_luts(samples=1 << 14, device=device)
     scene = scenes.cornell_box(seed=1, cie_xyz=cie, width=width, height=height, spp=plain_spp, max_depth=depth)
     lt = lighttree.build_for_scene(scene)
     ri = RenderingInterface(device=device, failed_sample_mode=failed_mode)

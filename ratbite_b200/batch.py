@@ -92,7 +92,8 @@ class BatchRenderer:
     def __init__(self, jobs: list[Job], device: int = 0, max_depth: int = 12, threads: int = 8):
         self.jobs = jobs
         self.device = device
-        self.cie, self.basis, self.luts = assets.cie_xyz(), assets.basis_rgb(), assets.luts()
+        self.cie, self.basis = assets.cie_xyz(), assets.basis_rgb()
+        self.luts = assets.generated_luts(samples=1 << 14, device=device)   # regenerated on the GPU
 
         def build(job):
             sc = scenes.scale_scene(seed=job.seed, target_tris=job.triangles,
