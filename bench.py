@@ -75,16 +75,16 @@ WORKLOADS = {
 #           flags 8 + queue 4 written (for surface records)
 #   nee     per surface record: queue 4, record 48, normal 16, flags 8,
 #           wavelengths 16 read; record word 16 and the light sample 48 written
-#   bsdf    per surface record: queue 4, record 80, ray o/d 32, normal 16,
-#           flags 8, wavelengths + pdfs + throughput 48, light sample 32 read;
-#           throughput, flags, normal, pdfs, ray o/d 88, contribution 16 and
-#           two queue slots 8 written
+#   bsdf    per surface record (both BxDF kernels): queue 4, record 80, ray
+#           o/d 32, normal 16, flags 8, wavelengths + pdfs + throughput 48,
+#           light sample 32 read; throughput, flags, ray o/d 56, contribution
+#           16 and two queue slots 8 written
 EXTEND_BYTES_PER_RAY = 4 + 32 + 16
 SHADOW_BYTES_PER_RAY = 4 + 32 + 32 + 16
 SURFACE_BYTES_PER_PATH = 4 + 32 + 16 + 8 + 16 + 56
 SURFACE_BYTES_PER_RECORD = 12 + 48 + 80 + 16 + 8 + 4
 NEE_BYTES_PER_RECORD = 4 + 48 + 16 + 8 + 16 + 16 + 48
-BSDF_BYTES_PER_RECORD = 4 + 80 + 32 + 16 + 8 + 48 + 32 + 88 + 16 + 8
+BSDF_BYTES_PER_RECORD = 4 + 80 + 32 + 16 + 8 + 48 + 32 + 56 + 16 + 8
 NODE_BYTES, TRI_BYTES = 96, 48
 
 

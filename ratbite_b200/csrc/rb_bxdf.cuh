@@ -313,7 +313,16 @@ struct BxdfState
 	float refractionScale;
 };
 
+// Which part of a BxDF callable runs: the evaluation of the light sample
+// (the callable's direct-lighting block), the BxDF sample and everything
+// after it, or the whole body. The two parts read disjoint outputs of each
+// other: the light part writes only `nee`/`hasNee`, the sample part never
+// reads them, so running the parts in two kernels gives the whole body's
+// results bit for bit.
+enum BxdfPart : int { kBxdfAll = 0, kBxdfLight = 1, kBxdfSample = 2 };
+
 // __direct_callable__PureConductorBxDF (pathtrace.cu:464-547).
+template<int PART>
 RB_D void bxdfPureConductor(const DevScene& sc, const DevMaterial& mat, const LightSample& dl, const Qrng& q,
 	const Frame& local, BxdfState& s)
 {
@@ -341,7 +350,7 @@ RB_D void bxdfPureConductor(const DevScene& sc, const DevMaterial& mat, const Li
 		s.dir = normalize(local.fromLocal(wi));
 		return;
 	}
-	if (!dl.occluded)
+	if (PART != kBxdfSample && !dl.occluded)
 	{
 		const f3 wi = li;
 		if (wo.z * wi.z > 0.0f)
@@ -359,6 +368,7 @@ RB_D void bxdfPureConductor(const DevScene& sc, const DevMaterial& mat, const Li
 			s.hasNee = true;
 		}
 	}
+	if (PART == kBxdfLight) return;
 	float u, v;
 	sample2D(q, DIM_BXDF_0, u, v);
 	const f3 wm = vndfSampleBounded(wo, ax, ay, u, v);
@@ -376,6 +386,7 @@ RB_D void bxdfPureConductor(const DevScene& sc, const DevMaterial& mat, const Li
 
 // __direct_callable__ComplexSurface_BxDF (pathtrace.cu:548-905): sheen over a
 // metal / dielectric-specular / translucent / glossy-diffuse base.
+template<int PART>
 RB_D void bxdfComplexSurface(const DevScene& sc, const LightSample& dl, const Qrng& q, const Frame& local,
 	const Surface& surf, BxdfState& s)
 {
@@ -409,7 +420,7 @@ RB_D void bxdfComplexSurface(const DevScene& sc, const LightSample& dl, const Qr
 	const float* basis = sc.spectra.basis;
 
 	// Direct lighting (pathtrace.cu:660-771).
-	if (!dl.occluded)
+	if (PART != kBxdfSample && !dl.occluded)
 	{
 		const f3 wi = li;
 		const CtxDir ci = ctxDir(wi);
@@ -483,6 +494,7 @@ RB_D void bxdfComplexSurface(const DevScene& sc, const LightSample& dl, const Qr
 		}
 	}
 
+	if (PART == kBxdfLight) return;
 	// BxDF sampling (pathtrace.cu:773-892).
 	f3 wi;
 	{
@@ -579,12 +591,13 @@ RB_D void bxdfComplexSurface(const DevScene& sc, const LightSample& dl, const Qr
 // Dispatch on the material's callable index, as optixDirectCall does with
 // MaterialData::bxdfIndexSBT (pathtrace.cu:1724-1733). Index 1 (the pure
 // dielectric callable) has an empty body in the reference and changes nothing.
+template<int PART = kBxdfAll>
 RB_D void evalBxdf(const DevScene& sc, const DevMaterial& mat, const LightSample& dl, const Qrng& q,
 	const Frame& local, const Surface& surf, BxdfState& s)
 {
 	if (mat.bxdf == 2u)
-		bxdfComplexSurface(sc, dl, q, local, surf, s);
+		bxdfComplexSurface<PART>(sc, dl, q, local, surf, s);
 	else if (mat.bxdf == 0u)
-		bxdfPureConductor(sc, mat, dl, q, local, s);
+		bxdfPureConductor<PART>(sc, mat, dl, q, local, s);
 }
 } // namespace rb

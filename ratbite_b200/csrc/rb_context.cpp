@@ -1045,6 +1045,7 @@ int renderWaves(rb_ctx* ctx, uint32_t offset, uint32_t count, cudaStream_t st, c
 			timedStage(ctx, 5, st, [&] { rb::launchNee(sc, soa, w, b, shape, st); });
 			ctx->launches[5] += 2;   // launchNee runs the pick kernel and two light-sample kernels
 			timedStage(ctx, 6, st, [&] { rb::launchBsdf(sc, soa, w, b, shape, st); });
+			ctx->launches[6] += 1;   // launchBsdf runs the light-sample evaluation and the BxDF sample kernels
 			timedStage(ctx, 3, st, [&] { rb::launchShadow(sc, soa, b, shape, st, cnt); });
 		}
 		if (cached)

@@ -275,12 +275,14 @@ __global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, Wa
 }
 
 // Minimum resident blocks per SM requested for the shading kernels, which
-// caps their registers per thread (65536 / (128 x blocks)): 85, 64 and 32.
+// caps their registers per thread (65536 / (128 x blocks)): 85, 64 and 64.
 // These kernels are latency-bound, and on B200 (at-scale frame) the extra
 // warps outweigh the spilled bytes, which stay in L1: surface -8%, light
-// sample -6%, BxDF -38% against the compiler's own choice (BxDF at 5 / 6 /
-// 8 / 12 / 16 blocks: 339 / 306 / 265 / 236 / 232 ms per frame, with 100 B
-// to 1.2 KB of spills per thread).
+// sample -6% against the compiler's own choice. The BxDF stage runs as two
+// kernels (light-sample evaluation, BxDF sample; 94 and 109 registers
+// uncapped), both at 8 blocks: 188 ms per frame, against 202 / 216 / 220 /
+// 203 ms at 12 / 4 / 5 / 6 blocks, and 229 ms for the single kernel at its
+// best cap (16 blocks, 32 registers, 1.2 KB of spills per thread).
 #ifndef RB_SURFACE_MIN_BLOCKS
 #define RB_SURFACE_MIN_BLOCKS 6
 #endif
@@ -288,7 +290,7 @@ __global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, Wa
 #define RB_NEE_MIN_BLOCKS 8
 #endif
 #ifndef RB_BSDF_MIN_BLOCKS
-#define RB_BSDF_MIN_BLOCKS 16
+#define RB_BSDF_MIN_BLOCKS 8
 #endif
 
 // Block size of the shared-memory light-sample kernel: two blocks of 512
@@ -651,10 +653,47 @@ kNee(DevScene sc, PathSoA s, WaveParams w, int bounce, int which)
 	}
 }
 
-// Stage 3 of shading: the BxDF call with the light sample
-// (pathtrace.cu:1724-1733), Russian roulette, the next ray and the depth
-// limits (:1736-1785). Continuing paths go to the next extend queue, light
-// samples that passed to the shadow queue.
+// Stage 3a of shading: the BxDF callable's evaluation of the light sample
+// (pathtrace.cu:1724-1733 calling the direct-lighting block, :660-771 of the
+// complex surface, :498-520 of the conductor). Its contribution replaces the
+// light's spectrum in the record; a light sample that gets none is marked
+// occluded, so the next stage queues no shadow ray for it. Split from the
+// BxDF sample (stage 3b) so neither kernel holds both parts' registers.
+__global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdfLight(DevScene sc, PathSoA s, WaveParams w, int bounce)
+{
+	const uint32_t n = s.counts[kSurfaceCounts + bounce];
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const uint32_t p = s.surfQueue[i];
+		const uint32_t bits = __float_as_uint(lastWord(s.sfPi + p));
+		if (bits & (kSfSkipped | kSfOccluded)) continue;
+		const DevMaterial& mat = sc.materials[__float_as_uint(lastWord(s.sfP + p))];
+		const float4 rd = s.rayD[p], dd = s.shD[p];
+		const uint2 fd = s.fd[p];
+		BxdfState st;
+		st.hasNee = false;
+		st.wl.lambda = s4(s.lambda[p]);
+		st.T = s4(s.T[p]);
+		st.pdf = rd.w;
+		st.dir = f3_of(rd);
+		st.flags = fd.x;
+		st.refractionScale = lastWord(s.rayO + p);
+		LightSample dl;
+		dl.spectrum = s4(s.shC[p]);
+		dl.dir = f3_of(dd);
+		dl.pdf = dd.w;
+		dl.occluded = false;
+		const Frame frame{ f3_of(s.sfT[p]), f3_of(s.sfB[p]), f3_of(s.nrm[p]) };
+		evalBxdf<kBxdfLight>(sc, mat, dl, pathQrng(sc, w, p, fd.y), frame, surfaceOf(mat), st);
+		if (st.hasNee) s.shC[p] = f4(st.nee);
+		else reinterpret_cast<float*>(s.sfPi + p)[3] = __uint_as_float(bits | kSfOccluded);
+	}
+}
+
+// Stage 3b of shading: the BxDF sample (the rest of the callable,
+// pathtrace.cu:773-905 / :521-547), Russian roulette, the next ray and the
+// depth limits (:1736-1785). Continuing paths go to the next extend queue,
+// light samples that passed stage 3a to the shadow queue.
 __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(DevScene sc, PathSoA s, WaveParams w, int bounce)
 {
 	const uint32_t n = s.counts[kSurfaceCounts + bounce];
@@ -664,40 +703,39 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(DevScene s
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
 		const uint32_t p = s.surfQueue[i];
-		const float4 hp = s.sfP[p], pi = s.sfPi[p], gv = s.sfGn[p];
-		const uint32_t bits = __float_as_uint(pi.w);
+		// Only the words the BxDF sample needs are read before it; the hit
+		// points, the geometric normal and the ray origin are read after it,
+		// so they are not live (and spilled) across the call.
+		const uint32_t bits = __float_as_uint(lastWord(s.sfPi + p));
 		const bool skipped = (bits & kSfSkipped) != 0, backHit = (bits & kSfBackHit) != 0;
-		const f3 hitPos = f3_of(hp), hitPosInterp = f3_of(pi), gn = f3_of(gv);
-		const float4 ro = s.rayO[p], rd = s.rayD[p], nv = s.nrm[p];
+		const float4 rd = s.rayD[p];
 		const uint2 fd = s.fd[p];
 		uint32_t flags = fd.x, depth = fd.y;
 		const Qrng q = pathQrng(sc, w, p, depth);
-		const DevMaterial& mat = sc.materials[__float_as_uint(hp.w)];
+		const DevMaterial& mat = sc.materials[__float_as_uint(lastWord(s.sfP + p))];
 
+		// The BxDF reads the wavelengths and changes none of them: only
+		// their values are loaded, and nothing is written back.
 		BxdfState st;
 		st.hasNee = false;
-		st.wl = Wavelengths{ s4(s.lambda[p]), s4(s.lpdf[p]), nv.w };
+		st.wl.lambda = s4(s.lambda[p]);
 		st.T = s4(s.T[p]);
 		st.pdf = rd.w;
 		st.dir = f3_of(rd);
 		st.flags = flags;
-		st.refractionScale = ro.w;
+		st.refractionScale = lastWord(s.rayO + p);
 		bool hasShadow = false;
 		if (!skipped)
 		{
-			const float4 dd = s.shD[p];
 			LightSample dl;
-			dl.spectrum = s4(s.shC[p]);
-			dl.dir = f3_of(dd);
-			dl.pdf = dd.w;
-			dl.occluded = (bits & kSfOccluded) != 0;
-			const Frame frame{ f3_of(s.sfT[p]), f3_of(s.sfB[p]), f3_of(nv) };
-			evalBxdf(sc, mat, dl, q, frame, surfaceOf(mat), st);
-			hasShadow = !dl.occluded && st.hasNee && !(st.flags & PF_PATH_TERMINATED);
+			dl.occluded = true;      // not read by the sample part
+			const Frame frame{ f3_of(s.sfT[p]), f3_of(s.sfB[p]), f3_of(s.nrm[p]) };
+			evalBxdf<kBxdfSample>(sc, mat, dl, q, frame, surfaceOf(mat), st);
+			hasShadow = !(bits & kSfOccluded) && !(st.flags & PF_PATH_TERMINATED);
 		}
 		flags = st.flags;
 		S4 T = st.T;
-		f3 rayO = f3_of(ro), rayD = st.dir;
+		f3 rayO = f3_of(s.rayO[p]), rayD = st.dir;
 		const float refrScale = st.refractionScale;
 		bool done = false;
 		if (flags & PF_PATH_TERMINATED)
@@ -727,6 +765,7 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(DevScene s
 				const bool refracted = (flags & PF_RAY_REFRACTED) != 0;
 				const bool triGeo = (flags & PF_TRIANGULAR_GEOMETRY) != 0;
 				const bool in = refracted || skipped;
+				const f3 hitPos = f3_of(s.sfP[p]), hitPosInterp = f3_of(s.sfPi[p]), gn = f3_of(s.sfGn[p]);
 				const f3 origin = (in == backHit) && triGeo ? hitPosInterp : hitPos;
 				const f3 offset = in == backHit ? gn : -gn;
 				rayO = offsetPoint(origin, offset);
@@ -748,11 +787,8 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(DevScene s
 				done = (flags & PF_FINISHED) != 0;
 			}
 		}
-		if (hasShadow) s.shC[p] = f4(st.nee);
 		s.T[p] = f4(T);
 		s.fd[p] = make_uint2(flags, depth);
-		s.nrm[p] = make_float4(nv.x, nv.y, nv.z, st.wl.active);
-		s.lpdf[p] = f4(st.wl.pdf);
 		s.rayO[p] = f4_of(rayO, refrScale);
 		s.rayD[p] = f4_of(rayD, st.pdf);
 		if (hasShadow) s.shadowQueue[appendIndex(shadowCount)] = p;
@@ -991,6 +1027,7 @@ LaunchShape queryLaunchShape()
 	cudaFuncSetAttribute(reinterpret_cast<const void*>(kNee<true>), cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(kNeeSharedMaxBytes));
 	ls.blocksBsdf = occ(reinterpret_cast<const void*>(kBsdf));
+	ls.blocksBsdfLight = occ(reinterpret_cast<const void*>(kBsdfLight));
 	ls.blocksResolve = occ(reinterpret_cast<const void*>(kResolve));
 	queryTraceShape(ls);
 	return ls;
@@ -1028,6 +1065,7 @@ void launchNee(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bo
 }
 void launchBsdf(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
 {
+	kBsdfLight<<<capBlocks(ls.blocksBsdfLight, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce);
 	kBsdf<<<capBlocks(ls.blocksBsdf, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce);
 }
 void launchSetWaveDyn(uint32_t* dyn, uint32_t offset, uint32_t fresh, cudaStream_t st)

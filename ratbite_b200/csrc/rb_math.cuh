@@ -49,6 +49,8 @@ RB_HD float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi)
 RB_HD float mixf(float x, float y, float a) { return x * (1.0f - a) + y * a; }
 RB_HD f3 f3_of(float4 v) { return f3{ v.x, v.y, v.z }; }
 RB_HD float4 f4_of(f3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
+// The w word of a float4 in memory, read alone (a 4-byte load).
+RB_HD float lastWord(const float4* v) { return reinterpret_cast<const float*>(v)[3]; }
 
 // Four-wavelength spectrum sample (SampledSpectrum, src/device/spectral.h:14-194).
 struct S4

@@ -107,7 +107,7 @@ struct WaveParams
 struct LaunchShape
 {
 	int smCount;
-	int blocksGenerate, blocksExtend, blocksSurface, blocksEmission, blocksNeePick, blocksNee, blocksBsdf, blocksShadow,
+	int blocksGenerate, blocksExtend, blocksSurface, blocksEmission, blocksNeePick, blocksNee, blocksBsdf, blocksBsdfLight, blocksShadow,
 		blocksResolve;
 	int threads;
 	uint32_t items;   // paths of the wave (0: no limit): grids are capped at the blocks those need
