@@ -70,15 +70,16 @@ namespace sg
 {
 constexpr float kPiSG = 3.14159265359f;   // SphericalGaussian::Math::PI
 RB_D float mulsign(float x, float y) { return __uint_as_float((__float_as_uint(y) & 0x80000000u) ^ __float_as_uint(x)); }
-// exp(x) - 1 and (exp(x) - 1)/x with Higham's cancellation trick.
-RB_D float expm1c(float x)
+// exp(x) - 1 and (exp(x) - 1)/x with Higham's cancellation trick;
+// expm1cOf takes u = expf(x) already computed.
+RB_D float expm1cOf(float x, float u)
 {
-	const float u = expf(x);
 	if (u == 1.0f) return x;
 	const float y = u - 1.0f;
 	if (fabsf(x) < 1.0f) return y * x / logf(u);
 	return y;
 }
+RB_D float expm1c(float x) { return expm1cOf(x, expf(x)); }
 RB_D float expm1OverX(float x)
 {
 	const float u = expf(x);
@@ -125,21 +126,6 @@ RB_D Lobe product(f3 a1, float s1, f3 a2, float s2)
 	const float logAmp = 2.0f * sMin * (cosine - 1.0f) / (sqrtf(2.0f * ratio * cosine + ratio * ratio + 1.0f) + ratio + 1.0f);
 	return Lobe{ axis / fmaxf(sharp, FLT_MIN), sharp, logAmp };
 }
-RB_D float upperClampedCosineOverTwoPi(float s)
-{
-	if (s <= 0.5f)
-		return (((((((-1.0f / 362880.0f) * s + 1.0f / 40320.0f) * s - 1.0f / 5040.0f) * s + 1.0f / 720.0f) * s
-			- 1.0f / 120.0f) * s + 1.0f / 24.0f) * s - 1.0f / 6.0f) * s + 0.5f;
-	return (expm1c(-s) + s) / (s * s);
-}
-RB_D float lowerClampedCosineOverTwoPi(float s)
-{
-	const float e = expf(-s);
-	if (s <= 0.5f)
-		return e * (((((((((1.0f / 403200.0f) * s - 1.0f / 45360.0f) * s + 1.0f / 5760.0f) * s - 1.0f / 840.0f) * s
-			+ 1.0f / 144.0f) * s - 1.0f / 30.0f) * s + 1.0f / 8.0f) * s - 1.0f / 3.0f) * s + 0.5f);
-	return e * (-expm1c(-s) - s * e) / (s * s);
-}
 // SG x clamped-cosine product integral / pi (Tokuyoshi et al. 2024, Listing 7; math_util.h:508-534).
 RB_D float clampedCosineProductOverPi2024(float cosine, float s)
 {
@@ -152,8 +138,25 @@ RB_D float clampedCosineProductOverPi2024(float cosine, float s)
 	const float clampTh = 0.5f * FLT_EPSILON;
 	const float lerp = clampf(fmaxf(0.5f * (cosine * erfcApprox(-tz) + erfcApprox(t))
 		- 0.5f * invSqrtPi * expf(-tz * tz) * expm1c(t * t * (cosine * cosine - 1.0f)) / t, clampTh), 0.0f, 1.0f);
-	const float lo = lowerClampedCosineOverTwoPi(s);
-	const float up = upperClampedCosineOverTwoPi(s);
+	// LowerClampedCosineIntegralOverTwoPi(s) and
+	// UpperClampedCosineIntegralOverTwoPi(s) (math_util.h:464-506), with
+	// exp(-s) and expm1c(-s) evaluated once for both: the same operations on
+	// the same values.
+	const float e = expf(-s);
+	float lo, up;
+	if (s <= 0.5f)
+	{
+		lo = e * (((((((((1.0f / 403200.0f) * s - 1.0f / 45360.0f) * s + 1.0f / 5760.0f) * s - 1.0f / 840.0f) * s
+			+ 1.0f / 144.0f) * s - 1.0f / 30.0f) * s + 1.0f / 8.0f) * s - 1.0f / 3.0f) * s + 0.5f);
+		up = (((((((-1.0f / 362880.0f) * s + 1.0f / 40320.0f) * s - 1.0f / 5040.0f) * s + 1.0f / 720.0f) * s
+			- 1.0f / 120.0f) * s + 1.0f / 24.0f) * s - 1.0f / 6.0f) * s + 0.5f;
+	}
+	else
+	{
+		const float m = expm1cOf(-s, e);
+		lo = e * (-m - s * e) / (s * s);
+		up = (m + s) / (s * s);
+	}
 	return 2.0f * mixf(lo, up, lerp);
 }
 } // namespace sg
