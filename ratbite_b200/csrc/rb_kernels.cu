@@ -239,14 +239,31 @@ RB_D bool alphaSkipped(const DevMaterial& mat, const Qrng& q)
 	return false;
 }
 
+// Pixel (x, y) of path slot `slot` (0 .. W x H - 1) of a plane: slots run
+// over tiles of 8 x 4 pixels, so the 32 paths of a warp share a compact
+// tile (more coherent primary rays and hit points than a 32 x 1 row
+// strip), tiles row-major within bands of 4 rows. Where W or H is not a
+// multiple of the tile, the last tile of a band is narrower and the last
+// band lower. A bijection onto the pixels, so every pixel still gets
+// exactly one path per plane with the same sample sequence.
+RB_D uint2 slotPixel(uint32_t slot, uint32_t W, uint32_t H)
+{
+	const uint32_t band = slot / (4u * W);
+	const uint32_t hb = min(4u, H - 4u * band);
+	const uint32_t s = slot - band * 4u * W;
+	const uint32_t c = s / (8u * hb);
+	const uint32_t r = s - c * 8u * hb;
+	const uint32_t cw = min(8u, W - 8u * c);
+	return make_uint2(8u * c + r % cw, 4u * band + r / cw);
+}
+
 // ------------------------------------------------------------- kernels
 __global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, WaveParams w)
 {
-	const uint32_t W = sc.launch.width;
 	for (uint32_t p = gtid(); p < w.paths; p += gstride())
 	{
-		const uint32_t pix = p % w.pixels;
-		const uint32_t x = pix % W, y = pix / W;
+		const uint2 px = slotPixel(p % w.pixels, sc.launch.width, sc.launch.height);
+		const uint32_t x = px.x, y = px.y;
 		const uint32_t sample = waveSampleBase(w) + p / w.pixels;
 		const Qrng q = qrngAt(sample, pixelHash(x, y), 0);
 		const Wavelengths wl = sampleVisible(sample1D(q, DIM_WAVELENGTH));
@@ -309,8 +326,8 @@ constexpr uint32_t kSfOccluded = 1u << 3;
 
 RB_D Qrng pathQrng(const DevScene& sc, const WaveParams& w, uint32_t p, uint32_t depth)
 {
-	const uint32_t pix = p % w.pixels;
-	return qrngAt(waveSampleBase(w) + p / w.pixels, pixelHash(pix % sc.launch.width, pix / sc.launch.width), depth);
+	const uint2 px = slotPixel(p % w.pixels, sc.launch.width, sc.launch.height);
+	return qrngAt(waveSampleBase(w) + p / w.pixels, pixelHash(px.x, px.y), depth);
 }
 
 // wavelength range of the hero sampling, for the cache's normalised input
@@ -397,10 +414,10 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 			const bool prevNee = depth != 0 && !(flags & PF_PREVIOUS_HIT_SPECULAR);
 			// The light-tree pdf of an emitter hit replays ~2 SG importances
 			// per tree level; few lanes need it, so it is deferred to kEmission
-			// over a compacted queue. The sky's tree pdf is a constant.
+			// over a compacted queue. The sky's tree pdf is a constant: the
+			// environment's share, lightTreePdf's first return.
 			const bool deferTree = prevNee && it.lightType == kLightTypeTriangle;
-			const float treePdf = prevNee && !deferTree ? lightTreePdf(sc, it.lightType, it.lightIndex, rayO, lastNormal)
-				: 1.0f;
+			const float treePdf = prevNee && !deferTree ? (sc.env.enabled ? kEnvMapImportance : 0.0f) : 1.0f;
 			float lightPdf = 0.0f;
 			S4 Le = s4(0.0f);
 			bool noEmission = false;
@@ -845,12 +862,14 @@ __global__ void __launch_bounds__(kThreads) kResolve(DevScene sc, PathSoA s, Wav
 	const float* X = sc.spectra.sensor;
 	const float* Y = X + kSpectrumBins;
 	const float* Z = Y + kSpectrumBins;
-	for (uint32_t pix = gtid(); pix < w.pixels; pix += gstride())
+	for (uint32_t slot = gtid(); slot < w.pixels; slot += gstride())
 	{
+		const uint2 px = slotPixel(slot, sc.launch.width, sc.launch.height);
+		const uint32_t pix = px.y * sc.launch.width + px.x;
 		double4 acc = waveFresh(w) ? make_double4(0.0, 0.0, 0.0, 0.0) : accum[pix];
 		for (uint32_t k = 0; k < planes; ++k)
 		{
-			const uint32_t p = k * w.pixels + pix;
+			const uint32_t p = k * w.pixels + slot;
 			const uint32_t flags = s.fd[p].x;
 			if (!(flags & PF_PATH_TERMINATED) || w.keepFailed)
 			{
