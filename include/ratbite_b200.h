@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define RB_ABI_VERSION 2
+#define RB_ABI_VERSION 3
 
 /* Status codes. */
 #define RB_OK                  0

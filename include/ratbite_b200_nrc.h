@@ -104,6 +104,8 @@ typedef struct rb_cache_stats {
     float last_loss;           /* mean loss of the latest step */
     uint32_t launches;         /* this library's kernels launched for the cache */
     double ms_infer, ms_train; /* device time, with RB_STATS_TIME */
+    float drop_bias;           /* correction added to the predicted drop probability of
+                                  queries whose camera ray hit an emitter (current value) */
 } rb_cache_stats;
 /* Synchronizes, returns what was gathered since the last call, then resets. */
 int rb_get_cache_stats(rb_ctx* ctx, rb_cache_stats* out);

@@ -6,7 +6,7 @@ the sizes against the compiled library.
 """
 import ctypes as C
 
-RB_ABI_VERSION = 2
+RB_ABI_VERSION = 3
 
 RB_OK = 0
 RB_ERR_INVALID = -1
@@ -245,4 +245,5 @@ class rb_cache_params(C.Structure):
 
 class rb_cache_stats(C.Structure):
     _fields_ = [("queries", C.c_uint64), ("records", C.c_uint64), ("steps", C.c_uint64), ("last_loss", C.c_float),
-                ("launches", C.c_uint32), ("ms_infer", C.c_double), ("ms_train", C.c_double)]
+                ("launches", C.c_uint32), ("ms_infer", C.c_double), ("ms_train", C.c_double),
+                ("drop_bias", C.c_float)]

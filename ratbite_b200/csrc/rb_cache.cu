@@ -23,7 +23,7 @@ __global__ void __launch_bounds__(kThreads) kTrainTargets(PathSoA s, uint32_t ke
 	const uint32_t n = min(s.counts[kTrainRecordCount], s.trainCapacity);
 	for (uint32_t r = gtid(); r < n; r += gstride())
 	{
-		const uint32_t p = s.tPath[r];
+		const uint32_t p = s.tPath[r] & ~kLitPrefixBit;
 		if (!keepFailed && (s.fd[p].x & PF_PATH_TERMINATED))
 		{
 			s.tL[r] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(kThreads) kTrainTargets(PathSoA s, uint32_t ke
 
 // n training rows drawn uniformly (with replacement) from the wave's records:
 // inputs, and targets as rows of 8 floats (radiance, drop: 1 if the path was
-// dropped, 3 unused).
+// dropped, lit-prefix record: 1 or 0, 2 unused).
 __global__ void __launch_bounds__(kThreads) kTrainGather(PathSoA s, uint32_t keepFailed, uint32_t n, uint32_t step,
 	float* __restrict__ in, float4* __restrict__ target, uint32_t* __restrict__ valid)
 {
@@ -61,9 +61,23 @@ __global__ void __launch_bounds__(kThreads) kTrainGather(PathSoA s, uint32_t kee
 		const float* src = s.tIn + static_cast<size_t>(kNrcInputs) * r;
 		for (int k = 0; k < kNrcInputs; ++k) row[k] = src[k];
 		target[2 * j] = s.tL[r];
-		const float drop = !keepFailed && (s.fd[s.tPath[r]].x & PF_PATH_TERMINATED) ? 1.0f : 0.0f;
-		target[2 * j + 1] = make_float4(drop, 0.0f, 0.0f, 0.0f);
+		const uint32_t tp = s.tPath[r];
+		const float drop = !keepFailed && (s.fd[tp & ~kLitPrefixBit].x & PF_PATH_TERMINATED) ? 1.0f : 0.0f;
+		target[2 * j + 1] = make_float4(drop, (tp & kLitPrefixBit) ? 1.0f : 0.0f, 0.0f, 0.0f);
 	}
+}
+
+__global__ void kDropBiasUpdate(float* st)
+{
+	if (st[1] > 0.0f)
+	{
+		const float mean = st[0] / st[1];
+		const float a = fmaxf(1.0f / (st[3] + 1.0f), 0.1f);
+		st[2] += a * (mean - st[2]);
+		st[3] += 1.0f;
+	}
+	st[0] = 0.0f;
+	st[1] = 0.0f;
 }
 
 __global__ void kCacheTally(PathSoA s, unsigned long long* tally)
@@ -72,6 +86,11 @@ __global__ void kCacheTally(PathSoA s, unsigned long long* tally)
 	tally[1] += min(s.counts[kTrainRecordCount], s.trainCapacity);
 }
 } // namespace
+
+void launchDropBiasUpdate(float* state, cudaStream_t st)
+{
+	kDropBiasUpdate<<<1, 1, 0, st>>>(state);
+}
 
 void launchCacheTally(const PathSoA& s, unsigned long long* tally, cudaStream_t st)
 {

@@ -91,6 +91,7 @@ struct rb_ctx
 	float* batchTarget = nullptr;
 	uint32_t* batchValid = nullptr;
 	unsigned long long* cacheTally = nullptr;   // device: queries, records
+	float* dropBias = nullptr;                  // device: drop-bias state (launchDropBiasUpdate)
 	uint64_t cacheWaves = 0, cacheSteps = 0, cacheStepsReported = 0;
 	// replayed wave sequences (rb_render_graph): one per call shape and scene
 	// state; dyn holds the replayed call's offset and fresh flag
@@ -391,6 +392,15 @@ int rb_attach_radiance_cache(rb_ctx* ctx, rb_nrc* cache, const rb_cache_params* 
 		if (e == cudaSuccess) e = cudaMemset(ctx->cacheTally, 0, 2 * sizeof(unsigned long long));
 		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_attach_radiance_cache");
 	}
+	if (!ctx->dropBias)
+	{
+		const cudaError_t e = cudaMalloc(&ctx->dropBias, 4 * sizeof(float));
+		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_attach_radiance_cache");
+	}
+	// the drop bias is measured anew for every attached cache
+	cudaStreamSynchronize(ctx->stream);
+	if (const cudaError_t e = cudaMemset(ctx->dropBias, 0, 4 * sizeof(float)); e != cudaSuccess)
+		return cudaFail(ctx, e, "rb_attach_radiance_cache");
 	// per-path arrays are sized by the next render; batch buffers follow the new parameters
 	ctx->cache = cache;
 	ctx->cacheParams = P;
@@ -418,6 +428,8 @@ int rb_get_cache_stats(rb_ctx* ctx, rb_cache_stats* out)
 	if (ctx->cache)
 	{
 		e = cudaMemcpy(&out->last_loss, rb::nrc::lossDevice(ctx->cache), sizeof(float), cudaMemcpyDeviceToHost);
+		if (e == cudaSuccess && ctx->dropBias)
+			e = cudaMemcpy(&out->drop_bias, ctx->dropBias + 2, sizeof(float), cudaMemcpyDeviceToHost);
 		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_get_cache_stats");
 	}
 	out->steps = ctx->cacheSteps - ctx->cacheStepsReported;
@@ -472,6 +484,7 @@ int rb_destroy(rb_ctx* ctx)
 	releaseWave(ctx);
 	freeAll(ctx->cacheBufs);
 	if (ctx->cacheTally) cudaFree(ctx->cacheTally);
+	if (ctx->dropBias) cudaFree(ctx->dropBias);
 	for (const auto& t : ctx->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
 	for (cudaEvent_t e : ctx->eventPool) cudaEventDestroy(e);
 	if (ctx->counters) cudaFree(ctx->counters);
@@ -1053,7 +1066,7 @@ int renderWaves(rb_ctx* ctx, uint32_t offset, uint32_t count, cudaStream_t st, c
 			// answer the wave's cache queries, then train on its records
 			timedStage(ctx, 7, st, [&] {
 				rc = rb::nrc::applyQueries(ctx->cache, w.paths, soa.counts + rb::kCacheQueryCount, soa.cIn, soa.cPath,
-					soa.L, soa.T, st);
+					soa.L, soa.T, ctx->dropBias + 2, st);
 			});
 			if (rc != RB_OK) return fail(ctx, rc, "rb_render: cache queries");
 			if (!CP.frozen)
@@ -1067,11 +1080,12 @@ int renderWaves(rb_ctx* ctx, uint32_t offset, uint32_t count, cudaStream_t st, c
 						rb::launchTrainGather(soa, w.keepFailed, CP.batch, static_cast<uint32_t>(ctx->cacheSteps++),
 							ctx->batchIn, ctx->batchTarget, ctx->batchValid, st);
 						rc = rb::nrc::trainRows(ctx->cache, CP.batch, ctx->batchValid, ctx->batchIn, ctx->batchTarget, st,
-							true);
+							true, ctx->dropBias);
 					}
+					rb::launchDropBiasUpdate(ctx->dropBias, st);
 				});
 				if (rc != RB_OK) return fail(ctx, rc, "rb_render: cache training");
-				ctx->launches[8] += 9 * steps;   // per step: gather + 8 network kernels (cuBLAS GEMMs not counted)
+				ctx->launches[8] += 9 * steps + 1;   // per step: gather + 8 network kernels (cuBLAS GEMMs not counted); drop bias
 			}
 			rb::launchCacheTally(soa, ctx->cacheTally, st);
 			++ctx->launches[8];

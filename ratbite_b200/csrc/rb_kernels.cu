@@ -341,7 +341,7 @@ constexpr float kLambdaMin = 360.0f, kLambdaMax = 830.0f;
 // (summed spread)^2 > c a0 at a surface rough enough to cache (queued as a
 // query; returns true); a training path records the vertex (inputs,
 // radiance so far, throughput) instead.
-RB_D bool cacheVertex(const PathSoA& s, const WaveParams& w, uint32_t p, uint32_t flags, const f3& rayO,
+RB_D bool cacheVertex(const PathSoA& s, const WaveParams& w, uint32_t p, uint32_t& flags, const f3& rayO,
 	const f3& rayD, float bxdfPdf, const f3& hitPos, const f3& gn, const f3& nrm, float lambda0, bool rough)
 {
 	const f3 toHit = hitPos - rayO;
@@ -352,7 +352,8 @@ RB_D bool cacheVertex(const PathSoA& s, const WaveParams& w, uint32_t p, uint32_
 	else if (!(flags & PF_PREVIOUS_HIT_SPECULAR) && bxdfPdf > 0.0f) sp.y += sqrtf(d2 / (bxdfPdf * cosHit));
 	s.spread[p] = sp;
 	const uint32_t tr = s.trainRec[p];
-	const bool terminate = tr == kNotTraining && rough && sp.y > 0.0f && sp.y * sp.y > w.spreadC * sp.x;
+	const bool atQuery = rough && sp.y > 0.0f && sp.y * sp.y > w.spreadC * sp.x;
+	const bool terminate = tr == kNotTraining && atQuery;
 	if (tr == kNotTraining && !terminate) return false;
 	float in[kNrcInputs];
 	in[0] = (hitPos.x - w.posMin[0]) * w.posScale[0];
@@ -364,14 +365,19 @@ RB_D bool cacheVertex(const PathSoA& s, const WaveParams& w, uint32_t p, uint32_
 	if (terminate)
 	{
 		const uint32_t q = appendIndex(s.counts + kCacheQueryCount);
-		s.cPath[q] = p;
+		s.cPath[q] = p | ((flags & kPathLitPrefix) ? kLitPrefixBit : 0u);
 		for (int k = 0; k < kNrcInputs; ++k) s.cIn[static_cast<size_t>(kNrcInputs) * q + k] = in[k];
 		return true;
 	}
+	// a training path's vertex where the cache would have ended it, if the
+	// camera ray hit an emitter: the records the lit-prefix drop bias is
+	// measured on
+	const bool litRecord = atQuery && (flags & kPathLitPrefix) && !(flags & kPathQueryPassed);
+	if (atQuery) flags |= kPathQueryPassed;
 	const uint32_t r = appendIndex(s.counts + kTrainRecordCount);
 	if (r < s.trainCapacity)
 	{
-		s.tPath[r] = p;
+		s.tPath[r] = p | (litRecord ? kLitPrefixBit : 0u);
 		for (int k = 0; k < kNrcInputs; ++k) s.tIn[static_cast<size_t>(kNrcInputs) * r + k] = in[k];
 		s.tL[r] = s.L[p];
 		s.tT[r] = s.T[p];
@@ -479,6 +485,7 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 				{
 					const Surface sf = surfaceOf(mat);
 					const bool rough = (sf.metalness == 0.0f && sf.transmission == 0.0f) || sf.roughness >= w.minRoughness;
+					if (depth == 0 && it.lightType == kLightTypeTriangle) flags |= kPathLitPrefix;
 					if (cacheVertex(s, w, p, flags, rayO, rayD, bxdfPdf, it.hitPos, it.gn, lastNormal,
 							s.lambda[p].x, rough))
 					{

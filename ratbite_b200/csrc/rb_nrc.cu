@@ -310,7 +310,8 @@ constexpr int kInferMinBlocks = RB_INFER_MIN_BLOCKS;
 constexpr size_t kSmemInfer = kSmemWeights + sizeof(__nv_bfloat16) * (kInferThreads / 32) * kTile * kWStride;
 __global__ void __launch_bounds__(kInferThreads, kInferMinBlocks) kMlpInfer(uint32_t cap, const uint32_t* __restrict__ count,
 	const float* __restrict__ in, const __half2* __restrict__ grid, Resolutions R, const __nv_bfloat16* __restrict__ w,
-	float* __restrict__ out, const uint32_t* __restrict__ path, float4* __restrict__ L, const float4* __restrict__ T)
+	float* __restrict__ out, const uint32_t* __restrict__ path, float4* __restrict__ L, const float4* __restrict__ T,
+	const float* __restrict__ dropBias)
 {
 	extern __shared__ __nv_bfloat16 sw[];
 	stageWeights(w, sw);
@@ -381,10 +382,15 @@ __global__ void __launch_bounds__(kInferThreads, kInferMinBlocks) kMlpInfer(uint
 				if (path)
 				{
 					// the plain estimator drops a whole sample whose later BxDF
-					// sample fails: the prefix survives with 1 - q
-					const uint32_t p = path[rows[h]];
+					// sample fails: the prefix survives with 1 - q. A query
+					// flagged in the path index's high bit (the camera ray hit
+					// an emitter, whose radiance dominates the prefix) adds
+					// the measured bias of q on such paths.
+					const uint32_t pr = path[rows[h]];
+					const uint32_t p = pr & 0x7FFFFFFFu;
 					const float4 t = T[p];
-					const float keep = fminf(fmaxf(1.0f - q[h], 0.0f), 1.0f);
+					const float qq = q[h] + ((pr >> 31) && dropBias ? *dropBias : 0.0f);
+					const float keep = fminf(fmaxf(1.0f - qq, 0.0f), 1.0f);
 					float4 l = L[p];
 					l.x = l.x * keep + t.x * fmaxf(y[h].x, 0.0f);
 					l.y = l.y * keep + t.y * fmaxf(y[h].y, 0.0f);
@@ -404,7 +410,7 @@ __global__ void __launch_bounds__(kInferThreads, kInferMinBlocks) kMlpInfer(uint
 // others get a zero gradient).
 __global__ void kLoss(uint32_t n, const float* __restrict__ y, const float* __restrict__ t,
 	__nv_bfloat16* __restrict__ dY, float* __restrict__ lossSum, const uint32_t* __restrict__ valid, int outs,
-	int tStride)
+	int tStride, float* __restrict__ dropResid)
 {
 	float local = 0.0f;
 	const uint32_t nv = valid ? min(*valid, n) : n;
@@ -421,6 +427,13 @@ __global__ void kLoss(uint32_t n, const float* __restrict__ y, const float* __re
 				const float d = yy - tt;
 				local += d * d / den;
 				gk = 2.0f * d / den * scale;
+				// drop output of a lit-prefix row (flag after the drop target):
+				// residual of the prediction, for the renderer's bias estimate
+				if (dropResid && k == kDropOutput && t[static_cast<size_t>(tStride) * i + kDropOutput + 1] != 0.0f)
+				{
+					atomicAdd(dropResid, tt - yy);
+					atomicAdd(dropResid + 1, 1.0f);
+				}
 			}
 			dY[static_cast<size_t>(kOutPad) * i + k] = __float2bfloat16_rn(gk);
 		}
@@ -782,7 +795,7 @@ int rb_nrc_infer(rb_nrc* h, uint32_t n, const float* inputs, float* outputs, voi
 	cudaSetDevice(h->device);
 	const cudaStream_t st = static_cast<cudaStream_t>(stream);
 	kMlpInfer<<<inferBlocks(h, n), kInferThreads, kSmemInfer, st>>>(n, nullptr, inputs, reinterpret_cast<const __half2*>(h->grid),
-		h->R, h->w, outputs, nullptr, nullptr, nullptr);
+		h->R, h->w, outputs, nullptr, nullptr, nullptr, nullptr);
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
 
@@ -791,14 +804,14 @@ namespace
 // Forward, loss, backward: accumulates the batch's gradients into wGrad and
 // gridGrad (which the optimiser step or rb_nrc_gradients consume).
 int computeGradients(rb_nrc* h, uint32_t n, const float* inputs, const float* targets, cudaStream_t st,
-	const uint32_t* valid = nullptr, int outs = 4, int tStride = 4)
+	const uint32_t* valid = nullptr, int outs = 4, int tStride = 4, float* dropResid = nullptr)
 {
 	int rc = growScratch(h, n);
 	if (rc != RB_OK) return rc;
 	cudaMemsetAsync(h->loss, 0, sizeof(float), st);
 	kEncode<<<encodeBlocks(n), kThreads, 0, st>>>(n, inputs, reinterpret_cast<const __half2*>(h->grid), h->R, h->X);
 	kMlpForward<<<blocksFor(h, n), 128, kSmemWeights, st>>>(n, h->X, h->w, h->out, h->acts);
-	kLoss<<<gridFor(n), kThreads, 0, st>>>(n, h->out, targets, h->dY, h->loss, valid, outs, tStride);
+	kLoss<<<gridFor(n), kThreads, 0, st>>>(n, h->out, targets, h->dY, h->loss, valid, outs, tStride, dropResid);
 	kMlpBackward<<<blocksFor(h, n), 128, kSmemBackward, st>>>(n, h->dY, h->wt, h->acts, h->dH, h->dX0);
 	// weight gradients: dW_l[out][in] = sum over rows dY_l[r][out] X_l[r][in]
 	// (column-major view: dW^T = X^T dY with X [n][64] row-major = X^T column-major)
@@ -858,11 +871,11 @@ namespace rb
 namespace nrc
 {
 int applyQueries(rb_nrc* h, uint32_t cap, const uint32_t* count, const float* inputs, const uint32_t* path, float4* L,
-	const float4* T, cudaStream_t st)
+	const float4* T, const float* dropBias, cudaStream_t st)
 {
 	if (cap == 0) return RB_OK;
 	kMlpInfer<<<inferBlocks(h, cap), kInferThreads, kSmemInfer, st>>>(cap, count, inputs, reinterpret_cast<const __half2*>(h->grid),
-		h->R, h->w, nullptr, path, L, T);
+		h->R, h->w, nullptr, path, L, T, dropBias);
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
 
@@ -870,9 +883,9 @@ const float* lossDevice(const rb_nrc* h) { return h->loss; }
 int deviceOf(const rb_nrc* h) { return h->device; }
 
 int trainRows(rb_nrc* h, uint32_t n, const uint32_t* valid, const float* inputs, const float* targets, cudaStream_t st,
-	bool withDrop)
+	bool withDrop, float* dropResid)
 {
-	const int rc = withDrop ? computeGradients(h, n, inputs, targets, st, valid, kDropOutput + 1, 8)
+	const int rc = withDrop ? computeGradients(h, n, inputs, targets, st, valid, kDropOutput + 1, 8, dropResid)
 		: computeGradients(h, n, inputs, targets, st, valid);
 	if (rc != RB_OK) return rc;
 	++h->step;
