@@ -106,6 +106,8 @@ typedef struct rb_cache_stats {
     double ms_infer, ms_train; /* device time, with RB_STATS_TIME */
     float drop_bias;           /* correction added to the predicted drop probability of
                                   queries whose camera ray hit an emitter (current value) */
+    float drop_bias_other;     /* the same for the other queries */
+    float radiance_scale;      /* scale applied to the queries' radiance (current value) */
 } rb_cache_stats;
 /* Synchronizes, returns what was gathered since the last call, then resets. */
 int rb_get_cache_stats(rb_ctx* ctx, rb_cache_stats* out);

@@ -246,4 +246,4 @@ class rb_cache_params(C.Structure):
 class rb_cache_stats(C.Structure):
     _fields_ = [("queries", C.c_uint64), ("records", C.c_uint64), ("steps", C.c_uint64), ("last_loss", C.c_float),
                 ("launches", C.c_uint32), ("ms_infer", C.c_double), ("ms_train", C.c_double),
-                ("drop_bias", C.c_float)]
+                ("drop_bias", C.c_float), ("drop_bias_other", C.c_float), ("radiance_scale", C.c_float)]

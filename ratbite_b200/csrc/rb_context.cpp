@@ -91,7 +91,7 @@ struct rb_ctx
 	float* batchTarget = nullptr;
 	uint32_t* batchValid = nullptr;
 	unsigned long long* cacheTally = nullptr;   // device: queries, records
-	float* dropBias = nullptr;                  // device: drop-bias state (launchDropBiasUpdate)
+	float* cacheCorr = nullptr;                 // device: the cached form's correction state (rb::nrc::kCorr*)
 	uint64_t cacheWaves = 0, cacheSteps = 0, cacheStepsReported = 0;
 	// replayed wave sequences (rb_render_graph): one per call shape and scene
 	// state; dyn holds the replayed call's offset and fresh flag
@@ -392,14 +392,14 @@ int rb_attach_radiance_cache(rb_ctx* ctx, rb_nrc* cache, const rb_cache_params* 
 		if (e == cudaSuccess) e = cudaMemset(ctx->cacheTally, 0, 2 * sizeof(unsigned long long));
 		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_attach_radiance_cache");
 	}
-	if (!ctx->dropBias)
+	if (!ctx->cacheCorr)
 	{
-		const cudaError_t e = cudaMalloc(&ctx->dropBias, 4 * sizeof(float));
+		const cudaError_t e = cudaMalloc(&ctx->cacheCorr, rb::nrc::kCorrFloats * sizeof(float));
 		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_attach_radiance_cache");
 	}
-	// the drop bias is measured anew for every attached cache
+	// the corrections are measured anew for every attached cache
 	cudaStreamSynchronize(ctx->stream);
-	if (const cudaError_t e = cudaMemset(ctx->dropBias, 0, 4 * sizeof(float)); e != cudaSuccess)
+	if (const cudaError_t e = cudaMemset(ctx->cacheCorr, 0, rb::nrc::kCorrFloats * sizeof(float)); e != cudaSuccess)
 		return cudaFail(ctx, e, "rb_attach_radiance_cache");
 	// per-path arrays are sized by the next render; batch buffers follow the new parameters
 	ctx->cache = cache;
@@ -428,8 +428,12 @@ int rb_get_cache_stats(rb_ctx* ctx, rb_cache_stats* out)
 	if (ctx->cache)
 	{
 		e = cudaMemcpy(&out->last_loss, rb::nrc::lossDevice(ctx->cache), sizeof(float), cudaMemcpyDeviceToHost);
-		if (e == cudaSuccess && ctx->dropBias)
-			e = cudaMemcpy(&out->drop_bias, ctx->dropBias + 2, sizeof(float), cudaMemcpyDeviceToHost);
+		float corr[rb::nrc::kCorrFloats] = {};
+		if (e == cudaSuccess && ctx->cacheCorr)
+			e = cudaMemcpy(corr, ctx->cacheCorr, sizeof(corr), cudaMemcpyDeviceToHost);
+		out->drop_bias = corr[rb::nrc::kCorrDropLit + 2];
+		out->drop_bias_other = corr[rb::nrc::kCorrDropOther + 2];
+		out->radiance_scale = corr[rb::nrc::kCorrRadiance + 3] > 0.0f ? corr[rb::nrc::kCorrRadiance + 2] : 1.0f;
 		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_get_cache_stats");
 	}
 	out->steps = ctx->cacheSteps - ctx->cacheStepsReported;
@@ -484,7 +488,7 @@ int rb_destroy(rb_ctx* ctx)
 	releaseWave(ctx);
 	freeAll(ctx->cacheBufs);
 	if (ctx->cacheTally) cudaFree(ctx->cacheTally);
-	if (ctx->dropBias) cudaFree(ctx->dropBias);
+	if (ctx->cacheCorr) cudaFree(ctx->cacheCorr);
 	for (const auto& t : ctx->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
 	for (cudaEvent_t e : ctx->eventPool) cudaEventDestroy(e);
 	if (ctx->counters) cudaFree(ctx->counters);
@@ -1066,7 +1070,7 @@ int renderWaves(rb_ctx* ctx, uint32_t offset, uint32_t count, cudaStream_t st, c
 			// answer the wave's cache queries, then train on its records
 			timedStage(ctx, 7, st, [&] {
 				rc = rb::nrc::applyQueries(ctx->cache, w.paths, soa.counts + rb::kCacheQueryCount, soa.cIn, soa.cPath,
-					soa.L, soa.T, ctx->dropBias + 2, st);
+					soa.L, soa.T, ctx->cacheCorr, st);
 			});
 			if (rc != RB_OK) return fail(ctx, rc, "rb_render: cache queries");
 			if (!CP.frozen)
@@ -1080,12 +1084,12 @@ int renderWaves(rb_ctx* ctx, uint32_t offset, uint32_t count, cudaStream_t st, c
 						rb::launchTrainGather(soa, w.keepFailed, CP.batch, static_cast<uint32_t>(ctx->cacheSteps++),
 							ctx->batchIn, ctx->batchTarget, ctx->batchValid, st);
 						rc = rb::nrc::trainRows(ctx->cache, CP.batch, ctx->batchValid, ctx->batchIn, ctx->batchTarget, st,
-							true, ctx->dropBias);
+							true, ctx->cacheCorr);
 					}
-					rb::launchDropBiasUpdate(ctx->dropBias, st);
+					rb::launchCacheCorrectionUpdate(ctx->cacheCorr, st);
 				});
 				if (rc != RB_OK) return fail(ctx, rc, "rb_render: cache training");
-				ctx->launches[8] += 9 * steps + 1;   // per step: gather + 8 network kernels (cuBLAS GEMMs not counted); drop bias
+				ctx->launches[8] += 9 * steps + 1;   // per step: gather + 8 network kernels (cuBLAS GEMMs not counted); corrections
 			}
 			rb::launchCacheTally(soa, ctx->cacheTally, st);
 			++ctx->launches[8];

@@ -369,15 +369,16 @@ RB_D bool cacheVertex(const PathSoA& s, const WaveParams& w, uint32_t p, uint32_
 		for (int k = 0; k < kNrcInputs; ++k) s.cIn[static_cast<size_t>(kNrcInputs) * q + k] = in[k];
 		return true;
 	}
-	// a training path's vertex where the cache would have ended it, if the
-	// camera ray hit an emitter: the records the lit-prefix drop bias is
-	// measured on
-	const bool litRecord = atQuery && (flags & kPathLitPrefix) && !(flags & kPathQueryPassed);
+	// a training path's vertex where the cache would have ended it: the
+	// records the drop bias of the path's class (camera ray hit an emitter
+	// or not) is measured on
+	const bool queryRecord = atQuery && !(flags & kPathQueryPassed);
+	const uint32_t recordBits = !queryRecord ? 0u : ((flags & kPathLitPrefix) ? kLitPrefixBit : kQueryRecordBit);
 	if (atQuery) flags |= kPathQueryPassed;
 	const uint32_t r = appendIndex(s.counts + kTrainRecordCount);
 	if (r < s.trainCapacity)
 	{
-		s.tPath[r] = p | (litRecord ? kLitPrefixBit : 0u);
+		s.tPath[r] = p | recordBits;
 		for (int k = 0; k < kNrcInputs; ++k) s.tIn[static_cast<size_t>(kNrcInputs) * r + k] = in[k];
 		s.tL[r] = s.L[p];
 		s.tT[r] = s.T[p];

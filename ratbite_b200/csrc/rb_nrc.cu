@@ -311,7 +311,7 @@ constexpr size_t kSmemInfer = kSmemWeights + sizeof(__nv_bfloat16) * (kInferThre
 __global__ void __launch_bounds__(kInferThreads, kInferMinBlocks) kMlpInfer(uint32_t cap, const uint32_t* __restrict__ count,
 	const float* __restrict__ in, const __half2* __restrict__ grid, Resolutions R, const __nv_bfloat16* __restrict__ w,
 	float* __restrict__ out, const uint32_t* __restrict__ path, float4* __restrict__ L, const float4* __restrict__ T,
-	const float* __restrict__ dropBias)
+	const float* __restrict__ corr)
 {
 	extern __shared__ __nv_bfloat16 sw[];
 	stageWeights(w, sw);
@@ -382,20 +382,22 @@ __global__ void __launch_bounds__(kInferThreads, kInferMinBlocks) kMlpInfer(uint
 				if (path)
 				{
 					// the plain estimator drops a whole sample whose later BxDF
-					// sample fails: the prefix survives with 1 - q. A query
-					// flagged in the path index's high bit (the camera ray hit
-					// an emitter, whose radiance dominates the prefix) adds
-					// the measured bias of q on such paths.
+					// sample fails: the prefix survives with 1 - q, q plus the
+					// correction measured on the path's class (the path
+					// index's high bit: the camera ray hit an emitter, whose
+					// radiance dominates the prefix); the radiance is scaled
+					// by the measured ratio of targets to predictions
 					const uint32_t pr = path[rows[h]];
 					const uint32_t p = pr & 0x7FFFFFFFu;
 					const float4 t = T[p];
-					const float qq = q[h] + ((pr >> 31) && dropBias ? *dropBias : 0.0f);
+					const float qq = q[h] + (corr ? corr[((pr >> 31) ? kCorrDropLit : kCorrDropOther) + 2] : 0.0f);
 					const float keep = fminf(fmaxf(1.0f - qq, 0.0f), 1.0f);
+					const float sc = corr && corr[kCorrRadiance + 3] > 0.0f ? corr[kCorrRadiance + 2] : 1.0f;
 					float4 l = L[p];
-					l.x = l.x * keep + t.x * fmaxf(y[h].x, 0.0f);
-					l.y = l.y * keep + t.y * fmaxf(y[h].y, 0.0f);
-					l.z = l.z * keep + t.z * fmaxf(y[h].z, 0.0f);
-					l.w = l.w * keep + t.w * fmaxf(y[h].w, 0.0f);
+					l.x = l.x * keep + t.x * (sc * fmaxf(y[h].x, 0.0f));
+					l.y = l.y * keep + t.y * (sc * fmaxf(y[h].y, 0.0f));
+					l.z = l.z * keep + t.z * (sc * fmaxf(y[h].z, 0.0f));
+					l.w = l.w * keep + t.w * (sc * fmaxf(y[h].w, 0.0f));
 					L[p] = l;
 				}
 			}
@@ -410,9 +412,13 @@ __global__ void __launch_bounds__(kInferThreads, kInferMinBlocks) kMlpInfer(uint
 // others get a zero gradient).
 __global__ void kLoss(uint32_t n, const float* __restrict__ y, const float* __restrict__ t,
 	__nv_bfloat16* __restrict__ dY, float* __restrict__ lossSum, const uint32_t* __restrict__ valid, int outs,
-	int tStride, float* __restrict__ dropResid)
+	int tStride, float* __restrict__ corr)
 {
 	float local = 0.0f;
+	// sums of the renderer's correction state over this thread's rows of a
+	// class (1, 2): drop residual and count per class, radiance targets and
+	// clamped predictions
+	float cs[6] = { 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f };
 	const uint32_t nv = valid ? min(*valid, n) : n;
 	const float scale = nv ? 1.0f / static_cast<float>(nv) : 0.0f;
 	for (uint32_t i = gtid(); i < n; i += gstride())
@@ -427,12 +433,19 @@ __global__ void kLoss(uint32_t n, const float* __restrict__ y, const float* __re
 				const float d = yy - tt;
 				local += d * d / den;
 				gk = 2.0f * d / den * scale;
-				// drop output of a lit-prefix row (flag after the drop target):
-				// residual of the prediction, for the renderer's bias estimate
-				if (dropResid && k == kDropOutput && t[static_cast<size_t>(tStride) * i + kDropOutput + 1] != 0.0f)
+				const float cls = corr && outs > kDropOutput ? t[static_cast<size_t>(tStride) * i + kDropOutput + 1] : 0.0f;
+				if (cls != 0.0f)
 				{
-					atomicAdd(dropResid, tt - yy);
-					atomicAdd(dropResid + 1, 1.0f);
+					if (k == kDropOutput)
+					{
+						cs[cls == 1.0f ? 0 : 2] += tt - yy;
+						cs[cls == 1.0f ? 1 : 3] += 1.0f;
+					}
+					else
+					{
+						cs[4] += tt;
+						cs[5] += fmaxf(yy, 0.0f);
+					}
 				}
 			}
 			dY[static_cast<size_t>(kOutPad) * i + k] = __float2bfloat16_rn(gk);
@@ -440,6 +453,18 @@ __global__ void kLoss(uint32_t n, const float* __restrict__ y, const float* __re
 	}
 	for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xFFFFFFFFu, local, o);
 	if ((threadIdx.x & 31u) == 0) atomicAdd(lossSum, local * scale);
+	if (corr)
+	{
+		const int slot[6] = { kCorrDropLit, kCorrDropLit + 1, kCorrDropOther, kCorrDropOther + 1, kCorrRadiance,
+			kCorrRadiance + 1 };
+#pragma unroll
+		for (int j = 0; j < 6; ++j)
+		{
+			float v = cs[j];
+			for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+			if ((threadIdx.x & 31u) == 0 && v != 0.0f) atomicAdd(corr + slot[j], v);
+		}
+	}
 }
 
 // Backward through the layers on 16-row tiles: with the transposed weights
@@ -804,14 +829,14 @@ namespace
 // Forward, loss, backward: accumulates the batch's gradients into wGrad and
 // gridGrad (which the optimiser step or rb_nrc_gradients consume).
 int computeGradients(rb_nrc* h, uint32_t n, const float* inputs, const float* targets, cudaStream_t st,
-	const uint32_t* valid = nullptr, int outs = 4, int tStride = 4, float* dropResid = nullptr)
+	const uint32_t* valid = nullptr, int outs = 4, int tStride = 4, float* corr = nullptr)
 {
 	int rc = growScratch(h, n);
 	if (rc != RB_OK) return rc;
 	cudaMemsetAsync(h->loss, 0, sizeof(float), st);
 	kEncode<<<encodeBlocks(n), kThreads, 0, st>>>(n, inputs, reinterpret_cast<const __half2*>(h->grid), h->R, h->X);
 	kMlpForward<<<blocksFor(h, n), 128, kSmemWeights, st>>>(n, h->X, h->w, h->out, h->acts);
-	kLoss<<<gridFor(n), kThreads, 0, st>>>(n, h->out, targets, h->dY, h->loss, valid, outs, tStride, dropResid);
+	kLoss<<<gridFor(n), kThreads, 0, st>>>(n, h->out, targets, h->dY, h->loss, valid, outs, tStride, corr);
 	kMlpBackward<<<blocksFor(h, n), 128, kSmemBackward, st>>>(n, h->dY, h->wt, h->acts, h->dH, h->dX0);
 	// weight gradients: dW_l[out][in] = sum over rows dY_l[r][out] X_l[r][in]
 	// (column-major view: dW^T = X^T dY with X [n][64] row-major = X^T column-major)
@@ -871,11 +896,11 @@ namespace rb
 namespace nrc
 {
 int applyQueries(rb_nrc* h, uint32_t cap, const uint32_t* count, const float* inputs, const uint32_t* path, float4* L,
-	const float4* T, const float* dropBias, cudaStream_t st)
+	const float4* T, const float* corr, cudaStream_t st)
 {
 	if (cap == 0) return RB_OK;
 	kMlpInfer<<<inferBlocks(h, cap), kInferThreads, kSmemInfer, st>>>(cap, count, inputs, reinterpret_cast<const __half2*>(h->grid),
-		h->R, h->w, nullptr, path, L, T, dropBias);
+		h->R, h->w, nullptr, path, L, T, corr);
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
 
@@ -883,9 +908,9 @@ const float* lossDevice(const rb_nrc* h) { return h->loss; }
 int deviceOf(const rb_nrc* h) { return h->device; }
 
 int trainRows(rb_nrc* h, uint32_t n, const uint32_t* valid, const float* inputs, const float* targets, cudaStream_t st,
-	bool withDrop, float* dropResid)
+	bool withDrop, float* corr)
 {
-	const int rc = withDrop ? computeGradients(h, n, inputs, targets, st, valid, kDropOutput + 1, 8, dropResid)
+	const int rc = withDrop ? computeGradients(h, n, inputs, targets, st, valid, kDropOutput + 1, 8, corr)
 		: computeGradients(h, n, inputs, targets, st, valid);
 	if (rc != RB_OK) return rc;
 	++h->step;

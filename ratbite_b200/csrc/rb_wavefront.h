@@ -70,10 +70,13 @@ constexpr uint32_t kNoRecord = 0xFFFFFFFEu;
 // has passed the vertex where the cache would have ended it.
 constexpr uint32_t kPathLitPrefix = 1u << 16;
 constexpr uint32_t kPathQueryPassed = 1u << 17;
-// High bit of a query's path index (cPath): a lit-prefix path's query; of a
-// record's (tPath): a training record at the vertex where a lit-prefix
-// path would have queried the cache.
+// High bits of a query's path index (cPath): bit 31, a lit-prefix path's
+// query. Of a record's (tPath): bit 31, a training record at the vertex
+// where a lit-prefix path would have queried the cache; bit 30, the same
+// for any other path. Path indices stay below 2^30.
 constexpr uint32_t kLitPrefixBit = 1u << 31;
+constexpr uint32_t kQueryRecordBit = 1u << 30;
+constexpr uint32_t kRecordPathMask = kQueryRecordBit - 1u;
 constexpr int kMaxBounces = 64;
 // counts[b]: paths entering bounce b; counts[kShadowCounts + b]: shadow rays
 // of bounce b; counts[kSurfaceCounts + b]: surface records of bounce b;
@@ -172,13 +175,10 @@ void launchTrainTargets(const PathSoA& s, uint32_t keepFailed, int smCount, cuda
 void launchTrainGather(const PathSoA& s, uint32_t keepFailed, uint32_t n, uint32_t step, float* in, float* target,
 	uint32_t* valid, cudaStream_t st);
 // tally[0] += queries, tally[1] += training records of the wave.
-// Drop-bias state of the cached form, 4 floats: [0] sum and [1] count of
-// (drop target - predicted drop probability) over the lit-prefix training
-// rows of the wave's optimiser steps, [2] the bias added to the predicted
-// drop probability of lit-prefix queries, [3] waves seen. The update folds
-// the wave's mean residual into [2] (running mean over the first 10 waves,
-// then an exponential average with weight 0.1) and clears [0], [1].
-void launchDropBiasUpdate(float* state, cudaStream_t st);
+// Folds the wave's sums of the cached form's correction state
+// (rb::nrc::kCorr* layout, rb_nrc_internal.h) into its corrections and
+// clears the sums.
+void launchCacheCorrectionUpdate(float* state, cudaStream_t st);
 void launchCacheTally(const PathSoA& s, unsigned long long* tally, cudaStream_t st);
 
 // Per-function batch kernels (include/ratbite_b200_kernels.h).

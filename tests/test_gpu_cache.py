@@ -12,9 +12,13 @@ their vertices, and the optimiser steps the wave feeds.
    than the trained one: the gain comes from what the network learned.
 3. The cached form is close to unbiased against the plain estimator: after
    training, the mean of the image matches the reference's within 5 %
-   (measured -0.2 % to -2.8 % over runs: the training's float atomics make
-   each run's trajectory differ). An untrained cache is +43 % off, and a
-   cache that ignored the reference's dropped samples was +7 % off.
+   (measured +0.5 % with the drop and radiance corrections, -0.2 % to
+   -2.8 % before them; the training's float atomics make each run's
+   trajectory differ). An untrained cache is +43 % off, and a cache that
+   ignored the reference's dropped samples was +7 % off.
+4. The corrections measured on the training rows at the would-be query
+   vertex are in use after training: a finite drop-probability correction
+   per class and a radiance scale within its [0.5, 2] clamp.
 """
 from __future__ import annotations
 
@@ -108,6 +112,8 @@ def test_trained_cache_reduces_error_at_equal_samples(setup):
           f"loss {warm.last_loss:.4f} after {warm.steps} steps")
     assert np.all(np.isfinite(img)) and ri.status().flags == 0
     assert warm.steps == 256 and st.steps == spp and st.queries > W * H
+    assert np.isfinite(st.drop_bias) and np.isfinite(st.drop_bias_other) and abs(st.drop_bias_other) < 0.5
+    assert 0.5 <= st.radiance_scale <= 2.0 and st.radiance_scale != 1.0
     assert cached < 0.9 * plain
     assert cached < cold
     assert abs(bias) < 0.05
