@@ -86,6 +86,16 @@ def test_one_pixel_film_and_depth_one(tables):
     assert l1 < 1e-4
 
 
+@pytest.mark.parametrize("W,H", [(13, 9), (7, 3), (17, 2), (9, 5)])
+def test_films_that_are_not_whole_tiles(tables, W, H):
+    # path slots run over 8 x 4 pixel tiles; at sizes that are not multiples
+    # of the tile every pixel still gets its own samples (the oracle's per
+    # pixel counts and values)
+    sc = scenes.cornell_box(seed=1, width=W, height=H, spp=4)
+    g, w, l1 = _compare(tables, sc, W, H, 4)
+    assert l1 < 1e-4
+
+
 def test_degenerate_triangles_are_skipped(tables):
     sc = scenes.cornell_box(seed=1, width=24, height=24, spp=4)
     sc = copy.copy(sc)
