@@ -74,6 +74,22 @@ def test_abi_record_sizes(tmp_path):
     assert sizes == ours
 
 
+def test_abi_cache_record_layouts(tmp_path):
+    # the radiance-cache records: sizes and the offsets of the fields added last
+    src = tmp_path / "abi_nrc.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "ratbite_b200.h"\n#include "ratbite_b200_nrc.h"\n'
+                   'int main(){printf("%zu %zu %zu %zu %zu %zu %zu\\n",sizeof(rb_progress),sizeof(rb_nrc_config),'
+                   'sizeof(rb_cache_params),sizeof(rb_cache_stats),offsetof(rb_cache_stats,drop_bias),'
+                   'offsetof(rb_cache_stats,drop_bias_other),offsetof(rb_cache_stats,radiance_scale));}\n')
+    exe = src.with_suffix("")
+    subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    sizes = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    ours = [C.sizeof(abi.rb_progress), C.sizeof(abi.rb_nrc_config), C.sizeof(abi.rb_cache_params),
+            C.sizeof(abi.rb_cache_stats), abi.rb_cache_stats.drop_bias.offset, abi.rb_cache_stats.drop_bias_other.offset,
+            abi.rb_cache_stats.radiance_scale.offset]
+    assert sizes == ours
+
+
 # --------------------------------------------------------------- oracle
 @pytest.fixture(scope="module")
 def ref():
