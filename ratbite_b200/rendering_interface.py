@@ -243,6 +243,12 @@ class RenderingInterface:
         self._cache = cache   # the cache must outlive the attachment
 
     def cache_stats(self) -> abi.rb_cache_stats:
+        """What the cached form gathered since the last call (queries,
+        training records, optimiser steps, latest loss, launches, stage times)
+        and the corrections it currently applies: drop_bias and
+        drop_bias_other (added to the predicted drop probability of queries
+        whose camera ray hit an emitter, and of the others) and
+        radiance_scale. Synchronizes; the counters restart."""
         st = abi.rb_cache_stats()
         check(self.lib.rb_get_cache_stats(self.ctx, C.byref(st)), self.ctx, "rb_get_cache_stats")
         return st
