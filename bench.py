@@ -65,8 +65,8 @@ WORKLOADS = {
 # state it must stream in and out, plus the per-unit gathers from tables
 # larger than L2. Tables that stay cache-resident (materials, LUTs, spectra,
 # light-tree nodes, emitter records, the env-map CDF) are not counted.
-#   extend  per ray: queue slot 4, ray o/d 32, hit written 16; nodes (96 B)
-#           and triangles (48 B) per visit, counted from the traversal counters
+#   extend  per ray: 32 B ray in + 32 B hit out, plus 80 B per 8-wide node
+#           and 48 B per triangle visited (counted by the traversal counters)
 #   shadow  per ray: queue 4, shadow o/d 32, L read+write 32 when unoccluded
 #           (counted as always), pending contribution 16, plus visits as extend
 #   surface per path entering the bounce: queue 4, ray o/d 32, normal 16,
@@ -79,13 +79,13 @@ WORKLOADS = {
 #           o/d 32, normal 16, flags 8, wavelengths + pdfs + throughput 48,
 #           light sample 32 read; throughput, flags, ray o/d 56, contribution
 #           16 and two queue slots 8 written
-EXTEND_BYTES_PER_RAY = 4 + 32 + 16
+EXTEND_BYTES_PER_RAY = 32 + 32
 SHADOW_BYTES_PER_RAY = 4 + 32 + 32 + 16
 SURFACE_BYTES_PER_PATH = 4 + 32 + 16 + 8 + 16 + 56
 SURFACE_BYTES_PER_RECORD = 12 + 48 + 80 + 16 + 8 + 4
 NEE_BYTES_PER_RECORD = 4 + 48 + 16 + 8 + 16 + 16 + 48
 BSDF_BYTES_PER_RECORD = 4 + 80 + 32 + 16 + 8 + 48 + 32 + 56 + 16 + 8
-NODE_BYTES, TRI_BYTES = 96, 48
+NODE_BYTES, TRI_BYTES = 80, 48
 
 
 def peaks():
@@ -148,20 +148,50 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def bench_tables():
+    """CIE curves, RGB basis and multiple-scattering LUTs that both arms
+    render with: the reference's own (its bin/*.bin LUT files, and its
+    spectral tables from src/core/spectral.cpp, written as data by the oracle
+    build into oracle/_ref/bin/spectra.npz), read as plain files so that no
+    library is loaded for them. Without the oracle build, the built-in
+    stand-ins of ratbite_b200.assets."""
+    d = ROOT / "oracle" / "_ref" / "bin"
+    names = dict(conductor="albedoConductorLUT.bin", dielectric_outer="albedoDielectricOuterLUT.bin",
+                 dielectric_inner="albedoDielectricInnerLUT.bin",
+                 reflective_outer="albedoDielectricReflectiveOuterLUT.bin",
+                 reflective_inner="albedoDielectricReflectiveInnerLUT.bin", sheen="sheenLUT.bin")
+    if (d / "spectra.npz").exists() and all((d / f).exists() for f in names.values()):
+        sp = np.load(d / "spectra.npz")
+        luts = {k: np.fromfile(d / f, dtype=np.float32) for k, f in names.items()}
+        return sp["cie_xyz"], sp["basis_rgb"], luts, "reference (bin/*.bin LUTs, src/core/spectral.cpp curves)"
+    from ratbite_b200 import assets
+    return assets.cie_xyz(), assets.basis_rgb(), assets.luts(), "built-in stand-ins (ratbite_b200.assets)"
+
+
 def make_scene(wl: dict):
-    from ratbite_b200 import assets, scenes
-    cie = assets.cie_xyz()
-    basis = assets.basis_rgb()
-    # compensation tables regenerated on the GPU (rb_k_generate_luts: they
-    # match the reference's bin/*.bin to Monte Carlo noise); sheen: stand-in
-    luts = assets.generated_luts(samples=1 << 14)
+    from ratbite_b200 import scenes
+    cie, basis, luts, tables = bench_tables()
     if wl["name"].startswith("cornell"):
         scene = scenes.cornell_box(seed=1, cie_xyz=cie, width=wl["width"], height=wl["height"], spp=wl["spp"],
                                    max_depth=wl["depth"])
     else:
         scene = scenes.scale_scene(seed=3, width=wl["width"], height=wl["height"], spp=wl["spp"],
                                    max_depth=wl["depth"])
-    return scene, cie, basis, luts
+    return scene, cie, basis, luts, tables
+
+
+def workload_config(scene, wl: dict, world: int, tables: str) -> dict:
+    """The `config` object of both arms' lines (identical for the same
+    workload)."""
+    has_env = getattr(scene, "envmap", None) is not None
+    return {"workload": wl["name"], "width": wl["width"], "height": wl["height"], "spp": wl["spp"],
+            "max_depth": wl["depth"], "triangles": scene.triangle_count(),
+            "emitters": int(sum(len(e["prim"]) for e in scene.emissive)), "materials": len(scene.materials),
+            "envmap": list(scene.envmap.shape[1::-1]) if has_env else None,
+            "paths_per_step": wl["width"] * wl["height"] * wl["spp"] * world,
+            "parallelism": f"sample-range x{world}", "tables": tables,
+            "l2": "inputs larger than L2 (wavefront path state 344 B per path in flight, "
+                  "~5.8 GB at the default 16M paths per wave)"}
 
 
 # ------------------------------------------------------------- CPU baseline
@@ -173,58 +203,73 @@ def _ref_setup(scene, cie, basis, luts):
     return ref, keep
 
 
-def _calibrate(ref, wl, cores, target_s):
-    """Rows x spp of a band that takes about target_s on `cores` threads."""
+def _strided_sample(ref, wl, cores, target_s):
+    """A bounded CPU sample of the frame with the frame's cost mix: every
+    stride-th row from top to bottom (all columns), at spp samples per pixel
+    (sample indices 0..spp-1), sized to take about target_s on `cores`
+    threads. Returns (first_row, stride, spp)."""
     W, H = wl["width"], wl["height"]
-    rows = min(H, 8)
+    probe_stride = max(1, H // 16)
     t0 = time.perf_counter()
-    ref.lib.rbref_render_rows(0, 1, cores, 0, rows)
+    px = ref.lib.rbref_render_strided(0, 1, cores, probe_stride // 2, probe_stride)
     dt = max(time.perf_counter() - t0, 1e-3)
-    per_row_spp = dt / rows
-    budget_rows_spp = max(1.0, target_s / per_row_spp)
-    spp = int(min(wl["spp"], max(1, budget_rows_spp // H)))
-    rows = int(min(H, max(1, budget_rows_spp // spp)))
-    return rows, spp
+    assert px > 0, px
+    budget = max(1.0, target_s * px / dt)            # pixel-samples that fit in target_s
+    rows_full = H
+    spp = int(min(wl["spp"], max(1, budget // (64 * W))))  # at least 64 rows
+    rows = int(min(rows_full, max(1, budget // (spp * W))))
+    stride = max(1, H // rows)
+    return stride // 2, stride, spp
+
+
+def _render_sample(ref, cores, first, stride, spp):
+    px = ref.lib.rbref_render_strided(0, spp, cores, first, stride)
+    assert px > 0, px
+    return px * spp
+
+
+def _sample_text(wl, first, stride, spp, steps=None):
+    rows = len(range(first, wl["height"], stride))
+    s = (f"{wl['width']}x{rows} rows (every {stride}th row from row {first}, spread over the whole frame) "
+         f"at {spp} spp")
+    return s + (f" per step, {steps} steps" if steps else "")
 
 
 def cpu_baseline(scene, cie, basis, luts, wl, target_s):
     ref, keep = _ref_setup(scene, cie, basis, luts)
     cores = os.cpu_count() or 1
-    rows, spp = _calibrate(ref, wl, cores, target_s)
-    r0 = (wl["height"] - rows) // 2
+    first, stride, spp = _strided_sample(ref, wl, cores, target_s)
     t0 = time.perf_counter()
-    ref.lib.rbref_render_rows(0, spp, cores, r0, r0 + rows)
+    paths = _render_sample(ref, cores, first, stride, spp)
     dt = time.perf_counter() - t0
-    paths = wl["width"] * rows * spp
     del keep
-    return paths / dt, cores, f"{wl['width']}x{rows} rows (centre band) at {spp} spp: {paths} paths in {dt:.2f} s"
+    return paths / dt, cores, _sample_text(wl, first, stride, spp) + f": {paths} paths in {dt:.2f} s"
 
 
 # ----------------------------------------------------------- reference arm
 def run_reference(args, rank: int, world: int, wl: dict):
     if rank != 0:
         return
-    scene, cie, basis, luts = make_scene(wl)
+    scene, cie, basis, luts, tables = make_scene(wl)
     ref, keep = _ref_setup(scene, cie, basis, luts)
     cores = os.cpu_count() or 1
-    rows, spp = _calibrate(ref, wl, cores, args.ref_step_s)
-    r0 = (wl["height"] - rows) // 2
+    first, stride, spp = _strided_sample(ref, wl, cores, args.ref_step_s)
     for _ in range(args.warmup):
-        ref.lib.rbref_render_rows(0, spp, cores, r0, r0 + rows)
+        _render_sample(ref, cores, first, stride, spp)
     t0 = time.perf_counter()
+    paths = 0
     for _ in range(args.steps):
-        ref.lib.rbref_render_rows(0, spp, cores, r0, r0 + rows)
+        paths += _render_sample(ref, cores, first, stride, spp)
     dt = time.perf_counter() - t0
-    paths = wl["width"] * rows * spp * args.steps
     v = paths / dt
-    sample = f"{wl['width']}x{rows} rows (centre band) at {spp} spp per step, {args.steps} steps"
+    sample = _sample_text(wl, first, stride, spp, args.steps)
     line = {
         "metric": METRIC, "value": v, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
         "impl": "reference",
-        "config": {"workload": wl["name"], "width": wl["width"], "height": wl["height"], "spp": wl["spp"],
-                   "max_depth": wl["depth"], "triangles": scene.triangle_count(), "sample_per_step": sample},
+        "config": workload_config(scene, wl, world, tables),
+        "sample_per_step": sample,
         "cpu_baseline": {"value": v, "unit": "paths/s", "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -249,7 +294,7 @@ def run_ours(args, rank: int, world: int, wl: dict):
                                 device_id=torch.device("cuda", local))
 
     t_setup = time.perf_counter()
-    scene, cie, basis, luts = make_scene(wl)
+    scene, cie, basis, luts, tables = make_scene(wl)
     lt = lighttree.build_for_scene(scene)
     ri = RenderingInterface(device=local, max_paths_in_flight=args.max_paths)
     ri.load_scene(scene, luts, cie, basis, light_tree=lt)
@@ -379,6 +424,9 @@ def run_ours(args, rank: int, world: int, wl: dict):
             cpu_v, cores, sample = cpu_baseline(scene, cie, basis, luts, wl, args.cpu_seconds)
         else:
             cpu_v, cores, sample = None, 0, "skipped"
+        rows = None
+        if world == 1 and has_env and args.rows:
+            rows = reference_kernel_rows(scene.envmap, ri.accumulation_device_ptr(), W, H)
         ttr = None
         if args.ttr and world == 1 and args.workload == "scale":
             ri.cleanup()                     # free this workload's wave before the second one
@@ -387,13 +435,8 @@ def run_ours(args, rank: int, world: int, wl: dict):
             "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": {"workload": wl["name"], "width": W, "height": H, "spp": SPP, "max_depth": wl["depth"],
-                       "triangles": scene.triangle_count(), "emitters": int(sum(len(e["prim"]) for e in scene.emissive)),
-                       "materials": len(scene.materials), "envmap": list(scene.envmap.shape[1::-1]) if has_env else None,
-                       "paths_per_step": paths_per_step, "parallelism": f"sample-range x{world}",
-                       "l2": "inputs larger than L2 (wavefront path state 344 B per path in flight, "
-                             "~5.8 GB at the default 16M paths per wave)",
-                       "setup_s": setup_s},
+            "config": workload_config(scene, wl, world, tables),
+            "setup_s": setup_s,
             "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": C.sizeof(launch),
                     "d2h_bytes_per_step": W * H * 32, "steps": e2e_steps},
             "gpu_launches": int(launches_total),
@@ -417,6 +460,7 @@ def run_ours(args, rank: int, world: int, wl: dict):
             "cpu_baseline": {"value": cpu_v, "unit": "paths/s", "cores": cores, "kind": "reference",
                              "sample": sample},
             "time_to_rmse": ttr,
+            "reference_kernels": rows,
         }
         print(json.dumps(line), flush=True)
     ri.cleanup()
@@ -425,6 +469,94 @@ def run_ours(args, rank: int, world: int, wl: dict):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def reference_kernel_rows(envmap: np.ndarray, accum_ptr: int, width: int, height: int, iters: int = 20):
+    """The two rows whose reference implementation is itself a CUDA kernel,
+    timed head to head on this GPU: the env-map CDF build (ours:
+    rb_envmap_cdf, one fused kernel; the reference: buildCDFLatLongRGB* +
+    invertCDFToIndices of src/kernels/cdf.cu compiled for sm_100a and
+    launched as loadEnvironmentMap does, src/core/rendering_interface.cpp:
+    1374-1419) and the resolve (ours: rb_k_resolve; the reference:
+    renderResolve of src/kernels/image.cu with 16x16 blocks,
+    src/core/rendering_interface.cpp:1512-1532). Each launch is timed alone
+    with CUDA events after overwriting a 512 MiB buffer (L2 is 126 MB), so the
+    inputs come from HBM. Algorithmic bytes: CDF 16 B read + 2 B written per
+    texel plus 2 B per row (9.0 MiB at 1024x512); resolve 32 B read + 4 B
+    written per pixel."""
+    import torch
+    from ratbite_b200 import abi, color
+    from ratbite_b200._native import check, load
+    ref_dir = ROOT / "oracle" / "_ref"
+    lib = load()
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    p = lambda t: C.c_void_p(t.data_ptr())
+
+    def timed(fn):
+        total = 0.0
+        for i in range(iters + 3):
+            flush.fill_(i & 0xFF)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            if i >= 3:
+                total += a.elapsed_time(b)
+        return total / iters
+
+    out = {}
+    h, w = envmap.shape[:2]
+    img = torch.from_numpy(np.ascontiguousarray(envmap, np.float32)).cuda()
+    scratch = torch.zeros(int(lib.rb_envmap_cdf_scratch_bytes(w, h)), dtype=torch.uint8, device="cuda")
+    cond = torch.zeros(w * h, dtype=torch.int16, device="cuda")
+    marg = torch.zeros(h, dtype=torch.int16, device="cuda")
+    integ = torch.zeros(1, dtype=torch.float32, device="cuda")
+    cdf_bytes = w * h * 18 + h * 2
+    for mode, name in ((abi.RB_CDF_REFERENCE, "ours_mode0_f32_ms"), (abi.RB_CDF_FP64, "ours_mode1_f64_ms")):
+        out[name] = timed(lambda: check(lib.rb_envmap_cdf(w, h, p(img), mode, p(scratch), p(cond), p(marg),
+                                                          p(integ), sp), None, "rb_envmap_cdf"))
+    ref_ms = None
+    if (ref_dir / "libratbite_ref_cdf.so").exists():
+        rl = C.CDLL(str(ref_dir / "libratbite_ref_cdf.so"))
+        rl.rbrefgpu_envmap_cdf_time.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_int, C.c_int, C.c_void_p, C.c_size_t]
+        rl.rbrefgpu_envmap_cdf_time.restype = C.c_float
+        torch.cuda.synchronize()
+        ref_ms = float(rl.rbrefgpu_envmap_cdf_time(str(ref_dir / "cdf.cubin").encode(), w, h, p(img), p(cond),
+                                                   p(marg), 3, iters, p(flush), flush.numel()))
+    out["reference_ms"] = ref_ms
+    out["bytes"] = cdf_bytes
+    out["ours_mode1_gbs"] = cdf_bytes / (out["ours_mode1_f64_ms"] / 1e3) / 1e9
+    out["ours_mode0_gbs"] = cdf_bytes / (out["ours_mode0_f32_ms"] / 1e3) / 1e9
+    out["reference_gbs"] = cdf_bytes / (ref_ms / 1e3) / 1e9 if ref_ms and ref_ms > 0 else None
+    rows = {"envmap_cdf": dict(out, size=[w, h])}
+
+    cs = np.ascontiguousarray(color.colorspace_matrix("sRGB"), np.float32).ravel()
+    scale = float(2.0 ** (0.0 - 7.0))
+    rgba = torch.zeros((height, width, 4), dtype=torch.uint8, device="cuda")
+    res = {"ours_ms": timed(lambda: check(lib.rb_k_resolve(width, height, cs.ctypes.data, scale,
+                                                           C.c_void_p(accum_ptr), p(rgba), sp), None,
+                                          "rb_k_resolve"))}
+    ref_ms = None
+    if (ref_dir / "libratbite_ref_image.so").exists():
+        rl = C.CDLL(str(ref_dir / "libratbite_ref_image.so"))
+        rl.rbrefgpu_resolve_time.argtypes = [C.c_char_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_float, C.c_void_p,
+                                             C.c_int, C.c_int, C.c_void_p, C.c_size_t]
+        rl.rbrefgpu_resolve_time.restype = C.c_float
+        torch.cuda.synchronize()
+        ref_ms = float(rl.rbrefgpu_resolve_time(str(ref_dir / "image.cubin").encode(), width, height,
+                                                cs.ctypes.data, scale, C.c_void_p(accum_ptr), 3, iters, p(flush),
+                                                flush.numel()))
+    rbytes = width * height * 36
+    res.update(reference_ms=ref_ms, bytes=rbytes, size=[width, height],
+               ours_gbs=rbytes / (res["ours_ms"] / 1e3) / 1e9,
+               reference_gbs=rbytes / (ref_ms / 1e3) / 1e9 if ref_ms and ref_ms > 0 else None)
+    rows["resolve"] = res
+    del flush
+    return rows
 
 
 def run_batched(args):
@@ -478,11 +610,11 @@ def time_to_rmse(device: int = 0, width: int = 1920, height: int = 1080, depth: 
     from an untrained cache and stops at the target or at time_factor x the
     plain tracer's time."""
     import torch
-    from ratbite_b200 import assets, lighttree, scenes
+    from ratbite_b200 import lighttree, scenes
     from ratbite_b200.nrc import RadianceCache
     from ratbite_b200.rendering_interface import RenderingInterface
 
-    cie, basis, luts = assets.cie_xyz(), assets.basis_rgb(), assets.generated_luts(samples=1 << 14, device=device)
+    cie, basis, luts, _ = bench_tables()
     scene = scenes.cornell_box(seed=1, cie_xyz=cie, width=width, height=height, spp=plain_spp, max_depth=depth)
     lt = lighttree.build_for_scene(scene)
     ri = RenderingInterface(device=device, failed_sample_mode=failed_mode)
@@ -570,6 +702,9 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0 = the workload's)")
     ap.add_argument("--no-ttr", dest="ttr", action="store_false",
                     help="skip the time-to-RMSE measurement of the cached form (1920x1080 Cornell box, ~30 s)")
+    ap.add_argument("--no-rows", dest="rows", action="store_false",
+                    help="skip the head-to-head timing of the env-map CDF and resolve kernels against the "
+                         "reference's own CUDA kernels")
     ap.add_argument("--max-paths", type=int, default=0,
                     help="paths in flight per wave (0 = the library default, 16M); small values make profiling "
                          "captures small")

@@ -118,7 +118,9 @@ int rb_k_resolve(uint32_t width, uint32_t height, const float* colorspace, float
  * loadEnvironmentMap stores them (src/core/rendering_interface.cpp:1404-1431).
  * mode 0 = float32 sums in the reference's scan order (bit-exact indices),
  * mode 1 = float64 row/column sums. scratch must hold
- * rb_envmap_cdf_scratch_bytes(w, h) bytes of device memory. */
+ * rb_envmap_cdf_scratch_bytes(w, h) bytes of device memory; its contents on
+ * entry do not matter (the call zeroes its completion counter on `stream`
+ * before the build). */
 size_t rb_envmap_cdf_scratch_bytes(uint32_t width, uint32_t height);
 int rb_envmap_cdf(uint32_t width, uint32_t height, const float* rgba, int mode,
                   void* scratch, uint16_t* conditional_idx, uint16_t* marginal_idx,
@@ -132,9 +134,11 @@ int rb_envmap_cdf(uint32_t width, uint32_t height, const float* rgba, int mode,
  * still passes the image and the output tables; the scratch is a fixed
  * static device array inside this library, sized for images up to 8192
  * rows (about 100 KB), held by every GPU that loads the library until the
- * process exits. Taller images return RB_ERR_TOO_LARGE. The first call on a
- * device looks the array's device address up (cudaGetSymbolAddress), so make
- * that first call before any stream capture. All calls share the one array:
+ * process exits. Taller images return RB_ERR_TOO_LARGE. Every call looks the
+ * array's device address up in the current context (cudaGetSymbolAddress,
+ * which allocates nothing); the first lookup on a device may load this
+ * library's device code, so make the first call on a device before any
+ * stream capture. All calls share the one array:
  * calls that overlap on the GPU (on different streams, or from different
  * threads) race, so serialise them. */
 int rb_envmap_cdf_noalloc(uint32_t width, uint32_t height, const float* rgba, int mode,

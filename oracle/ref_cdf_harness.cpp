@@ -112,24 +112,33 @@ extern "C" int rbrefgpu_envmap_cdf(const char* cubinPath, int w, int h, const fl
 	return rc;
 }
 
-// Mean milliseconds per rebuild (build + invert) over `iters` launches after
-// `warmup`, timed with CUDA events on the default stream.
+// Mean milliseconds per rebuild (build + invert) over `iters` rebuilds after
+// `warmup`, each timed alone with CUDA events on the default stream. Before
+// each timed rebuild `flushBytes` of `flush` (device memory larger than L2,
+// or null) are overwritten so that the image is read from HBM, not L2.
 extern "C" float rbrefgpu_envmap_cdf_time(const char* cubinPath, int w, int h, const float* dRgba, uint16_t* dCond,
-	uint16_t* dMarg, int warmup, int iters)
+	uint16_t* dMarg, int warmup, int iters, void* flush, size_t flushBytes)
 {
-	if (ensureModule(cubinPath) != 0) return -1.0f;
+	if (ensureModule(cubinPath) != 0 || iters <= 0) return -1.0f;
 	RefCdfRun r;
 	if (r.prepare(dRgba, w, h) != 0) { r.release(); return -1.0f; }
 	for (int i = 0; i < warmup; ++i) r.run(dCond, dMarg, nullptr);
 	cudaEvent_t a, b;
 	cudaEventCreate(&a); cudaEventCreate(&b);
-	cudaEventRecord(a, 0);
-	for (int i = 0; i < iters; ++i) r.run(dCond, dMarg, nullptr);
-	cudaEventRecord(b, 0);
-	cudaEventSynchronize(b);
-	float ms = 0.0f;
-	cudaEventElapsedTime(&ms, a, b);
+	float total = 0.0f;
+	bool ok = true;
+	for (int i = 0; i < iters && ok; ++i)
+	{
+		if (flush) cudaMemsetAsync(flush, i & 0xFF, flushBytes, 0);
+		cudaEventRecord(a, 0);
+		ok = r.run(dCond, dMarg, nullptr) == 0;
+		cudaEventRecord(b, 0);
+		cudaEventSynchronize(b);
+		float ms = 0.0f;
+		cudaEventElapsedTime(&ms, a, b);
+		total += ms;
+	}
 	cudaEventDestroy(a); cudaEventDestroy(b);
 	r.release();
-	return ms / static_cast<float>(iters);
+	return ok ? total / static_cast<float>(iters) : -1.0f;
 }

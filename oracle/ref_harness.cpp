@@ -471,6 +471,44 @@ int rbref_render_rows(uint32_t offset, uint32_t count, int threads, uint32_t row
 	for (auto& t : pool) t.join();
 	return RB_OK;
 }
+// Bounded CPU sample of a frame for timing: rows first, first + stride,
+// first + 2 stride, ... (every column of each), samples [offset,
+// offset + count). Work is handed out in 64-pixel row segments so that
+// `threads` stay busy whatever the rows cost. Returns the number of pixels
+// rendered (>= 0) or an error code (< 0).
+int64_t rbref_render_strided(uint32_t offset, uint32_t count, int threads, uint32_t first, uint32_t stride)
+{
+	if (parameters.renderData == nullptr || parameters.traversable == 0) return RB_ERR_NO_SCENE;
+	if (stride == 0) return RB_ERR_INVALID;
+	parameters.samplingState.offset = offset;
+	parameters.samplingState.count = count;
+	const uint32_t W = parameters.resolutionState.filmWidth;
+	const uint32_t H = parameters.resolutionState.filmHeight;
+	const uint32_t rows = first < H ? (H - first + stride - 1) / stride : 0;
+	const uint32_t segs = (W + 63) / 64;
+	const uint64_t units = static_cast<uint64_t>(rows) * segs;
+	if (threads <= 0) threads = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+	std::atomic<uint64_t> next{ 0 };
+	auto worker = [&]() {
+		for (;;)
+		{
+			const uint64_t u = next.fetch_add(1);
+			if (u >= units) break;
+			const uint32_t y = first + static_cast<uint32_t>(u / segs) * stride;
+			const uint32_t x0 = static_cast<uint32_t>(u % segs) * 64;
+			const uint32_t x1 = std::min(W, x0 + 64);
+			for (uint32_t x = x0; x < x1; ++x)
+			{
+				oracle_optix::tls.launchIndex = uint3{ x, y, 0 };
+				__raygen__main();
+			}
+		}
+	};
+	std::vector<std::thread> pool;
+	for (int i = 0; i < threads; ++i) pool.emplace_back(worker);
+	for (auto& t : pool) t.join();
+	return static_cast<int64_t>(rows) * W;
+}
 int rbref_render(uint32_t offset, uint32_t count, int threads)
 {
 	return rbref_render_rows(offset, count, threads, 0, parameters.resolutionState.filmHeight);

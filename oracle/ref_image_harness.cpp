@@ -69,4 +69,57 @@ int rbrefgpu_resolve(const char* cubinPath, uint32_t w, uint32_t h, const float*
 	return rc;
 }
 
+// Mean milliseconds per renderResolve launch over `iters` launches after
+// `warmup`, each timed alone with CUDA events on the default stream (output
+// stays in the CUDA array; nothing is copied back). Before each timed launch
+// `flushBytes` of `flush` (device memory larger than L2, or null) are
+// overwritten so that the accumulation is read from HBM, not L2.
+float rbrefgpu_resolve_time(const char* cubinPath, uint32_t w, uint32_t h, const float* colorspace,
+	float exposureScale, const double* dRender, int warmup, int iters, void* flush, size_t flushBytes)
+{
+	if (ensureModule(cubinPath) != 0 || iters <= 0) return -1.0f;
+	cudaChannelFormatDesc desc = cudaCreateChannelDesc<uchar4>();
+	cudaArray_t array = nullptr;
+	cudaSurfaceObject_t surface = 0;
+	if (cudaMallocArray(&array, &desc, w, h, cudaArraySurfaceLoadStore) != cudaSuccess) return -1.0f;
+	cudaResourceDesc rd{};
+	rd.resType = cudaResourceTypeArray;
+	rd.res.array.array = array;
+	float ms = -1.0f;
+	if (cudaCreateSurfaceObject(&surface, &rd) == cudaSuccess)
+	{
+		Mat3 cs;
+		for (int i = 0; i < 9; ++i) cs.m[i] = colorspace[i];
+		uint32_t width = w, height = h;
+		float exposure = exposureScale;
+		const double* data = dRender;
+		void* params[] = { &width, &height, &cs, &exposure, &data, &surface };
+		bool ok = true;
+		auto launch = [&]() {
+			ok = ok && cuLaunchKernel(g_resolve, (w + 15) / 16, (h + 15) / 16, 1, 16, 16, 1, 0, nullptr, params,
+				nullptr) == CUDA_SUCCESS;
+		};
+		for (int i = 0; i < warmup; ++i) launch();
+		cudaEvent_t a, b;
+		cudaEventCreate(&a); cudaEventCreate(&b);
+		float total = 0.0f;
+		for (int i = 0; i < iters && ok; ++i)
+		{
+			if (flush) cudaMemsetAsync(flush, i & 0xFF, flushBytes, 0);
+			cudaEventRecord(a, 0);
+			launch();
+			cudaEventRecord(b, 0);
+			cudaEventSynchronize(b);
+			float t = 0.0f;
+			cudaEventElapsedTime(&t, a, b);
+			total += t;
+		}
+		if (ok) ms = total / static_cast<float>(iters);
+		cudaEventDestroy(a); cudaEventDestroy(b);
+		cudaDestroySurfaceObject(surface);
+	}
+	cudaFreeArray(array);
+	return ms;
+}
+
 } // extern "C"

@@ -19,8 +19,8 @@
 //   1  float64 sums (thread-serial, warp Kogge-Stone, warp-total scan), CDF
 //      values rounded to float once, sin weights in double.
 
+#include <atomic>
 #include <cstdint>
-#include <mutex>
 #include <cuda_runtime.h>
 
 #include "ratbite_b200_kernels.h"
@@ -300,6 +300,33 @@ size_t envCdfScratchBytes(uint32_t w, uint32_t h)
 	return 256 + alignUp(sizeof(double) * h, 256) + alignUp(sizeof(float) * h, 256);
 }
 
+namespace
+{
+constexpr int kMaxAttrDevices = 64;
+// Largest dynamic shared-memory size already granted to each kernel variant
+// on each device, so that cudaFuncSetAttribute runs once per device and size
+// class instead of on every build.
+std::atomic<int> g_smemGranted[2][kMaxAttrDevices];
+
+int grantSharedMemory(int mode, int bytes)
+{
+	int dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess) return RB_ERR_CUDA;
+	std::atomic<int>* granted = (dev >= 0 && dev < kMaxAttrDevices) ? &g_smemGranted[mode][dev] : nullptr;
+	if (granted && granted->load(std::memory_order_relaxed) >= bytes) return RB_OK;
+	const cudaError_t e = mode == 0
+		? cudaFuncSetAttribute(kEnvCdf<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)
+		: cudaFuncSetAttribute(kEnvCdf<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+	if (e != cudaSuccess) return RB_ERR_CUDA;
+	if (granted)
+	{
+		int cur = granted->load(std::memory_order_relaxed);
+		while (cur < bytes && !granted->compare_exchange_weak(cur, bytes)) {}
+	}
+	return RB_OK;
+}
+} // namespace
+
 int envCdfLaunch(uint32_t w, uint32_t h, const float* rgba, int mode, void* scratch, uint16_t* cond, uint16_t* marg,
 	float* integral, cudaStream_t st)
 {
@@ -308,19 +335,16 @@ int envCdfLaunch(uint32_t w, uint32_t h, const float* rgba, int mode, void* scra
 	const int B = blockSizeFor(w / 4);
 	const size_t smem = sizeof(float) * (w > h ? w : h) + sizeof(double) * 2 * 64 + sizeof(float) * 1024;
 	const Scratch scr = carve(scratch, h);
-	cudaError_t e;
+	const int rc = grantSharedMemory(mode, static_cast<int>(smem));
+	if (rc != RB_OK) return rc;
+	// The completion ticket starts at zero whatever the caller's scratch
+	// holds (the last block also resets it, but a fresh allocation is not
+	// zeroed); the rest of the scratch is written before it is read.
+	if (cudaMemsetAsync(scr.ticket, 0, sizeof(uint32_t), st) != cudaSuccess) return RB_ERR_CUDA;
 	if (mode == 0)
-	{
-		e = cudaFuncSetAttribute(kEnvCdf<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-		if (e != cudaSuccess) return RB_ERR_CUDA;
 		kEnvCdf<0><<<h, B, smem, st>>>(w, h, reinterpret_cast<const float4*>(rgba), scr, cond, marg, integral);
-	}
 	else
-	{
-		e = cudaFuncSetAttribute(kEnvCdf<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-		if (e != cudaSuccess) return RB_ERR_CUDA;
 		kEnvCdf<1><<<h, B, smem, st>>>(w, h, reinterpret_cast<const float4*>(rgba), scr, cond, marg, integral);
-	}
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
 } // namespace rb
@@ -342,25 +366,16 @@ constexpr size_t kNoAllocScratchBytes = 256 + ((sizeof(double) * kNoAllocMaxHeig
 	+ ((sizeof(float) * kNoAllocMaxHeight + 255) / 256) * 256;
 __device__ __align__(256) unsigned char g_envCdfScratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratchMutex;
-void* g_scratchAddress[kMaxDevices] = {};
-
-// Device address of g_envCdfScratch on the current device, looked up once
-// per device. In host code the array's name is only a host-side handle, so
-// the address has to come from cudaGetSymbolAddress.
+// Device address of g_envCdfScratch in the current device's context. In
+// host code the array's name is only a host-side handle, so the address has
+// to come from cudaGetSymbolAddress; it is looked up on every call (a lookup
+// allocates nothing), so a context that was torn down and created again
+// never leaves a stale address behind.
 int scratchAddress(void** out)
 {
-	int dev = 0;
-	if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return RB_ERR_CUDA;
-	std::lock_guard<std::mutex> lock(g_scratchMutex);
-	if (!g_scratchAddress[dev])
-	{
-		void* p = nullptr;
-		if (cudaGetSymbolAddress(&p, g_envCdfScratch) != cudaSuccess || !p) return RB_ERR_CUDA;
-		g_scratchAddress[dev] = p;
-	}
-	*out = g_scratchAddress[dev];
+	void* p = nullptr;
+	if (cudaGetSymbolAddress(&p, g_envCdfScratch) != cudaSuccess || !p) return RB_ERR_CUDA;
+	*out = p;
 	return RB_OK;
 }
 } // namespace
@@ -372,10 +387,9 @@ extern "C" int rb_envmap_cdf_noalloc(uint32_t width, uint32_t height, const floa
 	void* scratch = nullptr;
 	const int rc = scratchAddress(&scratch);
 	if (rc != RB_OK) return rc;
-	const cudaStream_t st = static_cast<cudaStream_t>(stream);
-	// The ticket must start at zero; the rest of the scratch is written before it is read.
-	if (cudaMemsetAsync(scratch, 0, sizeof(uint32_t), st) != cudaSuccess) return RB_ERR_CUDA;
-	return rb::envCdfLaunch(width, height, rgba, mode, scratch, conditional_idx, marginal_idx, integral, st);
+	// envCdfLaunch zeroes the completion ticket on the stream before the build.
+	return rb::envCdfLaunch(width, height, rgba, mode, scratch, conditional_idx, marginal_idx, integral,
+		static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int rb_envmap_cdf(uint32_t width, uint32_t height, const float* rgba, int mode, void* scratch,

@@ -47,11 +47,14 @@ def combine(accum, group=None):
 def render_range(ri, offset: int, count: int, stream=None):
     """Renders samples [offset, offset + count) into a fresh accumulation.
 
-    The reference restarts its accumulation only when the range starts at
-    sample 0; a rank whose range starts later clears it first."""
-    if offset != 0:
+    The reference restarts its accumulation only when a launch starts at
+    sample 0; a rank whose range starts later clears it first, and so does a
+    rank with an empty range (it launches nothing, and must contribute
+    zeros rather than its previous frame to the combine)."""
+    if offset != 0 or count == 0:
         ri.clear_accumulation(stream=stream)
-    ri.render(offset, count, stream=stream)
+    if count:
+        ri.render(offset, count, stream=stream)
 
 
 def render_frame(ri, accum, offset: int, count: int, stream=None, group=None):

@@ -53,6 +53,7 @@ class RefLib:
             ("rbref_set_launch", C.c_int, [_P]),
             ("rbref_render", C.c_int, [_U32, _U32, C.c_int]),
             ("rbref_render_rows", C.c_int, [_U32, _U32, C.c_int, _U32, _U32]),
+            ("rbref_render_strided", C.c_int64, [_U32, _U32, C.c_int, _U32, _U32]),
             ("rbref_read_accum", None, [_P]),
             ("rbref_write_accum", None, [_P]),
             ("rbref_sobol", None, [_U32, _U32, _P, _P, _P, _P, _P]),
@@ -69,6 +70,7 @@ class RefLib:
             ("rbref_build_light_tree", C.c_int, [_U32, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
             ("rbref_colorspace_matrix", None, [C.c_int, _P]),
             ("rbref_sizeof_material_data", _U32, []),
+            ("rbref_set_libm_jitter", None, [C.c_int, C.c_uint64]),
             ("rbref_sizeof_launch_parameters", _U32, []),
         ]:
             fn = getattr(L, name)

@@ -318,3 +318,33 @@ def test_progressive_plan_rejects_bad_input():
     assert lib.rb_progressive_plan(10, 2, None, None, 0) < 0
     assert lib.rb_progressive_plan(10, 1, None, None, 4) < 0
     assert lib.rb_progressive_plan(10, 1, None, None, 0) == len(_reference_schedule(10, True))
+
+
+def test_oracle_libm_jitter_is_off_by_default_and_reversible(ref):
+    """The libm jitter of the oracle (oracle/shim/libm_jitter.cpp) that the
+    GPU parity tests use to measure the reference's own sensitivity: off, the
+    light-tree pdfs are exactly the plain oracle's; on, some move by a few
+    ulps (the wrapped libm calls really go through it); off again, exact."""
+    sc = cases.many_lights_scene()
+    cie, basis = ref.cie_xyz(), ref.basis_rgb()
+    keep = load_scene_into_ref(ref, sc, reference_luts(), cie, basis)
+    cs = cases.light_cases(n=512)
+    n = len(cs)
+
+    def run():
+        out = (abi.rb_light_case * n).from_buffer_copy(bytes(cs))
+        ref.lib.rbref_light_tree(n, C.cast(out, C.c_void_p))
+        return np.array([c.pdf for c in out], np.float64)
+
+    base = run()
+    assert np.array_equal(run(), base)
+    ref.lib.rbref_set_libm_jitter(1, 7)
+    try:
+        moved = run()
+    finally:
+        ref.lib.rbref_set_libm_jitter(0, 0)
+    rel = np.abs(moved - base) / np.maximum(np.abs(base), 1e-30)
+    assert (rel > 0).mean() > 0.5
+    assert np.median(rel[rel > 0]) < 1e-5
+    assert np.array_equal(run(), base)
+    del keep

@@ -100,6 +100,24 @@ def test_repeated_builds_reuse_scratch():
     assert np.array_equal(host(marg).view(np.uint16), a[1])
 
 
+def test_scratch_contents_on_entry_do_not_matter():
+    """Scratch straight from an allocator holds anything: 0xFF bytes in the
+    completion counter must not stop the marginal from being built."""
+    img = _sky(512, 256, seed=9)
+    want_c, want_m, want_i, _ = ours(img, 0)
+    lib = load()
+    h, w = img.shape[:2]
+    d = dev(img)
+    scratch = torch().full((int(lib.rb_envmap_cdf_scratch_bytes(w, h)),), 0xFF, dtype=torch().uint8, device="cuda")
+    cond = empty(w * h, torch().int16)
+    marg = empty(h, torch().int16)
+    integ = empty(1, torch().float32)
+    assert lib.rb_envmap_cdf(w, h, ptr(d), 0, ptr(scratch), ptr(cond), ptr(marg), ptr(integ), None) == 0
+    assert np.array_equal(host(cond).view(np.uint16).reshape(h, w), want_c)
+    assert np.array_equal(host(marg).view(np.uint16), want_m)
+    assert float(host(integ)[0]) == want_i
+
+
 def test_rejects_bad_sizes():
     lib = load()
     x = empty(64, torch().uint8)

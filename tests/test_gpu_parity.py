@@ -18,7 +18,7 @@ import numpy as np
 import pytest
 
 import cases
-from gpu_util import dev, empty, host, ptr, run_bxdf, run_light, torch
+from gpu_util import assert_image_parity, dev, empty, host, ptr, run_bxdf, run_light, torch
 from oracle_lib import RefLib, light_tree_record, load_scene_into_ref, ref_render, reference_luts, _np_ptr
 from ratbite_b200 import abi, scenes
 from ratbite_b200._native import check, load
@@ -232,7 +232,33 @@ def _bxdf_setup(ref, tables):
     return ri, (recs, extra, lut_arrays)
 
 
+def _vec_rel(got, want, floor):
+    """Norm-wise relative difference per case: max |g - w| over the
+    components over max(max |w|, floor)."""
+    g = np.asarray(got, np.float64).reshape(len(got), -1)
+    w = np.asarray(want, np.float64).reshape(len(want), -1)
+    return np.abs(g - w).max(axis=1) / np.maximum(np.abs(w).max(axis=1), floor)
+
+
 def test_bxdf_parity(ref, tables):
+    """Each BxDF call (light-sample evaluation, then the BxDF sample with
+    roulette; src/kernels/pathtrace.cu:548-905 and :464-547) against the
+    reference's callable run by the oracle on the same inputs.
+
+    A call either takes the same branch on both sides (the same lobe, the
+    same discrete outcome) and then must agree within 1e-5 relative in every
+    output (direction, pdf, throughput, radiance), or it takes a different
+    branch: the lobe choice compares a float probability against the random
+    number, so a one-ulp libm difference can flip it. A flip is recognised by
+    different path flags or a sampled direction more than 1e-3 away; flips
+    are counted, printed and bounded (<= 0.5 %).
+
+    Where an output is itself ill-conditioned at that level (cancellation
+    after a powf or a cosf turns a few ulps of a libm result into hundreds in
+    the output), the bound is what the oracle's own output moves when its
+    libm results move by as much as CUDA's and glibc's may differ (the
+    oracle re-run with libm jitter, see oracle/shim/libm_jitter.cpp), if
+    that is larger than 1e-5. At most 0.2 % of the cases may need it."""
     ri, keep = _bxdf_setup(ref, tables)
     cs = cases.bxdf_cases()
     n = len(cs)
@@ -241,27 +267,65 @@ def test_bxdf_parity(ref, tables):
     got = run_bxdf(ri, cs)
     ri.cleanup()
 
-    def arr(cs_, f, k=None):
-        return np.array([getattr(c, f)[:] if k else getattr(c, f) for c in cs_], np.float64)
     flags_eq = np.array([a.flags == b.flags for a, b in zip(got, want)])
-    dirs_ok = close(arr(got, "dir", 1), arr(want, "dir", 1), rtol=1e-4, atol=2e-5).all(axis=1)
-    pdf_ok = close(arr(got, "bxdf_pdf"), arr(want, "bxdf_pdf"), rtol=1e-4, atol=1e-6)
-    thr_ok = close(arr(got, "throughput", 1), arr(want, "throughput", 1), rtol=1e-4, atol=1e-6).all(axis=1)
-    L_ok = close(arr(got, "L", 1), arr(want, "L", 1), rtol=1e-4, atol=1e-6).all(axis=1)
-    ok = flags_eq & dirs_ok & pdf_ok & thr_ok & L_ok
-    frac_bad = 1.0 - ok.mean()
-    for f in ("bxdf_pdf",):
-        report("bxdf pdf", arr(got, f), arr(want, f))
-    report("bxdf throughput", arr(got, "throughput", 1), arr(want, "throughput", 1))
-    report("bxdf L", arr(got, "L", 1), arr(want, "L", 1))
-    report("bxdf dir", arr(got, "dir", 1), arr(want, "dir", 1), floor=1e-3)
-    print(f"bxdf cases {n}: mismatch fraction {frac_bad:.4%} (flags {1 - flags_eq.mean():.4%}, "
-          f"dir {1 - dirs_ok.mean():.4%}, pdf {1 - pdf_ok.mean():.4%}, T {1 - thr_ok.mean():.4%}, L {1 - L_ok.mean():.4%})")
-    assert frac_bad <= 0.005
-    # the typical case is far tighter than the bound
-    good = ok & (arr(want, "bxdf_pdf") > 0)
-    rel = np.abs(arr(got, "bxdf_pdf")[good] - arr(want, "bxdf_pdf")[good]) / np.abs(arr(want, "bxdf_pdf")[good])
-    assert np.median(rel) < 1e-6
+    gd, wd = _bxdf_arr(got, "dir"), _bxdf_arr(want, "dir")
+    branch = ~flags_eq | (np.abs(gd - wd).max(axis=1) > 1e-3)
+    rel = {k: _vec_rel(_bxdf_arr(got, f), _bxdf_arr(want, f), floor) for k, (f, floor) in _BXDF_OUT.items()}
+    spread = _oracle_bxdf_spread(ref, cs, want)
+    same = ~branch
+    for k, r in rel.items():
+        r = r[same]
+        print(f"bxdf {k}: n={r.size} rel median {np.median(r):.2e} p99.9 {np.quantile(r, 0.999):.2e} "
+              f"max {r.max():.2e} exact {np.mean(r == 0):.2%}")
+    print(f"bxdf cases {n}: branch flips {branch.sum()} ({branch.mean():.4%}; flags {(~flags_eq).sum()})")
+    assert branch.mean() <= 0.005
+    for k, r in rel.items():
+        beyond = same & (r > RTOL)
+        assert beyond.mean() <= 0.002, f"{beyond.sum()} same-branch BxDF cases differ in {k} beyond 1e-5"
+        bad = beyond & (r > spread[k])
+        if beyond.any():
+            print(f"bxdf {k}: {beyond.sum()} cases beyond 1e-5, rel diff / oracle one-ulp spread: "
+                  f"max {np.max(r[beyond] / np.maximum(spread[k][beyond], 1e-30)):.2f}")
+        for i in np.flatnonzero(beyond)[:5]:
+            print(f"  {k} case {i} material {cs[i].material} roughness {cs[i].roughness:.4g}: rel {r[i]:.3e}, "
+                  f"oracle spread {spread[k][i]:.3e}")
+        assert not bad.any(), f"{bad.sum()} same-branch BxDF cases differ in {k} beyond the bound"
+
+
+# BxDF outputs compared: name -> (record field, absolute floor of the
+# norm-wise relative difference)
+_BXDF_OUT = {"dir": ("dir", 1.0), "pdf": ("bxdf_pdf", 1e-6), "throughput": ("throughput", 1e-6), "L": ("L", 1e-6)}
+
+
+def _bxdf_arr(cs_, f):
+    v = [getattr(c, f) for c in cs_]
+    return np.array([x[:] if hasattr(x, "__len__") or hasattr(x, "_length_") else [x] for x in v], np.float64)
+
+
+JITTER_SEEDS = 16
+
+
+def _oracle_bxdf_spread(ref, cs, want):
+    """Per output, the largest norm-wise relative change of the oracle's
+    result over JITTER_SEEDS runs with libm jitter on (runs that change the
+    branch of a case are skipped for it)."""
+    n = len(cs)
+    spread = {k: np.zeros(n) for k in _BXDF_OUT}
+    wd = _bxdf_arr(want, "dir")
+    wf = np.array([c.flags for c in want])
+    try:
+        for seed in range(1, JITTER_SEEDS + 1):
+            ref.lib.rbref_set_libm_jitter(1, seed)
+            run = (abi.rb_bxdf_case * n).from_buffer_copy(bytes(cs))
+            ref.lib.rbref_bxdf(n, C.cast(run, C.c_void_p))
+            rd = _bxdf_arr(run, "dir")
+            same = (np.array([c.flags for c in run]) == wf) & (np.abs(rd - wd).max(axis=1) <= 1e-3)
+            for k, (f, floor) in _BXDF_OUT.items():
+                r = _vec_rel(_bxdf_arr(run, f), _bxdf_arr(want, f), floor)
+                spread[k] = np.where(same, np.maximum(spread[k], r), spread[k])
+    finally:
+        ref.lib.rbref_set_libm_jitter(0, 0)
+    return spread
 
 
 # ------------------------------------------------------------- light tree
@@ -290,30 +354,63 @@ def test_light_tree_parity(ref, tables):
     # Tolerance. A pick's pdf is a product of one importance ratio per tree
     # level, and each importance goes through exp(logAmplitude) with
     # logAmplitude = 2 s (cos - 1) / (...) of magnitude up to ~1e2 for sharp,
-    # distant nodes, so a one-ulp difference of expf between CUDA and the host
-    # libm is up to ~1e2 ulps in the pdf. The shading kernels round every
-    # operation as the oracle does (no FMA contraction), so that is the only
-    # source: the 1e-5 relative bound holds for all but the worst-conditioned
-    # cases, and the tail stays below 2e-4 (measured on B200: sample pdf max
-    # 7.0e-5, replayed pdf max 5.8e-5, 99.9% within 1e-5). Picks must agree.
+    # distant nodes: exp's condition number there is ~1e2, so a one-ulp
+    # difference of a libm result (CUDA against glibc) upstream of it becomes
+    # ~1e2 ulps in the pdf. The shading kernels round every basic operation as
+    # the oracle does (no FMA contraction), so that is the only source. Every
+    # case must agree within 1e-5 relative, or, where the pdf itself is that
+    # ill-conditioned, within what the oracle's own pdf moves when its libm
+    # results move by as much as CUDA's and glibc's may differ (the oracle
+    # re-run with libm jitter). Picks must agree.
     ok_s = close(gp[same_pick], wp[same_pick], rtol=1e-5, atol=1e-9)
     ok_q = close(gq, wq, rtol=1e-5, atol=1e-9)
     print(f"within 1e-5: sample pdf {ok_s.mean():.4%}, replayed pdf {ok_q.mean():.4%}")
     assert ok_s.mean() >= 0.995
     assert ok_q.mean() >= 0.995
-    assert close(gp[same_pick], wp[same_pick], rtol=2e-4, atol=1e-9).all()
-    assert close(gq, wq, rtol=2e-4, atol=1e-9).all()
+    sens_s, sens_q = _oracle_pdf_spread(ref, cs, want)
+    rel_s = np.abs(gp - wp) / np.maximum(np.abs(wp), 1e-30)
+    rel_q = np.abs(gq - wq) / np.maximum(np.abs(wq), 1e-30)
+    tol_s = np.maximum(RTOL, sens_s)
+    tol_q = np.maximum(RTOL, sens_q)
+    bad_s = same_pick & (rel_s > tol_s) & ~close(gp, wp, rtol=1e-5, atol=1e-9)
+    bad_q = (rel_q > tol_q) & ~close(gq, wq, rtol=1e-5, atol=1e-9)
+    relaxed = same_pick & ~close(gp, wp, rtol=1e-5, atol=1e-9)
+    if relaxed.any():
+        print(f"sample pdfs beyond 1e-5: {relaxed.sum()}, rel diff / oracle libm-jitter spread: "
+              f"max {np.max(rel_s[relaxed] / np.maximum(sens_s[relaxed], 1e-30)):.2f}")
+    for i in np.flatnonzero(bad_s | bad_q)[:8]:
+        print(f"  case {i}: sample pdf rel {rel_s[i]:.2e} (spread {sens_s[i]:.2e}), "
+              f"replayed rel {rel_q[i]:.2e} (spread {sens_q[i]:.2e})")
+    assert not bad_s.any()
+    assert not bad_q.any()
+
+
+def _oracle_pdf_spread(ref, cs, want):
+    """Largest relative change of the oracle's sample pdf and replayed pdf
+    over JITTER_SEEDS runs with libm jitter on (runs that change the pick of
+    a case are skipped for it)."""
+    n = len(cs)
+    wp = np.array([c.pdf for c in want], np.float64)
+    wq = np.array([c.q_pdf for c in want], np.float64)
+    sens_s, sens_q = np.zeros(n), np.zeros(n)
+    try:
+        for seed in range(1, JITTER_SEEDS + 1):
+            ref.lib.rbref_set_libm_jitter(1, seed)
+            run = (abi.rb_light_case * n).from_buffer_copy(bytes(cs))
+            ref.lib.rbref_light_tree(n, C.cast(run, C.c_void_p))
+            same = np.array([(a.type, a.index) == (b.type, b.index) for a, b in zip(run, want)])
+            ps = np.array([c.pdf for c in run], np.float64)
+            pq = np.array([c.q_pdf for c in run], np.float64)
+            ds = np.abs(ps - wp) / np.maximum(np.abs(wp), 1e-30)
+            dq = np.abs(pq - wq) / np.maximum(np.abs(wq), 1e-30)
+            sens_s = np.where(same, np.maximum(sens_s, ds), sens_s)
+            sens_q = np.maximum(sens_q, dq)
+    finally:
+        ref.lib.rbref_set_libm_jitter(0, 0)
+    return sens_s, sens_q
 
 
 # ----------------------------------------------------------------- render
-def _image_stats(got, want):
-    g = got[..., :3] / np.maximum(got[..., 3:4], 1)
-    w = want[..., :3] / np.maximum(want[..., 3:4], 1)
-    rel_mean = abs(g.sum() - w.sum()) / abs(w.sum())
-    l1 = np.abs(g - w).sum() / np.abs(w).sum()
-    return rel_mean, l1
-
-
 def test_render_parity_cornell(ref, tables, cornell):
     sc, ri, _ = cornell
     reload_ref(ref, sc, tables)
@@ -323,11 +420,7 @@ def test_render_parity_cornell(ref, tables, cornell):
     got = ri.read_accumulation()
     st = ri.status()
     assert st.flags == 0
-    assert np.array_equal(got[..., 3], want[..., 3])
-    rel_mean, l1 = _image_stats(got, want)
-    print(f"cornell {W}x{H}x{spp}: image-mean rel diff {rel_mean:.3e}, per-pixel L1 {l1:.3e}")
-    assert rel_mean < 5e-3
-    assert l1 < 5e-2
+    assert_image_parity(f"cornell {W}x{H}x{spp}", got, want)
 
 
 def test_render_progressive_offsets(ref, tables, cornell):
@@ -353,10 +446,7 @@ def test_render_many_lights(ref, tables):
         ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lt, width=W, height=H)
         ri.render(0, spp)
         got = ri.read_accumulation()
-    rel_mean, l1 = _image_stats(got, want)
-    print(f"many lights {W}x{H}x{spp}: image-mean rel diff {rel_mean:.3e}, per-pixel L1 {l1:.3e}")
-    assert rel_mean < 1e-2
-    assert l1 < 1e-1
+    assert_image_parity(f"many lights {W}x{H}x{spp}", got, want)
 
 
 def test_render_parity_instanced_envmap(ref, tables):
@@ -377,8 +467,4 @@ def test_render_parity_instanced_envmap(ref, tables):
         ri.render(0, spp)
         got = ri.read_accumulation()
         assert ri.status().flags == 0
-    rel_mean, l1 = _image_stats(got, want)
-    print(f"instanced+envmap {W}x{H}x{spp}: image-mean rel diff {rel_mean:.3e}, per-pixel L1 {l1:.3e}")
-    assert np.array_equal(got[..., 3], want[..., 3])
-    assert rel_mean < 1e-2
-    assert l1 < 1e-1
+    assert_image_parity(f"instanced+envmap {W}x{H}x{spp}", got, want)

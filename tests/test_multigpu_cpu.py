@@ -105,7 +105,13 @@ def _rank(rank, world, port, out_dir):
         off, cnt = multigpu.weak_sample_range(3, rank)
         multigpu.render_frame(ri, accum, off, cnt)
         weak = accum.numpy().copy()
-        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), strong=strong, weak=weak, clears=ri.clears)
+        # an empty frame (0 samples): every range is empty, rank 0's included,
+        # and the combine must give zeros, not the previous frame
+        accum.zero_()
+        off, cnt = multigpu.sample_range(0, rank, world)
+        multigpu.render_frame(ri, accum, off, cnt)
+        empty = accum.numpy().copy()
+        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), strong=strong, weak=weak, empty=empty, clears=ri.clears)
         del keep
     finally:
         dist.destroy_process_group()
@@ -132,6 +138,9 @@ def test_two_gloo_ranks_combine_to_the_single_render(tmp_path):
             got = r[key]
             assert np.array_equal(got[..., 3], want[..., 3])      # sample counts
             np.testing.assert_allclose(got[..., :3], want[..., :3], rtol=1e-12, atol=1e-300)
-    # rank 0's ranges start at sample 0 (the renderer restarts by itself);
-    # rank 1 starts later in both frames and clears first
-    assert int(r0["clears"]) == 0 and int(r1["clears"]) == 2
+    for r in (r0, r1):
+        assert not r["empty"].any()
+    # rank 0's non-empty ranges start at sample 0 (the renderer restarts by
+    # itself); rank 1 starts later in both and clears first; both clear for
+    # the empty frame
+    assert int(r0["clears"]) == 1 and int(r1["clears"]) == 3

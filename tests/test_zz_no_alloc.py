@@ -62,6 +62,23 @@ def test_noalloc_matches_regular_entry_point_twice(mode):
         assert got[2] == want[2]
 
 
+@pytest.mark.parametrize("mode", [0, 1])
+def test_noalloc_at_its_maximum_height(mode):
+    """An image exactly as tall as the static scratch was sized for (8192
+    rows), against the regular entry point given scratch filled with 0xFF
+    bytes (its contents on entry must not matter)."""
+    import torch
+    from ratbite_b200._native import load
+    w, h = 8, 8192
+    img = _image(w, h, 7)
+    scratch = torch.full((int(load().rb_envmap_cdf_scratch_bytes(w, h)),), 0xFF, dtype=torch.uint8, device="cuda")
+    want = _run("rb_envmap_cdf", img, mode, scratch)
+    got = _run("rb_envmap_cdf_noalloc", img, mode)
+    assert np.array_equal(got[0], want[0])
+    assert np.array_equal(got[1], want[1])
+    assert got[2] == want[2]
+
+
 def test_noalloc_rejects_images_taller_than_its_scratch():
     import torch
     from ratbite_b200 import abi
