@@ -82,7 +82,20 @@ typedef struct rb_config {
     uint32_t max_paths_in_flight;/* wavefront capacity; 0 = default (16M paths) */
     uint32_t envmap_cdf_mode;    /* RB_CDF_FP64 (default, 0) or RB_CDF_REFERENCE */
     uint32_t failed_sample_mode; /* RB_FAILED_DROP (default, 0) or RB_FAILED_KEEP */
-    uint32_t reserved[4];
+    /* Fault injection for tests (no reference counterpart), all 0 in normal use:
+     * inject_queue_limit    wavefront queues accept at most this many entries
+     *                       per bounce (the rest are dropped and
+     *                       RB_DEV_QUEUE_OVERFLOW is set); 0 = their capacity;
+     * inject_alloc_failure  the n-th device allocation of the context (1-based,
+     *                       counted over all calls) fails once, as an
+     *                       out-of-memory cudaMalloc would; 0 = none;
+     * inject_stack_limit    BVH traversal stacks hold at most this many entries
+     *                       (RB_DEV_STACK_OVERFLOW when one is full); 0 = the
+     *                       full stack. */
+    uint32_t inject_queue_limit;
+    uint32_t inject_alloc_failure;
+    uint32_t inject_stack_limit;
+    uint32_t reserved;
 } rb_config;
 /* A BxDF sample that fails (a direction on the wrong side of the shading
  * hemisphere, a zero or infinite pdf) sets the path's terminated flag. The

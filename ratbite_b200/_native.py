@@ -85,7 +85,12 @@ _lib = None
 
 
 class NativeError(RuntimeError):
-    pass
+    """A library call failed; `code` is its RB_ERR_* status (None when the
+    library itself could not be loaded)."""
+
+    def __init__(self, msg: str, code: int | None = None):
+        super().__init__(msg)
+        self.code = code
 
 
 def load() -> C.CDLL:
@@ -113,4 +118,4 @@ def check(rc: int, ctx=None, what: str = ""):
         if ctx is not None:
             m = load().rb_last_error(ctx)
             msg = m.decode() if m else ""
-        raise NativeError(f"{what} failed with status {rc}: {msg}")
+        raise NativeError(f"{what} failed with status {rc}: {msg}", rc)

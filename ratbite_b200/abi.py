@@ -87,7 +87,9 @@ RB_CDF_REFERENCE = 1
 
 class rb_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_paths_in_flight", C.c_uint32),
-                ("envmap_cdf_mode", C.c_uint32), ("failed_sample_mode", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+                ("envmap_cdf_mode", C.c_uint32), ("failed_sample_mode", C.c_uint32),
+                ("inject_queue_limit", C.c_uint32), ("inject_alloc_failure", C.c_uint32),
+                ("inject_stack_limit", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 RB_FAILED_DROP = 0

@@ -16,16 +16,32 @@
 
 namespace rb
 {
-constexpr int kTraversalStack = 64;
+constexpr int kTraversalStack = kTraversalStackEntries;
 
 // Traversal variants (compile-time): RB_TRAV_SORT orders the entered
-// children near-to-far with a sorting network (0: descend the nearest, push
-// the rest unordered); RB_TRAV_WHILE_WHILE runs interior nodes until a leaf
-// before each leaf (0: one node or leaf per step). On B200, at-scale frame:
-// sort + one step 493 ms of extension, nearest-only 509 ms (4% more nodes
-// visited), while-while 559 ms.
+// children near-to-far with a sorting network (1, the default; 0: descend
+// the nearest, push the rest unordered; 2: direction-octant order, the
+// builder placing children in slots by octant after Ylitie, Karras and Laine
+// 2017, no sort); RB_TRAV_WHILE_WHILE runs interior nodes until a leaf
+// before each leaf (0: one node or leaf per step); RB_TRAV_POSTPONE keeps a
+// reached leaf aside and goes on with interior nodes, the warp testing the
+// postponed leaves one triangle per lane once half of its lanes hold one or
+// a lane has no node left (Aila and Laine 2009). On B200, at-scale frame
+// (2.03M triangles, 1920x1080x256, extension ms per frame; nodes and
+// triangles visited per ray): sorted 397 (13.3, 3.30); octant order 415
+// (14.3, 3.79); sorted + postponed leaves 416 (13.6, 3.64); octant +
+// postponed 440 (14.6, 4.15); octant order with one stack entry per node
+// group (node, remaining-child mask) 526 (14.8, 3.80); earlier: nearest-only
+// 509 against 493 sorted, while-while 559. Octant order saves the sort but
+// visits more nodes and triangles than it saves; postponing adds visits
+// (culling sees the postponed hits later) and the traversal is bound by
+// instruction issue and L1/L2 latency, not by the node-versus-leaf
+// divergence it removes.
 #ifndef RB_TRAV_SORT
 #define RB_TRAV_SORT 1
+#endif
+#ifndef RB_TRAV_POSTPONE
+#define RB_TRAV_POSTPONE 0
 #endif
 #ifndef RB_TRAV_WHILE_WHILE
 #define RB_TRAV_WHILE_WHILE 0
@@ -37,6 +53,7 @@ struct TraceRay
 	float ix, iy, iz;         // safe reciprocal direction for box tests
 	int kx, ky, kz;
 	float sx, sy, sz;
+	uint32_t oct;             // direction octant: bit 0 x < 0, bit 1 y < 0, bit 2 z < 0
 };
 
 RB_D float safeRcp(float d) { return 1.0f / (fabsf(d) < 1e-20f ? copysignf(1e-20f, d) : d); }
@@ -57,6 +74,7 @@ RB_D TraceRay makeTraceRay(f3 o, f3 d)
 	r.sx = __fdiv_rn(comp(d, r.kx), dz);
 	r.sy = __fdiv_rn(comp(d, r.ky), dz);
 	r.sz = __fdiv_rn(1.0f, dz);
+	r.oct = (signbit(r.ix) ? 1u : 0u) | (signbit(r.iy) ? 2u : 0u) | (signbit(r.iz) ? 4u : 0u);
 	return r;
 }
 
@@ -134,7 +152,10 @@ RB_D uint32_t planeWord(const NodeView& v, int w)
 }
 
 // Intersects the ray with the 8 child boxes; hitMask bit c set when child c
-// is entered within [tmin, tmax]; tnear[c] is its entry distance. Per axis the
+// is entered within [tmin, tmax]; tnear[c] is its entry distance. Empty
+// slots carry inverted boxes, which rays miss except where rounding flattens
+// the box (a ray far from a tiny node): the traversal skips empty references
+// (kEmptyChild) wherever it takes a child. Per axis the
 // near and far plane rows are chosen once from the sign of the reciprocal
 // direction, which gives the same distances as taking the min and max of the
 // two planes per child (the rounding is monotonic).
@@ -174,7 +195,7 @@ RB_D uint32_t childBoxes(const TraceRay& r, const NodeView& v, float tmin, float
 		const float n = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
 		const float f = fminf(fminf(tfx, tfy), fminf(tfz, tmax)) * 1.0000004f;
 		tnear[c] = n;
-		if (n <= f && nodeChild(v, c) != kEmptyChild) mask |= 1u << c;
+		if (n <= f) mask |= 1u << c;
 	}
 	return mask;
 }
@@ -206,6 +227,15 @@ RB_D uint32_t nodeChildAt(const NodeView& v, uint32_t s)
 	return __float_as_uint(k == 0u ? a.x : (k == 1u ? a.y : (k == 2u ? a.z : a.w)));
 }
 
+// Visit-order mask of a hit mask: bit v of the result is slot (v ^ oct).
+RB_D uint32_t visitOrder(uint32_t m, uint32_t oct)
+{
+	if (oct & 1u) m = ((m & 0x55u) << 1) | ((m >> 1) & 0x55u);
+	if (oct & 2u) m = ((m & 0x33u) << 2) | ((m >> 2) & 0x33u);
+	if (oct & 4u) m = ((m & 0x0Fu) << 4) | ((m >> 4) & 0x0Fu);
+	return m;
+}
+
 struct Hit
 {
 	int32_t tri;       // BVH-order triangle index, -1 on a miss
@@ -225,11 +255,13 @@ struct ClosestTraversal
 	Hit best;
 	uint32_t bestId;
 	uint32_t cur;
+	uint32_t leaf;         // postponed leaf (RB_TRAV_POSTPONE): its untested triangles, 0 for none
 	int sp;
 	bool done;
 
 	RB_D void init(const DevGeometry& g, f3 o, f3 d, float tmin_, float tmax)
 	{
+		leaf = 0u;
 		best = Hit{ -1, tmax, 0.0f, 0.0f };
 		bestId = 0xFFFFFFFFu;
 		tmin = tmin_;
@@ -278,7 +310,28 @@ struct ClosestTraversal
 		float tn[8];
 		const uint32_t mask = childBoxes(r, nv, tmin, best.t, tn);
 		if (!mask) return false;
-#if RB_TRAV_SORT
+#if RB_TRAV_SORT == 2
+		// visit index of slot c is c ^ oct; the children after the first are
+		// pushed so that the stack top holds the next one to visit
+		const uint32_t om = visitOrder(mask, r.oct);
+		const uint32_t firstV = static_cast<uint32_t>(__ffs(static_cast<int>(om)) - 1);
+		const uint32_t rest = om & (om - 1u);
+		const int nPush = __popc(rest);
+		if (sp + nPush <= static_cast<int>(g.stackLimit))
+		{
+#pragma unroll
+			for (int c = 0; c < 8; ++c)
+			{
+				const uint32_t v = static_cast<uint32_t>(c) ^ r.oct;
+				if ((rest >> v) & 1u)
+					stack[sp + __popc(rest >> (v + 1u))] = make_uint2(nodeChild(nv, c), __float_as_uint(tn[c]));
+			}
+			sp += nPush;
+		}
+		else if (nPush) atomicOr(status, RB_DEV_STACK_OVERFLOW);
+		cur = nodeChildAt(nv, firstV ^ r.oct);
+		if (cur == kEmptyChild) return false;
+#elif RB_TRAV_SORT
 		uint32_t key[8];
 #pragma unroll
 		for (int c = 0; c < 8; ++c)
@@ -291,11 +344,12 @@ struct ClosestTraversal
 		{
 			if (c < n)
 			{
-				if (sp < kTraversalStack) { stack[sp] = make_uint2(nodeChildAt(nv, key[c] & 7u), key[c] & ~7u); ++sp; }
+				if (sp < static_cast<int>(g.stackLimit)) { stack[sp] = make_uint2(nodeChildAt(nv, key[c] & 7u), key[c] & ~7u); ++sp; }
 				else atomicOr(status, RB_DEV_STACK_OVERFLOW);
 			}
 		}
 		cur = nodeChildAt(nv, key[0] & 7u);
+		if (cur == kEmptyChild) return false;
 #else
 		int nearest = 0;
 		float nk = INFINITY;
@@ -307,11 +361,12 @@ struct ClosestTraversal
 		{
 			if (((mask >> c) & 1u) && c != nearest)
 			{
-				if (sp < kTraversalStack) { stack[sp] = make_uint2(nodeChild(nv, c), __float_as_uint(tn[c])); ++sp; }
+				if (sp < static_cast<int>(g.stackLimit)) { stack[sp] = make_uint2(nodeChild(nv, c), __float_as_uint(tn[c])); ++sp; }
 				else atomicOr(status, RB_DEV_STACK_OVERFLOW);
 			}
 		}
 		cur = nodeChild(nv, nearest);
+		if (cur == kEmptyChild) return false;
 #endif
 		return true;
 	}
@@ -323,7 +378,7 @@ struct ClosestTraversal
 		{
 			--sp;
 			const uint2 e = stack[sp];
-			if (__uint_as_float(e.y) <= best.t) { cur = e.x; return true; }
+			if (__uint_as_float(e.y) <= best.t && e.x != kEmptyChild) { cur = e.x; return true; }
 		}
 		return false;
 	}
@@ -354,6 +409,33 @@ struct ClosestTraversal
 			leafStep<COUNT>(g, nTris);
 			if (!pop(stack)) done = true;
 		}
+#elif RB_TRAV_POSTPONE
+		// cur: an interior node, a leaf, or kEmptyChild when no node is left
+		for (int it = 0; it < budget && !done; ++it)
+		{
+			if ((cur & kLeafBit) && cur != kEmptyChild && leaf == 0u)
+			{
+				leaf = cur;                              // keep the leaf aside
+				if (!pop(stack)) cur = kEmptyChild;
+			}
+			const bool noNode = (cur & kLeafBit) != 0u;  // nothing, or a second leaf
+			if (noNode && leaf == 0u)
+			{
+				done = true;
+				break;
+			}
+			const unsigned am = __activemask();
+			const unsigned holding = __ballot_sync(am, leaf != 0u);
+			const unsigned stuck = __ballot_sync(am, noNode);
+			if (stuck || 2 * __popc(holding) >= __popc(am))
+			{
+				if (leaf) triangleStep<COUNT>(g, nTris);
+			}
+			else if (!nodeStep<COUNT>(g, status, nNodes, stack) && !pop(stack))
+			{
+				cur = kEmptyChild;
+			}
+		}
 #else
 		for (int it = 0; it < budget && !done; ++it)
 		{
@@ -369,6 +451,29 @@ struct ClosestTraversal
 		}
 #endif
 		return done;
+	}
+
+	// Tests the first untested triangle of the postponed leaf and advances it.
+	template<bool COUNT>
+	RB_D void triangleStep(const DevGeometry& g, uint32_t& nTris)
+	{
+		const uint32_t i = leaf & 0x0FFFFFFFu;
+		const uint32_t left = (leaf >> 28) & 0x7u;       // triangles after this one
+		if (COUNT) ++nTris;
+		const float4 a = __ldg(g.triVerts + 3 * i);
+		const float4 b = __ldg(g.triVerts + 3 * i + 1);
+		const float4 c = __ldg(g.triVerts + 3 * i + 2);
+		float t, u, v;
+		if (intersectTriangle(r, f3_of(a), f3_of(b), f3_of(c), tmin, best.t, best.tri >= 0, t, u, v))
+		{
+			const uint32_t id = __float_as_uint(a.w);
+			if (best.tri < 0 || t < best.t || id < bestId)
+			{
+				best = Hit{ static_cast<int32_t>(i), t, u, v };
+				bestId = id;
+			}
+		}
+		leaf = left ? (kLeafBit | ((left - 1u) << 28) | (i + 1u)) : 0u;
 	}
 };
 
@@ -399,7 +504,11 @@ struct AnyTraversal
 	{
 		for (int it = 0; it < budget && !done; ++it)
 		{
-			if (cur & kLeafBit)
+			if (cur == kEmptyChild)
+			{
+				// an empty slot entered through a flattened box: nothing to test
+			}
+			else if (cur & kLeafBit)
 			{
 				const uint32_t first = cur & 0x0FFFFFFFu;
 				const uint32_t count = ((cur >> 28) & 0x7u) + 1u;
@@ -430,7 +539,7 @@ struct AnyTraversal
 				{
 					if ((mask >> c) & 1u)
 					{
-						if (sp < kTraversalStack) stack[sp++] = nodeChild(nv, c);
+						if (sp < static_cast<int>(g.stackLimit)) stack[sp++] = nodeChild(nv, c);
 						else atomicOr(status, RB_DEV_STACK_OVERFLOW);
 					}
 				}

@@ -6,7 +6,10 @@
 //    repeatedly opens the interior child with the largest surface area until
 //    it has 8 children (the greedy collapse of Wald et al. 2008 / Ylitie et
 //    al. 2017).
-// 3. Quantize child boxes to 8 bits per plane against a node origin and a
+// 3. Place each wide node's children in its 8 slots by direction octant
+//    (Ylitie, Karras and Laine 2017, sec. 3.2), so that traversal can visit
+//    them roughly near to far without sorting: see assignSlots.
+// 4. Quantize child boxes to 8 bits per plane against a node origin and a
 //    power-of-two scale per axis. The scale is at least two float ulps of the
 //    node's coordinates and the origin is a multiple of it, so every decoded
 //    plane origin + q*scale is exact in float; boxes are rounded outward and
@@ -194,13 +197,20 @@ public:
 			kids[best] = m_bin[open].left;
 			kids[n++] = m_bin[open].right;
 		}
+		int slotOf[8];
+		assignSlots(bi, kids, n, slotOf);
 		const uint32_t me = static_cast<uint32_t>(nodes.size());
 		nodes.emplace_back();
 		BvhNode node{};
 		double lo[8][3], hi[8][3];
+		uint32_t slots = 0;
 		for (int c = 0; c < n; ++c)
-			for (int a = 0; a < 3; ++a) { lo[c][a] = m_bin[kids[c]].box.lo[a]; hi[c][a] = m_bin[kids[c]].box.hi[a]; }
-		quantizeChildren(n, lo, hi, node);
+		{
+			const int s = slotOf[c];
+			slots |= 1u << s;
+			for (int a = 0; a < 3; ++a) { lo[s][a] = m_bin[kids[c]].box.lo[a]; hi[s][a] = m_bin[kids[c]].box.hi[a]; }
+		}
+		quantizeChildren(slots, lo, hi, node);
 		for (int c = 0; c < 8; ++c) node.child[c] = kEmptyChild;
 		// Children: leaves reference their (re-emitted) triangle range, interior
 		// nodes recurse.
@@ -211,7 +221,7 @@ public:
 			{
 				const uint32_t first = static_cast<uint32_t>(triOrderOut.size());
 				for (int i = k.first; i < k.first + k.count; ++i) triOrderOut.push_back(binOrder[i]);
-				node.child[c] = kLeafBit | (static_cast<uint32_t>(k.count - 1) << 28) | first;
+				node.child[slotOf[c]] = kLeafBit | (static_cast<uint32_t>(k.count - 1) << 28) | first;
 			}
 		}
 		nodes[me] = node;
@@ -220,7 +230,7 @@ public:
 			if (!isLeaf(m_bin[kids[c]]))
 			{
 				const uint32_t ci = emit(kids[c], triOrderOut, binOrder);
-				nodes[me].child[c] = ci;
+				nodes[me].child[slotOf[c]] = ci;
 			}
 		}
 		return me;
@@ -228,6 +238,42 @@ public:
 
 private:
 	const std::vector<BinNode>& m_bin;
+
+	// Slot s (bit 0: x, bit 1: y, bit 2: z) holds the child that a ray whose
+	// direction has those negative components meets first: the child whose
+	// centre lies farthest back along that direction. The cost of child c in
+	// slot s is dot(centre_c - centre_parent, d_s) with d_s = (+-1, +-1, +-1)
+	// the octant's diagonal; pairs are taken greedily, cheapest first.
+	void assignSlots(int bi, const int* kids, int n, int* slotOf) const
+	{
+		const Box& pb = m_bin[bi].box;
+		double pc[3];
+		for (int a = 0; a < 3; ++a) pc[a] = 0.5 * (pb.lo[a] + pb.hi[a]);
+		double cost[8][8];
+		for (int c = 0; c < n; ++c)
+		{
+			const Box& b = m_bin[kids[c]].box;
+			double d[3];
+			for (int a = 0; a < 3; ++a) d[a] = 0.5 * (b.lo[a] + b.hi[a]) - pc[a];
+			for (int s = 0; s < 8; ++s)
+				cost[c][s] = ((s & 1) ? -d[0] : d[0]) + ((s & 2) ? -d[1] : d[1]) + ((s & 4) ? -d[2] : d[2]);
+		}
+		bool childDone[8] = {}, slotUsed[8] = {};
+		for (int k = 0; k < n; ++k)
+		{
+			int bc = -1, bs = -1;
+			double best = INFINITY;
+			for (int c = 0; c < n; ++c)
+			{
+				if (childDone[c]) continue;
+				for (int s = 0; s < 8; ++s)
+					if (!slotUsed[s] && (bc < 0 || cost[c][s] < best)) { best = cost[c][s]; bc = c; bs = s; }
+			}
+			childDone[bc] = true;
+			slotUsed[bs] = true;
+			slotOf[bc] = bs;
+		}
+	}
 };
 } // namespace
 
@@ -261,7 +307,7 @@ WideBvh buildWideBvh(const std::vector<float>& worldVerts)
 	std::vector<uint32_t> depth(out.nodes.size(), 0);
 	uint32_t maxDepth = 0;
 	for (uint32_t i = 0; i < out.nodes.size(); ++i)          // pre-order: parents come first
-		for (int c = 0; c < out.nodes[i].childCount; ++c)
+		for (int c = 0; c < 8; ++c)
 		{
 			const uint32_t ref = out.nodes[i].child[c];
 			if (ref != kEmptyChild && !(ref & kLeafBit))
@@ -270,6 +316,7 @@ WideBvh buildWideBvh(const std::vector<float>& worldVerts)
 				maxDepth = std::max(maxDepth, depth[ref]);
 			}
 		}
+	out.maxDepth = maxDepth;
 	out.levelStart.assign(1, 0);
 	for (int d = static_cast<int>(maxDepth); d >= 0; --d)
 	{

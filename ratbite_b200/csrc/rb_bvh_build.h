@@ -17,6 +17,7 @@ struct WideBvh
 	// level k is refitOrder[levelStart[k] .. levelStart[k+1]).
 	std::vector<uint32_t> refitOrder;
 	std::vector<uint32_t> levelStart;
+	uint32_t maxDepth = 0;           // wide levels below the root
 };
 
 // worldVerts: 9 floats per triangle. Degenerate triangles must already be removed.

@@ -32,13 +32,21 @@ RB_HD int scaleExponent(double extent, double mag)
 }
 
 // Fills origin, exponents, child count and the quantized planes of `node`
-// from the n (1..8) child boxes lo[c][axis], hi[c][axis]; child references
-// are left to the caller. Unused slots get empty boxes.
-RB_HD void quantizeChildren(int n, const double (*lo)[3], const double (*hi)[3], BvhNode& node)
+// from the child boxes lo[c][axis], hi[c][axis] of the slots set in `slots`
+// (bit c: slot c holds a child; at least one bit set); child references are
+// left to the caller. An empty slot gets an inverted box (low planes 255
+// steps, high planes 0), which no ray enters: for either sign of a
+// direction component the far-plane distance is then below the near one.
+RB_HD void quantizeChildren(uint32_t slots, const double (*lo)[3], const double (*hi)[3], BvhNode& node)
 {
-	double alo[3] = { lo[0][0], lo[0][1], lo[0][2] }, ahi[3] = { hi[0][0], hi[0][1], hi[0][2] };
-	for (int c = 1; c < n; ++c)
+	double alo[3] = { INFINITY, INFINITY, INFINITY }, ahi[3] = { -INFINITY, -INFINITY, -INFINITY };
+	int n = 0;
+	for (int c = 0; c < 8; ++c)
+	{
+		if (!((slots >> c) & 1u)) continue;
+		++n;
 		for (int a = 0; a < 3; ++a) { alo[a] = ::fmin(alo[a], lo[c][a]); ahi[a] = ::fmax(ahi[a], hi[c][a]); }
+	}
 	double origin[3], scale[3];
 	for (int a = 0; a < 3; ++a)
 	{
@@ -51,8 +59,10 @@ RB_HD void quantizeChildren(int n, const double (*lo)[3], const double (*hi)[3],
 	}
 	node.childCount = static_cast<uint8_t>(n);
 	for (int c = 0; c < 8; ++c)
-		for (int a = 0; a < 3; ++a) { node.qlo[a][c] = 0; node.qhi[a][c] = 0; }
-	for (int c = 0; c < n; ++c)
+		for (int a = 0; a < 3; ++a) { node.qlo[a][c] = 255; node.qhi[a][c] = 0; }
+	for (int c = 0; c < 8; ++c)
+	{
+		if (!((slots >> c) & 1u)) continue;
 		for (int a = 0; a < 3; ++a)
 		{
 			const double ql = ::floor((lo[c][a] - origin[a]) / scale[a]) - 1.0;
@@ -60,5 +70,6 @@ RB_HD void quantizeChildren(int n, const double (*lo)[3], const double (*hi)[3],
 			node.qlo[a][c] = static_cast<uint8_t>(::fmin(::fmax(ql, 0.0), 255.0));
 			node.qhi[a][c] = static_cast<uint8_t>(::fmin(::fmax(qh, 0.0), 255.0));
 		}
+	}
 }
 } // namespace rb

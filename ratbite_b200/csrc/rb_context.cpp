@@ -45,6 +45,9 @@ struct rb_ctx
 	uint32_t requestedCapacity = 0;
 	uint32_t cdfMode = RB_CDF_FP64;
 	uint32_t failedMode = RB_FAILED_DROP;
+	// fault injection (rb_config.inject_*; tests only)
+	uint32_t injectQueueLimit = 0, injectAllocFailure = 0, injectStackLimit = 0;
+	uint64_t allocCount = 0;                    // device allocations made so far
 	void* envScratch = nullptr;                 // CDF scratch of the current map (in envBufs)
 	float* envIntegral = nullptr;               // device scalar (in envBufs)
 	double4* accum = nullptr;
@@ -131,11 +134,24 @@ void freeAll(std::vector<void*>& bufs)
 	bufs.clear();
 }
 // Allocates and uploads `bytes` from host `src` (may be null: zero fill).
+// Every device allocation of a context goes through here, so that a test can
+// make the n-th one fail (rb_config.inject_alloc_failure) the way an
+// exhausted device would.
+cudaError_t devMalloc(rb_ctx* ctx, void** p, size_t bytes)
+{
+	++ctx->allocCount;
+	if (ctx->injectAllocFailure && ctx->allocCount == ctx->injectAllocFailure)
+	{
+		*p = nullptr;
+		return cudaErrorMemoryAllocation;
+	}
+	return cudaMalloc(p, bytes);
+}
 template<typename T>
 int upload(rb_ctx* ctx, std::vector<void*>& owner, const void* src, size_t bytes, T*& out)
 {
 	void* d = nullptr;
-	cudaError_t e = cudaMalloc(&d, std::max<size_t>(bytes, 16));
+	cudaError_t e = devMalloc(ctx, &d, std::max<size_t>(bytes, 16));
 	if (e != cudaSuccess) return cudaFail(ctx, e, "cudaMalloc");
 	owner.push_back(d);
 	e = src ? cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, ctx->stream)
@@ -302,6 +318,7 @@ int ensureWave(rb_ctx* ctx, uint32_t paths)
 		rc = upload(ctx, ctx->soaBufs, nullptr, sizeof(uint32_t) * rb::kCountSlots, s.counts);
 	if (rc != RB_OK) { releaseWave(ctx); return rc; }
 	s.capacity = paths;
+	s.queueCap = ctx->injectQueueLimit ? std::min(ctx->injectQueueLimit, paths) : paths;
 	ctx->capacity = paths;
 	return RB_OK;
 }
@@ -388,13 +405,13 @@ int rb_attach_radiance_cache(rb_ctx* ctx, rb_nrc* cache, const rb_cache_params* 
 	if (P.batch > (1u << 22)) return fail(ctx, RB_ERR_INVALID, "rb_attach_radiance_cache: batch above 2^22 rows");
 	if (!ctx->cacheTally)
 	{
-		cudaError_t e = cudaMalloc(&ctx->cacheTally, 2 * sizeof(unsigned long long));
+		cudaError_t e = devMalloc(ctx, reinterpret_cast<void**>(&ctx->cacheTally), 2 * sizeof(unsigned long long));
 		if (e == cudaSuccess) e = cudaMemset(ctx->cacheTally, 0, 2 * sizeof(unsigned long long));
 		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_attach_radiance_cache");
 	}
 	if (!ctx->cacheCorr)
 	{
-		const cudaError_t e = cudaMalloc(&ctx->cacheCorr, rb::nrc::kCorrFloats * sizeof(float));
+		const cudaError_t e = devMalloc(ctx, reinterpret_cast<void**>(&ctx->cacheCorr), rb::nrc::kCorrFloats * sizeof(float));
 		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_attach_radiance_cache");
 	}
 	// the corrections are measured anew for every attached cache
@@ -458,11 +475,17 @@ int rb_create(const rb_config* config, rb_ctx** out)
 	ctx->cdfMode = config ? config->envmap_cdf_mode : RB_CDF_FP64;
 	if (config && config->failed_sample_mode > RB_FAILED_KEEP) { delete ctx; return RB_ERR_INVALID; }
 	ctx->failedMode = config ? config->failed_sample_mode : RB_FAILED_DROP;
+	if (config)
+	{
+		ctx->injectQueueLimit = config->inject_queue_limit;
+		ctx->injectAllocFailure = config->inject_alloc_failure;
+		ctx->injectStackLimit = config->inject_stack_limit;
+	}
 	cudaError_t e = cudaSetDevice(ctx->device);
 	if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
-	if (e == cudaSuccess) e = cudaMalloc(&ctx->status, 2 * sizeof(uint32_t));
+	if (e == cudaSuccess) e = devMalloc(ctx, reinterpret_cast<void**>(&ctx->status), 2 * sizeof(uint32_t));
 	if (e == cudaSuccess) e = cudaMemset(ctx->status, 0, 2 * sizeof(uint32_t));
-	if (e == cudaSuccess) e = cudaMalloc(&ctx->dyn, 2 * sizeof(uint32_t));
+	if (e == cudaSuccess) e = devMalloc(ctx, reinterpret_cast<void**>(&ctx->dyn), 2 * sizeof(uint32_t));
 	if (e != cudaSuccess)
 	{
 		const int rc = e == cudaErrorMemoryAllocation ? RB_ERR_OOM : RB_ERR_CUDA;
@@ -680,6 +703,8 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 		++instIndex;
 	}
 	const rb::WideBvh bvh = rb::buildWideBvh(world);
+	if (bvh.nodes.size() > rb::kMaxBvhNodes || bvh.maxDepth + 1 > static_cast<uint32_t>(rb::kMaxBvhDepth))
+		return fail(ctx, RB_ERR_TOO_LARGE, "rb_set_geometry: BVH beyond the traversal limits (2^24 nodes, depth 48)");
 	const size_t nt = canon.size();
 	float lo[3] = { 0.0f, 0.0f, 0.0f }, hi[3] = { 0.0f, 0.0f, 0.0f };
 	for (size_t j = 0; j < world.size(); j += 3)
@@ -740,6 +765,8 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 	G.nodeCount = static_cast<uint32_t>(bvh.nodes.size());
 	G.triCount = static_cast<uint32_t>(nt);
 	G.rootIsLeaf = bvh.rootIsLeaf ? 1u : 0u;
+	G.stackLimit = static_cast<uint32_t>(rb::kTraversalStackEntries);
+	if (ctx->injectStackLimit) G.stackLimit = std::min(ctx->injectStackLimit, G.stackLimit);
 	ctx->scene.geo = G;
 	ctx->geoEmissive = emissivePrim;
 	for (int k = 0; k < 3; ++k) { ctx->geoMin[k] = lo[k]; ctx->geoMax[k] = hi[k]; }
@@ -956,7 +983,7 @@ int rb_set_launch(rb_ctx* ctx, const rb_launch* l)
 		if (ctx->accum) cudaFree(ctx->accum);
 		ctx->accum = nullptr;
 		ctx->accumPixels = 0;
-		const cudaError_t e = cudaMalloc(&ctx->accum, sizeof(double4) * pixels);
+		const cudaError_t e = devMalloc(ctx, reinterpret_cast<void**>(&ctx->accum), sizeof(double4) * pixels);
 		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_set_launch: accumulation buffer");
 		cudaMemsetAsync(ctx->accum, 0, sizeof(double4) * pixels, ctx->stream);
 		ctx->accumPixels = pixels;
@@ -1069,7 +1096,7 @@ int renderWaves(rb_ctx* ctx, uint32_t offset, uint32_t count, cudaStream_t st, c
 		{
 			// answer the wave's cache queries, then train on its records
 			timedStage(ctx, 7, st, [&] {
-				rc = rb::nrc::applyQueries(ctx->cache, w.paths, soa.counts + rb::kCacheQueryCount, soa.cIn, soa.cPath,
+				rc = rb::nrc::applyQueries(ctx->cache, std::min(w.paths, soa.queueCap), soa.counts + rb::kCacheQueryCount, soa.cIn, soa.cPath,
 					soa.L, soa.T, ctx->cacheCorr, st);
 			});
 			if (rc != RB_OK) return fail(ctx, rc, "rb_render: cache queries");
@@ -1296,7 +1323,7 @@ int rb_resolve(rb_ctx* ctx, const float colorspace[9], float exposure_scale, voi
 		if (ctx->image) cudaFree(ctx->image);
 		ctx->image = nullptr;
 		ctx->imagePixels = 0;
-		const cudaError_t e = cudaMalloc(&ctx->image, sizeof(uint32_t) * ctx->accumPixels);
+		const cudaError_t e = devMalloc(ctx, reinterpret_cast<void**>(&ctx->image), sizeof(uint32_t) * ctx->accumPixels);
 		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_resolve: image buffer");
 		ctx->imagePixels = ctx->accumPixels;
 	}
@@ -1368,7 +1395,7 @@ int rb_set_stats(rb_ctx* ctx, uint32_t mode)
 	cudaSetDevice(ctx->device);
 	if ((mode & RB_STATS_COUNT) && !ctx->counters)
 	{
-		const cudaError_t e = cudaMalloc(&ctx->counters, 7 * sizeof(unsigned long long));
+		const cudaError_t e = devMalloc(ctx, reinterpret_cast<void**>(&ctx->counters), 7 * sizeof(unsigned long long));
 		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_set_stats");
 		cudaMemset(ctx->counters, 0, 7 * sizeof(unsigned long long));
 	}

@@ -341,8 +341,9 @@ constexpr float kLambdaMin = 360.0f, kLambdaMax = 830.0f;
 // (summed spread)^2 > c a0 at a surface rough enough to cache (queued as a
 // query; returns true); a training path records the vertex (inputs,
 // radiance so far, throughput) instead.
-RB_D bool cacheVertex(const PathSoA& s, const WaveParams& w, uint32_t p, uint32_t& flags, const f3& rayO,
-	const f3& rayD, float bxdfPdf, const f3& hitPos, const f3& gn, const f3& nrm, float lambda0, bool rough)
+RB_D bool cacheVertex(const PathSoA& s, const WaveParams& w, uint32_t* status, uint32_t p, uint32_t& flags,
+	const f3& rayO, const f3& rayD, float bxdfPdf, const f3& hitPos, const f3& gn, const f3& nrm, float lambda0,
+	bool rough)
 {
 	const f3 toHit = hitPos - rayO;
 	const float d2 = dot(toHit, toHit);
@@ -364,9 +365,12 @@ RB_D bool cacheVertex(const PathSoA& s, const WaveParams& w, uint32_t p, uint32_
 	in[9] = (lambda0 - kLambdaMin) / (kLambdaMax - kLambdaMin);
 	if (terminate)
 	{
-		const uint32_t q = appendIndex(s.counts + kCacheQueryCount);
-		s.cPath[q] = p | ((flags & kPathLitPrefix) ? kLitPrefixBit : 0u);
-		for (int k = 0; k < kNrcInputs; ++k) s.cIn[static_cast<size_t>(kNrcInputs) * q + k] = in[k];
+		const uint32_t q = appendSlot(s.counts + kCacheQueryCount, s.queueCap, status);
+		if (q != kNoSlot)
+		{
+			s.cPath[q] = p | ((flags & kPathLitPrefix) ? kLitPrefixBit : 0u);
+			for (int k = 0; k < kNrcInputs; ++k) s.cIn[static_cast<size_t>(kNrcInputs) * q + k] = in[k];
+		}
 		return true;
 	}
 	// a training path's vertex where the cache would have ended it: the
@@ -395,7 +399,7 @@ RB_D bool cacheVertex(const PathSoA& s, const WaveParams& w, uint32_t p, uint32_
 __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevScene sc, PathSoA s, WaveParams w, int bounce,
 	unsigned long long* counters)
 {
-	const uint32_t n = s.counts[bounce];
+	const uint32_t n = min(s.counts[bounce], s.queueCap);
 	const uint32_t* queue = s.queue[bounce & 1];
 	uint32_t* surfCount = s.counts + kSurfaceCounts + bounce;
 	uint32_t records = 0;
@@ -454,12 +458,15 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 			}
 			if (!noEmission && deferTree)
 			{
-				const uint32_t slot = appendIndex(s.counts + kEmissionCounts + bounce);
-				s.emQueue[slot] = p;
-				s.emA[slot] = f4_of(rayO, bxdfPdf);
-				s.emB[slot] = f4_of(lastNormal, lightPdf);
-				s.emC[slot] = f4(Le);
-				s.emLight[slot] = it.lightIndex;
+				const uint32_t slot = appendSlot(s.counts + kEmissionCounts + bounce, s.queueCap, sc.status);
+				if (slot != kNoSlot)
+				{
+					s.emQueue[slot] = p;
+					s.emA[slot] = f4_of(rayO, bxdfPdf);
+					s.emB[slot] = f4_of(lastNormal, lightPdf);
+					s.emC[slot] = f4(Le);
+					s.emLight[slot] = it.lightIndex;
+				}
 			}
 			else if (!noEmission)
 			{
@@ -487,7 +494,7 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 					const Surface sf = surfaceOf(mat);
 					const bool rough = (sf.metalness == 0.0f && sf.transmission == 0.0f) || sf.roughness >= w.minRoughness;
 					if (depth == 0 && it.lightType == kLightTypeTriangle) flags |= kPathLitPrefix;
-					if (cacheVertex(s, w, p, flags, rayO, rayD, bxdfPdf, it.hitPos, it.gn, lastNormal,
+					if (cacheVertex(s, w, sc.status, p, flags, rayO, rayD, bxdfPdf, it.hitPos, it.gn, lastNormal,
 							s.lambda[p].x, rough))
 					{
 						s.fd[p] = make_uint2(flags | PF_FINISHED, depth);
@@ -507,7 +514,8 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 			s.sfT[p] = f4_of(frame.t, 0.0f);
 			s.sfB[p] = f4_of(frame.b, 0.0f);
 			s.nrm[p] = f4_of(lastNormal, nv.w);
-			s.surfQueue[appendIndex(surfCount)] = p;
+			const uint32_t slot = appendSlot(surfCount, s.queueCap, sc.status);
+			if (slot != kNoSlot) s.surfQueue[slot] = p;
 			++records;
 		}
 		else if (w.cached && s.trainRec[p] != kNotTraining)
@@ -525,7 +533,7 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 // values kSurface queued for it; the same arithmetic as the inline case.
 __global__ void __launch_bounds__(kThreads) kEmission(DevScene sc, PathSoA s, int bounce)
 {
-	const uint32_t n = s.counts[kEmissionCounts + bounce];
+	const uint32_t n = min(s.counts[kEmissionCounts + bounce], s.queueCap);
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
 		const uint32_t p = s.emQueue[i];
@@ -559,7 +567,7 @@ __global__ void __launch_bounds__(kThreads) kEmission(DevScene sc, PathSoA s, in
 // sample dimension and comparison as the light-sample body that follows.
 __global__ void __launch_bounds__(kThreads) kNeePick(DevScene sc, PathSoA s, WaveParams w, int bounce)
 {
-	const uint32_t n = s.counts[kSurfaceCounts + bounce];
+	const uint32_t n = min(s.counts[kSurfaceCounts + bounce], s.queueCap);
 	const bool envPresent = sc.env.enabled != 0;
 	const bool treePresent = sc.lights.nodes != nullptr;
 	const float envImp = envPresent ? (treePresent ? kEnvMapImportance : 1.0f) : 0.0f;
@@ -574,8 +582,16 @@ __global__ void __launch_bounds__(kThreads) kNeePick(DevScene sc, PathSoA s, Wav
 			sky = sample3D(q, DIM_LIGHT).z < envImp;
 		}
 		// one counter per branch: appendIndex aggregates over the lanes active at the call
-		if (sky) s.neeQueue[1][appendIndex(s.counts + kNeeSkyCounts + bounce)] = p;
-		else s.neeQueue[0][appendIndex(s.counts + kNeeTreeCounts + bounce)] = p;
+		if (sky)
+		{
+			const uint32_t slot = appendSlot(s.counts + kNeeSkyCounts + bounce, s.queueCap, sc.status);
+			if (slot != kNoSlot) s.neeQueue[1][slot] = p;
+		}
+		else
+		{
+			const uint32_t slot = appendSlot(s.counts + kNeeTreeCounts + bounce, s.queueCap, sc.status);
+			if (slot != kNoSlot) s.neeQueue[0][slot] = p;
+		}
 	}
 }
 
@@ -593,7 +609,7 @@ __global__ void __launch_bounds__(SHARED ? kNeeSharedThreads : kThreads, SHARED 
 kNee(DevScene sc, PathSoA s, WaveParams w, int bounce, int which)
 {
 	extern __shared__ float4 sharedTree[];
-	const uint32_t n = s.counts[(which ? kNeeSkyCounts : kNeeTreeCounts) + bounce];
+	const uint32_t n = min(s.counts[(which ? kNeeSkyCounts : kNeeTreeCounts) + bounce], s.queueCap);
 	const uint32_t* queue = s.neeQueue[which];
 	const TreeNodeU* nodes = sc.lights.unpacked;
 	if (SHARED)
@@ -686,7 +702,7 @@ kNee(DevScene sc, PathSoA s, WaveParams w, int bounce, int which)
 // BxDF sample (stage 3b) so neither kernel holds both parts' registers.
 __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdfLight(DevScene sc, PathSoA s, WaveParams w, int bounce)
 {
-	const uint32_t n = s.counts[kSurfaceCounts + bounce];
+	const uint32_t n = min(s.counts[kSurfaceCounts + bounce], s.queueCap);
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
 		const uint32_t p = s.surfQueue[i];
@@ -721,7 +737,7 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdfLight(DevSc
 // light samples that passed stage 3a to the shadow queue.
 __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(DevScene sc, PathSoA s, WaveParams w, int bounce)
 {
-	const uint32_t n = s.counts[kSurfaceCounts + bounce];
+	const uint32_t n = min(s.counts[kSurfaceCounts + bounce], s.queueCap);
 	uint32_t* nextQueue = s.queue[(bounce + 1) & 1];
 	uint32_t* nextCount = s.counts + bounce + 1;
 	uint32_t* shadowCount = s.counts + kShadowCounts + bounce;
@@ -816,8 +832,16 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(DevScene s
 		s.fd[p] = make_uint2(flags, depth);
 		s.rayO[p] = f4_of(rayO, refrScale);
 		s.rayD[p] = f4_of(rayD, st.pdf);
-		if (hasShadow) s.shadowQueue[appendIndex(shadowCount)] = p;
-		if (!done) nextQueue[appendIndex(nextCount)] = p;
+		if (hasShadow)
+		{
+			const uint32_t slot = appendSlot(shadowCount, s.queueCap, sc.status);
+			if (slot != kNoSlot) s.shadowQueue[slot] = p;
+		}
+		if (!done)
+		{
+			const uint32_t slot = appendSlot(nextCount, s.queueCap, sc.status);
+			if (slot != kNoSlot) nextQueue[slot] = p;
+		}
 	}
 }
 

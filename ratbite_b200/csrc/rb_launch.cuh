@@ -3,6 +3,7 @@
 
 #include <cstdint>
 
+#include "ratbite_b200.h"
 #include "rb_math.cuh"
 
 namespace rb
@@ -24,6 +25,17 @@ RB_D uint32_t appendIndex(uint32_t* counter)
 	if (lane == static_cast<uint32_t>(leader)) base = atomicAdd(counter, __popc(active));
 	base = __shfl_sync(active, base, leader);
 	return base + __popc(active & ((1u << lane) - 1u));
+}
+
+// Queue slot of one entry, or kNoSlot when the queue already holds `cap`
+// entries: the entry is dropped and RB_DEV_QUEUE_OVERFLOW set in *status.
+constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
+RB_D uint32_t appendSlot(uint32_t* counter, uint32_t cap, uint32_t* status)
+{
+	const uint32_t i = appendIndex(counter);
+	if (i < cap) return i;
+	atomicOr(status, RB_DEV_QUEUE_OVERFLOW);
+	return kNoSlot;
 }
 
 // Adds per-thread counts to a 64-bit counter with one atomic per warp.

@@ -69,11 +69,13 @@ __global__ void kRefitLevel(const uint32_t* __restrict__ order, uint32_t begin, 
 	{
 		const uint32_t i = order[k];
 		BvhNode node = nodes[i];
-		const int n = node.childCount;
+		uint32_t slots = 0;
 		double lo[8][3], hi[8][3];
-		for (int c = 0; c < n; ++c)
+		for (int c = 0; c < 8; ++c)
 		{
 			const uint32_t ref = node.child[c];
+			if (ref == kEmptyChild) continue;
+			slots |= 1u << c;
 			if (ref & kLeafBit)
 			{
 				const uint32_t first = ref & 0x0FFFFFFFu;
@@ -94,13 +96,14 @@ __global__ void kRefitLevel(const uint32_t* __restrict__ order, uint32_t begin, 
 				for (int a = 0; a < 3; ++a) { lo[c][a] = bx[a]; hi[c][a] = bx[3 + a]; }
 			}
 		}
-		quantizeChildren(n, lo, hi, node);
+		quantizeChildren(slots, lo, hi, node);
 		nodes[i] = node;
 		double* me = nodeBox + 6u * i;
 		for (int a = 0; a < 3; ++a)
 		{
-			double l = lo[0][a], h = hi[0][a];
-			for (int c = 1; c < n; ++c) { l = fmin(l, lo[c][a]); h = fmax(h, hi[c][a]); }
+			double l = INFINITY, h = -INFINITY;
+			for (int c = 0; c < 8; ++c)
+				if ((slots >> c) & 1u) { l = fmin(l, lo[c][a]); h = fmax(h, hi[c][a]); }
 			me[a] = l;
 			me[3 + a] = h;
 		}

@@ -97,6 +97,12 @@ static_assert(sizeof(BvhNode) == 96, "BVH node is 96 B");
 constexpr uint32_t kLeafBit = 0x80000000u;
 constexpr uint32_t kEmptyChild = 0xFFFFFFFFu;
 constexpr int kLeafMaxTris = 4;
+// Limits of the traversal's node-group stack entries (24-bit node index) and
+// depth (one entry per level); rb_set_geometry rejects trees beyond them.
+constexpr uint32_t kMaxBvhNodes = 1u << 24;
+constexpr int kMaxBvhDepth = 48;
+// Entries of a ray's traversal stack (one per entered child still owed).
+constexpr int kTraversalStackEntries = 64;
 
 // Per-triangle hit data in BVH leaf order. v[0..2] are the world-space
 // vertices; their w lanes carry the canonical triangle id (v0.w), the
@@ -111,7 +117,7 @@ struct DevGeometry
 	uint32_t nodeCount;
 	uint32_t triCount;
 	uint32_t rootIsLeaf;         // scenes of <= kLeafMaxTris triangles
-	uint32_t pad;
+	uint32_t stackLimit;         // traversal stack entries in use (kTraversalStackEntries unless injected)
 };
 
 // A light-tree node unpacked for the descent (48 B): mean and variance,

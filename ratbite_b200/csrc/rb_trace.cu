@@ -18,12 +18,22 @@ namespace
 // Node / leaf visits per step of the persistent loop, and the number of idle
 // lanes at which the warp fetches new rays (all lanes idle always fetches).
 // On B200, at-scale frame (extension ms): 16 / 1 (the default) 442; 2 / 8
-// 433 (but shadow 75 -> 86); 1 / 8 448; 4 / 8 709; 8 / 8 1185.
+// 433 (but shadow 75 -> 86); 1 / 8 448; 4 / 8 709; 8 / 8 1185. Measured
+// with an instrumented build: a refill (warp atomic, queue slot and ray
+// loads) takes about 4.8k of the 80k cycles of a 16-visit step, and 75 % of
+// the lane-visit slots of a step do work. Staging each lane's next ray in
+// shared memory with cp.async while it traces the current one (indices
+// claimed 64 per atomic) was slower: extension 397 -> 483 ms.
 #ifndef RB_STEP_BUDGET
 #define RB_STEP_BUDGET 16
 #endif
 #ifndef RB_REFILL_LANES
 #define RB_REFILL_LANES 1
+#endif
+// Resident blocks of 128 per SM the traversal kernels are compiled for
+// (register cap 65536 / (128 x blocks)).
+#ifndef RB_TRACE_MIN_BLOCKS
+#define RB_TRACE_MIN_BLOCKS 8
 #endif
 constexpr int kStepBudget = RB_STEP_BUDGET;
 constexpr int kRefillLanes = RB_REFILL_LANES;
@@ -65,26 +75,26 @@ RB_D void persistentTraversal(uint32_t n, uint32_t* workCounter, Begin&& begin, 
 
 // counters (COUNT only): [0] rays, [1] nodes, [2] triangles.
 template<bool COUNT>
-__global__ void __launch_bounds__(kThreads) kExtend(DevScene sc, PathSoA s, int bounce, unsigned long long* counters)
+__global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kExtend(DevScene sc, PathSoA s, int bounce, unsigned long long* counters)
 {
-	const uint32_t n = s.counts[bounce];
+	const uint32_t n = min(s.counts[bounce], s.queueCap);
 	const uint32_t* q = s.queue[bounce & 1];
 	uint32_t rays = 0, nodes = 0, tris = 0;
 	uint32_t p = 0;
 	ClosestTraversal tr;
 	uint2 stack[kTraversalStack];
+	auto step = [&]() {
+		if (!tr.template run<COUNT>(sc.geo, kStepBudget, sc.status, nodes, tris, stack)) return false;
+		s.hit[p] = make_float4(__int_as_float(tr.best.tri), tr.best.t, tr.best.b1, tr.best.b2);
+		return true;
+	};
 	persistentTraversal<ClosestTraversal>(n, s.counts + kExtendFetch + bounce,
 		[&](uint32_t idx) {
 			p = q[idx];
 			const float4 o = s.rayO[p], d = s.rayD[p];
 			tr.init(sc.geo, f3_of(o), f3_of(d), 0.0f, FLT_MAX);
 			++rays;
-		},
-		[&]() {
-			if (!tr.template run<COUNT>(sc.geo, kStepBudget, sc.status, nodes, tris, stack)) return false;
-			s.hit[p] = make_float4(__int_as_float(tr.best.tri), tr.best.t, tr.best.b1, tr.best.b2);
-			return true;
-		});
+		}, step);
 	if (COUNT)
 	{
 		warpAdd(counters + 0, rays);
@@ -94,30 +104,30 @@ __global__ void __launch_bounds__(kThreads) kExtend(DevScene sc, PathSoA s, int 
 }
 
 template<bool COUNT>
-__global__ void __launch_bounds__(kThreads) kShadow(DevScene sc, PathSoA s, int bounce, unsigned long long* counters)
+__global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kShadow(DevScene sc, PathSoA s, int bounce, unsigned long long* counters)
 {
-	const uint32_t n = s.counts[kShadowCounts + bounce];
+	const uint32_t n = min(s.counts[kShadowCounts + bounce], s.queueCap);
 	uint32_t rays = 0, nodes = 0, tris = 0;
 	uint32_t p = 0;
 	AnyTraversal tr;
 	uint32_t stack[kTraversalStack];
+	auto step = [&]() {
+		if (!tr.template run<COUNT>(sc.geo, kStepBudget, sc.status, nodes, tris, stack)) return false;
+		if (!tr.hit)
+		{
+			S4 L = s4(s.L[p]);
+			L += s4(s.shC[p]);
+			s.L[p] = f4(L);
+		}
+		return true;
+	};
 	persistentTraversal<AnyTraversal>(n, s.counts + kShadowFetch + bounce,
 		[&](uint32_t idx) {
 			p = s.shadowQueue[idx];
 			const float4 o = s.shO[p], d = s.shD[p];
 			tr.init(sc.geo, f3_of(o), f3_of(d), 0.0f, o.w);
 			++rays;
-		},
-		[&]() {
-			if (!tr.template run<COUNT>(sc.geo, kStepBudget, sc.status, nodes, tris, stack)) return false;
-			if (!tr.hit)
-			{
-				S4 L = s4(s.L[p]);
-				L += s4(s.shC[p]);
-				s.L[p] = f4(L);
-			}
-			return true;
-		});
+		}, step);
 	if (COUNT)
 	{
 		warpAdd(counters + 3, rays);

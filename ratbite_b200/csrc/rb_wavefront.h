@@ -46,6 +46,10 @@ struct PathSoA
 	uint32_t* shadowQueue;
 	uint32_t* counts;  // kCountSlots words: see kShadowCounts, kSurfaceCounts
 	uint32_t capacity;
+	// entries a queue accepts per bounce (capacity, or the injected limit of
+	// rb_config.inject_queue_limit); an append beyond it is dropped with
+	// RB_DEV_QUEUE_OVERFLOW, and readers take at most this many
+	uint32_t queueCap;
 	// radiance-cache form (all null without a cache): per path, the spread
 	// (primary footprint a0, summed spread) and, for training paths, the
 	// record of the current vertex (kNoRecord: none this vertex; kNotTraining

@@ -22,13 +22,17 @@ def _ptr(a: np.ndarray):
 
 class RenderingInterface:
     def __init__(self, device: int = 0, max_paths_in_flight: int = 0, envmap_cdf_mode: int = abi.RB_CDF_FP64,
-                 failed_sample_mode: int = abi.RB_FAILED_DROP):
+                 failed_sample_mode: int = abi.RB_FAILED_DROP, inject: dict | None = None):
+        """inject: fault injection for tests, keys of rb_config without the
+        `inject_` prefix (queue_limit, alloc_failure, stack_limit)."""
         self.lib = load()
         cfg = abi.rb_config()
         cfg.device = device
         cfg.max_paths_in_flight = max_paths_in_flight
         cfg.envmap_cdf_mode = envmap_cdf_mode
         cfg.failed_sample_mode = failed_sample_mode
+        for k, v in (inject or {}).items():
+            setattr(cfg, f"inject_{k}", int(v))
         h = C.c_void_p()
         check(self.lib.rb_create(C.byref(cfg), C.byref(h)), None, "rb_create")
         self.ctx = h

@@ -176,3 +176,99 @@ def test_rejections_leave_the_context_usable(tables):
     assert np.all(acc[..., 3] == 2.0) and acc[..., :3].sum() > 0
     assert ri.status().flags == 0
     ri.cleanup()
+
+
+# ------------------------------------------------ failure detection (host-side injection)
+def _cornell(tables, W=24, H=24, spp=4):
+    sc = scenes.cornell_box(seed=1, cie_xyz=tables["cie"], width=W, height=H, spp=spp)
+    return sc, lighttree.build_for_scene(sc)
+
+
+def _render(tables, sc, lt, spp, **kw):
+    with RenderingInterface(device=0, **kw) as ri:
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lt)
+        ri.render(0, spp)
+        return ri.read_accumulation(), ri.status().flags
+
+
+def test_small_wavefront_capacity_renders_identically(tables):
+    """A wavefront of 1,000 paths (the frame's 18,432 paths then take 19
+    waves) gives the accumulation of the default capacity, bit for bit."""
+    sc, lt = _cornell(tables, 48, 48, 8)
+    want, f0 = _render(tables, sc, lt, 8)
+    got, f1 = _render(tables, sc, lt, 8, max_paths_in_flight=1000)
+    assert f0 == 0 and f1 == 0
+    assert np.array_equal(got, want)
+
+
+def test_injected_queue_limit_sets_the_overflow_flag(tables):
+    """Queues that accept only 64 entries per bounce: appends beyond drop
+    their entry and raise RB_DEV_QUEUE_OVERFLOW; nothing is written out of
+    bounds, every pixel still counts its samples, and the context renders
+    again."""
+    sc, lt = _cornell(tables)
+    with RenderingInterface(device=0, inject={"queue_limit": 64}) as ri:
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lt)
+        ri.render(0, 4)
+        acc = ri.read_accumulation()
+        flags = ri.status().flags
+        assert flags & abi.RB_DEV_QUEUE_OVERFLOW
+        assert np.isfinite(acc).all() and (acc[..., 3] == 4).all()
+        ri.render(0, 1)
+        assert np.isfinite(ri.read_accumulation()).all()
+
+
+def test_injected_stack_limit_sets_the_overflow_flag(tables):
+    """A traversal stack of one entry cannot hold the children a ray owes at
+    an 8-wide node: RB_DEV_STACK_OVERFLOW is raised, the render completes."""
+    sc, lt = _cornell(tables)
+    acc, flags = _render(tables, sc, lt, 4, inject={"stack_limit": 1})
+    assert flags & abi.RB_DEV_STACK_OVERFLOW
+    assert np.isfinite(acc).all()
+
+
+def test_non_finite_radiance_sets_its_flag(tables):
+    """An emitter of 3e38 (finite, but its samples overflow to infinity in
+    the radiance estimate) raises RB_DEV_NAN_RADIANCE."""
+    sc, lt = _cornell(tables)
+    for m in sc.materials:
+        if m.emissive:
+            m.emissive = (3e38, 3e38, 3e38)
+    _, flags = _render(tables, sc, lt, 2)
+    assert flags & abi.RB_DEV_NAN_RADIANCE
+
+
+def test_injected_allocation_failure_leaves_the_context_usable(tables):
+    """The n-th device allocation of a context fails once, for every n up to
+    the allocations of a whole load-and-render: the failing call returns an
+    error (out of memory) with a message and changes nothing, and repeating
+    the load and the render then gives the clean accumulation bit for bit."""
+    from ratbite_b200._native import NativeError
+    sc, lt = _cornell(tables)
+    want, _ = _render(tables, sc, lt, 4)
+    failures = 0
+    for n in range(1, 80):
+        try:
+            ri = RenderingInterface(device=0, inject={"alloc_failure": n})
+        except NativeError as e:
+            assert e.code == abi.RB_ERR_OOM
+            failures += 1
+            continue
+        with ri:
+            try:
+                ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lt)
+                ri.render(0, 4)
+                failed = False
+            except NativeError as e:
+                assert e.code in (abi.RB_ERR_OOM, abi.RB_ERR_CUDA)
+                assert str(e).strip()
+                failed = True
+                failures += 1
+                ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lt)
+                ri.render(0, 4)
+            got = ri.read_accumulation()
+            assert np.array_equal(got, want), n
+            assert ri.status().flags == 0
+        if not failed and n > 2:
+            break                       # n is past the last allocation
+    assert failures >= 10

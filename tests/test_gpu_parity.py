@@ -284,7 +284,7 @@ def test_bxdf_parity(ref, tables):
         assert beyond.mean() <= 0.002, f"{beyond.sum()} same-branch BxDF cases differ in {k} beyond 1e-5"
         bad = beyond & (r > spread[k])
         if beyond.any():
-            print(f"bxdf {k}: {beyond.sum()} cases beyond 1e-5, rel diff / oracle one-ulp spread: "
+            print(f"bxdf {k}: {beyond.sum()} cases beyond 1e-5, rel diff / oracle libm-jitter spread: "
                   f"max {np.max(r[beyond] / np.maximum(spread[k][beyond], 1e-30)):.2f}")
         for i in np.flatnonzero(beyond)[:5]:
             print(f"  {k} case {i} material {cs[i].material} roughness {cs[i].roughness:.4g}: rel {r[i]:.3e}, "
