@@ -35,6 +35,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import subprocess
 import sys
@@ -599,16 +600,23 @@ def run_batched(args):
 
 def time_to_rmse(device: int = 0, width: int = 1920, height: int = 1080, depth: int = 12, ref_spp: int = 4096,
                  plain_spp: int = 1024, chunk: int = 32, failed_mode: int = 0, cache_kw: dict | None = None,
-                 time_factor: float = 2.0):
+                 time_factor: float = 2.0, repeats: int = 3):
     """The cached form against the plain tracer on the Cornell box at
     width x height, depth `depth`: device seconds until each reaches the
-    plain tracer's plain_spp RMSE against a ref_spp plain oracle (FP64
-    accumulation, sample indices disjoint from both runs). RMSE is taken on
-    the linear XYZ mean image, relative to the oracle's mean, between chunks
-    and outside the timed spans. Both runs get one untimed warm-up chunk
-    (first-launch costs and buffer allocation); the cached form then starts
-    from an untrained cache and stops at the target or at time_factor x the
-    plain tracer's time."""
+    plain tracer's plain_spp RMSE against the FP64 oracle.
+
+    Oracle: two independent plain renders of ref_spp samples each (FP64
+    accumulation, sample indices disjoint from each other and from every
+    timed run), averaged; the oracle's own noise, estimated per pixel from
+    the two halves (E[(A - B)^2] / 4 is the variance of their mean), is
+    subtracted from every mean squared error, so the RMSEs compared are those
+    against the converged image. RMSE is taken on the linear XYZ mean image,
+    relative to the oracle's mean, between chunks and outside the timed
+    spans. The comparison runs `repeats` times (different sample ranges, a
+    fresh untrained cache with a different seed each time); the line reports
+    every ratio and their median. Both forms get one untimed warm-up chunk
+    per run (first-launch costs and buffer allocation); the cached form stops
+    at the target or at time_factor x the plain tracer's time."""
     import torch
     from ratbite_b200 import lighttree, scenes
     from ratbite_b200.nrc import RadianceCache
@@ -628,12 +636,25 @@ def time_to_rmse(device: int = 0, width: int = 1920, height: int = 1080, depth: 
         acc = torch.from_numpy(ri.read_accumulation().reshape(n, 4)).cuda()
         return acc[:, :3] / acc[:, 3:4].clamp_min(1.0)
 
-    ri.render(1 << 20, ref_spp, stream=sp)
-    ref = mean_image()
+    ri.clear_accumulation(stream=sp)
+    ri.render(1 << 24, ref_spp, stream=sp)
+    half_a = mean_image()
+    ri.clear_accumulation(stream=sp)
+    ri.render((1 << 24) + ref_spp, ref_spp, stream=sp)
+    half_b = mean_image()
+    ref = 0.5 * (half_a + half_b)
     ref_mean = float(ref.mean())
+    ref_noise = float(((half_a - half_b) ** 2).mean() / 4.0)       # per-pixel variance of the mean, averaged
+    # pixels that see the emitter directly: the brightest 0.5 % of the oracle
+    lum = ref[:, 1]
+    lit = lum >= torch.quantile(lum[::97].float(), 0.995)
 
     def rel_rmse(img):
-        return float(torch.sqrt(((img - ref) ** 2).mean()) / ref_mean)
+        mse = float(((img - ref) ** 2).mean()) - ref_noise
+        return math.sqrt(max(mse, 0.0)) / ref_mean
+
+    def biases(img):
+        return (float(img.mean() / ref.mean() - 1.0), float(img[lit].mean() / ref[lit].mean() - 1.0))
 
     def timed(offset, count):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -643,49 +664,71 @@ def time_to_rmse(device: int = 0, width: int = 1920, height: int = 1080, depth: 
         b.synchronize()
         return a.elapsed_time(b) / 1e3
 
-    ri.render(0, chunk, stream=sp)
-    plain_curve, t = [], 0.0
-    for k in range(plain_spp // chunk):
-        t += timed(k * chunk, chunk)
-        plain_curve.append(((k + 1) * chunk, t, rel_rmse(mean_image())))
-    target, t_plain = plain_curve[-1][2], plain_curve[-1][1]
-
+    runs = []
     kw = dict(cache_kw or {})
-    scratch = RadianceCache(device=device, seed=99)
-    ri.attach_radiance_cache(scratch, **kw)
-    ri.render(1 << 22, chunk, stream=sp)          # warm-up: sizes the cache's wave buffers
-    cache = RadianceCache(device=device, seed=2)
-    ri.attach_radiance_cache(cache, **kw)
-    ri.cache_stats()
-    cached_curve, t, done, reached = [], 0.0, 0, None
-    while t < time_factor * t_plain:
-        t += timed(done, chunk)
-        done += chunk
-        r = rel_rmse(mean_image())
-        cached_curve.append((done, t, r))
-        if r <= target:
-            reached = t
-            break
-    st = ri.cache_stats()
+    for rep in range(repeats):
+        base = rep << 20                        # disjoint sample ranges per repetition
+        ri.attach_radiance_cache(None)
+        ri.clear_accumulation(stream=sp)
+        ri.render(base + (1 << 19), chunk, stream=sp)                    # warm-up
+        ri.clear_accumulation(stream=sp)
+        plain_curve, t = [], 0.0
+        for k in range(plain_spp // chunk):
+            t += timed(base + k * chunk, chunk)
+            plain_curve.append(((k + 1) * chunk, t, rel_rmse(mean_image())))
+        target, t_plain = plain_curve[-1][2], plain_curve[-1][1]
+        plain_bias = biases(mean_image())
+
+        scratch = RadianceCache(device=device, seed=1000 + rep)
+        ri.attach_radiance_cache(scratch, **kw)
+        ri.clear_accumulation(stream=sp)
+        ri.render(base + (1 << 19) + chunk, chunk, stream=sp)            # warm-up: sizes the cache's wave buffers
+        cache = RadianceCache(device=device, seed=2 + rep)
+        ri.attach_radiance_cache(cache, **kw)
+        ri.cache_stats()
+        ri.clear_accumulation(stream=sp)
+        cached_curve, t, done, reached = [], 0.0, 0, None
+        while t < time_factor * t_plain:
+            t += timed(base + (1 << 18) + done, chunk)
+            done += chunk
+            r = rel_rmse(mean_image())
+            cached_curve.append((done, t, r))
+            if r <= target:
+                reached = t
+                break
+        st = ri.cache_stats()
+        cached_bias = biases(mean_image())
+        ri.attach_radiance_cache(None)
+        cache.close()
+        scratch.close()
+        best = min(cached_curve, key=lambda c: c[2])
+        runs.append({
+            "plain": {"spp": plain_spp, "s": t_plain, "rel_rmse": target, "paths_per_s": n * plain_spp / t_plain,
+                      "bias_image": plain_bias[0], "bias_lit_pixels": plain_bias[1]},
+            "cached": {"s_to_target": reached, "spp_to_target": done if reached else None,
+                       "best_rel_rmse": best[2], "best_at_spp": best[0], "spp_rendered": done, "s_rendered": t,
+                       "paths_per_s": n * done / t, "queries_per_sample": st.queries / max(1, done),
+                       "records_per_sample": st.records / max(1, done), "train_steps": st.steps,
+                       "last_loss": st.last_loss, "bias_image": cached_bias[0], "bias_lit_pixels": cached_bias[1]},
+            "time_ratio": (reached / t_plain) if reached else None,
+            "plain_curve": [(a, round(b, 4), round(c, 5)) for a, b, c in plain_curve[::max(1, len(plain_curve) // 6)]],
+            "cached_curve": [(a, round(b, 4), round(c, 5)) for a, b, c in cached_curve[::max(1, len(cached_curve) // 6)]],
+        })
     ri.cleanup()
-    cache.close()
-    scratch.close()
-    best = min(cached_curve, key=lambda c: c[2])
-    at_plain_time = min((c for c in cached_curve if c[1] <= t_plain), key=lambda c: c[2], default=None)
+    ratios = [r["time_ratio"] for r in runs]
+    done_ratios = sorted(x if x is not None else float("inf") for x in ratios)
+    med = done_ratios[len(done_ratios) // 2]
     return {
         "workload": f"cornell_box_{width}x{height}_depth{depth}",
-        "rmse": f"relative RMSE of the XYZ mean image vs a {ref_spp}-spp FP64-accumulated plain render",
+        "rmse": (f"relative RMSE of the XYZ mean image vs the mean of two {ref_spp}-spp FP64-accumulated plain "
+                 f"renders, the oracle's own noise ({math.sqrt(ref_noise) / ref_mean:.4f} relative) subtracted"),
         "failed_sample_mode": "keep" if failed_mode else "drop (reference)",
-        "plain": {"spp": plain_spp, "s": t_plain, "rel_rmse": target, "paths_per_s": n * plain_spp / t_plain},
-        "cached": {"s_to_target": reached, "spp_to_target": done if reached else None,
-                   "best_rel_rmse": best[2], "best_at_spp": best[0],
-                   "rel_rmse_at_plain_time": at_plain_time[2] if at_plain_time else None,
-                   "spp_rendered": done, "s_rendered": t, "paths_per_s": n * done / t,
-                   "queries_per_sample": st.queries / max(1, done), "records_per_sample": st.records / max(1, done),
-                   "train_steps": st.steps, "last_loss": st.last_loss, "params": kw or "library defaults"},
-        "time_ratio": (reached / t_plain) if reached else None,
-        "plain_curve": [(a, round(b, 4), round(c, 5)) for a, b, c in plain_curve[::max(1, len(plain_curve) // 8)]],
-        "cached_curve": [(a, round(b, 4), round(c, 5)) for a, b, c in cached_curve[::max(1, len(cached_curve) // 8)]],
+        "params": kw or "library defaults",
+        "repeats": repeats,
+        "time_ratios": ratios,
+        "time_ratio": med if math.isfinite(med) else None,
+        "time_ratio_spread": [done_ratios[0], done_ratios[-1]] if all(map(math.isfinite, done_ratios)) else None,
+        "runs": runs,
     }
 
 

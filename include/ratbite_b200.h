@@ -260,6 +260,16 @@ int rb_update_instances(rb_ctx* ctx, const float* instance_transforms, const flo
  * bitmasks. The triangle vertices and node means are taken relative to the
  * light origin (rb_set_light_origin; 0 until set, which uses them as given). */
 int rb_set_lights(rb_ctx* ctx, const rb_light_tree* tree);
+/* Builds the light tree on the device from emissive triangles in device
+ * memory (world: 9 floats each, flux, material, primitive; the inputs
+ * rb_build_light_tree takes, origin-independent) and installs it as
+ * rb_set_lights installs host-built records, the light origin of
+ * rb_set_light_origin applied. No reference counterpart: the reference
+ * rebuilds on the host (LightTree::Builder, src/core/light_tree.cpp:47-418)
+ * on every light change. The tree is a binned-SAOH tree in the reference's
+ * layouts (rb_k_build_light_tree). Synchronizes. */
+int rb_build_lights(rb_ctx* ctx, uint32_t n, const float* world, const float* flux, const uint32_t* material,
+                    const uint32_t* primitive, void* stream);
 /* The camera-move refresh of the light data on the device (the reference's
  * fillLightDataBuffer and fillLightTreeDataBuffers,
  * src/core/rendering_interface.cpp:1433-1510, run on CHANGE_CAMERA_POS

@@ -55,6 +55,11 @@ int rb_nrc_infer(rb_nrc* nrc, uint32_t n, const float* inputs, float* outputs, v
 int rb_nrc_train(rb_nrc* nrc, uint32_t n, const float* inputs, const float* targets, float* loss_out,
                  void* stream);
 
+/* RB_DEV_* bits raised by the network's kernels since the handle was created
+ * (RB_DEV_ITERATION_LIMIT: a tensor-core wait gave up and its tile was
+ * skipped); synchronizes. No reference counterpart. */
+int rb_nrc_status(rb_nrc* nrc, uint32_t* flags);
+
 /* The gradients of the batch's mean loss with respect to the FP32 master
  * parameters (grid and weights, host buffers of the sizes above), without an
  * optimiser step; synchronizes. For checking the backward pass. */

@@ -875,6 +875,84 @@ int rb_set_lights(rb_ctx* ctx, const rb_light_tree* t)
 	return RB_OK;
 }
 
+int rb_build_lights(rb_ctx* ctx, uint32_t n, const float* world, const float* flux, const uint32_t* material,
+	const uint32_t* primitive, void* stream)
+{
+	if (!ctx) return RB_ERR_INVALID;
+	if (n && (!world || !flux || !material || !primitive)) return fail(ctx, RB_ERR_INVALID, "rb_build_lights: null input");
+	if (n > (1u << 27) - 1u) return fail(ctx, RB_ERR_INVALID, "rb_build_lights: too many emitters");
+	cudaSetDevice(ctx->device);
+	const cudaStream_t st = pick(ctx, stream);
+	std::vector<void*> fresh;
+	rb::DevLights L{};
+	rb::EmissiveTri *worldTris = nullptr, *tris = nullptr;
+	rb::PackedNode *worldNodes = nullptr, *dn = nullptr;
+	rb::TreeNodeU* du = nullptr;
+	void* scratch = nullptr;
+	uint32_t* dCount = nullptr;
+	const size_t nodesMax = std::max<size_t>(2 * static_cast<size_t>(n), 1);
+	int rc = upload(ctx, fresh, nullptr, sizeof(rb::EmissiveTri) * std::max<uint32_t>(n, 1), worldTris);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(rb::EmissiveTri) * std::max<uint32_t>(n, 1), tris);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(uint64_t) * std::max<uint32_t>(n, 1), L.bitmasks);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(uint32_t) * std::max<uint32_t>(n, 1), L.pointers);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(rb::PackedNode) * nodesMax, worldNodes);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(rb::PackedNode) * nodesMax, dn);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(rb::TreeNodeU) * nodesMax, du);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, rb_k_build_light_tree_scratch_bytes(n), scratch);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(uint32_t), dCount);
+	uint32_t nodeCount = 0;
+	if (rc == RB_OK && n)
+	{
+		// origin-independent records (light origin 0), then the working copies as rb_set_lights makes them
+		cudaStreamSynchronize(ctx->stream);
+		const double zero[3] = { 0.0, 0.0, 0.0 };
+		rc = rb_k_build_light_tree(n, world, flux, material, primitive, zero, scratch, worldTris, worldNodes,
+			const_cast<uint32_t*>(L.pointers), const_cast<uint64_t*>(L.bitmasks), dCount, st);
+		if (rc != RB_OK) rc = fail(ctx, rc, "rb_build_lights: build");
+		if (rc == RB_OK && cudaMemcpyAsync(&nodeCount, dCount, sizeof(uint32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+			rc = fail(ctx, RB_ERR_CUDA, "rb_build_lights: node count");
+		if (rc == RB_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = fail(ctx, RB_ERR_CUDA, "rb_build_lights: build");
+		if (rc == RB_OK && (nodeCount == 0 || nodeCount > nodesMax)) rc = fail(ctx, RB_ERR_CUDA, "rb_build_lights: bad tree");
+	}
+	if (rc == RB_OK && n)
+	{
+		rb::launchLightOrigin(worldTris, tris, n, worldNodes, dn, nodeCount, ctx->lightOrigin[0], ctx->lightOrigin[1],
+			ctx->lightOrigin[2], ctx->stream);
+		rb::launchUnpackLightTree(dn, du, nodeCount, ctx->stream);
+		const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+		if (e != cudaSuccess) rc = cudaFail(ctx, e, "rb_build_lights: install");
+	}
+	// the largest material index, for the render-time cross-table check
+	uint32_t maxMaterial = 0;
+	if (rc == RB_OK && n)
+	{
+		std::vector<uint32_t> mats(n);
+		if (cudaMemcpy(mats.data(), material, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+			rc = fail(ctx, RB_ERR_CUDA, "rb_build_lights: materials");
+		for (uint32_t m : mats) maxMaterial = std::max(maxMaterial, m + 1);
+	}
+	// the scratch and the count are not kept
+	if (rc == RB_OK)
+	{
+		fresh.erase(std::remove(fresh.begin(), fresh.end(), scratch), fresh.end());
+		fresh.erase(std::remove(fresh.begin(), fresh.end(), static_cast<void*>(dCount)), fresh.end());
+		cudaFree(scratch);
+		cudaFree(dCount);
+	}
+	rc = commit(ctx, ctx->lightBufs, fresh, rc);
+	if (rc != RB_OK) return rc;
+	L.triangles = n ? tris : nullptr;
+	L.nodes = n ? dn : nullptr;
+	L.unpacked = n ? du : nullptr;
+	L.nodeCount = nodeCount;
+	L.triangleCount = n;
+	ctx->scene.lights = L;
+	ctx->lightWorldTris = worldTris;
+	ctx->lightWorldNodes = worldNodes;
+	ctx->lightMaxMaterial = maxMaterial;
+	return RB_OK;
+}
+
 int rb_set_light_origin(rb_ctx* ctx, const float origin[3], void* stream)
 {
 	if (!ctx || !origin) return RB_ERR_INVALID;

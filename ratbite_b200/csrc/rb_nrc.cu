@@ -13,24 +13,25 @@
 // would drop the sample, which only the renderer's cached form trains. No
 // biases except through the constant input.
 //
-// Tensor cores: the fused forward kernel keeps a 16-row tile of activations
-// in registers as mma.sync m16n8k16 BF16 fragments (FP32 accumulation); an
-// accumulator fragment of one layer is repacked in registers into the A
-// fragment of the next. The fused backward kernel chains dX = dY W the same
-// way with the transposed weights; the weight gradients dW = dY^T X over the
-// batch are plain GEMMs (cuBLAS). Adam runs in FP32 on the master copies.
+// Tensor cores: inference (with the encoding fused in), the training forward
+// and the backward chain dX = dY W run on tcgen05 (rb_umma.cuh): 128-row
+// tiles in swizzled shared memory, BF16 operands, FP32 accumulators in
+// tensor memory, one thread per row for the epilogue (ReLU, repack to BF16
+// in place as the next layer's input). The weight gradients dW = dY^T X of
+// all five layers are one hand-written kernel (mma.sync over the batch,
+// operands transposed by ldmatrix). Adam runs in FP32 on the master copies.
 
 #include <cstdint>
 #include <cstring>
 #include <vector>
 
-#include <cublas_v2.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include "rb_launch.cuh"
 #include "ratbite_b200_nrc.h"
 #include "rb_nrc_internal.h"
+#include "rb_umma.cuh"
 
 namespace rb
 {
@@ -42,8 +43,7 @@ constexpr int kGridFeatures = kLevels * kFeat;          // 32
 // offset of W_l in the packed weights: W0..W3 are 64 x 64, W4 is 16 x 64
 __host__ __device__ constexpr int wOffset(int l) { return l < 5 ? l * kH * kH : 4 * kH * kH + kOutPad * kH; }
 constexpr int kWTotal = wOffset(5);                     // 17408 weights
-constexpr int kWStride = 72;                            // smem row stride (bf16), conflict-free fragment loads
-constexpr int kTile = 16;                               // rows per warp tile
+constexpr int kWStride = 72;                            // smem row stride (bf16) of kWeightGrad, conflict-free ldmatrix
 constexpr uint32_t kMaxTrainRows = 1u << 24;          // rows per training batch (encode kernels index rows x levels)
 constexpr int kOutStride = 8;                           // forward outputs per row in the training scratch
 constexpr int kDropOutput = 4;                          // output trained by the renderer: drop probability
@@ -152,259 +152,6 @@ RB_D void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t 
 		: "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// Four 8x8 b16 matrices from shared memory (ldmatrix.x4): lanes 8m..8m+7
-// give the row addresses of matrix m; register m receives matrix m's
-// fragment (row lane / 4, columns 2 (lane % 4), +1).
-RB_D void ldsm4(uint32_t (&r)[4], const __nv_bfloat16* p)
-{
-	const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
-	asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-		: "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
-}
-
-// One layer on a 16-row tile: C[16 x 8*NT] = A[16 x 64] x W^T, W in smem as
-// [out][in] rows of kWStride bf16. A: 4 k-tiles of fragments. The B
-// fragments of two k-tiles come from one ldmatrix.x4 (matrices at k offsets
-// 0, 8, 16, 24 of the lane's weight row).
-template<int NT>
-RB_D void layer(const uint32_t (&A)[4][4], const __nv_bfloat16* W, float (&C)[NT][4])
-{
-	const uint32_t lane = threadIdx.x & 31u, r = lane & 7u, m = lane >> 3;
-#pragma unroll
-	for (int j = 0; j < NT; ++j)
-	{
-		C[j][0] = C[j][1] = C[j][2] = C[j][3] = 0.0f;
-		const __nv_bfloat16* wr = W + (8 * j + r) * kWStride + 8 * m;
-		uint32_t b[4];
-		ldsm4(b, wr);
-		mma16816(C[j], A[0], b[0], b[1]);
-		mma16816(C[j], A[1], b[2], b[3]);
-		ldsm4(b, wr + 32);
-		mma16816(C[j], A[2], b[0], b[1]);
-		mma16816(C[j], A[3], b[2], b[3]);
-	}
-}
-// Accumulator fragments of 8 n-tiles -> A fragments of the next layer, with ReLU.
-RB_D void toA(const float (&C)[8][4], uint32_t (&A)[4][4], bool relu)
-{
-#pragma unroll
-	for (int t = 0; t < 4; ++t)
-	{
-		const float* a = C[2 * t];
-		const float* b = C[2 * t + 1];
-		auto r = [relu](float x) { return relu ? fmaxf(x, 0.0f) : x; };
-		A[t][0] = pack2(r(a[0]), r(a[1]));
-		A[t][1] = pack2(r(a[2]), r(a[3]));
-		A[t][2] = pack2(r(b[0]), r(b[1]));
-		A[t][3] = pack2(r(b[2]), r(b[3]));
-	}
-}
-// A fragments of rows r0..r0+15 of a row-major [rows][64] bf16 array.
-RB_D void loadA(const __nv_bfloat16* X, uint32_t r0, uint32_t rows, uint32_t (&A)[4][4])
-{
-	const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, c = lane & 3u;
-	const uint32_t ra = r0 + g, rb = r0 + g + 8;
-#pragma unroll
-	for (int t = 0; t < 4; ++t)
-	{
-		const uint32_t k0 = 16 * t + 2 * c;
-		A[t][0] = ra < rows ? *reinterpret_cast<const uint32_t*>(X + static_cast<size_t>(ra) * kIn + k0) : 0u;
-		A[t][1] = rb < rows ? *reinterpret_cast<const uint32_t*>(X + static_cast<size_t>(rb) * kIn + k0) : 0u;
-		A[t][2] = ra < rows ? *reinterpret_cast<const uint32_t*>(X + static_cast<size_t>(ra) * kIn + k0 + 8) : 0u;
-		A[t][3] = rb < rows ? *reinterpret_cast<const uint32_t*>(X + static_cast<size_t>(rb) * kIn + k0 + 8) : 0u;
-	}
-}
-RB_D void storeA(__nv_bfloat16* Y, uint32_t r0, uint32_t rows, const uint32_t (&A)[4][4])
-{
-	const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, c = lane & 3u;
-	const uint32_t ra = r0 + g, rb = r0 + g + 8;
-#pragma unroll
-	for (int t = 0; t < 4; ++t)
-	{
-		const uint32_t k0 = 16 * t + 2 * c;
-		if (ra < rows)
-		{
-			*reinterpret_cast<uint32_t*>(Y + static_cast<size_t>(ra) * kIn + k0) = A[t][0];
-			*reinterpret_cast<uint32_t*>(Y + static_cast<size_t>(ra) * kIn + k0 + 8) = A[t][2];
-		}
-		if (rb < rows)
-		{
-			*reinterpret_cast<uint32_t*>(Y + static_cast<size_t>(rb) * kIn + k0) = A[t][1];
-			*reinterpret_cast<uint32_t*>(Y + static_cast<size_t>(rb) * kIn + k0 + 8) = A[t][3];
-		}
-	}
-}
-
-// Copies the 5 weight matrices (global, [out][in] bf16, dense) into shared
-// memory with the padded stride.
-RB_D void stageWeights(const __nv_bfloat16* __restrict__ w, __nv_bfloat16* sw)
-{
-	for (int i = threadIdx.x; i < kWTotal / 2; i += blockDim.x)
-	{
-		const int e = 2 * i, row = e / kH, col = e % kH;
-		*reinterpret_cast<uint32_t*>(sw + row * kWStride + col) = *reinterpret_cast<const uint32_t*>(w + e);
-	}
-	__syncthreads();
-}
-constexpr int kWRowsTotal = kWTotal / kH;   // 272 rows of 64
-constexpr size_t kSmemWeights = sizeof(__nv_bfloat16) * kWRowsTotal * kWStride;
-// backward: W4^T as 64 rows (16 used columns) + W3^T..W0^T as 4 x 64 rows
-constexpr int kWtRows = 64 + 4 * 64;
-constexpr size_t kSmemBackward = sizeof(__nv_bfloat16) * kWtRows * kWStride;
-
-// Forward: out[n][kOutStride] (FP32; outputs 0..3 radiance, 4 the drop
-// probability the renderer trains, 5..7 unused). With acts, the post-ReLU hidden activations of
-// layers 1..4 are stored ([4][n][64] bf16) for the backward pass.
-__global__ void __launch_bounds__(128) kMlpForward(uint32_t n, const __nv_bfloat16* __restrict__ X,
-	const __nv_bfloat16* __restrict__ w, float* __restrict__ out, __nv_bfloat16* __restrict__ acts)
-{
-	extern __shared__ __nv_bfloat16 sw[];
-	stageWeights(w, sw);
-	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
-	const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, c = lane & 3u;
-	for (uint32_t r0 = warp * kTile; r0 < n; r0 += warps * kTile)
-	{
-		uint32_t A[4][4];
-		loadA(X, r0, n, A);
-		float C[8][4];
-#pragma unroll
-		for (int l = 0; l < 4; ++l)
-		{
-			layer<8>(A, sw + wOffset(l) / kH * kWStride, C);
-			toA(C, A, true);
-			if (acts) storeA(acts + static_cast<size_t>(l) * n * kIn, r0, n, A);
-		}
-		float O[1][4];
-		layer<1>(A, sw + wOffset(4) / kH * kWStride, O);
-		// O: rows g, g+8; cols 2c, 2c+1: the first 8 output rows of W4
-		const uint32_t ra = r0 + g, rb = r0 + g + 8;
-		if (ra < n) { out[kOutStride * ra + 2 * c] = O[0][0]; out[kOutStride * ra + 2 * c + 1] = O[0][1]; }
-		if (rb < n) { out[kOutStride * rb + 2 * c] = O[0][2]; out[kOutStride * rb + 2 * c + 1] = O[0][3]; }
-	}
-}
-
-// Inference with the encoding fused in: each warp encodes its 16-row tile
-// into a shared-memory tile (lanes split the 16 rows x 16 levels of grid
-// lookups, then the 32 remaining columns), reads the A fragments from it and
-// runs the layers as kMlpForward. Rows: min(*count, cap) when count is given,
-// else cap. Outputs 0..3 go to out[rows][4] and/or, with path, are applied
-// as L[p] = L[p] (1 - q) + T[p] max(y, 0), p = path[r], q = output 4
-// clamped to [0, 1] (radiance-cache queries).
-// RB_INFER_THREADS threads share one copy of the weights; as many blocks per
-// SM as fit (3 at 256 threads: 56 KB of shared memory each, registers capped
-// for 3). Measured on the cached Cornell frame (1920x1080, 64 spp): 256
-// threads 8.06 ms of inference, 384: 8.14, 512: 8.71 (spills at the
-// 64-register cap).
-#ifndef RB_INFER_THREADS
-#define RB_INFER_THREADS 256
-#endif
-#ifndef RB_INFER_GATHER_UNROLL
-#define RB_INFER_GATHER_UNROLL 2
-#endif
-constexpr int kInferThreads = RB_INFER_THREADS;
-constexpr int kGatherUnroll = RB_INFER_GATHER_UNROLL;
-#ifndef RB_INFER_MIN_BLOCKS
-#define RB_INFER_MIN_BLOCKS 3
-#endif
-constexpr int kInferMinBlocks = RB_INFER_MIN_BLOCKS;
-constexpr size_t kSmemInfer = kSmemWeights + sizeof(__nv_bfloat16) * (kInferThreads / 32) * kTile * kWStride;
-__global__ void __launch_bounds__(kInferThreads, kInferMinBlocks) kMlpInfer(uint32_t cap, const uint32_t* __restrict__ count,
-	const float* __restrict__ in, const __half2* __restrict__ grid, Resolutions R, const __nv_bfloat16* __restrict__ w,
-	float* __restrict__ out, const uint32_t* __restrict__ path, float4* __restrict__ L, const float4* __restrict__ T,
-	const float* __restrict__ corr)
-{
-	extern __shared__ __nv_bfloat16 sw[];
-	stageWeights(w, sw);
-	const uint32_t n = count ? min(*count, cap) : cap;
-	__nv_bfloat16* tile = sw + kWRowsTotal * kWStride + (threadIdx.x >> 5) * kTile * kWStride;
-	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
-	const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, c = lane & 3u;
-	for (uint32_t r0 = warp * kTile; r0 < n; r0 += warps * kTile)
-	{
-		// grid features: lane handles (row k / 16, level k % 16) for k = lane + 32 i
-#pragma unroll kGatherUnroll
-		for (uint32_t k = lane; k < kTile * kLevels; k += 32)
-		{
-			const uint32_t row = k >> 4, l = k & 15u, r = r0 + row;
-			float f0 = 0.0f, f1 = 0.0f;
-			if (r < n)
-			{
-				const float* v = in + static_cast<size_t>(kNrcInputs) * r;
-				levelFeatures(R, grid, static_cast<int>(l), clamp01(v[0]), clamp01(v[1]), clamp01(v[2]), f0, f1);
-			}
-			*reinterpret_cast<uint32_t*>(tile + row * kWStride + 2 * l) = pack2(f0, f1);
-		}
-		// columns 32..63: lane handles 16 columns of row lane / 2
-		{
-			const uint32_t row = lane >> 1, r = r0 + row, k0 = 16 * (lane & 1u);
-			const float* v = in + static_cast<size_t>(kNrcInputs) * r;
-#pragma unroll
-			for (uint32_t k = 0; k < 16; k += 2)
-			{
-				const float a = r < n ? restColumn(v, static_cast<int>(k0 + k)) : 0.0f;
-				const float b = r < n ? restColumn(v, static_cast<int>(k0 + k + 1)) : 0.0f;
-				*reinterpret_cast<uint32_t*>(tile + row * kWStride + 32 + k0 + k) = pack2(a, b);
-			}
-		}
-		__syncwarp();
-		// A fragments (ldmatrix.x4 per k-tile: rows 0-7 / 8-15 x columns 0-7 / 8-15 of the tile)
-		uint32_t A[4][4];
-		{
-			const uint32_t m = lane >> 3, rr = (lane & 7u) + 8u * (m & 1u);
-#pragma unroll
-			for (int t = 0; t < 4; ++t) ldsm4(A[t], tile + rr * kWStride + 16 * t + 8 * (m >> 1));
-		}
-		__syncwarp();
-		float C[8][4];
-#pragma unroll
-		for (int l = 0; l < 4; ++l)
-		{
-			layer<8>(A, sw + wOffset(l) / kH * kWStride, C);
-			toA(C, A, true);
-		}
-		float O[1][4];
-		layer<1>(A, sw + wOffset(4) / kH * kWStride, O);
-		// lanes c = 0 hold outputs 0, 1, lanes c = 1 outputs 2, 3 and lanes
-		// c = 2 output 4 (drop probability) of rows g and g + 8
-		const float a2 = __shfl_down_sync(0xFFFFFFFFu, O[0][0], 1), a3 = __shfl_down_sync(0xFFFFFFFFu, O[0][1], 1);
-		const float b2 = __shfl_down_sync(0xFFFFFFFFu, O[0][2], 1), b3 = __shfl_down_sync(0xFFFFFFFFu, O[0][3], 1);
-		const float aq = __shfl_down_sync(0xFFFFFFFFu, O[0][0], 2), bq = __shfl_down_sync(0xFFFFFFFFu, O[0][2], 2);
-		if (c == 0)
-		{
-			const uint32_t rows[2] = { r0 + g, r0 + g + 8 };
-			const float4 y[2] = { make_float4(O[0][0], O[0][1], a2, a3), make_float4(O[0][2], O[0][3], b2, b3) };
-			const float q[2] = { aq, bq };
-#pragma unroll
-			for (int h = 0; h < 2; ++h)
-			{
-				if (rows[h] >= n) continue;
-				if (out) reinterpret_cast<float4*>(out)[rows[h]] = y[h];
-				if (path)
-				{
-					// the plain estimator drops a whole sample whose later BxDF
-					// sample fails: the prefix survives with 1 - q, q plus the
-					// correction measured on the path's class (the path
-					// index's high bit: the camera ray hit an emitter, whose
-					// radiance dominates the prefix); the radiance is scaled
-					// by the measured ratio of targets to predictions
-					const uint32_t pr = path[rows[h]];
-					const uint32_t p = pr & 0x7FFFFFFFu;
-					const float4 t = T[p];
-					const float qq = q[h] + (corr ? corr[((pr >> 31) ? kCorrDropLit : kCorrDropOther) + 2] : 0.0f);
-					const float keep = fminf(fmaxf(1.0f - qq, 0.0f), 1.0f);
-					const float sc = corr && corr[kCorrRadiance + 3] > 0.0f ? corr[kCorrRadiance + 2] : 1.0f;
-					float4 l = L[p];
-					l.x = l.x * keep + t.x * (sc * fmaxf(y[h].x, 0.0f));
-					l.y = l.y * keep + t.y * (sc * fmaxf(y[h].y, 0.0f));
-					l.z = l.z * keep + t.z * (sc * fmaxf(y[h].z, 0.0f));
-					l.w = l.w * keep + t.w * (sc * fmaxf(y[h].w, 0.0f));
-					L[p] = l;
-				}
-			}
-		}
-	}
-}
-
 // Relative L2 loss (Mueller et al. 2021): sum over the first `outs` outputs
 // of (y - t)^2 / (sg(y)^2 + 0.01), averaged over the batch; targets are rows
 // of tStride floats; dY is written as bf16 rows of 16 and the loss sum
@@ -467,81 +214,502 @@ __global__ void kLoss(uint32_t n, const float* __restrict__ y, const float* __re
 	}
 }
 
-// Backward through the layers on 16-row tiles: with the transposed weights
-// wt ([in][out] per layer, the output layer padded to 16 columns), dH4 = dY W4
-// masked by ReLU', ..., dX0 = dH1 W0. Writes the masked gradients of the
-// hidden layers ([4][n][64] bf16, for the weight gradients) and the
-// gradient of the 32 grid features (FP32).
-__global__ void __launch_bounds__(128) kMlpBackward(uint32_t n, const __nv_bfloat16* __restrict__ dY,
-	const __nv_bfloat16* __restrict__ wt, const __nv_bfloat16* __restrict__ acts, __nv_bfloat16* __restrict__ dH,
-	float* __restrict__ dX0)
+// ------------------------------------------------- tcgen05 (Blackwell) tiles
+// The MLP on the 5th-generation tensor cores (rb_umma.cuh): a CTA of 128
+// threads owns a tile of 128 rows; thread t owns row t of the tile for the
+// whole pass (it writes the row's inputs into the swizzled activation tile,
+// reads the row's accumulator lane back from TMEM, applies ReLU, and writes
+// the row of the next layer's input in place). One thread issues each
+// layer's MMAs (M = 128, N = 64 or 16, four K steps of 16) and commits them
+// to an mbarrier; the CTA waits on it (bounded; a wait that gives up sets
+// RB_DEV_ITERATION_LIMIT in *status and the CTA stops). Several CTAs per SM
+// (about 51 KB of shared memory and 64 TMEM columns each) overlap one
+// tile's grid gathers with another's MMAs.
+namespace t5
 {
-	extern __shared__ __nv_bfloat16 sw[];
-	// wt layout: W4^T [64][16] first (as 64 rows of 16), then W3^T..W0^T [64][64]
-	for (int i = threadIdx.x; i < (64 * 16) / 2; i += blockDim.x)
+constexpr uint32_t kRows = 128;
+constexpr uint32_t kWBytes = 8192;                       // one 64 x 64 layer
+constexpr uint32_t kOffW4 = 4 * kWBytes;                 // output layer: 16 rows (2 KB)
+constexpr uint32_t kOffAct = kOffW4 + 2048;              // 34816: activation tile, 16 KB
+constexpr uint32_t kOffBar = kOffAct + kRows * 128;      // mbarrier (8 B) + TMEM slot (4 B)
+constexpr uint32_t kSmem = kOffBar + 16 + 1024;          // + alignment slack of the dynamic base
+constexpr uint32_t kTmemCols = 64;
+constexpr uint32_t kWaitLimit = 1u << 22;
+static_assert(kOffAct % 1024 == 0, "operand tiles start on 1024-byte boundaries");
+
+RB_D unsigned char* alignBase(unsigned char* p)
+{
+	return reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 1023u) & ~static_cast<uintptr_t>(1023u));
+}
+RB_D unsigned char* layerTile(unsigned char* base, int l) { return base + (l < 4 ? l * kWBytes : kOffW4); }
+
+// Copies 272 rows of 64 bf16 ([out][in] per layer, or [in][out] for the
+// transposed copy) into the swizzled tiles: rows 0..255 layers 0..3, rows
+// 256..271 the 16-row output block.
+RB_D void stageLayers(const __nv_bfloat16* __restrict__ w, unsigned char* base)
+{
+	for (uint32_t i = threadIdx.x; i < 272u * 8u; i += blockDim.x)
 	{
-		const int e = 2 * i, row = e / 16, col = e % 16;
-		*reinterpret_cast<uint32_t*>(sw + row * kWStride + col) = *reinterpret_cast<const uint32_t*>(wt + e);
+		const uint32_t row = i >> 3, c = i & 7u;
+		const int l = row < 256u ? static_cast<int>(row >> 6) : 4;
+		const uint32_t r = row < 256u ? (row & 63u) : row - 256u;
+		*reinterpret_cast<uint4*>(layerTile(base, l) + r * 128u + (((c ^ r) & 7u) << 4)) =
+			*reinterpret_cast<const uint4*>(w + static_cast<size_t>(row) * 64u + 8u * c);
 	}
-	for (int i = threadIdx.x; i < (4 * 64 * 64) / 2; i += blockDim.x)
-	{
-		const int e = 2 * i, row = e / 64, col = e % 64;
-		*reinterpret_cast<uint32_t*>(sw + (64 + row) * kWStride + col) = *reinterpret_cast<const uint32_t*>(wt + 64 * 16 + e);
-	}
+}
+
+struct Ctx
+{
+	unsigned char* base;
+	unsigned char* act;
+	uint64_t* bar;
+	uint32_t tmem;
+	uint32_t phase;
+};
+
+// Prologue shared by the tcgen05 kernels: barrier, TMEM, weights.
+RB_D Ctx begin(unsigned char* smraw, const __nv_bfloat16* __restrict__ w)
+{
+	Ctx c;
+	c.base = alignBase(smraw);
+	c.act = c.base + kOffAct;
+	c.bar = reinterpret_cast<uint64_t*>(c.base + kOffBar);
+	uint32_t* slot = reinterpret_cast<uint32_t*>(c.base + kOffBar + 8);
+	if (threadIdx.x == 0) umma::barrierInit(c.bar, 1);
+	if ((threadIdx.x >> 5) == 0) umma::tmemAlloc(slot, kTmemCols);
+	stageLayers(w, c.base);
+	umma::fenceProxyAsync();
+	umma::fenceBeforeSync();
 	__syncthreads();
-	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
-	const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, c = lane & 3u;
-	for (uint32_t r0 = warp * kTile; r0 < n; r0 += warps * kTile)
+	umma::fenceAfterSync();
+	c.tmem = *slot;
+	c.phase = 0;
+	return c;
+}
+RB_D void end(const Ctx& c)
+{
+	umma::fenceBeforeSync();
+	__syncthreads();
+	if ((threadIdx.x >> 5) == 0) umma::tmemFree(c.tmem, kTmemCols);
+}
+
+// D = act (128 x 64) x layer(l)^T with nK K steps, then the CTA waits for
+// it. Every thread must have written its row of `act` (and fenced it for
+// the tensor cores) before. Returns false (uniformly) when the wait gave up.
+RB_D bool layerMma(Ctx& c, const unsigned char* bTile, uint32_t n, int nK, uint32_t* status)
+{
+	if (threadIdx.x == 0)
 	{
-		// dY tile as one k-tile (16 columns, 4 used)
-		uint32_t A[4][4];
-		const uint32_t ra = r0 + g, rb = r0 + g + 8;
-		{
-			const __nv_bfloat16* base = dY;
-			A[0][0] = ra < n ? *reinterpret_cast<const uint32_t*>(base + static_cast<size_t>(ra) * kOutPad + 2 * c) : 0u;
-			A[0][1] = rb < n ? *reinterpret_cast<const uint32_t*>(base + static_cast<size_t>(rb) * kOutPad + 2 * c) : 0u;
-			A[0][2] = ra < n ? *reinterpret_cast<const uint32_t*>(base + static_cast<size_t>(ra) * kOutPad + 8 + 2 * c) : 0u;
-			A[0][3] = rb < n ? *reinterpret_cast<const uint32_t*>(base + static_cast<size_t>(rb) * kOutPad + 8 + 2 * c) : 0u;
-		}
-		float C[8][4];
-		// dH4 = dY[16 x 16] x W4 (B(k = out, n = in) = W4^T[in][out])
+		umma::fenceAfterSync();
+		const uint32_t idesc = umma::idescBf16(kRows, n);
+		for (int k = 0; k < nK; ++k)
+			umma::mma(c.tmem, umma::descK(c.act, static_cast<uint32_t>(k)), umma::descK(bTile, static_cast<uint32_t>(k)),
+				idesc, k > 0);
+		umma::commit(c.bar);
+	}
+	const bool ok = __syncthreads_and(umma::barrierWait(c.bar, c.phase, kWaitLimit)) != 0;
+	c.phase ^= 1u;
+	if (!ok)
+	{
+		if (threadIdx.x == 0) atomicOr(status, RB_DEV_ITERATION_LIMIT);
+		// give the MMAs in flight a second bounded wait before TMEM is freed
+		umma::barrierWait(c.bar, c.phase ^ 1u, kWaitLimit);
+		return false;
+	}
+	umma::fenceAfterSync();
+	return true;
+}
+
+// This thread's 64 accumulator columns.
+RB_D void readAcc64(const Ctx& c, float (&v)[64])
+{
+	uint32_t r[4][16];
 #pragma unroll
-		for (int j = 0; j < 8; ++j)
-		{
-			C[j][0] = C[j][1] = C[j][2] = C[j][3] = 0.0f;
-			const __nv_bfloat16* wr = sw + (8 * j + g) * kWStride;
-			const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wr + 2 * c);
-			const uint32_t b1 = *reinterpret_cast<const uint32_t*>(wr + 8 + 2 * c);
-			mma16816(C[j], A[0], b0, b1);
-		}
-		for (int l = 3; l >= 0; --l)
-		{
-			// mask by ReLU' of the stored activation of layer l (post-ReLU > 0)
-			uint32_t H[4][4];
-			loadA(acts + static_cast<size_t>(l) * n * kIn, r0, n, H);
+	for (int q = 0; q < 4; ++q) umma::tmemLoad16(umma::laneAddr(c.tmem, 16u * q), r[q]);
+	umma::tmemWaitLoad();
 #pragma unroll
-			for (int t = 0; t < 4; ++t)
+	for (int q = 0; q < 4; ++q)
+#pragma unroll
+		for (int j = 0; j < 16; ++j) v[16 * q + j] = __uint_as_float(r[q][j]);
+}
+RB_D void readAcc16(const Ctx& c, float (&v)[16])
+{
+	uint32_t r[16];
+	umma::tmemLoad16(umma::laneAddr(c.tmem, 0), r);
+	umma::tmemWaitLoad();
+#pragma unroll
+	for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+// After this thread's TMEM reads and its write of its row of `act`: make both
+// safe for the next MMA.
+RB_D void rowWritten()
+{
+	umma::fenceBeforeSync();
+	umma::fenceProxyAsync();
+	__syncthreads();
+}
+RB_D void reluPack(const float (&v)[64], uint32_t (&row)[32])
+{
+#pragma unroll
+	for (int j = 0; j < 32; ++j) row[j] = pack2(fmaxf(v[2 * j], 0.0f), fmaxf(v[2 * j + 1], 0.0f));
+}
+RB_D void encodeRow(uint32_t r, uint32_t n, const float* __restrict__ in, const __half2* __restrict__ grid,
+	const Resolutions& R, uint32_t (&row)[32])
+{
+	if (r >= n)
+	{
+#pragma unroll
+		for (int j = 0; j < 32; ++j) row[j] = 0u;
+		return;
+	}
+	const float* v = in + static_cast<size_t>(kNrcInputs) * r;
+	const float px = clamp01(v[0]), py = clamp01(v[1]), pz = clamp01(v[2]);
+#pragma unroll
+	for (int l = 0; l < kLevels; ++l)
+	{
+		float f0, f1;
+		levelFeatures(R, grid, l, px, py, pz, f0, f1);
+		row[l] = pack2(f0, f1);
+	}
+#pragma unroll
+	for (int k = 0; k < 32; k += 2) row[16 + k / 2] = pack2(restColumn(v, k), restColumn(v, k + 1));
+}
+} // namespace t5
+
+// Inference with the encoding fused in (kMlpInfer's contract, on tcgen05).
+__global__ void __launch_bounds__(128) kMlpInferT(uint32_t cap, const uint32_t* __restrict__ count,
+	const float* __restrict__ in, const __half2* __restrict__ grid, Resolutions R, const __nv_bfloat16* __restrict__ w,
+	float* __restrict__ out, const uint32_t* __restrict__ path, float4* __restrict__ L, const float4* __restrict__ T,
+	const float* __restrict__ corr, uint32_t* __restrict__ status)
+{
+	extern __shared__ unsigned char smraw[];
+	t5::Ctx c = t5::begin(smraw, w);
+	const uint32_t n = count ? min(*count, cap) : cap;
+	bool ok = true;
+	for (uint32_t r0 = blockIdx.x * t5::kRows; r0 < n && ok; r0 += gridDim.x * t5::kRows)
+	{
+		const uint32_t r = r0 + threadIdx.x;
+		{
+			uint32_t row[32];
+			t5::encodeRow(r, n, in, grid, R, row);
+			umma::storeRow(c.act, threadIdx.x, row);
+		}
+		umma::fenceProxyAsync();
+		__syncthreads();
+		for (int l = 0; l < 4 && ok; ++l)
+		{
+			ok = t5::layerMma(c, t5::layerTile(c.base, l), 64, 4, status);
+			if (!ok) break;
+			float v[64];
+			t5::readAcc64(c, v);
+			uint32_t row[32];
+			t5::reluPack(v, row);
+			umma::storeRow(c.act, threadIdx.x, row);
+			t5::rowWritten();
+		}
+		if (!ok) break;
+		ok = t5::layerMma(c, t5::layerTile(c.base, 4), 16, 4, status);
+		if (!ok) break;
+		float o[16];
+		t5::readAcc16(c, o);
+		if (r < n)
+		{
+			const float4 y = make_float4(o[0], o[1], o[2], o[3]);
+			if (out) reinterpret_cast<float4*>(out)[r] = y;
+			if (path)
 			{
-				const float2 h00 = unpack2(H[t][0]), h10 = unpack2(H[t][1]), h01 = unpack2(H[t][2]), h11 = unpack2(H[t][3]);
-				float* a = C[2 * t];
-				float* b = C[2 * t + 1];
-				a[0] = h00.x > 0.0f ? a[0] : 0.0f; a[1] = h00.y > 0.0f ? a[1] : 0.0f;
-				a[2] = h10.x > 0.0f ? a[2] : 0.0f; a[3] = h10.y > 0.0f ? a[3] : 0.0f;
-				b[0] = h01.x > 0.0f ? b[0] : 0.0f; b[1] = h01.y > 0.0f ? b[1] : 0.0f;
-				b[2] = h11.x > 0.0f ? b[2] : 0.0f; b[3] = h11.y > 0.0f ? b[3] : 0.0f;
+				// the plain estimator drops a whole sample whose later BxDF
+				// sample fails: the prefix survives with 1 - q, q plus the
+				// correction measured on the path's class (the path index's
+				// high bit: the camera ray hit an emitter); the radiance is
+				// scaled by the measured ratio of targets to predictions
+				const uint32_t pr = path[r];
+				const uint32_t p = pr & 0x7FFFFFFFu;
+				const float4 t = T[p];
+				const float qq = o[4] + (corr ? corr[((pr >> 31) ? kCorrDropLit : kCorrDropOther) + 2] : 0.0f);
+				const float keep = fminf(fmaxf(1.0f - qq, 0.0f), 1.0f);
+				const float sc = corr && corr[kCorrRadiance + 3] > 0.0f ? corr[kCorrRadiance + 2] : 1.0f;
+				float4 l = L[p];
+				l.x = l.x * keep + t.x * (sc * fmaxf(y.x, 0.0f));
+				l.y = l.y * keep + t.y * (sc * fmaxf(y.y, 0.0f));
+				l.z = l.z * keep + t.z * (sc * fmaxf(y.z, 0.0f));
+				l.w = l.w * keep + t.w * (sc * fmaxf(y.w, 0.0f));
+				L[p] = l;
 			}
-			toA(C, A, false);
-			storeA(dH + static_cast<size_t>(l) * n * kIn, r0, n, A);
-			// next: dH_{l} x W_l  (W_l^T at row block 64 + (3 - l) * 64)
-			layer<8>(A, sw + (64 + (3 - l) * 64) * kWStride, C);
 		}
-		// C = dX0 (64 columns); the first 32 are the grid features
-#pragma unroll
-		for (int j = 0; j < 4; ++j)
+		umma::fenceBeforeSync();
+		__syncthreads();
+	}
+	t5::end(c);
+}
+
+// Training forward on the encoded rows X [n][64] (kMlpForward's contract):
+// out [n][kOutStride] f32 and the post-ReLU hidden rows acts [4][n][64] bf16.
+__global__ void __launch_bounds__(128) kMlpForwardT(uint32_t n, const __nv_bfloat16* __restrict__ X,
+	const __nv_bfloat16* __restrict__ w, float* __restrict__ out, __nv_bfloat16* __restrict__ acts,
+	uint32_t* __restrict__ status)
+{
+	extern __shared__ unsigned char smraw[];
+	t5::Ctx c = t5::begin(smraw, w);
+	bool ok = true;
+	for (uint32_t r0 = blockIdx.x * t5::kRows; r0 < n && ok; r0 += gridDim.x * t5::kRows)
+	{
+		const uint32_t r = r0 + threadIdx.x;
 		{
-			if (ra < n) { dX0[32 * ra + 8 * j + 2 * c] = C[j][0]; dX0[32 * ra + 8 * j + 2 * c + 1] = C[j][1]; }
-			if (rb < n) { dX0[32 * rb + 8 * j + 2 * c] = C[j][2]; dX0[32 * rb + 8 * j + 2 * c + 1] = C[j][3]; }
+			uint32_t row[32];
+#pragma unroll
+			for (int j = 0; j < 8; ++j)
+			{
+				const uint4 q = r < n ? *reinterpret_cast<const uint4*>(X + static_cast<size_t>(r) * kIn + 8 * j)
+					: make_uint4(0u, 0u, 0u, 0u);
+				row[4 * j] = q.x; row[4 * j + 1] = q.y; row[4 * j + 2] = q.z; row[4 * j + 3] = q.w;
+			}
+			umma::storeRow(c.act, threadIdx.x, row);
 		}
+		umma::fenceProxyAsync();
+		__syncthreads();
+		for (int l = 0; l < 4 && ok; ++l)
+		{
+			ok = t5::layerMma(c, t5::layerTile(c.base, l), 64, 4, status);
+			if (!ok) break;
+			float v[64];
+			t5::readAcc64(c, v);
+			uint32_t row[32];
+			t5::reluPack(v, row);
+			umma::storeRow(c.act, threadIdx.x, row);
+			if (acts && r < n)
+			{
+				uint4* dst = reinterpret_cast<uint4*>(acts + (static_cast<size_t>(l) * n + r) * kIn);
+#pragma unroll
+				for (int j = 0; j < 8; ++j) dst[j] = make_uint4(row[4 * j], row[4 * j + 1], row[4 * j + 2], row[4 * j + 3]);
+			}
+			t5::rowWritten();
+		}
+		if (!ok) break;
+		ok = t5::layerMma(c, t5::layerTile(c.base, 4), 16, 4, status);
+		if (!ok) break;
+		float o[16];
+		t5::readAcc16(c, o);
+		if (r < n)
+		{
+			float4* dst = reinterpret_cast<float4*>(out + static_cast<size_t>(kOutStride) * r);
+			dst[0] = make_float4(o[0], o[1], o[2], o[3]);
+			dst[1] = make_float4(o[4], o[5], o[6], o[7]);
+		}
+		umma::fenceBeforeSync();
+		__syncthreads();
+	}
+	t5::end(c);
+}
+
+// Backward through the layers (kMlpBackward's contract) with the
+// transposed weights wt (rows [in][out]: W4^T as 64 rows of 16 outputs, then
+// W3^T..W0^T): g4 = dY W4 masked by ReLU'(h4), ..., dX = g1 W0. Writes the
+// masked gradients dH [4][n][64] (layer l at block l: g_{l+1}) and the
+// gradient of the 32 grid features dX0 [n][32] (f32).
+__global__ void __launch_bounds__(128) kMlpBackwardT(uint32_t n, const __nv_bfloat16* __restrict__ dY,
+	const __nv_bfloat16* __restrict__ wt, const __nv_bfloat16* __restrict__ acts, __nv_bfloat16* __restrict__ dH,
+	float* __restrict__ dX0, uint32_t* __restrict__ status)
+{
+	extern __shared__ unsigned char smraw[];
+	unsigned char* base = t5::alignBase(smraw);
+	// transposed tiles: W4^T (64 rows of 16 outputs, zero-padded to 64
+	// columns) at tile 0, then W3^T, W2^T, W1^T, W0^T at tiles 1..4 (all 64
+	// rows; the output-layer slot of the forward layout is not used)
+	{
+		for (uint32_t i = threadIdx.x; i < 64u * 8u; i += blockDim.x)
+		{
+			const uint32_t r = i >> 3, ch = i & 7u;
+			uint4 v = make_uint4(0u, 0u, 0u, 0u);
+			if (ch < 2u) v = *reinterpret_cast<const uint4*>(wt + static_cast<size_t>(r) * 16u + 8u * ch);
+			*reinterpret_cast<uint4*>(base + r * 128u + (((ch ^ r) & 7u) << 4)) = v;
+		}
+	}
+	t5::Ctx c;
+	c.base = base;
+	c.act = base + 5 * t5::kWBytes;      // activation tile after the five 8 KB tiles
+	c.bar = reinterpret_cast<uint64_t*>(c.act + t5::kRows * 128u);
+	uint32_t* slot = reinterpret_cast<uint32_t*>(c.act + t5::kRows * 128u + 8u);
+	if (threadIdx.x == 0) umma::barrierInit(c.bar, 1);
+	if ((threadIdx.x >> 5) == 0) umma::tmemAlloc(slot, t5::kTmemCols);
+	for (uint32_t i = threadIdx.x; i < 256u * 8u; i += blockDim.x)
+	{
+		const uint32_t row = i >> 3, ch = i & 7u, tile = 1u + (row >> 6), r = row & 63u;
+		*reinterpret_cast<uint4*>(base + tile * t5::kWBytes + r * 128u + (((ch ^ r) & 7u) << 4)) =
+			*reinterpret_cast<const uint4*>(wt + 64u * 16u + static_cast<size_t>(row) * 64u + 8u * ch);
+	}
+	umma::fenceProxyAsync();
+	umma::fenceBeforeSync();
+	__syncthreads();
+	umma::fenceAfterSync();
+	c.tmem = *slot;
+	c.phase = 0;
+	bool ok = true;
+	for (uint32_t r0 = blockIdx.x * t5::kRows; r0 < n && ok; r0 += gridDim.x * t5::kRows)
+	{
+		const uint32_t r = r0 + threadIdx.x;
+		{
+			// dY row: 16 columns (4 used), zero-padded to 64
+			uint32_t row[32];
+#pragma unroll
+			for (int j = 0; j < 32; ++j) row[j] = 0u;
+			if (r < n)
+			{
+				const uint4 a = *reinterpret_cast<const uint4*>(dY + static_cast<size_t>(r) * kOutPad);
+				const uint4 b = *reinterpret_cast<const uint4*>(dY + static_cast<size_t>(r) * kOutPad + 8);
+				row[0] = a.x; row[1] = a.y; row[2] = a.z; row[3] = a.w;
+				row[4] = b.x; row[5] = b.y; row[6] = b.z; row[7] = b.w;
+			}
+			umma::storeRow(c.act, threadIdx.x, row);
+		}
+		umma::fenceProxyAsync();
+		__syncthreads();
+		// tile 0: K = 16 (one step); tiles 1..4: K = 64
+		for (int l = 3; l >= -1 && ok; --l)
+		{
+			const int tile = 3 - l;                  // W4^T, W3^T, ..., W0^T
+			ok = t5::layerMma(c, base + tile * t5::kWBytes, 64, tile == 0 ? 1 : 4, status);
+			if (!ok) break;
+			float v[64];
+			t5::readAcc64(c, v);
+			if (l < 0)
+			{
+				// dX: the first 32 columns are the grid features
+				if (r < n)
+				{
+					float4* dst = reinterpret_cast<float4*>(dX0 + static_cast<size_t>(kGridFeatures) * r);
+#pragma unroll
+					for (int j = 0; j < 8; ++j) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+				}
+				umma::fenceBeforeSync();
+				__syncthreads();
+				break;
+			}
+			// mask by ReLU' of the layer's stored activation
+			uint32_t row[32];
+			if (r < n)
+			{
+				const uint4* hsrc = reinterpret_cast<const uint4*>(acts + (static_cast<size_t>(l) * n + r) * kIn);
+#pragma unroll
+				for (int j = 0; j < 8; ++j)
+				{
+					const uint4 h = hsrc[j];
+					const uint32_t hw[4] = { h.x, h.y, h.z, h.w };
+#pragma unroll
+					for (int q = 0; q < 4; ++q)
+					{
+						const float2 hh = unpack2(hw[q]);
+						const int k = 8 * j + 2 * q;
+						row[4 * j + q] = pack2(hh.x > 0.0f ? v[k] : 0.0f, hh.y > 0.0f ? v[k + 1] : 0.0f);
+					}
+				}
+				uint4* dst = reinterpret_cast<uint4*>(dH + (static_cast<size_t>(l) * n + r) * kIn);
+#pragma unroll
+				for (int j = 0; j < 8; ++j) dst[j] = make_uint4(row[4 * j], row[4 * j + 1], row[4 * j + 2], row[4 * j + 3]);
+			}
+			else
+			{
+#pragma unroll
+				for (int j = 0; j < 32; ++j) row[j] = 0u;
+			}
+			umma::storeRow(c.act, threadIdx.x, row);
+			t5::rowWritten();
+		}
+	}
+	t5::end(c);
+}
+constexpr size_t kSmemBackwardT = 5 * t5::kWBytes + t5::kRows * 128 + 16 + 1024;
+
+// Weight gradients dW_l[out][in] += sum over rows G_l[r][out] A_l[r][in]
+// for all five layers in one launch (no library GEMM): G = dY (layer 4, 16
+// columns) or dH block l, A = X (layer 0) or acts block l - 1. Block b takes
+// layer b % 5 and a chunk of rows; its 4 warps each own 16 outputs x 64
+// inputs (8 m16n8k16 tiles, FP32 accumulation), read through shared memory
+// with ldmatrix.trans (both operands are row-major over the batch), and the
+// partial sums are added to wGrad with one atomic per element.
+constexpr uint32_t kWgRows = 1024;                      // rows per block
+constexpr uint32_t kWgChunk = 64;                       // rows staged per step
+RB_D void ldsm4t(uint32_t (&r)[4], const __nv_bfloat16* p)
+{
+	const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
+	asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+		: "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
+}
+__global__ void __launch_bounds__(128) kWeightGrad(uint32_t n, const __nv_bfloat16* __restrict__ X,
+	const __nv_bfloat16* __restrict__ acts, const __nv_bfloat16* __restrict__ dY, const __nv_bfloat16* __restrict__ dH,
+	float* __restrict__ wGrad)
+{
+	__shared__ __align__(16) __nv_bfloat16 sG[kWgChunk][kWStride];
+	__shared__ __align__(16) __nv_bfloat16 sA[kWgChunk][kWStride];
+	const uint32_t layer = blockIdx.x % 5u, chunk = blockIdx.x / 5u;
+	const uint32_t rBegin = chunk * kWgRows;
+	if (rBegin >= n) return;
+	const uint32_t rEnd = min(n, rBegin + kWgRows);
+	const uint32_t outs = layer == 4u ? static_cast<uint32_t>(kOutPad) : 64u;
+	const __nv_bfloat16* G = layer == 4u ? dY : dH + static_cast<size_t>(layer) * n * kIn;
+	const uint32_t gStride = layer == 4u ? static_cast<uint32_t>(kOutPad) : static_cast<uint32_t>(kIn);
+	const __nv_bfloat16* A = layer == 0u ? X : acts + static_cast<size_t>(layer - 1u) * n * kIn;
+	const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+	const bool active = warp * 16u < outs;           // layer 4: one warp (16 outputs)
+	float acc[8][4];
+#pragma unroll
+	for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+	for (uint32_t c0 = rBegin; c0 < rEnd; c0 += kWgChunk)
+	{
+		__syncthreads();
+		// stage rows c0 .. c0+63 of G (outs columns) and A (64 columns), zero beyond rEnd
+		for (uint32_t i = threadIdx.x; i < kWgChunk * 8u; i += blockDim.x)
+		{
+			const uint32_t rr = i >> 3, ch = i & 7u, r = c0 + rr;
+			uint4 a = make_uint4(0u, 0u, 0u, 0u), g = a;
+			if (r < rEnd)
+			{
+				a = *reinterpret_cast<const uint4*>(A + static_cast<size_t>(r) * kIn + 8u * ch);
+				if (8u * ch < outs) g = *reinterpret_cast<const uint4*>(G + static_cast<size_t>(r) * gStride + 8u * ch);
+			}
+			*reinterpret_cast<uint4*>(&sA[rr][8u * ch]) = a;
+			*reinterpret_cast<uint4*>(&sG[rr][8u * ch]) = g;
+		}
+		__syncthreads();
+		if (!active) continue;
+		// K steps of 16 rows: A fragment (16 outputs x 16 rows) = G^T, B (16 rows x 8 inputs) = A
+#pragma unroll
+		for (uint32_t k = 0; k < kWgChunk; k += 16)
+		{
+			// G^T fragment: matrices (rows k..k+7 | k+8..k+15) x (outputs o..o+7 | o+8..o+15), transposed
+			uint32_t af[4];
+			{
+				const uint32_t m = lane >> 3, rr = lane & 7u;
+				// a0: out 0-7 x rows 0-7; a1: out 8-15 x rows 0-7; a2: out 0-7 x rows 8-15; a3: out 8-15 x rows 8-15
+				const uint32_t rowOff = (m & 2u) ? 8u : 0u, colOff = (m & 1u) ? 8u : 0u;
+				ldsm4t(af, &sG[k + rowOff + rr][warp * 16u + colOff]);
+			}
+#pragma unroll
+			for (int j = 0; j < 8; j += 2)
+			{
+				// B fragments of input tiles j, j+1: (rows k..k+15) x (inputs 8j..8j+7), col-major = A rows
+				uint32_t bf[4];
+				const uint32_t m = lane >> 3, rr = lane & 7u;
+				// b0(j): rows 0-7, b1(j): rows 8-15, b0(j+1): rows 0-7, b1(j+1): rows 8-15
+				const uint32_t rowOff = (m & 1u) ? 8u : 0u, col = 8u * (j + (m >> 1));
+				ldsm4t(bf, &sA[k + rowOff + rr][col]);
+				mma16816(acc[j], af, bf[0], bf[1]);
+				mma16816(acc[j + 1], af, bf[2], bf[3]);
+			}
+		}
+	}
+	if (!active) return;
+	// accumulator fragment: rows (outputs) g, g+8 of the warp's 16; columns 2c, 2c+1 of tile j
+	const uint32_t g = lane >> 2, c = lane & 3u;
+	float* dst = wGrad + wOffset(static_cast<int>(layer));
+#pragma unroll
+	for (int j = 0; j < 8; ++j)
+	{
+		const uint32_t o0 = warp * 16u + g, in0 = 8u * j + 2u * c;
+		atomicAdd(dst + o0 * kH + in0, acc[j][0]);
+		atomicAdd(dst + o0 * kH + in0 + 1, acc[j][1]);
+		atomicAdd(dst + (o0 + 8u) * kH + in0, acc[j][2]);
+		atomicAdd(dst + (o0 + 8u) * kH + in0 + 1, acc[j][3]);
 	}
 }
 
@@ -629,10 +797,10 @@ struct rb_nrc
 	uint32_t cap = 0;
 	__nv_bfloat16 *X = nullptr, *acts = nullptr, *dY = nullptr, *dH = nullptr;
 	float *out = nullptr, *dX0 = nullptr, *loss = nullptr;
-	cublasHandle_t blas = nullptr;
+	uint32_t* status = nullptr;            // RB_DEV_* bits of the network's kernels
 	uint32_t step = 0;
 	int smCount = 148;
-	uint32_t inferBlocksPerSm = 2;
+	uint32_t inferBlocksPerSm = 2, trainBlocksPerSm = 1;
 };
 
 namespace
@@ -672,21 +840,15 @@ int growScratch(rb_nrc* h, uint32_t n)
 	return RB_OK;
 }
 
-int blocksFor(const rb_nrc* h, uint32_t rows)
+// Blocks of the tcgen05 kernels: one 128-row tile per block and step, at
+// most perSm resident blocks per SM (the kernels loop over tiles).
+int tileBlocks(const rb_nrc* h, uint32_t rows, uint32_t perSm)
 {
-	const uint32_t tiles = (rows + kTile - 1) / kTile, perBlock = 4;   // 4 warps, one tile each
-	const uint32_t need = (tiles + perBlock - 1) / perBlock;
-	const uint32_t cap = static_cast<uint32_t>(h->smCount) * 4;
-	return static_cast<int>(need < 1 ? 1 : (need < cap ? need : cap));
+	const uint32_t tiles = (rows + t5::kRows - 1) / t5::kRows;
+	const uint32_t cap = static_cast<uint32_t>(h->smCount) * perSm;
+	return static_cast<int>(tiles < 1 ? 1 : (tiles < cap ? tiles : cap));
 }
-
-int inferBlocks(const rb_nrc* h, uint32_t rows)
-{
-	const uint32_t tiles = (rows + kTile - 1) / kTile, perBlock = kInferThreads / 32;
-	const uint32_t need = (tiles + perBlock - 1) / perBlock;
-	const uint32_t cap = static_cast<uint32_t>(h->smCount) * h->inferBlocksPerSm;
-	return static_cast<int>(need < 1 ? 1 : (need < cap ? need : cap));
-}
+int inferBlocks(const rb_nrc* h, uint32_t rows) { return tileBlocks(h, rows, h->inferBlocksPerSm); }
 
 int encodeBlocks(uint32_t rows)
 {
@@ -733,6 +895,8 @@ int rb_nrc_create(const rb_nrc_config* config, rb_nrc** out)
 	if (e == cudaSuccess) e = cudaMalloc(&h->w, sizeof(__nv_bfloat16) * kWTotal);
 	if (e == cudaSuccess) e = cudaMalloc(&h->wt, sizeof(__nv_bfloat16) * kWTotal);
 	if (e == cudaSuccess) e = cudaMalloc(&h->loss, sizeof(float));
+	if (e == cudaSuccess) e = cudaMalloc(&h->status, sizeof(uint32_t));
+	if (e == cudaSuccess) e = cudaMemset(h->status, 0, sizeof(uint32_t));
 	if (e != cudaSuccess) { rb_nrc_destroy(h); return nrcFail(e); }
 	cudaMemset(h->gridGrad, 0, sizeof(float) * gridN);
 	cudaMemset(h->gridM, 0, sizeof(float) * gridN);
@@ -754,16 +918,18 @@ int rb_nrc_create(const rb_nrc_config* config, rb_nrc** out)
 	std::memcpy(w.data() + wOffset(4), wo.data(), sizeof(float) * wo.size());
 	const int rc = rb_nrc_set_parameters(h, g.data(), w.data());
 	if (rc != RB_OK) { rb_nrc_destroy(h); return rc; }
-	if (cublasCreate(&h->blas) != CUBLAS_STATUS_SUCCESS) { rb_nrc_destroy(h); return RB_ERR_CUDA; }
-	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpForward), cudaFuncAttributeMaxDynamicSharedMemorySize,
-		static_cast<int>(kSmemWeights));
-	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpBackward), cudaFuncAttributeMaxDynamicSharedMemorySize,
-		static_cast<int>(kSmemBackward));
-	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpInfer), cudaFuncAttributeMaxDynamicSharedMemorySize,
-		static_cast<int>(kSmemInfer));
+	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpInferT), cudaFuncAttributeMaxDynamicSharedMemorySize,
+		static_cast<int>(t5::kSmem));
+	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpForwardT), cudaFuncAttributeMaxDynamicSharedMemorySize,
+		static_cast<int>(t5::kSmem));
+	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpBackwardT), cudaFuncAttributeMaxDynamicSharedMemorySize,
+		static_cast<int>(kSmemBackwardT));
 	int perSm = 0;
-	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMlpInfer, kInferThreads, kSmemInfer) == cudaSuccess && perSm > 0)
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMlpInferT, 128, t5::kSmem) == cudaSuccess && perSm > 0)
 		h->inferBlocksPerSm = static_cast<uint32_t>(perSm);
+	perSm = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMlpBackwardT, 128, kSmemBackwardT) == cudaSuccess && perSm > 0)
+		h->trainBlocksPerSm = static_cast<uint32_t>(perSm);
 	*out = h;
 	return RB_OK;
 }
@@ -775,14 +941,23 @@ int rb_nrc_destroy(rb_nrc* h)
 	cudaDeviceSynchronize();
 	for (void* p : { (void*)h->gridF32, (void*)h->gridGrad, (void*)h->gridM, (void*)h->gridV, (void*)h->grid,
 			(void*)h->wF32, (void*)h->wGrad, (void*)h->wM, (void*)h->wV, (void*)h->w, (void*)h->wt, (void*)h->X,
-			(void*)h->acts, (void*)h->dY, (void*)h->dH, (void*)h->out, (void*)h->dX0, (void*)h->loss })
+			(void*)h->acts, (void*)h->dY, (void*)h->dH, (void*)h->out, (void*)h->dX0, (void*)h->loss,
+			(void*)h->status })
 		if (p) cudaFree(p);
-	if (h->blas) cublasDestroy(h->blas);
 	delete h;
 	return RB_OK;
 }
 
 size_t rb_nrc_grid_size(void) { return static_cast<size_t>(kLevels) * kTable * kFeat; }
+
+int rb_nrc_status(rb_nrc* h, uint32_t* flags)
+{
+	if (!h || !flags) return RB_ERR_INVALID;
+	cudaSetDevice(h->device);
+	cudaError_t e = cudaDeviceSynchronize();
+	if (e == cudaSuccess) e = cudaMemcpy(flags, h->status, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+	return e == cudaSuccess ? RB_OK : nrcFail(e);
+}
 size_t rb_nrc_weight_count(void) { return kWTotal; }
 
 int rb_nrc_set_parameters(rb_nrc* h, const float* grid, const float* weights)
@@ -819,8 +994,8 @@ int rb_nrc_infer(rb_nrc* h, uint32_t n, const float* inputs, float* outputs, voi
 	if (n == 0) return RB_OK;
 	cudaSetDevice(h->device);
 	const cudaStream_t st = static_cast<cudaStream_t>(stream);
-	kMlpInfer<<<inferBlocks(h, n), kInferThreads, kSmemInfer, st>>>(n, nullptr, inputs, reinterpret_cast<const __half2*>(h->grid),
-		h->R, h->w, outputs, nullptr, nullptr, nullptr, nullptr);
+	kMlpInferT<<<inferBlocks(h, n), 128, t5::kSmem, st>>>(n, nullptr, inputs, reinterpret_cast<const __half2*>(h->grid),
+		h->R, h->w, outputs, nullptr, nullptr, nullptr, nullptr, h->status);
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
 
@@ -835,27 +1010,13 @@ int computeGradients(rb_nrc* h, uint32_t n, const float* inputs, const float* ta
 	if (rc != RB_OK) return rc;
 	cudaMemsetAsync(h->loss, 0, sizeof(float), st);
 	kEncode<<<encodeBlocks(n), kThreads, 0, st>>>(n, inputs, reinterpret_cast<const __half2*>(h->grid), h->R, h->X);
-	kMlpForward<<<blocksFor(h, n), 128, kSmemWeights, st>>>(n, h->X, h->w, h->out, h->acts);
+	kMlpForwardT<<<tileBlocks(h, n, h->inferBlocksPerSm), 128, t5::kSmem, st>>>(n, h->X, h->w, h->out, h->acts,
+		h->status);
 	kLoss<<<gridFor(n), kThreads, 0, st>>>(n, h->out, targets, h->dY, h->loss, valid, outs, tStride, corr);
-	kMlpBackward<<<blocksFor(h, n), 128, kSmemBackward, st>>>(n, h->dY, h->wt, h->acts, h->dH, h->dX0);
-	// weight gradients: dW_l[out][in] = sum over rows dY_l[r][out] X_l[r][in]
-	// (column-major view: dW^T = X^T dY with X [n][64] row-major = X^T column-major)
-	cublasSetStream(h->blas, st);
-	const float one = 1.0f;
-	const __nv_bfloat16* inputsOf[5] = { h->X, h->acts, h->acts + static_cast<size_t>(n) * kIn,
-		h->acts + 2 * static_cast<size_t>(n) * kIn, h->acts + 3 * static_cast<size_t>(n) * kIn };
-	for (int l = 0; l < 5; ++l)
-	{
-		const int outDim = l < 4 ? kH : kOutPad;
-		const __nv_bfloat16* dOut = l < 4 ? h->dH + static_cast<size_t>(l) * n * kIn : h->dY;
-		const int ldd = l < 4 ? kIn : kOutPad;
-		// C (col-major, in x out) = A (in x n) * B^T... written as C[in][out] += sum_r X[r][in] dOut[r][out]:
-		// A = X viewed col-major (in x n, lda = 64), B = dOut viewed col-major (out x n, ldb = ldd), op(B) = T.
-		if (cublasGemmEx(h->blas, CUBLAS_OP_N, CUBLAS_OP_T, kIn, outDim, static_cast<int>(n), &one, inputsOf[l],
-				CUDA_R_16BF, kIn, dOut, CUDA_R_16BF, ldd, &one, h->wGrad + wOffset(l), CUDA_R_32F, kIn,
-				CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT) != CUBLAS_STATUS_SUCCESS)
-			return RB_ERR_CUDA;
-	}
+	kMlpBackwardT<<<tileBlocks(h, n, h->trainBlocksPerSm), 128, kSmemBackwardT, st>>>(n, h->dY, h->wt, h->acts, h->dH,
+		h->dX0, h->status);
+	// weight gradients of the five layers, one launch
+	kWeightGrad<<<5 * ((n + kWgRows - 1) / kWgRows), 128, 0, st>>>(n, h->X, h->acts, h->dY, h->dH, h->wGrad);
 	kEncodeBackward<<<encodeBlocks(n), kThreads, 0, st>>>(n, inputs, h->dX0, h->R, h->gridGrad);
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
@@ -899,8 +1060,8 @@ int applyQueries(rb_nrc* h, uint32_t cap, const uint32_t* count, const float* in
 	const float4* T, const float* corr, cudaStream_t st)
 {
 	if (cap == 0) return RB_OK;
-	kMlpInfer<<<inferBlocks(h, cap), kInferThreads, kSmemInfer, st>>>(cap, count, inputs, reinterpret_cast<const __half2*>(h->grid),
-		h->R, h->w, nullptr, path, L, T, corr);
+	kMlpInferT<<<inferBlocks(h, cap), 128, t5::kSmem, st>>>(cap, count, inputs, reinterpret_cast<const __half2*>(h->grid),
+		h->R, h->w, nullptr, path, L, T, corr, h->status);
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
 

@@ -52,3 +52,42 @@ def build_for_scene(scene, camera=(0.0, 0.0, 0.0)) -> abi.rb_light_tree | None:
     if len(flux) == 0:
         return None
     return record(*build(world, flux, mat, prim, camera))
+
+
+def build_on_device(world: np.ndarray, flux: np.ndarray, material: np.ndarray, primitive: np.ndarray,
+                    camera=(0.0, 0.0, 0.0), stream=None, timing: list | None = None):
+    """The same records built on the device (rb_k_build_light_tree), copied
+    back: (triangles, nodes, pointers, bitmasks). Inputs are uploaded from
+    host arrays; with `timing`, the device milliseconds of the build (CUDA
+    events around the launch) are appended to it."""
+    import torch
+    n = len(flux)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    w = dev(np.asarray(world, np.float32).reshape(n, 9))
+    f = dev(np.asarray(flux, np.float32))
+    m = dev(np.asarray(material, np.uint32).view(np.int32))
+    pr = dev(np.asarray(primitive, np.uint32).view(np.int32))
+    lib = load()
+    scratch = torch.empty(max(int(lib.rb_k_build_light_tree_scratch_bytes(n)), 1), dtype=torch.uint8, device="cuda")
+    tris = torch.zeros(max(n, 1) * 68, dtype=torch.uint8, device="cuda")
+    nodes = torch.zeros(max(2 * n, 1) * 32, dtype=torch.uint8, device="cuda")
+    ptrs = torch.zeros(max(n, 1), dtype=torch.int32, device="cuda")
+    masks = torch.zeros(max(n, 1), dtype=torch.int64, device="cuda")
+    count = torch.zeros(1, dtype=torch.int32, device="cuda")
+    cam = np.ascontiguousarray(camera, np.float64)
+    p = lambda t: C.c_void_p(t.data_ptr())
+    s = torch.cuda.current_stream() if stream is None else stream
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    rc = lib.rb_k_build_light_tree(n, p(w), p(f), p(m), p(pr), C.c_void_p(cam.ctypes.data), p(scratch), p(tris),
+                                   p(nodes), p(ptrs), p(masks), p(count), C.c_void_p(s.cuda_stream))
+    b.record(s)
+    if rc != 0:
+        raise NativeError(f"rb_k_build_light_tree failed with status {rc}", rc)
+    b.synchronize()
+    if timing is not None:
+        timing.append(a.elapsed_time(b))
+    k = int(count.item())
+    out_tris = np.frombuffer(tris.cpu().numpy().tobytes(), abi.emissive_triangle_dtype())[:n].copy()
+    out_nodes = np.frombuffer(nodes.cpu().numpy().tobytes(), abi.packed_node_dtype())[:k].copy()
+    return out_tris, out_nodes, ptrs.cpu().numpy().view(np.uint32)[:n].copy(), masks.cpu().numpy().view(np.uint64)[:n].copy()

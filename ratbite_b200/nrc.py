@@ -55,6 +55,12 @@ class RadianceCache:
         check(self.lib.rb_nrc_train(self.h, n, C.c_void_p(inputs_ptr), C.c_void_p(targets_ptr),
                                     None if loss_ptr is None else C.c_void_p(loss_ptr), s), None, "rb_nrc_train")
 
+    def status(self) -> int:
+        """RB_DEV_* bits raised by the network's kernels (synchronizes)."""
+        f = C.c_uint32()
+        check(self.lib.rb_nrc_status(self.h, C.byref(f)), None, "rb_nrc_status")
+        return int(f.value)
+
     def gradients(self, n: int, inputs_ptr: int, targets_ptr: int):
         """(grid gradient, weight gradient) of the batch's mean loss, host arrays."""
         g = np.zeros(self.grid_size, np.float32)

@@ -125,6 +125,18 @@ class RenderingInterface:
         self._keep.append(launch)
         self.prepare_data_for_rendering(launch)
 
+    def build_lights(self, world, flux, material, primitive, stream=None):
+        """Builds the light tree on the device (rb_build_lights) from the
+        emissive triangles (host arrays, uploaded first) and installs it."""
+        import torch
+        n = len(flux)
+        dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        bufs = (dev(np.asarray(world, np.float32).reshape(n, 9)), dev(np.asarray(flux, np.float32)),
+                dev(np.asarray(material, np.uint32).view(np.int32)), dev(np.asarray(primitive, np.uint32).view(np.int32)))
+        torch.cuda.synchronize()
+        check(self.lib.rb_build_lights(self.ctx, n, *[C.c_void_p(b.data_ptr()) for b in bufs], stream), self.ctx,
+              "rb_build_lights")
+
     def update_instances(self, instance_transforms, subset_transforms=None, stream=None):
         """Moves the instances of the loaded geometry (the reference's
         updateInstanceAccelerationStructure on a camera move): (n, 3, 4)

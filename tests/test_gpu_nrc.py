@@ -127,6 +127,7 @@ def test_forward_matches_torch(torch):
     err = ((out - ref).abs() / (ref.abs() + 1e-2)).max().item()
     print(f"nrc forward: max rel err {err:.2e}, mean |y| {ref.abs().mean().item():.3e}")
     assert err < 2e-2
+    assert cache.status() == 0
     cache.close()
 
 
@@ -157,6 +158,14 @@ def test_gradients_match_torch_autograd(torch):
     assert cw > 0.999 and cg > 0.99
     assert abs(np.linalg.norm(wg) / np.linalg.norm(rw) - 1.0) < 2e-2
     assert abs(np.linalg.norm(gg) / np.linalg.norm(rg) - 1.0) < 2e-2
+    # every layer's weight gradient on its own (the output layer's live rows 0..3)
+    for l in range(5):
+        a, b = (l * 4096, (l + 1) * 4096) if l < 4 else (4 * 4096, 4 * 4096 + 4 * 64)
+        cl = cos(wg[a:b], rw[a:b])
+        print(f"  layer {l}: weight gradient cos {cl:.6f}")
+        assert cl > 0.999
+    assert not np.any(wg[4 * 4096 + 4 * 64:])        # padded output rows get no gradient
+    assert cache.status() == 0
     cache.close()
 
 
@@ -184,4 +193,5 @@ def test_training_fits_a_target(torch):
     print(f"nrc training: loss {first:.3e} -> {last:.3e}, held-out mean rel err {rel:.3e}")
     assert last < 0.05 * first
     assert rel < 0.1
+    assert cache.status() == 0
     cache.close()
