@@ -429,9 +429,13 @@ def run_ours(args, rank: int, world: int, wl: dict):
         if world == 1 and has_env and args.rows:
             rows = reference_kernel_rows(scene.envmap, ri.accumulation_device_ptr(), W, H)
         ttr = None
-        if args.ttr and world == 1 and args.workload == "scale":
-            ri.cleanup()                     # free this workload's wave before the second one
-            ttr = time_to_rmse(device=local)
+        batched = None
+        if world == 1 and args.workload == "scale" and (args.ttr or args.batched):
+            ri.cleanup()                     # free this workload's wave before the next ones
+            if args.ttr:
+                ttr = time_to_rmse(device=local)
+            if args.batched:
+                batched = batched_jobs(args.jobs, 1, device=local)
         line = {
             "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -461,6 +465,7 @@ def run_ours(args, rank: int, world: int, wl: dict):
             "cpu_baseline": {"value": cpu_v, "unit": "paths/s", "cores": cores, "kind": "reference",
                              "sample": sample},
             "time_to_rmse": ttr,
+            "batched_jobs": batched,
             "reference_kernels": rows,
         }
         print(json.dumps(line), flush=True)
@@ -560,40 +565,53 @@ def reference_kernel_rows(envmap: np.ndarray, accum_ptr: int, width: int, height
     return rows
 
 
-def run_batched(args):
-    """Batched jobs: 64 render jobs drawn from a seed (ratbite_b200.batch),
-    schedule chosen by the autotuner, aggregate paths/s and p50 / p99 job
-    completion latency (device events)."""
-    import torch
+def batched_jobs(n_jobs: int = 64, steps: int = 1, device: int = 0):
+    """Batched jobs: n_jobs render jobs drawn from a seed (ratbite_b200.batch),
+    the plain ones in one shared wavefront, schedule chosen by the autotuner;
+    aggregate paths/s and p50 / p99 job completion latency (device events)."""
     from ratbite_b200 import batch
 
     t0 = time.perf_counter()
-    jobs = batch.draw_jobs(seed=5, n=args.jobs)
-    br = batch.BatchRenderer(jobs, device=0)
+    jobs = batch.draw_jobs(seed=5, n=n_jobs)
+    cie, basis, luts, tables = bench_tables()
+    br = batch.BatchRenderer(jobs, device=device, tables=(cie, basis, luts))
     setup_s = time.perf_counter() - t0
+    t1 = time.perf_counter()
     best, trials = br.autotune()
+    tune_s = time.perf_counter() - t1
     runs = []
-    with ClockSampler(0) as clocks:
-        for _ in range(max(1, args.steps)):
+    with ClockSampler(device) as clocks:
+        for _ in range(max(1, steps)):
             runs.append(br.run(best))
     r = min(runs, key=lambda x: x.seconds)
-    line = {
-        "metric": METRIC, "value": r.paths_per_s, "unit": "paths/s", "n_gpus": 1, "steps": len(runs),
-        "warmup": 1, "ms_per_step": r.seconds * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scenes)",
-        "config": {"workload": f"batched_{len(jobs)}_jobs", "jobs": len(jobs),
-                   "sides": sorted({j.side for j in jobs}), "spp_range": [min(j.spp for j in jobs), max(j.spp for j in jobs)],
-                   "triangles_range": [min(j.triangles for j in jobs), max(j.triangles for j in jobs)],
-                   "forms": {f: sum(j.form == f for j in jobs) for f in ("plain", "cached")},
-                   "total_paths": r.total_paths, "setup_s": setup_s,
-                   "schedule": {"streams": best.streams, "samples_per_call": best.chunk, "paths_in_flight_per_job": best.max_paths},
-                   "autotune": [{"streams": c.streams, "samples_per_call": c.chunk, "paths_in_flight_per_job": c.max_paths,
-                                 "paths_per_s": v} for c, v in trials],
-                   "l2": "inputs larger than L2 (path state of every job's wave)"},
+    sched = lambda c: {"paths_in_flight": c.max_paths, "grid_percent": c.grid_percent, "cached_streams": c.streams,
+                       "cached_samples_per_call": c.chunk}
+    return {
+        "workload": f"batched_{len(jobs)}_jobs", "jobs": len(jobs), "value": r.paths_per_s, "unit": "paths/s",
+        "seconds": r.seconds, "runs": len(runs),
         "latency_s": {"p50": r.percentile(50), "p99": r.percentile(99), "max": max(r.latencies)},
-        "host_enqueue_s": r.host_seconds,
-        "gpu_launches": r.gpu_launches,
-        "clocks": clocks.summary(),
+        "sides": sorted({j.side for j in jobs}), "spp_range": [min(j.spp for j in jobs), max(j.spp for j in jobs)],
+        "triangles_range": [min(j.triangles for j in jobs), max(j.triangles for j in jobs)],
+        "forms": {f: sum(j.form == f for j in jobs) for f in ("plain", "cached")},
+        "plain_jobs": "one shared wavefront (rb_render_jobs)", "total_paths": r.total_paths,
+        "schedule": sched(best),
+        "autotune": [dict(sched(c), paths_per_s=v) for c, v in trials],
+        "setup_s": setup_s, "autotune_s": tune_s, "host_enqueue_s": r.host_seconds, "gpu_launches": r.gpu_launches,
+        "tables": tables, "clocks": clocks.summary(),
+    }
+
+
+def run_batched(args):
+    """The batched-jobs workload as its own bench line."""
+    b = batched_jobs(args.jobs, args.steps)
+    line = {
+        "metric": METRIC, "value": b["value"], "unit": "paths/s", "n_gpus": 1, "steps": b["runs"],
+        "warmup": 1, "ms_per_step": b["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scenes)",
+        "config": {k: b[k] for k in ("workload", "jobs", "sides", "spp_range", "triangles_range", "forms",
+                                     "total_paths", "schedule", "autotune", "plain_jobs", "tables")},
+        "latency_s": b["latency_s"], "host_enqueue_s": b["host_enqueue_s"], "gpu_launches": b["gpu_launches"],
+        "clocks": b["clocks"],
     }
     print(json.dumps(line), flush=True)
 
@@ -745,6 +763,8 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0 = the workload's)")
     ap.add_argument("--no-ttr", dest="ttr", action="store_false",
                     help="skip the time-to-RMSE measurement of the cached form (1920x1080 Cornell box, ~30 s)")
+    ap.add_argument("--no-batched", dest="batched", action="store_false",
+                    help="skip the batched-jobs measurement (64 jobs in one shared wavefront, ~1 min)")
     ap.add_argument("--no-rows", dest="rows", action="store_false",
                     help="skip the head-to-head timing of the env-map CDF and resolve kernels against the "
                          "reference's own CUDA kernels")

@@ -315,6 +315,26 @@ int rb_render(rb_ctx* ctx, uint32_t sample_offset, uint32_t sample_count, void* 
  * any setter, a new launch size or a new wave capacity captures anew. With a
  * radiance cache attached or statistics on, it is rb_render. */
 int rb_render_graph(rb_ctx* ctx, uint32_t sample_offset, uint32_t sample_count, void* stream);
+
+/* Several render jobs in one shared wavefront (no reference counterpart:
+ * the reference renders one scene per launch). Job j is context jobs[j] with
+ * its own scene, launch parameters and accumulation buffer; it renders
+ * samples [offsets[j], offsets[j] + counts[j]) as rb_render(jobs[j], ...)
+ * would (the same sample sequences and accumulation order, so the same
+ * bits). Waves are filled with whole sample planes of the jobs in order and
+ * mix jobs freely: every kernel of a wave serves all of its jobs' paths, each
+ * path reading its job's scene. The wave buffers live in jobs[0]. Plain form
+ * only (no attached radiance cache); films up to 65535 pixels a side. Jobs
+ * must not render elsewhere while the call runs. Stream-ordered on `stream`
+ * (0: jobs[0]'s stream) after the job and chunk tables are copied. */
+typedef struct rb_jobs_options {
+    uint32_t max_paths_in_flight; /* wave capacity (queue capacity) in paths; 0 = jobs[0]'s */
+    uint32_t grid_percent;        /* blocks per kernel launch, % of the resident maximum; 0 = 100 */
+    void* const* done_events;     /* per job a cudaEvent_t recorded on `stream` after the wave that
+                                     finishes the job, or NULL */
+} rb_jobs_options;
+int rb_render_jobs(rb_ctx* const* jobs, uint32_t n, const uint32_t* offsets, const uint32_t* counts,
+                   const rb_jobs_options* options, void* stream);
 /* Copies the width*height*4 doubles (sum X, sum Y, sum Z, sample count) of
  * the accumulation buffer (renderData) to host memory; synchronizes. */
 int rb_read_accum(rb_ctx* ctx, double* out);

@@ -96,6 +96,10 @@ RB_FAILED_DROP = 0
 RB_FAILED_KEEP = 1
 
 
+class rb_jobs_options(C.Structure):
+    _fields_ = [("max_paths_in_flight", C.c_uint32), ("grid_percent", C.c_uint32), ("done_events", C.c_void_p)]
+
+
 class rb_material(C.Structure):
     _fields_ = [
         ("bxdf", C.c_uint32), ("double_sided", C.c_uint32), ("sheen_present", C.c_uint32),

@@ -2,18 +2,20 @@
 count and scene size rendered together (no counterpart in the reference,
 which renders one scene interactively).
 
-Every job has its own context (scene, light tree, wavefront buffers) on the
-same device. The scheduler spreads the jobs over `streams` CUDA streams
-(longest job first onto the least-loaded stream, then shortest first within
-each stream, which keeps the median completion time low), and renders each
-job in calls of `chunk` samples per pixel through rb_render_graph, so a
-job's wave sequence is one graph launch per call after the first. All work
-is enqueued up front; a job's completion time is a CUDA event after its last
-call, against one start event that every stream waits on.
+Every job has its own context (scene, light tree, accumulation) on the same
+device. The plain jobs render in one shared wavefront (rb_render_jobs):
+waves are filled with whole sample planes of the jobs, shortest job first
+(which keeps the median completion time low), and every kernel of a wave
+serves all of its jobs' paths. Jobs of the cached form (the radiance cache,
+whose network is per job) render on their own contexts on `streams` CUDA
+streams alongside, in calls of `chunk` samples per pixel. A job's
+completion time is a CUDA event recorded after the wave (or call) that
+finishes it, against one start event.
 
-The autotuner picks the stream count, the samples per call and the paths in
-flight per job (the wavefront queue capacity) by timing the schedule on a
-small, shortened sample of the jobs.
+The autotuner picks the shared wavefront's queue capacity (paths in flight
+per wave) and its grid size (blocks launched per kernel, as a percentage of
+the resident maximum), and the stream count of the cached jobs, by timing
+the schedule on a small, shortened sample of the jobs.
 """
 from __future__ import annotations
 
@@ -26,7 +28,7 @@ import numpy as np
 
 from . import assets, lighttree, scenes
 from .nrc import RadianceCache
-from .rendering_interface import RenderingInterface
+from .rendering_interface import RenderingInterface, render_jobs
 
 SIDES = tuple(128 * k for k in range(1, 9))      # square images 128^2 .. 1024^2
 
@@ -63,11 +65,13 @@ def draw_jobs(seed: int = 5, n: int = 64, forms=("plain", "cached")) -> list[Job
 
 @dataclass
 class Schedule:
-    streams: int = 4
-    chunk: int = 64                 # samples per pixel per render call
-    max_paths: int = 2 << 20        # wavefront capacity per job
+    max_paths: int = 8 << 20        # shared wavefront: paths in flight per wave (queue capacity)
+    grid_percent: int = 100         # shared wavefront: blocks per kernel launch, % of the resident maximum
+    streams: int = 4                # cached jobs: CUDA streams
+    chunk: int = 64                 # cached jobs: samples per pixel per render call
 
     def capacity(self, job: Job) -> int:
+        """Wavefront capacity of a cached job's own context."""
         return min(job.side * job.side * min(self.chunk, job.spp), self.max_paths)
 
 
@@ -87,13 +91,16 @@ class Result:
 
 
 class BatchRenderer:
-    """Holds the jobs' scenes on the host; contexts are created per run."""
+    """Holds the jobs' scenes on the host; contexts are created per run.
+    tables: (cie_xyz, basis_rgb, luts) for every job (default: the built-in
+    stand-ins with LUTs regenerated on the GPU)."""
 
-    def __init__(self, jobs: list[Job], device: int = 0, max_depth: int = 12, threads: int = 8):
+    def __init__(self, jobs: list[Job], device: int = 0, max_depth: int = 12, threads: int = 8, tables=None):
         self.jobs = jobs
         self.device = device
-        self.cie, self.basis = assets.cie_xyz(), assets.basis_rgb()
-        self.luts = assets.generated_luts(samples=1 << 14, device=device)   # regenerated on the GPU
+        if tables is None:
+            tables = (assets.cie_xyz(), assets.basis_rgb(), assets.generated_luts(samples=1 << 14, device=device))
+        self.cie, self.basis, self.luts = tables
 
         def build(job):
             sc = scenes.scale_scene(seed=job.seed, target_tris=job.triangles,
@@ -118,49 +125,61 @@ class BatchRenderer:
     def run(self, schedule: Schedule, jobs: list[Job] | None = None, spp_cap: int | None = None,
             keep_images: bool = False) -> Result:
         """Renders `jobs` (default: all) under `schedule`; spp_cap shortens
-        every job (autotuning). Contexts are set up, and wave buffers and
-        graphs allocated by one untimed call each, before the timed region."""
+        every job (autotuning). Contexts are set up, and wave buffers
+        allocated by one untimed call each, before the timed region."""
         import torch
 
         jobs = list(self.jobs if jobs is None else jobs)
         torch.cuda.set_device(self.device)
         spp_of = {j.index: (min(j.spp, spp_cap) if spp_cap else j.spp) for j in jobs}
+        plain = sorted([j for j in jobs if j.form == "plain"], key=lambda j: (j.side * j.side * spp_of[j.index], j.index))
+        cached = [j for j in jobs if j.form != "plain"]
         ctxs, caches = {}, {}
         for j in jobs:
             sc, lt = self.scenes[j.index]
-            ri = RenderingInterface(device=self.device, max_paths_in_flight=schedule.capacity(j))
+            cap = schedule.max_paths if j.form == "plain" else schedule.capacity(j)
+            ri = RenderingInterface(device=self.device, max_paths_in_flight=cap)
             ri.load_scene(sc, self.luts, self.cie, self.basis, light_tree=lt, max_depth=sc.max_depth)
             if j.form == "cached":
                 caches[j.index] = RadianceCache(device=self.device, seed=j.seed)
                 ri.attach_radiance_cache(caches[j.index])
             ctxs[j.index] = ri
-        streams = [torch.cuda.Stream(device=self.device) for _ in range(schedule.streams)]
-        lanes = self._assign(jobs, schedule.streams)
-        # untimed warm-up: allocate every job's buffers and capture its graph shapes
+        streams = [torch.cuda.Stream(device=self.device) for _ in range(max(1, schedule.streams))]
+        shared = torch.cuda.Stream(device=self.device)
+        lanes = self._assign(cached, len(streams))
+        plain_ris = [ctxs[j.index] for j in plain]
+
+        def shared_call(offsets, counts, events=None):
+            render_jobs(plain_ris, offsets, counts, max_paths=schedule.max_paths, grid_percent=schedule.grid_percent,
+                        done_events=events, stream=shared.cuda_stream)
+
+        # untimed warm-up: the shared wave's buffers, every cached job's buffers
+        if plain:
+            shared_call([1 << 24] * len(plain), [1] * len(plain))
         for k, lane in enumerate(lanes):
             for j in lane:
-                n = spp_of[j.index]
-                sizes = {min(schedule.chunk, n)} | ({n % schedule.chunk} if n % schedule.chunk else set())
-                for c in sizes:
-                    self._call(ctxs[j.index], j, 1 << 24, c, streams[k])
+                ctxs[j.index].render(1 << 24, min(schedule.chunk, spp_of[j.index]), stream=streams[k].cuda_stream)
         torch.cuda.synchronize()
         for ri in ctxs.values():                      # launch counters start here
             ri.get_stats()
             ri.cache_stats() if ri._cache is not None else None
+        ends = {j.index: torch.cuda.Event(enable_timing=True) for j in jobs}
+        for e in ends.values():
+            e.record()                               # creates the events (the shared call records them again)
         start = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
         start.record(torch.cuda.current_stream())
-        for s in streams:
+        for s in streams + [shared]:
             s.wait_event(start)
-        ends = {}
         t0 = time.perf_counter()
         for k, lane in enumerate(lanes):
             for j in lane:
                 n = spp_of[j.index]
                 for off in range(0, n, schedule.chunk):
-                    self._call(ctxs[j.index], j, off, min(schedule.chunk, n - off), streams[k])
-                e = torch.cuda.Event(enable_timing=True)
-                e.record(streams[k])
-                ends[j.index] = e
+                    ctxs[j.index].render(off, min(schedule.chunk, n - off), stream=streams[k].cuda_stream)
+                ends[j.index].record(streams[k])
+        if plain:
+            shared_call([0] * len(plain), [spp_of[j.index] for j in plain], [ends[j.index] for j in plain])
         torch.cuda.synchronize()
         host_s = time.perf_counter() - t0
         lat = [start.elapsed_time(ends[j.index]) / 1e3 for j in jobs]
@@ -183,19 +202,12 @@ class BatchRenderer:
         res.gpu_launches = launches
         return res
 
-    @staticmethod
-    def _call(ri, job: Job, offset: int, count: int, stream):
-        if job.form == "cached":
-            ri.render(offset, count, stream=stream.cuda_stream)
-        else:
-            ri.render_graph(offset, count, stream=stream.cuda_stream)
-
-    def autotune(self, candidates=None, sample: int = 12, spp_cap: int = 32) -> tuple[Schedule, list]:
+    def autotune(self, candidates=None, sample: int = 8, spp_cap: int = 16) -> tuple[Schedule, list]:
         """Times each candidate schedule on `sample` jobs (spread over the
         job sizes) shortened to spp_cap samples, and returns the one with the
         highest throughput with the table of trials."""
         if candidates is None:
-            candidates = [Schedule(s, c, 2 << 20) for s in (4, 8, 16) for c in (32, 64, 128)]
+            candidates = [Schedule(m << 20, g, 4, 64) for m in (4, 16) for g in (50, 100, 200)]
         order = sorted(self.jobs, key=lambda j: j.paths)
         pick = [order[int(i)] for i in np.linspace(0, len(order) - 1, min(sample, len(order)))]
         trials = []

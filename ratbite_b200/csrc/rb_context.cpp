@@ -45,6 +45,16 @@ struct rb_ctx
 	uint32_t requestedCapacity = 0;
 	uint32_t cdfMode = RB_CDF_FP64;
 	uint32_t failedMode = RB_FAILED_DROP;
+	// shared wavefront of rb_render_jobs (this context hosts it): per-path job
+	// index and key, the job table and the chunk table of a call
+	std::vector<void*> jobBufs;
+	uint32_t* jobIdx = nullptr;
+	uint2* jobKey = nullptr;
+	uint32_t jobPathCap = 0;
+	rb::DevJob* jobTable = nullptr;
+	uint32_t jobTableCap = 0;
+	rb::WaveChunk* chunkTable = nullptr;
+	uint32_t chunkCap = 0;
 	// fault injection (rb_config.inject_*; tests only)
 	uint32_t injectQueueLimit = 0, injectAllocFailure = 0, injectStackLimit = 0;
 	uint64_t allocCount = 0;                    // device allocations made so far
@@ -509,6 +519,7 @@ int rb_destroy(rb_ctx* ctx)
 	for (auto* v : { &ctx->lutBufs, &ctx->spectraBufs, &ctx->materialBufs, &ctx->geoBufs, &ctx->lightBufs, &ctx->envBufs })
 		freeAll(*v);
 	releaseWave(ctx);
+	freeAll(ctx->jobBufs);
 	freeAll(ctx->cacheBufs);
 	if (ctx->cacheTally) cudaFree(ctx->cacheTally);
 	if (ctx->cacheCorr) cudaFree(ctx->cacheCorr);
@@ -1222,6 +1233,160 @@ int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 	if (rc != RB_OK) return rc;
 	cudaSetDevice(ctx->device);
 	return renderWaves(ctx, offset, count, pick(ctx, stream), nullptr);
+}
+
+int rb_render_jobs(rb_ctx* const* jobs, uint32_t n, const uint32_t* offsets, const uint32_t* counts,
+	const rb_jobs_options* options, void* stream)
+{
+	if (!jobs || n == 0 || !offsets || !counts || !jobs[0]) return RB_ERR_INVALID;
+	rb_ctx* host = jobs[0];
+	for (uint32_t j = 0; j < n; ++j)
+	{
+		rb_ctx* c = jobs[j];
+		if (!c || c->device != host->device) return fail(host, RB_ERR_INVALID, "rb_render_jobs: jobs must share one device");
+		int rc = renderReady(c);
+		if (rc == RB_OK) rc = checkReferences(c);
+		if (rc != RB_OK) return fail(host, rc, "rb_render_jobs: a job's scene is incomplete");
+		if (c->cache) return fail(host, RB_ERR_UNSUPPORTED, "rb_render_jobs: jobs render the plain form");
+		if (c->scene.launch.width > 65535 || c->scene.launch.height > 65535)
+			return fail(host, RB_ERR_INVALID, "rb_render_jobs: film side above 65535");
+		if (static_cast<uint64_t>(offsets[j]) + counts[j] > 0xFFFFFFFFull)
+			return fail(host, RB_ERR_INVALID, "rb_render_jobs: sample range overflows");
+	}
+	cudaSetDevice(host->device);
+	const cudaStream_t st = pick(host, stream);
+	// wave capacity: at least the largest job's plane
+	uint32_t maxPixels = 1;
+	int bounces = 1;
+	for (uint32_t j = 0; j < n; ++j)
+	{
+		const rb::DevLaunch& L = jobs[j]->scene.launch;
+		maxPixels = std::max(maxPixels, L.width * L.height);
+		bounces = std::max(bounces, static_cast<int>(std::min<uint32_t>(rb::kMaxBounces,
+			std::max({ L.maxDepth, L.maxReflected, L.maxTransmitted }))));
+	}
+	const uint32_t want = options && options->max_paths_in_flight ? options->max_paths_in_flight
+		: (host->requestedCapacity ? host->requestedCapacity : (16u << 20));
+	const uint32_t cap = std::max(want, maxPixels);
+	// the waves: jobs in order, whole sample planes, chunks of consecutive planes
+	struct Wave { uint32_t firstChunk, chunks, paths, pixelSlots; };
+	std::vector<uint32_t> lastWave(n, 0);
+	std::vector<rb::WaveChunk> chunks;
+	std::vector<Wave> waves;
+	{
+		Wave cur{ 0, 0, 0, 0 };
+		for (uint32_t j = 0; j < n; ++j)
+		{
+			const rb::DevLaunch& L = jobs[j]->scene.launch;
+			const uint32_t pixels = L.width * L.height;
+			uint32_t done = 0;
+			while (done < counts[j])
+			{
+				uint32_t fit = (cap - cur.paths) / pixels;
+				if (fit == 0)
+				{
+					waves.push_back(cur);
+					cur = Wave{ static_cast<uint32_t>(chunks.size()), 0, 0, 0 };
+					continue;
+				}
+				const uint32_t planes = std::min(fit, counts[j] - done);
+				rb::WaveChunk c{};
+				c.job = j;
+				c.slot = cur.paths;
+				c.pixel = cur.pixelSlots;
+				c.planes = planes;
+				c.sample = offsets[j] + done;
+				c.fresh = (offsets[j] == 0 && done == 0) ? 1u : 0u;
+				c.pixels = pixels;
+				c.width = L.width;
+				c.height = L.height;
+				chunks.push_back(c);
+				lastWave[j] = static_cast<uint32_t>(waves.size());
+				++cur.chunks;
+				cur.paths += planes * pixels;
+				cur.pixelSlots += pixels;
+				done += planes;
+			}
+		}
+		if (cur.chunks) waves.push_back(cur);
+	}
+	if (waves.empty()) return RB_OK;
+	uint32_t wavePaths = 0;
+	for (const Wave& w : waves) wavePaths = std::max(wavePaths, w.paths);
+	int rc = ensureWave(host, wavePaths);
+	if (rc != RB_OK) return rc;
+	// per-path job arrays, job and chunk tables (grown on demand)
+	if (host->jobPathCap < host->capacity || host->jobTableCap < n || host->chunkCap < chunks.size())
+	{
+		cudaStreamSynchronize(host->stream);
+		cudaStreamSynchronize(st);
+		freeAll(host->jobBufs);
+		host->jobPathCap = host->jobTableCap = host->chunkCap = 0;
+		rc = upload(host, host->jobBufs, nullptr, sizeof(uint32_t) * host->capacity, host->jobIdx);
+		if (rc == RB_OK) rc = upload(host, host->jobBufs, nullptr, sizeof(uint2) * host->capacity, host->jobKey);
+		if (rc == RB_OK) rc = upload(host, host->jobBufs, nullptr, sizeof(rb::DevJob) * n, host->jobTable);
+		if (rc == RB_OK) rc = upload(host, host->jobBufs, nullptr, sizeof(rb::WaveChunk) * chunks.size(), host->chunkTable);
+		if (rc != RB_OK) { freeAll(host->jobBufs); return rc; }
+		host->jobPathCap = host->capacity;
+		host->jobTableCap = n;
+		host->chunkCap = static_cast<uint32_t>(chunks.size());
+	}
+	std::vector<rb::DevJob> table(n);
+	for (uint32_t j = 0; j < n; ++j)
+	{
+		table[j] = rb::DevJob{};
+		table[j].scene = jobs[j]->scene;
+		table[j].accum = jobs[j]->accum;
+		table[j].keepFailed = jobs[j]->failedMode == RB_FAILED_KEEP ? 1u : 0u;
+	}
+	// the tables are copied from host memory that lives until the copies are done
+	if (cudaMemcpyAsync(host->jobTable, table.data(), sizeof(rb::DevJob) * n, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+		cudaMemcpyAsync(host->chunkTable, chunks.data(), sizeof(rb::WaveChunk) * chunks.size(), cudaMemcpyHostToDevice, st)
+			!= cudaSuccess)
+		return fail(host, RB_ERR_CUDA, "rb_render_jobs: tables");
+	rb::PathSoA soa = host->soa;
+	soa.jobs = host->jobTable;
+	soa.job = host->jobIdx;
+	soa.key = host->jobKey;
+	rb::LaunchShape shape = host->shape;
+	const uint32_t pct = options && options->grid_percent ? options->grid_percent : 100u;
+	for (int* b : { &shape.blocksGenerate, &shape.blocksExtend, &shape.blocksSurface, &shape.blocksEmission,
+			&shape.blocksNeePick, &shape.blocksNee, &shape.blocksBsdf, &shape.blocksBsdfLight, &shape.blocksShadow,
+			&shape.blocksResolve })
+		*b = std::max(1, static_cast<int>(static_cast<uint64_t>(*b) * pct / 100u));
+	const rb::DevScene& sc = host->scene;
+	for (uint32_t k = 0; k < waves.size(); ++k)
+	{
+		const Wave& wv = waves[k];
+		rb::WaveParams w{};
+		w.paths = wv.paths;
+		w.pixels = 1;
+		w.chunks = host->chunkTable + wv.firstChunk;
+		w.nChunks = wv.chunks;
+		w.pixelSlots = wv.pixelSlots;
+		shape.items = w.paths;
+		cudaMemsetAsync(soa.counts, 0, sizeof(uint32_t) * rb::kCountSlots, st);
+		rb::launchGenerate(sc, soa, w, shape, st);
+		for (int b = 0; b < bounces; ++b)
+		{
+			rb::launchExtend(sc, soa, b, shape, st, nullptr);
+			rb::launchSurface(sc, soa, w, b, shape, st, nullptr);
+			rb::launchEmission(sc, soa, b, shape, st);
+			rb::launchNee(sc, soa, w, b, shape, st);
+			rb::launchBsdf(sc, soa, w, b, shape, st);
+			rb::launchShadow(sc, soa, b, shape, st, nullptr);
+		}
+		rb::launchResolve(sc, soa, w, nullptr, shape, st);
+		host->pathsTraced += w.paths;
+		++host->waves;
+		if (options && options->done_events)
+			for (uint32_t j = 0; j < n; ++j)
+				if (counts[j] && lastWave[j] == k && options->done_events[j])
+					cudaEventRecord(static_cast<cudaEvent_t>(options->done_events[j]), st);
+	}
+	const cudaError_t e = cudaGetLastError();
+	if (e != cudaSuccess) return cudaFail(host, e, "rb_render_jobs");
+	return RB_OK;
 }
 
 int rb_render_graph(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)

@@ -257,14 +257,61 @@ RB_D uint2 slotPixel(uint32_t slot, uint32_t W, uint32_t H)
 	return make_uint2(8u * c + r % cw, 4u * band + r / cw);
 }
 
+// Shared wavefront (rb_render_jobs): the chunk holding path slot `slot`, or
+// pixel slot `px` of the resolve (the last chunk starting at or before it).
+RB_D uint32_t chunkOfSlot(const WaveParams& w, uint32_t slot)
+{
+	uint32_t lo = 0, hi = w.nChunks;
+	while (hi - lo > 1)
+	{
+		const uint32_t mid = (lo + hi) >> 1;
+		if (w.chunks[mid].slot <= slot) lo = mid; else hi = mid;
+	}
+	return lo;
+}
+RB_D uint32_t chunkOfPixel(const WaveParams& w, uint32_t px)
+{
+	uint32_t lo = 0, hi = w.nChunks;
+	while (hi - lo > 1)
+	{
+		const uint32_t mid = (lo + hi) >> 1;
+		if (w.chunks[mid].pixel <= px) lo = mid; else hi = mid;
+	}
+	return lo;
+}
+// The scene of path p: the kernel's own, or in a shared wavefront its job's.
+template<bool JOBS>
+RB_D const DevScene& pathScene(const DevScene& own, const PathSoA& s, uint32_t p)
+{
+	return JOBS ? s.jobs[s.job[p]].scene : own;
+}
+
 // ------------------------------------------------------------- kernels
-__global__ void __launch_bounds__(kThreads) kGenerate(DevScene sc, PathSoA s, WaveParams w)
+template<bool JOBS>
+__global__ void __launch_bounds__(kThreads) kGenerate(const __grid_constant__ DevScene scK, PathSoA s, WaveParams w)
 {
 	for (uint32_t p = gtid(); p < w.paths; p += gstride())
 	{
-		const uint2 px = slotPixel(p % w.pixels, sc.launch.width, sc.launch.height);
-		const uint32_t x = px.x, y = px.y;
-		const uint32_t sample = waveSampleBase(w) + p / w.pixels;
+		uint32_t x, y, sample;
+		const DevScene* scp = &scK;
+		if (JOBS)
+		{
+			const WaveChunk c = w.chunks[chunkOfSlot(w, p)];
+			const uint32_t local = p - c.slot;
+			const uint2 px = slotPixel(local % c.pixels, c.width, c.height);
+			x = px.x; y = px.y;
+			sample = c.sample + local / c.pixels;
+			s.job[p] = c.job;
+			s.key[p] = make_uint2(x | (y << 16), sample);
+			scp = &s.jobs[c.job].scene;
+		}
+		else
+		{
+			const uint2 px = slotPixel(p % w.pixels, scK.launch.width, scK.launch.height);
+			x = px.x; y = px.y;
+			sample = waveSampleBase(w) + p / w.pixels;
+		}
+		const DevScene& sc = *scp;
 		const Qrng q = qrngAt(sample, pixelHash(x, y), 0);
 		const Wavelengths wl = sampleVisible(sample1D(q, DIM_WAVELENGTH));
 		float fu, fv, dx, dy, lu = 0.0f, lv = 0.0f;
@@ -328,6 +375,17 @@ RB_D Qrng pathQrng(const DevScene& sc, const WaveParams& w, uint32_t p, uint32_t
 {
 	const uint2 px = slotPixel(p % w.pixels, sc.launch.width, sc.launch.height);
 	return qrngAt(waveSampleBase(w) + p / w.pixels, pixelHash(px.x, px.y), depth);
+}
+// ... of a path of either kind of wave (a shared wavefront keeps the keys).
+template<bool JOBS>
+RB_D Qrng pathQrngT(const DevScene& sc, const WaveParams& w, const PathSoA& s, uint32_t p, uint32_t depth)
+{
+	if (JOBS)
+	{
+		const uint2 k = s.key[p];
+		return qrngAt(k.y, pixelHash(k.x & 0xFFFFu, k.x >> 16), depth);
+	}
+	return pathQrng(sc, w, p, depth);
 }
 
 // wavelength range of the hero sampling, for the cache's normalised input
@@ -396,8 +454,9 @@ RB_D bool cacheVertex(const PathSoA& s, const WaveParams& w, uint32_t* status, u
 // continue get a surface record and join the surface queue, which the light
 // sampling and BxDF stages read.
 // counters (optional): [6] surface records.
-__global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevScene sc, PathSoA s, WaveParams w, int bounce,
-	unsigned long long* counters)
+template<bool JOBS>
+__global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(const __grid_constant__ DevScene scK, PathSoA s,
+	WaveParams w, int bounce, unsigned long long* counters)
 {
 	const uint32_t n = min(s.counts[bounce], s.queueCap);
 	const uint32_t* queue = s.queue[bounce & 1];
@@ -406,6 +465,7 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
 		const uint32_t p = queue[i];
+		const DevScene& sc = pathScene<JOBS>(scK, s, p);
 		const float4 ro = s.rayO[p], rd = s.rayD[p];
 		const f3 rayO = f3_of(ro), rayD = f3_of(rd);
 		const float bxdfPdf = rd.w;
@@ -485,7 +545,7 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 			if (flags & PF_TRIANGULAR_GEOMETRY)
 			{
 				shadingFrame(sc, mat, it, rayD, frame, lastNormal);
-				skipped = alphaSkipped(mat, pathQrng(sc, w, p, depth));
+				skipped = alphaSkipped(mat, pathQrngT<JOBS>(sc, w, s, p, depth));
 			}
 			if (w.cached)
 			{
@@ -531,12 +591,14 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(DevS
 // (pathtrace.cu:1185-1274): the light-tree pdf of the hit light replayed from
 // the previous vertex, the power heuristic, and the contribution, with the
 // values kSurface queued for it; the same arithmetic as the inline case.
-__global__ void __launch_bounds__(kThreads) kEmission(DevScene sc, PathSoA s, int bounce)
+template<bool JOBS>
+__global__ void __launch_bounds__(kThreads) kEmission(const __grid_constant__ DevScene scK, PathSoA s, int bounce)
 {
 	const uint32_t n = min(s.counts[kEmissionCounts + bounce], s.queueCap);
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
 		const uint32_t p = s.emQueue[i];
+		const DevScene& sc = pathScene<JOBS>(scK, s, p);
 		const float4 a = s.emA[i], b = s.emB[i];
 		const float treePdf = lightTreePdf(sc, kLightTypeTriangle, s.emLight[i], f3_of(a), f3_of(b));
 		float lightPdf = b.w;
@@ -565,20 +627,22 @@ __global__ void __launch_bounds__(kThreads) kEmission(DevScene sc, PathSoA s, in
 // environment (and all records when neither the tree nor the environment
 // exists) go to queue 1, tree picks to queue 0. The choice uses the same
 // sample dimension and comparison as the light-sample body that follows.
-__global__ void __launch_bounds__(kThreads) kNeePick(DevScene sc, PathSoA s, WaveParams w, int bounce)
+template<bool JOBS>
+__global__ void __launch_bounds__(kThreads) kNeePick(const __grid_constant__ DevScene scK, PathSoA s, WaveParams w, int bounce)
 {
 	const uint32_t n = min(s.counts[kSurfaceCounts + bounce], s.queueCap);
-	const bool envPresent = sc.env.enabled != 0;
-	const bool treePresent = sc.lights.nodes != nullptr;
-	const float envImp = envPresent ? (treePresent ? kEnvMapImportance : 1.0f) : 0.0f;
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
 		const uint32_t p = s.surfQueue[i];
 		if (__float_as_uint(s.sfPi[p].w) & kSfSkipped) continue;
+		const DevScene& sc = pathScene<JOBS>(scK, s, p);
+		const bool envPresent = sc.env.enabled != 0;
+		const bool treePresent = sc.lights.nodes != nullptr;
+		const float envImp = envPresent ? (treePresent ? kEnvMapImportance : 1.0f) : 0.0f;
 		bool sky = true;
 		if (envPresent || treePresent)
 		{
-			const Qrng q = pathQrng(sc, w, p, s.fd[p].y);
+			const Qrng q = pathQrngT<JOBS>(sc, w, s, p, s.fd[p].y);
 			sky = sample3D(q, DIM_LIGHT).z < envImp;
 		}
 		// one counter per branch: appendIndex aggregates over the lanes active at the call
@@ -604,27 +668,30 @@ __global__ void __launch_bounds__(kThreads) kNeePick(DevScene sc, PathSoA s, Wav
 // The records come from one of kNeePick's queues (`which`: 0 tree picks,
 // 1 environment picks), so a warp's lanes take the same branch of the light
 // choice; the body is the same for both.
-template<bool SHARED>
+// JOBS (a shared wavefront; never with SHARED): each record's tree is its job's.
+template<bool SHARED, bool JOBS>
 __global__ void __launch_bounds__(SHARED ? kNeeSharedThreads : kThreads, SHARED ? 2 : RB_NEE_MIN_BLOCKS)
-kNee(DevScene sc, PathSoA s, WaveParams w, int bounce, int which)
+kNee(const __grid_constant__ DevScene scK, PathSoA s, WaveParams w, int bounce, int which)
 {
 	extern __shared__ float4 sharedTree[];
 	const uint32_t n = min(s.counts[(which ? kNeeSkyCounts : kNeeTreeCounts) + bounce], s.queueCap);
 	const uint32_t* queue = s.neeQueue[which];
-	const TreeNodeU* nodes = sc.lights.unpacked;
+	const TreeNodeU* sharedNodes = scK.lights.unpacked;
 	if (SHARED)
 	{
-		const float4* src = reinterpret_cast<const float4*>(sc.lights.unpacked);
-		const uint32_t words = 3u * sc.lights.nodeCount;
+		const float4* src = reinterpret_cast<const float4*>(scK.lights.unpacked);
+		const uint32_t words = 3u * scK.lights.nodeCount;
 		for (uint32_t k = threadIdx.x; k < words; k += blockDim.x) sharedTree[k] = __ldg(src + k);
 		__syncthreads();
-		nodes = reinterpret_cast<const TreeNodeU*>(sharedTree);
+		sharedNodes = reinterpret_cast<const TreeNodeU*>(sharedTree);
 	}
-	const bool envPresent = sc.env.enabled != 0;
-	const bool treePresent = sc.lights.nodes != nullptr;
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
 		const uint32_t p = queue[i];
+		const DevScene& sc = pathScene<JOBS>(scK, s, p);
+		const TreeNodeU* nodes = JOBS ? sc.lights.unpacked : sharedNodes;
+		const bool envPresent = sc.env.enabled != 0;
+		const bool treePresent = sc.lights.nodes != nullptr;
 		const float4 pi = s.sfPi[p];
 		uint32_t bits = __float_as_uint(pi.w);
 		const float4 hp = s.sfP[p];
@@ -641,7 +708,7 @@ kNee(DevScene sc, PathSoA s, WaveParams w, int bounce, int which)
 		{
 			const DevMaterial& mat = sc.materials[__float_as_uint(hp.w)];
 			const bool canTransmit = surfaceOf(mat).transmission != 0.0f;
-			const Qrng q = pathQrng(sc, w, p, s.fd[p].y);
+			const Qrng q = pathQrngT<JOBS>(sc, w, s, p, s.fd[p].y);
 			const f3 r = sample3D(q, DIM_LIGHT);
 			const bool tri = (bits & kSfTriangle) != 0;
 			const S4 lambda = s4(s.lambda[p]);
@@ -700,7 +767,9 @@ kNee(DevScene sc, PathSoA s, WaveParams w, int bounce, int which)
 // light's spectrum in the record; a light sample that gets none is marked
 // occluded, so the next stage queues no shadow ray for it. Split from the
 // BxDF sample (stage 3b) so neither kernel holds both parts' registers.
-__global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdfLight(DevScene sc, PathSoA s, WaveParams w, int bounce)
+template<bool JOBS>
+__global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdfLight(const __grid_constant__ DevScene scK, PathSoA s,
+	WaveParams w, int bounce)
 {
 	const uint32_t n = min(s.counts[kSurfaceCounts + bounce], s.queueCap);
 	for (uint32_t i = gtid(); i < n; i += gstride())
@@ -708,6 +777,7 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdfLight(DevSc
 		const uint32_t p = s.surfQueue[i];
 		const uint32_t bits = __float_as_uint(lastWord(s.sfPi + p));
 		if (bits & (kSfSkipped | kSfOccluded)) continue;
+		const DevScene& sc = pathScene<JOBS>(scK, s, p);
 		const DevMaterial& mat = sc.materials[__float_as_uint(lastWord(s.sfP + p))];
 		const float4 rd = s.rayD[p], dd = s.shD[p];
 		const uint2 fd = s.fd[p];
@@ -725,7 +795,7 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdfLight(DevSc
 		dl.pdf = dd.w;
 		dl.occluded = false;
 		const Frame frame{ f3_of(s.sfT[p]), f3_of(s.sfB[p]), f3_of(s.nrm[p]) };
-		evalBxdf<kBxdfLight>(sc, mat, dl, pathQrng(sc, w, p, fd.y), frame, surfaceOf(mat), st);
+		evalBxdf<kBxdfLight>(sc, mat, dl, pathQrngT<JOBS>(sc, w, s, p, fd.y), frame, surfaceOf(mat), st);
 		if (st.hasNee) s.shC[p] = f4(st.nee);
 		else reinterpret_cast<float*>(s.sfPi + p)[3] = __uint_as_float(bits | kSfOccluded);
 	}
@@ -735,7 +805,9 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdfLight(DevSc
 // pathtrace.cu:773-905 / :521-547), Russian roulette, the next ray and the
 // depth limits (:1736-1785). Continuing paths go to the next extend queue,
 // light samples that passed stage 3a to the shadow queue.
-__global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(DevScene sc, PathSoA s, WaveParams w, int bounce)
+template<bool JOBS>
+__global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(const __grid_constant__ DevScene scK, PathSoA s,
+	WaveParams w, int bounce)
 {
 	const uint32_t n = min(s.counts[kSurfaceCounts + bounce], s.queueCap);
 	uint32_t* nextQueue = s.queue[(bounce + 1) & 1];
@@ -744,6 +816,7 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(DevScene s
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
 		const uint32_t p = s.surfQueue[i];
+		const DevScene& sc = pathScene<JOBS>(scK, s, p);
 		// Only the words the BxDF sample needs are read before it; the hit
 		// points, the geometric normal and the ray origin are read after it,
 		// so they are not live (and spilled) across the call.
@@ -752,7 +825,7 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(DevScene s
 		const float4 rd = s.rayD[p];
 		const uint2 fd = s.fd[p];
 		uint32_t flags = fd.x, depth = fd.y;
-		const Qrng q = pathQrng(sc, w, p, depth);
+		const Qrng q = pathQrngT<JOBS>(sc, w, s, p, depth);
 		const DevMaterial& mat = sc.materials[__float_as_uint(lastWord(s.sfP + p))];
 
 		// The BxDF reads the wavelengths and changes none of them: only
@@ -888,22 +961,53 @@ __global__ void kUnpackLightTree(const PackedNode* in, TreeNodeU* out, uint32_t 
 }
 
 // Sample resolve and FP64 accumulation (pathtrace.cu:1789-1812, color::toRGB).
-__global__ void __launch_bounds__(kThreads) kResolve(DevScene sc, PathSoA s, WaveParams w, double4* accum)
+template<bool JOBS>
+__global__ void __launch_bounds__(kThreads) kResolve(const __grid_constant__ DevScene scK, PathSoA s, WaveParams w,
+	double4* accumK)
 {
-	const uint32_t planes = w.paths / w.pixels;
-	const float* X = sc.spectra.sensor;
-	const float* Y = X + kSpectrumBins;
-	const float* Z = Y + kSpectrumBins;
-	for (uint32_t slot = gtid(); slot < w.pixels; slot += gstride())
+	const uint32_t slots = JOBS ? w.pixelSlots : w.pixels;
+	for (uint32_t slot = gtid(); slot < slots; slot += gstride())
 	{
-		const uint2 px = slotPixel(slot, sc.launch.width, sc.launch.height);
-		const uint32_t pix = px.y * sc.launch.width + px.x;
-		double4 acc = waveFresh(w) ? make_double4(0.0, 0.0, 0.0, 0.0) : accum[pix];
+		// the pixel, its planes' path slots (first + k stride) and its job
+		const DevScene* scp = &scK;
+		double4* accum = accumK;
+		uint32_t first, stride, planes, pix;
+		bool fresh, keepFailed;
+		if (JOBS)
+		{
+			const WaveChunk c = w.chunks[chunkOfPixel(w, slot)];
+			const uint32_t local = slot - c.pixel;
+			const uint2 px = slotPixel(local, c.width, c.height);
+			pix = px.y * c.width + px.x;
+			first = c.slot + local;
+			stride = c.pixels;
+			planes = c.planes;
+			fresh = c.fresh != 0;
+			const DevJob& job = s.jobs[c.job];
+			scp = &job.scene;
+			accum = job.accum;
+			keepFailed = job.keepFailed != 0;
+		}
+		else
+		{
+			const uint2 px = slotPixel(slot, scK.launch.width, scK.launch.height);
+			pix = px.y * scK.launch.width + px.x;
+			first = slot;
+			stride = w.pixels;
+			planes = w.paths / w.pixels;
+			fresh = waveFresh(w);
+			keepFailed = w.keepFailed != 0;
+		}
+		const DevScene& sc = *scp;
+		const float* X = sc.spectra.sensor;
+		const float* Y = X + kSpectrumBins;
+		const float* Z = Y + kSpectrumBins;
+		double4 acc = fresh ? make_double4(0.0, 0.0, 0.0, 0.0) : accum[pix];
 		for (uint32_t k = 0; k < planes; ++k)
 		{
-			const uint32_t p = k * w.pixels + slot;
+			const uint32_t p = first + k * stride;
 			const uint32_t flags = s.fd[p].x;
-			if (!(flags & PF_PATH_TERMINATED) || w.keepFailed)
+			if (!(flags & PF_PATH_TERMINATED) || keepFailed)
 			{
 				S4 L = s4(s.L[p]);
 				const S4 pdf = s4(s.lpdf[p]);
@@ -1070,54 +1174,80 @@ LaunchShape queryLaunchShape()
 		return (b < 1 ? 1 : b) * ls.smCount;
 	};
 	ls.threads = kThreads;
-	ls.blocksGenerate = occ(reinterpret_cast<const void*>(kGenerate));
-	ls.blocksSurface = occ(reinterpret_cast<const void*>(kSurface));
-	ls.blocksNee = occ(reinterpret_cast<const void*>(kNee<false>));
-	ls.blocksEmission = occ(reinterpret_cast<const void*>(kEmission));
-	ls.blocksNeePick = occ(reinterpret_cast<const void*>(kNeePick));
-	cudaFuncSetAttribute(reinterpret_cast<const void*>(kNee<true>), cudaFuncAttributeMaxDynamicSharedMemorySize,
+	ls.blocksGenerate = occ(reinterpret_cast<const void*>(kGenerate<false>));
+	ls.blocksSurface = occ(reinterpret_cast<const void*>(kSurface<false>));
+	ls.blocksNee = occ(reinterpret_cast<const void*>(kNee<false, false>));
+	ls.blocksEmission = occ(reinterpret_cast<const void*>(kEmission<false>));
+	ls.blocksNeePick = occ(reinterpret_cast<const void*>(kNeePick<false>));
+	cudaFuncSetAttribute(reinterpret_cast<const void*>(kNee<true, false>), cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(kNeeSharedMaxBytes));
-	ls.blocksBsdf = occ(reinterpret_cast<const void*>(kBsdf));
-	ls.blocksBsdfLight = occ(reinterpret_cast<const void*>(kBsdfLight));
-	ls.blocksResolve = occ(reinterpret_cast<const void*>(kResolve));
+	ls.blocksBsdf = occ(reinterpret_cast<const void*>(kBsdf<false>));
+	ls.blocksBsdfLight = occ(reinterpret_cast<const void*>(kBsdfLight<false>));
+	ls.blocksResolve = occ(reinterpret_cast<const void*>(kResolve<false>));
 	queryTraceShape(ls);
 	return ls;
 }
 
+// The launchers run the shared-wavefront variants when the path arrays
+// carry a job table (rb_render_jobs).
 void launchGenerate(const DevScene& sc, const PathSoA& s, const WaveParams& w, const LaunchShape& ls, cudaStream_t st)
 {
-	kGenerate<<<capBlocks(ls.blocksGenerate, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w);
+	const int g = capBlocks(ls.blocksGenerate, ls.items, kThreads);
+	if (s.jobs) kGenerate<true><<<g, kThreads, 0, st>>>(sc, s, w);
+	else kGenerate<false><<<g, kThreads, 0, st>>>(sc, s, w);
 }
 void launchSurface(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st,
 	unsigned long long* counters)
 {
-	kSurface<<<capBlocks(ls.blocksSurface, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce, counters);
+	const int g = capBlocks(ls.blocksSurface, ls.items, kThreads);
+	if (s.jobs) kSurface<true><<<g, kThreads, 0, st>>>(sc, s, w, bounce, counters);
+	else kSurface<false><<<g, kThreads, 0, st>>>(sc, s, w, bounce, counters);
 }
 void launchEmission(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st)
 {
-	kEmission<<<capBlocks(ls.blocksEmission, ls.items, kThreads), kThreads, 0, st>>>(sc, s, bounce);
+	const int g = capBlocks(ls.blocksEmission, ls.items, kThreads);
+	if (s.jobs) kEmission<true><<<g, kThreads, 0, st>>>(sc, s, bounce);
+	else kEmission<false><<<g, kThreads, 0, st>>>(sc, s, bounce);
 }
 void launchNee(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
 {
-	kNeePick<<<capBlocks(ls.blocksNeePick, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce);
+	const int g = capBlocks(ls.blocksNee, ls.items, kThreads);
+	if (s.jobs)
+	{
+		kNeePick<true><<<capBlocks(ls.blocksNeePick, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce);
+		kNee<false, true><<<g, kThreads, 0, st>>>(sc, s, w, bounce, 0);
+		kNee<false, true><<<g, kThreads, 0, st>>>(sc, s, w, bounce, 1);
+		return;
+	}
+	kNeePick<false><<<capBlocks(ls.blocksNeePick, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce);
 	const size_t treeBytes = sizeof(TreeNodeU) * sc.lights.nodeCount;
 	if (sc.lights.unpacked && treeBytes <= kNeeSharedMaxBytes)
 	{
 		int b = 0;
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, reinterpret_cast<const void*>(kNee<true>), kNeeSharedThreads,
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, reinterpret_cast<const void*>(kNee<true, false>), kNeeSharedThreads,
 			treeBytes);
-		kNee<true><<<capBlocks((b < 1 ? 1 : b) * ls.smCount, ls.items, kNeeSharedThreads), kNeeSharedThreads, treeBytes, st>>>(sc, s, w, bounce, 0);
+		kNee<true, false><<<capBlocks((b < 1 ? 1 : b) * ls.smCount, ls.items, kNeeSharedThreads), kNeeSharedThreads, treeBytes,
+			st>>>(sc, s, w, bounce, 0);
 	}
 	else
 	{
-		kNee<false><<<capBlocks(ls.blocksNee, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce, 0);
+		kNee<false, false><<<g, kThreads, 0, st>>>(sc, s, w, bounce, 0);
 	}
-	kNee<false><<<capBlocks(ls.blocksNee, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce, 1);
+	kNee<false, false><<<g, kThreads, 0, st>>>(sc, s, w, bounce, 1);
 }
 void launchBsdf(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
 {
-	kBsdfLight<<<capBlocks(ls.blocksBsdfLight, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce);
-	kBsdf<<<capBlocks(ls.blocksBsdf, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce);
+	const int gl = capBlocks(ls.blocksBsdfLight, ls.items, kThreads), gs = capBlocks(ls.blocksBsdf, ls.items, kThreads);
+	if (s.jobs)
+	{
+		kBsdfLight<true><<<gl, kThreads, 0, st>>>(sc, s, w, bounce);
+		kBsdf<true><<<gs, kThreads, 0, st>>>(sc, s, w, bounce);
+	}
+	else
+	{
+		kBsdfLight<false><<<gl, kThreads, 0, st>>>(sc, s, w, bounce);
+		kBsdf<false><<<gs, kThreads, 0, st>>>(sc, s, w, bounce);
+	}
 }
 void launchSetWaveDyn(uint32_t* dyn, uint32_t offset, uint32_t fresh, cudaStream_t st)
 {
@@ -1135,7 +1265,10 @@ void launchUnpackLightTree(const PackedNode* in, TreeNodeU* out, uint32_t n, cud
 }
 void launchResolve(const DevScene& sc, const PathSoA& s, const WaveParams& w, double4* accum, const LaunchShape& ls, cudaStream_t st)
 {
-	kResolve<<<capBlocks(ls.blocksResolve, w.pixels, kThreads), kThreads, 0, st>>>(sc, s, w, accum);
+	if (s.jobs)
+		kResolve<true><<<capBlocks(ls.blocksResolve, w.pixelSlots, kThreads), kThreads, 0, st>>>(sc, s, w, accum);
+	else
+		kResolve<false><<<capBlocks(ls.blocksResolve, w.pixels, kThreads), kThreads, 0, st>>>(sc, s, w, accum);
 }
 
 void launchSobol(uint32_t n, uint32_t dims, const uint32_t* sample, const uint32_t* hash, const uint32_t* bounce,

@@ -73,26 +73,31 @@ RB_D void persistentTraversal(uint32_t n, uint32_t* workCounter, Begin&& begin, 
 	}
 }
 
-// counters (COUNT only): [0] rays, [1] nodes, [2] triangles.
-template<bool COUNT>
-__global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kExtend(DevScene sc, PathSoA s, int bounce, unsigned long long* counters)
+// counters (COUNT only): [0] rays, [1] nodes, [2] triangles. JOBS: a shared
+// wavefront, each ray traced in its job's geometry.
+template<bool COUNT, bool JOBS>
+__global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kExtend(const __grid_constant__ DevScene sc, PathSoA s,
+	int bounce, unsigned long long* counters)
 {
 	const uint32_t n = min(s.counts[bounce], s.queueCap);
 	const uint32_t* q = s.queue[bounce & 1];
 	uint32_t rays = 0, nodes = 0, tris = 0;
 	uint32_t p = 0;
+	const DevScene* js = &sc;
 	ClosestTraversal tr;
 	uint2 stack[kTraversalStack];
 	auto step = [&]() {
-		if (!tr.template run<COUNT>(sc.geo, kStepBudget, sc.status, nodes, tris, stack)) return false;
+		const DevGeometry& g = JOBS ? js->geo : sc.geo;
+		if (!tr.template run<COUNT>(g, kStepBudget, JOBS ? js->status : sc.status, nodes, tris, stack)) return false;
 		s.hit[p] = make_float4(__int_as_float(tr.best.tri), tr.best.t, tr.best.b1, tr.best.b2);
 		return true;
 	};
 	persistentTraversal<ClosestTraversal>(n, s.counts + kExtendFetch + bounce,
 		[&](uint32_t idx) {
 			p = q[idx];
+			if (JOBS) js = &s.jobs[s.job[p]].scene;
 			const float4 o = s.rayO[p], d = s.rayD[p];
-			tr.init(sc.geo, f3_of(o), f3_of(d), 0.0f, FLT_MAX);
+			tr.init(JOBS ? js->geo : sc.geo, f3_of(o), f3_of(d), 0.0f, FLT_MAX);
 			++rays;
 		}, step);
 	if (COUNT)
@@ -103,16 +108,19 @@ __global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kExtend(DevScen
 	}
 }
 
-template<bool COUNT>
-__global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kShadow(DevScene sc, PathSoA s, int bounce, unsigned long long* counters)
+template<bool COUNT, bool JOBS>
+__global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kShadow(const __grid_constant__ DevScene sc, PathSoA s,
+	int bounce, unsigned long long* counters)
 {
 	const uint32_t n = min(s.counts[kShadowCounts + bounce], s.queueCap);
 	uint32_t rays = 0, nodes = 0, tris = 0;
 	uint32_t p = 0;
+	const DevScene* js = &sc;
 	AnyTraversal tr;
 	uint32_t stack[kTraversalStack];
 	auto step = [&]() {
-		if (!tr.template run<COUNT>(sc.geo, kStepBudget, sc.status, nodes, tris, stack)) return false;
+		const DevGeometry& g = JOBS ? js->geo : sc.geo;
+		if (!tr.template run<COUNT>(g, kStepBudget, JOBS ? js->status : sc.status, nodes, tris, stack)) return false;
 		if (!tr.hit)
 		{
 			S4 L = s4(s.L[p]);
@@ -124,8 +132,9 @@ __global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kShadow(DevScen
 	persistentTraversal<AnyTraversal>(n, s.counts + kShadowFetch + bounce,
 		[&](uint32_t idx) {
 			p = s.shadowQueue[idx];
+			if (JOBS) js = &s.jobs[s.job[p]].scene;
 			const float4 o = s.shO[p], d = s.shD[p];
-			tr.init(sc.geo, f3_of(o), f3_of(d), 0.0f, o.w);
+			tr.init(JOBS ? js->geo : sc.geo, f3_of(o), f3_of(d), 0.0f, o.w);
 			++rays;
 		}, step);
 	if (COUNT)
@@ -192,21 +201,33 @@ void queryTraceShape(LaunchShape& ls)
 		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, 0);
 		return (b < 1 ? 1 : b) * ls.smCount;
 	};
-	ls.blocksExtend = occ(reinterpret_cast<const void*>(kExtend<false>));
-	ls.blocksShadow = occ(reinterpret_cast<const void*>(kShadow<false>));
+	ls.blocksExtend = occ(reinterpret_cast<const void*>(kExtend<false, false>));
+	ls.blocksShadow = occ(reinterpret_cast<const void*>(kShadow<false, false>));
 }
 
 void launchExtend(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
 	unsigned long long* counters)
 {
-	if (counters) kExtend<true><<<capBlocks(ls.blocksExtend, ls.items, kThreads), kThreads, 0, st>>>(sc, s, bounce, counters);
-	else kExtend<false><<<capBlocks(ls.blocksExtend, ls.items, kThreads), kThreads, 0, st>>>(sc, s, bounce, nullptr);
+	const int g = capBlocks(ls.blocksExtend, ls.items, kThreads);
+	if (s.jobs)
+	{
+		if (counters) kExtend<true, true><<<g, kThreads, 0, st>>>(sc, s, bounce, counters);
+		else kExtend<false, true><<<g, kThreads, 0, st>>>(sc, s, bounce, nullptr);
+	}
+	else if (counters) kExtend<true, false><<<g, kThreads, 0, st>>>(sc, s, bounce, counters);
+	else kExtend<false, false><<<g, kThreads, 0, st>>>(sc, s, bounce, nullptr);
 }
 void launchShadow(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st,
 	unsigned long long* counters)
 {
-	if (counters) kShadow<true><<<capBlocks(ls.blocksShadow, ls.items, kThreads), kThreads, 0, st>>>(sc, s, bounce, counters);
-	else kShadow<false><<<capBlocks(ls.blocksShadow, ls.items, kThreads), kThreads, 0, st>>>(sc, s, bounce, nullptr);
+	const int g = capBlocks(ls.blocksShadow, ls.items, kThreads);
+	if (s.jobs)
+	{
+		if (counters) kShadow<true, true><<<g, kThreads, 0, st>>>(sc, s, bounce, counters);
+		else kShadow<false, true><<<g, kThreads, 0, st>>>(sc, s, bounce, nullptr);
+	}
+	else if (counters) kShadow<true, false><<<g, kThreads, 0, st>>>(sc, s, bounce, counters);
+	else kShadow<false, false><<<g, kThreads, 0, st>>>(sc, s, bounce, nullptr);
 }
 void launchTrace(const DevScene& sc, uint32_t n, const float* rays, uint32_t* payload, float* t, int32_t* tri, cudaStream_t st)
 {

@@ -46,6 +46,11 @@ struct PathSoA
 	uint32_t* shadowQueue;
 	uint32_t* counts;  // kCountSlots words: see kShadowCounts, kSurfaceCounts
 	uint32_t capacity;
+	// jobs of a shared wavefront (rb_render_jobs; null for a single render):
+	// the job table, and per path its job and key (x | y << 16, sample index)
+	const struct DevJob* jobs;
+	uint32_t* job;
+	uint2* key;
 	// entries a queue accepts per bounce (capacity, or the injected limit of
 	// rb_config.inject_queue_limit); an append beyond it is dropped with
 	// RB_DEV_QUEUE_OVERFLOW, and readers take at most this many
@@ -101,6 +106,24 @@ constexpr uint32_t kCacheQueryCount = 8 * (kMaxBounces + 1);
 constexpr uint32_t kTrainRecordCount = kCacheQueryCount + 1;
 constexpr uint32_t kCountSlots = kCacheQueryCount + 2;
 
+// One render job of a shared wavefront (rb_render_jobs): its scene, its
+// accumulation buffer and whether its failed samples keep their radiance.
+struct DevJob
+{
+	DevScene scene;
+	double4* accum;
+	uint32_t keepFailed;
+	uint32_t pad[3];
+};
+// A run of sample planes of one job inside a wave: path slots [slot, slot +
+// planes x pixels) (plane-major, slotPixel order within a plane), pixel
+// slots [pixel, pixel + pixels) of the wave's resolve, sample indices
+// [sample, sample + planes); fresh: the job's accumulation restarts here.
+struct WaveChunk
+{
+	uint32_t job, slot, pixel, planes, sample, fresh, pixels, width, height, pad[3];
+};
+
 struct WaveParams
 {
 	uint32_t paths;        // slots in this wave
@@ -119,6 +142,11 @@ struct WaveParams
 	float spreadC;         // terminate once (summed spread)^2 > spreadC * a0
 	float minRoughness;    // ... at a surface that is not metallic or transmissive, or at least this rough
 	float posMin[3], posScale[3];  // hit position -> [0,1]^3
+	// shared wavefront (PathSoA::jobs set): the wave's chunks, sorted by slot
+	// and by pixel slot, and the number of pixel slots the resolve covers
+	const WaveChunk* chunks;
+	uint32_t nChunks;
+	uint32_t pixelSlots;
 };
 
 struct LaunchShape

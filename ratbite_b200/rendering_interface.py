@@ -268,3 +268,24 @@ class RenderingInterface:
         st = abi.rb_cache_stats()
         check(self.lib.rb_get_cache_stats(self.ctx, C.byref(st)), self.ctx, "rb_get_cache_stats")
         return st
+
+
+def render_jobs(interfaces, offsets, counts, max_paths: int = 0, grid_percent: int = 0, done_events=None,
+                stream=None):
+    """Renders several RenderingInterface jobs in one shared wavefront
+    (rb_render_jobs): job j renders samples [offsets[j], offsets[j] +
+    counts[j]). done_events: optional torch.cuda.Event per job, recorded when
+    the job's last wave completes."""
+    lib = load()
+    n = len(interfaces)
+    ctxs = (C.c_void_p * n)(*[ri.ctx.value for ri in interfaces])
+    offs = (C.c_uint32 * n)(*offsets)
+    cnts = (C.c_uint32 * n)(*counts)
+    opt = abi.rb_jobs_options()
+    opt.max_paths_in_flight = max_paths
+    opt.grid_percent = grid_percent
+    ev = None
+    if done_events is not None:
+        ev = (C.c_void_p * n)(*[e.cuda_event if e is not None else None for e in done_events])
+        opt.done_events = C.cast(ev, C.c_void_p)
+    check(lib.rb_render_jobs(ctxs, n, offs, cnts, C.byref(opt), stream), interfaces[0].ctx, "rb_render_jobs")

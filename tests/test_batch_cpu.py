@@ -27,7 +27,7 @@ def test_job_draw_is_deterministic_and_in_range():
 
 
 def test_schedule_capacity():
-    s = batch.Schedule(streams=4, chunk=64, max_paths=1 << 20)
+    s = batch.Schedule(max_paths=1 << 20, grid_percent=100, streams=4, chunk=64)
     small = batch.Job(0, 0, 128, 16, 10_000, "plain")
     big = batch.Job(1, 0, 1024, 512, 10_000, "plain")
     assert s.capacity(small) == 128 * 128 * 16
