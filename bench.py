@@ -633,8 +633,9 @@ def time_to_rmse(device: int = 0, width: int = 1920, height: int = 1080, depth: 
     spans. The comparison runs `repeats` times (different sample ranges, a
     fresh untrained cache with a different seed each time); the line reports
     every ratio and their median. Both forms get one untimed warm-up chunk
-    per run (first-launch costs and buffer allocation); the cached form stops
-    at the target or at time_factor x the plain tracer's time."""
+    per run (first-launch costs and buffer allocation; the cache is then
+    reset to its initial parameters); the cached form stops at the target or
+    at time_factor x the plain tracer's time."""
     import torch
     from ratbite_b200 import lighttree, scenes
     from ratbite_b200.nrc import RadianceCache
@@ -697,11 +698,18 @@ def time_to_rmse(device: int = 0, width: int = 1920, height: int = 1080, depth: 
         target, t_plain = plain_curve[-1][2], plain_curve[-1][1]
         plain_bias = biases(mean_image())
 
-        scratch = RadianceCache(device=device, seed=1000 + rep)
-        ri.attach_radiance_cache(scratch, **kw)
-        ri.clear_accumulation(stream=sp)
-        ri.render(base + (1 << 19) + chunk, chunk, stream=sp)            # warm-up: sizes the cache's wave buffers
+        # warm-up with the cache that is then timed: it sizes the context's
+        # cache buffers and the network's training scratch; the network then
+        # goes back to its initial parameters (optimiser state reset) and is
+        # attached again (corrections reset), so the timed run starts from an
+        # untrained cache with nothing left to allocate
         cache = RadianceCache(device=device, seed=2 + rep)
+        init = cache.parameters()
+        ri.attach_radiance_cache(cache, **kw)
+        ri.clear_accumulation(stream=sp)
+        ri.render(base + (1 << 19) + chunk, chunk, stream=sp)
+        ri.synchronize()
+        cache.set_parameters(*init)
         ri.attach_radiance_cache(cache, **kw)
         ri.cache_stats()
         ri.clear_accumulation(stream=sp)
@@ -718,7 +726,6 @@ def time_to_rmse(device: int = 0, width: int = 1920, height: int = 1080, depth: 
         cached_bias = biases(mean_image())
         ri.attach_radiance_cache(None)
         cache.close()
-        scratch.close()
         best = min(cached_curve, key=lambda c: c[2])
         runs.append({
             "plain": {"spp": plain_spp, "s": t_plain, "rel_rmse": target, "paths_per_s": n * plain_spp / t_plain,

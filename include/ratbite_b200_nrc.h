@@ -43,7 +43,7 @@ int rb_nrc_destroy(rb_nrc* nrc);
 size_t rb_nrc_grid_size(void);
 size_t rb_nrc_weight_count(void);
 /* Host copies of the FP32 master parameters (synchronizes). Setting them
- * also resets the optimiser's moments. */
+ * also resets the optimiser (moments and step count). */
 int rb_nrc_set_parameters(rb_nrc* nrc, const float* grid_host, const float* weights_host);
 int rb_nrc_get_parameters(rb_nrc* nrc, float* grid_host, float* weights_host);
 /* outputs[n][4] = network(inputs[n][kNrcInputs]), stream-ordered; outputs

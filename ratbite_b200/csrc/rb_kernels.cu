@@ -335,7 +335,12 @@ __global__ void __launch_bounds__(kThreads) kGenerate(const __grid_constant__ De
 			s.trainRec[p] = w.trainOneIn && mix32(p ^ w.trainSeed) % w.trainOneIn == 0 ? kNoRecord : kNotTraining;
 		}
 	}
-	if (gtid() == 0) s.counts[0] = w.paths;
+	if (gtid() == 0)
+	{
+		// the first extension queue holds every path of the wave
+		s.counts[0] = w.paths;
+		if (w.paths > s.queueCap) atomicOr(scK.status, RB_DEV_QUEUE_OVERFLOW);
+	}
 }
 
 // Minimum resident blocks per SM requested for the shading kernels, which

@@ -374,6 +374,41 @@ RB_D void encodeRow(uint32_t r, uint32_t n, const float* __restrict__ in, const 
 #pragma unroll
 	for (int k = 0; k < 32; k += 2) row[16 + k / 2] = pack2(restColumn(v, k), restColumn(v, k + 1));
 }
+// The tile's encoded rows, spread over the warp: warp w encodes rows
+// 32 w .. 32 w + 31; lane l takes the (row, level) pairs l, l + 32, ...
+// (16 per lane, their 8 corner gathers independent of each other), then the
+// 32 remaining columns of row 32 w + l. Each feature pair is one 32-bit
+// word of the swizzled tile.
+#ifndef RB_INFER_ROW_ENCODE
+#define RB_INFER_ROW_ENCODE 0
+#endif
+RB_D void encodeTile(uint32_t r0, uint32_t n, const float* __restrict__ in, const __half2* __restrict__ grid,
+	const Resolutions& R, unsigned char* tile)
+{
+	const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+#pragma unroll 4
+	for (uint32_t k = lane; k < 32u * kLevels; k += 32u)
+	{
+		const uint32_t rl = 32u * warp + (k >> 4), l = k & 15u, r = r0 + rl;
+		float f0 = 0.0f, f1 = 0.0f;
+		if (r < n)
+		{
+			const float* v = in + static_cast<size_t>(kNrcInputs) * r;
+			levelFeatures(R, grid, static_cast<int>(l), clamp01(v[0]), clamp01(v[1]), clamp01(v[2]), f0, f1);
+		}
+		*reinterpret_cast<uint32_t*>(tile + umma::swzOffset(rl, 2u * l)) = pack2(f0, f1);
+	}
+	const uint32_t rl = 32u * warp + lane, r = r0 + rl;
+	const float* v = in + static_cast<size_t>(kNrcInputs) * r;
+	uint32_t rest[16];
+#pragma unroll
+	for (int k = 0; k < 32; k += 2)
+		rest[k / 2] = r < n ? pack2(restColumn(v, k), restColumn(v, k + 1)) : 0u;
+#pragma unroll
+	for (uint32_t c = 0; c < 4; ++c)
+		*reinterpret_cast<uint4*>(tile + rl * 128u + ((((4u + c) ^ rl) & 7u) << 4)) =
+			make_uint4(rest[4 * c], rest[4 * c + 1], rest[4 * c + 2], rest[4 * c + 3]);
+}
 } // namespace t5
 
 // Inference with the encoding fused in (kMlpInfer's contract, on tcgen05).
@@ -389,11 +424,15 @@ __global__ void __launch_bounds__(128) kMlpInferT(uint32_t cap, const uint32_t* 
 	for (uint32_t r0 = blockIdx.x * t5::kRows; r0 < n && ok; r0 += gridDim.x * t5::kRows)
 	{
 		const uint32_t r = r0 + threadIdx.x;
+#if RB_INFER_ROW_ENCODE
 		{
 			uint32_t row[32];
 			t5::encodeRow(r, n, in, grid, R, row);
 			umma::storeRow(c.act, threadIdx.x, row);
 		}
+#else
+		t5::encodeTile(r0, n, in, grid, R, c.act);
+#endif
 		umma::fenceProxyAsync();
 		__syncthreads();
 		for (int l = 0; l < 4 && ok; ++l)
@@ -973,6 +1012,7 @@ int rb_nrc_set_parameters(rb_nrc* h, const float* grid, const float* weights)
 		0.0f, 0.0f, 1.0f, 1.0f, 1.0f, nullptr, h->grid);
 	kAdam<<<64, 256>>>(kWTotal, h->wF32, h->wGrad, h->wM, h->wV, 0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f, h->w, nullptr);
 	kTransposeWeights<<<64, 256>>>(h->wF32, h->wt);
+	h->step = 0;              // the optimiser starts over with the new parameters
 	e = cudaDeviceSynchronize();
 	return e == cudaSuccess ? RB_OK : nrcFail(e);
 }

@@ -93,17 +93,28 @@ __device__ __forceinline__ void barrierInit(uint64_t* bar, uint32_t count)
 }
 // Waits for the phase with the given parity to complete, at most `limit`
 // polls; false when it gave up.
+#ifndef RB_UMMA_SPIN_WAIT
+#define RB_UMMA_SPIN_WAIT 0
+#endif
 __device__ __forceinline__ bool barrierWait(uint64_t* bar, uint32_t parity, uint32_t limit)
 {
 	const uint32_t a = smemAddr(bar);
 	for (uint32_t i = 0; i < limit; ++i)
 	{
 		uint32_t done = 0;
+#if RB_UMMA_SPIN_WAIT
+		asm volatile(
+			"{\n\t.reg .pred p;\n\t"
+			"mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+			"selp.u32 %0, 1, 0, p;\n\t}\n"
+			: "=r"(done) : "r"(a), "r"(parity) : "memory");
+#else
 		asm volatile(
 			"{\n\t.reg .pred p;\n\t"
 			"mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
 			"selp.u32 %0, 1, 0, p;\n\t}\n"
 			: "=r"(done) : "r"(a), "r"(parity) : "memory");
+#endif
 		if (done) return true;
 	}
 	return false;
