@@ -191,8 +191,8 @@ def workload_config(scene, wl: dict, world: int, tables: str) -> dict:
             "envmap": list(scene.envmap.shape[1::-1]) if has_env else None,
             "paths_per_step": wl["width"] * wl["height"] * wl["spp"] * world,
             "parallelism": f"sample-range x{world}", "tables": tables,
-            "l2": "inputs larger than L2 (wavefront path state 344 B per path in flight, "
-                  "~5.8 GB at the default 16M paths per wave)"}
+            "l2": "inputs larger than L2 (wavefront path state 376 B per path in flight, "
+                  "~6.3 GB at the default 16M paths per wave)"}
 
 
 # ------------------------------------------------------------- CPU baseline
@@ -416,11 +416,15 @@ def run_ours(args, rank: int, world: int, wl: dict):
         # profiles/traffic.json) times the units one launch processes here
         units_step = {"extend": ext_rays, "shadow": sh_rays, "surface": ext_rays, "nee": recs, "bsdf": recs}
         traffic = None
+        limiter = None
         tp = ROOT / "profiles" / "traffic.json"
         if tp.exists():
             t = json.loads(tp.read_text()).get(WORKLOADS[args.workload]["name"], {}).get(kernel_names[dom])
             if t:
                 traffic = t["dram_bytes_per_unit"] * units_step[dom] / max(1.0, launches / args.steps)
+                # what bounds the kernel, from one ncu capture of it: the HBM
+                # fraction above is an upper bound on how memory-bound it is
+                limiter = t.get("limiter")
         if args.cpu_seconds > 0:
             cpu_v, cores, sample = cpu_baseline(scene, cie, basis, luts, wl, args.cpu_seconds)
         else:
@@ -447,7 +451,8 @@ def run_ours(args, rank: int, world: int, wl: dict):
             "gpu_launches": int(launches_total),
             "roofline": {"kernel": kernel_names[dom], "bound": "hbm", "achieved": achieved, "peak": hbm,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": traffic, "bytes_per_launch": bytes_step / max(1, launches / args.steps)},
+                         "traffic": traffic, "bytes_per_launch": bytes_step / max(1, launches / args.steps),
+                         "limiter": limiter},
             "stages_ms_per_step": {k: v / args.steps for k, v in shares.items()},
             "stage_share": {k: (v / total_ms if total_ms else None) for k, v in shares.items()},
             "kernel_gbs": {k: (step_bytes[k] * args.steps / (shares[k] / 1e3) / 1e9 if shares[k] else None)

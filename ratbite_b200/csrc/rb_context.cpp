@@ -172,6 +172,20 @@ int upload(rb_ctx* ctx, std::vector<void*>& owner, const void* src, size_t bytes
 }
 cudaStream_t pick(rb_ctx* ctx, void* s) { return s ? static_cast<cudaStream_t>(s) : ctx->stream; }
 
+// Buffers a render call allocates on demand (the wave, the cache arrays, a
+// shared wavefront's job tables) are zero-filled on the context's own
+// stream (upload). A call that renders on a caller's stream waits for those
+// fills before it enqueues anything that writes the buffers, or a fill that
+// runs late would overwrite what the render wrote (a zeroed job table has
+// null scene and accumulation pointers). `allocs0`: the context's allocation
+// count at the start of the call.
+int settleFills(rb_ctx* ctx, uint64_t allocs0, cudaStream_t st)
+{
+	if (ctx->allocCount == allocs0 || st == ctx->stream) return RB_OK;
+	const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+	return e == cudaSuccess ? RB_OK : cudaFail(ctx, e, "zero-fill of new buffers");
+}
+
 // Setters are transactional: new tables are uploaded into `fresh` first, and
 // only when every upload succeeded does the context switch to them, after
 // all queued work (renders may run on caller streams) has finished with the
@@ -318,7 +332,8 @@ int ensureWave(rb_ctx* ctx, uint32_t paths)
 	alloc(s.T, sizeof(float4)); alloc(s.fd, sizeof(uint2)); alloc(s.hit, sizeof(float4));
 	alloc(s.shO, sizeof(float4)); alloc(s.shD, sizeof(float4)); alloc(s.shC, sizeof(float4));
 	alloc(s.sfP, sizeof(float4)); alloc(s.sfPi, sizeof(float4)); alloc(s.sfGn, sizeof(float4));
-	alloc(s.sfT, sizeof(float4)); alloc(s.sfB, sizeof(float4));
+	alloc(s.sfT, sizeof(float4)); alloc(s.sfB, sizeof(float4)); alloc(s.sfN, sizeof(float4));
+	alloc(s.sfL, sizeof(float4));
 	alloc(s.queue[0], sizeof(uint32_t)); alloc(s.queue[1], sizeof(uint32_t)); alloc(s.shadowQueue, sizeof(uint32_t));
 	alloc(s.surfQueue, sizeof(uint32_t));
 	alloc(s.neeQueue[0], sizeof(uint32_t)); alloc(s.neeQueue[1], sizeof(uint32_t));
@@ -1074,7 +1089,11 @@ int rb_set_launch(rb_ctx* ctx, const rb_launch* l)
 		ctx->accumPixels = 0;
 		const cudaError_t e = devMalloc(ctx, reinterpret_cast<void**>(&ctx->accum), sizeof(double4) * pixels);
 		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_set_launch: accumulation buffer");
-		cudaMemsetAsync(ctx->accum, 0, sizeof(double4) * pixels, ctx->stream);
+		// finished before the call returns: a render on a caller's stream
+		// that adds to the accumulation must not race the fill
+		const cudaError_t f = cudaMemsetAsync(ctx->accum, 0, sizeof(double4) * pixels, ctx->stream);
+		if (f != cudaSuccess || cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+			return cudaFail(ctx, f != cudaSuccess ? f : cudaGetLastError(), "rb_set_launch: accumulation fill");
 		ctx->accumPixels = pixels;
 	}
 	ctx->haveLaunch = true;
@@ -1111,11 +1130,12 @@ int renderWaves(rb_ctx* ctx, uint32_t offset, uint32_t count, cudaStream_t st, c
 	const rb::DevScene& sc = ctx->scene;
 	const uint32_t pixels = sc.launch.width * sc.launch.height;
 	// Wave size: whole sample planes, up to the capacity (default 16M paths,
-	// about 5.8 GB of path state).
+	// about 6.3 GB of path state).
 	const bool cached = ctx->cache != nullptr;
 	const rb_cache_params& CP = ctx->cacheParams;
 	const uint32_t planesPerWave = planesPerWaveFor(ctx, count);
 	const uint32_t wavePaths = planesPerWave * pixels;
+	const uint64_t allocs0 = ctx->allocCount;
 	int rc = ensureWave(ctx, wavePaths);
 	if (rc != RB_OK) return rc;
 	const int bounces = static_cast<int>(std::min<uint32_t>(rb::kMaxBounces,
@@ -1129,6 +1149,8 @@ int renderWaves(rb_ctx* ctx, uint32_t offset, uint32_t count, cudaStream_t st, c
 		soa.spread = c.spread; soa.trainRec = c.trainRec; soa.cPath = c.cPath; soa.cIn = c.cIn;
 		soa.tPath = c.tPath; soa.tIn = c.tIn; soa.tL = c.tL; soa.tT = c.tT; soa.trainCapacity = c.trainCapacity;
 	}
+	rc = settleFills(ctx, allocs0, st);
+	if (rc != RB_OK) return rc;
 	// scene box -> [0,1]^3 (cache inputs): the cache's
 	// given box, or the geometry's bounds grown by 1 %
 	float posMin[3] = {}, posScale[3] = {};
@@ -1313,6 +1335,7 @@ int rb_render_jobs(rb_ctx* const* jobs, uint32_t n, const uint32_t* offsets, con
 	if (waves.empty()) return RB_OK;
 	uint32_t wavePaths = 0;
 	for (const Wave& w : waves) wavePaths = std::max(wavePaths, w.paths);
+	const uint64_t allocs0 = host->allocCount;
 	int rc = ensureWave(host, wavePaths);
 	if (rc != RB_OK) return rc;
 	// per-path job arrays, job and chunk tables (grown on demand)
@@ -1331,6 +1354,8 @@ int rb_render_jobs(rb_ctx* const* jobs, uint32_t n, const uint32_t* offsets, con
 		host->jobTableCap = n;
 		host->chunkCap = static_cast<uint32_t>(chunks.size());
 	}
+	rc = settleFills(host, allocs0, st);
+	if (rc != RB_OK) return rc;
 	std::vector<rb::DevJob> table(n);
 	for (uint32_t j = 0; j < n; ++j)
 	{
@@ -1402,7 +1427,9 @@ int rb_render_graph(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 	const cudaStream_t st = pick(ctx, stream);
 	// buffers first: the capture must not allocate
 	const uint32_t pixels = ctx->scene.launch.width * ctx->scene.launch.height;
+	const uint64_t allocs0 = ctx->allocCount;
 	rc = ensureWave(ctx, planesPerWaveFor(ctx, count) * pixels);
+	if (rc == RB_OK) rc = settleFills(ctx, allocs0, st);
 	if (rc != RB_OK) return rc;
 	rb_ctx::GraphKey key{};
 	key.scene = ctx->scene;

@@ -370,11 +370,15 @@ __global__ void __launch_bounds__(kThreads) kGenerate(const __grid_constant__ De
 constexpr int kNeeSharedThreads = 512;
 constexpr uint32_t kNeeSharedMaxBytes = RB_NEE_SHARED_MAX_BYTES;
 
-// Surface-record bits (PathSoA::sfPi.w).
+// Surface-record bits (PathSoA::sfPi.w); bits 8..15 hold the path's depth,
+// so the light-sample kernels need not read the path's flags for it.
 constexpr uint32_t kSfBackHit = 1u << 0;
 constexpr uint32_t kSfSkipped = 1u << 1;
 constexpr uint32_t kSfTriangle = 1u << 2;
 constexpr uint32_t kSfOccluded = 1u << 3;
+constexpr uint32_t kSfDepthShift = 8;
+static_assert(kMaxBounces <= 255, "depth fits bits 8..15");
+RB_D uint32_t sfDepth(uint32_t bits) { return (bits >> kSfDepthShift) & 0xFFu; }
 
 RB_D Qrng pathQrng(const DevScene& sc, const WaveParams& w, uint32_t p, uint32_t depth)
 {
@@ -572,15 +576,22 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(cons
 				}
 			}
 			const uint32_t bits = (it.backHit ? kSfBackHit : 0u) | (skipped ? kSfSkipped : 0u)
-				| ((flags & PF_TRIANGULAR_GEOMETRY) ? kSfTriangle : 0u);
-			s.sfP[p] = f4_of(it.hitPos, __uint_as_float(it.material));
-			s.sfPi[p] = f4_of(it.hitPosInterp, __uint_as_float(bits));
-			s.sfGn[p] = f4_of(it.gn, 0.0f);
-			s.sfT[p] = f4_of(frame.t, 0.0f);
-			s.sfB[p] = f4_of(frame.b, 0.0f);
+				| ((flags & PF_TRIANGULAR_GEOMETRY) ? kSfTriangle : 0u) | (depth << kSfDepthShift);
 			s.nrm[p] = f4_of(lastNormal, nv.w);
-			const uint32_t slot = appendSlot(surfCount, s.queueCap, sc.status);
-			if (slot != kNoSlot) s.surfQueue[slot] = p;
+			// the record lives at its queue position: a warp's records are
+			// adjacent, so the shading kernels read them in whole sectors
+			const uint32_t r = appendSlot(surfCount, s.queueCap, sc.status);
+			if (r != kNoSlot)
+			{
+				s.surfQueue[r] = p;
+				s.sfP[r] = f4_of(it.hitPos, __uint_as_float(it.material));
+				s.sfPi[r] = f4_of(it.hitPosInterp, __uint_as_float(bits));
+				s.sfGn[r] = f4_of(it.gn, 0.0f);
+				s.sfT[r] = f4_of(frame.t, 0.0f);
+				s.sfB[r] = f4_of(frame.b, 0.0f);
+				s.sfN[r] = f4_of(lastNormal, 0.0f);
+				s.sfL[r] = s.lambda[p];
+			}
 			++records;
 		}
 		else if (w.cached && s.trainRec[p] != kNotTraining)
@@ -638,8 +649,9 @@ __global__ void __launch_bounds__(kThreads) kNeePick(const __grid_constant__ Dev
 	const uint32_t n = min(s.counts[kSurfaceCounts + bounce], s.queueCap);
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
+		const uint32_t bits = __float_as_uint(lastWord(s.sfPi + i));
+		if (bits & kSfSkipped) continue;
 		const uint32_t p = s.surfQueue[i];
-		if (__float_as_uint(s.sfPi[p].w) & kSfSkipped) continue;
 		const DevScene& sc = pathScene<JOBS>(scK, s, p);
 		const bool envPresent = sc.env.enabled != 0;
 		const bool treePresent = sc.lights.nodes != nullptr;
@@ -647,19 +659,19 @@ __global__ void __launch_bounds__(kThreads) kNeePick(const __grid_constant__ Dev
 		bool sky = true;
 		if (envPresent || treePresent)
 		{
-			const Qrng q = pathQrngT<JOBS>(sc, w, s, p, s.fd[p].y);
+			const Qrng q = pathQrngT<JOBS>(sc, w, s, p, sfDepth(bits));
 			sky = sample3D(q, DIM_LIGHT).z < envImp;
 		}
 		// one counter per branch: appendIndex aggregates over the lanes active at the call
 		if (sky)
 		{
 			const uint32_t slot = appendSlot(s.counts + kNeeSkyCounts + bounce, s.queueCap, sc.status);
-			if (slot != kNoSlot) s.neeQueue[1][slot] = p;
+			if (slot != kNoSlot) s.neeQueue[1][slot] = i;
 		}
 		else
 		{
 			const uint32_t slot = appendSlot(s.counts + kNeeTreeCounts + bounce, s.queueCap, sc.status);
-			if (slot != kNoSlot) s.neeQueue[0][slot] = p;
+			if (slot != kNoSlot) s.neeQueue[0][slot] = i;
 		}
 	}
 }
@@ -692,15 +704,16 @@ kNee(const __grid_constant__ DevScene scK, PathSoA s, WaveParams w, int bounce, 
 	}
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
-		const uint32_t p = queue[i];
+		const uint32_t rec = queue[i];
+		const uint32_t p = s.surfQueue[rec];
 		const DevScene& sc = pathScene<JOBS>(scK, s, p);
 		const TreeNodeU* nodes = JOBS ? sc.lights.unpacked : sharedNodes;
 		const bool envPresent = sc.env.enabled != 0;
 		const bool treePresent = sc.lights.nodes != nullptr;
-		const float4 pi = s.sfPi[p];
+		const float4 pi = s.sfPi[rec];
 		uint32_t bits = __float_as_uint(pi.w);
-		const float4 hp = s.sfP[p];
-		const f3 hitPos = f3_of(hp), hitPosInterp = f3_of(pi), gn = f3_of(s.sfGn[p]), sn = f3_of(s.nrm[p]);
+		const float4 hp = s.sfP[rec];
+		const f3 hitPos = f3_of(hp), hitPosInterp = f3_of(pi), gn = f3_of(s.sfGn[rec]), sn = f3_of(s.sfN[rec]);
 		f3 dir = mk(0.0f), shadowO = mk(0.0f);
 		S4 spectrum = s4(0.0f);
 		float pdf = 0.0f, dToL = 0.0f;
@@ -713,10 +726,10 @@ kNee(const __grid_constant__ DevScene scK, PathSoA s, WaveParams w, int bounce, 
 		{
 			const DevMaterial& mat = sc.materials[__float_as_uint(hp.w)];
 			const bool canTransmit = surfaceOf(mat).transmission != 0.0f;
-			const Qrng q = pathQrngT<JOBS>(sc, w, s, p, s.fd[p].y);
+			const Qrng q = pathQrngT<JOBS>(sc, w, s, p, sfDepth(bits));
 			const f3 r = sample3D(q, DIM_LIGHT);
 			const bool tri = (bits & kSfTriangle) != 0;
-			const S4 lambda = s4(s.lambda[p]);
+			const S4 lambda = s4(s.sfL[rec]);
 			uint32_t type = 0, index = 0;
 			float treePdf = 0.0f, lightPdf = 0.0f;
 			lightTreeSample<SHARED>(sc, nodes, r.z, hitPos, sn, type, index, treePdf);
@@ -758,11 +771,10 @@ kNee(const __grid_constant__ DevScene scK, PathSoA s, WaveParams w, int bounce, 
 			}
 			pdf = lightPdf * treePdf;
 		}
-		if (occluded) bits |= kSfOccluded;
-		s.sfPi[p] = f4_of(hitPosInterp, __uint_as_float(bits));
-		s.shO[p] = f4_of(shadowO, dToL - 0.1f);
-		s.shD[p] = f4_of(dir, pdf);
-		s.shC[p] = f4(spectrum);
+		if (occluded) reinterpret_cast<float*>(s.sfPi + rec)[3] = __uint_as_float(bits | kSfOccluded);
+		s.shO[rec] = f4_of(shadowO, dToL - 0.1f);
+		s.shD[rec] = f4_of(dir, pdf);
+		s.shC[rec] = f4(spectrum);
 	}
 }
 
@@ -779,30 +791,30 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdfLight(const
 	const uint32_t n = min(s.counts[kSurfaceCounts + bounce], s.queueCap);
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
-		const uint32_t p = s.surfQueue[i];
-		const uint32_t bits = __float_as_uint(lastWord(s.sfPi + p));
+		const uint32_t bits = __float_as_uint(lastWord(s.sfPi + i));
 		if (bits & (kSfSkipped | kSfOccluded)) continue;
+		const uint32_t p = s.surfQueue[i];
 		const DevScene& sc = pathScene<JOBS>(scK, s, p);
-		const DevMaterial& mat = sc.materials[__float_as_uint(lastWord(s.sfP + p))];
-		const float4 rd = s.rayD[p], dd = s.shD[p];
+		const DevMaterial& mat = sc.materials[__float_as_uint(lastWord(s.sfP + i))];
+		const float4 rd = s.rayD[p], dd = s.shD[i];
 		const uint2 fd = s.fd[p];
 		BxdfState st;
 		st.hasNee = false;
-		st.wl.lambda = s4(s.lambda[p]);
+		st.wl.lambda = s4(s.sfL[i]);
 		st.T = s4(s.T[p]);
 		st.pdf = rd.w;
 		st.dir = f3_of(rd);
 		st.flags = fd.x;
 		st.refractionScale = lastWord(s.rayO + p);
 		LightSample dl;
-		dl.spectrum = s4(s.shC[p]);
+		dl.spectrum = s4(s.shC[i]);
 		dl.dir = f3_of(dd);
 		dl.pdf = dd.w;
 		dl.occluded = false;
-		const Frame frame{ f3_of(s.sfT[p]), f3_of(s.sfB[p]), f3_of(s.nrm[p]) };
+		const Frame frame{ f3_of(s.sfT[i]), f3_of(s.sfB[i]), f3_of(s.sfN[i]) };
 		evalBxdf<kBxdfLight>(sc, mat, dl, pathQrngT<JOBS>(sc, w, s, p, fd.y), frame, surfaceOf(mat), st);
-		if (st.hasNee) s.shC[p] = f4(st.nee);
-		else reinterpret_cast<float*>(s.sfPi + p)[3] = __uint_as_float(bits | kSfOccluded);
+		if (st.hasNee) s.shC[i] = f4(st.nee);
+		else reinterpret_cast<float*>(s.sfPi + i)[3] = __uint_as_float(bits | kSfOccluded);
 	}
 }
 
@@ -825,19 +837,19 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(const __gr
 		// Only the words the BxDF sample needs are read before it; the hit
 		// points, the geometric normal and the ray origin are read after it,
 		// so they are not live (and spilled) across the call.
-		const uint32_t bits = __float_as_uint(lastWord(s.sfPi + p));
+		const uint32_t bits = __float_as_uint(lastWord(s.sfPi + i));
 		const bool skipped = (bits & kSfSkipped) != 0, backHit = (bits & kSfBackHit) != 0;
 		const float4 rd = s.rayD[p];
 		const uint2 fd = s.fd[p];
 		uint32_t flags = fd.x, depth = fd.y;
 		const Qrng q = pathQrngT<JOBS>(sc, w, s, p, depth);
-		const DevMaterial& mat = sc.materials[__float_as_uint(lastWord(s.sfP + p))];
+		const DevMaterial& mat = sc.materials[__float_as_uint(lastWord(s.sfP + i))];
 
 		// The BxDF reads the wavelengths and changes none of them: only
 		// their values are loaded, and nothing is written back.
 		BxdfState st;
 		st.hasNee = false;
-		st.wl.lambda = s4(s.lambda[p]);
+		st.wl.lambda = s4(s.sfL[i]);
 		st.T = s4(s.T[p]);
 		st.pdf = rd.w;
 		st.dir = f3_of(rd);
@@ -848,7 +860,7 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(const __gr
 		{
 			LightSample dl;
 			dl.occluded = true;      // not read by the sample part
-			const Frame frame{ f3_of(s.sfT[p]), f3_of(s.sfB[p]), f3_of(s.nrm[p]) };
+			const Frame frame{ f3_of(s.sfT[i]), f3_of(s.sfB[i]), f3_of(s.sfN[i]) };
 			evalBxdf<kBxdfSample>(sc, mat, dl, q, frame, surfaceOf(mat), st);
 			hasShadow = !(bits & kSfOccluded) && !(st.flags & PF_PATH_TERMINATED);
 		}
@@ -884,7 +896,7 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(const __gr
 				const bool refracted = (flags & PF_RAY_REFRACTED) != 0;
 				const bool triGeo = (flags & PF_TRIANGULAR_GEOMETRY) != 0;
 				const bool in = refracted || skipped;
-				const f3 hitPos = f3_of(s.sfP[p]), hitPosInterp = f3_of(s.sfPi[p]), gn = f3_of(s.sfGn[p]);
+				const f3 hitPos = f3_of(s.sfP[i]), hitPosInterp = f3_of(s.sfPi[i]), gn = f3_of(s.sfGn[i]);
 				const f3 origin = (in == backHit) && triGeo ? hitPosInterp : hitPos;
 				const f3 offset = in == backHit ? gn : -gn;
 				rayO = offsetPoint(origin, offset);
@@ -913,7 +925,7 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(const __gr
 		if (hasShadow)
 		{
 			const uint32_t slot = appendSlot(shadowCount, s.queueCap, sc.status);
-			if (slot != kNoSlot) s.shadowQueue[slot] = p;
+			if (slot != kNoSlot) s.shadowQueue[slot] = i;
 		}
 		if (!done)
 		{

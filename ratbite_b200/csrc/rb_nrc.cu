@@ -21,6 +21,7 @@
 // all five layers are one hand-written kernel (mma.sync over the batch,
 // operands transposed by ldmatrix). Adam runs in FP32 on the master copies.
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -348,6 +349,148 @@ RB_D void rowWritten()
 	umma::fenceProxyAsync();
 	__syncthreads();
 }
+// Tile groups: a CTA of G x 128 threads runs G tiles side by side, group g
+// (threads 128 g ..) with its own activation tile, mbarrier and 64 TMEM
+// columns, all sharing one copy of the weights; a group synchronises on its
+// own named barrier (1 + g), so one group's gathers overlap another's MMAs
+// within the CTA, and more warps per SM fit than with one tile per CTA
+// (the weights are staged once per CTA).
+// Barrier ids are immediates (1 .. G), so the kernel reserves G + 1
+// barriers rather than all 16.
+template<int ID>
+RB_D void namedSync() { asm volatile("bar.sync %0, 128;" :: "n"(ID) : "memory"); }
+template<int ID>
+RB_D bool namedAnd(bool p)
+{
+	uint32_t out;
+	asm volatile(
+		"{\n\t.reg .pred pi, po;\n\t"
+		"setp.ne.u32 pi, %1, 0;\n\t"
+		"bar.red.and.pred po, %2, 128, pi;\n\t"
+		"selp.u32 %0, 1, 0, po;\n\t}\n"
+		: "=r"(out) : "r"(p ? 1u : 0u), "n"(ID) : "memory");
+	return out != 0;
+}
+template<int G>
+RB_D void groupSync(uint32_t g)
+{
+	static_assert(G == 1 || G == 2 || G == 4, "1, 2 or 4 tile groups");
+	if (G == 1) { __syncthreads(); return; }
+	switch (g)
+	{
+	case 0: namedSync<1>(); break;
+	case 1: namedSync<2>(); break;
+	case 2: namedSync<3>(); break;
+	default: namedSync<4>(); break;
+	}
+}
+template<int G>
+RB_D bool groupAnd(uint32_t g, bool p)
+{
+	if (G == 1) return __syncthreads_and(p) != 0;
+	switch (g)
+	{
+	case 0: return namedAnd<1>(p);
+	case 1: return namedAnd<2>(p);
+	case 2: return namedAnd<3>(p);
+	default: return namedAnd<4>(p);
+	}
+}
+template<int G>
+constexpr uint32_t smemGroups() { return kOffAct + G * kRows * 128u + 16u * G + 16u + 1024u; }
+
+struct GroupCtx
+{
+	unsigned char* base;
+	unsigned char* act;
+	uint64_t* bar;
+	uint32_t tmemBase;    // the CTA's allocation
+	uint32_t tmem;        // this group's 64 columns
+	uint32_t phase;
+	uint32_t g;           // group index
+	uint32_t tig;         // thread index in the group
+};
+template<int G>
+RB_D GroupCtx beginGroups(unsigned char* smraw, const __nv_bfloat16* __restrict__ w)
+{
+	GroupCtx c;
+	c.base = alignBase(smraw);
+	c.g = threadIdx.x >> 7;
+	c.tig = threadIdx.x & 127u;
+	c.act = c.base + kOffAct + c.g * kRows * 128u;
+	uint64_t* bars = reinterpret_cast<uint64_t*>(c.base + kOffAct + G * kRows * 128u);
+	uint32_t* slot = reinterpret_cast<uint32_t*>(bars + G);
+	c.bar = bars + c.g;
+	if (threadIdx.x < static_cast<uint32_t>(G)) umma::barrierInit(bars + threadIdx.x, 1);
+	if ((threadIdx.x >> 5) == 0) umma::tmemAlloc(slot, kTmemCols * G);
+	stageLayers(w, c.base);
+	umma::fenceProxyAsync();
+	umma::fenceBeforeSync();
+	__syncthreads();
+	umma::fenceAfterSync();
+	c.tmemBase = *slot;
+	c.tmem = c.tmemBase + kTmemCols * c.g;
+	c.phase = 0;
+	return c;
+}
+template<int G>
+RB_D void endGroups(const GroupCtx& c)
+{
+	umma::fenceBeforeSync();
+	__syncthreads();
+	if ((threadIdx.x >> 5) == 0) umma::tmemFree(c.tmemBase, kTmemCols * G);
+}
+// layerMma for a group: the group's first thread issues, the group waits.
+template<int G>
+RB_D bool groupLayerMma(GroupCtx& c, const unsigned char* bTile, uint32_t n, int nK, uint32_t* status)
+{
+	if (c.tig == 0)
+	{
+		umma::fenceAfterSync();
+		const uint32_t idesc = umma::idescBf16(kRows, n);
+		for (int k = 0; k < nK; ++k)
+			umma::mma(c.tmem, umma::descK(c.act, static_cast<uint32_t>(k)), umma::descK(bTile, static_cast<uint32_t>(k)),
+				idesc, k > 0);
+		umma::commit(c.bar);
+	}
+	const bool ok = groupAnd<G>(c.g, umma::barrierWait(c.bar, c.phase, kWaitLimit));
+	c.phase ^= 1u;
+	if (!ok)
+	{
+		if (c.tig == 0) atomicOr(status, RB_DEV_ITERATION_LIMIT);
+		umma::barrierWait(c.bar, c.phase ^ 1u, kWaitLimit);
+		return false;
+	}
+	umma::fenceAfterSync();
+	return true;
+}
+RB_D void groupReadAcc64(const GroupCtx& c, float (&v)[64])
+{
+	uint32_t r[4][16];
+#pragma unroll
+	for (int q = 0; q < 4; ++q) umma::tmemLoad16(umma::laneAddr(c.tmem, 16u * q), r[q]);
+	umma::tmemWaitLoad();
+#pragma unroll
+	for (int q = 0; q < 4; ++q)
+#pragma unroll
+		for (int j = 0; j < 16; ++j) v[16 * q + j] = __uint_as_float(r[q][j]);
+}
+RB_D void groupReadAcc16(const GroupCtx& c, float (&v)[16])
+{
+	uint32_t r[16];
+	umma::tmemLoad16(umma::laneAddr(c.tmem, 0), r);
+	umma::tmemWaitLoad();
+#pragma unroll
+	for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+template<int G>
+RB_D void groupRowWritten(uint32_t g)
+{
+	umma::fenceBeforeSync();
+	umma::fenceProxyAsync();
+	groupSync<G>(g);
+}
+
 RB_D void reluPack(const float (&v)[64], uint32_t (&row)[32])
 {
 #pragma unroll
@@ -378,14 +521,18 @@ RB_D void encodeRow(uint32_t r, uint32_t n, const float* __restrict__ in, const 
 // 32 w .. 32 w + 31; lane l takes the (row, level) pairs l, l + 32, ...
 // (16 per lane, their 8 corner gathers independent of each other), then the
 // 32 remaining columns of row 32 w + l. Each feature pair is one 32-bit
-// word of the swizzled tile.
+// word of the swizzled tile. RB_INFER_ROW_ENCODE=1 (the default) encodes
+// one row per thread instead (encodeRow). On B200, cached Cornell frame
+// 1920x1080x64 (inference ms per frame): row 14.3, warp-distributed 14.9 at
+// one tile per block (4 blocks per SM); with 2 tile groups 15.1 / 14.9,
+// with 4 (64 registers) 16.1.
 #ifndef RB_INFER_ROW_ENCODE
-#define RB_INFER_ROW_ENCODE 0
+#define RB_INFER_ROW_ENCODE 1
 #endif
 RB_D void encodeTile(uint32_t r0, uint32_t n, const float* __restrict__ in, const __half2* __restrict__ grid,
 	const Resolutions& R, unsigned char* tile)
 {
-	const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+	const uint32_t warp = (threadIdx.x >> 5) & 3u, lane = threadIdx.x & 31u;
 #pragma unroll 4
 	for (uint32_t k = lane; k < 32u * kLevels; k += 32u)
 	{
@@ -411,46 +558,57 @@ RB_D void encodeTile(uint32_t r0, uint32_t n, const float* __restrict__ in, cons
 }
 } // namespace t5
 
-// Inference with the encoding fused in (kMlpInfer's contract, on tcgen05).
-__global__ void __launch_bounds__(128) kMlpInferT(uint32_t cap, const uint32_t* __restrict__ count,
+// Inference with the encoding fused in (kMlpInfer's contract, on tcgen05),
+// G tiles per CTA (tile groups).
+#ifndef RB_INFER_GROUPS
+#define RB_INFER_GROUPS 1
+#endif
+constexpr int kInferGroups = RB_INFER_GROUPS;
+// Resident blocks the register allocation is capped for: 4 warps x G per
+// block, 16 tile warps per SM at G = 1 (shared memory allows 4 blocks), 24
+// at G = 2 (3 blocks), 32 at G = 4 (2 blocks).
+template<int G>
+constexpr int inferMinBlocks() { return G == 1 ? 4 : (G == 2 ? 3 : 2); }
+template<int G>
+__global__ void __launch_bounds__(128 * G, inferMinBlocks<G>()) kMlpInferT(uint32_t cap, const uint32_t* __restrict__ count,
 	const float* __restrict__ in, const __half2* __restrict__ grid, Resolutions R, const __nv_bfloat16* __restrict__ w,
 	float* __restrict__ out, const uint32_t* __restrict__ path, float4* __restrict__ L, const float4* __restrict__ T,
 	const float* __restrict__ corr, uint32_t* __restrict__ status)
 {
 	extern __shared__ unsigned char smraw[];
-	t5::Ctx c = t5::begin(smraw, w);
+	t5::GroupCtx c = t5::beginGroups<G>(smraw, w);
 	const uint32_t n = count ? min(*count, cap) : cap;
 	bool ok = true;
-	for (uint32_t r0 = blockIdx.x * t5::kRows; r0 < n && ok; r0 += gridDim.x * t5::kRows)
+	for (uint32_t r0 = (blockIdx.x * G + c.g) * t5::kRows; r0 < n && ok; r0 += gridDim.x * G * t5::kRows)
 	{
-		const uint32_t r = r0 + threadIdx.x;
+		const uint32_t r = r0 + c.tig;
 #if RB_INFER_ROW_ENCODE
 		{
 			uint32_t row[32];
 			t5::encodeRow(r, n, in, grid, R, row);
-			umma::storeRow(c.act, threadIdx.x, row);
+			umma::storeRow(c.act, c.tig, row);
 		}
 #else
 		t5::encodeTile(r0, n, in, grid, R, c.act);
 #endif
 		umma::fenceProxyAsync();
-		__syncthreads();
+		t5::groupSync<G>(c.g);
 		for (int l = 0; l < 4 && ok; ++l)
 		{
-			ok = t5::layerMma(c, t5::layerTile(c.base, l), 64, 4, status);
+			ok = t5::groupLayerMma<G>(c, t5::layerTile(c.base, l), 64, 4, status);
 			if (!ok) break;
 			float v[64];
-			t5::readAcc64(c, v);
+			t5::groupReadAcc64(c, v);
 			uint32_t row[32];
 			t5::reluPack(v, row);
-			umma::storeRow(c.act, threadIdx.x, row);
-			t5::rowWritten();
+			umma::storeRow(c.act, c.tig, row);
+			t5::groupRowWritten<G>(c.g);
 		}
 		if (!ok) break;
-		ok = t5::layerMma(c, t5::layerTile(c.base, 4), 16, 4, status);
+		ok = t5::groupLayerMma<G>(c, t5::layerTile(c.base, 4), 16, 4, status);
 		if (!ok) break;
 		float o[16];
-		t5::readAcc16(c, o);
+		t5::groupReadAcc16(c, o);
 		if (r < n)
 		{
 			const float4 y = make_float4(o[0], o[1], o[2], o[3]);
@@ -477,10 +635,11 @@ __global__ void __launch_bounds__(128) kMlpInferT(uint32_t cap, const uint32_t* 
 			}
 		}
 		umma::fenceBeforeSync();
-		__syncthreads();
+		t5::groupSync<G>(c.g);
 	}
-	t5::end(c);
+	t5::endGroups<G>(c);
 }
+constexpr uint32_t kSmemInfer = t5::smemGroups<kInferGroups>();
 
 // Training forward on the encoded rows X [n][64] (kMlpForward's contract):
 // out [n][kOutStride] f32 and the post-ReLU hidden rows acts [4][n][64] bf16.
@@ -839,7 +998,7 @@ struct rb_nrc
 	uint32_t* status = nullptr;            // RB_DEV_* bits of the network's kernels
 	uint32_t step = 0;
 	int smCount = 148;
-	uint32_t inferBlocksPerSm = 2, trainBlocksPerSm = 1;
+	uint32_t inferBlocksPerSm = 1, forwardBlocksPerSm = 1, trainBlocksPerSm = 1;
 };
 
 namespace
@@ -879,15 +1038,40 @@ int growScratch(rb_nrc* h, uint32_t n)
 	return RB_OK;
 }
 
+// Resident blocks per SM of a 128-thread tcgen05 kernel, from the SM's
+// limits: shared memory (with the per-block reservation), registers (per
+// warp in units of 256), threads, and tensor memory (t5::kTmemCols columns
+// of 512 per block). The kernels loop over tiles, so the grid is this many
+// blocks per SM; a grid of one block per SM leaves the grid gathers with
+// 4 warps per SM to hide their latency.
+uint32_t residentTileBlocks(const void* fn, size_t dynSmem, int device, uint32_t groups)
+{
+	int smemSm = 0, reserved = 0, regsSm = 0, threadsSm = 0;
+	cudaDeviceGetAttribute(&smemSm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
+	cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device);
+	cudaDeviceGetAttribute(&regsSm, cudaDevAttrMaxRegistersPerMultiprocessor, device);
+	cudaDeviceGetAttribute(&threadsSm, cudaDevAttrMaxThreadsPerMultiProcessor, device);
+	cudaFuncAttributes fa{};
+	if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess || smemSm <= 0 || regsSm <= 0 || threadsSm <= 0) return 1;
+	const size_t perBlockSmem = dynSmem + fa.sharedSizeBytes + static_cast<size_t>(reserved);
+	const uint32_t bySmem = static_cast<uint32_t>(static_cast<size_t>(smemSm) / perBlockSmem);
+	const uint32_t warpRegs = (static_cast<uint32_t>(fa.numRegs) * 32u + 255u) / 256u * 256u;
+	const uint32_t byRegs = warpRegs ? static_cast<uint32_t>(regsSm) / (4u * groups * warpRegs) : 32u;
+	const uint32_t byThreads = static_cast<uint32_t>(threadsSm) / (128u * groups);
+	const uint32_t byTmem = 512u / (t5::kTmemCols * groups);
+	const uint32_t b = std::min({ bySmem, byRegs, byThreads, byTmem });
+	return b < 1 ? 1u : b;
+}
+
 // Blocks of the tcgen05 kernels: one 128-row tile per block and step, at
 // most perSm resident blocks per SM (the kernels loop over tiles).
-int tileBlocks(const rb_nrc* h, uint32_t rows, uint32_t perSm)
+int tileBlocks(const rb_nrc* h, uint32_t rows, uint32_t perSm, uint32_t groups)
 {
-	const uint32_t tiles = (rows + t5::kRows - 1) / t5::kRows;
+	const uint32_t tiles = (rows + t5::kRows * groups - 1) / (t5::kRows * groups);
 	const uint32_t cap = static_cast<uint32_t>(h->smCount) * perSm;
 	return static_cast<int>(tiles < 1 ? 1 : (tiles < cap ? tiles : cap));
 }
-int inferBlocks(const rb_nrc* h, uint32_t rows) { return tileBlocks(h, rows, h->inferBlocksPerSm); }
+int inferBlocks(const rb_nrc* h, uint32_t rows) { return tileBlocks(h, rows, h->inferBlocksPerSm, kInferGroups); }
 
 int encodeBlocks(uint32_t rows)
 {
@@ -957,18 +1141,16 @@ int rb_nrc_create(const rb_nrc_config* config, rb_nrc** out)
 	std::memcpy(w.data() + wOffset(4), wo.data(), sizeof(float) * wo.size());
 	const int rc = rb_nrc_set_parameters(h, g.data(), w.data());
 	if (rc != RB_OK) { rb_nrc_destroy(h); return rc; }
-	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpInferT), cudaFuncAttributeMaxDynamicSharedMemorySize,
-		static_cast<int>(t5::kSmem));
+	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpInferT<kInferGroups>), cudaFuncAttributeMaxDynamicSharedMemorySize,
+		static_cast<int>(kSmemInfer));
 	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpForwardT), cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(t5::kSmem));
 	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpBackwardT), cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(kSmemBackwardT));
-	int perSm = 0;
-	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMlpInferT, 128, t5::kSmem) == cudaSuccess && perSm > 0)
-		h->inferBlocksPerSm = static_cast<uint32_t>(perSm);
-	perSm = 0;
-	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMlpBackwardT, 128, kSmemBackwardT) == cudaSuccess && perSm > 0)
-		h->trainBlocksPerSm = static_cast<uint32_t>(perSm);
+	h->inferBlocksPerSm = residentTileBlocks(reinterpret_cast<const void*>(kMlpInferT<kInferGroups>), kSmemInfer,
+		h->device, kInferGroups);
+	h->forwardBlocksPerSm = residentTileBlocks(reinterpret_cast<const void*>(kMlpForwardT), t5::kSmem, h->device, 1);
+	h->trainBlocksPerSm = residentTileBlocks(reinterpret_cast<const void*>(kMlpBackwardT), kSmemBackwardT, h->device, 1);
 	*out = h;
 	return RB_OK;
 }
@@ -1034,7 +1216,8 @@ int rb_nrc_infer(rb_nrc* h, uint32_t n, const float* inputs, float* outputs, voi
 	if (n == 0) return RB_OK;
 	cudaSetDevice(h->device);
 	const cudaStream_t st = static_cast<cudaStream_t>(stream);
-	kMlpInferT<<<inferBlocks(h, n), 128, t5::kSmem, st>>>(n, nullptr, inputs, reinterpret_cast<const __half2*>(h->grid),
+	kMlpInferT<kInferGroups><<<inferBlocks(h, n), 128 * kInferGroups, kSmemInfer, st>>>(n, nullptr, inputs,
+		reinterpret_cast<const __half2*>(h->grid),
 		h->R, h->w, outputs, nullptr, nullptr, nullptr, nullptr, h->status);
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
@@ -1050,10 +1233,10 @@ int computeGradients(rb_nrc* h, uint32_t n, const float* inputs, const float* ta
 	if (rc != RB_OK) return rc;
 	cudaMemsetAsync(h->loss, 0, sizeof(float), st);
 	kEncode<<<encodeBlocks(n), kThreads, 0, st>>>(n, inputs, reinterpret_cast<const __half2*>(h->grid), h->R, h->X);
-	kMlpForwardT<<<tileBlocks(h, n, h->inferBlocksPerSm), 128, t5::kSmem, st>>>(n, h->X, h->w, h->out, h->acts,
+	kMlpForwardT<<<tileBlocks(h, n, h->forwardBlocksPerSm, 1), 128, t5::kSmem, st>>>(n, h->X, h->w, h->out, h->acts,
 		h->status);
 	kLoss<<<gridFor(n), kThreads, 0, st>>>(n, h->out, targets, h->dY, h->loss, valid, outs, tStride, corr);
-	kMlpBackwardT<<<tileBlocks(h, n, h->trainBlocksPerSm), 128, kSmemBackwardT, st>>>(n, h->dY, h->wt, h->acts, h->dH,
+	kMlpBackwardT<<<tileBlocks(h, n, h->trainBlocksPerSm, 1), 128, kSmemBackwardT, st>>>(n, h->dY, h->wt, h->acts, h->dH,
 		h->dX0, h->status);
 	// weight gradients of the five layers, one launch
 	kWeightGrad<<<5 * ((n + kWgRows - 1) / kWgRows), 128, 0, st>>>(n, h->X, h->acts, h->dY, h->dH, h->wGrad);
@@ -1100,7 +1283,8 @@ int applyQueries(rb_nrc* h, uint32_t cap, const uint32_t* count, const float* in
 	const float4* T, const float* corr, cudaStream_t st)
 {
 	if (cap == 0) return RB_OK;
-	kMlpInferT<<<inferBlocks(h, cap), 128, t5::kSmem, st>>>(cap, count, inputs, reinterpret_cast<const __half2*>(h->grid),
+	kMlpInferT<kInferGroups><<<inferBlocks(h, cap), 128 * kInferGroups, kSmemInfer, st>>>(cap, count, inputs,
+		reinterpret_cast<const __half2*>(h->grid),
 		h->R, h->w, nullptr, path, L, T, corr, h->status);
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }

@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kShadow(const _
 {
 	const uint32_t n = min(s.counts[kShadowCounts + bounce], s.queueCap);
 	uint32_t rays = 0, nodes = 0, tris = 0;
-	uint32_t p = 0;
+	uint32_t r = 0;             // the shadow ray's surface record (queue position)
 	const DevScene* js = &sc;
 	AnyTraversal tr;
 	uint32_t stack[kTraversalStack];
@@ -123,17 +123,18 @@ __global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kShadow(const _
 		if (!tr.template run<COUNT>(g, kStepBudget, JOBS ? js->status : sc.status, nodes, tris, stack)) return false;
 		if (!tr.hit)
 		{
+			const uint32_t p = s.surfQueue[r];
 			S4 L = s4(s.L[p]);
-			L += s4(s.shC[p]);
+			L += s4(s.shC[r]);
 			s.L[p] = f4(L);
 		}
 		return true;
 	};
 	persistentTraversal<AnyTraversal>(n, s.counts + kShadowFetch + bounce,
 		[&](uint32_t idx) {
-			p = s.shadowQueue[idx];
-			if (JOBS) js = &s.jobs[s.job[p]].scene;
-			const float4 o = s.shO[p], d = s.shD[p];
+			r = s.shadowQueue[idx];
+			if (JOBS) js = &s.jobs[s.job[s.surfQueue[r]]].scene;
+			const float4 o = s.shO[r], d = s.shD[r];
 			tr.init(JOBS ? js->geo : sc.geo, f3_of(o), f3_of(d), 0.0f, o.w);
 			++rays;
 		}, step);

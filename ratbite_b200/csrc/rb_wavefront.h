@@ -23,27 +23,33 @@ struct PathSoA
 	float4* T;         // throughput
 	uint2* fd;         // flags, depth
 	float4* hit;       // closest hit: triangle (bits, -1 miss), t, b1, b2
+	// Surface records of the current bounce, and their light samples, are
+	// indexed by record (the position in surfQueue that kSurface took for
+	// the path), not by path slot: a warp's records are adjacent, so the
+	// shading kernels move them in whole sectors. surfQueue[record] is the
+	// path slot.
 	float4* shO;       // shadow ray origin, w: tmax
 	float4* shD;       // shadow ray direction
 	float4* shC;       // light sample spectrum, then the pending light-sample contribution
-	// surface record of the current bounce (written by kSurface)
 	float4* sfP;       // hit position, w: material index (bits)
 	float4* sfPi;      // shadow-terminator-offset position, w: surface bits (kSf*)
 	float4* sfGn;      // geometric normal
-	float4* sfT;       // shading frame tangent (the normal is nrm)
+	float4* sfT;       // shading frame tangent
 	float4* sfB;       // shading frame bitangent
+	float4* sfN;       // shading normal (the path keeps its own copy in nrm for the next bounce)
+	float4* sfL;       // the path's hero wavelengths (a copy of lambda)
 	uint32_t* queue[2];// active path slots, ping-pong by bounce parity
-	uint32_t* surfQueue;   // paths with a surface record this bounce
+	uint32_t* surfQueue;   // per record: its path slot
 	// emitter hits whose MIS weight needs the light-tree pdf (kEmission),
 	// indexed by queue position: path, (previous origin, BxDF pdf),
 	// (previous normal, area pdf), emitted spectrum, light index
-	uint32_t* neeQueue[2]; // light-sample records by light choice: tree picks, environment picks
+	uint32_t* neeQueue[2]; // records by light choice: tree picks, environment picks
 	uint32_t* emQueue;
 	float4* emA;
 	float4* emB;
 	float4* emC;
 	uint32_t* emLight;
-	uint32_t* shadowQueue;
+	uint32_t* shadowQueue;  // records whose shadow ray is traced
 	uint32_t* counts;  // kCountSlots words: see kShadowCounts, kSurfaceCounts
 	uint32_t capacity;
 	// jobs of a shared wavefront (rb_render_jobs; null for a single render):

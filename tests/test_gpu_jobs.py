@@ -93,3 +93,28 @@ def test_shared_wavefront_rejects_bad_jobs(tables):
         render_jobs([ris[0], empty], [0, 0], [1, 1])
     for ri in ris + [empty]:
         ri.cleanup()
+
+
+@pytest.mark.parametrize("grid_percent", [50, 200])
+def test_shared_wavefront_on_a_caller_stream(tables, grid_percent):
+    """The first call on fresh contexts allocates the wave and the job tables
+    (zero-filled on the host context's own stream) and renders on a caller's
+    stream with a large wave: the render must wait for the fills. Grids at
+    half and twice the resident maximum give the same accumulations."""
+    import torch
+    jobs = _jobs(tables)
+    counts = [5, 3, 2, 4]
+    alone = []
+    for (sc, lt), cnt in zip(jobs, counts):
+        with _open(tables, sc, lt) as ri:
+            ri.render(0, cnt)
+            alone.append(ri.read_accumulation())
+    ris = [_open(tables, sc, lt) for sc, lt in jobs]
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    render_jobs(ris, [0] * len(ris), counts, max_paths=12 << 20, grid_percent=grid_percent, stream=side.cuda_stream)
+    side.synchronize()
+    for k, (ri, want) in enumerate(zip(ris, alone)):
+        assert ri.status().flags == 0
+        assert np.array_equal(ri.read_accumulation(), want), k
+        ri.cleanup()
