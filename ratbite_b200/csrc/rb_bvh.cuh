@@ -18,6 +18,20 @@ namespace rb
 {
 constexpr int kTraversalStack = kTraversalStackEntries;
 
+// Traversal stack with its first S entries in shared memory and the rest in
+// local memory. Entry k of thread t is word k * kStride + t of the block's
+// shared array, so the lanes of a warp at one depth touch consecutive words.
+// In shared memory the entries no longer compete with the BVH nodes and
+// triangles for L1 (local memory is cached there). The traversal takes any
+// stack type with operator[] (a plain local array, or this).
+template<typename T, int S, int kStride>
+struct HybridStack
+{
+	T* sm;                                   // the block's array + threadIdx.x
+	T local[kTraversalStack - S];
+	RB_D T& operator[](int k) { return k < S ? sm[k * kStride] : local[k - S]; }
+};
+
 // Traversal variants (compile-time): RB_TRAV_SORT orders the entered
 // children near-to-far with a sorting network (1, the default; 0: descend
 // the nearest, push the rest unordered; 2: direction-octant order, the
@@ -302,8 +316,8 @@ struct ClosestTraversal
 	// Stack entries: (child reference, entry-distance bits, truncated down:
 	// popping compares a value <= the true distance, so culling stays
 	// conservative).
-	template<bool COUNT>
-	RB_D bool nodeStep(const DevGeometry& g, uint32_t* status, uint32_t& nNodes, uint2 (&stack)[kTraversalStack])
+	template<bool COUNT, class Stack>
+	RB_D bool nodeStep(const DevGeometry& g, uint32_t* status, uint32_t& nNodes, Stack& stack)
 	{
 		if (COUNT) ++nNodes;
 		const NodeView nv = loadNode(g.nodes, cur);
@@ -372,7 +386,8 @@ struct ClosestTraversal
 	}
 
 	// Pops the next entry that may still hold a closer hit; false when none is left.
-	RB_D bool pop(const uint2 (&stack)[kTraversalStack])
+	template<class Stack>
+	RB_D bool pop(Stack& stack)
 	{
 		while (sp > 0)
 		{
@@ -385,9 +400,8 @@ struct ClosestTraversal
 
 	// The stack lives outside the state (separate local arrays) so that the
 	// scalar state can stay in registers.
-	template<bool COUNT>
-	RB_D bool run(const DevGeometry& g, int budget, uint32_t* status, uint32_t& nNodes, uint32_t& nTris,
-		uint2 (&stack)[kTraversalStack])
+	template<bool COUNT, class Stack>
+	RB_D bool run(const DevGeometry& g, int budget, uint32_t* status, uint32_t& nNodes, uint32_t& nTris, Stack& stack)
 	{
 #if RB_TRAV_WHILE_WHILE
 		// interior nodes until a leaf, then the leaf: lanes of a warp meet at
@@ -498,9 +512,8 @@ struct AnyTraversal
 		cur = g.rootIsLeaf ? (kLeafBit | (static_cast<uint32_t>(g.triCount - 1) << 28)) : 0u;
 	}
 
-	template<bool COUNT>
-	RB_D bool run(const DevGeometry& g, int budget, uint32_t* status, uint32_t& nNodes, uint32_t& nTris,
-		uint32_t (&stack)[kTraversalStack])
+	template<bool COUNT, class Stack>
+	RB_D bool run(const DevGeometry& g, int budget, uint32_t* status, uint32_t& nNodes, uint32_t& nTris, Stack& stack)
 	{
 		for (int it = 0; it < budget && !done; ++it)
 		{

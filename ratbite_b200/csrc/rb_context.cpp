@@ -335,8 +335,7 @@ int ensureWave(rb_ctx* ctx, uint32_t paths)
 	alloc(s.sfT, sizeof(float4)); alloc(s.sfB, sizeof(float4)); alloc(s.sfN, sizeof(float4));
 	alloc(s.sfL, sizeof(float4));
 	alloc(s.queue[0], sizeof(uint32_t)); alloc(s.queue[1], sizeof(uint32_t)); alloc(s.shadowQueue, sizeof(uint32_t));
-	alloc(s.surfQueue, sizeof(uint32_t));
-	alloc(s.neeQueue[0], sizeof(uint32_t)); alloc(s.neeQueue[1], sizeof(uint32_t));
+	alloc(s.surfQueue, sizeof(uint32_t)); alloc(s.recOrder, sizeof(uint32_t));
 	alloc(s.emQueue, sizeof(uint32_t)); alloc(s.emA, sizeof(float4)); alloc(s.emB, sizeof(float4));
 	alloc(s.emC, sizeof(float4)); alloc(s.emLight, sizeof(uint32_t));
 	if (rc == RB_OK)
@@ -1130,7 +1129,7 @@ int renderWaves(rb_ctx* ctx, uint32_t offset, uint32_t count, cudaStream_t st, c
 	const rb::DevScene& sc = ctx->scene;
 	const uint32_t pixels = sc.launch.width * sc.launch.height;
 	// Wave size: whole sample planes, up to the capacity (default 16M paths,
-	// about 6.3 GB of path state).
+	// about 6.2 GB of path state).
 	const bool cached = ctx->cache != nullptr;
 	const rb_cache_params& CP = ctx->cacheParams;
 	const uint32_t planesPerWave = planesPerWaveFor(ctx, count);
@@ -1198,7 +1197,7 @@ int renderWaves(rb_ctx* ctx, uint32_t offset, uint32_t count, cudaStream_t st, c
 			timedStage(ctx, 2, st, [&] { rb::launchSurface(sc, soa, w, b, shape, st, cnt); });
 			timedStage(ctx, 2, st, [&] { rb::launchEmission(sc, soa, b, shape, st); });
 			timedStage(ctx, 5, st, [&] { rb::launchNee(sc, soa, w, b, shape, st); });
-			ctx->launches[5] += 2;   // launchNee runs the pick kernel and two light-sample kernels
+			ctx->launches[5] += 1;   // launchNee runs two light-sample kernels (tree and environment picks)
 			timedStage(ctx, 6, st, [&] { rb::launchBsdf(sc, soa, w, b, shape, st); });
 			ctx->launches[6] += 1;   // launchBsdf runs the light-sample evaluation and the BxDF sample kernels
 			timedStage(ctx, 3, st, [&] { rb::launchShadow(sc, soa, b, shape, st, cnt); });
@@ -1227,7 +1226,9 @@ int renderWaves(rb_ctx* ctx, uint32_t offset, uint32_t count, cudaStream_t st, c
 					rb::launchCacheCorrectionUpdate(ctx->cacheCorr, st);
 				});
 				if (rc != RB_OK) return fail(ctx, rc, "rb_render: cache training");
-				ctx->launches[8] += 9 * steps + 1;   // per step: gather + 8 network kernels (cuBLAS GEMMs not counted); corrections
+				// targets, per step the row gather and 9 network kernels (encode, forward, loss,
+				// backward, weight gradients, grid backward, two Adam, transposed weights), corrections
+				ctx->launches[8] += 10 * steps + 1;
 			}
 			rb::launchCacheTally(soa, ctx->cacheTally, st);
 			++ctx->launches[8];
@@ -1376,7 +1377,7 @@ int rb_render_jobs(rb_ctx* const* jobs, uint32_t n, const uint32_t* offsets, con
 	rb::LaunchShape shape = host->shape;
 	const uint32_t pct = options && options->grid_percent ? options->grid_percent : 100u;
 	for (int* b : { &shape.blocksGenerate, &shape.blocksExtend, &shape.blocksSurface, &shape.blocksEmission,
-			&shape.blocksNeePick, &shape.blocksNee, &shape.blocksBsdf, &shape.blocksBsdfLight, &shape.blocksShadow,
+			&shape.blocksNee, &shape.blocksBsdf, &shape.blocksBsdfLight, &shape.blocksShadow,
 			&shape.blocksResolve })
 		*b = std::max(1, static_cast<int>(static_cast<uint64_t>(*b) * pct / 100u));
 	const rb::DevScene& sc = host->scene;
@@ -1402,6 +1403,14 @@ int rb_render_jobs(rb_ctx* const* jobs, uint32_t n, const uint32_t* offsets, con
 			rb::launchShadow(sc, soa, b, shape, st, nullptr);
 		}
 		rb::launchResolve(sc, soa, w, nullptr, shape, st);
+		// kernels launched, by stage as rb_render counts them
+		host->launches[0] += 1;
+		host->launches[1] += bounces;
+		host->launches[2] += 2 * bounces;
+		host->launches[5] += 2 * bounces;
+		host->launches[6] += 2 * bounces;
+		host->launches[3] += bounces;
+		host->launches[4] += 1;
 		host->pathsTraced += w.paths;
 		++host->waves;
 		if (options && options->done_events)

@@ -380,6 +380,7 @@ constexpr uint32_t kSfDepthShift = 8;
 static_assert(kMaxBounces <= 255, "depth fits bits 8..15");
 RB_D uint32_t sfDepth(uint32_t bits) { return (bits >> kSfDepthShift) & 0xFFu; }
 
+
 RB_D Qrng pathQrng(const DevScene& sc, const WaveParams& w, uint32_t p, uint32_t depth)
 {
 	const uint2 px = slotPixel(p % w.pixels, sc.launch.width, sc.launch.height);
@@ -469,7 +470,7 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(cons
 {
 	const uint32_t n = min(s.counts[bounce], s.queueCap);
 	const uint32_t* queue = s.queue[bounce & 1];
-	uint32_t* surfCount = s.counts + kSurfaceCounts + bounce;
+	unsigned long long* regions = reinterpret_cast<unsigned long long*>(s.counts + kRegionCounts + 2 * bounce);
 	uint32_t records = 0;
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
@@ -578,11 +579,25 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(cons
 			const uint32_t bits = (it.backHit ? kSfBackHit : 0u) | (skipped ? kSfSkipped : 0u)
 				| ((flags & PF_TRIANGULAR_GEOMETRY) ? kSfTriangle : 0u) | (depth << kSfDepthShift);
 			s.nrm[p] = f4_of(lastNormal, nv.w);
-			// the record lives at its queue position: a warp's records are
-			// adjacent, so the shading kernels read them in whole sectors
-			const uint32_t r = appendSlot(surfCount, s.queueCap, sc.status);
+			// The light choice of the record's light sample (pathtrace.cu:
+			// 1572-1590: the environment with probability envImp, else the
+			// tree) decides its region: tree picks from record 0 up, the rest
+			// (environment picks and skipped surfaces, which take no light
+			// sample) from queueCap - 1 down, so each light-sample launch
+			// reads its records densely.
+			bool sky = true;
+			if (!skipped)
+			{
+				const bool envPresent = sc.env.enabled != 0;
+				const bool treePresent = sc.lights.nodes != nullptr;
+				const float envImp = envPresent ? (treePresent ? kEnvMapImportance : 1.0f) : 0.0f;
+				if (envPresent || treePresent) sky = sample3DZ(pathQrngT<JOBS>(sc, w, s, p, depth), DIM_LIGHT) < envImp;
+			}
+			uint32_t order = 0;
+			const uint32_t r = appendRegion(regions, sky, s.queueCap, sc.status, order);
 			if (r != kNoSlot)
 			{
+				s.recOrder[order] = r;
 				s.surfQueue[r] = p;
 				s.sfP[r] = f4_of(it.hitPos, __uint_as_float(it.material));
 				s.sfPi[r] = f4_of(it.hitPosInterp, __uint_as_float(bits));
@@ -638,61 +653,26 @@ __global__ void __launch_bounds__(kThreads) kEmission(const __grid_constant__ De
 	}
 }
 
-// Sorts the surface records that need a light sample by the light choice
-// of sampleLightTree (pathtrace.cu:1064-1076): records that pick the
-// environment (and all records when neither the tree nor the environment
-// exists) go to queue 1, tree picks to queue 0. The choice uses the same
-// sample dimension and comparison as the light-sample body that follows.
-template<bool JOBS>
-__global__ void __launch_bounds__(kThreads) kNeePick(const __grid_constant__ DevScene scK, PathSoA s, WaveParams w, int bounce)
-{
-	const uint32_t n = min(s.counts[kSurfaceCounts + bounce], s.queueCap);
-	for (uint32_t i = gtid(); i < n; i += gstride())
-	{
-		const uint32_t bits = __float_as_uint(lastWord(s.sfPi + i));
-		if (bits & kSfSkipped) continue;
-		const uint32_t p = s.surfQueue[i];
-		const DevScene& sc = pathScene<JOBS>(scK, s, p);
-		const bool envPresent = sc.env.enabled != 0;
-		const bool treePresent = sc.lights.nodes != nullptr;
-		const float envImp = envPresent ? (treePresent ? kEnvMapImportance : 1.0f) : 0.0f;
-		bool sky = true;
-		if (envPresent || treePresent)
-		{
-			const Qrng q = pathQrngT<JOBS>(sc, w, s, p, sfDepth(bits));
-			sky = sample3D(q, DIM_LIGHT).z < envImp;
-		}
-		// one counter per branch: appendIndex aggregates over the lanes active at the call
-		if (sky)
-		{
-			const uint32_t slot = appendSlot(s.counts + kNeeSkyCounts + bounce, s.queueCap, sc.status);
-			if (slot != kNoSlot) s.neeQueue[1][slot] = i;
-		}
-		else
-		{
-			const uint32_t slot = appendSlot(s.counts + kNeeTreeCounts + bounce, s.queueCap, sc.status);
-			if (slot != kNoSlot) s.neeQueue[0][slot] = i;
-		}
-	}
-}
-
 // Stage 2 of shading: the light sample (pathtrace.cu:1572-1721) for every
 // surface that is not skipped: pick a light from the light tree (held in the
 // read-only cache: it is read by every thread) or the environment, sample a
 // point on it and write the shadow ray and the light sample.
 // SHARED: the block first copies the unpacked tree into shared memory
 // (dynamic, nodeCount x 48 B) and descends it there; used when the tree fits.
-// The records come from one of kNeePick's queues (`which`: 0 tree picks,
-// 1 environment picks), so a warp's lanes take the same branch of the light
-// choice; the body is the same for both.
+// The records come from one region of the record arrays (`which`: 0 the
+// tree picks, records 0 ..; 1 the environment picks, records queueCap - 1
+// down), which kSurface chose with the light choice of sampleLightTree
+// (pathtrace.cu:1064-1076: the same sample dimension and comparison as the
+// body below), so a warp's lanes take the same branch of the light choice
+// and read their records densely; the body is the same for both.
 // JOBS (a shared wavefront; never with SHARED): each record's tree is its job's.
 template<bool SHARED, bool JOBS>
 __global__ void __launch_bounds__(SHARED ? kNeeSharedThreads : kThreads, SHARED ? 2 : RB_NEE_MIN_BLOCKS)
 kNee(const __grid_constant__ DevScene scK, PathSoA s, WaveParams w, int bounce, int which)
 {
 	extern __shared__ float4 sharedTree[];
-	const uint32_t n = min(s.counts[(which ? kNeeSkyCounts : kNeeTreeCounts) + bounce], s.queueCap);
-	const uint32_t* queue = s.neeQueue[which];
+	const uint2 nr = regionCounts(s.counts + kRegionCounts + 2 * bounce, s.queueCap);
+	const uint32_t n = which ? nr.y : nr.x;
 	const TreeNodeU* sharedNodes = scK.lights.unpacked;
 	if (SHARED)
 	{
@@ -704,14 +684,15 @@ kNee(const __grid_constant__ DevScene scK, PathSoA s, WaveParams w, int bounce, 
 	}
 	for (uint32_t i = gtid(); i < n; i += gstride())
 	{
-		const uint32_t rec = queue[i];
+		const uint32_t rec = which ? s.queueCap - 1u - i : i;
+		const float4 pi = s.sfPi[rec];
+		uint32_t bits = __float_as_uint(pi.w);
+		if (bits & kSfSkipped) continue;              // environment region only: no light sample
 		const uint32_t p = s.surfQueue[rec];
 		const DevScene& sc = pathScene<JOBS>(scK, s, p);
 		const TreeNodeU* nodes = JOBS ? sc.lights.unpacked : sharedNodes;
 		const bool envPresent = sc.env.enabled != 0;
 		const bool treePresent = sc.lights.nodes != nullptr;
-		const float4 pi = s.sfPi[rec];
-		uint32_t bits = __float_as_uint(pi.w);
 		const float4 hp = s.sfP[rec];
 		const f3 hitPos = f3_of(hp), hitPosInterp = f3_of(pi), gn = f3_of(s.sfGn[rec]), sn = f3_of(s.sfN[rec]);
 		f3 dir = mk(0.0f), shadowO = mk(0.0f);
@@ -788,9 +769,11 @@ template<bool JOBS>
 __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdfLight(const __grid_constant__ DevScene scK, PathSoA s,
 	WaveParams w, int bounce)
 {
-	const uint32_t n = min(s.counts[kSurfaceCounts + bounce], s.queueCap);
-	for (uint32_t i = gtid(); i < n; i += gstride())
+	const uint2 nr = regionCounts(s.counts + kRegionCounts + 2 * bounce, s.queueCap);
+	const uint32_t n = nr.x + nr.y;
+	for (uint32_t j = gtid(); j < n; j += gstride())
 	{
+		const uint32_t i = s.recOrder[j];
 		const uint32_t bits = __float_as_uint(lastWord(s.sfPi + i));
 		if (bits & (kSfSkipped | kSfOccluded)) continue;
 		const uint32_t p = s.surfQueue[i];
@@ -826,12 +809,14 @@ template<bool JOBS>
 __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(const __grid_constant__ DevScene scK, PathSoA s,
 	WaveParams w, int bounce)
 {
-	const uint32_t n = min(s.counts[kSurfaceCounts + bounce], s.queueCap);
+	const uint2 nr = regionCounts(s.counts + kRegionCounts + 2 * bounce, s.queueCap);
+	const uint32_t n = nr.x + nr.y;
 	uint32_t* nextQueue = s.queue[(bounce + 1) & 1];
 	uint32_t* nextCount = s.counts + bounce + 1;
 	uint32_t* shadowCount = s.counts + kShadowCounts + bounce;
-	for (uint32_t i = gtid(); i < n; i += gstride())
+	for (uint32_t j = gtid(); j < n; j += gstride())
 	{
+		const uint32_t i = s.recOrder[j];
 		const uint32_t p = s.surfQueue[i];
 		const DevScene& sc = pathScene<JOBS>(scK, s, p);
 		// Only the words the BxDF sample needs are read before it; the hit
@@ -1195,7 +1180,6 @@ LaunchShape queryLaunchShape()
 	ls.blocksSurface = occ(reinterpret_cast<const void*>(kSurface<false>));
 	ls.blocksNee = occ(reinterpret_cast<const void*>(kNee<false, false>));
 	ls.blocksEmission = occ(reinterpret_cast<const void*>(kEmission<false>));
-	ls.blocksNeePick = occ(reinterpret_cast<const void*>(kNeePick<false>));
 	cudaFuncSetAttribute(reinterpret_cast<const void*>(kNee<true, false>), cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(kNeeSharedMaxBytes));
 	ls.blocksBsdf = occ(reinterpret_cast<const void*>(kBsdf<false>));
@@ -1231,12 +1215,10 @@ void launchNee(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bo
 	const int g = capBlocks(ls.blocksNee, ls.items, kThreads);
 	if (s.jobs)
 	{
-		kNeePick<true><<<capBlocks(ls.blocksNeePick, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce);
 		kNee<false, true><<<g, kThreads, 0, st>>>(sc, s, w, bounce, 0);
 		kNee<false, true><<<g, kThreads, 0, st>>>(sc, s, w, bounce, 1);
 		return;
 	}
-	kNeePick<false><<<capBlocks(ls.blocksNeePick, ls.items, kThreads), kThreads, 0, st>>>(sc, s, w, bounce);
 	const size_t treeBytes = sizeof(TreeNodeU) * sc.lights.nodeCount;
 	if (sc.lights.unpacked && treeBytes <= kNeeSharedMaxBytes)
 	{

@@ -38,6 +38,43 @@ RB_D uint32_t appendSlot(uint32_t* counter, uint32_t cap, uint32_t* status)
 	return kNoSlot;
 }
 
+// Record of a surface in one of two regions of the record arrays, `sky`
+// choosing the region: the tree region grows from 0 up (low word of
+// *counter), the other from cap - 1 down (high word). One 64-bit atomic per
+// warp for both. A record is kept only while the two regions together hold
+// at most `cap`, so they never overlap; beyond it the entry is dropped with
+// RB_DEV_QUEUE_OVERFLOW and kNoSlot returned. `order` gets the record's
+// position in the order of arrival over both regions (0 .. total - 1).
+RB_D uint32_t appendRegion(unsigned long long* counter, bool sky, uint32_t cap, uint32_t* status, uint32_t& order)
+{
+	const uint32_t active = __activemask();
+	const uint32_t skyMask = __ballot_sync(active, sky), treeMask = active & ~skyMask;
+	const int leader = __ffs(active) - 1;
+	const uint32_t lane = threadIdx.x & 31u, below = (1u << lane) - 1u;
+	unsigned long long base = 0;
+	if (lane == static_cast<uint32_t>(leader))
+		base = atomicAdd(counter, static_cast<unsigned long long>(__popc(treeMask))
+			| (static_cast<unsigned long long>(__popc(skyMask)) << 32));
+	base = __shfl_sync(active, base, leader);
+	const uint32_t treeBase = static_cast<uint32_t>(base), skyBase = static_cast<uint32_t>(base >> 32);
+	// records of both regions up to and including this one
+	const uint64_t total = static_cast<uint64_t>(treeBase) + skyBase + __popc(active & below) + 1u;
+	if (total > cap)
+	{
+		atomicOr(status, RB_DEV_QUEUE_OVERFLOW);
+		return kNoSlot;
+	}
+	order = static_cast<uint32_t>(total - 1u);
+	return sky ? cap - 1u - (skyBase + __popc(skyMask & below)) : treeBase + __popc(treeMask & below);
+}
+// The two region counts of a bounce (kRegionCounts), each at most cap and
+// together at most cap.
+RB_D uint2 regionCounts(const uint32_t* counts2, uint32_t cap)
+{
+	const uint32_t t = min(counts2[0], cap);
+	return make_uint2(t, min(counts2[1], cap - t));
+}
+
 // Adds per-thread counts to a 64-bit counter with one atomic per warp.
 RB_D void warpAdd(unsigned long long* dst, uint32_t v)
 {

@@ -640,6 +640,237 @@ __global__ void __launch_bounds__(128 * G, inferMinBlocks<G>()) kMlpInferT(uint3
 	t5::endGroups<G>(c);
 }
 constexpr uint32_t kSmemInfer = t5::smemGroups<kInferGroups>();
+// RB_INFER_WS=1 (the default) answers queries with the warp-specialized
+// kernel (kMlpInferWS); 0 with kMlpInferT<RB_INFER_GROUPS>.
+#ifndef RB_INFER_WS
+#define RB_INFER_WS 1
+#endif
+
+// Inference, warp-specialized (the default for queries): 8 encoder warps
+// fill a ring of activation tiles with encoded rows (two threads per row,
+// 8 grid levels each), 4 MLP warps run the five tcgen05 layers on each
+// filled tile and apply the output. mbarriers pass the tiles (full: one
+// arrival per encoder thread; empty: one arrival once the tile's last MMA
+// has completed), so the encoders' grid gathers for the next tiles overlap
+// the layers of the current one and no warp waits on a block-wide barrier.
+// Every wait is bounded: one that gives up sets RB_DEV_ITERATION_LIMIT and
+// its role stops; the other role's waits then give up too.
+namespace ws
+{
+// Encoder warps per block (8 or 12 or 16). On B200, cached Cornell frame
+// 1920x1080x64 (inference ms per frame): 8 encoder warps 14.9 - 16.5 for
+// every encoder layout and unroll tried (one level per thread, half a row
+// per thread; 2 / 4 / 8 rows in flight), the same as one tile per 128-thread
+// block (14.3): the MLP side alone takes 2.6 ms, the gathers the rest, so
+// what moves it is the number of warps gathering per SM.
+#ifndef RB_WS_ENC_WARPS
+#define RB_WS_ENC_WARPS 12
+#endif
+constexpr uint32_t kEncWarps = RB_WS_ENC_WARPS, kMlpWarps = 4;
+constexpr uint32_t kEncThreads = 32u * kEncWarps;
+constexpr uint32_t kThreads = kEncThreads + 32u * kMlpWarps;
+constexpr uint32_t kStages = 4;
+constexpr uint32_t kTileBytes = t5::kRows * 128u;
+constexpr uint32_t kOffStages = t5::kOffAct;
+constexpr uint32_t kOffBars = kOffStages + kStages * kTileBytes;  // full[kStages], empty[kStages], mma, TMEM slot
+constexpr uint32_t kSmem = kOffBars + 8u * (2u * kStages + 1u) + 8u + 1024u;
+constexpr int kMinBlocks = 2;
+static_assert(kOffStages % 1024 == 0 && kTileBytes % 1024 == 0, "operand tiles start on 1024-byte boundaries");
+static_assert(kEncThreads % 16u == 0 && kEncThreads >= 256u, "whole levels per thread; the remaining columns in one pass");
+#ifndef RB_WS_ENCODE_UNROLL
+#define RB_WS_ENCODE_UNROLL 2
+#endif
+constexpr int kWsEncodeUnroll = RB_WS_ENCODE_UNROLL;
+
+// Encoder thread e keeps one grid level, l = e % 16, and encodes it for rows
+// e / 16, e / 16 + kEncThreads / 16, ... of the tile, so a warp's gathers at
+// one instruction cover 16 levels of 2 rows (the level's resolution and table
+// are per-thread constants); then threads 0..255 write the 32 remaining
+// columns, 16 for each of rows e / 2.
+RB_D void encodeLevels(uint32_t t0, uint32_t n, const float* __restrict__ in, const __half2* __restrict__ grid,
+	const Resolutions& R, unsigned char* tile)
+{
+	const uint32_t e = threadIdx.x, l = e & 15u;
+#pragma unroll kWsEncodeUnroll
+	for (uint32_t rl = e >> 4; rl < t5::kRows; rl += kEncThreads / 16u)
+	{
+		const uint32_t r = t0 + rl;
+		float f0 = 0.0f, f1 = 0.0f;
+		if (r < n)
+		{
+			const float* v = in + static_cast<size_t>(kNrcInputs) * r;
+			levelFeatures(R, grid, static_cast<int>(l), clamp01(v[0]), clamp01(v[1]), clamp01(v[2]), f0, f1);
+		}
+		*reinterpret_cast<uint32_t*>(tile + umma::swzOffset(rl, 2u * l)) = pack2(f0, f1);
+	}
+	if (e >= 2u * t5::kRows) return;
+	const uint32_t rl = e >> 1, r = t0 + rl, k0 = 16u * (e & 1u);
+	const float* v = in + static_cast<size_t>(kNrcInputs) * r;
+	uint32_t w[8];
+#pragma unroll
+	for (int j = 0; j < 8; ++j)
+		w[j] = r < n ? pack2(restColumn(v, static_cast<int>(k0) + 2 * j), restColumn(v, static_cast<int>(k0) + 2 * j + 1)) : 0u;
+	const uint32_t c = 4u + (k0 >> 3);
+	unsigned char* row = tile + rl * 128u;
+	*reinterpret_cast<uint4*>(row + (((c ^ rl) & 7u) << 4)) = make_uint4(w[0], w[1], w[2], w[3]);
+	*reinterpret_cast<uint4*>(row + ((((c + 1u) ^ rl) & 7u) << 4)) = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+// Hidden layer epilogue for row m, in two halves of 32 columns (so that the
+// 64-register cap of 16 warps per block holds): TMEM -> ReLU -> BF16 ->
+// chunks 4 h .. 4 h + 3 of the row, in place.
+RB_D void reluRowHalves(uint32_t tmem, unsigned char* act, uint32_t m)
+{
+#pragma unroll
+	for (uint32_t h = 0; h < 2; ++h)
+	{
+		uint32_t q0[16], q1[16];
+		umma::tmemLoad16(umma::laneAddr(tmem, 32u * h), q0);
+		umma::tmemLoad16(umma::laneAddr(tmem, 32u * h + 16u), q1);
+		umma::tmemWaitLoad();
+		uint32_t w[16];
+#pragma unroll
+		for (int j = 0; j < 8; ++j)
+		{
+			w[j] = pack2(fmaxf(__uint_as_float(q0[2 * j]), 0.0f), fmaxf(__uint_as_float(q0[2 * j + 1]), 0.0f));
+			w[8 + j] = pack2(fmaxf(__uint_as_float(q1[2 * j]), 0.0f), fmaxf(__uint_as_float(q1[2 * j + 1]), 0.0f));
+		}
+		unsigned char* row = act + m * 128u;
+#pragma unroll
+		for (uint32_t c = 0; c < 4; ++c)
+			*reinterpret_cast<uint4*>(row + ((((4u * h + c) ^ m) & 7u) << 4)) =
+				make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
+	}
+}
+} // namespace ws
+
+__global__ void __launch_bounds__(ws::kThreads, ws::kMinBlocks) kMlpInferWS(uint32_t cap, const uint32_t* __restrict__ count,
+	const float* __restrict__ in, const __half2* __restrict__ grid, Resolutions R, const __nv_bfloat16* __restrict__ w,
+	float* __restrict__ out, const uint32_t* __restrict__ path, float4* __restrict__ L, const float4* __restrict__ T,
+	const float* __restrict__ corr, uint32_t* __restrict__ status)
+{
+	extern __shared__ unsigned char smraw[];
+	unsigned char* base = t5::alignBase(smraw);
+	uint64_t* full = reinterpret_cast<uint64_t*>(base + ws::kOffBars);
+	uint64_t* empty = full + ws::kStages;
+	uint64_t* mmaBar = empty + ws::kStages;
+	uint32_t* slot = reinterpret_cast<uint32_t*>(mmaBar + 1);
+	const uint32_t warp = threadIdx.x >> 5;
+	if (threadIdx.x == 0)
+	{
+		for (uint32_t s = 0; s < ws::kStages; ++s)
+		{
+			umma::barrierInit(full + s, 32u * ws::kEncWarps);
+			umma::barrierInit(empty + s, 1);
+		}
+		umma::barrierInit(mmaBar, 1);
+	}
+	if (warp == 0) umma::tmemAlloc(slot, t5::kTmemCols);
+	t5::stageLayers(w, base);
+	umma::fenceProxyAsync();
+	umma::fenceBeforeSync();
+	__syncthreads();
+	umma::fenceAfterSync();
+	const uint32_t tmem = *slot;
+	const uint32_t n = count ? min(*count, cap) : cap;
+	const uint32_t tiles = (n + t5::kRows - 1) / t5::kRows;
+	if (warp < ws::kEncWarps)
+	{
+		uint32_t k = 0;
+		for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++k)
+		{
+			const uint32_t s = k % ws::kStages;
+			if (k >= ws::kStages && !umma::barrierWait(empty + s, ((k / ws::kStages) + 1u) & 1u, t5::kWaitLimit))
+			{
+				atomicOr(status, RB_DEV_ITERATION_LIMIT);
+				break;
+			}
+			unsigned char* tile = base + ws::kOffStages + s * ws::kTileBytes;
+			ws::encodeLevels(t * t5::kRows, n, in, grid, R, tile);
+			umma::fenceProxyAsync();
+			umma::barrierArrive(full + s);
+		}
+	}
+	else
+	{
+		// MLP: thread m owns row m of the tile and TMEM lane m
+		const uint32_t m = threadIdx.x - 32u * ws::kEncWarps;
+		uint32_t k = 0, mmaPhase = 0;
+		bool ok = true;
+		for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++k)
+		{
+			const uint32_t s = k % ws::kStages;
+			unsigned char* act = base + ws::kOffStages + s * ws::kTileBytes;
+			ok = t5::namedAnd<1>(umma::barrierWait(full + s, (k / ws::kStages) & 1u, t5::kWaitLimit));
+			if (!ok)
+			{
+				if (m == 0) atomicOr(status, RB_DEV_ITERATION_LIMIT);
+				break;
+			}
+			umma::fenceAfterSync();
+			for (int l = 0; l < 5; ++l)
+			{
+				if (m == 0)
+				{
+					const uint32_t idesc = umma::idescBf16(t5::kRows, l < 4 ? 64u : 16u);
+					const unsigned char* bTile = t5::layerTile(base, l);
+					for (uint32_t kk = 0; kk < 4; ++kk)
+						umma::mma(tmem, umma::descK(act, kk), umma::descK(bTile, kk), idesc, kk > 0);
+					umma::commit(mmaBar);
+				}
+				ok = t5::namedAnd<1>(umma::barrierWait(mmaBar, mmaPhase, t5::kWaitLimit));
+				mmaPhase ^= 1u;
+				if (!ok) break;
+				umma::fenceAfterSync();
+				if (l == 4) break;
+				ws::reluRowHalves(tmem, act, m);
+				umma::fenceBeforeSync();
+				umma::fenceProxyAsync();
+				t5::namedSync<1>();
+			}
+			if (!ok)
+			{
+				if (m == 0) atomicOr(status, RB_DEV_ITERATION_LIMIT);
+				umma::barrierWait(mmaBar, mmaPhase ^ 1u, t5::kWaitLimit);
+				break;
+			}
+			uint32_t ro[16];
+			umma::tmemLoad16(umma::laneAddr(tmem, 0), ro);
+			umma::tmemWaitLoad();
+			umma::fenceBeforeSync();
+			t5::namedSync<1>();              // every lane read before the next tile's MMAs
+			if (m == 0) umma::barrierArrive(empty + s);
+			const uint32_t r = t * t5::kRows + m;
+			if (r < n)
+			{
+				const float4 y = make_float4(__uint_as_float(ro[0]), __uint_as_float(ro[1]), __uint_as_float(ro[2]),
+					__uint_as_float(ro[3]));
+				if (out) reinterpret_cast<float4*>(out)[r] = y;
+				if (path)
+				{
+					// as kMlpInferT: the prefix survives with 1 - q (q plus the
+					// class's drop correction), the radiance scaled by the
+					// measured ratio of targets to predictions
+					const uint32_t pr = path[r];
+					const uint32_t p = pr & 0x7FFFFFFFu;
+					const float4 tt = T[p];
+					const float qq = __uint_as_float(ro[4]) + (corr ? corr[((pr >> 31) ? kCorrDropLit : kCorrDropOther) + 2] : 0.0f);
+					const float keep = fminf(fmaxf(1.0f - qq, 0.0f), 1.0f);
+					const float sc = corr && corr[kCorrRadiance + 3] > 0.0f ? corr[kCorrRadiance + 2] : 1.0f;
+					float4 l = L[p];
+					l.x = l.x * keep + tt.x * (sc * fmaxf(y.x, 0.0f));
+					l.y = l.y * keep + tt.y * (sc * fmaxf(y.y, 0.0f));
+					l.z = l.z * keep + tt.z * (sc * fmaxf(y.z, 0.0f));
+					l.w = l.w * keep + tt.w * (sc * fmaxf(y.w, 0.0f));
+					L[p] = l;
+				}
+			}
+		}
+	}
+	umma::fenceBeforeSync();
+	__syncthreads();
+	if (warp == 0) umma::tmemFree(tmem, t5::kTmemCols);
+}
 
 // Training forward on the encoded rows X [n][64] (kMlpForward's contract):
 // out [n][kOutStride] f32 and the post-ReLU hidden rows acts [4][n][64] bf16.
@@ -998,7 +1229,7 @@ struct rb_nrc
 	uint32_t* status = nullptr;            // RB_DEV_* bits of the network's kernels
 	uint32_t step = 0;
 	int smCount = 148;
-	uint32_t inferBlocksPerSm = 1, forwardBlocksPerSm = 1, trainBlocksPerSm = 1;
+	uint32_t inferBlocksPerSm = 1, wsBlocksPerSm = 1, forwardBlocksPerSm = 1, trainBlocksPerSm = 1;
 };
 
 namespace
@@ -1038,13 +1269,13 @@ int growScratch(rb_nrc* h, uint32_t n)
 	return RB_OK;
 }
 
-// Resident blocks per SM of a 128-thread tcgen05 kernel, from the SM's
-// limits: shared memory (with the per-block reservation), registers (per
-// warp in units of 256), threads, and tensor memory (t5::kTmemCols columns
-// of 512 per block). The kernels loop over tiles, so the grid is this many
+// Resident blocks per SM of a tcgen05 kernel of `threads` threads that
+// allocates `tmemCols` TMEM columns, from the SM's limits: shared memory
+// (with the per-block reservation), registers (per warp in units of 256),
+// threads, and tensor memory (512 columns). The kernels loop over tiles, so the grid is this many
 // blocks per SM; a grid of one block per SM leaves the grid gathers with
 // 4 warps per SM to hide their latency.
-uint32_t residentTileBlocks(const void* fn, size_t dynSmem, int device, uint32_t groups)
+uint32_t residentTileBlocks(const void* fn, size_t dynSmem, int device, uint32_t threads, uint32_t tmemCols)
 {
 	int smemSm = 0, reserved = 0, regsSm = 0, threadsSm = 0;
 	cudaDeviceGetAttribute(&smemSm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
@@ -1056,9 +1287,9 @@ uint32_t residentTileBlocks(const void* fn, size_t dynSmem, int device, uint32_t
 	const size_t perBlockSmem = dynSmem + fa.sharedSizeBytes + static_cast<size_t>(reserved);
 	const uint32_t bySmem = static_cast<uint32_t>(static_cast<size_t>(smemSm) / perBlockSmem);
 	const uint32_t warpRegs = (static_cast<uint32_t>(fa.numRegs) * 32u + 255u) / 256u * 256u;
-	const uint32_t byRegs = warpRegs ? static_cast<uint32_t>(regsSm) / (4u * groups * warpRegs) : 32u;
-	const uint32_t byThreads = static_cast<uint32_t>(threadsSm) / (128u * groups);
-	const uint32_t byTmem = 512u / (t5::kTmemCols * groups);
+	const uint32_t byRegs = warpRegs ? static_cast<uint32_t>(regsSm) / ((threads / 32u) * warpRegs) : 32u;
+	const uint32_t byThreads = static_cast<uint32_t>(threadsSm) / threads;
+	const uint32_t byTmem = 512u / tmemCols;
 	const uint32_t b = std::min({ bySmem, byRegs, byThreads, byTmem });
 	return b < 1 ? 1u : b;
 }
@@ -1071,7 +1302,27 @@ int tileBlocks(const rb_nrc* h, uint32_t rows, uint32_t perSm, uint32_t groups)
 	const uint32_t cap = static_cast<uint32_t>(h->smCount) * perSm;
 	return static_cast<int>(tiles < 1 ? 1 : (tiles < cap ? tiles : cap));
 }
-int inferBlocks(const rb_nrc* h, uint32_t rows) { return tileBlocks(h, rows, h->inferBlocksPerSm, kInferGroups); }
+[[maybe_unused]] int inferBlocks(const rb_nrc* h, uint32_t rows)
+{
+	return tileBlocks(h, rows, h->inferBlocksPerSm, kInferGroups);
+}
+// Queries [0, min(*count, cap)) (count null: cap rows): outputs to `out`
+// and/or the cached-form update of L (path, T, corr).
+void launchInfer(const rb_nrc* h, uint32_t cap, const uint32_t* count, const float* in, float* out, const uint32_t* path,
+	float4* L, const float4* T, const float* corr, cudaStream_t st)
+{
+	const __half2* grid = reinterpret_cast<const __half2*>(h->grid);
+#if RB_INFER_WS
+	const uint32_t tiles = (cap + t5::kRows - 1) / t5::kRows;
+	const uint32_t most = static_cast<uint32_t>(h->smCount) * h->wsBlocksPerSm;
+	const int blocks = static_cast<int>(tiles < 1 ? 1 : (tiles < most ? tiles : most));
+	kMlpInferWS<<<blocks, ws::kThreads, ws::kSmem, st>>>(cap, count, in, grid, h->R, h->w, out, path, L, T, corr,
+		h->status);
+#else
+	kMlpInferT<kInferGroups><<<inferBlocks(h, cap), 128 * kInferGroups, kSmemInfer, st>>>(cap, count, in, grid, h->R,
+		h->w, out, path, L, T, corr, h->status);
+#endif
+}
 
 int encodeBlocks(uint32_t rows)
 {
@@ -1148,9 +1399,15 @@ int rb_nrc_create(const rb_nrc_config* config, rb_nrc** out)
 	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpBackwardT), cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(kSmemBackwardT));
 	h->inferBlocksPerSm = residentTileBlocks(reinterpret_cast<const void*>(kMlpInferT<kInferGroups>), kSmemInfer,
-		h->device, kInferGroups);
-	h->forwardBlocksPerSm = residentTileBlocks(reinterpret_cast<const void*>(kMlpForwardT), t5::kSmem, h->device, 1);
-	h->trainBlocksPerSm = residentTileBlocks(reinterpret_cast<const void*>(kMlpBackwardT), kSmemBackwardT, h->device, 1);
+		h->device, 128u * kInferGroups, t5::kTmemCols * kInferGroups);
+	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpInferWS), cudaFuncAttributeMaxDynamicSharedMemorySize,
+		static_cast<int>(ws::kSmem));
+	h->wsBlocksPerSm = residentTileBlocks(reinterpret_cast<const void*>(kMlpInferWS), ws::kSmem, h->device, ws::kThreads,
+		t5::kTmemCols);
+	h->forwardBlocksPerSm = residentTileBlocks(reinterpret_cast<const void*>(kMlpForwardT), t5::kSmem, h->device, 128u,
+		t5::kTmemCols);
+	h->trainBlocksPerSm = residentTileBlocks(reinterpret_cast<const void*>(kMlpBackwardT), kSmemBackwardT, h->device, 128u,
+		t5::kTmemCols);
 	*out = h;
 	return RB_OK;
 }
@@ -1216,9 +1473,7 @@ int rb_nrc_infer(rb_nrc* h, uint32_t n, const float* inputs, float* outputs, voi
 	if (n == 0) return RB_OK;
 	cudaSetDevice(h->device);
 	const cudaStream_t st = static_cast<cudaStream_t>(stream);
-	kMlpInferT<kInferGroups><<<inferBlocks(h, n), 128 * kInferGroups, kSmemInfer, st>>>(n, nullptr, inputs,
-		reinterpret_cast<const __half2*>(h->grid),
-		h->R, h->w, outputs, nullptr, nullptr, nullptr, nullptr, h->status);
+	launchInfer(h, n, nullptr, inputs, outputs, nullptr, nullptr, nullptr, nullptr, st);
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
 
@@ -1283,9 +1538,7 @@ int applyQueries(rb_nrc* h, uint32_t cap, const uint32_t* count, const float* in
 	const float4* T, const float* corr, cudaStream_t st)
 {
 	if (cap == 0) return RB_OK;
-	kMlpInferT<kInferGroups><<<inferBlocks(h, cap), 128 * kInferGroups, kSmemInfer, st>>>(cap, count, inputs,
-		reinterpret_cast<const __half2*>(h->grid),
-		h->R, h->w, nullptr, path, L, T, corr, h->status);
+	launchInfer(h, cap, count, inputs, nullptr, path, L, T, corr, st);
 	return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
 }
 

@@ -118,6 +118,14 @@ RB_D f3 sample3D(const Qrng& q, uint32_t dim)
 	return f3{ sobolBurley(idx, 0, seed ^ 0x9e78e391u), sobolBurley(idx, 1, seed ^ 0x67c33241u),
 	           sobolBurley(idx, 2, seed ^ 0x78c395c5u) };
 }
+// The third component of sample3D(q, dim) alone (the components are
+// independent, so this is bit-identical to sample3D(q, dim).z).
+RB_D float sample3DZ(const Qrng& q, uint32_t dim)
+{
+	const uint32_t seed = q.hash ^ dimHash(q.base + dim);
+	const uint32_t idx = owenReversed(__brev(q.sample), seed ^ 0xcaa726acu);
+	return sobolBurley(idx, 2, seed ^ 0x78c395c5u);
+}
 
 // ------------------------------------------------------------ wavelengths
 // Hero-wavelength sampling of the visible range with the atanh warp of

@@ -91,6 +91,11 @@ __device__ __forceinline__ void barrierInit(uint64_t* bar, uint32_t count)
 {
 	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smemAddr(bar)), "r"(count) : "memory");
 }
+// Arrives once on the mbarrier (release at CTA scope).
+__device__ __forceinline__ void barrierArrive(uint64_t* bar)
+{
+	asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" :: "r"(smemAddr(bar)) : "memory");
+}
 // Waits for the phase with the given parity to complete, at most `limit`
 // polls; false when it gave up.
 #ifndef RB_UMMA_SPIN_WAIT

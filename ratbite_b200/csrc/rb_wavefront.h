@@ -24,10 +24,12 @@ struct PathSoA
 	uint2* fd;         // flags, depth
 	float4* hit;       // closest hit: triangle (bits, -1 miss), t, b1, b2
 	// Surface records of the current bounce, and their light samples, are
-	// indexed by record (the position in surfQueue that kSurface took for
-	// the path), not by path slot: a warp's records are adjacent, so the
-	// shading kernels move them in whole sectors. surfQueue[record] is the
-	// path slot.
+	// indexed by record, not by path slot: kSurface takes a record in one of
+	// two regions by the record's light choice (tree picks from 0 up, the
+	// rest from queueCap - 1 down; see kRegionCounts), a warp's records of
+	// one region adjacent, so the shading kernels move them in whole sectors
+	// and each light-sample launch reads one region densely.
+	// surfQueue[record] is the path slot.
 	float4* shO;       // shadow ray origin, w: tmax
 	float4* shD;       // shadow ray direction
 	float4* shC;       // light sample spectrum, then the pending light-sample contribution
@@ -40,17 +42,19 @@ struct PathSoA
 	float4* sfL;       // the path's hero wavelengths (a copy of lambda)
 	uint32_t* queue[2];// active path slots, ping-pong by bounce parity
 	uint32_t* surfQueue;   // per record: its path slot
+	uint32_t* recOrder;    // records in order of arrival (both regions): the BxDF kernels take them in
+	                       // this order, which follows the paths' queue order, so the path state they
+	                       // read and write by slot, and the next queue they fill, keep that order
 	// emitter hits whose MIS weight needs the light-tree pdf (kEmission),
 	// indexed by queue position: path, (previous origin, BxDF pdf),
 	// (previous normal, area pdf), emitted spectrum, light index
-	uint32_t* neeQueue[2]; // records by light choice: tree picks, environment picks
 	uint32_t* emQueue;
 	float4* emA;
 	float4* emB;
 	float4* emC;
 	uint32_t* emLight;
 	uint32_t* shadowQueue;  // records whose shadow ray is traced
-	uint32_t* counts;  // kCountSlots words: see kShadowCounts, kSurfaceCounts
+	uint32_t* counts;  // kCountSlots words: see kShadowCounts, kRegionCounts
 	uint32_t capacity;
 	// jobs of a shared wavefront (rb_render_jobs; null for a single render):
 	// the job table, and per path its job and key (x | y << 16, sample index)
@@ -94,20 +98,21 @@ constexpr uint32_t kQueryRecordBit = 1u << 30;
 constexpr uint32_t kRecordPathMask = kQueryRecordBit - 1u;
 constexpr int kMaxBounces = 64;
 // counts[b]: paths entering bounce b; counts[kShadowCounts + b]: shadow rays
-// of bounce b; counts[kSurfaceCounts + b]: surface records of bounce b;
-// counts[kExtendFetch + b], counts[kShadowFetch + b]: work counters from
-// which the persistent traversal warps take their next rays;
+// of bounce b; counts[kExtendFetch + b], counts[kShadowFetch + b]: work
+// counters from which the persistent traversal warps take their next rays;
 // counts[kEmissionCounts + b]: deferred emission-MIS records of bounce b;
-// counts[kNeeTreeCounts + b], counts[kNeeSkyCounts + b]: light-sample records
-// by light choice; counts[kCacheQueryCount], counts[kTrainRecordCount]:
+// counts[kRegionCounts + 2 b], counts[kRegionCounts + 2 b + 1]: surface
+// records of bounce b in the tree-pick region (records 0 ..) and in the
+// other region (environment picks and skipped surfaces, records queueCap - 1
+// down), one 64-bit word per bounce that kSurface adds to with one atomic
+// per warp; counts[kCacheQueryCount], counts[kTrainRecordCount]:
 // radiance-cache queries and training records of the wave (all bounces).
 constexpr uint32_t kShadowCounts = kMaxBounces + 1;
-constexpr uint32_t kSurfaceCounts = 2 * (kMaxBounces + 1);
 constexpr uint32_t kExtendFetch = 3 * (kMaxBounces + 1);
 constexpr uint32_t kShadowFetch = 4 * (kMaxBounces + 1);
 constexpr uint32_t kEmissionCounts = 5 * (kMaxBounces + 1);
-constexpr uint32_t kNeeTreeCounts = 6 * (kMaxBounces + 1);
-constexpr uint32_t kNeeSkyCounts = 7 * (kMaxBounces + 1);
+constexpr uint32_t kRegionCounts = 6 * (kMaxBounces + 1);
+static_assert(kRegionCounts % 2 == 0, "64-bit region counters are 8-byte aligned");
 constexpr uint32_t kCacheQueryCount = 8 * (kMaxBounces + 1);
 constexpr uint32_t kTrainRecordCount = kCacheQueryCount + 1;
 constexpr uint32_t kCountSlots = kCacheQueryCount + 2;
@@ -158,7 +163,7 @@ struct WaveParams
 struct LaunchShape
 {
 	int smCount;
-	int blocksGenerate, blocksExtend, blocksSurface, blocksEmission, blocksNeePick, blocksNee, blocksBsdf, blocksBsdfLight, blocksShadow,
+	int blocksGenerate, blocksExtend, blocksSurface, blocksEmission, blocksNee, blocksBsdf, blocksBsdfLight, blocksShadow,
 		blocksResolve;
 	int threads;
 	uint32_t items;   // paths of the wave (0: no limit): grids are capped at the blocks those need
