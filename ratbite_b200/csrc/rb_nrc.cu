@@ -349,14 +349,8 @@ RB_D void rowWritten()
 	umma::fenceProxyAsync();
 	__syncthreads();
 }
-// Tile groups: a CTA of G x 128 threads runs G tiles side by side, group g
-// (threads 128 g ..) with its own activation tile, mbarrier and 64 TMEM
-// columns, all sharing one copy of the weights; a group synchronises on its
-// own named barrier (1 + g), so one group's gathers overlap another's MMAs
-// within the CTA, and more warps per SM fit than with one tile per CTA
-// (the weights are staged once per CTA).
-// Barrier ids are immediates (1 .. G), so the kernel reserves G + 1
-// barriers rather than all 16.
+// Named barrier among the 128 threads of one role (the ids are immediates,
+// so the kernel reserves only the barriers it uses), and its AND-reduction.
 template<int ID>
 RB_D void namedSync() { asm volatile("bar.sync %0, 128;" :: "n"(ID) : "memory"); }
 template<int ID>
@@ -371,282 +365,15 @@ RB_D bool namedAnd(bool p)
 		: "=r"(out) : "r"(p ? 1u : 0u), "n"(ID) : "memory");
 	return out != 0;
 }
-template<int G>
-RB_D void groupSync(uint32_t g)
-{
-	static_assert(G == 1 || G == 2 || G == 4, "1, 2 or 4 tile groups");
-	if (G == 1) { __syncthreads(); return; }
-	switch (g)
-	{
-	case 0: namedSync<1>(); break;
-	case 1: namedSync<2>(); break;
-	case 2: namedSync<3>(); break;
-	default: namedSync<4>(); break;
-	}
-}
-template<int G>
-RB_D bool groupAnd(uint32_t g, bool p)
-{
-	if (G == 1) return __syncthreads_and(p) != 0;
-	switch (g)
-	{
-	case 0: return namedAnd<1>(p);
-	case 1: return namedAnd<2>(p);
-	case 2: return namedAnd<3>(p);
-	default: return namedAnd<4>(p);
-	}
-}
-template<int G>
-constexpr uint32_t smemGroups() { return kOffAct + G * kRows * 128u + 16u * G + 16u + 1024u; }
-
-struct GroupCtx
-{
-	unsigned char* base;
-	unsigned char* act;
-	uint64_t* bar;
-	uint32_t tmemBase;    // the CTA's allocation
-	uint32_t tmem;        // this group's 64 columns
-	uint32_t phase;
-	uint32_t g;           // group index
-	uint32_t tig;         // thread index in the group
-};
-template<int G>
-RB_D GroupCtx beginGroups(unsigned char* smraw, const __nv_bfloat16* __restrict__ w)
-{
-	GroupCtx c;
-	c.base = alignBase(smraw);
-	c.g = threadIdx.x >> 7;
-	c.tig = threadIdx.x & 127u;
-	c.act = c.base + kOffAct + c.g * kRows * 128u;
-	uint64_t* bars = reinterpret_cast<uint64_t*>(c.base + kOffAct + G * kRows * 128u);
-	uint32_t* slot = reinterpret_cast<uint32_t*>(bars + G);
-	c.bar = bars + c.g;
-	if (threadIdx.x < static_cast<uint32_t>(G)) umma::barrierInit(bars + threadIdx.x, 1);
-	if ((threadIdx.x >> 5) == 0) umma::tmemAlloc(slot, kTmemCols * G);
-	stageLayers(w, c.base);
-	umma::fenceProxyAsync();
-	umma::fenceBeforeSync();
-	__syncthreads();
-	umma::fenceAfterSync();
-	c.tmemBase = *slot;
-	c.tmem = c.tmemBase + kTmemCols * c.g;
-	c.phase = 0;
-	return c;
-}
-template<int G>
-RB_D void endGroups(const GroupCtx& c)
-{
-	umma::fenceBeforeSync();
-	__syncthreads();
-	if ((threadIdx.x >> 5) == 0) umma::tmemFree(c.tmemBase, kTmemCols * G);
-}
-// layerMma for a group: the group's first thread issues, the group waits.
-template<int G>
-RB_D bool groupLayerMma(GroupCtx& c, const unsigned char* bTile, uint32_t n, int nK, uint32_t* status)
-{
-	if (c.tig == 0)
-	{
-		umma::fenceAfterSync();
-		const uint32_t idesc = umma::idescBf16(kRows, n);
-		for (int k = 0; k < nK; ++k)
-			umma::mma(c.tmem, umma::descK(c.act, static_cast<uint32_t>(k)), umma::descK(bTile, static_cast<uint32_t>(k)),
-				idesc, k > 0);
-		umma::commit(c.bar);
-	}
-	const bool ok = groupAnd<G>(c.g, umma::barrierWait(c.bar, c.phase, kWaitLimit));
-	c.phase ^= 1u;
-	if (!ok)
-	{
-		if (c.tig == 0) atomicOr(status, RB_DEV_ITERATION_LIMIT);
-		umma::barrierWait(c.bar, c.phase ^ 1u, kWaitLimit);
-		return false;
-	}
-	umma::fenceAfterSync();
-	return true;
-}
-RB_D void groupReadAcc64(const GroupCtx& c, float (&v)[64])
-{
-	uint32_t r[4][16];
-#pragma unroll
-	for (int q = 0; q < 4; ++q) umma::tmemLoad16(umma::laneAddr(c.tmem, 16u * q), r[q]);
-	umma::tmemWaitLoad();
-#pragma unroll
-	for (int q = 0; q < 4; ++q)
-#pragma unroll
-		for (int j = 0; j < 16; ++j) v[16 * q + j] = __uint_as_float(r[q][j]);
-}
-RB_D void groupReadAcc16(const GroupCtx& c, float (&v)[16])
-{
-	uint32_t r[16];
-	umma::tmemLoad16(umma::laneAddr(c.tmem, 0), r);
-	umma::tmemWaitLoad();
-#pragma unroll
-	for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
-}
-template<int G>
-RB_D void groupRowWritten(uint32_t g)
-{
-	umma::fenceBeforeSync();
-	umma::fenceProxyAsync();
-	groupSync<G>(g);
-}
 
 RB_D void reluPack(const float (&v)[64], uint32_t (&row)[32])
 {
 #pragma unroll
 	for (int j = 0; j < 32; ++j) row[j] = pack2(fmaxf(v[2 * j], 0.0f), fmaxf(v[2 * j + 1], 0.0f));
 }
-RB_D void encodeRow(uint32_t r, uint32_t n, const float* __restrict__ in, const __half2* __restrict__ grid,
-	const Resolutions& R, uint32_t (&row)[32])
-{
-	if (r >= n)
-	{
-#pragma unroll
-		for (int j = 0; j < 32; ++j) row[j] = 0u;
-		return;
-	}
-	const float* v = in + static_cast<size_t>(kNrcInputs) * r;
-	const float px = clamp01(v[0]), py = clamp01(v[1]), pz = clamp01(v[2]);
-#pragma unroll
-	for (int l = 0; l < kLevels; ++l)
-	{
-		float f0, f1;
-		levelFeatures(R, grid, l, px, py, pz, f0, f1);
-		row[l] = pack2(f0, f1);
-	}
-#pragma unroll
-	for (int k = 0; k < 32; k += 2) row[16 + k / 2] = pack2(restColumn(v, k), restColumn(v, k + 1));
-}
-// The tile's encoded rows, spread over the warp: warp w encodes rows
-// 32 w .. 32 w + 31; lane l takes the (row, level) pairs l, l + 32, ...
-// (16 per lane, their 8 corner gathers independent of each other), then the
-// 32 remaining columns of row 32 w + l. Each feature pair is one 32-bit
-// word of the swizzled tile. RB_INFER_ROW_ENCODE=1 (the default) encodes
-// one row per thread instead (encodeRow). On B200, cached Cornell frame
-// 1920x1080x64 (inference ms per frame): row 14.3, warp-distributed 14.9 at
-// one tile per block (4 blocks per SM); with 2 tile groups 15.1 / 14.9,
-// with 4 (64 registers) 16.1.
-#ifndef RB_INFER_ROW_ENCODE
-#define RB_INFER_ROW_ENCODE 1
-#endif
-RB_D void encodeTile(uint32_t r0, uint32_t n, const float* __restrict__ in, const __half2* __restrict__ grid,
-	const Resolutions& R, unsigned char* tile)
-{
-	const uint32_t warp = (threadIdx.x >> 5) & 3u, lane = threadIdx.x & 31u;
-#pragma unroll 4
-	for (uint32_t k = lane; k < 32u * kLevels; k += 32u)
-	{
-		const uint32_t rl = 32u * warp + (k >> 4), l = k & 15u, r = r0 + rl;
-		float f0 = 0.0f, f1 = 0.0f;
-		if (r < n)
-		{
-			const float* v = in + static_cast<size_t>(kNrcInputs) * r;
-			levelFeatures(R, grid, static_cast<int>(l), clamp01(v[0]), clamp01(v[1]), clamp01(v[2]), f0, f1);
-		}
-		*reinterpret_cast<uint32_t*>(tile + umma::swzOffset(rl, 2u * l)) = pack2(f0, f1);
-	}
-	const uint32_t rl = 32u * warp + lane, r = r0 + rl;
-	const float* v = in + static_cast<size_t>(kNrcInputs) * r;
-	uint32_t rest[16];
-#pragma unroll
-	for (int k = 0; k < 32; k += 2)
-		rest[k / 2] = r < n ? pack2(restColumn(v, k), restColumn(v, k + 1)) : 0u;
-#pragma unroll
-	for (uint32_t c = 0; c < 4; ++c)
-		*reinterpret_cast<uint4*>(tile + rl * 128u + ((((4u + c) ^ rl) & 7u) << 4)) =
-			make_uint4(rest[4 * c], rest[4 * c + 1], rest[4 * c + 2], rest[4 * c + 3]);
-}
 } // namespace t5
 
-// Inference with the encoding fused in (kMlpInfer's contract, on tcgen05),
-// G tiles per CTA (tile groups).
-#ifndef RB_INFER_GROUPS
-#define RB_INFER_GROUPS 1
-#endif
-constexpr int kInferGroups = RB_INFER_GROUPS;
-// Resident blocks the register allocation is capped for: 4 warps x G per
-// block, 16 tile warps per SM at G = 1 (shared memory allows 4 blocks), 24
-// at G = 2 (3 blocks), 32 at G = 4 (2 blocks).
-template<int G>
-constexpr int inferMinBlocks() { return G == 1 ? 4 : (G == 2 ? 3 : 2); }
-template<int G>
-__global__ void __launch_bounds__(128 * G, inferMinBlocks<G>()) kMlpInferT(uint32_t cap, const uint32_t* __restrict__ count,
-	const float* __restrict__ in, const __half2* __restrict__ grid, Resolutions R, const __nv_bfloat16* __restrict__ w,
-	float* __restrict__ out, const uint32_t* __restrict__ path, float4* __restrict__ L, const float4* __restrict__ T,
-	const float* __restrict__ corr, uint32_t* __restrict__ status)
-{
-	extern __shared__ unsigned char smraw[];
-	t5::GroupCtx c = t5::beginGroups<G>(smraw, w);
-	const uint32_t n = count ? min(*count, cap) : cap;
-	bool ok = true;
-	for (uint32_t r0 = (blockIdx.x * G + c.g) * t5::kRows; r0 < n && ok; r0 += gridDim.x * G * t5::kRows)
-	{
-		const uint32_t r = r0 + c.tig;
-#if RB_INFER_ROW_ENCODE
-		{
-			uint32_t row[32];
-			t5::encodeRow(r, n, in, grid, R, row);
-			umma::storeRow(c.act, c.tig, row);
-		}
-#else
-		t5::encodeTile(r0, n, in, grid, R, c.act);
-#endif
-		umma::fenceProxyAsync();
-		t5::groupSync<G>(c.g);
-		for (int l = 0; l < 4 && ok; ++l)
-		{
-			ok = t5::groupLayerMma<G>(c, t5::layerTile(c.base, l), 64, 4, status);
-			if (!ok) break;
-			float v[64];
-			t5::groupReadAcc64(c, v);
-			uint32_t row[32];
-			t5::reluPack(v, row);
-			umma::storeRow(c.act, c.tig, row);
-			t5::groupRowWritten<G>(c.g);
-		}
-		if (!ok) break;
-		ok = t5::groupLayerMma<G>(c, t5::layerTile(c.base, 4), 16, 4, status);
-		if (!ok) break;
-		float o[16];
-		t5::groupReadAcc16(c, o);
-		if (r < n)
-		{
-			const float4 y = make_float4(o[0], o[1], o[2], o[3]);
-			if (out) reinterpret_cast<float4*>(out)[r] = y;
-			if (path)
-			{
-				// the plain estimator drops a whole sample whose later BxDF
-				// sample fails: the prefix survives with 1 - q, q plus the
-				// correction measured on the path's class (the path index's
-				// high bit: the camera ray hit an emitter); the radiance is
-				// scaled by the measured ratio of targets to predictions
-				const uint32_t pr = path[r];
-				const uint32_t p = pr & 0x7FFFFFFFu;
-				const float4 t = T[p];
-				const float qq = o[4] + (corr ? corr[((pr >> 31) ? kCorrDropLit : kCorrDropOther) + 2] : 0.0f);
-				const float keep = fminf(fmaxf(1.0f - qq, 0.0f), 1.0f);
-				const float sc = corr && corr[kCorrRadiance + 3] > 0.0f ? corr[kCorrRadiance + 2] : 1.0f;
-				float4 l = L[p];
-				l.x = l.x * keep + t.x * (sc * fmaxf(y.x, 0.0f));
-				l.y = l.y * keep + t.y * (sc * fmaxf(y.y, 0.0f));
-				l.z = l.z * keep + t.z * (sc * fmaxf(y.z, 0.0f));
-				l.w = l.w * keep + t.w * (sc * fmaxf(y.w, 0.0f));
-				L[p] = l;
-			}
-		}
-		umma::fenceBeforeSync();
-		t5::groupSync<G>(c.g);
-	}
-	t5::endGroups<G>(c);
-}
-constexpr uint32_t kSmemInfer = t5::smemGroups<kInferGroups>();
-// RB_INFER_WS=1 (the default) answers queries with the warp-specialized
-// kernel (kMlpInferWS); 0 with kMlpInferT<RB_INFER_GROUPS>.
-#ifndef RB_INFER_WS
-#define RB_INFER_WS 1
-#endif
-
-// Inference, warp-specialized (the default for queries): 8 encoder warps
+// Inference (the query path), warp-specialized: 8 encoder warps
 // fill a ring of activation tiles with encoded rows (two threads per row,
 // 8 grid levels each), 4 MLP warps run the five tcgen05 layers on each
 // filled tile and apply the output. mbarriers pass the tiles (full: one
@@ -657,30 +384,49 @@ constexpr uint32_t kSmemInfer = t5::smemGroups<kInferGroups>();
 // its role stops; the other role's waits then give up too.
 namespace ws
 {
-// Encoder warps per block (8 or 12 or 16). On B200, cached Cornell frame
-// 1920x1080x64 (inference ms per frame): 8 encoder warps 14.9 - 16.5 for
-// every encoder layout and unroll tried (one level per thread, half a row
-// per thread; 2 / 4 / 8 rows in flight), the same as one tile per 128-thread
-// block (14.3): the MLP side alone takes 2.6 ms, the gathers the rest, so
-// what moves it is the number of warps gathering per SM.
+// Shape of the kernel, measured on B200 (cached Cornell frame 1920x1080x64,
+// inference ms per frame). The grid gathers decide it: without the MLP the
+// encoders alone took the whole time, and they depend on L1 hits (nearby
+// queries share cells; loading the hashed levels without allocating in L1
+// made it 41 ms). Shared memory the blocks take is carved out of the SM's
+// 256 KB of L1, so the ring is short: 2 stages x 2 blocks 7.4 ms (164 KB
+// carve-out config, about 90 KB of L1); 3 stages 8.3; 4 stages 14.5 (228 KB,
+// about 28 KB of L1); one block of 16 encoder warps with 2 / 4 stages 8.2 /
+// 8.4. At 4 stages, 12 or 16 encoder warps per block (64 / 48 registers) or
+// 16-32 gathers issued together per thread were slower (16.3 - 20.5), and
+// the encoder layout (one level per thread, half a row per thread, rows
+// consecutive or strided per warp) moved it by less than 2 ms.
 #ifndef RB_WS_ENC_WARPS
-#define RB_WS_ENC_WARPS 12
+#define RB_WS_ENC_WARPS 8
 #endif
 constexpr uint32_t kEncWarps = RB_WS_ENC_WARPS, kMlpWarps = 4;
 constexpr uint32_t kEncThreads = 32u * kEncWarps;
 constexpr uint32_t kThreads = kEncThreads + 32u * kMlpWarps;
-constexpr uint32_t kStages = 4;
+#ifndef RB_WS_STAGES
+#define RB_WS_STAGES 2
+#endif
+constexpr uint32_t kStages = RB_WS_STAGES;
 constexpr uint32_t kTileBytes = t5::kRows * 128u;
 constexpr uint32_t kOffStages = t5::kOffAct;
 constexpr uint32_t kOffBars = kOffStages + kStages * kTileBytes;  // full[kStages], empty[kStages], mma, TMEM slot
 constexpr uint32_t kSmem = kOffBars + 8u * (2u * kStages + 1u) + 8u + 1024u;
-constexpr int kMinBlocks = 2;
+// Blocks per SM the kernel is compiled and launched for. Shared memory the
+// blocks do not take is L1, which the grid gathers depend on.
+#ifndef RB_WS_CTAS
+#define RB_WS_CTAS 2
+#endif
+constexpr int kMinBlocks = RB_WS_CTAS;
 static_assert(kOffStages % 1024 == 0 && kTileBytes % 1024 == 0, "operand tiles start on 1024-byte boundaries");
 static_assert(kEncThreads % 16u == 0 && kEncThreads >= 256u, "whole levels per thread; the remaining columns in one pass");
 #ifndef RB_WS_ENCODE_UNROLL
-#define RB_WS_ENCODE_UNROLL 2
+#define RB_WS_ENCODE_UNROLL 8
 #endif
 constexpr int kWsEncodeUnroll = RB_WS_ENCODE_UNROLL;
+// Rows of an encoder warp: 1, 16 consecutive rows per warp; 0, rows strided
+// over the tile.
+#ifndef RB_WS_ENCODE_MAP
+#define RB_WS_ENCODE_MAP 1
+#endif
 
 // Encoder thread e keeps one grid level, l = e % 16, and encodes it for rows
 // e / 16, e / 16 + kEncThreads / 16, ... of the tile, so a warp's gathers at
@@ -691,6 +437,26 @@ RB_D void encodeLevels(uint32_t t0, uint32_t n, const float* __restrict__ in, co
 	const Resolutions& R, unsigned char* tile)
 {
 	const uint32_t e = threadIdx.x, l = e & 15u;
+#if RB_WS_ENCODE_MAP
+	// warp w takes rows W w .. W w + W - 1, W = 128 / encoder warps
+	// (consecutive queries, nearby pixels): lane k gathers level k % 16 of
+	// rows W w + k / 16 + 2 i
+	constexpr uint32_t kWarpRows = t5::kRows / kEncWarps;
+	static_assert(t5::kRows % kEncWarps == 0 && kWarpRows % 2 == 0, "whole row pairs per encoder warp");
+	const uint32_t base = kWarpRows * (e >> 5) + ((e >> 4) & 1u);
+#pragma unroll kWsEncodeUnroll
+	for (uint32_t i = 0; i < kWarpRows / 2; ++i)
+	{
+		const uint32_t rl = base + 2u * i, r = t0 + rl;
+		float f0 = 0.0f, f1 = 0.0f;
+		if (r < n)
+		{
+			const float* v = in + static_cast<size_t>(kNrcInputs) * r;
+			levelFeatures(R, grid, static_cast<int>(l), clamp01(v[0]), clamp01(v[1]), clamp01(v[2]), f0, f1);
+		}
+		*reinterpret_cast<uint32_t*>(tile + umma::swzOffset(rl, 2u * l)) = pack2(f0, f1);
+	}
+#else
 #pragma unroll kWsEncodeUnroll
 	for (uint32_t rl = e >> 4; rl < t5::kRows; rl += kEncThreads / 16u)
 	{
@@ -703,6 +469,7 @@ RB_D void encodeLevels(uint32_t t0, uint32_t n, const float* __restrict__ in, co
 		}
 		*reinterpret_cast<uint32_t*>(tile + umma::swzOffset(rl, 2u * l)) = pack2(f0, f1);
 	}
+#endif
 	if (e >= 2u * t5::kRows) return;
 	const uint32_t rl = e >> 1, r = t0 + rl, k0 = 16u * (e & 1u);
 	const float* v = in + static_cast<size_t>(kNrcInputs) * r;
@@ -848,9 +615,11 @@ __global__ void __launch_bounds__(ws::kThreads, ws::kMinBlocks) kMlpInferWS(uint
 				if (out) reinterpret_cast<float4*>(out)[r] = y;
 				if (path)
 				{
-					// as kMlpInferT: the prefix survives with 1 - q (q plus the
-					// class's drop correction), the radiance scaled by the
-					// measured ratio of targets to predictions
+					// the plain estimator drops a whole sample whose later BxDF
+					// sample fails: the prefix survives with 1 - q, q plus the
+					// correction measured on the path's class (the path index's
+					// high bit: the camera ray hit an emitter); the radiance is
+					// scaled by the measured ratio of targets to predictions
 					const uint32_t pr = path[r];
 					const uint32_t p = pr & 0x7FFFFFFFu;
 					const float4 tt = T[p];
@@ -1229,7 +998,7 @@ struct rb_nrc
 	uint32_t* status = nullptr;            // RB_DEV_* bits of the network's kernels
 	uint32_t step = 0;
 	int smCount = 148;
-	uint32_t inferBlocksPerSm = 1, wsBlocksPerSm = 1, forwardBlocksPerSm = 1, trainBlocksPerSm = 1;
+	uint32_t wsBlocksPerSm = 1, forwardBlocksPerSm = 1, trainBlocksPerSm = 1;
 };
 
 namespace
@@ -1296,15 +1065,11 @@ uint32_t residentTileBlocks(const void* fn, size_t dynSmem, int device, uint32_t
 
 // Blocks of the tcgen05 kernels: one 128-row tile per block and step, at
 // most perSm resident blocks per SM (the kernels loop over tiles).
-int tileBlocks(const rb_nrc* h, uint32_t rows, uint32_t perSm, uint32_t groups)
+int tileBlocks(const rb_nrc* h, uint32_t rows, uint32_t perSm)
 {
-	const uint32_t tiles = (rows + t5::kRows * groups - 1) / (t5::kRows * groups);
+	const uint32_t tiles = (rows + t5::kRows - 1) / t5::kRows;
 	const uint32_t cap = static_cast<uint32_t>(h->smCount) * perSm;
 	return static_cast<int>(tiles < 1 ? 1 : (tiles < cap ? tiles : cap));
-}
-[[maybe_unused]] int inferBlocks(const rb_nrc* h, uint32_t rows)
-{
-	return tileBlocks(h, rows, h->inferBlocksPerSm, kInferGroups);
 }
 // Queries [0, min(*count, cap)) (count null: cap rows): outputs to `out`
 // and/or the cached-form update of L (path, T, corr).
@@ -1312,16 +1077,11 @@ void launchInfer(const rb_nrc* h, uint32_t cap, const uint32_t* count, const flo
 	float4* L, const float4* T, const float* corr, cudaStream_t st)
 {
 	const __half2* grid = reinterpret_cast<const __half2*>(h->grid);
-#if RB_INFER_WS
 	const uint32_t tiles = (cap + t5::kRows - 1) / t5::kRows;
 	const uint32_t most = static_cast<uint32_t>(h->smCount) * h->wsBlocksPerSm;
 	const int blocks = static_cast<int>(tiles < 1 ? 1 : (tiles < most ? tiles : most));
 	kMlpInferWS<<<blocks, ws::kThreads, ws::kSmem, st>>>(cap, count, in, grid, h->R, h->w, out, path, L, T, corr,
 		h->status);
-#else
-	kMlpInferT<kInferGroups><<<inferBlocks(h, cap), 128 * kInferGroups, kSmemInfer, st>>>(cap, count, in, grid, h->R,
-		h->w, out, path, L, T, corr, h->status);
-#endif
 }
 
 int encodeBlocks(uint32_t rows)
@@ -1392,18 +1152,17 @@ int rb_nrc_create(const rb_nrc_config* config, rb_nrc** out)
 	std::memcpy(w.data() + wOffset(4), wo.data(), sizeof(float) * wo.size());
 	const int rc = rb_nrc_set_parameters(h, g.data(), w.data());
 	if (rc != RB_OK) { rb_nrc_destroy(h); return rc; }
-	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpInferT<kInferGroups>), cudaFuncAttributeMaxDynamicSharedMemorySize,
-		static_cast<int>(kSmemInfer));
 	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpForwardT), cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(t5::kSmem));
 	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpBackwardT), cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(kSmemBackwardT));
-	h->inferBlocksPerSm = residentTileBlocks(reinterpret_cast<const void*>(kMlpInferT<kInferGroups>), kSmemInfer,
-		h->device, 128u * kInferGroups, t5::kTmemCols * kInferGroups);
 	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpInferWS), cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(ws::kSmem));
-	h->wsBlocksPerSm = residentTileBlocks(reinterpret_cast<const void*>(kMlpInferWS), ws::kSmem, h->device, ws::kThreads,
-		t5::kTmemCols);
+	h->wsBlocksPerSm = std::min<uint32_t>(static_cast<uint32_t>(ws::kMinBlocks),
+		residentTileBlocks(reinterpret_cast<const void*>(kMlpInferWS), ws::kSmem, h->device, ws::kThreads, t5::kTmemCols));
+	// shared memory for exactly that many blocks, the rest of the SM's 256 KB as L1
+	cudaFuncSetAttribute(reinterpret_cast<const void*>(kMlpInferWS), cudaFuncAttributePreferredSharedMemoryCarveout,
+		static_cast<int>(std::min<uint32_t>(100u, (h->wsBlocksPerSm * (ws::kSmem + 1024u) * 100u + 233471u) / 233472u)));
 	h->forwardBlocksPerSm = residentTileBlocks(reinterpret_cast<const void*>(kMlpForwardT), t5::kSmem, h->device, 128u,
 		t5::kTmemCols);
 	h->trainBlocksPerSm = residentTileBlocks(reinterpret_cast<const void*>(kMlpBackwardT), kSmemBackwardT, h->device, 128u,
@@ -1488,10 +1247,10 @@ int computeGradients(rb_nrc* h, uint32_t n, const float* inputs, const float* ta
 	if (rc != RB_OK) return rc;
 	cudaMemsetAsync(h->loss, 0, sizeof(float), st);
 	kEncode<<<encodeBlocks(n), kThreads, 0, st>>>(n, inputs, reinterpret_cast<const __half2*>(h->grid), h->R, h->X);
-	kMlpForwardT<<<tileBlocks(h, n, h->forwardBlocksPerSm, 1), 128, t5::kSmem, st>>>(n, h->X, h->w, h->out, h->acts,
+	kMlpForwardT<<<tileBlocks(h, n, h->forwardBlocksPerSm), 128, t5::kSmem, st>>>(n, h->X, h->w, h->out, h->acts,
 		h->status);
 	kLoss<<<gridFor(n), kThreads, 0, st>>>(n, h->out, targets, h->dY, h->loss, valid, outs, tStride, corr);
-	kMlpBackwardT<<<tileBlocks(h, n, h->trainBlocksPerSm, 1), 128, kSmemBackwardT, st>>>(n, h->dY, h->wt, h->acts, h->dH,
+	kMlpBackwardT<<<tileBlocks(h, n, h->trainBlocksPerSm), 128, kSmemBackwardT, st>>>(n, h->dY, h->wt, h->acts, h->dH,
 		h->dX0, h->status);
 	// weight gradients of the five layers, one launch
 	kWeightGrad<<<5 * ((n + kWgRows - 1) / kWgRows), 128, 0, st>>>(n, h->X, h->acts, h->dY, h->dH, h->wGrad);
