@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define RB_ABI_VERSION 3
+#define RB_ABI_VERSION 4
 
 /* Status codes. */
 #define RB_OK                  0
@@ -71,6 +71,29 @@ extern "C" {
 #define RB_FACTOR_SHEEN_COLOR  (1u << 6)
 #define RB_FACTOR_SHEEN_ROUGH  (1u << 7)
 #define RB_FACTOR_EMISSION     (1u << 8)
+/* rb_material.textures bits and texture slots (MaterialData::TextureTypeBitfield,
+ * src/core/material.h:30-41): bit t set = texture_index[t] is used. */
+#define RB_TEXTURE_BASE_COLOR   0u
+#define RB_TEXTURE_NORMAL       1u
+#define RB_TEXTURE_MET_ROUGH    2u
+#define RB_TEXTURE_TRANSMISSION 3u
+#define RB_TEXTURE_SHEEN_COLOR  4u
+#define RB_TEXTURE_SHEEN_ROUGH  5u
+#define RB_TEXTURE_EMISSION     6u
+#define RB_TEXTURE_SLOTS        7u
+/* rb_texture.format: 8-bit channels read as normalized floats (the
+ * reference's R8_UNORM / R8G8B8A8_UNORM images, cudaReadModeNormalizedFloat),
+ * with the sRGB curve applied per texel before filtering when `srgb` is set
+ * (texDesc.sRGB, set for base-colour textures; src/core/texture.h:245-265). */
+#define RB_TEXFMT_R8     0u
+#define RB_TEXFMT_RGBA8  1u
+/* rb_texture.address_u / address_v (TextureAddress, src/core/texture.h:33-38) */
+#define RB_TEXADDR_WRAP   0u
+#define RB_TEXADDR_CLAMP  1u
+#define RB_TEXADDR_MIRROR 2u
+/* rb_texture.filter (TextureFilter) */
+#define RB_TEXFILTER_NEAREST 0u
+#define RB_TEXFILTER_LINEAR  1u
 
 #define RB_SPECTRUM_BINS 471   /* 360..830 nm, src/core/spectral_settings.h:5-9 */
 #define RB_LUT_SIZE 32         /* LUT edge, src/core/rendering_interface.cpp:530-533 */
@@ -109,10 +132,10 @@ typedef struct rb_config {
 
 /*
  * One material record: MaterialData (src/core/material.h:17-107) field for
- * field, minus OptiX and texture-object specifics. Textures are outside this
- * build's scope: `textures` must be 0. The index and attribute buffers are the
- * per-submesh vertex data the shading step reads
- * (src/kernels/pathtrace.cu:1290-1431); they are copied at upload.
+ * field, minus OptiX specifics; texture objects are indices into the table
+ * of rb_set_textures. The index and attribute buffers are the per-submesh
+ * vertex data the shading step reads (src/kernels/pathtrace.cu:1290-1431);
+ * they are copied at upload.
  */
 typedef struct rb_material {
     uint32_t bxdf;               /* RB_BXDF_* (bxdfIndexSBT) */
@@ -128,7 +151,7 @@ typedef struct rb_material {
     float mf_roughness;          /* mfRoughnessValue */
     float ior;
     float alpha_cutoff;
-    uint32_t textures;           /* must be 0 */
+    uint32_t textures;           /* bit RB_TEXTURE_*: that slot of texture_index is sampled */
     uint32_t factors;            /* RB_FACTOR_* bits */
     float base_color[4];
     float metalness;
@@ -141,7 +164,24 @@ typedef struct rb_material {
     const void* indices;         /* triangle_count * 3 indices of index_type */
     uint32_t vertex_count;       /* vertices in attribute_data */
     const void* attribute_data;  /* vertex_count * attribute_stride bytes, or NULL */
+    uint32_t texcoord_sets;      /* bit RB_TEXTURE_*: that texture reads texture coordinate set 2
+                                  * (the *TexCoordSetIndex flags) */
+    uint32_t texture_index[RB_TEXTURE_SLOTS];  /* per slot, an index into the rb_set_textures table */
 } rb_material;
+
+/* One texture of the rb_set_textures table (an image with its sampler:
+ * CudaCombinedTexture, src/core/texture.h:280-380). Texels are width x
+ * height, row-major from the first row of the image, 1 (RB_TEXFMT_R8) or 4
+ * bytes each; normalized coordinates, texel centres at (i + 0.5) / width. */
+typedef struct rb_texture {
+    uint32_t width, height;
+    uint32_t format;             /* RB_TEXFMT_* */
+    uint32_t srgb;               /* 1: the sRGB curve decodes r, g, b (r of an R8 texture) */
+    uint32_t address_u, address_v;  /* RB_TEXADDR_* */
+    uint32_t filter;             /* RB_TEXFILTER_* */
+    uint32_t reserved;
+    const void* data;            /* copied at upload */
+} rb_texture;
 
 /* Geometry: meshes of submeshes, placed by instances (SceneData::Mesh /
  * Submesh / Instance, src/core/scene.h:85-152). */
@@ -241,6 +281,10 @@ int rb_set_luts(rb_ctx* ctx, const float* conductor_albedo,
 int rb_set_spectra(rb_ctx* ctx, const float* sensor_xyz, const float* basis_rgb,
                    const float* extra, uint32_t n_extra);
 int rb_set_materials(rb_ctx* ctx, const rb_material* materials, uint32_t count);
+/* The texture table materials index (replaces the images and textures of
+ * fillModelMaterials, src/core/rendering_interface.cpp:46-66). Set it before
+ * the materials that use it; materials are checked against it. */
+int rb_set_textures(rb_ctx* ctx, const rb_texture* textures, uint32_t count);
 /* Replaces buildGeometryAccelerationStructures (:733), buildLightAccelerationStructure
  * (:849) and updateInstanceAccelerationStructure (:943): builds the wide BVH. */
 int rb_set_geometry(rb_ctx* ctx, const rb_geometry* geometry);
@@ -262,14 +306,16 @@ int rb_update_instances(rb_ctx* ctx, const float* instance_transforms, const flo
 int rb_set_lights(rb_ctx* ctx, const rb_light_tree* tree);
 /* Builds the light tree on the device from emissive triangles in device
  * memory (world: 9 floats each, flux, material, primitive; the inputs
- * rb_build_light_tree takes, origin-independent) and installs it as
+ * rb_build_light_tree takes, origin-independent; uvs: 6 floats each, the
+ * emission texture's coordinates at the triangle's vertices, or NULL when no
+ * emitter has an emission texture) and installs it as
  * rb_set_lights installs host-built records, the light origin of
  * rb_set_light_origin applied. No reference counterpart: the reference
  * rebuilds on the host (LightTree::Builder, src/core/light_tree.cpp:47-418)
  * on every light change. The tree is a binned-SAOH tree in the reference's
  * layouts (rb_k_build_light_tree). Synchronizes. */
 int rb_build_lights(rb_ctx* ctx, uint32_t n, const float* world, const float* flux, const uint32_t* material,
-                    const uint32_t* primitive, void* stream);
+                    const uint32_t* primitive, const float* uvs, void* stream);
 /* The camera-move refresh of the light data on the device (the reference's
  * fillLightDataBuffer and fillLightTreeDataBuffers,
  * src/core/rendering_interface.cpp:1433-1510, run on CHANGE_CAMERA_POS

@@ -150,7 +150,9 @@ int rb_envmap_cdf_noalloc(uint32_t width, uint32_t height, const float* rgba, in
  * src/core/light_tree.cpp:47-418, which rb_build_light_tree restates). Same
  * inputs and output layouts as rb_build_light_tree, all in device memory
  * except `camera` (host, 3 doubles): world (9 floats per emissive triangle),
- * flux, material and primitive per triangle; outputs triangles (68-byte
+ * flux, material and primitive per triangle, uvs (6 floats per triangle: the
+ * emission texture's coordinates at its vertices, copied into the records;
+ * NULL for zeros); outputs triangles (68-byte
  * EmissiveTriangleLightData, camera-relative), nodes (at most 2n - 1 32-byte
  * PackedNode), pointers (n), bitmasks (n) and *node_count (device). The tree
  * is a binned-SAOH tree in the reference's layouts, not a byte copy of the
@@ -158,7 +160,8 @@ int rb_envmap_cdf_noalloc(uint32_t width, uint32_t height, const float* rgba, in
  * device memory (contents on entry do not matter). Stream-ordered. */
 size_t rb_k_build_light_tree_scratch_bytes(uint32_t n);
 int rb_k_build_light_tree(uint32_t n, const float* world, const float* flux, const uint32_t* material,
-                          const uint32_t* primitive, const double* camera, void* scratch, void* triangles,
+                          const uint32_t* primitive, const float* uvs, const double* camera, void* scratch,
+                          void* triangles,
                           void* nodes, uint32_t* pointers, uint64_t* bitmasks, uint32_t* node_count, void* stream);
 
 /* Regenerates the multiple-scattering compensation tables (no counterpart in

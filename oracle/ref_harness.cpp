@@ -69,6 +69,7 @@ namespace
 
 	std::vector<MaterialData> g_materials;
 	std::vector<std::vector<uint8_t>> g_materialBuffers;
+	std::vector<cudaTextureObject_t> g_materialTextures;   // rb_set_textures index -> registry handle
 
 	struct TriRecord
 	{
@@ -190,6 +191,7 @@ int rbref_abi_version() { return RB_ABI_VERSION; }
 void rbref_reset()
 {
 	g_textures.clear();
+	g_materialTextures.clear();
 	g_materials.clear();
 	g_materialBuffers.clear();
 	g_tris.clear();
@@ -262,6 +264,52 @@ int rbref_set_luts(const float* conductor, const float* dielOuter, const float* 
 	return RB_OK;
 }
 
+// Material textures (the product's rb_set_textures table): texels decoded
+// to floats as the texture hardware reads them (8-bit / 255; the sRGB curve
+// for r, g, b of sRGB textures, r of a one-channel one, IEC 61966-2-1 in
+// double precision), a
+// one-channel texture stored as (r, 0, 0, 1); handles registered for
+// rbref_set_materials to use. Call after rbref_set_luts.
+int rbref_set_textures(const rb_texture* tex, uint32_t count)
+{
+	g_materialTextures.clear();
+	float lut[256];
+	for (int c = 0; c < 256; ++c)
+	{
+		const double x = c / 255.0;
+		lut[c] = static_cast<float>(x <= 0.04045 ? x / 12.92 : std::pow((x + 0.055) / 1.055, 2.4));
+	}
+	for (uint32_t i = 0; i < count; ++i)
+	{
+		const rb_texture& t = tex[i];
+		if (t.format > RB_TEXFMT_RGBA8 || !t.data || t.width == 0 || t.height == 0) return RB_ERR_INVALID;
+		const size_t n = static_cast<size_t>(t.width) * t.height;
+		const uint8_t* src = static_cast<const uint8_t*>(t.data);
+		std::vector<float> texels(n * 4);
+		for (size_t k = 0; k < n; ++k)
+		{
+			if (t.format == RB_TEXFMT_R8)
+			{
+				texels[4 * k] = t.srgb ? lut[src[k]] : static_cast<float>(src[k]) / 255.0f;
+				texels[4 * k + 1] = 0.0f; texels[4 * k + 2] = 0.0f; texels[4 * k + 3] = 1.0f;
+				continue;
+			}
+			for (int ch = 0; ch < 4; ++ch)
+			{
+				const uint8_t b = src[4 * k + ch];
+				texels[4 * k + ch] = (t.srgb && ch < 3) ? lut[b] : static_cast<float>(b) / 255.0f;
+			}
+		}
+		const cudaTextureObject_t h = addTexture(texels.data(), static_cast<int>(t.width), static_cast<int>(t.height), 1, 4);
+		oracle_tex::Texture& view = g_textures.back()->view;
+		view.addrU = static_cast<int>(t.address_u == RB_TEXADDR_WRAP ? 0 : (t.address_u == RB_TEXADDR_CLAMP ? 1 : 2));
+		view.addrV = static_cast<int>(t.address_v == RB_TEXADDR_WRAP ? 0 : (t.address_v == RB_TEXADDR_CLAMP ? 1 : 2));
+		view.linear = t.filter == RB_TEXFILTER_LINEAR ? 1 : 0;
+		g_materialTextures.push_back(h);
+	}
+	return RB_OK;
+}
+
 int rbref_set_materials(const rb_material* mats, uint32_t count)
 {
 	g_materials.assign(count, MaterialData{});
@@ -270,7 +318,9 @@ int rbref_set_materials(const rb_material* mats, uint32_t count)
 	for (uint32_t i = 0; i < count; ++i)
 	{
 		const rb_material& m = mats[i];
-		if (m.textures != 0) return RB_ERR_UNSUPPORTED;
+		if (m.textures >> RB_TEXTURE_SLOTS) return RB_ERR_INVALID;
+		for (uint32_t t = 0; t < RB_TEXTURE_SLOTS; ++t)
+			if (((m.textures >> t) & 1u) && m.texture_index[t] >= g_materialTextures.size()) return RB_ERR_INVALID;
 		MaterialData& d = g_materials[i];
 		d.bxdfIndexSBT = m.bxdf;
 		d.doubleSided = m.double_sided != 0;
@@ -298,7 +348,25 @@ int rbref_set_materials(const rb_material* mats, uint32_t count)
 		d.mfRoughnessValue = m.mf_roughness;
 		d.ior = m.ior;
 		d.alphaCutoff = m.alpha_cutoff;
-		d.textures = MaterialData::TextureTypeBitfield::NONE;
+		d.textures = static_cast<MaterialData::TextureTypeBitfield>(m.textures);
+		auto handle = [&](uint32_t slot) -> cudaTextureObject_t {
+			return ((m.textures >> slot) & 1u) ? g_materialTextures[m.texture_index[slot]] : 0;
+		};
+		auto set2 = [&](uint32_t slot) { return ((m.texcoord_sets >> slot) & 1u) != 0; };
+		d.baseColorTexture = handle(RB_TEXTURE_BASE_COLOR);
+		d.normalTexture = handle(RB_TEXTURE_NORMAL);
+		d.pbrMetalRoughnessTexture = handle(RB_TEXTURE_MET_ROUGH);
+		d.transmissionTexture = handle(RB_TEXTURE_TRANSMISSION);
+		d.sheenColorTexture = handle(RB_TEXTURE_SHEEN_COLOR);
+		d.sheenRoughTexture = handle(RB_TEXTURE_SHEEN_ROUGH);
+		d.emissiveTexture = handle(RB_TEXTURE_EMISSION);
+		d.bcTexCoordSetIndex = set2(RB_TEXTURE_BASE_COLOR);
+		d.nmTexCoordSetIndex = set2(RB_TEXTURE_NORMAL);
+		d.mrTexCoordSetIndex = set2(RB_TEXTURE_MET_ROUGH);
+		d.trTexCoordSetIndex = set2(RB_TEXTURE_TRANSMISSION);
+		d.shcTexCoordSetIndex = set2(RB_TEXTURE_SHEEN_COLOR);
+		d.shrTexCoordSetIndex = set2(RB_TEXTURE_SHEEN_ROUGH);
+		d.emTexCoordSetIndex = set2(RB_TEXTURE_EMISSION);
 		d.factors = static_cast<MaterialData::FactorTypeBitfield>(m.factors);
 		for (int k = 0; k < 4; ++k) d.baseColorFactor[k] = m.base_color[k];
 		d.metalnessFactor = m.metalness;

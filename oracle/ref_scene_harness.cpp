@@ -3,7 +3,9 @@
 // The reference's own glTF loader (SceneData::loadModel and loadGLTF,
 // src/core/scene.cpp:92-656, on the vendored cgltf) compiled host-side, with
 // plain C getters over the SceneData it fills, so the project's loader
-// (ratbite_b200/gltf.py) can be compared with it on the same files.
+// (ratbite_b200/gltf.py) can be compared with it on the same files, and the
+// reference's tangent-frame packing (src/core/rendering_interface.cpp:258-284)
+// for the FRAME vertex attribute.
 
 #define STB_IMAGE_IMPLEMENTATION
 #include <stb/stb_image.h>
@@ -12,6 +14,7 @@
 #include "_ref/src/core/scene.h"
 
 #include <cstring>
+#include <glm/gtc/quaternion.hpp>
 
 namespace
 {
@@ -38,6 +41,7 @@ struct rbref_submesh_info
 	const float* texcoords0;      // vec2 per vertex or null
 	uint32_t discarded_count;
 	const uint32_t* discarded;
+	const float* texcoords1;      // vec2 per vertex or null
 };
 
 struct rbref_material_info
@@ -61,6 +65,8 @@ struct rbref_material_info
 	int32_t emissive_present;
 	float emissive[3];
 	int32_t textures;             // bit per texture slot that is set
+	int32_t tex_index[7];         // bc, mr, nm, tr, shc, shr, em (-1: none)
+	int32_t tex_coord[7];         // the slots' texture-coordinate sets
 };
 
 // Loads `path` into a fresh SceneData with the identity model transform.
@@ -105,6 +111,7 @@ int rbref_scene_submesh(int mesh, int sub, rbref_submesh_info* out)
 	out->texcoords0 = s.texCoordsSets.empty() || s.texCoordsSets[0].empty() ? nullptr : &s.texCoordsSets[0][0].x;
 	out->discarded_count = s.discardedPrimitives.size();
 	out->discarded = s.discardedPrimitives.empty() ? nullptr : s.discardedPrimitives.data();
+	out->texcoords1 = s.texCoordsSets.size() < 2 || s.texCoordsSets[1].empty() ? nullptr : &s.texCoordsSets[1][0].x;
 	return 0;
 }
 
@@ -136,8 +143,14 @@ int rbref_scene_material(int i, rbref_material_info* out)
 	for (int k = 0; k < 3; ++k) out->emissive[k] = d.emissiveFactor[k];
 	const int tex[7] = { d.baseColorTextureIndex, d.metalRoughnessTextureIndex, d.normalTextureIndex,
 		d.transmissionTextureIndex, d.sheenColorTextureIndex, d.sheenRoughTextureIndex, d.emissiveTextureIndex };
+	const int crd[7] = { d.bcTexCoordIndex, d.mrTexCoordIndex, d.nmTexCoordIndex, d.trTexCoordIndex,
+		d.shcTexCoordIndex, d.shrTexCoordIndex, d.emTexCoordIndex };
 	for (int k = 0; k < 7; ++k)
+	{
 		if (tex[k] >= 0) out->textures |= 1 << k;
+		out->tex_index[k] = tex[k];
+		out->tex_coord[k] = crd[k];
+	}
 	return 0;
 }
 
@@ -179,6 +192,72 @@ int rbref_scene_emissive_triangle(int i, int k, float* out)
 	std::memcpy(out + 18, &prim, 4);
 	out[19] = t.flux;
 	return 0;
+}
+
+// [images, textures]
+void rbref_scene_texture_counts(int64_t* out)
+{
+	const SceneData::Model* m = model();
+	out[0] = m ? m->imageData.size() : 0;
+	out[1] = m ? m->textureData.size() : 0;
+}
+
+// width, height, channels and the 8-bit texels of image i
+int rbref_scene_image(int i, int32_t* dims3, const uint8_t** data)
+{
+	const SceneData::Model* m = model();
+	if (!m || i < 0 || i >= static_cast<int>(m->imageData.size())) return -1;
+	const auto& im = m->imageData[i];
+	dims3[0] = im.width;
+	dims3[1] = im.height;
+	dims3[2] = im.channelCount;
+	*data = static_cast<const uint8_t*>(im.data);
+	return 0;
+}
+
+// image index, sRGB, filter, address x, address y of texture i
+int rbref_scene_texture(int i, int32_t* out5)
+{
+	const SceneData::Model* m = model();
+	if (!m || i < 0 || i >= static_cast<int>(m->textureData.size())) return -1;
+	const auto& t = m->textureData[i];
+	out5[0] = t.imageIndex;
+	out5[1] = t.sRGB;
+	out5[2] = static_cast<int32_t>(t.filter);
+	out5[3] = static_cast<int32_t>(t.addressX);
+	out5[4] = static_cast<int32_t>(t.addressY);
+	return 0;
+}
+
+// uv0, uv1, uv2 of triangle k of emissive subset i
+int rbref_scene_emissive_uvs(int i, int k, float* out6)
+{
+	const SceneData::Model* m = model();
+	if (!m || i < 0 || i >= static_cast<int>(m->instancedEmissiveMeshSubsets.size())) return -1;
+	const auto& tris = m->instancedEmissiveMeshSubsets[i].triangles;
+	if (k < 0 || k >= static_cast<int>(tris.size())) return -1;
+	const glm::vec2 uv[3] = { tris[k].uv0, tris[k].uv1, tris[k].uv2 };
+	for (int j = 0; j < 3; ++j) { out6[2 * j] = uv[j].x; out6[2 * j + 1] = uv[j].y; }
+	return 0;
+}
+
+// The FRAME attribute of n vertices (normals and tangents as vec4): the
+// quaternion (x, y, z, w) of the frame (tangent, normal x tangent, normal),
+// w signed by the tangent's handedness, as the reference packs it
+// (src/core/rendering_interface.cpp:258-284, glm::quat_cast).
+void rbref_pack_frames(int n, const float* normals4, const float* tangents4, float* out4)
+{
+	for (int i = 0; i < n; ++i)
+	{
+		const glm::vec4 nv{ normals4[4 * i], normals4[4 * i + 1], normals4[4 * i + 2], normals4[4 * i + 3] };
+		const glm::vec4 tv{ tangents4[4 * i], tangents4[4 * i + 1], tangents4[4 * i + 2], tangents4[4 * i + 3] };
+		glm::quat q{ glm::quat_cast(glm::mat3{ tv, glm::cross(glm::vec3{ nv }, glm::vec3{ tv }), nv }) };
+		if (q.w == 0.0f)
+			q.w = tv.w > 0.0f ? 0.0f : -0.0f;
+		else if (q.w * tv.w < 0.0f)
+			q = -q;
+		out4[4 * i] = q.x; out4[4 * i + 1] = q.y; out4[4 * i + 2] = q.z; out4[4 * i + 3] = q.w;
+	}
 }
 
 } // extern "C"

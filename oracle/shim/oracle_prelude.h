@@ -9,10 +9,13 @@
 //   __fmaf_rn                 (src/device/surface.h:323,346)
 //   __frsqrt_rn / rsqrt       (src/kernels/pathtrace.cu:110,989)
 //   tex2D / tex3D             (src/kernels/pathtrace.cu:646-658, src/device/surface.h:48)
-// Texture fetches go to a registry of host arrays with linear filtering,
-// normalized coordinates and clamp addressing, the sampler state the reference
-// creates for its LUTs and environment map (src/core/rendering_interface.cpp:
-// 540-616, 1358-1360).
+// Texture fetches go to a registry of host arrays with normalized
+// coordinates: linear filtering and clamp addressing, the sampler state the
+// reference creates for its LUTs and environment map
+// (src/core/rendering_interface.cpp: 540-616, 1358-1360), or the material
+// textures' own address modes (wrap, clamp, mirror) and filter (nearest,
+// linear; src/core/texture.h:280-380), their texels already decoded to
+// floats (8-bit / 255, the sRGB curve where the texture is sRGB).
 #pragma once
 
 #include <cfloat>
@@ -57,6 +60,8 @@ namespace oracle_tex
 	{
 		const float* data;
 		int w, h, d, c;
+		int addrU = 1, addrV = 1;   // 0 wrap, 1 clamp, 2 mirror
+		int linear = 1;             // 0 nearest
 	};
 	// Registry lookups (implemented in ref_harness.cpp). Handles start at 1.
 	const Texture& get(cudaTextureObject_t handle);
@@ -70,23 +75,45 @@ namespace oracle_tex
 			return std::nearbyint(frac * 256.0f) / 256.0f;
 		return frac;
 	}
-	// Texel coordinate setup of linear filtering with normalized coordinates
-	// and clamp addressing: x = u*N - 0.5, i0 = floor(x), a = frac(x),
-	// both taps clamped to [0, N-1].
-	inline void taps(float u, int n, int& i0, int& i1, float& a)
+	// Texel index along one axis for the address mode.
+	inline int address(int i, int n, int mode)
 	{
-		float x = u * static_cast<float>(n) - 0.5f;
+		if (mode == 0) { int m = i % n; return m < 0 ? m + n : m; }
+		if (mode == 2) { int m = i % (2 * n); if (m < 0) m += 2 * n; return m < n ? m : 2 * n - 1 - m; }
+		return i < 0 ? 0 : (i > n - 1 ? n - 1 : i);
+	}
+	// The coordinate the filter works on: wrap takes the fraction, mirror
+	// reflects into [0, 1], clamp keeps it.
+	inline float coord(float u, int mode)
+	{
+		if (mode == 0) return u - std::floor(u);
+		if (mode == 2) { float f = u - 2.0f * std::floor(u * 0.5f); return f <= 1.0f ? f : 2.0f - f; }
+		return u;
+	}
+	// Texel coordinate setup of linear filtering with normalized coordinates:
+	// x = u*N - 0.5, i0 = floor(x), a = frac(x), the taps addressed by the
+	// mode (clamp: both clamped to [0, N-1]).
+	inline void taps(float u, int n, int& i0, int& i1, float& a, int mode = 1)
+	{
+		float x = coord(u, mode) * static_cast<float>(n) - 0.5f;
 		float fl = std::floor(x);
 		a = weight(x - fl);
 		int i = static_cast<int>(fl);
-		i0 = i < 0 ? 0 : (i > n - 1 ? n - 1 : i);
-		i1 = i + 1 < 0 ? 0 : (i + 1 > n - 1 ? n - 1 : i + 1);
+		i0 = address(i, n, mode);
+		i1 = address(i + 1, n, mode);
 	}
 	inline void fetch2D(const Texture& t, float u, float v, float* out)
 	{
+		if (!t.linear)
+		{
+			const int x = address(static_cast<int>(std::floor(coord(u, t.addrU) * static_cast<float>(t.w))), t.w, t.addrU);
+			const int y = address(static_cast<int>(std::floor(coord(v, t.addrV) * static_cast<float>(t.h))), t.h, t.addrV);
+			for (int ch = 0; ch < t.c; ++ch) out[ch] = t.data[(y * t.w + x) * t.c + ch];
+			return;
+		}
 		int x0, x1, y0, y1; float a, b;
-		taps(u, t.w, x0, x1, a);
-		taps(v, t.h, y0, y1, b);
+		taps(u, t.w, x0, x1, a, t.addrU);
+		taps(v, t.h, y0, y1, b, t.addrV);
 		for (int ch = 0; ch < t.c; ++ch)
 		{
 			float t00 = t.data[(y0 * t.w + x0) * t.c + ch];

@@ -26,10 +26,11 @@ SIGNATURES = {
     "rb_set_luts": (C.c_int, [_P] * 7),
     "rb_set_spectra": (C.c_int, [_P, _P, _P, _P, _U32]),
     "rb_set_materials": (C.c_int, [_P, _P, _U32]),
+    "rb_set_textures": (C.c_int, [_P, _P, _U32]),
     "rb_set_geometry": (C.c_int, [_P, _P]),
     "rb_set_lights": (C.c_int, [_P, _P]),
     "rb_set_light_origin": (C.c_int, [_P, _P, _P]),
-    "rb_build_lights": (C.c_int, [_P, _U32, _P, _P, _P, _P, _P]),
+    "rb_build_lights": (C.c_int, [_P, _U32, _P, _P, _P, _P, _P, _P]),
     "rb_update_instances": (C.c_int, [_P, _P, _P, _P]),
     "rb_build_light_tree": (C.c_int, [_U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "rb_set_envmap": (C.c_int, [_P, _P, _U32, _U32]),
@@ -81,7 +82,7 @@ SIGNATURES = {
     "rb_nrc_gradients": (C.c_int, [_P, _U32, _P, _P, _P, _P]),
     "rb_nrc_status": (C.c_int, [_P, _P]),
     "rb_k_build_light_tree_scratch_bytes": (C.c_size_t, [_U32]),
-    "rb_k_build_light_tree": (C.c_int, [_U32] + [_P] * 11 + [_P]),
+    "rb_k_build_light_tree": (C.c_int, [_U32] + [_P] * 12 + [_P]),
     "rb_attach_radiance_cache": (C.c_int, [_P, _P, C.POINTER(abi.rb_cache_params)]),
     "rb_get_cache_stats": (C.c_int, [_P, C.POINTER(abi.rb_cache_stats)]),
 }

@@ -6,7 +6,7 @@ the sizes against the compiled library.
 """
 import ctypes as C
 
-RB_ABI_VERSION = 3
+RB_ABI_VERSION = 4
 
 RB_OK = 0
 RB_ERR_INVALID = -1
@@ -46,6 +46,22 @@ RB_FACTOR_BLEND = 1 << 5
 RB_FACTOR_SHEEN_COLOR = 1 << 6
 RB_FACTOR_SHEEN_ROUGH = 1 << 7
 RB_FACTOR_EMISSION = 1 << 8
+# texture slots of rb_material.textures / texture_index (TextureTypeBitfield)
+RB_TEXTURE_BASE_COLOR = 0
+RB_TEXTURE_NORMAL = 1
+RB_TEXTURE_MET_ROUGH = 2
+RB_TEXTURE_TRANSMISSION = 3
+RB_TEXTURE_SHEEN_COLOR = 4
+RB_TEXTURE_SHEEN_ROUGH = 5
+RB_TEXTURE_EMISSION = 6
+RB_TEXTURE_SLOTS = 7
+RB_TEXFMT_R8 = 0
+RB_TEXFMT_RGBA8 = 1
+RB_TEXADDR_WRAP = 0
+RB_TEXADDR_CLAMP = 1
+RB_TEXADDR_MIRROR = 2
+RB_TEXFILTER_NEAREST = 0
+RB_TEXFILTER_LINEAR = 1
 
 RB_SPECTRUM_BINS = 471
 RB_LUT_SIZE = 32
@@ -114,6 +130,15 @@ class rb_material(C.Structure):
         ("emissive", F3),
         ("triangle_count", C.c_uint32), ("indices", C.c_void_p),
         ("vertex_count", C.c_uint32), ("attribute_data", C.c_void_p),
+        ("texcoord_sets", C.c_uint32), ("texture_index", C.c_uint32 * RB_TEXTURE_SLOTS),
+    ]
+
+
+class rb_texture(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32), ("height", C.c_uint32), ("format", C.c_uint32), ("srgb", C.c_uint32),
+        ("address_u", C.c_uint32), ("address_v", C.c_uint32), ("filter", C.c_uint32), ("reserved", C.c_uint32),
+        ("data", C.c_void_p),
     ]
 
 

@@ -37,7 +37,7 @@ struct rb_ctx
 	rb::LaunchShape shape{};
 	uint32_t* status = nullptr;          // [0] flags, [1] detail
 	// owned device buffers by role
-	std::vector<void*> lutBufs, spectraBufs, materialBufs, geoBufs, lightBufs, envBufs;
+	std::vector<void*> lutBufs, spectraBufs, materialBufs, geoBufs, lightBufs, envBufs, textureBufs;
 	// wavefront state
 	rb::PathSoA soa{};
 	std::vector<void*> soaBufs;
@@ -58,6 +58,7 @@ struct rb_ctx
 	// fault injection (rb_config.inject_*; tests only)
 	uint32_t injectQueueLimit = 0, injectAllocFailure = 0, injectStackLimit = 0;
 	uint64_t allocCount = 0;                    // device allocations made so far
+	uint32_t texturesNeeded = 0;                // 1 + the largest texture index the materials use
 	void* envScratch = nullptr;                 // CDF scratch of the current map (in envBufs)
 	float* envIntegral = nullptr;               // device scalar (in envBufs)
 	double4* accum = nullptr;
@@ -308,6 +309,8 @@ int checkReferences(rb_ctx* ctx)
 		return fail(ctx, RB_ERR_INVALID, "material index out of range of the material table");
 	if (ctx->geoEmissive > ctx->scene.lights.triangleCount)
 		return fail(ctx, RB_ERR_INVALID, "geometry traces more emissive triangles than the light data holds");
+	if (ctx->texturesNeeded > ctx->scene.textureCount)
+		return fail(ctx, RB_ERR_INVALID, "texture index out of range of the texture table");
 	return RB_OK;
 }
 
@@ -333,7 +336,7 @@ int ensureWave(rb_ctx* ctx, uint32_t paths)
 	alloc(s.shO, sizeof(float4)); alloc(s.shD, sizeof(float4)); alloc(s.shC, sizeof(float4));
 	alloc(s.sfP, sizeof(float4)); alloc(s.sfPi, sizeof(float4)); alloc(s.sfGn, sizeof(float4));
 	alloc(s.sfT, sizeof(float4)); alloc(s.sfB, sizeof(float4)); alloc(s.sfN, sizeof(float4));
-	alloc(s.sfL, sizeof(float4));
+	alloc(s.sfL, sizeof(float4)); alloc(s.sfUV, sizeof(float4));
 	alloc(s.queue[0], sizeof(uint32_t)); alloc(s.queue[1], sizeof(uint32_t)); alloc(s.shadowQueue, sizeof(uint32_t));
 	alloc(s.surfQueue, sizeof(uint32_t)); alloc(s.recOrder, sizeof(uint32_t));
 	alloc(s.emQueue, sizeof(uint32_t)); alloc(s.emA, sizeof(float4)); alloc(s.emB, sizeof(float4));
@@ -530,7 +533,8 @@ int rb_destroy(rb_ctx* ctx)
 	if (!ctx) return RB_ERR_INVALID;
 	cudaSetDevice(ctx->device);
 	cudaStreamSynchronize(ctx->stream);
-	for (auto* v : { &ctx->lutBufs, &ctx->spectraBufs, &ctx->materialBufs, &ctx->geoBufs, &ctx->lightBufs, &ctx->envBufs })
+	for (auto* v : { &ctx->lutBufs, &ctx->spectraBufs, &ctx->materialBufs, &ctx->geoBufs, &ctx->lightBufs, &ctx->envBufs,
+			&ctx->textureBufs })
 		freeAll(*v);
 	releaseWave(ctx);
 	freeAll(ctx->jobBufs);
@@ -594,7 +598,20 @@ int rb_set_materials(rb_ctx* ctx, const rb_material* mats, uint32_t count)
 	for (uint32_t i = 0; i < count; ++i)
 	{
 		const rb_material& m = mats[i];
-		if (m.textures != 0) return fail(ctx, RB_ERR_UNSUPPORTED, "rb_set_materials: textures are not supported");
+		if (m.textures >> RB_TEXTURE_SLOTS) return fail(ctx, RB_ERR_INVALID, "rb_set_materials: unknown texture slot");
+		for (uint32_t t = 0; t < RB_TEXTURE_SLOTS; ++t)
+			if (((m.textures >> t) & 1u) && m.texture_index[t] >= ctx->scene.textureCount)
+				return fail(ctx, RB_ERR_INVALID, "rb_set_materials: texture index beyond the rb_set_textures table");
+		if (m.textures & ~(1u << RB_TEXTURE_EMISSION))
+		{
+			// the surface textures read vertex texture coordinates
+			if (!m.attribute_data || m.attribute_stride == 0)
+				return fail(ctx, RB_ERR_INVALID, "rb_set_materials: textures without attribute data");
+			for (uint32_t set = 0; set < 2; ++set)
+				if ((m.attributes & (set ? RB_ATTR_TEX_COORD_2 : RB_ATTR_TEX_COORD_1)) &&
+					(set ? m.texcoord2_offset : m.texcoord1_offset) + 8u > m.attribute_stride)
+					return fail(ctx, RB_ERR_INVALID, "rb_set_materials: texture coordinates outside the vertex");
+		}
 		if (m.bxdf > RB_BXDF_COMPLEX_SURFACE) return fail(ctx, RB_ERR_INVALID, "rb_set_materials: unknown bxdf");
 		if (m.index_type > RB_INDEX_U32) return fail(ctx, RB_ERR_INVALID, "rb_set_materials: unknown index type");
 		if ((m.attributes & (RB_ATTR_NORMAL | RB_ATTR_FRAME)) && (!m.attribute_data || m.attribute_stride == 0))
@@ -630,6 +647,12 @@ int rb_set_materials(rb_ctx* ctx, const rb_material* mats, uint32_t count)
 		d.sheenRoughness = m.sheen_roughness;
 		d.triangleCount = m.triangle_count;
 		d.vertexCount = m.vertex_count;
+		d.textures = m.textures;
+		d.texSets = m.texcoord_sets;
+		d.texcoordOffset[0] = m.texcoord1_offset;
+		d.texcoordOffset[1] = m.texcoord2_offset;
+		for (uint32_t t = 0; t < RB_TEXTURE_SLOTS; ++t)
+			d.tex[t] = ((m.textures >> t) & 1u) ? static_cast<uint16_t>(m.texture_index[t]) : 0;
 		const size_t ib = static_cast<size_t>(m.triangle_count) * 3 * (m.index_type == RB_INDEX_U16 ? 2 : 4);
 		uint8_t* dptr = nullptr;
 		int rc = upload(ctx, fresh, m.indices, ib, dptr);
@@ -647,6 +670,63 @@ int rb_set_materials(rb_ctx* ctx, const rb_material* mats, uint32_t count)
 	if (rc != RB_OK) return rc;
 	ctx->scene.materials = dptr;
 	ctx->scene.materialCount = count;
+	ctx->texturesNeeded = 0;
+	for (uint32_t i = 0; i < count; ++i)
+		for (uint32_t t = 0; t < RB_TEXTURE_SLOTS; ++t)
+			if ((mats[i].textures >> t) & 1u) ctx->texturesNeeded = std::max(ctx->texturesNeeded, mats[i].texture_index[t] + 1u);
+	return RB_OK;
+}
+
+int rb_set_textures(rb_ctx* ctx, const rb_texture* textures, uint32_t count)
+{
+	if (!ctx || (count && !textures)) return fail(ctx, RB_ERR_INVALID, "rb_set_textures: null textures");
+	if (count > 65535u) return fail(ctx, RB_ERR_TOO_LARGE, "rb_set_textures: more than 65535 textures");
+	for (uint32_t i = 0; i < count; ++i)
+	{
+		const rb_texture& t = textures[i];
+		if (t.width == 0 || t.height == 0 || t.width > 32768u || t.height > 32768u || !t.data)
+			return fail(ctx, RB_ERR_INVALID, "rb_set_textures: empty, oversized or null texture");
+		if (t.format > RB_TEXFMT_RGBA8 || t.address_u > RB_TEXADDR_MIRROR || t.address_v > RB_TEXADDR_MIRROR ||
+			t.filter > RB_TEXFILTER_LINEAR || t.srgb > 1u)
+			return fail(ctx, RB_ERR_INVALID, "rb_set_textures: unknown format, address mode or filter");
+	}
+	cudaSetDevice(ctx->device);
+	std::vector<void*> fresh;
+	std::vector<rb::DevTexture> dt(std::max<uint32_t>(count, 1));
+	int rc = RB_OK;
+	for (uint32_t i = 0; i < count && rc == RB_OK; ++i)
+	{
+		const rb_texture& t = textures[i];
+		rb::DevTexture& d = dt[i];
+		d = rb::DevTexture{};
+		d.width = t.width;
+		d.height = t.height;
+		d.channels = t.format == RB_TEXFMT_R8 ? 1u : 4u;
+		d.srgb = t.srgb ? 1u : 0u;
+		d.addrU = t.address_u;
+		d.addrV = t.address_v;
+		d.filter = t.filter;
+		uint8_t* dptr = nullptr;
+		rc = upload(ctx, fresh, t.data, static_cast<size_t>(t.width) * t.height * d.channels, dptr);
+		d.data = dptr;
+	}
+	// the sRGB decode of each 8-bit code (IEC 61966-2-1), in double precision
+	float lut[256];
+	for (int c = 0; c < 256; ++c)
+	{
+		const double x = c / 255.0;
+		lut[c] = static_cast<float>(x <= 0.04045 ? x / 12.92 : std::pow((x + 0.055) / 1.055, 2.4));
+	}
+	rb::DevTexture* table = nullptr;
+	float* lutDev = nullptr;
+	if (rc == RB_OK) rc = upload(ctx, fresh, dt.data(), sizeof(rb::DevTexture) * dt.size(), table);
+	if (rc == RB_OK) rc = upload(ctx, fresh, lut, sizeof(lut), lutDev);
+	if (rc == RB_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = fail(ctx, RB_ERR_CUDA, "texture upload");
+	rc = commit(ctx, ctx->textureBufs, fresh, rc);
+	if (rc != RB_OK) return rc;
+	ctx->scene.textures = table;
+	ctx->scene.textureCount = count;
+	ctx->scene.srgbLut = lutDev;
 	return RB_OK;
 }
 
@@ -901,7 +981,7 @@ int rb_set_lights(rb_ctx* ctx, const rb_light_tree* t)
 }
 
 int rb_build_lights(rb_ctx* ctx, uint32_t n, const float* world, const float* flux, const uint32_t* material,
-	const uint32_t* primitive, void* stream)
+	const uint32_t* primitive, const float* uvs, void* stream)
 {
 	if (!ctx) return RB_ERR_INVALID;
 	if (n && (!world || !flux || !material || !primitive)) return fail(ctx, RB_ERR_INVALID, "rb_build_lights: null input");
@@ -931,7 +1011,7 @@ int rb_build_lights(rb_ctx* ctx, uint32_t n, const float* world, const float* fl
 		// origin-independent records (light origin 0), then the working copies as rb_set_lights makes them
 		cudaStreamSynchronize(ctx->stream);
 		const double zero[3] = { 0.0, 0.0, 0.0 };
-		rc = rb_k_build_light_tree(n, world, flux, material, primitive, zero, scratch, worldTris, worldNodes,
+		rc = rb_k_build_light_tree(n, world, flux, material, primitive, uvs, zero, scratch, worldTris, worldNodes,
 			const_cast<uint32_t*>(L.pointers), const_cast<uint64_t*>(L.bitmasks), dCount, st);
 		if (rc != RB_OK) rc = fail(ctx, rc, "rb_build_lights: build");
 		if (rc == RB_OK && cudaMemcpyAsync(&nodeCount, dCount, sizeof(uint32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess)
@@ -1177,6 +1257,7 @@ int renderWaves(rb_ctx* ctx, uint32_t offset, uint32_t count, cudaStream_t st, c
 		w.sampleBase = dyn ? done : offset + done;
 		w.fresh = dyn ? (done == 0 ? 1u : 0u) : ((offset == 0 && done == 0) ? 1u : 0u);
 		w.keepFailed = ctx->failedMode == RB_FAILED_KEEP ? 1u : 0u;
+		w.textured = ctx->texturesNeeded ? 1u : 0u;
 		if (cached)
 		{
 			w.cached = 1;
@@ -1381,6 +1462,8 @@ int rb_render_jobs(rb_ctx* const* jobs, uint32_t n, const uint32_t* offsets, con
 			&shape.blocksResolve })
 		*b = std::max(1, static_cast<int>(static_cast<uint64_t>(*b) * pct / 100u));
 	const rb::DevScene& sc = host->scene;
+	bool textured = false;
+	for (uint32_t j = 0; j < n; ++j) textured = textured || jobs[j]->texturesNeeded != 0;
 	for (uint32_t k = 0; k < waves.size(); ++k)
 	{
 		const Wave& wv = waves[k];
@@ -1390,6 +1473,7 @@ int rb_render_jobs(rb_ctx* const* jobs, uint32_t n, const uint32_t* offsets, con
 		w.chunks = host->chunkTable + wv.firstChunk;
 		w.nChunks = wv.chunks;
 		w.pixelSlots = wv.pixelSlots;
+		w.textured = textured ? 1u : 0u;
 		shape.items = w.paths;
 		cudaMemsetAsync(soa.counts, 0, sizeof(uint32_t) * rb::kCountSlots, st);
 		rb::launchGenerate(sc, soa, w, shape, st);

@@ -24,6 +24,7 @@
 #include "rb_light.cuh"
 #include "rb_launch.cuh"
 #include "rb_qrng.cuh"
+#include "rb_texture.cuh"
 #include "rb_wavefront.h"
 #include "ratbite_b200_kernels.h"
 #include "ratbite_b200_nrc.h"
@@ -119,9 +120,35 @@ RB_D uint32_t readIndex(const DevMaterial& m, uint32_t i)
 	                        : reinterpret_cast<const uint32_t*>(m.indices)[i];
 }
 
-// Shading frame and shadow-terminator offset (pathtrace.cu:1279-1461).
+// Texture coordinates of a textured material's hit (x, y: set 1; z, w: set
+// 2; zero where the mesh has none), and the normal texture's direction in
+// the frame ((0, 0, 1) without one).
+RB_D void textureFrameInputs(const DevScene& sc, const DevMaterial& mat, uint32_t idx0, uint32_t idx1,
+	uint32_t idx2, float w0, float w1, float w2, float4& uv, f3& nm)
+{
+	for (uint32_t set = 0; set < 2; ++set)
+	{
+		if (!(mat.attributes & (set ? RB_ATTR_TEX_COORD_2 : RB_ATTR_TEX_COORD_1))) continue;
+		const uint8_t* at = mat.attributeData + mat.texcoordOffset[set];
+		const float2 c0 = *reinterpret_cast<const float2*>(at + mat.attributeStride * idx0);
+		const float2 c1 = *reinterpret_cast<const float2*>(at + mat.attributeStride * idx1);
+		const float2 c2 = *reinterpret_cast<const float2*>(at + mat.attributeStride * idx2);
+		const float tu = w0 * c0.x + w1 * c1.x + w2 * c2.x, tv = w0 * c0.y + w1 * c1.y + w2 * c2.y;
+		if (set) { uv.z = tu; uv.w = tv; } else { uv.x = tu; uv.y = tv; }
+	}
+	if (mat.textures & (1u << RB_TEXTURE_NORMAL))
+	{
+		const float4 t = materialTexture(sc, mat, RB_TEXTURE_NORMAL, RB_TEXTURE_NORMAL, uv);
+		nm = normalize(mk(t.x * 2.0f - 1.0f, t.y * 2.0f - 1.0f, t.z * 2.0f - 1.0f));
+	}
+}
+
+// Shading frame and shadow-terminator offset (pathtrace.cu:1279-1461), and
+// the texture coordinates at the hit (x, y: set 1; z, w: set 2; zero where
+// the mesh has none), with the normal texture applied to the frame.
+template<bool TEX>
 RB_D void shadingFrame(const DevScene& sc, const DevMaterial& mat, Interaction& it, f3 rayD, Frame& frame,
-	f3& lastNormal)
+	f3& lastNormal, float4& uv)
 {
 	const float w0 = 1.0f - it.b1 - it.b2, w1 = it.b1, w2 = it.b2;
 	const float* M = sc.geo.normalMatrix + 9u * it.instance;
@@ -193,11 +220,16 @@ RB_D void shadingFrame(const DevScene& sc, const DevMaterial& mat, Interaction& 
 		normal = it.gn;
 		tangent = tangentOf(it.gn);
 	}
-	// Frame and shading-normal correction (pathtrace.cu:1434-1461).
+	// texture coordinates (pathtrace.cu:1414-1430), read only for textured
+	// materials; without TEX (a scene without textures) the code is not compiled in
+	uv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	f3 nm = mk(0.0f, 0.0f, 1.0f);
+	if (TEX && mat.textures) textureFrameInputs(sc, mat, idx0, idx1, idx2, w0, w1, w2, uv, nm);
+	// Frame, normal texture and shading-normal correction (pathtrace.cu:1434-1461).
 	const f3 bitangent = cross(normal, tangent) * (flipTangent ? -1.0f : 1.0f);
-	f3 n = mk(tangent.x * 0.0f + bitangent.x * 0.0f + normal.x * 1.0f,
-	          tangent.y * 0.0f + bitangent.y * 0.0f + normal.y * 1.0f,
-	          tangent.z * 0.0f + bitangent.z * 0.0f + normal.z * 1.0f);
+	f3 n = mk(tangent.x * nm.x + bitangent.x * nm.y + normal.x * nm.z,
+	          tangent.y * nm.x + bitangent.y * nm.y + normal.y * nm.z,
+	          tangent.z * nm.x + bitangent.z * nm.y + normal.z * nm.z);
 	const float dNs = dot(n, rayD), dNg = dot(it.gn, rayD);
 	const bool fromOutside = dNs > 0.0f && dNg < 0.0f;
 	const bool fromInside = dNs < 0.0f && dNg > 0.0f;
@@ -210,8 +242,8 @@ RB_D void shadingFrame(const DevScene& sc, const DevMaterial& mat, Interaction& 
 	lastNormal = n;
 }
 
-// Surface description from the material factors (pathtrace.cu:1463-1560);
-// textures are not supported.
+// Surface description from the material factors (pathtrace.cu:1463-1560),
+// for a material without textures.
 RB_D Surface surfaceOf(const DevMaterial& mat)
 {
 	Surface surf = defaultSurface();
@@ -229,14 +261,93 @@ RB_D Surface surfaceOf(const DevMaterial& mat)
 	return surf;
 }
 
-// Alpha cutoff or stochastic alpha blending (pathtrace.cu:1485-1496): true
-// if the interaction is skipped and the path continues through the surface.
-RB_D bool alphaSkipped(const DevMaterial& mat, const Qrng& q)
+// Surface description with the material's textures at the record's
+// coordinates (pathtrace.cu:1463-1560). The base-colour texture is read
+// with the normal texture's coordinate set, as the reference does (:1468).
+RB_D Surface surfaceTextured(const DevScene& sc, const DevMaterial& mat, float4 uv)
 {
-	const float alpha = (mat.factors & RB_FACTOR_BASE_COLOR) ? mat.baseColor[3] : 0.0f;
+	Surface surf = surfaceOf(mat);
+	const uint32_t T = mat.textures;
+	if (T & (1u << RB_TEXTURE_BASE_COLOR))
+	{
+		const float4 t = materialTexture(sc, mat, RB_TEXTURE_BASE_COLOR, RB_TEXTURE_NORMAL, uv);
+		surf.baseColor = mk(t.x, t.y, t.z);
+		if (mat.factors & RB_FACTOR_BASE_COLOR)
+			surf.baseColor = mk(surf.baseColor.x * mat.baseColor[0], surf.baseColor.y * mat.baseColor[1],
+				surf.baseColor.z * mat.baseColor[2]);
+	}
+	if (T & (1u << RB_TEXTURE_MET_ROUGH))
+	{
+		const float4 t = materialTexture(sc, mat, RB_TEXTURE_MET_ROUGH, RB_TEXTURE_MET_ROUGH, uv);
+		surf.metalness = t.z * ((mat.factors & RB_FACTOR_METALNESS) ? mat.metalness : 1.0f);
+		surf.roughness = t.y * ((mat.factors & RB_FACTOR_ROUGHNESS) ? mat.roughness : 1.0f);
+	}
+	if (T & (1u << RB_TEXTURE_TRANSMISSION))
+	{
+		const float4 t = materialTexture(sc, mat, RB_TEXTURE_TRANSMISSION, RB_TEXTURE_TRANSMISSION, uv);
+		surf.transmission = t.x * ((mat.factors & RB_FACTOR_TRANSMISSION) ? mat.transmission : 1.0f);
+	}
+	if (mat.sheenPresent)
+	{
+		if (T & (1u << RB_TEXTURE_SHEEN_COLOR))
+		{
+			const float4 t = materialTexture(sc, mat, RB_TEXTURE_SHEEN_COLOR, RB_TEXTURE_SHEEN_COLOR, uv);
+			const bool f = (mat.factors & RB_FACTOR_SHEEN_COLOR) != 0;
+			surf.sheenColor = mk(t.x * (f ? mat.sheenColor[0] : 1.0f), t.y * (f ? mat.sheenColor[1] : 1.0f),
+				t.z * (f ? mat.sheenColor[2] : 1.0f));
+		}
+		if (T & (1u << RB_TEXTURE_SHEEN_ROUGH))
+		{
+			// the texture's fourth channel, squared (the factor alone is taken as is)
+			const float4 t = materialTexture(sc, mat, RB_TEXTURE_SHEEN_ROUGH, RB_TEXTURE_SHEEN_ROUGH, uv);
+			const float r = t.w * ((mat.factors & RB_FACTOR_SHEEN_ROUGH) ? mat.sheenRoughness : 1.0f);
+			surf.sheenAlpha = r * r;
+		}
+	}
+	return surf;
+}
+template<bool TEX>
+RB_D Surface surfaceAt(const DevScene& sc, const DevMaterial& mat, float4 uv)
+{
+	return (TEX && mat.textures) ? surfaceTextured(sc, mat, uv) : surfaceOf(mat);
+}
+
+// Alpha of a base-colour texture, times the factor's (pathtrace.cu:1466-1477).
+RB_D float texturedAlpha(const DevScene& sc, const DevMaterial& mat, float4 uv)
+{
+	float alpha = materialTexture(sc, mat, RB_TEXTURE_BASE_COLOR, RB_TEXTURE_NORMAL, uv).w;
+	if (mat.factors & RB_FACTOR_BASE_COLOR) alpha *= mat.baseColor[3];
+	return alpha;
+}
+// Alpha cutoff or stochastic alpha blending (pathtrace.cu:1470-1496): true
+// if the interaction is skipped and the path continues through the surface.
+template<bool TEX>
+RB_D bool alphaSkipped(const DevScene& sc, const DevMaterial& mat, float4 uv, const Qrng& q)
+{
+	float alpha = (mat.factors & RB_FACTOR_BASE_COLOR) ? mat.baseColor[3] : 0.0f;
+	if (TEX && (mat.textures & (1u << RB_TEXTURE_BASE_COLOR))) alpha = texturedAlpha(sc, mat, uv);
 	if (mat.factors & RB_FACTOR_CUTOFF) return alpha < mat.alphaCutoff;
 	if (mat.factors & RB_FACTOR_BLEND) return sample1D(q, DIM_ALPHA_BLEND) > alpha;
 	return false;
+}
+// Emitted RGB of an emissive triangle at barycentrics (w1, w2) (the
+// emissive factor, times the emission texture at the triangle's
+// coordinates: pathtrace.cu:1215-1228, 1638-1648).
+RB_D f3 texturedEmission(const DevScene& sc, const EmissiveTri& et, const DevMaterial& em, f3 e,
+	float w1, float w2)
+{
+	const float w0 = 1.0f - w1 - w2;
+	const float u = w0 * et.uv[0] + w1 * et.uv[2] + w2 * et.uv[4];
+	const float v = w0 * et.uv[1] + w1 * et.uv[3] + w2 * et.uv[5];
+	const float4 t = texSample(sc, em.tex[RB_TEXTURE_EMISSION], u, v);
+	return mk(e.x * t.x, e.y * t.y, e.z * t.z);
+}
+template<bool TEX>
+RB_D f3 emissionAt(const DevScene& sc, const EmissiveTri& et, float w1, float w2)
+{
+	const DevMaterial& em = sc.materials[et.material];
+	const f3 e = mk(em.emissive[0], em.emissive[1], em.emissive[2]);
+	return (TEX && (em.textures & (1u << RB_TEXTURE_EMISSION))) ? texturedEmission(sc, et, em, e, w1, w2) : e;
 }
 
 // Pixel (x, y) of path slot `slot` (0 .. W x H - 1) of a plane: slots run
@@ -352,6 +463,9 @@ __global__ void __launch_bounds__(kThreads) kGenerate(const __grid_constant__ De
 // uncapped), both at 8 blocks: 188 ms per frame, against 202 / 216 / 220 /
 // 203 ms at 12 / 4 / 5 / 6 blocks, and 229 ms for the single kernel at its
 // best cap (16 blocks, 32 registers, 1.2 KB of spills per thread).
+// Re-swept with the records at their queue position (frame ms): surface 4 /
+// 6 / 8 blocks 976 / 970 / 970, BxDF 6 / 8 / 12 982 / 970 / 974, light
+// sample 6 / 8 / 12 970 / 970 / 971.
 #ifndef RB_SURFACE_MIN_BLOCKS
 #define RB_SURFACE_MIN_BLOCKS 6
 #endif
@@ -464,7 +578,7 @@ RB_D bool cacheVertex(const PathSoA& s, const WaveParams& w, uint32_t* status, u
 // continue get a surface record and join the surface queue, which the light
 // sampling and BxDF stages read.
 // counters (optional): [6] surface records.
-template<bool JOBS>
+template<bool JOBS, bool TEX>
 __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(const __grid_constant__ DevScene scK, PathSoA s,
 	WaveParams w, int bounce, unsigned long long* counters)
 {
@@ -515,8 +629,7 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(cons
 				const float lCos = -dot(rayD, nn);
 				noEmission = lCos <= 0.0f;
 				lightPdf = (1.0f / area) * d2 / lCos;
-				const DevMaterial& em = sc.materials[et.material];
-				Le = rgbToSpectrum(sc.spectra.basis, mk(em.emissive[0], em.emissive[1], em.emissive[2]), lambda);
+				Le = rgbToSpectrum(sc.spectra.basis, emissionAt<TEX>(sc, et, it.b1, it.b2), lambda);
 			}
 			else
 			{
@@ -552,16 +665,17 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(cons
 			const DevMaterial& mat = sc.materials[it.material];
 			Frame frame{};
 			bool skipped = false;
+			float4 uv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 			if (flags & PF_TRIANGULAR_GEOMETRY)
 			{
-				shadingFrame(sc, mat, it, rayD, frame, lastNormal);
-				skipped = alphaSkipped(mat, pathQrngT<JOBS>(sc, w, s, p, depth));
+				shadingFrame<TEX>(sc, mat, it, rayD, frame, lastNormal, uv);
+				skipped = alphaSkipped<TEX>(sc, mat, uv, pathQrngT<JOBS>(sc, w, s, p, depth));
 			}
 			if (w.cached)
 			{
 				if (!skipped && (flags & PF_TRIANGULAR_GEOMETRY))
 				{
-					const Surface sf = surfaceOf(mat);
+					const Surface sf = surfaceAt<TEX>(sc, mat, uv);
 					const bool rough = (sf.metalness == 0.0f && sf.transmission == 0.0f) || sf.roughness >= w.minRoughness;
 					if (depth == 0 && it.lightType == kLightTypeTriangle) flags |= kPathLitPrefix;
 					if (cacheVertex(s, w, sc.status, p, flags, rayO, rayD, bxdfPdf, it.hitPos, it.gn, lastNormal,
@@ -606,6 +720,7 @@ __global__ void __launch_bounds__(kThreads, RB_SURFACE_MIN_BLOCKS) kSurface(cons
 				s.sfB[r] = f4_of(frame.b, 0.0f);
 				s.sfN[r] = f4_of(lastNormal, 0.0f);
 				s.sfL[r] = s.lambda[p];
+				if (TEX && mat.textures) s.sfUV[r] = uv;
 			}
 			++records;
 		}
@@ -666,7 +781,7 @@ __global__ void __launch_bounds__(kThreads) kEmission(const __grid_constant__ De
 // body below), so a warp's lanes take the same branch of the light choice
 // and read their records densely; the body is the same for both.
 // JOBS (a shared wavefront; never with SHARED): each record's tree is its job's.
-template<bool SHARED, bool JOBS>
+template<bool SHARED, bool JOBS, bool TEX>
 __global__ void __launch_bounds__(SHARED ? kNeeSharedThreads : kThreads, SHARED ? 2 : RB_NEE_MIN_BLOCKS)
 kNee(const __grid_constant__ DevScene scK, PathSoA s, WaveParams w, int bounce, int which)
 {
@@ -706,7 +821,7 @@ kNee(const __grid_constant__ DevScene scK, PathSoA s, WaveParams w, int bounce, 
 		else
 		{
 			const DevMaterial& mat = sc.materials[__float_as_uint(hp.w)];
-			const bool canTransmit = surfaceOf(mat).transmission != 0.0f;
+			const bool canTransmit = surfaceAt<TEX>(sc, mat, (TEX && mat.textures) ? s.sfUV[rec] : make_float4(0.0f, 0.0f, 0.0f, 0.0f)).transmission != 0.0f;
 			const Qrng q = pathQrngT<JOBS>(sc, w, s, p, sfDepth(bits));
 			const f3 r = sample3D(q, DIM_LIGHT);
 			const bool tri = (bits & kSfTriangle) != 0;
@@ -737,8 +852,7 @@ kNee(const __grid_constant__ DevScene scK, PathSoA s, WaveParams w, int bounce, 
 				// the reference overwrites the flag set above here (pathtrace.cu:1633)
 				occluded = lCos <= 0.0f;
 				lightPdf = (1.0f / area) * d2 / lCos;
-				const DevMaterial& em = sc.materials[et.material];
-				spectrum = rgbToSpectrum(sc.spectra.basis, mk(em.emissive[0], em.emissive[1], em.emissive[2]), lambda);
+				spectrum = rgbToSpectrum(sc.spectra.basis, emissionAt<TEX>(sc, et, u, v), lambda);
 			}
 			else if (type == kLightTypeSky)
 			{
@@ -765,7 +879,7 @@ kNee(const __grid_constant__ DevScene scK, PathSoA s, WaveParams w, int bounce, 
 // light's spectrum in the record; a light sample that gets none is marked
 // occluded, so the next stage queues no shadow ray for it. Split from the
 // BxDF sample (stage 3b) so neither kernel holds both parts' registers.
-template<bool JOBS>
+template<bool JOBS, bool TEX>
 __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdfLight(const __grid_constant__ DevScene scK, PathSoA s,
 	WaveParams w, int bounce)
 {
@@ -795,7 +909,8 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdfLight(const
 		dl.pdf = dd.w;
 		dl.occluded = false;
 		const Frame frame{ f3_of(s.sfT[i]), f3_of(s.sfB[i]), f3_of(s.sfN[i]) };
-		evalBxdf<kBxdfLight>(sc, mat, dl, pathQrngT<JOBS>(sc, w, s, p, fd.y), frame, surfaceOf(mat), st);
+		evalBxdf<kBxdfLight>(sc, mat, dl, pathQrngT<JOBS>(sc, w, s, p, fd.y), frame,
+			(TEX && mat.textures) ? surfaceAt<TEX>(sc, mat, s.sfUV[i]) : surfaceOf(mat), st);
 		if (st.hasNee) s.shC[i] = f4(st.nee);
 		else reinterpret_cast<float*>(s.sfPi + i)[3] = __uint_as_float(bits | kSfOccluded);
 	}
@@ -805,7 +920,7 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdfLight(const
 // pathtrace.cu:773-905 / :521-547), Russian roulette, the next ray and the
 // depth limits (:1736-1785). Continuing paths go to the next extend queue,
 // light samples that passed stage 3a to the shadow queue.
-template<bool JOBS>
+template<bool JOBS, bool TEX>
 __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(const __grid_constant__ DevScene scK, PathSoA s,
 	WaveParams w, int bounce)
 {
@@ -846,7 +961,8 @@ __global__ void __launch_bounds__(kThreads, RB_BSDF_MIN_BLOCKS) kBsdf(const __gr
 			LightSample dl;
 			dl.occluded = true;      // not read by the sample part
 			const Frame frame{ f3_of(s.sfT[i]), f3_of(s.sfB[i]), f3_of(s.sfN[i]) };
-			evalBxdf<kBxdfSample>(sc, mat, dl, q, frame, surfaceOf(mat), st);
+			evalBxdf<kBxdfSample>(sc, mat, dl, q, frame,
+				(TEX && mat.textures) ? surfaceAt<TEX>(sc, mat, s.sfUV[i]) : surfaceOf(mat), st);
 			hasShadow = !(bits & kSfOccluded) && !(st.flags & PF_PATH_TERMINATED);
 		}
 		flags = st.flags;
@@ -1177,13 +1293,15 @@ LaunchShape queryLaunchShape()
 	};
 	ls.threads = kThreads;
 	ls.blocksGenerate = occ(reinterpret_cast<const void*>(kGenerate<false>));
-	ls.blocksSurface = occ(reinterpret_cast<const void*>(kSurface<false>));
-	ls.blocksNee = occ(reinterpret_cast<const void*>(kNee<false, false>));
+	ls.blocksSurface = occ(reinterpret_cast<const void*>(kSurface<false, false>));
+	ls.blocksNee = occ(reinterpret_cast<const void*>(kNee<false, false, false>));
 	ls.blocksEmission = occ(reinterpret_cast<const void*>(kEmission<false>));
-	cudaFuncSetAttribute(reinterpret_cast<const void*>(kNee<true, false>), cudaFuncAttributeMaxDynamicSharedMemorySize,
+	cudaFuncSetAttribute(reinterpret_cast<const void*>(kNee<true, false, false>), cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(kNeeSharedMaxBytes));
-	ls.blocksBsdf = occ(reinterpret_cast<const void*>(kBsdf<false>));
-	ls.blocksBsdfLight = occ(reinterpret_cast<const void*>(kBsdfLight<false>));
+	cudaFuncSetAttribute(reinterpret_cast<const void*>(kNee<true, false, true>), cudaFuncAttributeMaxDynamicSharedMemorySize,
+		static_cast<int>(kNeeSharedMaxBytes));
+	ls.blocksBsdf = occ(reinterpret_cast<const void*>(kBsdf<false, false>));
+	ls.blocksBsdfLight = occ(reinterpret_cast<const void*>(kBsdfLight<false, false>));
 	ls.blocksResolve = occ(reinterpret_cast<const void*>(kResolve<false>));
 	queryTraceShape(ls);
 	return ls;
@@ -1201,8 +1319,13 @@ void launchSurface(const DevScene& sc, const PathSoA& s, const WaveParams& w, in
 	unsigned long long* counters)
 {
 	const int g = capBlocks(ls.blocksSurface, ls.items, kThreads);
-	if (s.jobs) kSurface<true><<<g, kThreads, 0, st>>>(sc, s, w, bounce, counters);
-	else kSurface<false><<<g, kThreads, 0, st>>>(sc, s, w, bounce, counters);
+	if (s.jobs)
+	{
+		if (w.textured) kSurface<true, true><<<g, kThreads, 0, st>>>(sc, s, w, bounce, counters);
+		else kSurface<true, false><<<g, kThreads, 0, st>>>(sc, s, w, bounce, counters);
+	}
+	else if (w.textured) kSurface<false, true><<<g, kThreads, 0, st>>>(sc, s, w, bounce, counters);
+	else kSurface<false, false><<<g, kThreads, 0, st>>>(sc, s, w, bounce, counters);
 }
 void launchEmission(const DevScene& sc, const PathSoA& s, int bounce, const LaunchShape& ls, cudaStream_t st)
 {
@@ -1210,42 +1333,58 @@ void launchEmission(const DevScene& sc, const PathSoA& s, int bounce, const Laun
 	if (s.jobs) kEmission<true><<<g, kThreads, 0, st>>>(sc, s, bounce);
 	else kEmission<false><<<g, kThreads, 0, st>>>(sc, s, bounce);
 }
-void launchNee(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
+template<bool TEX>
+void launchNeeT(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
 {
 	const int g = capBlocks(ls.blocksNee, ls.items, kThreads);
 	if (s.jobs)
 	{
-		kNee<false, true><<<g, kThreads, 0, st>>>(sc, s, w, bounce, 0);
-		kNee<false, true><<<g, kThreads, 0, st>>>(sc, s, w, bounce, 1);
+		kNee<false, true, TEX><<<g, kThreads, 0, st>>>(sc, s, w, bounce, 0);
+		kNee<false, true, TEX><<<g, kThreads, 0, st>>>(sc, s, w, bounce, 1);
 		return;
 	}
 	const size_t treeBytes = sizeof(TreeNodeU) * sc.lights.nodeCount;
 	if (sc.lights.unpacked && treeBytes <= kNeeSharedMaxBytes)
 	{
 		int b = 0;
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, reinterpret_cast<const void*>(kNee<true, false>), kNeeSharedThreads,
-			treeBytes);
-		kNee<true, false><<<capBlocks((b < 1 ? 1 : b) * ls.smCount, ls.items, kNeeSharedThreads), kNeeSharedThreads, treeBytes,
-			st>>>(sc, s, w, bounce, 0);
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, reinterpret_cast<const void*>(kNee<true, false, TEX>),
+			kNeeSharedThreads, treeBytes);
+		kNee<true, false, TEX><<<capBlocks((b < 1 ? 1 : b) * ls.smCount, ls.items, kNeeSharedThreads), kNeeSharedThreads,
+			treeBytes, st>>>(sc, s, w, bounce, 0);
 	}
 	else
 	{
-		kNee<false, false><<<g, kThreads, 0, st>>>(sc, s, w, bounce, 0);
+		kNee<false, false, TEX><<<g, kThreads, 0, st>>>(sc, s, w, bounce, 0);
 	}
-	kNee<false, false><<<g, kThreads, 0, st>>>(sc, s, w, bounce, 1);
+	kNee<false, false, TEX><<<g, kThreads, 0, st>>>(sc, s, w, bounce, 1);
+}
+void launchNee(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
+{
+	if (w.textured) launchNeeT<true>(sc, s, w, bounce, ls, st);
+	else launchNeeT<false>(sc, s, w, bounce, ls, st);
 }
 void launchBsdf(const DevScene& sc, const PathSoA& s, const WaveParams& w, int bounce, const LaunchShape& ls, cudaStream_t st)
 {
 	const int gl = capBlocks(ls.blocksBsdfLight, ls.items, kThreads), gs = capBlocks(ls.blocksBsdf, ls.items, kThreads);
-	if (s.jobs)
+	if (s.jobs && w.textured)
 	{
-		kBsdfLight<true><<<gl, kThreads, 0, st>>>(sc, s, w, bounce);
-		kBsdf<true><<<gs, kThreads, 0, st>>>(sc, s, w, bounce);
+		kBsdfLight<true, true><<<gl, kThreads, 0, st>>>(sc, s, w, bounce);
+		kBsdf<true, true><<<gs, kThreads, 0, st>>>(sc, s, w, bounce);
+	}
+	else if (s.jobs)
+	{
+		kBsdfLight<true, false><<<gl, kThreads, 0, st>>>(sc, s, w, bounce);
+		kBsdf<true, false><<<gs, kThreads, 0, st>>>(sc, s, w, bounce);
+	}
+	else if (w.textured)
+	{
+		kBsdfLight<false, true><<<gl, kThreads, 0, st>>>(sc, s, w, bounce);
+		kBsdf<false, true><<<gs, kThreads, 0, st>>>(sc, s, w, bounce);
 	}
 	else
 	{
-		kBsdfLight<false><<<gl, kThreads, 0, st>>>(sc, s, w, bounce);
-		kBsdf<false><<<gs, kThreads, 0, st>>>(sc, s, w, bounce);
+		kBsdfLight<false, false><<<gl, kThreads, 0, st>>>(sc, s, w, bounce);
+		kBsdf<false, false><<<gs, kThreads, 0, st>>>(sc, s, w, bounce);
 	}
 }
 void launchSetWaveDyn(uint32_t* dyn, uint32_t offset, uint32_t fresh, cudaStream_t st)

@@ -395,7 +395,7 @@ __device__ uint32_t findSplit(const Scratch& S, uint32_t b, uint32_t e, WarpBins
 
 __global__ void __launch_bounds__(kThreads, 1) kBuildLightTree(uint32_t n, const float* __restrict__ world,
 	const float* __restrict__ fluxIn, const uint32_t* __restrict__ material, const uint32_t* __restrict__ prim,
-	float camX, float camY, float camZ, double camXd, double camYd, double camZd, void* scratch,
+	const float* __restrict__ uvs, float camX, float camY, float camZ, double camXd, double camYd, double camZd, void* scratch,
 	EmissiveTri* __restrict__ tris, PackedNode* __restrict__ nodes, uint32_t* __restrict__ pointers,
 	uint64_t* __restrict__ masks, uint32_t* __restrict__ nodeCount)
 {
@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(kThreads, 1) kBuildLightTree(uint32_t n, const
 		S.idx[k] = k;
 		EmissiveTri& et = tris[k];
 		for (int j = 0; j < 9; ++j) et.v[j] = static_cast<float>(static_cast<double>(v[j]) - cam[j % 3]);
-		for (int j = 0; j < 6; ++j) et.uv[j] = 0.0f;
+		for (int j = 0; j < 6; ++j) et.uv[j] = uvs ? uvs[6 * static_cast<size_t>(k) + j] : 0.0f;
 		et.material = material[k];
 		et.prim = prim[k];
 	}
@@ -637,7 +637,7 @@ constexpr size_t kSmemBins = sizeof(WarpBins) * kWarps;
 extern "C" size_t rb_k_build_light_tree_scratch_bytes(uint32_t n) { return rb::ltg::scratchBytes(n); }
 
 extern "C" int rb_k_build_light_tree(uint32_t n, const float* world, const float* flux, const uint32_t* material,
-	const uint32_t* primitive, const double* camera, void* scratch, void* triangles, void* nodes, uint32_t* pointers,
+	const uint32_t* primitive, const float* uvs, const double* camera, void* scratch, void* triangles, void* nodes, uint32_t* pointers,
 	uint64_t* bitmasks, uint32_t* node_count, void* stream)
 {
 	if (!camera || !node_count) return RB_ERR_INVALID;
@@ -650,7 +650,7 @@ extern "C" int rb_k_build_light_tree(uint32_t n, const float* world, const float
 	if (cudaFuncSetAttribute(rb::ltg::kBuildLightTree, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			static_cast<int>(rb::ltg::kSmemBins)) != cudaSuccess)
 		return RB_ERR_CUDA;
-	rb::ltg::kBuildLightTree<<<1, rb::ltg::kThreads, rb::ltg::kSmemBins, st>>>(n, world, flux, material, primitive,
+	rb::ltg::kBuildLightTree<<<1, rb::ltg::kThreads, rb::ltg::kSmemBins, st>>>(n, world, flux, material, primitive, uvs,
 		static_cast<float>(camera[0]), static_cast<float>(camera[1]), static_cast<float>(camera[2]), camera[0], camera[1],
 		camera[2], scratch, static_cast<rb::EmissiveTri*>(triangles), static_cast<rb::PackedNode*>(nodes), pointers,
 		bitmasks, node_count);

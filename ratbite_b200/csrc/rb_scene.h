@@ -57,6 +57,21 @@ struct alignas(16) DevMaterial
 	const uint8_t* indices;
 	const uint8_t* attributeData;
 	uint32_t vertexCount;
+	uint32_t textures;           // RB_TEXTURE_* bits (TextureTypeBitfield)
+	uint32_t texSets;            // bit t: texture slot t reads texture coordinate set 2
+	uint32_t texcoordOffset[2];  // byte offsets of TEXCOORD_1 / TEXCOORD_2 in a vertex
+	uint16_t tex[8];             // texture table index per slot
+};
+
+// One texture of the material texture table (rb_set_textures).
+struct DevTexture
+{
+	const uint8_t* data;         // width x height texels, 1 or 4 bytes each
+	uint32_t width, height;
+	uint32_t channels;           // 1 (R8) or 4 (RGBA8)
+	uint32_t srgb;
+	uint32_t addrU, addrV;       // RB_TEXADDR_*
+	uint32_t filter;             // RB_TEXFILTER_*
 	uint32_t pad;
 };
 
@@ -193,6 +208,9 @@ struct DevScene
 	DevLaunch launch;
 	const DevMaterial* materials;
 	uint32_t materialCount;
+	uint32_t textureCount;
+	const DevTexture* textures;
+	const float* srgbLut;        // 256 entries: the sRGB decode of each 8-bit code
 	uint32_t* status;            // device status word (RB_DEV_* bits), [0] flags, [1] detail
 };
 } // namespace rb

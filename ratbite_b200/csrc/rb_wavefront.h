@@ -40,6 +40,7 @@ struct PathSoA
 	float4* sfB;       // shading frame bitangent
 	float4* sfN;       // shading normal (the path keeps its own copy in nrm for the next bounce)
 	float4* sfL;       // the path's hero wavelengths (a copy of lambda)
+	float4* sfUV;      // texture coordinates (sets 1 and 2), written for textured materials
 	uint32_t* queue[2];// active path slots, ping-pong by bounce parity
 	uint32_t* surfQueue;   // per record: its path slot
 	uint32_t* recOrder;    // records in order of arrival (both regions): the BxDF kernels take them in
@@ -158,6 +159,9 @@ struct WaveParams
 	const WaveChunk* chunks;
 	uint32_t nChunks;
 	uint32_t pixelSlots;
+	// 1: some material of the wave's scene(s) samples textures; the shading
+	// kernels then run their variants with the texture reads compiled in
+	uint32_t textured;
 };
 
 struct LaunchShape

@@ -51,11 +51,13 @@ def build_for_scene(scene, camera=(0.0, 0.0, 0.0)) -> abi.rb_light_tree | None:
     world, flux, mat, prim = scene.emissive_arrays()
     if len(flux) == 0:
         return None
-    return record(*build(world, flux, mat, prim, camera))
+    tris, nodes, ptrs, masks = build(world, flux, mat, prim, camera)
+    tris["uvs"] = scene.emissive_uvs()          # the triangles keep the input order
+    return record(tris, nodes, ptrs, masks)
 
 
 def build_on_device(world: np.ndarray, flux: np.ndarray, material: np.ndarray, primitive: np.ndarray,
-                    camera=(0.0, 0.0, 0.0), stream=None, timing: list | None = None):
+                    camera=(0.0, 0.0, 0.0), stream=None, timing: list | None = None, uvs=None):
     """The same records built on the device (rb_k_build_light_tree), copied
     back: (triangles, nodes, pointers, bitmasks). Inputs are uploaded from
     host arrays; with `timing`, the device milliseconds of the build (CUDA
@@ -67,6 +69,7 @@ def build_on_device(world: np.ndarray, flux: np.ndarray, material: np.ndarray, p
     f = dev(np.asarray(flux, np.float32))
     m = dev(np.asarray(material, np.uint32).view(np.int32))
     pr = dev(np.asarray(primitive, np.uint32).view(np.int32))
+    uv = None if uvs is None else dev(np.asarray(uvs, np.float32).reshape(n, 6))
     lib = load()
     scratch = torch.empty(max(int(lib.rb_k_build_light_tree_scratch_bytes(n)), 1), dtype=torch.uint8, device="cuda")
     tris = torch.zeros(max(n, 1) * 68, dtype=torch.uint8, device="cuda")
@@ -79,7 +82,8 @@ def build_on_device(world: np.ndarray, flux: np.ndarray, material: np.ndarray, p
     s = torch.cuda.current_stream() if stream is None else stream
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(s)
-    rc = lib.rb_k_build_light_tree(n, p(w), p(f), p(m), p(pr), C.c_void_p(cam.ctypes.data), p(scratch), p(tris),
+    rc = lib.rb_k_build_light_tree(n, p(w), p(f), p(m), p(pr), None if uv is None else p(uv),
+                                   C.c_void_p(cam.ctypes.data), p(scratch), p(tris),
                                    p(nodes), p(ptrs), p(masks), p(count), C.c_void_p(s.cuda_stream))
     b.record(s)
     if rc != 0:

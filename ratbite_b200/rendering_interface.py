@@ -78,6 +78,10 @@ class RenderingInterface:
         check(self.lib.rb_set_spectra(self.ctx, _ptr(s), _ptr(b), _ptr(e) if len(e) else None, len(e)),
               self.ctx, "rb_set_spectra")
 
+    def load_textures(self, records):
+        check(self.lib.rb_set_textures(self.ctx, C.cast(records, C.c_void_p), len(records)),
+              self.ctx, "rb_set_textures")
+
     def fill_model_materials(self, records):
         check(self.lib.rb_set_materials(self.ctx, C.cast(records, C.c_void_p), len(records)),
               self.ctx, "rb_set_materials")
@@ -109,6 +113,9 @@ class RenderingInterface:
         """Uploads a ratbite_b200.scenes.Scene (and its light tree records)."""
         self.load_look_up_tables(luts)
         self.fill_spectral_curves_data(sensor_xyz, basis_rgb, extra)
+        texs = scene.texture_records()
+        self._keep.append(texs)
+        self.load_textures(texs)
         mats = scene.material_records()
         self._keep.append(mats)
         self.fill_model_materials(mats)
@@ -125,17 +132,20 @@ class RenderingInterface:
         self._keep.append(launch)
         self.prepare_data_for_rendering(launch)
 
-    def build_lights(self, world, flux, material, primitive, stream=None):
+    def build_lights(self, world, flux, material, primitive, uvs=None, stream=None):
         """Builds the light tree on the device (rb_build_lights) from the
-        emissive triangles (host arrays, uploaded first) and installs it."""
+        emissive triangles (host arrays, uploaded first; `uvs`, (n, 6), the
+        emission texture's coordinates per triangle, e.g. Scene.emissive_uvs)
+        and installs it."""
         import torch
         n = len(flux)
         dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
-        bufs = (dev(np.asarray(world, np.float32).reshape(n, 9)), dev(np.asarray(flux, np.float32)),
-                dev(np.asarray(material, np.uint32).view(np.int32)), dev(np.asarray(primitive, np.uint32).view(np.int32)))
+        bufs = [dev(np.asarray(world, np.float32).reshape(n, 9)), dev(np.asarray(flux, np.float32)),
+                dev(np.asarray(material, np.uint32).view(np.int32)), dev(np.asarray(primitive, np.uint32).view(np.int32))]
+        uv = None if uvs is None else dev(np.asarray(uvs, np.float32).reshape(n, 6))
         torch.cuda.synchronize()
-        check(self.lib.rb_build_lights(self.ctx, n, *[C.c_void_p(b.data_ptr()) for b in bufs], stream), self.ctx,
-              "rb_build_lights")
+        ptrs = [C.c_void_p(b.data_ptr()) for b in bufs] + [None if uv is None else C.c_void_p(uv.data_ptr())]
+        check(self.lib.rb_build_lights(self.ctx, n, *ptrs, stream), self.ctx, "rb_build_lights")
 
     def update_instances(self, instance_transforms, subset_transforms=None, stream=None):
         """Moves the instances of the loaded geometry (the reference's

@@ -56,6 +56,53 @@ def oct_encode(n: np.ndarray) -> np.ndarray:
     return np.where((n[:, 2] <= 0)[:, None], folded, p).astype(np.float32)
 
 
+def frame_encode(normals: np.ndarray, tangents: np.ndarray) -> np.ndarray:
+    """Tangent frames as unit quaternions (x, y, z, w), the encoding the
+    reference uses for the FRAME vertex attribute
+    (src/core/rendering_interface.cpp:258-284): the rotation of the matrix
+    with columns (tangent, normal x tangent, normal) by the largest-diagonal
+    method (Shoemake's matrix-to-quaternion conversion, as glm::quat_cast
+    evaluates it), then signed so that w carries the sign of the tangent's
+    handedness (tangent.w); a w of zero becomes +0 or -0. float32 throughout."""
+    F = np.float32
+    n = np.asarray(normals, F)[:, :3]
+    t4 = np.asarray(tangents, F)
+    t = t4[:, :3]
+    b = np.stack([n[:, 1] * t[:, 2] - t[:, 1] * n[:, 2],
+                  n[:, 2] * t[:, 0] - t[:, 2] * n[:, 0],
+                  n[:, 0] * t[:, 1] - t[:, 0] * n[:, 1]], 1).astype(F)
+    m = np.stack([t, b, n], 1)                      # m[:, column, row]
+    d0, d1, d2 = m[:, 0, 0], m[:, 1, 1], m[:, 2, 2]
+    four = np.stack([(d0 + d1) + d2, (d0 - d1) - d2, (d1 - d0) - d2, (d2 - d0) - d1], 1).astype(F)
+    big = np.zeros(len(n), np.int64)
+    best = four[:, 0].copy()
+    for k in (1, 2, 3):                             # strictly greater, in order, as the reference's glm
+        take = four[:, k] > best
+        best = np.where(take, four[:, k], best)
+        big = np.where(take, k, big)
+    val = (np.sqrt((best + F(1.0)).astype(F)) * F(0.5)).astype(F)
+    mult = (F(0.25) / val).astype(F)
+    a12, a21 = m[:, 1, 2], m[:, 2, 1]
+    a20, a02 = m[:, 2, 0], m[:, 0, 2]
+    a01, a10 = m[:, 0, 1], m[:, 1, 0]
+    cand = {   # (w, x, y, z) per largest index
+        0: (val, (a12 - a21) * mult, (a20 - a02) * mult, (a01 - a10) * mult),
+        1: ((a12 - a21) * mult, val, (a01 + a10) * mult, (a20 + a02) * mult),
+        2: ((a20 - a02) * mult, (a01 + a10) * mult, val, (a12 + a21) * mult),
+        3: ((a01 - a10) * mult, (a20 + a02) * mult, (a12 + a21) * mult, val),
+    }
+    q = np.zeros((len(n), 4), F)                    # x, y, z, w
+    for k, (w, x, y, z) in cand.items():
+        sel = big == k
+        q[sel] = np.stack([x, y, z, w], 1).astype(F)[sel]
+    tw = t4[:, 3]
+    zero = q[:, 3] == 0.0
+    q[zero, 3] = np.where(tw[zero] > 0.0, F(0.0), F(-0.0))
+    flip = ~zero & (q[:, 3] * tw < 0.0)
+    q[flip] = -q[flip]
+    return q
+
+
 def icosphere(subdiv: int):
     """Unit icosphere: subdivision s gives 20*4^s triangles."""
     t = (1.0 + math.sqrt(5.0)) / 2.0
@@ -90,6 +137,27 @@ class Submesh:
     material: int
     normals: np.ndarray | None = None   # (V, 3) float32 shading normals
     discarded: list = field(default_factory=list)
+    texcoords: np.ndarray | None = None   # (V, 2) float32, texture coordinate set 1
+    texcoords2: np.ndarray | None = None  # (V, 2) float32, set 2
+    tangents: np.ndarray | None = None    # (V, 4) float32, xyz and handedness w (with normals: FRAME)
+
+
+@dataclass
+class Texture:
+    """An image with its sampler (rb_texture): (H, W, 4) or (H, W) uint8
+    texels, row 0 first; `srgb` decodes r, g, b (r of a one-channel image)
+    with the sRGB curve (the reference sets it for base-colour textures)."""
+    data: np.ndarray
+    srgb: bool = False
+    address: tuple = (abi.RB_TEXADDR_WRAP, abi.RB_TEXADDR_WRAP)
+    filter: int = abi.RB_TEXFILTER_LINEAR
+
+    def texel(self, x: int, y: int) -> np.ndarray:
+        """Raw 8-bit texel (4 channels; a one-channel image as (r, 0, 0, 255))."""
+        d = self.data
+        if d.ndim == 2:
+            return np.array([d[y, x], 0, 0, 255], np.uint8)
+        return d[y, x]
 
 
 @dataclass
@@ -112,6 +180,8 @@ class Material:
     alpha: float = 1.0
     alpha_cutoff: float = 0.0
     double_sided: bool = False
+    # texture slot (abi.RB_TEXTURE_*) -> (index into Scene.textures, coordinate set 1 or 2)
+    textures: dict = field(default_factory=dict)
 
 
 @dataclass
@@ -132,6 +202,7 @@ class Scene:
     cam_u: tuple = (1.0, 0.0, 0.0)
     cam_v: tuple = (0.0, 0.0, -1.0)
     cam_w: tuple = (0.0, 1.0, 0.0)
+    textures: list = field(default_factory=list)   # list[Texture]
     _keep: list = field(default_factory=list)
 
     # ---- counts ---------------------------------------------------------
@@ -143,10 +214,51 @@ class Scene:
 
     # ---- ABI records ----------------------------------------------------
     def _attr_buffer(self, sm: Submesh):
-        if sm.normals is None:
-            return None, 0, 0
-        enc = oct_encode(sm.normals)
-        return np.ascontiguousarray(enc, dtype=np.float32), 8, abi.RB_ATTR_NORMAL
+        """Interleaved vertex attributes in the reference's order
+        (src/core/rendering_interface.cpp:209-235): a tangent-frame
+        quaternion (16 bytes) when both normals and tangents are present,
+        else an octahedral normal (8 bytes), then texture coordinate sets 1
+        and 2 (8 bytes each), as present. Returns the buffer, the stride, the
+        RB_ATTR_* bits and the byte offsets of (normal or frame, set 1, set 2)."""
+        parts, bits, offs, off = [], 0, [0, 0, 0], 0
+        if sm.normals is not None and sm.tangents is not None:
+            parts.append(frame_encode(sm.normals, sm.tangents))
+            bits |= abi.RB_ATTR_FRAME
+            off = 16
+        elif sm.normals is not None:
+            parts.append(oct_encode(sm.normals).astype(np.float32))
+            bits |= abi.RB_ATTR_NORMAL
+            off = 8
+        for k, (arr, bit) in enumerate(((sm.texcoords, abi.RB_ATTR_TEX_COORD_1),
+                                        (sm.texcoords2, abi.RB_ATTR_TEX_COORD_2)), start=1):
+            if arr is None:
+                continue
+            parts.append(np.asarray(arr, np.float32).reshape(-1, 2))
+            bits |= bit
+            offs[k] = off
+            off += 8
+        if not parts:
+            return None, 0, 0, offs
+        return np.ascontiguousarray(np.concatenate(parts, axis=1), dtype=np.float32), off, bits, offs
+
+    def texture_records(self):
+        """One rb_texture per Scene.textures entry."""
+        recs = (abi.rb_texture * max(len(self.textures), 1))()
+        for i, t in enumerate(self.textures):
+            d = np.ascontiguousarray(t.data, np.uint8)
+            self._keep.append(d)
+            r = recs[i]
+            r.height, r.width = d.shape[0], d.shape[1]
+            r.format = abi.RB_TEXFMT_R8 if d.ndim == 2 else abi.RB_TEXFMT_RGBA8
+            if d.ndim == 3 and d.shape[2] != 4:
+                raise ValueError("textures are (H, W) or (H, W, 4) uint8")
+            r.srgb = 1 if t.srgb else 0
+            r.address_u, r.address_v = t.address
+            r.filter = t.filter
+            r.data = d.ctypes.data
+        self._keep.append(recs)
+        # an empty table still passes a valid pointer; its length is len(self.textures)
+        return recs if self.textures else (abi.rb_texture * 0)()
 
     def material_records(self):
         """One rb_material per submesh material slot."""
@@ -184,16 +296,22 @@ class Scene:
                 r.base_color = abi.F4(*m.base_color, m.alpha)
                 r.alpha_cutoff = m.alpha_cutoff
             r.factors = factors
+            for slot, (tex, coord_set) in m.textures.items():
+                r.textures |= 1 << slot
+                r.texture_index[slot] = tex
+                if coord_set == 2:
+                    r.texcoord_sets |= 1 << slot
             if sm is not None:
                 idx = np.ascontiguousarray(sm.indices)
                 self._keep.append(idx)
                 r.index_type = abi.RB_INDEX_U16 if idx.dtype == np.uint16 else abi.RB_INDEX_U32
                 r.triangle_count = len(idx)
                 r.indices = idx.ctypes.data
-                attr, stride, bits = self._attr_buffer(sm)
+                attr, stride, bits, offs = self._attr_buffer(sm)
                 r.attributes = bits
                 r.attribute_stride = stride
-                r.normal_offset = 0
+                r.normal_offset, r.texcoord1_offset, r.texcoord2_offset = offs
+                r.frame_offset = offs[0]
                 r.vertex_count = len(sm.vertices)
                 if attr is not None:
                     self._keep.append(attr)
@@ -256,6 +374,16 @@ class Scene:
         prim = np.concatenate([np.asarray(e["prim"], np.uint32) for e in self.emissive])
         return (np.ascontiguousarray(world), np.ascontiguousarray(flux),
                 np.ascontiguousarray(mat), np.ascontiguousarray(prim))
+
+    def emissive_uvs(self):
+        """Texture coordinates of the emissive triangles' vertices, (N, 6),
+        in the order of emissive_arrays (zero where an emitter has none): the
+        `uvs` of EmissiveTriangleLightData (src/core/light_tree_types.h:40-46)."""
+        if not self.emissive:
+            return np.zeros((0, 6), np.float32)
+        return np.ascontiguousarray(np.concatenate(
+            [np.asarray(e["uv"], np.float32).reshape(-1, 6) if e.get("uv") is not None
+             else np.zeros((len(e["prim"]), 6), np.float32) for e in self.emissive]))
 
     def launch_record(self, width=None, height=None, max_depth=None):
         w = width or self.width
@@ -590,3 +718,144 @@ def cornell_box(seed: int = 1, cie_xyz: np.ndarray | None = None, light_scale: f
     return Scene(name="cornell_box", seed=seed, meshes=meshes, instances=instances,
                  materials=materials, emissive=emissive, width=width, height=height,
                  spp=spp, max_depth=max_depth)
+
+
+def _checker(n: int, cells: int, a, b, alpha_a: int = 255, alpha_b: int = 255) -> np.ndarray:
+    """(n, n, 4) uint8 checkerboard of `cells` x `cells` squares."""
+    y, x = np.mgrid[0:n, 0:n]
+    on = ((x * cells // n) + (y * cells // n)) % 2 == 0
+    img = np.zeros((n, n, 4), np.uint8)
+    img[on] = (*a, alpha_a)
+    img[~on] = (*b, alpha_b)
+    return img
+
+
+def textured_cornell(seed: int = 1, cie_xyz: np.ndarray | None = None, light_scale: float = 12.0,
+                     width: int = 128, height: int = 128, spp: int = 16, max_depth: int = 8) -> Scene:
+    """Cornell box with material textures on every surface kind the shading
+    step samples (src/kernels/pathtrace.cu:1217-1228, 1437-1560, 1640-1650):
+    base colour (sRGB, nearest and bilinear filtering, wrap / mirror / clamp
+    addressing, coordinates beyond [0, 1]), alpha cutout from the base-colour
+    alpha, a normal map, metal-roughness, transmission, sheen colour and
+    roughness read from texture coordinate set 2, a one-channel texture, and
+    an emissive texture on the light (its flux scaled by the texture's mean
+    emission). Procedural textures from PCG32(seed)."""
+    rng = PCG32(seed)
+    cz = -3.2
+    x0, x1, y0, y1, z0, z1 = -1.0, 1.0, -1.0, 1.0, cz - 1.0, cz + 1.0
+    n = 32
+    yy, xx = np.mgrid[0:n, 0:n]
+    # textures
+    tex: list[Texture] = []
+
+    def add(t: Texture) -> int:
+        tex.append(t)
+        return len(tex) - 1
+
+    col = lambda: tuple(int(rng.uniform(40, 230)) for _ in range(3))
+    t_floor = add(Texture(_checker(n, 8, col(), col()), srgb=True, filter=abi.RB_TEXFILTER_NEAREST))
+    mr = np.zeros((n, n, 4), np.uint8)
+    mr[..., 1] = (60 + 190 * (xx / (n - 1))).astype(np.uint8)           # roughness
+    mr[..., 2] = np.where((yy // 8) % 2 == 0, 0, 200).astype(np.uint8)  # metalness stripes
+    mr[..., 3] = 255
+    t_mr = add(Texture(mr))
+    t_back = add(Texture(_checker(n, 4, col(), col()), srgb=True,
+                         address=(abi.RB_TEXADDR_MIRROR, abi.RB_TEXADDR_MIRROR)))
+    ph = 2.0 * math.pi * 3.0 * xx / n
+    nm = np.zeros((n, n, 4), np.uint8)
+    nm[..., 0] = np.clip(127.5 + 100.0 * np.sin(ph), 0, 255).astype(np.uint8)
+    nm[..., 1] = 128
+    nm[..., 2] = np.clip(127.5 + 127.0 * np.sqrt(np.clip(1.0 - (100.0 / 127.5 * np.sin(ph)) ** 2, 0.0, 1.0)),
+                         0, 255).astype(np.uint8)
+    nm[..., 3] = 255
+    t_normal = add(Texture(nm))
+    t_cut = add(Texture(_checker(n, 6, col(), col(), 255, 0), srgb=True,
+                        address=(abi.RB_TEXADDR_CLAMP, abi.RB_TEXADDR_CLAMP)))
+    t_gray = add(Texture(((xx + yy) * (255 // (2 * n - 2))).astype(np.uint8), srgb=True))   # one channel
+    shc = _checker(n, 2, col(), col())
+    t_shc = add(Texture(shc))
+    shr = np.zeros((n, n, 4), np.uint8)
+    shr[..., 3] = (50 + 200 * (yy / (n - 1))).astype(np.uint8)
+    t_shr = add(Texture(shr))
+    tr = ((xx // 4) % 2 * 255).astype(np.uint8)
+    t_tr = add(Texture(tr, address=(abi.RB_TEXADDR_WRAP, abi.RB_TEXADDR_CLAMP)))
+    em = np.zeros((n, n, 4), np.uint8)
+    em[..., 0] = (128 + 127 * np.cos(2 * math.pi * xx / n)).astype(np.uint8)
+    em[..., 1] = 200
+    em[..., 2] = (128 + 127 * np.sin(2 * math.pi * yy / n)).astype(np.uint8)
+    em[..., 3] = 255
+    t_em = add(Texture(em))
+
+    materials: list[Material] = []
+    walls: list[Submesh] = []
+    S = abi
+    quads = [
+        (((x0, y0, z1), (x1, y0, z1), (x1, y0, z0), (x0, y0, z0)), 3.0,     # floor: checker (nearest) + metal-rough
+         Material(base_color=(1.0, 1.0, 1.0), metalness=1.0, roughness=0.8,
+                  textures={S.RB_TEXTURE_BASE_COLOR: (t_floor, 1), S.RB_TEXTURE_MET_ROUGH: (t_mr, 1)})),
+        (((x0, y1, z0), (x1, y1, z0), (x1, y1, z1), (x0, y1, z1)), 1.0,     # ceiling: sheen textures on set 2
+         Material(base_color=(0.7, 0.7, 0.7), sheen_color=(1.0, 1.0, 1.0), sheen_roughness=0.6,
+                  textures={S.RB_TEXTURE_SHEEN_COLOR: (t_shc, 2), S.RB_TEXTURE_SHEEN_ROUGH: (t_shr, 2)})),
+        (((x0, y0, z0), (x1, y0, z0), (x1, y1, z0), (x0, y1, z0)), 2.5,     # back: mirror-addressed colour + normal map
+         Material(base_color=(0.9, 0.9, 0.9),
+                  textures={S.RB_TEXTURE_BASE_COLOR: (t_back, 1), S.RB_TEXTURE_NORMAL: (t_normal, 1)})),
+        (((x0, y0, z1), (x0, y0, z0), (x0, y1, z0), (x0, y1, z1)), 1.0,     # left: one-channel colour texture
+         Material(textures={S.RB_TEXTURE_BASE_COLOR: (t_gray, 1)})),
+        (((x1, y0, z0), (x1, y0, z1), (x1, y1, z1), (x1, y1, z0)), 1.2,     # right: alpha cutout (clamp)
+         Material(base_color=(1.0, 1.0, 1.0), factors=S.RB_FACTOR_BASE_COLOR | S.RB_FACTOR_CUTOFF, alpha=1.0,
+                  alpha_cutoff=0.5, textures={S.RB_TEXTURE_BASE_COLOR: (t_cut, 1)})),
+    ]
+    quad_uv = lambda s: np.array([[0.0, 0.0], [s, 0.0], [s, s], [0.0, s]], np.float32)
+    for q, scale, mat in quads:
+        materials.append(mat)
+        v, i = _quad(*q)
+        uv = quad_uv(scale)
+        walls.append(Submesh(v, i, len(materials) - 1, texcoords=uv - 0.13 * scale,
+                             texcoords2=(uv * 0.5 + 0.25).astype(np.float32)))
+    rgb = np.array([1.0, 0.97, 0.93]) if cie_xyz is None else blackbody_rgb(6500.0, cie_xyz)
+    emissive_rgb = tuple(float(np.float32(c * light_scale)) for c in rgb)
+    ly = y1 - 1e-3
+    lq = ((-0.25, ly, cz - 0.25), (0.25, ly, cz - 0.25), (0.25, ly, cz + 0.25), (-0.25, ly, cz + 0.25))
+    materials.append(Material(base_color=(0.78, 0.78, 0.78), emissive=emissive_rgb,
+                              textures={S.RB_TEXTURE_EMISSION: (t_em, 1)}))
+    lv, li = _quad(*lq)
+    luv = quad_uv(2.0)
+    light_sub = Submesh(lv, li, len(materials) - 1, discarded=[0, 1], texcoords=luv)
+    walls.append(light_sub)
+
+    sv, sf = icosphere(3)
+    sph_uv = np.stack([np.arctan2(sv[:, 0], sv[:, 2]) / (2 * math.pi) + 0.5,
+                       np.arccos(np.clip(sv[:, 1], -1.0, 1.0)) / math.pi], axis=1).astype(np.float32)
+    spheres = []
+    for (cx, cy, czz, r), kind in (((-0.45, -0.6, cz - 0.3, 0.4), "metal"), ((0.45, -0.6, cz + 0.35, 0.4), "glass")):
+        if kind == "metal":
+            materials.append(Material(base_color=(0.9, 0.8, 0.6), metalness=1.0, roughness=0.5,
+                                      textures={S.RB_TEXTURE_BASE_COLOR: (t_back, 1), S.RB_TEXTURE_MET_ROUGH: (t_mr, 1)}))
+        else:
+            materials.append(Material(base_color=(1.0, 1.0, 1.0), metalness=0.0, roughness=0.05,
+                                      transmission=1.0, ior=1.5,
+                                      textures={S.RB_TEXTURE_TRANSMISSION: (t_tr, 1)}))
+        pos = (sv * r + np.array([cx, cy, czz])).astype(np.float32)
+        v4 = np.concatenate([pos, np.zeros((len(pos), 1), np.float32)], axis=1)
+        spheres.append([Submesh(v4, sf.astype(np.uint16), len(materials) - 1, normals=sv.astype(np.float32),
+                                texcoords=sph_uv)])
+
+    # emissive subset: the light quad's triangles, their texture coordinates,
+    # and flux = mean factor x mean texture emission x area x pi
+    tris_obj = np.stack([lv[li[k], :3].reshape(9) for k in range(2)]).astype(np.float32)
+    tri_uv = np.stack([luv[li[k]].reshape(6) for k in range(2)]).astype(np.float32)
+    e = em.astype(np.float64) / 255.0
+    mean_em = float(np.mean((e[..., 0] + e[..., 1] + e[..., 2]) * e[..., 3] / 3.0))
+    flux = []
+    for k in range(2):
+        a, b, c = tris_obj[k, 0:3], tris_obj[k, 3:6], tris_obj[k, 6:9]
+        area2 = np.linalg.norm(np.cross((b - a).astype(np.float32), (c - a).astype(np.float32)).astype(np.float32))
+        f = np.float32((np.float32(emissive_rgb[0]) + np.float32(emissive_rgb[1]) + np.float32(emissive_rgb[2])) / np.float32(3.0))
+        f = np.float32(f * np.float32(mean_em))
+        flux.append(np.float32(f * (np.float32(area2) * np.float32(0.5) * np.float32(math.pi))))
+    emissive = [dict(transform=IDENTITY, tris=tris_obj, world=tris_obj.copy(), prim=[0, 1],
+                     flux=np.array(flux, np.float32), material=light_sub.material, uv=tri_uv)]
+    meshes = [walls, spheres[0], spheres[1]]
+    instances = [(0, IDENTITY), (1, IDENTITY), (2, IDENTITY)]
+    return Scene(name="textured_cornell", seed=seed, meshes=meshes, instances=instances, materials=materials,
+                 emissive=emissive, width=width, height=height, spp=spp, max_depth=max_depth, textures=tex)

@@ -46,6 +46,7 @@ class RefLib:
             ("rbref_set_spectra", C.c_int, [_P, _P, _P, _U32]),
             ("rbref_set_luts", C.c_int, [_P] * 6),
             ("rbref_set_materials", C.c_int, [_P, _U32]),
+            ("rbref_set_textures", C.c_int, [_P, _U32]),
             ("rbref_set_geometry", C.c_int, [_P]),
             ("rbref_set_lights", C.c_int, [_P]),
             ("rbref_set_envmap", C.c_int, [_P, _U32, _U32, _P, _P, C.c_float]),
@@ -156,6 +157,9 @@ def load_scene_into_ref(ref: RefLib, scene, luts: dict, cie, basis, extra=None, 
                    "reflective_inner", "sheen")]
     keep += lut_arrays
     L.rbref_set_luts(*[_np_ptr(a) for a in lut_arrays])
+    texs = scene.texture_records()
+    keep.append(texs)
+    assert L.rbref_set_textures(C.cast(texs, C.c_void_p), len(texs)) == 0
     mats = scene.material_records()
     assert L.rbref_set_materials(C.cast(mats, C.c_void_p), len(mats)) == 0
     g = scene.geometry_record()
@@ -163,6 +167,7 @@ def load_scene_into_ref(ref: RefLib, scene, luts: dict, cie, basis, extra=None, 
     world, flux, mat, prim = scene.emissive_arrays()
     if len(flux):
         tris, nodes, ptrs, masks = ref.build_light_tree(world, flux, mat, prim)
+        tris["uvs"] = scene.emissive_uvs()
         lt = light_tree_record(tris, nodes, ptrs, masks, keep)
         L.rbref_set_lights(C.byref(lt))
     env = getattr(scene, "envmap", None)

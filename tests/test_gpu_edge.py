@@ -140,10 +140,12 @@ def test_rejections_leave_the_context_usable(tables):
     assert lib.rb_set_materials(ctx, C.cast(mats, C.c_void_p), 2) == 0
     assert lib.rb_render(ctx, 0, 1, None) == abi.RB_ERR_INVALID
     assert lib.rb_set_materials(ctx, C.cast(mats, C.c_void_p), len(mats)) == 0
-    # textured material, unknown BxDF
+    # a texture index beyond the (empty) texture table, an unknown texture slot, unknown BxDF
     m1 = (abi.rb_material * 1).from_buffer_copy(bytes(mats)[:C.sizeof(abi.rb_material)])
     m1[0].textures = 1
-    assert lib.rb_set_materials(ctx, C.cast(m1, C.c_void_p), 1) == abi.RB_ERR_UNSUPPORTED
+    assert lib.rb_set_materials(ctx, C.cast(m1, C.c_void_p), 1) == abi.RB_ERR_INVALID
+    m1[0].textures = 1 << abi.RB_TEXTURE_SLOTS
+    assert lib.rb_set_materials(ctx, C.cast(m1, C.c_void_p), 1) == abi.RB_ERR_INVALID
     m1[0].textures = 0
     m1[0].bxdf = 7
     assert lib.rb_set_materials(ctx, C.cast(m1, C.c_void_p), 1) == abi.RB_ERR_INVALID

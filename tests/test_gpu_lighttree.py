@@ -87,15 +87,17 @@ def test_device_tree_structure(which):
             base[:] = base[0]                              # 100 copies of one triangle: no plane separates them
         world, flux = base, rng.uniform(0.5, 2.0, n).astype(np.float32)
         mat, prim = np.zeros(n, np.uint32), np.arange(n, dtype=np.uint32)
-    tris, nodes, ptrs, masks = lighttree.build_on_device(world, flux, mat, prim, camera=(0.25, -0.5, 1.0))
+    uvs = np.random.default_rng(4).uniform(-2, 3, (len(flux), 6)).astype(np.float32)
+    tris, nodes, ptrs, masks = lighttree.build_on_device(world, flux, mat, prim, camera=(0.25, -0.5, 1.0), uvs=uvs)
     n = len(flux)
     _check_structure(n, flux, tris, nodes, ptrs, masks)
+    assert np.array_equal(tris["uvs"].reshape(n, 6), uvs)        # emission-texture coordinates, in input order
     # triangles are the inputs, camera-relative, with their material and primitive
     v = tris["vertices"].reshape(n, 3, 3).astype(np.float64)
     assert np.allclose(v + np.array([0.25, -0.5, 1.0]), np.asarray(world, np.float64).reshape(n, 3, 3), atol=1e-5)
     assert np.array_equal(tris["material"], mat) and np.array_equal(tris["prim"], prim)
     # deterministic: a second build gives the same bytes
-    again = lighttree.build_on_device(world, flux, mat, prim, camera=(0.25, -0.5, 1.0))
+    again = lighttree.build_on_device(world, flux, mat, prim, camera=(0.25, -0.5, 1.0), uvs=uvs)
     for a, b in zip((tris, nodes, ptrs, masks), again):
         assert a.tobytes() == b.tobytes()
 

@@ -1,0 +1,125 @@
+"""Material textures (rb_set_textures; the reference's tex2D reads of
+base colour, alpha, normal, metal-roughness, transmission, sheen colour and
+roughness, and emission: src/kernels/pathtrace.cu:1217-1228, 1437-1560,
+1640-1650) against the oracle, which runs the reference's own shading code
+with its texture objects backed by the same texels.
+
+The scene exercises sRGB decoding, nearest and bilinear filtering, wrap /
+mirror / clamp addressing with coordinates beyond [0, 1], an alpha cutout,
+texture coordinate set 2, a one-channel texture and a textured emitter hit
+by camera rays and picked by light sampling."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from gpu_util import assert_image_parity
+from oracle_lib import RefLib, light_tree_record, load_scene_into_ref, ref_render, reference_luts
+from ratbite_b200 import abi, lighttree, scenes
+from ratbite_b200._native import NativeError
+from ratbite_b200.rendering_interface import RenderingInterface
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ref():
+    return RefLib()
+
+
+@pytest.fixture(scope="module")
+def tables(ref):
+    return dict(cie=ref.cie_xyz(), basis=ref.basis_rgb(), luts=reference_luts())
+
+
+def test_textured_render_matches_oracle(ref, tables):
+    sc = scenes.textured_cornell(seed=3, cie_xyz=tables["cie"], width=64, height=64, spp=16, max_depth=8)
+    W, H, spp = 64, 64, 16
+    keep = load_scene_into_ref(ref, sc, tables["luts"], tables["cie"], tables["basis"])
+    want = ref_render(ref, W, H, 0, spp)
+    lt = lighttree.build_for_scene(sc)
+    with RenderingInterface(device=0) as ri:
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lt)
+        ri.render(0, spp)
+        got = ri.read_accumulation()
+        assert ri.status().flags == 0
+    assert (got[..., 3] == spp).all()
+    assert_image_parity(f"textured cornell {W}x{H}x{spp}", got, want)
+    # the textures are seen: the same scene without them renders a different image
+    plain = scenes.textured_cornell(seed=3, cie_xyz=tables["cie"], width=64, height=64, spp=16, max_depth=8)
+    for m in plain.materials:
+        m.textures = {}
+    with RenderingInterface(device=0) as ri:
+        ri.load_scene(plain, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(plain))
+        ri.render(0, spp)
+        other = ri.read_accumulation()
+    assert np.mean(np.abs(other[..., :3] - got[..., :3])) > 1e-2 * np.mean(np.abs(got[..., :3]))
+
+
+def test_textured_render_other_sample_range(ref, tables):
+    """Another Sobol range and a second seed's textures (other colours)."""
+    sc = scenes.textured_cornell(seed=8, cie_xyz=tables["cie"], width=48, height=40, spp=8, max_depth=6)
+    keep = load_scene_into_ref(ref, sc, tables["luts"], tables["cie"], tables["basis"])
+    launch = sc.launch_record()
+    assert ref.lib.rbref_set_launch(C.byref(launch)) == 0
+    want = ref_render(ref, 48, 40, 1000, 8)
+    with RenderingInterface(device=0) as ri:
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(sc))
+        ri.clear_accumulation()
+        ri.render(1000, 8)
+        got = ri.read_accumulation()
+        assert ri.status().flags == 0
+    assert_image_parity("textured cornell 48x40, samples [1000, 1008)", got, want)
+
+
+def test_texture_tables_are_checked(tables):
+    sc = scenes.textured_cornell(seed=3, width=16, height=16, spp=1)
+    with RenderingInterface(device=0) as ri:
+        # a material that names a texture beyond the table
+        ri.load_textures((abi.rb_texture * 0)())
+        with pytest.raises(NativeError):
+            ri.fill_model_materials(sc.material_records())
+        # malformed textures
+        bad = (abi.rb_texture * 1)()
+        img = np.zeros((4, 4, 4), np.uint8)
+        bad[0].width, bad[0].height, bad[0].format, bad[0].data = 4, 4, 7, img.ctypes.data
+        with pytest.raises(NativeError):
+            ri.load_textures(bad)
+        bad[0].format, bad[0].address_u = abi.RB_TEXFMT_RGBA8, 9
+        with pytest.raises(NativeError):
+            ri.load_textures(bad)
+        bad[0].address_u, bad[0].filter = 0, 4
+        with pytest.raises(NativeError):
+            ri.load_textures(bad)
+        # a valid table, then materials that use it, then a smaller table: the render refuses
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(sc))
+        ri.load_textures((abi.rb_texture * 0)())
+        with pytest.raises(NativeError):
+            ri.render(0, 1)
+
+
+def test_device_tree_samples_the_emission_texture(tables):
+    """The light tree built on the device carries the emitters' texture
+    coordinates (rb_build_lights' uvs): its image matches the host-built
+    tree's up to sampling noise (a tree without them would read the emission
+    texture at (0, 0) in light sampling)."""
+    sc = scenes.textured_cornell(seed=3, cie_xyz=tables["cie"], width=48, height=48, spp=64, max_depth=4)
+    out = []
+    for device in (False, True):
+        with RenderingInterface(device=0) as ri:
+            if device:
+                ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=None)
+                ri.build_lights(*sc.emissive_arrays(), uvs=sc.emissive_uvs())
+            else:
+                ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(sc))
+            ri.render(0, 256)
+            out.append(ri.read_accumulation())
+            assert ri.status().flags == 0
+    a, b = (o[..., :3] / o[..., 3:4] for o in out)
+    rel = abs(b.sum() - a.sum()) / a.sum()
+    d = (b - a)[..., 1].ravel()
+    z = d.mean() / (d.std() / np.sqrt(d.size))
+    print(f"textured emitters, device vs host tree: image mean rel diff {rel:.3e}, per-pixel difference z {z:.2f}")
+    assert rel < 1e-2 and abs(z) < 5.0
