@@ -191,8 +191,8 @@ def workload_config(scene, wl: dict, world: int, tables: str) -> dict:
             "envmap": list(scene.envmap.shape[1::-1]) if has_env else None,
             "paths_per_step": wl["width"] * wl["height"] * wl["spp"] * world,
             "parallelism": f"sample-range x{world}", "tables": tables,
-            "l2": "inputs larger than L2 (wavefront path state 372 B per path in flight, "
-                  "~6.2 GB at the default 16M paths per wave)"}
+            "l2": "inputs larger than L2 (wavefront path state 388 B per path in flight, "
+                  "~6.5 GB at the default 16M paths per wave)"}
 
 
 # ------------------------------------------------------------- CPU baseline

@@ -143,7 +143,9 @@ typedef struct rb_material {
     uint32_t sheen_present;
     uint32_t index_type;         /* RB_INDEX_U16 / RB_INDEX_U32 */
     uint32_t attributes;         /* RB_ATTR_* bits */
-    uint32_t attribute_stride;   /* bytes per vertex in attribute_data */
+    uint32_t attribute_stride;   /* bytes per vertex in attribute_data; it and the offsets of
+                                  * the fields present are multiples of 8 (the reference's
+                                  * packing: frame 16 B or normal 8 B, then 8 B per set) */
     uint32_t normal_offset, frame_offset, color_offset, texcoord1_offset, texcoord2_offset;
     uint32_t ior_spectrum;       /* index into the extra spectra (indexOfRefractSpectrumDataIndex) */
     uint32_t absorp_spectrum;    /* absorpCoefSpectrumDataIndex */

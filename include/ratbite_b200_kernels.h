@@ -174,6 +174,15 @@ int rb_k_build_light_tree(uint32_t n, const float* world, const float* flux, con
 int rb_k_generate_luts(uint32_t samples, float* conductor, float* dielectric_outer, float* dielectric_inner,
                        float* reflective_outer, float* reflective_inner, void* stream);
 
+/* Regenerates the sheen LTC table (the reference's bin/sheenLUT.bin, no
+ * generator shipped): per texel (x = cos theta_o = i / 31, at least 0.01;
+ * y = sheen roughness alpha = j / 31) the LTC coefficients A, B and the
+ * albedo R of a volumetric sheen layer simulated by random walks (`paths`
+ * per texel; definitions in rb_lut.cu), A and B fitted by maximum
+ * likelihood. Output: 32 x 32 float4 (A, B, R, 0) in device memory, the
+ * layout rb_set_luts takes. Stream-ordered. */
+int rb_k_generate_sheen_lut(uint32_t paths, float* sheen, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

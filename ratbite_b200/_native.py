@@ -67,6 +67,7 @@ SIGNATURES = {
     "rb_k_trace": (C.c_int, [_P, _U32, _P, _P, _P, _P, _P]),
     "rb_k_occluded": (C.c_int, [_P, _U32, _P, _P, _P, _P]),
     "rb_k_resolve": (C.c_int, [_U32, _U32, _P, C.c_float, _P, _P, _P]),
+    "rb_k_generate_sheen_lut": (C.c_int, [_U32, _P, _P]),
     "rb_k_generate_luts": (C.c_int, [_U32, _P, _P, _P, _P, _P, _P]),
     "rb_envmap_cdf_scratch_bytes": (C.c_size_t, [_U32, _U32]),
     "rb_envmap_cdf": (C.c_int, [_U32, _U32, _P, C.c_int, _P, _P, _P, _P, _P]),

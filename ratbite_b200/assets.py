@@ -114,10 +114,11 @@ def luts(n_mc: int = 256) -> dict:
                 reflective_outer=refl.reshape(-1), reflective_inner=refl.reshape(-1), sheen=sheen.reshape(-1))
 
 
-def generated_luts(samples: int = 1 << 14, device: int = 0) -> dict:
+def generated_luts(samples: int = 1 << 14, device: int = 0, sheen_paths: int = 1 << 18) -> dict:
     """The multiple-scattering tables regenerated on the GPU by Monte Carlo
-    integration of the BxDF lobes (rb_k_generate_luts); the sheen table is
-    the stand-in of luts() (an LTC fit, not an albedo)."""
+    integration of the BxDF lobes (rb_k_generate_luts), and the sheen LTC
+    table fitted to a simulated volumetric sheen layer
+    (rb_k_generate_sheen_lut)."""
     import ctypes as C
 
     import torch
@@ -127,11 +128,14 @@ def generated_luts(samples: int = 1 << 14, device: int = 0) -> dict:
     with torch.cuda.device(device):
         cond = torch.zeros(32 * 32, dtype=torch.float32, device="cuda")
         t3 = [torch.zeros(32 ** 3, dtype=torch.float32, device="cuda") for _ in range(4)]
+        sheen = torch.zeros(32 * 32 * 4, dtype=torch.float32, device="cuda")
         check(lib.rb_k_generate_luts(samples, C.c_void_p(cond.data_ptr()), *[C.c_void_p(t.data_ptr()) for t in t3],
                                      None), None, "rb_k_generate_luts")
+        check(lib.rb_k_generate_sheen_lut(sheen_paths, C.c_void_p(sheen.data_ptr()), None), None,
+              "rb_k_generate_sheen_lut")
         torch.cuda.synchronize()
     out = luts(n_mc=1)
     out.update(conductor=cond.cpu().numpy(), dielectric_outer=t3[0].cpu().numpy(),
                dielectric_inner=t3[1].cpu().numpy(), reflective_outer=t3[2].cpu().numpy(),
-               reflective_inner=t3[3].cpu().numpy())
+               reflective_inner=t3[3].cpu().numpy(), sheen=sheen.cpu().numpy())
     return out

@@ -616,6 +616,18 @@ int rb_set_materials(rb_ctx* ctx, const rb_material* mats, uint32_t count)
 		if (m.index_type > RB_INDEX_U32) return fail(ctx, RB_ERR_INVALID, "rb_set_materials: unknown index type");
 		if ((m.attributes & (RB_ATTR_NORMAL | RB_ATTR_FRAME)) && (!m.attribute_data || m.attribute_stride == 0))
 			return fail(ctx, RB_ERR_INVALID, "rb_set_materials: attributes declared without attribute data");
+		// the vertex layout the shading step reads with 8-byte loads: stride and
+		// field offsets multiples of 8, each field inside the vertex
+		if (m.attributes)
+		{
+			bool ok = m.attribute_stride % 8u == 0;
+			if (m.attributes & RB_ATTR_FRAME) ok = ok && m.frame_offset % 8u == 0 && m.frame_offset + 16u <= m.attribute_stride;
+			else if (m.attributes & RB_ATTR_NORMAL)
+				ok = ok && m.normal_offset % 8u == 0 && m.normal_offset + 8u <= m.attribute_stride;
+			if (m.attributes & RB_ATTR_TEX_COORD_1) ok = ok && m.texcoord1_offset % 8u == 0 && m.texcoord1_offset + 8u <= m.attribute_stride;
+			if (m.attributes & RB_ATTR_TEX_COORD_2) ok = ok && m.texcoord2_offset % 8u == 0 && m.texcoord2_offset + 8u <= m.attribute_stride;
+			if (!ok) return fail(ctx, RB_ERR_INVALID, "rb_set_materials: vertex attributes not at multiples of 8 bytes inside the stride");
+		}
 		if (m.triangle_count && !m.indices) return fail(ctx, RB_ERR_INVALID, "rb_set_materials: null indices");
 	}
 	cudaSetDevice(ctx->device);

@@ -146,6 +146,13 @@ RB_D void textureFrameInputs(const DevScene& sc, const DevMaterial& mat, uint32_
 // Shading frame and shadow-terminator offset (pathtrace.cu:1279-1461), and
 // the texture coordinates at the hit (x, y: set 1; z, w: set 2; zero where
 // the mesh has none), with the normal texture applied to the frame.
+// Four floats from an 8-byte-aligned address.
+RB_D float4 load8x2(const uint8_t* p)
+{
+	const float2 a = reinterpret_cast<const float2*>(p)[0], b = reinterpret_cast<const float2*>(p)[1];
+	return make_float4(a.x, a.y, b.x, b.y);
+}
+
 template<bool TEX>
 RB_D void shadingFrame(const DevScene& sc, const DevMaterial& mat, Interaction& it, f3 rayD, Frame& frame,
 	f3& lastNormal, float4& uv)
@@ -164,10 +171,12 @@ RB_D void shadingFrame(const DevScene& sc, const DevMaterial& mat, Interaction& 
 		const uint32_t stride = mat.attributeStride;
 		if (mat.attributes & RB_ATTR_FRAME)
 		{
+			// 8-byte loads: a frame sits at a multiple of 8 bytes (a 24-byte
+			// vertex, frame + one coordinate set, puts every other one off 16)
 			const uint8_t* at = base + mat.frameOffset;
-			const float4 q0 = *reinterpret_cast<const float4*>(at + stride * idx0);
-			const float4 q1 = *reinterpret_cast<const float4*>(at + stride * idx1);
-			const float4 q2 = *reinterpret_cast<const float4*>(at + stride * idx2);
+			const float4 q0 = load8x2(at + stride * idx0);
+			const float4 q1 = load8x2(at + stride * idx1);
+			const float4 q2 = load8x2(at + stride * idx2);
 			flipTangent = signbit(q0.w);
 			f3 t0, t1, t2;
 			quatColumns(q0, t0, n0);

@@ -149,6 +149,16 @@ def test_rejections_leave_the_context_usable(tables):
     m1[0].textures = 0
     m1[0].bxdf = 7
     assert lib.rb_set_materials(ctx, C.cast(m1, C.c_void_p), 1) == abi.RB_ERR_INVALID
+    # vertex attributes off the 8-byte grid, or outside the vertex
+    m1[0].bxdf = mats[0].bxdf
+    attr = np.zeros(64, np.float32)
+    m1[0].attribute_data, m1[0].vertex_count = attr.ctypes.data, 4
+    for bits, stride, offs in ((abi.RB_ATTR_FRAME, 20, (0, 0, 0)), (abi.RB_ATTR_NORMAL, 16, (12, 0, 0)),
+                               (abi.RB_ATTR_FRAME, 16, (8, 0, 0)), (abi.RB_ATTR_TEX_COORD_1, 8, (0, 4, 0))):
+        m1[0].attributes, m1[0].attribute_stride = bits, stride
+        m1[0].frame_offset = m1[0].normal_offset = offs[0]
+        m1[0].texcoord1_offset = offs[1]
+        assert lib.rb_set_materials(ctx, C.cast(m1, C.c_void_p), 1) == abi.RB_ERR_INVALID, (bits, stride, offs)
     # light tree whose child index points outside the node array
     world, flux, mat, prim = sc.emissive_arrays()
     tris, nodes, ptrs, masks = lighttree.build(world, flux, mat, prim)

@@ -103,23 +103,27 @@ def test_texture_tables_are_checked(tables):
 def test_device_tree_samples_the_emission_texture(tables):
     """The light tree built on the device carries the emitters' texture
     coordinates (rb_build_lights' uvs): its image matches the host-built
-    tree's up to sampling noise (a tree without them would read the emission
-    texture at (0, 0) in light sampling)."""
+    tree's (bit for bit when both builders make the same tree, as for this
+    scene's two emitters; else up to sampling noise), and a tree built
+    without them, which reads the emission texture at (0, 0) in light
+    sampling, renders a different image."""
     sc = scenes.textured_cornell(seed=3, cie_xyz=tables["cie"], width=48, height=48, spp=64, max_depth=4)
     out = []
-    for device in (False, True):
+    for mode in ("host", "device", "device without uvs"):
         with RenderingInterface(device=0) as ri:
-            if device:
-                ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=None)
-                ri.build_lights(*sc.emissive_arrays(), uvs=sc.emissive_uvs())
-            else:
+            if mode == "host":
                 ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(sc))
+            else:
+                ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=None)
+                ri.build_lights(*sc.emissive_arrays(), uvs=sc.emissive_uvs() if mode == "device" else None)
             ri.render(0, 256)
             out.append(ri.read_accumulation())
             assert ri.status().flags == 0
-    a, b = (o[..., :3] / o[..., 3:4] for o in out)
-    rel = abs(b.sum() - a.sum()) / a.sum()
+    a, b, c = (o[..., :3] / o[..., 3:4] for o in out)
     d = (b - a)[..., 1].ravel()
-    z = d.mean() / (d.std() / np.sqrt(d.size))
-    print(f"textured emitters, device vs host tree: image mean rel diff {rel:.3e}, per-pixel difference z {z:.2f}")
+    rel = abs(b.sum() - a.sum()) / a.sum()
+    z = 0.0 if d.std() == 0 else d.mean() / (d.std() / np.sqrt(d.size))
+    print(f"textured emitters, device vs host tree: image mean rel diff {rel:.3e}, per-pixel difference z {z:.2f}; "
+          f"without uvs: image mean rel diff {abs(c.sum() - a.sum()) / a.sum():.3e}")
     assert rel < 1e-2 and abs(z) < 5.0
+    assert np.abs(c - a).sum() > 1e-3 * np.abs(a).sum()
