@@ -118,8 +118,22 @@ typedef struct rb_config {
     uint32_t inject_queue_limit;
     uint32_t inject_alloc_failure;
     uint32_t inject_stack_limit;
-    uint32_t reserved;
+    uint32_t acceleration;       /* RB_ACCEL_FLAT (default, 0) or RB_ACCEL_INSTANCED */
 } rb_config;
+/* Ray-traversal structure built by rb_set_geometry. RB_ACCEL_FLAT: one BVH
+ * over every instance's triangles in world space (memory and instance
+ * updates scale with the instanced triangles). RB_ACCEL_INSTANCED: two
+ * levels, as the reference's GAS per mesh and IAS over instances
+ * (src/core/rendering_interface.cpp:733-848, 943-1064): one BVH per unique
+ * mesh and per emissive subset in object space, and a top-level BVH over
+ * the instances' world boxes that rb_update_instances rebuilds on the host
+ * (memory scales with the unique triangles, an instance update with the
+ * instance count). Both give bit-identical hits and images: rays enter
+ * object space for the box tests, and triangles are intersected in world
+ * space after the same transform the flat upload applies. The shared
+ * wavefront (rb_render_jobs) takes flat contexts only. */
+#define RB_ACCEL_FLAT       0u
+#define RB_ACCEL_INSTANCED  1u
 /* A BxDF sample that fails (a direction on the wrong side of the shading
  * hemisphere, a zero or infinite pdf) sets the path's terminated flag. The
  * reference then drops the whole sample, radiance gathered before included

@@ -62,6 +62,8 @@ RB_TEXADDR_CLAMP = 1
 RB_TEXADDR_MIRROR = 2
 RB_TEXFILTER_NEAREST = 0
 RB_TEXFILTER_LINEAR = 1
+RB_ACCEL_FLAT = 0
+RB_ACCEL_INSTANCED = 1
 
 RB_SPECTRUM_BINS = 471
 RB_LUT_SIZE = 32
@@ -105,7 +107,7 @@ class rb_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_paths_in_flight", C.c_uint32),
                 ("envmap_cdf_mode", C.c_uint32), ("failed_sample_mode", C.c_uint32),
                 ("inject_queue_limit", C.c_uint32), ("inject_alloc_failure", C.c_uint32),
-                ("inject_stack_limit", C.c_uint32), ("reserved", C.c_uint32)]
+                ("inject_stack_limit", C.c_uint32), ("acceleration", C.c_uint32)]
 
 
 RB_FAILED_DROP = 0

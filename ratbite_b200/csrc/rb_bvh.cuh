@@ -11,6 +11,7 @@
 // triangle id, which makes the result independent of traversal order.
 #pragma once
 
+#include "rb_instance.cuh"
 #include "rb_math.cuh"
 #include "rb_scene.h"
 
@@ -559,6 +560,245 @@ struct AnyTraversal
 			}
 			if (sp == 0) { done = true; break; }
 			cur = stack[--sp];
+		}
+		return done;
+	}
+};
+
+// ---------------------------------------------------------------------------
+// Two-level traversal (RB_ACCEL_INSTANCED). The top level's leaves hold
+// instances; entering one pushes a return marker, takes the ray into the
+// instance's object space for the box tests of its unit's BVH, and popping
+// the marker brings the world ray back. Triangles are intersected in world
+// space, each transformed with the flat upload's arithmetic
+// (instancedTriangle), so hits equal the flat structure's bit for bit. The
+// other instances of a top-level leaf wait on the stack as instance entries.
+constexpr uint32_t kInstanceEntry = 0x40000000u;   // | position; node indices stay below 2^24
+constexpr uint32_t kReturnEntry = 0x7FFFFFFFu;
+constexpr uint32_t kNoInstance = 0xFFFFFFFFu;
+
+RB_D bool isInstanceEntry(uint32_t e) { return (e >> 30) == 1u; }
+
+struct ClosestTraversal2 : ClosestTraversal
+{
+	TraceRay rw;               // the world ray
+	uint32_t inst;             // position of the instance being traversed, kNoInstance at the top level
+	uint32_t bestInst;
+
+	RB_D void init(const DevGeometry& g, f3 o, f3 d, float tmin_, float tmax)
+	{
+		leaf = 0u;
+		best = Hit{ -1, tmax, 0.0f, 0.0f };
+		bestId = 0xFFFFFFFFu;
+		bestInst = 0u;
+		tmin = tmin_;
+		sp = 0;
+		done = g.instanceCount == 0;
+		rw = makeTraceRay(o, d);
+		r = rw;
+		inst = kNoInstance;
+		cur = g.topRoot;
+	}
+
+	// Takes the ray into instance `pos`; false when the stack has no room
+	// for the return marker.
+	template<class Stack>
+	RB_D bool enter(const DevGeometry& g, uint32_t* status, uint32_t pos, Stack& stack)
+	{
+		if (sp >= static_cast<int>(g.stackLimit)) { atomicOr(status, RB_DEV_STACK_OVERFLOW); return false; }
+		stack[sp++] = make_uint2(kReturnEntry, 0u);
+		const DevInstance& in = g.instances[pos];
+		const float4 o = make_float4(rw.o.x, rw.o.y, rw.o.z, 0.0f);
+		r = makeTraceRay(xfPoint(in.wi, o), xfDir(in.wi, rw.d));
+		inst = pos;
+		cur = __ldg(&in.root);
+		return true;
+	}
+
+	// A top-level leaf: its first instance is entered, the others wait.
+	template<class Stack>
+	RB_D bool instanceLeaf(const DevGeometry& g, uint32_t* status, Stack& stack)
+	{
+		const uint32_t first = cur & 0x0FFFFFFFu;
+		const uint32_t count = ((cur >> 28) & 0x7u) + 1u;
+		for (uint32_t k = count - 1; k >= 1; --k)
+		{
+			if (sp < static_cast<int>(g.stackLimit)) stack[sp++] = make_uint2(kInstanceEntry | (first + k), 0u);
+			else atomicOr(status, RB_DEV_STACK_OVERFLOW);
+		}
+		return enter(g, status, first, stack);
+	}
+
+	template<bool COUNT>
+	RB_D void leafStep(const DevGeometry& g, uint32_t& nTris)
+	{
+		const uint32_t first = cur & 0x0FFFFFFFu;
+		const uint32_t count = ((cur >> 28) & 0x7u) + 1u;
+		if (COUNT) nTris += count;
+		for (uint32_t i = first; i < first + count; ++i)
+		{
+			float4 a, b, c;
+			uint2 aux;
+			instancedTriangle(g, i, inst, a, b, c, aux);
+			float t, u, v;
+			if (intersectTriangle(rw, f3_of(a), f3_of(b), f3_of(c), tmin, best.t, best.tri >= 0, t, u, v))
+			{
+				const uint32_t id = __float_as_uint(a.w);
+				if (best.tri < 0 || t < best.t || id < bestId)
+				{
+					best = Hit{ static_cast<int32_t>(i), t, u, v };
+					bestId = id;
+					bestInst = inst;
+				}
+			}
+		}
+	}
+
+	template<class Stack>
+	RB_D bool pop(const DevGeometry& g, uint32_t* status, Stack& stack)
+	{
+		while (sp > 0)
+		{
+			--sp;
+			const uint2 e = stack[sp];
+			if (e.x == kReturnEntry) { r = rw; inst = kNoInstance; continue; }
+			if (isInstanceEntry(e.x))
+			{
+				if (enter(g, status, e.x & 0x00FFFFFFu, stack)) return true;
+				continue;
+			}
+			if (__uint_as_float(e.y) <= best.t && e.x != kEmptyChild) { cur = e.x; return true; }
+		}
+		return false;
+	}
+
+	template<bool COUNT, class Stack>
+	RB_D bool run(const DevGeometry& g, int budget, uint32_t* status, uint32_t& nNodes, uint32_t& nTris, Stack& stack)
+	{
+		for (int it = 0; it < budget && !done; ++it)
+		{
+			if (cur == kEmptyChild)
+			{
+				if (!pop(g, status, stack)) done = true;
+			}
+			else if (cur & kLeafBit)
+			{
+				if (inst == kNoInstance)
+				{
+					if (!instanceLeaf(g, status, stack) && !pop(g, status, stack)) done = true;
+				}
+				else
+				{
+					leafStep<COUNT>(g, nTris);
+					if (!pop(g, status, stack)) done = true;
+				}
+			}
+			else if (!nodeStep<COUNT>(g, status, nNodes, stack) && !pop(g, status, stack))
+			{
+				done = true;
+			}
+		}
+		return done;
+	}
+};
+
+struct AnyTraversal2 : AnyTraversal
+{
+	TraceRay rw;
+	uint32_t inst;
+
+	RB_D void init(const DevGeometry& g, f3 o, f3 d, float tmin_, float tmax_)
+	{
+		tmin = tmin_;
+		tmax = tmax_;
+		sp = 0;
+		hit = false;
+		done = g.instanceCount == 0;
+		rw = makeTraceRay(o, d);
+		r = rw;
+		inst = kNoInstance;
+		cur = g.topRoot;
+	}
+
+	template<class Stack>
+	RB_D bool enter(const DevGeometry& g, uint32_t* status, uint32_t pos, Stack& stack)
+	{
+		if (sp >= static_cast<int>(g.stackLimit)) { atomicOr(status, RB_DEV_STACK_OVERFLOW); return false; }
+		stack[sp++] = kReturnEntry;
+		const DevInstance& in = g.instances[pos];
+		const float4 o = make_float4(rw.o.x, rw.o.y, rw.o.z, 0.0f);
+		r = makeTraceRay(xfPoint(in.wi, o), xfDir(in.wi, rw.d));
+		inst = pos;
+		cur = __ldg(&in.root);
+		return true;
+	}
+
+	template<bool COUNT, class Stack>
+	RB_D bool run(const DevGeometry& g, int budget, uint32_t* status, uint32_t& nNodes, uint32_t& nTris, Stack& stack)
+	{
+		for (int it = 0; it < budget && !done; ++it)
+		{
+			bool next = true;        // take the next entry from the stack after this step
+			if (cur == kEmptyChild)
+			{
+			}
+			else if ((cur & kLeafBit) && inst == kNoInstance)
+			{
+				const uint32_t first = cur & 0x0FFFFFFFu;
+				const uint32_t count = ((cur >> 28) & 0x7u) + 1u;
+				for (uint32_t k = count - 1; k >= 1; --k)
+				{
+					if (sp < static_cast<int>(g.stackLimit)) stack[sp++] = kInstanceEntry | (first + k);
+					else atomicOr(status, RB_DEV_STACK_OVERFLOW);
+				}
+				next = !enter(g, status, first, stack);
+			}
+			else if (cur & kLeafBit)
+			{
+				const uint32_t first = cur & 0x0FFFFFFFu;
+				const uint32_t count = ((cur >> 28) & 0x7u) + 1u;
+				for (uint32_t i = first; i < first + count; ++i)
+				{
+					if (COUNT) ++nTris;
+					float4 a, b, c;
+					uint2 aux;
+					instancedTriangle(g, i, inst, a, b, c, aux);
+					float t, u, v;
+					if (intersectTriangle(rw, f3_of(a), f3_of(b), f3_of(c), tmin, tmax, false, t, u, v))
+					{
+						hit = true;
+						done = true;
+						break;
+					}
+				}
+				if (done) break;
+			}
+			else
+			{
+				if (COUNT) ++nNodes;
+				const NodeView nv = loadNode(g.nodes, cur);
+				float tn[8];
+				const uint32_t mask = childBoxes(r, nv, tmin, tmax, tn);
+#pragma unroll
+				for (int c = 0; c < 8; ++c)
+				{
+					if ((mask >> c) & 1u)
+					{
+						if (sp < static_cast<int>(g.stackLimit)) stack[sp++] = nodeChild(nv, c);
+						else atomicOr(status, RB_DEV_STACK_OVERFLOW);
+					}
+				}
+			}
+			if (!next) continue;
+			bool found = false;
+			while (sp > 0 && !found)
+			{
+				const uint32_t e = stack[--sp];
+				if (e == kReturnEntry) { r = rw; inst = kNoInstance; }
+				else if (isInstanceEntry(e)) found = enter(g, status, e & 0x00FFFFFFu, stack);
+				else { cur = e; found = true; }
+			}
+			if (!found) { done = true; break; }
 		}
 		return done;
 	}

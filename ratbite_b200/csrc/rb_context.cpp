@@ -70,6 +70,17 @@ struct rb_ctx
 	// cross-table references checked before any kernel reads them
 	// refit of moved instances (rb_update_instances)
 	rb::RefitData refit;
+	// two-level structure (RB_ACCEL_INSTANCED): per flat instance its unit
+	// (-1: no triangles) and canonical base; per unit its root and object box;
+	// the top level's node slots and the instance table on the device
+	bool instanced = false;
+	std::vector<int32_t> instUnit;
+	std::vector<uint32_t> instCanon;
+	std::vector<uint32_t> unitRoot;
+	std::vector<float> unitBox;                 // 6 per unit: lo, hi
+	rb::BvhNode* topNodes = nullptr;            // the top level's slots inside scene.geo.nodes
+	uint32_t topBase = 0, topCapacity = 0;
+	rb::DevInstance* instDev = nullptr;
 	uint32_t geoInstances = 0, geoSubsets = 0;
 	float* xfDev = nullptr;                     // 12 floats per flattened instance (in geoBufs)
 	float* wiDev = nullptr;
@@ -502,6 +513,8 @@ int rb_create(const rb_config* config, rb_ctx** out)
 	ctx->cdfMode = config ? config->envmap_cdf_mode : RB_CDF_FP64;
 	if (config && config->failed_sample_mode > RB_FAILED_KEEP) { delete ctx; return RB_ERR_INVALID; }
 	ctx->failedMode = config ? config->failed_sample_mode : RB_FAILED_DROP;
+	if (config && config->acceleration > RB_ACCEL_INSTANCED) { delete ctx; return RB_ERR_INVALID; }
+	ctx->instanced = config && config->acceleration == RB_ACCEL_INSTANCED;
 	if (config)
 	{
 		ctx->injectQueueLimit = config->inject_queue_limit;
@@ -742,6 +755,288 @@ int rb_set_textures(rb_ctx* ctx, const rb_texture* textures, uint32_t count)
 	return RB_OK;
 }
 
+namespace
+{
+// Relocates a unit's (or the top level's) BVH node into the shared node
+// array: interior children by the node base, leaf references by the base of
+// the unit's triangles (or of the instance table, which is 0).
+void relocate(rb::BvhNode& n, uint32_t nodeBase, uint32_t leafBase)
+{
+	for (int c = 0; c < 8; ++c)
+	{
+		const uint32_t ref = n.child[c];
+		if (ref == rb::kEmptyChild) continue;
+		if (ref & rb::kLeafBit) n.child[c] = (ref & 0xF0000000u) | ((ref & 0x0FFFFFFFu) + leafBase);
+		else n.child[c] = ref + nodeBase;
+	}
+}
+
+// The top level over the instances' world boxes (each unit's object box
+// through the instance's transform, all eight corners), as "triangles"
+// (lo, hi, centre) that bound the box; the instance table in its leaf order.
+int buildTopLevel(rb_ctx* ctx, const std::vector<float>& xfAll, const std::vector<float>& wiAll,
+	std::vector<rb::BvhNode>& nodes, std::vector<rb::DevInstance>& table, uint32_t& root)
+{
+	std::vector<float> boxes;
+	std::vector<uint32_t> flat;
+	for (size_t i = 0; i < ctx->instUnit.size(); ++i)
+	{
+		if (ctx->instUnit[i] < 0) continue;
+		const float* b = ctx->unitBox.data() + 6 * ctx->instUnit[i];
+		const float* W = xfAll.data() + 12 * i;
+		float lo[3] = { INFINITY, INFINITY, INFINITY }, hi[3] = { -INFINITY, -INFINITY, -INFINITY };
+		for (int k = 0; k < 8; ++k)
+		{
+			const float p[3] = { b[(k & 1) ? 3 : 0], b[(k & 2) ? 4 : 1], b[(k & 4) ? 5 : 2] };
+			float w[3];
+			toWorld(W, p, w);
+			for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], w[a]); hi[a] = std::max(hi[a], w[a]); }
+		}
+		for (int a = 0; a < 3; ++a)
+			if (!std::isfinite(lo[a]) || !std::isfinite(hi[a])) return RB_ERR_INVALID;
+		const float tri[9] = { lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], 0.5f * (lo[0] + hi[0]), 0.5f * (lo[1] + hi[1]),
+			0.5f * (lo[2] + hi[2]) };
+		boxes.insert(boxes.end(), tri, tri + 9);
+		flat.push_back(static_cast<uint32_t>(i));
+	}
+	table.clear();
+	nodes.clear();
+	root = rb::kEmptyChild;
+	if (flat.empty()) return RB_OK;
+	const rb::WideBvh top = rb::buildWideBvh(boxes);
+	if (top.maxDepth + 1 > 8u) return RB_ERR_TOO_LARGE;
+	nodes = top.nodes;
+	for (rb::BvhNode& n : nodes) relocate(n, ctx->topBase, 0u);
+	root = top.rootIsLeaf ? (rb::kLeafBit | (static_cast<uint32_t>(flat.size() - 1) << 28)) : ctx->topBase;
+	for (uint32_t j = 0; j < flat.size(); ++j)
+	{
+		const uint32_t i = flat[top.triOrder[j]];
+		rb::DevInstance d{};
+		std::memcpy(d.xf, xfAll.data() + 12 * i, sizeof(d.xf));
+		std::memcpy(d.wi, wiAll.data() + 12 * i, sizeof(d.wi));
+		d.root = ctx->unitRoot[ctx->instUnit[i]];
+		d.canonBase = ctx->instCanon[i];
+		d.index = i;
+		table.push_back(d);
+	}
+	return RB_OK;
+}
+
+// rb_set_geometry for RB_ACCEL_INSTANCED: one BVH per unit (each mesh an
+// instance uses, each emissive subset) over its object-space triangles, the
+// top level over the instances. Triangle numbering (canonical ids,
+// primitive and emissive indices) and the skipped degenerate triangles are
+// the flat upload's.
+int setGeometryInstanced(rb_ctx* ctx, const rb_geometry* g)
+{
+	struct Unit
+	{
+		std::vector<float> obj;
+		std::vector<uint32_t> canon, sbt, prim;
+	};
+	std::vector<Unit> units;
+	std::vector<int32_t> meshUnit(g->mesh_count, -2);      // -2: not built yet
+	std::vector<uint32_t> meshTris(g->mesh_count, 0);
+	std::vector<int32_t> instUnit;
+	std::vector<uint32_t> instCanon;
+	std::vector<float> xfAll, wiAll, normalMatrix;
+	uint32_t canonical = 0, emissivePrim = 0;
+	auto addInstance = [&](const float* xf, int32_t unit, uint32_t canonBase) {
+		for (int k = 0; k < 12; ++k)
+			if (!std::isfinite(xf[k])) return false;
+		float wi[12];
+		invert3x4(xf, wi);
+		const float nm[9] = { wi[0], wi[4], wi[8], wi[1], wi[5], wi[9], wi[2], wi[6], wi[10] };
+		normalMatrix.insert(normalMatrix.end(), nm, nm + 9);
+		xfAll.insert(xfAll.end(), xf, xf + 12);
+		wiAll.insert(wiAll.end(), wi, wi + 12);
+		instUnit.push_back(unit);
+		instCanon.push_back(canonBase);
+		return true;
+	};
+	auto keep = [&](Unit& u, const float* obj, uint32_t canon, uint32_t sbt, uint32_t prim) {
+		for (int k = 0; k < 9; ++k)
+			if (!std::isfinite(obj[k])) return false;
+		if (degenerate(obj)) return true;
+		u.obj.insert(u.obj.end(), obj, obj + 9);
+		u.canon.push_back(canon);
+		u.sbt.push_back(sbt);
+		u.prim.push_back(prim);
+		return true;
+	};
+	for (uint32_t s = 0; s < g->emissive_subset_count; ++s)
+	{
+		const rb_emissive_subset& es = g->emissive_subsets[s];
+		if (es.triangle_count && !es.vertices) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: null emissive vertices");
+		Unit u;
+		for (uint32_t t = 0; t < es.triangle_count; ++t)
+			if (!keep(u, es.vertices + 9 * t, t, 0xFFFFFFFFu, emissivePrim++))
+				return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: non-finite emissive vertex");
+		const int32_t id = u.obj.empty() ? -1 : static_cast<int32_t>(units.size());
+		if (!u.obj.empty()) units.push_back(std::move(u));
+		if (!addInstance(es.transform, id, canonical)) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: non-finite transform");
+		canonical += es.triangle_count;
+	}
+	for (uint32_t i = 0; i < g->instance_count; ++i)
+	{
+		const rb_instance& in = g->instances[i];
+		if (in.mesh >= g->mesh_count) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: instance mesh out of range");
+		if (meshUnit[in.mesh] == -2)
+		{
+			const rb_mesh& mesh = g->meshes[in.mesh];
+			if (mesh.submesh_count && !mesh.submeshes) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: null submeshes");
+			Unit u;
+			uint32_t local = 0;
+			for (uint32_t s = 0; s < mesh.submesh_count; ++s)
+			{
+				const rb_submesh& sm = mesh.submeshes[s];
+				if (sm.triangle_count && (!sm.indices || !sm.vertices)) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: null submesh data");
+				if (sm.index_type > RB_INDEX_U32) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: unknown index type");
+				std::vector<uint8_t> discarded(sm.triangle_count, 0);
+				for (uint32_t k = 0; k < sm.discarded_count; ++k)
+					if (sm.discarded[k] < sm.triangle_count) discarded[sm.discarded[k]] = 1;
+				for (uint32_t t = 0; t < sm.triangle_count; ++t)
+				{
+					float obj[9];
+					for (int k = 0; k < 3; ++k)
+					{
+						const uint32_t vi = discarded[t] ? 0u : readIndex(sm.indices, sm.index_type, static_cast<size_t>(t) * 3 + k);
+						if (vi >= sm.vertex_count) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: vertex index out of range");
+						obj[3 * k + 0] = sm.vertices[4 * vi + 0];
+						obj[3 * k + 1] = sm.vertices[4 * vi + 1];
+						obj[3 * k + 2] = sm.vertices[4 * vi + 2];
+					}
+					if (!keep(u, obj, local++, sm.material, t)) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: non-finite vertex");
+				}
+			}
+			meshTris[in.mesh] = local;
+			meshUnit[in.mesh] = u.obj.empty() ? -1 : static_cast<int32_t>(units.size());
+			if (!u.obj.empty()) units.push_back(std::move(u));
+		}
+		if (!addInstance(in.transform, meshUnit[in.mesh], canonical)) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: non-finite transform");
+		canonical += meshTris[in.mesh];
+	}
+	// the units' BVHs in one node array and one triangle array
+	std::vector<rb::BvhNode> nodes;
+	std::vector<float4> triVerts;
+	std::vector<uint2> triAux;
+	std::vector<uint32_t> unitRoot(units.size());
+	std::vector<float> unitBox(6 * units.size());
+	for (size_t u = 0; u < units.size(); ++u)
+	{
+		const Unit& U = units[u];
+		const rb::WideBvh b = rb::buildWideBvh(U.obj);
+		if (b.maxDepth + 1 > static_cast<uint32_t>(rb::kMaxBvhDepth) - 8u)
+			return fail(ctx, RB_ERR_TOO_LARGE, "rb_set_geometry: BVH beyond the traversal limits");
+		const uint32_t nodeBase = static_cast<uint32_t>(nodes.size()), triBase = static_cast<uint32_t>(triVerts.size() / 3);
+		const size_t nt = U.canon.size();
+		if (static_cast<size_t>(triBase) + nt >= (1u << 28)) return fail(ctx, RB_ERR_TOO_LARGE, "rb_set_geometry: more than 2^28 unique triangles");
+		for (rb::BvhNode n : b.nodes)
+		{
+			relocate(n, nodeBase, triBase);
+			nodes.push_back(n);
+		}
+		unitRoot[u] = b.rootIsLeaf ? (rb::kLeafBit | (static_cast<uint32_t>(nt - 1) << 28) | triBase) : nodeBase;
+		float* box = unitBox.data() + 6 * u;
+		for (int k = 0; k < 3; ++k) { box[k] = INFINITY; box[3 + k] = -INFINITY; }
+		for (size_t j = 0; j < nt; ++j)
+		{
+			const uint32_t t = b.triOrder[j];
+			const float* o = U.obj.data() + 9 * t;
+			float4 v[3];
+			for (int k = 0; k < 3; ++k)
+			{
+				v[k] = make_float4(o[3 * k], o[3 * k + 1], o[3 * k + 2], 0.0f);
+				for (int a = 0; a < 3; ++a) { box[a] = std::min(box[a], o[3 * k + a]); box[3 + a] = std::max(box[3 + a], o[3 * k + a]); }
+			}
+			std::memcpy(&v[0].w, &U.canon[t], 4);
+			std::memcpy(&v[2].w, &U.sbt[t], 4);
+			triVerts.insert(triVerts.end(), v, v + 3);
+			triAux.push_back(make_uint2(0u, U.prim[t]));
+		}
+	}
+	ctx->instUnit = instUnit;
+	ctx->instCanon = instCanon;
+	ctx->unitRoot = unitRoot;
+	ctx->unitBox = unitBox;
+	const uint32_t nInst = static_cast<uint32_t>(instUnit.size());
+	ctx->topBase = static_cast<uint32_t>(nodes.size());
+	ctx->topCapacity = std::max<uint32_t>(nInst, 1u) + 1u;
+	if (static_cast<size_t>(ctx->topBase) + ctx->topCapacity > rb::kMaxBvhNodes)
+		return fail(ctx, RB_ERR_TOO_LARGE, "rb_set_geometry: BVH beyond the traversal limits (2^24 nodes)");
+	std::vector<rb::BvhNode> top;
+	std::vector<rb::DevInstance> table;
+	uint32_t topRoot = rb::kEmptyChild;
+	int rc = buildTopLevel(ctx, xfAll, wiAll, top, table, topRoot);
+	if (rc != RB_OK) return fail(ctx, rc, "rb_set_geometry: top level (non-finite or too deep)");
+	if (top.size() > ctx->topCapacity) return fail(ctx, RB_ERR_TOO_LARGE, "rb_set_geometry: top level larger than its slots");
+	nodes.resize(static_cast<size_t>(ctx->topBase) + ctx->topCapacity);
+	std::copy(top.begin(), top.end(), nodes.begin() + ctx->topBase);
+	// world bounds over the kept triangles, as the flat upload computes them
+	float lo[3] = { 0.0f, 0.0f, 0.0f }, hi[3] = { 0.0f, 0.0f, 0.0f };
+	bool first = true;
+	for (uint32_t i = 0; i < nInst; ++i)
+	{
+		if (instUnit[i] < 0) continue;
+		const Unit& U = units[instUnit[i]];
+		for (size_t j = 0; j < U.obj.size(); j += 3)
+		{
+			float w[3];
+			toWorld(xfAll.data() + 12 * i, U.obj.data() + j, w);
+			for (int k = 0; k < 3; ++k)
+			{
+				if (!std::isfinite(w[k])) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: non-finite vertex");
+				lo[k] = first ? w[k] : std::min(lo[k], w[k]);
+				hi[k] = first ? w[k] : std::max(hi[k], w[k]);
+			}
+			first = false;
+		}
+	}
+	if (triVerts.empty()) { triVerts.resize(3); triAux.resize(1); }
+	std::vector<void*> fresh;
+	rb::DevGeometry G{};
+	rb::BvhNode* nodeDev = nullptr;
+	rb::DevInstance* instDev = nullptr;
+	rc = upload(ctx, fresh, nodes.data(), sizeof(rb::BvhNode) * nodes.size(), nodeDev);
+	if (rc == RB_OK) rc = upload(ctx, fresh, triVerts.data(), sizeof(float4) * triVerts.size(), G.triVerts);
+	if (rc == RB_OK) rc = upload(ctx, fresh, triAux.data(), sizeof(uint2) * triAux.size(), G.triAux);
+	if (rc == RB_OK) rc = upload(ctx, fresh, normalMatrix.empty() ? nullptr : normalMatrix.data(),
+		sizeof(float) * std::max<size_t>(normalMatrix.size(), 9), G.normalMatrix);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(rb::DevInstance) * std::max<uint32_t>(nInst, 1u), instDev);
+	if (rc == RB_OK && !table.empty() &&
+		cudaMemcpyAsync(instDev, table.data(), sizeof(rb::DevInstance) * table.size(), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+		rc = fail(ctx, RB_ERR_CUDA, "geometry upload");
+	if (rc == RB_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = fail(ctx, RB_ERR_CUDA, "geometry upload");
+	rc = commit(ctx, ctx->geoBufs, fresh, rc);
+	if (rc != RB_OK) return rc;
+	G.nodes = nodeDev;
+	G.instances = instDev;
+	G.nodeCount = static_cast<uint32_t>(nodes.size());
+	G.triCount = static_cast<uint32_t>(triVerts.size() / 3);
+	G.rootIsLeaf = 0u;
+	G.stackLimit = static_cast<uint32_t>(rb::kTraversalStackEntries);
+	if (ctx->injectStackLimit) G.stackLimit = std::min(ctx->injectStackLimit, G.stackLimit);
+	G.instanced = 1u;
+	G.topRoot = topRoot;
+	G.instanceCount = static_cast<uint32_t>(table.size());
+	ctx->scene.geo = G;
+	ctx->topNodes = nodeDev + ctx->topBase;
+	ctx->instDev = instDev;
+	ctx->refit = rb::RefitData{};
+	ctx->xfDev = ctx->wiDev = nullptr;
+	ctx->geoInstances = g->instance_count;
+	ctx->geoSubsets = g->emissive_subset_count;
+	ctx->geoEmissive = emissivePrim;
+	for (int k = 0; k < 3; ++k) { ctx->geoMin[k] = lo[k]; ctx->geoMax[k] = hi[k]; }
+	ctx->geoMaxMaterial = 0;
+	for (const Unit& U : units)
+		for (uint32_t s : U.sbt)
+			if (s != 0xFFFFFFFFu) ctx->geoMaxMaterial = std::max(ctx->geoMaxMaterial, s + 1);
+	ctx->haveGeometry = true;
+	return RB_OK;
+}
+} // namespace
+
 int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 {
 	if (!ctx || !g) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: null geometry");
@@ -749,6 +1044,7 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 		(g->emissive_subset_count && !g->emissive_subsets))
 		return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: null array");
 	cudaSetDevice(ctx->device);
+	if (ctx->instanced) return setGeometryInstanced(ctx, g);
 	// Triangles in canonical order: emissive subsets, then instances x submeshes.
 	std::vector<float> world;          // 9 per kept triangle
 	std::vector<float> objAll;         // 9 object-space floats per kept triangle
@@ -916,6 +1212,28 @@ int rb_update_instances(rb_ctx* ctx, const float* instXf, const float* subsetXf,
 	}
 	cudaSetDevice(ctx->device);
 	const cudaStream_t st = pick(ctx, stream);
+	if (ctx->instanced)
+	{
+		// rebuild the top level over the moved instances; the units stay
+		std::vector<rb::BvhNode> top;
+		std::vector<rb::DevInstance> table;
+		uint32_t root = rb::kEmptyChild;
+		const int rc = buildTopLevel(ctx, xf, wi, top, table, root);
+		if (rc != RB_OK) return fail(ctx, rc, "rb_update_instances: top level (non-finite or too deep)");
+		if (top.size() > ctx->topCapacity) return fail(ctx, RB_ERR_TOO_LARGE, "rb_update_instances: top level larger than its slots");
+		cudaError_t e2 = cudaSuccess;
+		if (!top.empty()) e2 = cudaMemcpyAsync(ctx->topNodes, top.data(), sizeof(rb::BvhNode) * top.size(), cudaMemcpyHostToDevice, st);
+		if (e2 == cudaSuccess && !table.empty())
+			e2 = cudaMemcpyAsync(ctx->instDev, table.data(), sizeof(rb::DevInstance) * table.size(), cudaMemcpyHostToDevice, st);
+		if (e2 == cudaSuccess)
+			e2 = cudaMemcpyAsync(const_cast<float*>(ctx->scene.geo.normalMatrix), nm.data(), sizeof(float) * 9 * n,
+				cudaMemcpyHostToDevice, st);
+		if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(st);
+		if (e2 != cudaSuccess) return cudaFail(ctx, e2, "rb_update_instances");
+		ctx->scene.geo.topRoot = root;
+		ctx->scene.geo.instanceCount = static_cast<uint32_t>(table.size());
+		return RB_OK;
+	}
 	cudaError_t e = cudaMemcpyAsync(ctx->xfDev, xf.data(), sizeof(float) * 12 * n, cudaMemcpyHostToDevice, st);
 	if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->wiDev, wi.data(), sizeof(float) * 12 * n, cudaMemcpyHostToDevice, st);
 	if (e == cudaSuccess)
@@ -1364,6 +1682,7 @@ int rb_render_jobs(rb_ctx* const* jobs, uint32_t n, const uint32_t* offsets, con
 		if (rc == RB_OK) rc = checkReferences(c);
 		if (rc != RB_OK) return fail(host, rc, "rb_render_jobs: a job's scene is incomplete");
 		if (c->cache) return fail(host, RB_ERR_UNSUPPORTED, "rb_render_jobs: jobs render the plain form");
+		if (c->instanced) return fail(host, RB_ERR_UNSUPPORTED, "rb_render_jobs: jobs take flat geometry (RB_ACCEL_FLAT)");
 		if (c->scene.launch.width > 65535 || c->scene.launch.height > 65535)
 			return fail(host, RB_ERR_INVALID, "rb_render_jobs: film side above 65535");
 		if (static_cast<uint64_t>(offsets[j]) + counts[j] > 0xFFFFFFFFull)

@@ -82,10 +82,20 @@ RB_D void unpackHit(const DevScene& sc, float4 h, f3 rayD, Interaction& it)
 		it.backHit = dot(it.gn, rayD) > 0.0f;
 		return;
 	}
-	const float4 a = __ldg(sc.geo.triVerts + 3 * tri);
-	const float4 b = __ldg(sc.geo.triVerts + 3 * tri + 1);
-	const float4 c = __ldg(sc.geo.triVerts + 3 * tri + 2);
-	const uint2 aux = __ldg(sc.geo.triAux + tri);
+	float4 a, b, c;
+	uint2 aux;
+	if (sc.geo.instanced)
+	{
+		// two-level: h.y holds the hit's instance (its position in the top level)
+		instancedTriangle(sc.geo, static_cast<uint32_t>(tri), __float_as_uint(h.y), a, b, c, aux);
+	}
+	else
+	{
+		a = __ldg(sc.geo.triVerts + 3 * tri);
+		b = __ldg(sc.geo.triVerts + 3 * tri + 1);
+		c = __ldg(sc.geo.triVerts + 3 * tri + 2);
+		aux = __ldg(sc.geo.triAux + tri);
+	}
 	it.v0 = f3_of(a); it.v1 = f3_of(b); it.v2 = f3_of(c);
 	it.instance = __float_as_uint(b.w);
 	const uint32_t sbt = __float_as_uint(c.w);

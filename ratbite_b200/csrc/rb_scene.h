@@ -119,20 +119,44 @@ constexpr int kMaxBvhDepth = 48;
 // Entries of a ray's traversal stack (one per entered child still owed).
 constexpr int kTraversalStackEntries = 64;
 
-// Per-triangle hit data in BVH leaf order. v[0..2] are the world-space
+// An instance of the two-level structure (RB_ACCEL_INSTANCED), in the
+// top-level BVH's leaf order: object-to-world and world-to-object 3x4
+// transforms, the reference of its unit's BVH root (node index, or a leaf
+// reference for units of <= kLeafMaxTris triangles), the canonical id of its
+// first triangle, and its index in the flat numbering (emissive subsets,
+// then instances), which the normal matrices and hit records use.
+struct alignas(16) DevInstance
+{
+	float xf[12];
+	float wi[12];
+	uint32_t root;
+	uint32_t canonBase;
+	uint32_t index;
+	uint32_t pad;
+};
+
+// Per-triangle hit data in BVH leaf order. Flat: v[0..2] are the world-space
 // vertices; their w lanes carry the canonical triangle id (v0.w), the
 // instance index (v1.w) and the hit-group data (v2.w: material index, or
-// 0xFFFFFFFF for emissive triangles) as raw bits.
+// 0xFFFFFFFF for emissive triangles) as raw bits. Instanced: the triangles
+// of every unit (mesh or emissive subset) in object space, v0.w the
+// canonical id within the unit, v1.w unused, v2.w as flat; triAux.x unused
+// (the encoded normal depends on the instance).
 struct DevGeometry
 {
-	const BvhNode* nodes;
+	const BvhNode* nodes;        // instanced: the units' BVHs, then the top level
 	const float4* triVerts;      // 3 per triangle
 	const uint2* triAux;         // (encoded geometric normal, primitive index)
 	const float* normalMatrix;   // 9 per instance: payload words 9..17 (src/kernels/pathtrace.cu:134-142)
+	const DevInstance* instances;  // instanced: top-level leaf order
 	uint32_t nodeCount;
 	uint32_t triCount;
 	uint32_t rootIsLeaf;         // scenes of <= kLeafMaxTris triangles
 	uint32_t stackLimit;         // traversal stack entries in use (kTraversalStackEntries unless injected)
+	uint32_t instanced;          // 1: two-level structure
+	uint32_t topRoot;            // instanced: reference of the top-level root
+	uint32_t instanceCount;      // instanced: entries of `instances`
+	uint32_t pad;
 };
 
 // A light-tree node unpacked for the descent (48 B): mean and variance,

@@ -6,6 +6,7 @@
 // decides the reported hit, is written with explicitly rounded operations.
 
 #include <cfloat>
+#include <type_traits>
 
 #include "rb_bvh.cuh"
 #include "rb_launch.cuh"
@@ -82,9 +83,15 @@ RB_D void persistentTraversal(uint32_t n, uint32_t* workCounter, Begin&& begin, 
 	}
 }
 
+// The hit record's second word: the distance (flat), or the position of the
+// hit's instance (two-level; the distance is not read downstream).
+RB_D float hitWord(const ClosestTraversal& tr) { return tr.best.t; }
+RB_D float hitWord(const ClosestTraversal2& tr) { return __uint_as_float(tr.bestInst); }
+
 // counters (COUNT only): [0] rays, [1] nodes, [2] triangles. JOBS: a shared
-// wavefront, each ray traced in its job's geometry.
-template<bool COUNT, bool JOBS>
+// wavefront, each ray traced in its job's geometry. TWO: the two-level
+// structure (RB_ACCEL_INSTANCED).
+template<bool COUNT, bool JOBS, bool TWO = false>
 __global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kExtend(const __grid_constant__ DevScene sc, PathSoA s,
 	int bounce, unsigned long long* counters)
 {
@@ -93,7 +100,7 @@ __global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kExtend(const _
 	uint32_t rays = 0, nodes = 0, tris = 0;
 	uint32_t p = 0;
 	const DevScene* js = &sc;
-	ClosestTraversal tr;
+	typename std::conditional<TWO, ClosestTraversal2, ClosestTraversal>::type tr;
 #if RB_TRAV_SMEM_STACK
 	__shared__ uint2 smStack[RB_TRAV_SMEM_STACK * kThreads];
 	HybridStack<uint2, RB_TRAV_SMEM_STACK, kThreads> stack{ smStack + threadIdx.x };
@@ -103,7 +110,7 @@ __global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kExtend(const _
 	auto step = [&]() {
 		const DevGeometry& g = JOBS ? js->geo : sc.geo;
 		if (!tr.template run<COUNT>(g, kStepBudget, JOBS ? js->status : sc.status, nodes, tris, stack)) return false;
-		s.hit[p] = make_float4(__int_as_float(tr.best.tri), tr.best.t, tr.best.b1, tr.best.b2);
+		s.hit[p] = make_float4(__int_as_float(tr.best.tri), hitWord(tr), tr.best.b1, tr.best.b2);
 		return true;
 	};
 	persistentTraversal<ClosestTraversal>(n, s.counts + kExtendFetch + bounce,
@@ -122,7 +129,7 @@ __global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kExtend(const _
 	}
 }
 
-template<bool COUNT, bool JOBS>
+template<bool COUNT, bool JOBS, bool TWO = false>
 __global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kShadow(const __grid_constant__ DevScene sc, PathSoA s,
 	int bounce, unsigned long long* counters)
 {
@@ -130,7 +137,7 @@ __global__ void __launch_bounds__(kThreads, RB_TRACE_MIN_BLOCKS) kShadow(const _
 	uint32_t rays = 0, nodes = 0, tris = 0;
 	uint32_t r = 0;             // the shadow ray's surface record (queue position)
 	const DevScene* js = &sc;
-	AnyTraversal tr;
+	typename std::conditional<TWO, AnyTraversal2, AnyTraversal>::type tr;
 #if RB_TRAV_SMEM_STACK
 	__shared__ uint32_t smStack[RB_TRAV_SMEM_STACK * kThreads];
 	HybridStack<uint32_t, RB_TRAV_SMEM_STACK, kThreads> stack{ smStack + threadIdx.x };
@@ -172,7 +179,19 @@ __global__ void kTrace(DevScene sc, uint32_t n, const float* rays, uint32_t* pay
 	{
 		const f3 o = mk(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
 		const f3 d = mk(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
-		const Hit h = traceClosest(sc.geo, o, d, 0.0f, FLT_MAX, sc.status);
+		Hit h;
+		uint32_t pos = 0;
+		if (sc.geo.instanced)
+		{
+			ClosestTraversal2 tr;
+			uint2 stack[kTraversalStack];
+			uint32_t nn = 0, nt = 0;
+			tr.init(sc.geo, o, d, 0.0f, FLT_MAX);
+			while (!tr.run<false>(sc.geo, 1 << 30, sc.status, nn, nt, stack)) {}
+			h = tr.best;
+			pos = tr.bestInst;
+		}
+		else h = traceClosest(sc.geo, o, d, 0.0f, FLT_MAX, sc.status);
 		uint32_t* pl = payload + 24 * static_cast<size_t>(i);
 		for (int k = 0; k < 24; ++k) pl[k] = 0u;
 		if (h.tri < 0)
@@ -182,8 +201,14 @@ __global__ void kTrace(DevScene sc, uint32_t n, const float* rays, uint32_t* pay
 			triOut[i] = -1;
 			continue;
 		}
-		const float4 a = sc.geo.triVerts[3 * h.tri], b = sc.geo.triVerts[3 * h.tri + 1], c = sc.geo.triVerts[3 * h.tri + 2];
-		const uint2 aux = sc.geo.triAux[h.tri];
+		float4 a, b, c;
+		uint2 aux;
+		if (sc.geo.instanced) instancedTriangle(sc.geo, static_cast<uint32_t>(h.tri), pos, a, b, c, aux);
+		else
+		{
+			a = sc.geo.triVerts[3 * h.tri]; b = sc.geo.triVerts[3 * h.tri + 1]; c = sc.geo.triVerts[3 * h.tri + 2];
+			aux = sc.geo.triAux[h.tri];
+		}
 		const uint32_t sbt = __float_as_uint(c.w);
 		uint32_t prim = aux.y, mat = sbt, lptr = kLightTypeNone << 30;
 		if (sbt == 0xFFFFFFFFu)
@@ -209,7 +234,16 @@ __global__ void kOccluded(DevScene sc, uint32_t n, const float* rays, const floa
 	{
 		const f3 o = mk(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
 		const f3 d = mk(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
-		out[i] = traceAny(sc.geo, o, d, 0.0f, tmax[i], sc.status) ? 1u : 0u;
+		if (sc.geo.instanced)
+		{
+			AnyTraversal2 tr;
+			uint32_t stack[kTraversalStack];
+			uint32_t nn = 0, nt = 0;
+			tr.init(sc.geo, o, d, 0.0f, tmax[i]);
+			while (!tr.run<false>(sc.geo, 1 << 30, sc.status, nn, nt, stack)) {}
+			out[i] = tr.hit ? 1u : 0u;
+		}
+		else out[i] = traceAny(sc.geo, o, d, 0.0f, tmax[i], sc.status) ? 1u : 0u;
 	}
 }
 } // namespace
@@ -234,6 +268,11 @@ void launchExtend(const DevScene& sc, const PathSoA& s, int bounce, const Launch
 		if (counters) kExtend<true, true><<<g, kThreads, 0, st>>>(sc, s, bounce, counters);
 		else kExtend<false, true><<<g, kThreads, 0, st>>>(sc, s, bounce, nullptr);
 	}
+	else if (sc.geo.instanced)
+	{
+		if (counters) kExtend<true, false, true><<<g, kThreads, 0, st>>>(sc, s, bounce, counters);
+		else kExtend<false, false, true><<<g, kThreads, 0, st>>>(sc, s, bounce, nullptr);
+	}
 	else if (counters) kExtend<true, false><<<g, kThreads, 0, st>>>(sc, s, bounce, counters);
 	else kExtend<false, false><<<g, kThreads, 0, st>>>(sc, s, bounce, nullptr);
 }
@@ -245,6 +284,11 @@ void launchShadow(const DevScene& sc, const PathSoA& s, int bounce, const Launch
 	{
 		if (counters) kShadow<true, true><<<g, kThreads, 0, st>>>(sc, s, bounce, counters);
 		else kShadow<false, true><<<g, kThreads, 0, st>>>(sc, s, bounce, nullptr);
+	}
+	else if (sc.geo.instanced)
+	{
+		if (counters) kShadow<true, false, true><<<g, kThreads, 0, st>>>(sc, s, bounce, counters);
+		else kShadow<false, false, true><<<g, kThreads, 0, st>>>(sc, s, bounce, nullptr);
 	}
 	else if (counters) kShadow<true, false><<<g, kThreads, 0, st>>>(sc, s, bounce, counters);
 	else kShadow<false, false><<<g, kThreads, 0, st>>>(sc, s, bounce, nullptr);

@@ -22,15 +22,18 @@ def _ptr(a: np.ndarray):
 
 class RenderingInterface:
     def __init__(self, device: int = 0, max_paths_in_flight: int = 0, envmap_cdf_mode: int = abi.RB_CDF_FP64,
-                 failed_sample_mode: int = abi.RB_FAILED_DROP, inject: dict | None = None):
+                 failed_sample_mode: int = abi.RB_FAILED_DROP, inject: dict | None = None,
+                 acceleration: int = abi.RB_ACCEL_FLAT):
         """inject: fault injection for tests, keys of rb_config without the
-        `inject_` prefix (queue_limit, alloc_failure, stack_limit)."""
+        `inject_` prefix (queue_limit, alloc_failure, stack_limit).
+        acceleration: RB_ACCEL_FLAT or RB_ACCEL_INSTANCED (two-level)."""
         self.lib = load()
         cfg = abi.rb_config()
         cfg.device = device
         cfg.max_paths_in_flight = max_paths_in_flight
         cfg.envmap_cdf_mode = envmap_cdf_mode
         cfg.failed_sample_mode = failed_sample_mode
+        cfg.acceleration = acceleration
         for k, v in (inject or {}).items():
             setattr(cfg, f"inject_{k}", int(v))
         h = C.c_void_p()
