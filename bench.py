@@ -191,6 +191,7 @@ def workload_config(scene, wl: dict, world: int, tables: str) -> dict:
             "envmap": list(scene.envmap.shape[1::-1]) if has_env else None,
             "paths_per_step": wl["width"] * wl["height"] * wl["spp"] * world,
             "parallelism": f"sample-range x{world}", "tables": tables,
+            "acceleration": wl.get("acceleration", "flat"),
             "l2": "inputs larger than L2 (wavefront path state 388 B per path in flight, "
                   "~6.5 GB at the default 16M paths per wave)"}
 
@@ -297,7 +298,8 @@ def run_ours(args, rank: int, world: int, wl: dict):
     t_setup = time.perf_counter()
     scene, cie, basis, luts, tables = make_scene(wl)
     lt = lighttree.build_for_scene(scene)
-    ri = RenderingInterface(device=local, max_paths_in_flight=args.max_paths)
+    accel = abi.RB_ACCEL_INSTANCED if args.acceleration == "instanced" else abi.RB_ACCEL_FLAT
+    ri = RenderingInterface(device=local, max_paths_in_flight=args.max_paths, acceleration=accel)
     ri.load_scene(scene, luts, cie, basis, light_tree=lt)
     cache = None
     if wl.get("cached"):
@@ -780,6 +782,9 @@ def main():
     ap.add_argument("--no-rows", dest="rows", action="store_false",
                     help="skip the head-to-head timing of the env-map CDF and resolve kernels against the "
                          "reference's own CUDA kernels")
+    ap.add_argument("--acceleration", choices=["flat", "instanced"], default="flat",
+                    help="ray-traversal structure (rb_config.acceleration): one flattened BVH (the default) or "
+                         "the two-level one (a BVH per unique mesh under a top level over the instances)")
     ap.add_argument("--max-paths", type=int, default=0,
                     help="paths in flight per wave (0 = the library default, 16M); small values make profiling "
                          "captures small")
@@ -788,6 +793,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     args.warmup = max(args.warmup, 3)
     wl = dict(WORKLOADS.get(args.workload, WORKLOADS["scale"]))
+    wl["acceleration"] = args.acceleration
     if args.spp:
         wl["spp"] = args.spp
         wl["name"] = wl["name"].replace(f"{WORKLOADS[args.workload]['spp']}spp", f"{args.spp}spp")

@@ -638,8 +638,7 @@ struct ClosestTraversal2 : ClosestTraversal
 		for (uint32_t i = first; i < first + count; ++i)
 		{
 			float4 a, b, c;
-			uint2 aux;
-			instancedTriangle(g, i, inst, a, b, c, aux);
+			instancedVerts(g, i, inst, a, b, c);
 			float t, u, v;
 			if (intersectTriangle(rw, f3_of(a), f3_of(b), f3_of(c), tmin, best.t, best.tri >= 0, t, u, v))
 			{
@@ -761,8 +760,7 @@ struct AnyTraversal2 : AnyTraversal
 				{
 					if (COUNT) ++nTris;
 					float4 a, b, c;
-					uint2 aux;
-					instancedTriangle(g, i, inst, a, b, c, aux);
+					instancedVerts(g, i, inst, a, b, c);
 					float t, u, v;
 					if (intersectTriangle(rw, f3_of(a), f3_of(b), f3_of(c), tmin, tmax, false, t, u, v))
 					{

@@ -57,8 +57,8 @@ class BinaryBuilder
 {
 public:
 	BinaryBuilder(const std::vector<Box>& boxes, const std::vector<float>& cx, const std::vector<float>& cy,
-		const std::vector<float>& cz)
-		: m_boxes(boxes)
+		const std::vector<float>& cz, int maxLeaf)
+		: m_boxes(boxes), m_maxLeaf(maxLeaf)
 	{
 		m_c[0] = &cx; m_c[1] = &cy; m_c[2] = &cz;
 		m_order.resize(boxes.size());
@@ -76,6 +76,7 @@ public:
 
 private:
 	const std::vector<Box>& m_boxes;
+	const int m_maxLeaf;
 	const std::vector<float>* m_c[3];
 
 	void buildNode(int ni, int first, int count)
@@ -132,7 +133,7 @@ private:
 		const double leafCost = static_cast<double>(count);
 		const double parentArea = box.area();
 		const double splitCost = parentArea > 0.0 ? 1.0 + bestCost / parentArea : INFINITY;
-		if (count <= kLeafMaxTris && (bestAxis < 0 || leafCost <= splitCost)) return;
+		if (count <= m_maxLeaf && (bestAxis < 0 || leafCost <= splitCost)) return;
 
 		int mid;
 		if (bestAxis < 0)
@@ -277,7 +278,7 @@ private:
 };
 } // namespace
 
-WideBvh buildWideBvh(const std::vector<float>& worldVerts)
+WideBvh buildWideBvh(const std::vector<float>& worldVerts, int maxLeaf)
 {
 	WideBvh out;
 	const size_t n = worldVerts.size() / 9;
@@ -292,7 +293,7 @@ WideBvh buildWideBvh(const std::vector<float>& worldVerts)
 		cy[t] = (v[1] + v[4] + v[7]) / 3.0f;
 		cz[t] = (v[2] + v[5] + v[8]) / 3.0f;
 	}
-	BinaryBuilder bb(boxes, cx, cy, cz);
+	BinaryBuilder bb(boxes, cx, cy, cz, std::min(std::max(maxLeaf, 1), kLeafMaxTris));
 	bb.build();
 	if (isLeaf(bb.nodes[0]))
 	{

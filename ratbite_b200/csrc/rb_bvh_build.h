@@ -20,6 +20,7 @@ struct WideBvh
 	uint32_t maxDepth = 0;           // wide levels below the root
 };
 
-// worldVerts: 9 floats per triangle. Degenerate triangles must already be removed.
-WideBvh buildWideBvh(const std::vector<float>& worldVerts);
+// worldVerts: 9 floats per triangle. Degenerate triangles must already be
+// removed. Leaves hold at most maxLeaf (1..kLeafMaxTris) triangles.
+WideBvh buildWideBvh(const std::vector<float>& worldVerts, int maxLeaf = kLeafMaxTris);
 } // namespace rb

@@ -71,13 +71,16 @@ struct rb_ctx
 	// refit of moved instances (rb_update_instances)
 	rb::RefitData refit;
 	// two-level structure (RB_ACCEL_INSTANCED): per flat instance its unit
-	// (-1: no triangles) and canonical base; per unit its root and object box;
-	// the top level's node slots and the instance table on the device
+	// (-1: no triangles) and canonical base; per unit its root; the top
+	// level's node slots, the instance table and the world-box inputs on the
+	// device
 	bool instanced = false;
 	std::vector<int32_t> instUnit;
 	std::vector<uint32_t> instCanon;
 	std::vector<uint32_t> unitRoot;
-	std::vector<float> unitBox;                 // 6 per unit: lo, hi
+	uint32_t* instRangeDev = nullptr;           // per flat instance: its unit's first triangle and count
+	float* instXfDev = nullptr;                 // per flat instance: 12 floats
+	float* instBoxDev = nullptr;                // per flat instance: world box (6 floats)
 	rb::BvhNode* topNodes = nullptr;            // the top level's slots inside scene.geo.nodes
 	uint32_t topBase = 0, topCapacity = 0;
 	rb::DevInstance* instDev = nullptr;
@@ -755,6 +758,11 @@ int rb_set_textures(rb_ctx* ctx, const rb_texture* textures, uint32_t count)
 	return RB_OK;
 }
 
+#ifndef RB_TOP_LEAF
+#define RB_TOP_LEAF 4
+#endif
+
+
 namespace
 {
 // Relocates a unit's (or the top level's) BVH node into the shared node
@@ -771,29 +779,41 @@ void relocate(rb::BvhNode& n, uint32_t nodeBase, uint32_t leafBase)
 	}
 }
 
-// The top level over the instances' world boxes (each unit's object box
-// through the instance's transform, all eight corners), as "triangles"
-// (lo, hi, centre) that bound the box; the instance table in its leaf order.
+// The instances' world boxes, exact over their world triangles (the flat
+// upload's vertex arithmetic, on the device: the corners of the object box
+// through a rotation bound a box up to sqrt(3) times as wide), copied back.
+int instanceBoxes(rb_ctx* ctx, const std::vector<float>& xfAll, std::vector<float>& boxes, cudaStream_t st)
+{
+	const size_t n = ctx->instUnit.size();
+	boxes.assign(6 * n, 0.0f);
+	if (!n) return RB_OK;
+	cudaError_t e = cudaMemcpyAsync(ctx->instXfDev, xfAll.data(), sizeof(float) * 12 * n, cudaMemcpyHostToDevice, st);
+	if (e == cudaSuccess)
+	{
+		rb::launchInstanceBoxes(ctx->scene.geo.triVerts, ctx->instRangeDev, ctx->instXfDev, ctx->instBoxDev,
+			static_cast<uint32_t>(n), st);
+		e = cudaGetLastError();
+	}
+	if (e == cudaSuccess) e = cudaMemcpyAsync(boxes.data(), ctx->instBoxDev, sizeof(float) * 6 * n, cudaMemcpyDeviceToHost, st);
+	if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+	return e == cudaSuccess ? RB_OK : RB_ERR_CUDA;
+}
+
+// The top level over the instances' world boxes, as "triangles" (lo, hi,
+// centre) that bound each box; the instance table in its leaf order.
 int buildTopLevel(rb_ctx* ctx, const std::vector<float>& xfAll, const std::vector<float>& wiAll,
-	std::vector<rb::BvhNode>& nodes, std::vector<rb::DevInstance>& table, uint32_t& root)
+	const std::vector<float>& worldBoxes, std::vector<rb::BvhNode>& nodes, std::vector<rb::DevInstance>& table,
+	uint32_t& root)
 {
 	std::vector<float> boxes;
 	std::vector<uint32_t> flat;
 	for (size_t i = 0; i < ctx->instUnit.size(); ++i)
 	{
 		if (ctx->instUnit[i] < 0) continue;
-		const float* b = ctx->unitBox.data() + 6 * ctx->instUnit[i];
-		const float* W = xfAll.data() + 12 * i;
-		float lo[3] = { INFINITY, INFINITY, INFINITY }, hi[3] = { -INFINITY, -INFINITY, -INFINITY };
-		for (int k = 0; k < 8; ++k)
-		{
-			const float p[3] = { b[(k & 1) ? 3 : 0], b[(k & 2) ? 4 : 1], b[(k & 4) ? 5 : 2] };
-			float w[3];
-			toWorld(W, p, w);
-			for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], w[a]); hi[a] = std::max(hi[a], w[a]); }
-		}
+		const float* lo = worldBoxes.data() + 6 * i;
+		const float* hi = lo + 3;
 		for (int a = 0; a < 3; ++a)
-			if (!std::isfinite(lo[a]) || !std::isfinite(hi[a])) return RB_ERR_INVALID;
+			if (!std::isfinite(lo[a]) || !std::isfinite(hi[a]) || lo[a] > hi[a]) return RB_ERR_INVALID;
 		const float tri[9] = { lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], 0.5f * (lo[0] + hi[0]), 0.5f * (lo[1] + hi[1]),
 			0.5f * (lo[2] + hi[2]) };
 		boxes.insert(boxes.end(), tri, tri + 9);
@@ -803,7 +823,10 @@ int buildTopLevel(rb_ctx* ctx, const std::vector<float>& xfAll, const std::vecto
 	nodes.clear();
 	root = rb::kEmptyChild;
 	if (flat.empty()) return RB_OK;
-	const rb::WideBvh top = rb::buildWideBvh(boxes);
+	// RB_TOP_LEAF instances per leaf at most (1: each instance's own box is
+	// tested in its parent node, entered near to far, and skipped beyond the
+	// closest hit so far)
+	const rb::WideBvh top = rb::buildWideBvh(boxes, RB_TOP_LEAF);
 	if (top.maxDepth + 1 > 8u) return RB_ERR_TOO_LARGE;
 	nodes = top.nodes;
 	for (rb::BvhNode& n : nodes) relocate(n, ctx->topBase, 0u);
@@ -921,7 +944,6 @@ int setGeometryInstanced(rb_ctx* ctx, const rb_geometry* g)
 	std::vector<float4> triVerts;
 	std::vector<uint2> triAux;
 	std::vector<uint32_t> unitRoot(units.size());
-	std::vector<float> unitBox(6 * units.size());
 	for (size_t u = 0; u < units.size(); ++u)
 	{
 		const Unit& U = units[u];
@@ -937,18 +959,12 @@ int setGeometryInstanced(rb_ctx* ctx, const rb_geometry* g)
 			nodes.push_back(n);
 		}
 		unitRoot[u] = b.rootIsLeaf ? (rb::kLeafBit | (static_cast<uint32_t>(nt - 1) << 28) | triBase) : nodeBase;
-		float* box = unitBox.data() + 6 * u;
-		for (int k = 0; k < 3; ++k) { box[k] = INFINITY; box[3 + k] = -INFINITY; }
 		for (size_t j = 0; j < nt; ++j)
 		{
 			const uint32_t t = b.triOrder[j];
 			const float* o = U.obj.data() + 9 * t;
 			float4 v[3];
-			for (int k = 0; k < 3; ++k)
-			{
-				v[k] = make_float4(o[3 * k], o[3 * k + 1], o[3 * k + 2], 0.0f);
-				for (int a = 0; a < 3; ++a) { box[a] = std::min(box[a], o[3 * k + a]); box[3 + a] = std::max(box[3 + a], o[3 * k + a]); }
-			}
+			for (int k = 0; k < 3; ++k) v[k] = make_float4(o[3 * k], o[3 * k + 1], o[3 * k + 2], 0.0f);
 			std::memcpy(&v[0].w, &U.canon[t], 4);
 			std::memcpy(&v[2].w, &U.sbt[t], 4);
 			triVerts.insert(triVerts.end(), v, v + 3);
@@ -958,20 +974,12 @@ int setGeometryInstanced(rb_ctx* ctx, const rb_geometry* g)
 	ctx->instUnit = instUnit;
 	ctx->instCanon = instCanon;
 	ctx->unitRoot = unitRoot;
-	ctx->unitBox = unitBox;
 	const uint32_t nInst = static_cast<uint32_t>(instUnit.size());
 	ctx->topBase = static_cast<uint32_t>(nodes.size());
 	ctx->topCapacity = std::max<uint32_t>(nInst, 1u) + 1u;
 	if (static_cast<size_t>(ctx->topBase) + ctx->topCapacity > rb::kMaxBvhNodes)
 		return fail(ctx, RB_ERR_TOO_LARGE, "rb_set_geometry: BVH beyond the traversal limits (2^24 nodes)");
-	std::vector<rb::BvhNode> top;
-	std::vector<rb::DevInstance> table;
-	uint32_t topRoot = rb::kEmptyChild;
-	int rc = buildTopLevel(ctx, xfAll, wiAll, top, table, topRoot);
-	if (rc != RB_OK) return fail(ctx, rc, "rb_set_geometry: top level (non-finite or too deep)");
-	if (top.size() > ctx->topCapacity) return fail(ctx, RB_ERR_TOO_LARGE, "rb_set_geometry: top level larger than its slots");
-	nodes.resize(static_cast<size_t>(ctx->topBase) + ctx->topCapacity);
-	std::copy(top.begin(), top.end(), nodes.begin() + ctx->topBase);
+	nodes.resize(static_cast<size_t>(ctx->topBase) + ctx->topCapacity);   // top-level slots, filled below
 	// world bounds over the kept triangles, as the flat upload computes them
 	float lo[3] = { 0.0f, 0.0f, 0.0f }, hi[3] = { 0.0f, 0.0f, 0.0f };
 	bool first = true;
@@ -993,22 +1001,69 @@ int setGeometryInstanced(rb_ctx* ctx, const rb_geometry* g)
 		}
 	}
 	if (triVerts.empty()) { triVerts.resize(3); triAux.resize(1); }
+	// per flat instance: its unit's triangle range, for the world boxes
+	std::vector<uint32_t> range(2 * std::max<uint32_t>(nInst, 1u), 0u);
+	{
+		std::vector<uint32_t> unitFirst(units.size(), 0u);
+		uint32_t acc = 0;
+		for (size_t u = 0; u < units.size(); ++u) { unitFirst[u] = acc; acc += static_cast<uint32_t>(units[u].canon.size()); }
+		for (uint32_t i = 0; i < nInst; ++i)
+			if (instUnit[i] >= 0)
+			{
+				range[2 * i] = unitFirst[instUnit[i]];
+				range[2 * i + 1] = static_cast<uint32_t>(units[instUnit[i]].canon.size());
+			}
+	}
 	std::vector<void*> fresh;
 	rb::DevGeometry G{};
 	rb::BvhNode* nodeDev = nullptr;
 	rb::DevInstance* instDev = nullptr;
-	rc = upload(ctx, fresh, nodes.data(), sizeof(rb::BvhNode) * nodes.size(), nodeDev);
+	uint32_t* rangeDev = nullptr;
+	float *xfDev = nullptr, *boxDev = nullptr;
+	int rc = upload(ctx, fresh, nodes.data(), sizeof(rb::BvhNode) * nodes.size(), nodeDev);
 	if (rc == RB_OK) rc = upload(ctx, fresh, triVerts.data(), sizeof(float4) * triVerts.size(), G.triVerts);
 	if (rc == RB_OK) rc = upload(ctx, fresh, triAux.data(), sizeof(uint2) * triAux.size(), G.triAux);
 	if (rc == RB_OK) rc = upload(ctx, fresh, normalMatrix.empty() ? nullptr : normalMatrix.data(),
 		sizeof(float) * std::max<size_t>(normalMatrix.size(), 9), G.normalMatrix);
 	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(rb::DevInstance) * std::max<uint32_t>(nInst, 1u), instDev);
+	if (rc == RB_OK) rc = upload(ctx, fresh, range.data(), sizeof(uint32_t) * range.size(), rangeDev);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(float) * 12 * std::max<uint32_t>(nInst, 1u), xfDev);
+	if (rc == RB_OK) rc = upload(ctx, fresh, nullptr, sizeof(float) * 6 * std::max<uint32_t>(nInst, 1u), boxDev);
+	// the top level over the instances' exact world boxes
+	std::vector<rb::BvhNode> top;
+	std::vector<rb::DevInstance> table;
+	uint32_t topRoot = rb::kEmptyChild;
+	if (rc == RB_OK)
+	{
+		rb::DevGeometry keepGeo = ctx->scene.geo;
+		uint32_t* keepRange = ctx->instRangeDev;
+		float *keepXf = ctx->instXfDev, *keepBox = ctx->instBoxDev;
+		ctx->scene.geo.triVerts = G.triVerts;
+		ctx->instRangeDev = rangeDev;
+		ctx->instXfDev = xfDev;
+		ctx->instBoxDev = boxDev;
+		std::vector<float> boxes;
+		rc = instanceBoxes(ctx, xfAll, boxes, ctx->stream);
+		if (rc == RB_OK) rc = buildTopLevel(ctx, xfAll, wiAll, boxes, top, table, topRoot);
+		if (rc == RB_OK && top.size() > ctx->topCapacity) rc = RB_ERR_TOO_LARGE;
+		ctx->scene.geo = keepGeo;
+		ctx->instRangeDev = keepRange;
+		ctx->instXfDev = keepXf;
+		ctx->instBoxDev = keepBox;
+		if (rc != RB_OK) rc = fail(ctx, rc, "rb_set_geometry: top level (non-finite, too deep or too large)");
+	}
+	if (rc == RB_OK && !top.empty() &&
+		cudaMemcpyAsync(nodeDev + ctx->topBase, top.data(), sizeof(rb::BvhNode) * top.size(), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+		rc = fail(ctx, RB_ERR_CUDA, "geometry upload");
 	if (rc == RB_OK && !table.empty() &&
 		cudaMemcpyAsync(instDev, table.data(), sizeof(rb::DevInstance) * table.size(), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
 		rc = fail(ctx, RB_ERR_CUDA, "geometry upload");
 	if (rc == RB_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = fail(ctx, RB_ERR_CUDA, "geometry upload");
 	rc = commit(ctx, ctx->geoBufs, fresh, rc);
 	if (rc != RB_OK) return rc;
+	ctx->instRangeDev = rangeDev;
+	ctx->instXfDev = xfDev;
+	ctx->instBoxDev = boxDev;
 	G.nodes = nodeDev;
 	G.instances = instDev;
 	G.nodeCount = static_cast<uint32_t>(nodes.size());
@@ -1218,7 +1273,10 @@ int rb_update_instances(rb_ctx* ctx, const float* instXf, const float* subsetXf,
 		std::vector<rb::BvhNode> top;
 		std::vector<rb::DevInstance> table;
 		uint32_t root = rb::kEmptyChild;
-		const int rc = buildTopLevel(ctx, xf, wi, top, table, root);
+		std::vector<float> boxes;
+		int rc = instanceBoxes(ctx, xf, boxes, st);
+		if (rc != RB_OK) return fail(ctx, rc, "rb_update_instances: instance boxes");
+		rc = buildTopLevel(ctx, xf, wi, boxes, top, table, root);
 		if (rc != RB_OK) return fail(ctx, rc, "rb_update_instances: top level (non-finite or too deep)");
 		if (top.size() > ctx->topCapacity) return fail(ctx, RB_ERR_TOO_LARGE, "rb_update_instances: top level larger than its slots");
 		cudaError_t e2 = cudaSuccess;

@@ -45,18 +45,24 @@ RB_D uint32_t encodedNormalOf(float4 o0, float4 o1, float4 o2, const float* Wi)
 	return octEncodeU32(mk(__fmul_rn(nx, r), __fmul_rn(ny, r), __fmul_rn(nz, r)));
 }
 
-// The hit triangle `tri` (leaf order) of instance position `pos` as the flat
-// structure stores it: world vertices with the w lanes of the flat layout
-// (canonical id, instance index, hit-group data), and (encoded normal,
-// primitive index).
-RB_D void instancedTriangle(const DevGeometry& g, uint32_t tri, uint32_t pos, float4& a, float4& b, float4& c, uint2& aux)
+// The world vertices of triangle `tri` (leaf order) of instance position
+// `pos`, with the w lanes of the flat layout (canonical id, instance index,
+// hit-group data): what the traversal intersects.
+RB_D void instancedVerts(const DevGeometry& g, uint32_t tri, uint32_t pos, float4& a, float4& b, float4& c)
 {
 	const DevInstance& in = g.instances[pos];
 	const float4 o0 = __ldg(g.triVerts + 3 * tri), o1 = __ldg(g.triVerts + 3 * tri + 1), o2 = __ldg(g.triVerts + 3 * tri + 2);
 	const f3 w0 = xfPoint(in.xf, o0), w1 = xfPoint(in.xf, o1), w2 = xfPoint(in.xf, o2);
-	a = make_float4(w0.x, w0.y, w0.z, __uint_as_float(in.canonBase + __float_as_uint(o0.w)));
-	b = make_float4(w1.x, w1.y, w1.z, __uint_as_float(in.index));
+	a = make_float4(w0.x, w0.y, w0.z, __uint_as_float(__ldg(&in.canonBase) + __float_as_uint(o0.w)));
+	b = make_float4(w1.x, w1.y, w1.z, __uint_as_float(__ldg(&in.index)));
 	c = make_float4(w2.x, w2.y, w2.z, o2.w);
-	aux = make_uint2(encodedNormalOf(o0, o1, o2, in.wi), __ldg(g.triAux + tri).y);
+}
+// The hit triangle as the flat structure stores it: the world vertices and
+// (encoded normal, primitive index).
+RB_D void instancedTriangle(const DevGeometry& g, uint32_t tri, uint32_t pos, float4& a, float4& b, float4& c, uint2& aux)
+{
+	instancedVerts(g, tri, pos, a, b, c);
+	const float4 o0 = __ldg(g.triVerts + 3 * tri), o1 = __ldg(g.triVerts + 3 * tri + 1), o2 = __ldg(g.triVerts + 3 * tri + 2);
+	aux = make_uint2(encodedNormalOf(o0, o1, o2, g.instances[pos].wi), __ldg(g.triAux + tri).y);
 }
 } // namespace rb

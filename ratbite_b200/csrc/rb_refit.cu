@@ -111,6 +111,54 @@ __global__ void kRefitLevel(const uint32_t* __restrict__ order, uint32_t begin, 
 }
 } // namespace
 
+namespace
+{
+__global__ void __launch_bounds__(256) kInstanceBoxes(const float4* __restrict__ objVerts, const uint32_t* __restrict__ range,
+	const float* __restrict__ xf, float* __restrict__ boxes)
+{
+	const uint32_t i = blockIdx.x;
+	const uint32_t first = range[2 * i], count = range[2 * i + 1];
+	const float* W = xf + 12u * i;
+	float lo[3] = { INFINITY, INFINITY, INFINITY }, hi[3] = { -INFINITY, -INFINITY, -INFINITY };
+	for (uint32_t v = threadIdx.x; v < 3u * count; v += blockDim.x)
+	{
+		const float4 o = objVerts[3u * first + v];
+		for (int k = 0; k < 3; ++k)
+		{
+			const float w = world1(W, o.x, o.y, o.z, k);
+			lo[k] = fminf(lo[k], w);
+			hi[k] = fmaxf(hi[k], w);
+		}
+	}
+	__shared__ float red[6][8];
+	for (int k = 0; k < 3; ++k)
+	{
+		for (int o = 16; o > 0; o >>= 1)
+		{
+			lo[k] = fminf(lo[k], __shfl_xor_sync(0xFFFFFFFFu, lo[k], o));
+			hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xFFFFFFFFu, hi[k], o));
+		}
+	}
+	const int warp = threadIdx.x >> 5;
+	if ((threadIdx.x & 31) == 0)
+		for (int k = 0; k < 3; ++k) { red[k][warp] = lo[k]; red[3 + k][warp] = hi[k]; }
+	__syncthreads();
+	if (threadIdx.x < 6)
+	{
+		float r = red[threadIdx.x][0];
+		for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w)
+			r = threadIdx.x < 3 ? fminf(r, red[threadIdx.x][w]) : fmaxf(r, red[threadIdx.x][w]);
+		boxes[6u * i + threadIdx.x] = r;
+	}
+}
+} // namespace
+
+void launchInstanceBoxes(const float4* objVerts, const uint32_t* range, const float* xf, float* boxes, uint32_t n,
+	cudaStream_t st)
+{
+	if (n) kInstanceBoxes<<<n, 256, 0, st>>>(objVerts, range, xf, boxes);
+}
+
 void launchRefit(const RefitData& r, DevGeometry& g, const float* xf, const float* wi, uint32_t* status, int smCount,
 	cudaStream_t st)
 {
