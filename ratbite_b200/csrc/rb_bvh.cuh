@@ -51,7 +51,11 @@ struct HybridStack
 // visits more nodes and triangles than it saves; postponing adds visits
 // (culling sees the postponed hits later) and the traversal is bound by
 // instruction issue and L1/L2 latency, not by the node-versus-leaf
-// divergence it removes.
+// divergence it removes. Triangle loads cached in L2 only (ld.global.cg,
+// leaving L1 to the nodes and stacks) changed nothing (392.9 against 392.3
+// ms), nor did register caps of 48 and 40 (10 and 12 resident blocks of 128:
+// 391.4 and 402.3 ms) or step budgets of 32 (398.4 ms) and 4 refill lanes
+// (390.5 ms).
 #ifndef RB_TRAV_SORT
 #define RB_TRAV_SORT 1
 #endif
