@@ -19,7 +19,7 @@ from gpu_util import assert_image_parity
 from oracle_lib import RefLib, light_tree_record, load_scene_into_ref, ref_render, reference_luts
 from ratbite_b200 import abi, lighttree, scenes
 from ratbite_b200._native import NativeError
-from ratbite_b200.rendering_interface import RenderingInterface
+from ratbite_b200.rendering_interface import RenderingInterface, render_jobs
 
 pytestmark = pytest.mark.gpu
 
@@ -127,3 +127,50 @@ def test_device_tree_samples_the_emission_texture(tables):
           f"without uvs: image mean rel diff {abs(c.sum() - a.sum()) / a.sum():.3e}")
     assert rel < 1e-2 and abs(z) < 5.0
     assert np.abs(c - a).sum() > 1e-3 * np.abs(a).sum()
+
+
+def test_textured_jobs_in_a_shared_wavefront(tables):
+    """The textured kernels of the shared wavefront (rb_render_jobs): a
+    textured job and an untextured one in one wave, each bit-identical to
+    its own render."""
+    scs = [scenes.textured_cornell(seed=3, cie_xyz=tables["cie"], width=40, height=32, spp=6, max_depth=6),
+           scenes.cornell_box(seed=2, cie_xyz=tables["cie"], width=24, height=20, spp=6, max_depth=6)]
+    alone = []
+    for sc in scs:
+        with RenderingInterface(device=0) as ri:
+            ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(sc))
+            ri.render(0, 6)
+            alone.append(ri.read_accumulation())
+    ris = []
+    for sc in scs:
+        ri = RenderingInterface(device=0)
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(sc))
+        ris.append(ri)
+    render_jobs(ris, [0, 0], [6, 6])
+    for ri, want in zip(ris, alone):
+        assert ri.status().flags == 0
+        assert np.array_equal(ri.read_accumulation(), want)
+        ri.cleanup()
+
+
+def test_textured_scene_in_the_cached_form(tables):
+    """The cached form on a textured scene: with paths that never stop at
+    the cache it renders the plain image bit for bit (the textured shading
+    kernels under the cache's record and query bookkeeping), and with
+    training on it keeps a finite loss and clean status."""
+    from ratbite_b200.nrc import RadianceCache
+    sc = scenes.textured_cornell(seed=3, cie_xyz=tables["cie"], width=48, height=40, spp=8, max_depth=8)
+    with RenderingInterface(device=0) as ri:
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(sc))
+        ri.render(0, 8)
+        want = ri.read_accumulation()
+        cache = RadianceCache(seed=1)
+        ri.attach_radiance_cache(cache, spread_threshold=1e30, frozen=True, samples_per_wave=8)
+        ri.render(0, 8)
+        assert np.array_equal(ri.read_accumulation(), want)
+        ri.attach_radiance_cache(cache, samples_per_wave=8)
+        ri.render(0, 16)
+        st = ri.cache_stats()
+        assert ri.status().flags == 0 and np.isfinite(st.last_loss) and st.queries > 0
+        ri.attach_radiance_cache(None)
+        cache.close()
