@@ -20,7 +20,7 @@ import pytest
 import cases
 from gpu_util import assert_image_parity, dev, empty, host, ptr, run_bxdf, run_light, torch
 from oracle_lib import RefLib, light_tree_record, load_scene_into_ref, ref_render, reference_luts, _np_ptr
-from ratbite_b200 import abi, scenes
+from ratbite_b200 import abi, lighttree, scenes
 from ratbite_b200._native import check, load
 from ratbite_b200.rendering_interface import RenderingInterface
 
@@ -421,6 +421,42 @@ def test_render_parity_cornell(ref, tables, cornell):
     st = ri.status()
     assert st.flags == 0
     assert_image_parity(f"cornell {W}x{H}x{spp}", got, want)
+
+
+def test_render_parity_depth_of_field(ref, tables):
+    """Thin-lens camera (the reference's depth of field, launch parameters
+    dof / aperture / focus distance; pathtrace.cu:1140-1150): camera rays
+    and the image against the oracle."""
+    sc = scenes.cornell_box(seed=1, cie_xyz=tables["cie"], width=48, height=48, spp=8, max_depth=8)
+    W, H, spp = 48, 48, 8
+    keep = load_scene_into_ref(ref, sc, tables["luts"], tables["cie"], tables["basis"])
+    launch = sc.launch_record()
+    launch.dof_enabled, launch.aperture, launch.focus_distance = 1, 0.08, 2.9
+    assert ref.lib.rbref_set_launch(C.byref(launch)) == 0
+    want = ref_render(ref, W, H, 0, spp)
+    pix, fuv, luv = cases.camera_rays(w=W, h=H)
+    n = len(pix)
+    want_rays = np.zeros(n * 6, np.float32)
+    ref.lib.rbref_camera_ray(n, _np_ptr(pix), _np_ptr(fuv), _np_ptr(luv), _np_ptr(want_rays))
+    with RenderingInterface(device=0) as ri:
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(sc))
+        ri.prepare_data_for_rendering(launch)
+        out = empty(n * 6, torch().float32)
+        tp, tf, tl = dev(pix), dev(fuv), dev(luv)
+        check(load().rb_k_camera_ray(ri.ctx, n, ptr(tp), ptr(tf), ptr(tl), ptr(out), None), ri.ctx, "camera")
+        got_rays = host(out)
+        ri.render(0, spp)
+        got = ri.read_accumulation()
+        assert ri.status().flags == 0
+    report("thin-lens camera ray", got_rays, want_rays)
+    assert close(got_rays, want_rays, atol=1e-6).all()
+    assert_image_parity(f"cornell, depth of field, {W}x{H}x{spp}", got, want)
+    # the lens is in use: the pinhole image differs
+    with RenderingInterface(device=0) as ri:
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(sc))
+        ri.render(0, spp)
+        pin = ri.read_accumulation()
+    assert np.abs(pin - got).sum() > 1e-3 * np.abs(got).sum()
 
 
 def test_render_progressive_offsets(ref, tables, cornell):
