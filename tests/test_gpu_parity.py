@@ -459,6 +459,30 @@ def test_render_parity_depth_of_field(ref, tables):
     assert np.abs(pin - got).sum() > 1e-3 * np.abs(got).sum()
 
 
+def test_render_parity_spectral_conductors(ref, tables):
+    """The PureConductor BxDF (pathtrace.cu:464-547) in whole renders: the
+    Cornell box with a rough gold sphere and a back wall of smooth copper
+    (measured complex IOR spectra, extra spectra 0..3), against the
+    oracle."""
+    sc = scenes.cornell_box(seed=1, cie_xyz=tables["cie"], width=48, height=48, spp=8, max_depth=8)
+    sc.materials[6] = scenes.Material(bxdf=abi.RB_BXDF_PURE_CONDUCTOR, ior_spectrum=0, absorp_spectrum=1,
+                                      mf_roughness=0.3)
+    sc.materials[3] = scenes.Material(bxdf=abi.RB_BXDF_PURE_CONDUCTOR, ior_spectrum=2, absorp_spectrum=3,
+                                      mf_roughness=0.0)
+    extra = np.stack([ref.named_spectrum(cases.SPEC_AU_IOR), ref.named_spectrum(cases.SPEC_AU_AC),
+                      ref.named_spectrum(cases.SPEC_CU_IOR), ref.named_spectrum(cases.SPEC_CU_AC)])
+    W, H, spp = 48, 48, 8
+    keep = load_scene_into_ref(ref, sc, tables["luts"], tables["cie"], tables["basis"], extra=extra)
+    want = ref_render(ref, W, H, 0, spp)
+    with RenderingInterface(device=0) as ri:
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(sc),
+                      extra=extra)
+        ri.render(0, spp)
+        got = ri.read_accumulation()
+        assert ri.status().flags == 0
+    assert_image_parity(f"cornell with spectral conductors {W}x{H}x{spp}", got, want)
+
+
 def test_render_progressive_offsets(ref, tables, cornell):
     """Sample ranges accumulate like one launch: [0,3) + [3,8) == [0,8)."""
     sc, ri, _ = cornell
