@@ -483,6 +483,28 @@ def test_render_parity_spectral_conductors(ref, tables):
     assert_image_parity(f"cornell with spectral conductors {W}x{H}x{spp}", got, want)
 
 
+@pytest.mark.parametrize("depths", [(8, 2, 6), (6, 5, 1), (3, 8, 8)])
+def test_render_parity_separate_depth_limits(ref, tables, depths):
+    """The launch's three depth limits (path, reflected, transmitted;
+    the reference's maxPathDepth / maxReflectedPathDepth /
+    maxTransmittedPathDepth) set apart, against the oracle: the dielectric
+    sphere counts transmissions, the other surfaces reflections."""
+    sc = scenes.cornell_box(seed=1, cie_xyz=tables["cie"], width=40, height=40, spp=8, max_depth=8)
+    W, H, spp = 40, 40, 8
+    keep = load_scene_into_ref(ref, sc, tables["luts"], tables["cie"], tables["basis"])
+    launch = sc.launch_record()
+    launch.max_path_depth, launch.max_reflected_depth, launch.max_transmitted_depth = depths
+    assert ref.lib.rbref_set_launch(C.byref(launch)) == 0
+    want = ref_render(ref, W, H, 0, spp)
+    with RenderingInterface(device=0) as ri:
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(sc))
+        ri.prepare_data_for_rendering(launch)
+        ri.render(0, spp)
+        got = ri.read_accumulation()
+        assert ri.status().flags == 0
+    assert_image_parity(f"cornell, depths {depths}, {W}x{H}x{spp}", got, want)
+
+
 def test_render_progressive_offsets(ref, tables, cornell):
     """Sample ranges accumulate like one launch: [0,3) + [3,8) == [0,8)."""
     sc, ri, _ = cornell
