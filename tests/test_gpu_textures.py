@@ -174,3 +174,26 @@ def test_textured_scene_in_the_cached_form(tables):
         assert ri.status().flags == 0 and np.isfinite(st.last_loss) and st.queries > 0
         ri.attach_radiance_cache(None)
         cache.close()
+
+
+def test_failed_samples_kept_or_dropped(tables):
+    """rb_config.failed_sample_mode on a scene whose normal map makes BxDF
+    samples fail: RB_FAILED_DROP (the reference's behaviour, the image the
+    parity tests compare) drops a failed sample's radiance, RB_FAILED_KEEP
+    keeps what the path gathered before the failure. Same sample sequence,
+    so per pixel the kept image is at least the dropped one, and larger
+    somewhere."""
+    sc = scenes.textured_cornell(seed=3, cie_xyz=tables["cie"], width=48, height=48, spp=16, max_depth=8)
+    out = []
+    for mode in (abi.RB_FAILED_DROP, abi.RB_FAILED_KEEP):
+        with RenderingInterface(device=0, failed_sample_mode=mode) as ri:
+            ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(sc))
+            ri.render(0, 16)
+            out.append(ri.read_accumulation())
+            assert ri.status().flags == 0
+    drop, keep = out
+    assert np.array_equal(drop[..., 3], keep[..., 3])
+    d = keep[..., :3] - drop[..., :3]
+    print(f"failed samples: kept image {d.sum() / drop[..., :3].sum():.3%} brighter, pixels changed {np.mean(np.any(d != 0, -1)):.1%}")
+    assert d.min() >= -1e-9 * np.abs(drop[..., :3]).max()
+    assert d.sum() > 0.0
