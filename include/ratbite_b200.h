@@ -400,6 +400,12 @@ int rb_render_jobs(rb_ctx* const* jobs, uint32_t n, const uint32_t* offsets, con
 /* Copies the width*height*4 doubles (sum X, sum Y, sum Z, sample count) of
  * the accumulation buffer (renderData) to host memory; synchronizes. */
 int rb_read_accum(rb_ctx* ctx, double* out);
+/* Overwrites the accumulation buffer from host memory (width*height
+ * double4, the layout rb_read_accum returns); synchronizes. With the next
+ * sample offset, what a checkpoint needs to resume a progressive render
+ * exactly: rb_render(ctx, offset, ...) with offset > 0 adds to it. No
+ * reference counterpart (its accumulation lives only in the process). */
+int rb_write_accum(rb_ctx* ctx, const double* in);
 /* Device pointer of the accumulation buffer (width*height double4). */
 int rb_accum_device_ptr(rb_ctx* ctx, void** out);
 /* Stream-ordered copy of the accumulation buffer to `dst` (device or pinned

@@ -41,6 +41,7 @@ SIGNATURES = {
     "rb_render_graph": (C.c_int, [_P, _U32, _U32, _P]),
     "rb_render_jobs": (C.c_int, [_P, _U32, _P, _P, _P, _P]),
     "rb_read_accum": (C.c_int, [_P, _P]),
+    "rb_write_accum": (C.c_int, [_P, _P]),
     "rb_accum_device_ptr": (C.c_int, [_P, C.POINTER(_P)]),
     "rb_copy_accum_async": (C.c_int, [_P, _P, _P]),
     "rb_clear_accum": (C.c_int, [_P, _P]),

@@ -1983,6 +1983,18 @@ int rb_read_accum(rb_ctx* ctx, double* out)
 	return RB_OK;
 }
 
+int rb_write_accum(rb_ctx* ctx, const double* in)
+{
+	if (!ctx || !in) return RB_ERR_INVALID;
+	if (!ctx->accum) return fail(ctx, RB_ERR_NO_SCENE, "rb_write_accum: no accumulation buffer");
+	cudaSetDevice(ctx->device);
+	cudaError_t e = cudaStreamSynchronize(ctx->stream);
+	if (e == cudaSuccess) e = cudaDeviceSynchronize();
+	if (e == cudaSuccess) e = cudaMemcpy(ctx->accum, in, sizeof(double4) * ctx->accumPixels, cudaMemcpyHostToDevice);
+	if (e != cudaSuccess) return cudaFail(ctx, e, "rb_write_accum");
+	return RB_OK;
+}
+
 int rb_accum_device_ptr(rb_ctx* ctx, void** out)
 {
 	if (!ctx || !out) return RB_ERR_INVALID;

@@ -200,6 +200,38 @@ class RenderingInterface:
         check(self.lib.rb_read_accum(self.ctx, _ptr(out)), self.ctx, "rb_read_accum")
         return out
 
+    def write_accumulation(self, accum: np.ndarray):
+        """Overwrites the accumulation buffer (rb_write_accum)."""
+        a = np.ascontiguousarray(accum, np.float64)
+        if a.shape != (self.height, self.width, 4):
+            raise ValueError(f"accumulation is {a.shape}, the film is {(self.height, self.width, 4)}")
+        check(self.lib.rb_write_accum(self.ctx, _ptr(a)), self.ctx, "rb_write_accum")
+
+    def save_checkpoint(self, path, next_offset: int, cache=None):
+        """Writes what resumes this render (np.savez): the FP64
+        accumulation, the next sample offset and the film size, and with a
+        radiance cache its parameters (grid and weights; the optimiser's
+        moments restart on resume)."""
+        extra = {}
+        if cache is not None:
+            grid, weights = cache.parameters()
+            extra = dict(cache_grid=grid, cache_weights=weights)
+        np.savez(path, accum=self.read_accumulation(), next_offset=np.int64(next_offset),
+                 film=np.array([self.width, self.height], np.int64), **extra)
+
+    def load_checkpoint(self, path, cache=None) -> int:
+        """Restores a checkpoint of save_checkpoint into this context (scene
+        and launch already loaded, same film) and returns the next sample
+        offset: rendering on from it adds to the restored accumulation
+        exactly as the interrupted render would have."""
+        with np.load(path) as z:
+            if tuple(int(v) for v in z["film"]) != (self.width, self.height):
+                raise ValueError("checkpoint film size differs from the loaded launch")
+            self.write_accumulation(z["accum"])
+            if cache is not None and "cache_grid" in z:
+                cache.set_parameters(z["cache_grid"], z["cache_weights"])
+            return int(z["next_offset"])
+
     def copy_accumulation_async(self, dst_ptr: int, stream=None):
         """Stream-ordered copy into device or pinned host memory at dst_ptr."""
         s = None if stream is None else C.c_void_p(stream)
