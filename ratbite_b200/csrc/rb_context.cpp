@@ -15,6 +15,7 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "ratbite_b200.h"
 #include "ratbite_b200_kernels.h"
@@ -139,6 +140,16 @@ struct rb_ctx
 	};
 	std::vector<Graph> graphs;
 	uint32_t* dyn = nullptr;
+};
+
+// NVTX range over a host-side phase (render calls, structure builds), for
+// timeline tools; free when no tool is attached.
+struct NvtxRange
+{
+	explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+	~NvtxRange() { nvtxRangePop(); }
+	NvtxRange(const NvtxRange&) = delete;
+	NvtxRange& operator=(const NvtxRange&) = delete;
 };
 
 namespace
@@ -1094,6 +1105,7 @@ int setGeometryInstanced(rb_ctx* ctx, const rb_geometry* g)
 
 int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 {
+	const NvtxRange range("rb_set_geometry");
 	if (!ctx || !g) return fail(ctx, RB_ERR_INVALID, "rb_set_geometry: null geometry");
 	if ((g->mesh_count && !g->meshes) || (g->instance_count && !g->instances) ||
 		(g->emissive_subset_count && !g->emissive_subsets))
@@ -1247,6 +1259,7 @@ int rb_set_geometry(rb_ctx* ctx, const rb_geometry* g)
 
 int rb_update_instances(rb_ctx* ctx, const float* instXf, const float* subsetXf, void* stream)
 {
+	const NvtxRange range("rb_update_instances");
 	if (!ctx) return RB_ERR_INVALID;
 	if (!ctx->haveGeometry) return fail(ctx, RB_ERR_NO_SCENE, "rb_update_instances: no geometry");
 	if ((ctx->geoInstances && !instXf) || (ctx->geoSubsets && !subsetXf))
@@ -1371,6 +1384,7 @@ int rb_set_lights(rb_ctx* ctx, const rb_light_tree* t)
 int rb_build_lights(rb_ctx* ctx, uint32_t n, const float* world, const float* flux, const uint32_t* material,
 	const uint32_t* primitive, const float* uvs, void* stream)
 {
+	const NvtxRange range("rb_build_lights");
 	if (!ctx) return RB_ERR_INVALID;
 	if (n && (!world || !flux || !material || !primitive)) return fail(ctx, RB_ERR_INVALID, "rb_build_lights: null input");
 	if (n > (1u << 27) - 1u) return fail(ctx, RB_ERR_INVALID, "rb_build_lights: too many emitters");
@@ -1717,6 +1731,7 @@ extern "C" {
 
 int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 {
+	const NvtxRange range("rb_render");
 	if (!ctx) return RB_ERR_INVALID;
 	int rc = renderReady(ctx);
 	if (rc != RB_OK) return rc;
@@ -1730,6 +1745,7 @@ int rb_render(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 int rb_render_jobs(rb_ctx* const* jobs, uint32_t n, const uint32_t* offsets, const uint32_t* counts,
 	const rb_jobs_options* options, void* stream)
 {
+	const NvtxRange range("rb_render_jobs");
 	if (!jobs || n == 0 || !offsets || !counts || !jobs[0]) return RB_ERR_INVALID;
 	rb_ctx* host = jobs[0];
 	for (uint32_t j = 0; j < n; ++j)
@@ -1898,6 +1914,7 @@ int rb_render_jobs(rb_ctx* const* jobs, uint32_t n, const uint32_t* offsets, con
 
 int rb_render_graph(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 {
+	const NvtxRange range("rb_render_graph");
 	if (!ctx) return RB_ERR_INVALID;
 	int rc = renderReady(ctx);
 	if (rc != RB_OK) return rc;
