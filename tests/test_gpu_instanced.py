@@ -186,3 +186,30 @@ def test_shared_wavefront_rejects_instanced_contexts(tables):
         render_jobs([a, b], [0, 0], [1, 1])
     a.cleanup()
     b.cleanup()
+
+
+def test_instanced_cached_form_and_graphs(tables):
+    """The two-level structure under the cached form (paths that never stop
+    at the cache give the plain image bit for bit; with queries and training
+    the status stays clean) and under graph replay (rb_render_graph equals
+    rb_render)."""
+    from ratbite_b200.nrc import RadianceCache
+    sc = scenes.scale_scene(seed=5, target_tris=100_000, n_emitters=64, width=64, height=36, spp=8, max_depth=8,
+                            envmap_size=(128, 64))
+    lt = lighttree.build_for_scene(sc)
+    with _open(tables, sc, abi.RB_ACCEL_FLAT, lt) as ri:
+        ri.render(0, 8)
+        want = ri.read_accumulation()
+    with _open(tables, sc, abi.RB_ACCEL_INSTANCED, lt) as ri:
+        cache = RadianceCache(seed=1)
+        ri.attach_radiance_cache(cache, spread_threshold=1e30, frozen=True, samples_per_wave=8)
+        ri.render(0, 8)
+        assert np.array_equal(ri.read_accumulation(), want)
+        ri.attach_radiance_cache(cache, samples_per_wave=8)
+        ri.render(0, 16)
+        st = ri.cache_stats()
+        assert ri.status().flags == 0 and st.queries > 0 and np.isfinite(st.last_loss)
+        ri.attach_radiance_cache(None)
+        cache.close()
+        ri.render_graph(0, 8)
+        assert np.array_equal(ri.read_accumulation(), want)
