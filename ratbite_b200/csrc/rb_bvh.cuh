@@ -97,6 +97,20 @@ RB_D TraceRay makeTraceRay(f3 o, f3 d)
 	return r;
 }
 
+// The part of a TraceRay the box tests read (origin, direction, safe
+// reciprocal direction, octant): the two-level traversal's object-space
+// rays, whose triangles are intersected with the world ray instead.
+RB_D TraceRay makeBoxRay(f3 o, f3 d)
+{
+	TraceRay r;
+	r.o = o; r.d = d;
+	r.ix = safeRcp(d.x); r.iy = safeRcp(d.y); r.iz = safeRcp(d.z);
+	r.kx = 0; r.ky = 1; r.kz = 2;
+	r.sx = r.sy = r.sz = 0.0f;
+	r.oct = (signbit(r.ix) ? 1u : 0u) | (signbit(r.iy) ? 2u : 0u) | (signbit(r.iz) ? 4u : 0u);
+	return r;
+}
+
 // Watertight ray/triangle test. Returns true for a hit with tmin < t < tmax
 // (t <= tmax when `inclusive`), writing t and the barycentrics of v1, v2.
 RB_D bool intersectTriangle(const TraceRay& r, f3 v0, f3 v1, f3 v2, float tmin, float tmax, bool inclusive,
@@ -613,7 +627,7 @@ struct ClosestTraversal2 : ClosestTraversal
 		stack[sp++] = make_uint2(kReturnEntry, 0u);
 		const DevInstance& in = g.instances[pos];
 		const float4 o = make_float4(rw.o.x, rw.o.y, rw.o.z, 0.0f);
-		r = makeTraceRay(xfPoint(in.wi, o), xfDir(in.wi, rw.d));
+		r = makeBoxRay(xfPoint(in.wi, o), xfDir(in.wi, rw.d));
 		inst = pos;
 		cur = __ldg(&in.root);
 		return true;
@@ -730,7 +744,7 @@ struct AnyTraversal2 : AnyTraversal
 		stack[sp++] = kReturnEntry;
 		const DevInstance& in = g.instances[pos];
 		const float4 o = make_float4(rw.o.x, rw.o.y, rw.o.z, 0.0f);
-		r = makeTraceRay(xfPoint(in.wi, o), xfDir(in.wi, rw.d));
+		r = makeBoxRay(xfPoint(in.wi, o), xfDir(in.wi, rw.d));
 		inst = pos;
 		cur = __ldg(&in.root);
 		return true;
