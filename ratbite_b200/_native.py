@@ -120,6 +120,21 @@ def load() -> C.CDLL:
     return lib
 
 
+# cudaStreamLegacy: the legacy default stream as an explicit handle.
+CUDA_STREAM_LEGACY = 0x1
+
+
+def stream_arg(stream):
+    """The ctypes stream argument of the context calls (rb_render and the
+    rest): None keeps the library's own stream (the C ABI's NULL); a handle
+    of 0, which is what torch reports for the default stream, is passed as
+    cudaStreamLegacy so that the work is ordered on that stream as the
+    caller means, not on the library's."""
+    if stream is None:
+        return None
+    return C.c_void_p(int(stream) if int(stream) else CUDA_STREAM_LEGACY)
+
+
 def check(rc: int, ctx=None, what: str = ""):
     if rc != 0:
         msg = ""

@@ -1944,11 +1944,13 @@ int rb_render_graph(rb_ctx* ctx, uint32_t offset, uint32_t count, void* stream)
 		uint32_t launches[9];
 		std::memcpy(launches, ctx->launches, sizeof(launches));
 		const uint64_t paths0 = ctx->pathsTraced, waves0 = ctx->waves;
+		// captured on the context's own stream (the caller's may be the legacy
+		// default stream, which cannot be captured), launched on the caller's
 		cudaGraph_t graph = nullptr;
-		cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+		cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
 		if (e != cudaSuccess) return cudaFail(ctx, e, "rb_render_graph: begin capture");
-		rc = renderWaves(ctx, 0, count, st, ctx->dyn);
-		e = cudaStreamEndCapture(st, &graph);
+		rc = renderWaves(ctx, 0, count, ctx->stream, ctx->dyn);
+		e = cudaStreamEndCapture(ctx->stream, &graph);
 		if (rc != RB_OK || e != cudaSuccess)
 		{
 			if (graph) cudaGraphDestroy(graph);

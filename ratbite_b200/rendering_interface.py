@@ -13,7 +13,7 @@ import ctypes as C
 import numpy as np
 
 from . import abi
-from ._native import check, load
+from ._native import check, load, stream_arg
 
 
 def _ptr(a: np.ndarray):
@@ -101,7 +101,7 @@ class RenderingInterface:
         check(self.lib.rb_set_envmap(self.ctx, _ptr(img), w, h), self.ctx, "rb_set_envmap")
 
     def rebuild_environment_cdf(self, stream=None):
-        s = None if stream is None else C.c_void_p(stream)
+        s = stream_arg(stream)
         check(self.lib.rb_rebuild_envmap_cdf(self.ctx, s), self.ctx, "rb_rebuild_envmap_cdf")
 
     def clear_environment_map(self):
@@ -148,7 +148,7 @@ class RenderingInterface:
         uv = None if uvs is None else dev(np.asarray(uvs, np.float32).reshape(n, 6))
         torch.cuda.synchronize()
         ptrs = [C.c_void_p(b.data_ptr()) for b in bufs] + [None if uv is None else C.c_void_p(uv.data_ptr())]
-        check(self.lib.rb_build_lights(self.ctx, n, *ptrs, stream), self.ctx, "rb_build_lights")
+        check(self.lib.rb_build_lights(self.ctx, n, *ptrs, stream_arg(stream)), self.ctx, "rb_build_lights")
 
     def update_instances(self, instance_transforms, subset_transforms=None, stream=None):
         """Moves the instances of the loaded geometry (the reference's
@@ -158,7 +158,7 @@ class RenderingInterface:
         inst = np.ascontiguousarray(instance_transforms, np.float32).reshape(-1)
         sub = np.ascontiguousarray(np.zeros(0, np.float32) if subset_transforms is None else subset_transforms,
                                    np.float32).reshape(-1)
-        s = None if stream is None else C.c_void_p(stream)
+        s = stream_arg(stream)
         check(self.lib.rb_update_instances(self.ctx, _ptr(inst) if inst.size else None,
                                            _ptr(sub) if sub.size else None, s), self.ctx, "rb_update_instances")
 
@@ -166,19 +166,19 @@ class RenderingInterface:
         """Camera-move refresh of the light data on the device: emissive
         triangle vertices and light-tree means become (as loaded) - origin."""
         o = np.ascontiguousarray(origin, np.float32).reshape(3)
-        s = None if stream is None else C.c_void_p(stream)
+        s = stream_arg(stream)
         check(self.lib.rb_set_light_origin(self.ctx, _ptr(o), s), self.ctx, "rb_set_light_origin")
 
     # ---- rendering -----------------------------------------------------------
     def render(self, sample_offset: int, sample_count: int, stream=None):
         """Asynchronous: renders samples [offset, offset+count) of every pixel."""
-        s = None if stream is None else C.c_void_p(stream)
+        s = stream_arg(stream)
         check(self.lib.rb_render(self.ctx, sample_offset, sample_count, s), self.ctx, "rb_render")
 
     def render_graph(self, sample_offset: int, sample_count: int, stream=None):
         """render() through a captured CUDA graph of the call's waves (same
         accumulation); the first call of a sample count captures it."""
-        s = None if stream is None else C.c_void_p(stream)
+        s = stream_arg(stream)
         check(self.lib.rb_render_graph(self.ctx, sample_offset, sample_count, s), self.ctx, "rb_render_graph")
 
     def progressive_restart(self, total_samples: int, mode: int = abi.RB_MODE_GRADUAL):
@@ -188,7 +188,7 @@ class RenderingInterface:
     def progressive_step(self, stream=None) -> abi.rb_progress:
         """Launches the next sub-launch of the progressive render (asynchronous)."""
         out = abi.rb_progress()
-        s = None if stream is None else C.c_void_p(stream)
+        s = stream_arg(stream)
         check(self.lib.rb_progressive_step(self.ctx, s, C.byref(out)), self.ctx, "rb_progressive_step")
         return out
 
@@ -234,7 +234,7 @@ class RenderingInterface:
 
     def copy_accumulation_async(self, dst_ptr: int, stream=None):
         """Stream-ordered copy into device or pinned host memory at dst_ptr."""
-        s = None if stream is None else C.c_void_p(stream)
+        s = stream_arg(stream)
         check(self.lib.rb_copy_accum_async(self.ctx, C.c_void_p(dst_ptr), s), self.ctx, "rb_copy_accum_async")
 
     def resolve(self, exposure: float = 0.0, colorspace=None, stream=None):
@@ -245,7 +245,7 @@ class RenderingInterface:
         cs = colorspace_matrix("sRGB") if colorspace is None else np.ascontiguousarray(colorspace, np.float32)
         if cs.size != 9:
             raise ValueError("colorspace must hold 9 floats")
-        s = None if stream is None else C.c_void_p(stream)
+        s = stream_arg(stream)
         check(self.lib.rb_resolve(self.ctx, _ptr(cs), float(2.0 ** (exposure - 7.0)), s), self.ctx, "rb_resolve")
 
     def read_image(self) -> np.ndarray:
@@ -256,7 +256,7 @@ class RenderingInterface:
 
     def clear_accumulation(self, stream=None):
         """Zeroes the FP64 accumulation (stream-ordered)."""
-        s = None if stream is None else C.c_void_p(stream)
+        s = stream_arg(stream)
         check(self.lib.rb_clear_accum(self.ctx, s), self.ctx, "rb_clear_accum")
 
     def accumulation_device_ptr(self) -> int:
@@ -333,4 +333,5 @@ def render_jobs(interfaces, offsets, counts, max_paths: int = 0, grid_percent: i
     if done_events is not None:
         ev = (C.c_void_p * n)(*[e.cuda_event if e is not None else None for e in done_events])
         opt.done_events = C.cast(ev, C.c_void_p)
-    check(lib.rb_render_jobs(ctxs, n, offs, cnts, C.byref(opt), stream), interfaces[0].ctx, "rb_render_jobs")
+    check(lib.rb_render_jobs(ctxs, n, offs, cnts, C.byref(opt), stream_arg(stream)), interfaces[0].ctx,
+          "rb_render_jobs")

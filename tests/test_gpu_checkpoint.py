@@ -67,3 +67,39 @@ def test_write_accumulation_round_trip():
     from ratbite_b200._native import load
     assert load().rb_write_accum(empty.ctx, a.ctypes.data) != 0     # no film yet
     empty.cleanup()
+
+
+def test_render_on_the_default_stream_is_ordered_there():
+    """A caller that passes torch's default stream (handle 0) gets its work
+    ordered on that stream (cudaStreamLegacy), not on the library's own
+    stream: an event recorded after the call completes only after the
+    render, and a device-to-device copy of the accumulation enqueued behind
+    it on the same stream sees the finished samples."""
+    import torch
+    ref = RefLib()
+    t = dict(cie=ref.cie_xyz(), basis=ref.basis_rgb(), luts=reference_luts())
+    sc = scenes.scale_scene(seed=5, target_tris=60_000, n_emitters=64, width=320, height=180, spp=64, max_depth=8,
+                            envmap_size=(128, 64))
+    with _open(sc, t) as ri:
+        ri.render(0, 4)
+        torch.cuda.synchronize()
+        s = torch.cuda.current_stream()
+        assert s.cuda_stream == 0
+        out = torch.empty((180, 320, 4), dtype=torch.float64, device="cuda")
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        ri.render(4, 60, stream=s.cuda_stream)
+        ri.copy_accumulation_async(out.data_ptr(), stream=s.cuda_stream)
+        b.record()
+        b.synchronize()
+        ms = a.elapsed_time(b)
+        got = out.cpu().numpy()
+        assert np.array_equal(got, ri.read_accumulation())
+        assert (got[..., 3] == 64).all()
+        print(f"render on the default stream: {ms:.1f} ms between the events")
+        assert ms > 1.0
+        # graph replay too: captured on the library's stream, launched on the caller's
+        ri.render_graph(64, 8, stream=s.cuda_stream)
+        ri.copy_accumulation_async(out.data_ptr(), stream=s.cuda_stream)
+        s.synchronize()
+        assert (out[..., 3] == 72).all().item()
