@@ -39,6 +39,15 @@ int rb_k_wavelengths(uint32_t n, const float* u, float* lambda, float* pdf, void
 int rb_k_camera_ray(rb_ctx* ctx, uint32_t n, const float* pixel_xy, const float* filter_uv,
                     const float* lens_uv, float* out, void* stream);
 
+/* Texture `texture` of the context's rb_set_textures table sampled at n
+ * (u, v) pairs by the shading kernels' software sampler (soft, 4 floats
+ * each) and by the texture unit through a CUDA texture object made from the
+ * same texels and sampler settings, as the reference's CudaCombinedTexture
+ * (src/core/texture.h:237-380) makes it (hw, 4 floats each): a check of the
+ * sampler's semantics. Synchronizes. */
+int rb_k_texture_sample(rb_ctx* ctx, uint32_t texture, uint32_t n, const float* uv, float* soft, float* hw,
+                        void* stream);
+
 /* One BxDF call as the raygen makes it (src/kernels/pathtrace.cu:1724-1733):
  * inputs and the in/out path state in one record. */
 typedef struct rb_bxdf_case {

@@ -267,8 +267,8 @@ int rbref_set_luts(const float* conductor, const float* dielOuter, const float* 
 // Material textures (the product's rb_set_textures table): texels decoded
 // to floats as the texture hardware reads them (8-bit / 255; the sRGB curve
 // for r, g, b of sRGB textures, r of a one-channel one, IEC 61966-2-1 in
-// double precision), a
-// one-channel texture stored as (r, 0, 0, 1); handles registered for
+// double precision), a one-channel texture stored as (r, 0, 0, 0), which
+// is what the texture unit returns for it; handles registered for
 // rbref_set_materials to use. Call after rbref_set_luts.
 int rbref_set_textures(const rb_texture* tex, uint32_t count)
 {
@@ -291,7 +291,7 @@ int rbref_set_textures(const rb_texture* tex, uint32_t count)
 			if (t.format == RB_TEXFMT_R8)
 			{
 				texels[4 * k] = t.srgb ? lut[src[k]] : static_cast<float>(src[k]) / 255.0f;
-				texels[4 * k + 1] = 0.0f; texels[4 * k + 2] = 0.0f; texels[4 * k + 3] = 1.0f;
+				texels[4 * k + 1] = 0.0f; texels[4 * k + 2] = 0.0f; texels[4 * k + 3] = 0.0f;
 				continue;
 			}
 			for (int ch = 0; ch < 4; ++ch)

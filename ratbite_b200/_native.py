@@ -59,6 +59,7 @@ SIGNATURES = {
     "rb_k_sobol": (C.c_int, [_U32, _U32, _P, _P, _P, _P, _P, _P]),
     "rb_k_pixel_hash": (C.c_int, [_U32, _P, _P, _P, _P]),
     "rb_k_wavelengths": (C.c_int, [_U32, _P, _P, _P, _P]),
+    "rb_k_texture_sample": (C.c_int, [_P, _U32, _U32, _P, _P, _P, _P]),
     "rb_k_camera_ray": (C.c_int, [_P, _U32, _P, _P, _P, _P, _P]),
     "rb_k_bxdf": (C.c_int, [_P, _U32, _P, _P]),
     "rb_k_light_tree": (C.c_int, [_P, _U32, _P, _P]),

@@ -2255,6 +2255,52 @@ int rb_k_camera_ray(rb_ctx* ctx, uint32_t n, const float* pixel, const float* fu
 	rb::launchCameraRay(ctx->scene, n, pixel, fuv, luv, out, pick(ctx, stream));
 	return lastLaunch();
 }
+int rb_k_texture_sample(rb_ctx* ctx, uint32_t texture, uint32_t n, const float* uv, float* soft, float* hw,
+	void* stream)
+{
+	RB_K_CHECK(ctx && texture < ctx->scene.textureCount);
+	if (n == 0) return RB_OK;
+	RB_K_CHECK(uv && soft && hw);
+	cudaSetDevice(ctx->device);
+	const cudaStream_t st = pick(ctx, stream);
+	rb::DevTexture t{};
+	if (cudaMemcpy(&t, ctx->scene.textures + texture, sizeof(t), cudaMemcpyDeviceToHost) != cudaSuccess)
+		return fail(ctx, RB_ERR_CUDA, "rb_k_texture_sample: texture record");
+	const cudaChannelFormatDesc fmt = t.channels == 1 ? cudaCreateChannelDesc<unsigned char>()
+	                                                  : cudaCreateChannelDesc<uchar4>();
+	cudaArray_t arr = nullptr;
+	cudaTextureObject_t obj = 0;
+	cudaError_t e = cudaMallocArray(&arr, &fmt, t.width, t.height);
+	if (e == cudaSuccess)
+		e = cudaMemcpy2DToArray(arr, 0, 0, t.data, static_cast<size_t>(t.width) * t.channels,
+			static_cast<size_t>(t.width) * t.channels, t.height, cudaMemcpyDeviceToDevice);
+	if (e == cudaSuccess)
+	{
+		cudaResourceDesc res{};
+		res.resType = cudaResourceTypeArray;
+		res.res.array.array = arr;
+		auto mode = [](uint32_t m) {
+			return m == RB_TEXADDR_WRAP ? cudaAddressModeWrap : (m == RB_TEXADDR_MIRROR ? cudaAddressModeMirror : cudaAddressModeClamp);
+		};
+		cudaTextureDesc td{};
+		td.addressMode[0] = mode(t.addrU);
+		td.addressMode[1] = mode(t.addrV);
+		td.filterMode = t.filter == RB_TEXFILTER_LINEAR ? cudaFilterModeLinear : cudaFilterModePoint;
+		td.readMode = cudaReadModeNormalizedFloat;
+		td.normalizedCoords = 1;
+		td.sRGB = t.srgb ? 1 : 0;
+		e = cudaCreateTextureObject(&obj, &res, &td, nullptr);
+	}
+	if (e == cudaSuccess)
+	{
+		rb::launchTextureSample(ctx->scene, texture, obj, n, uv, soft, hw, st);
+		e = cudaGetLastError();
+	}
+	if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+	if (obj) cudaDestroyTextureObject(obj);
+	if (arr) cudaFreeArray(arr);
+	return e == cudaSuccess ? RB_OK : cudaFail(ctx, e, "rb_k_texture_sample");
+}
 int rb_k_bxdf(rb_ctx* ctx, uint32_t n, rb_bxdf_case* cases, void* stream)
 {
 	RB_K_CHECK(ctx && ctx->scene.materials && ctx->scene.luts.conductor && ctx->scene.spectra.basis);

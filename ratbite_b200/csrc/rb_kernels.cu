@@ -1441,6 +1441,30 @@ void launchWavelengths(uint32_t n, const float* u, float* lambda, float* pdf, cu
 {
 	kWavelengths<<<gridFor(n), kThreads, 0, st>>>(n, u, lambda, pdf);
 }
+namespace
+{
+// The software sampler and the texture unit on the same texture and
+// coordinates (a check of the sampler's semantics against the hardware the
+// reference samples with).
+__global__ void kTextureSample(const __grid_constant__ DevScene sc, uint32_t texture, cudaTextureObject_t hw,
+	uint32_t n, const float* __restrict__ uv, float4* __restrict__ soft, float4* __restrict__ hwOut)
+{
+	for (uint32_t i = gtid(); i < n; i += gstride())
+	{
+		const float u = uv[2 * i], v = uv[2 * i + 1];
+		soft[i] = texSample(sc, texture, u, v);
+		hwOut[i] = tex2D<float4>(hw, u, v);
+	}
+}
+} // namespace
+
+void launchTextureSample(const DevScene& sc, uint32_t texture, cudaTextureObject_t hw, uint32_t n, const float* uv,
+	float* soft, float* hwOut, cudaStream_t st)
+{
+	kTextureSample<<<gridFor(n), kThreads, 0, st>>>(sc, texture, hw, n, uv, reinterpret_cast<float4*>(soft),
+		reinterpret_cast<float4*>(hwOut));
+}
+
 void launchCameraRay(const DevScene& sc, uint32_t n, const float* pixel, const float* fuv, const float* luv, float* out, cudaStream_t st)
 {
 	kCameraRay<<<gridFor(n), kThreads, 0, st>>>(sc, n, pixel, fuv, luv, out);

@@ -6,7 +6,9 @@
 // channels read as normalized floats, the sRGB curve applied per texel
 // before filtering (a 256-entry table of IEC 61966-2-1's decode, computed on
 // the host in double precision; r alone of a one-channel texture, the colour
-// channel of an R8 sRGB format), a one-channel texture read as (r, 0, 0, 1).
+// channel of an R8 sRGB format), a one-channel texture read as (r, 0, 0, 0)
+// as the texture unit returns it (alpha 0: measured on B200 through a CUDA
+// texture object).
 // Bilinear weights are FP32 (the texture hardware rounds them to 8-bit
 // fixed point; the oracle's parity mode uses FP32 as here).
 #pragma once
@@ -48,7 +50,7 @@ RB_D float4 texel(const DevTexture& t, const float* srgb, int x, int y)
 {
 	const size_t i = static_cast<size_t>(y) * t.width + static_cast<size_t>(x);
 	if (t.channels == 1)
-		return make_float4(t.srgb ? srgb[t.data[i]] : static_cast<float>(t.data[i]) / 255.0f, 0.0f, 0.0f, 1.0f);
+		return make_float4(t.srgb ? srgb[t.data[i]] : static_cast<float>(t.data[i]) / 255.0f, 0.0f, 0.0f, 0.0f);
 	const uchar4 c = reinterpret_cast<const uchar4*>(t.data)[i];
 	if (t.srgb) return make_float4(srgb[c.x], srgb[c.y], srgb[c.z], static_cast<float>(c.w) / 255.0f);
 	return make_float4(static_cast<float>(c.x) / 255.0f, static_cast<float>(c.y) / 255.0f,

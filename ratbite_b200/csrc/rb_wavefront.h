@@ -234,6 +234,8 @@ void launchSobol(uint32_t n, uint32_t dims, const uint32_t* sample, const uint32
 void launchPixelHash(uint32_t n, const uint32_t* x, const uint32_t* y, uint32_t* out, cudaStream_t st);
 void launchWavelengths(uint32_t n, const float* u, float* lambda, float* pdf, cudaStream_t st);
 void launchCameraRay(const DevScene& sc, uint32_t n, const float* pixel, const float* fuv, const float* luv, float* out, cudaStream_t st);
+void launchTextureSample(const DevScene& sc, uint32_t texture, cudaTextureObject_t hw, uint32_t n, const float* uv,
+	float* soft, float* hwOut, cudaStream_t st);
 void launchBxdfCases(const DevScene& sc, uint32_t n, void* cases, cudaStream_t st);
 void launchLightCases(const DevScene& sc, uint32_t n, void* cases, cudaStream_t st);
 void launchOffsetPoint(uint32_t n, const float* p, const float* nrm, float* out, cudaStream_t st);

@@ -153,10 +153,11 @@ class Texture:
     filter: int = abi.RB_TEXFILTER_LINEAR
 
     def texel(self, x: int, y: int) -> np.ndarray:
-        """Raw 8-bit texel (4 channels; a one-channel image as (r, 0, 0, 255))."""
+        """Raw 8-bit texel (4 channels; a one-channel image as (r, 0, 0, 0),
+        as the texture unit reads it)."""
         d = self.data
         if d.ndim == 2:
-            return np.array([d[y, x], 0, 0, 255], np.uint8)
+            return np.array([d[y, x], 0, 0, 0], np.uint8)
         return d[y, x]
 
 

@@ -197,3 +197,59 @@ def test_failed_samples_kept_or_dropped(tables):
     print(f"failed samples: kept image {d.sum() / drop[..., :3].sum():.3%} brighter, pixels changed {np.mean(np.any(d != 0, -1)):.1%}")
     assert d.min() >= -1e-9 * np.abs(drop[..., :3]).max()
     assert d.sum() > 0.0
+
+
+def test_software_sampler_matches_the_texture_unit(tables):
+    """The shading kernels' software sampler against the texture unit the
+    reference samples with (a CUDA texture object from the same texels and
+    sampler settings, rb_k_texture_sample): nearest filtering returns the
+    same texel except where a coordinate rounds across a texel edge,
+    bilinear filtering differs only by the unit's 8-bit fixed-point weights
+    (at most a few 1e-3), and the unit's sRGB decode is an approximation of
+    the curve within a few 1e-3 (measured on B200: bilinear RGBA8 max
+    5.4e-3, mean 1.2e-3; sRGB nearest max 3.8e-3, mean 1.1e-3); for every
+    address mode, RGBA8 and R8 (whose sRGB flag the unit applies to its one
+    channel)."""
+    import torch
+    from ratbite_b200._native import check, load
+    rng = np.random.default_rng(12)
+    texs = [
+        scenes.Texture(rng.integers(0, 256, (13, 17, 4)).astype(np.uint8), srgb=False,
+                       address=(abi.RB_TEXADDR_WRAP, abi.RB_TEXADDR_WRAP), filter=abi.RB_TEXFILTER_LINEAR),
+        scenes.Texture(rng.integers(0, 256, (9, 11, 4)).astype(np.uint8), srgb=True,
+                       address=(abi.RB_TEXADDR_MIRROR, abi.RB_TEXADDR_CLAMP), filter=abi.RB_TEXFILTER_NEAREST),
+        scenes.Texture(rng.integers(0, 256, (8, 6, 4)).astype(np.uint8), srgb=True,
+                       address=(abi.RB_TEXADDR_MIRROR, abi.RB_TEXADDR_WRAP), filter=abi.RB_TEXFILTER_LINEAR),
+        scenes.Texture(rng.integers(0, 256, (7, 10)).astype(np.uint8), srgb=False,
+                       address=(abi.RB_TEXADDR_CLAMP, abi.RB_TEXADDR_MIRROR), filter=abi.RB_TEXFILTER_LINEAR),
+        scenes.Texture(rng.integers(0, 256, (12, 5)).astype(np.uint8), srgb=True,
+                       address=(abi.RB_TEXADDR_WRAP, abi.RB_TEXADDR_CLAMP), filter=abi.RB_TEXFILTER_NEAREST),
+        scenes.Texture(rng.integers(0, 256, (6, 6)).astype(np.uint8), srgb=True,
+                       address=(abi.RB_TEXADDR_WRAP, abi.RB_TEXADDR_WRAP), filter=abi.RB_TEXFILTER_LINEAR),
+    ]
+    sc = scenes.cornell_box(seed=1, cie_xyz=tables["cie"], width=8, height=8, spp=1, max_depth=2)
+    sc.textures = texs
+    n = 20000
+    uv = rng.uniform(-2.3, 3.1, (n, 2)).astype(np.float32)
+    with RenderingInterface(device=0) as ri:
+        ri.load_scene(sc, tables["luts"], tables["cie"], tables["basis"], light_tree=lighttree.build_for_scene(sc))
+        d_uv = torch.from_numpy(uv).cuda()
+        for k, t in enumerate(texs):
+            soft = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+            hw = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+            check(load().rb_k_texture_sample(ri.ctx, k, n, C.c_void_p(d_uv.data_ptr()), C.c_void_p(soft.data_ptr()),
+                                             C.c_void_p(hw.data_ptr()), None), ri.ctx, "texture sample")
+            s_, h_ = soft.cpu().numpy(), hw.cpu().numpy()
+            d = np.abs(s_ - h_).max(axis=1)
+            kind = ("R8" if t.data.ndim == 2 else "RGBA8") + (" sRGB" if t.srgb else "") + \
+                (" nearest" if t.filter == abi.RB_TEXFILTER_NEAREST else " bilinear")
+            print(f"texture {k} ({kind}): max |soft - hw| {d.max():.2e}, mean {d.mean():.2e}, exact {np.mean(d == 0):.2%}; "
+                  f"per channel mean {np.round(np.abs(s_ - h_).mean(axis=0), 4)}; hw[0] {np.round(h_[0], 4)} soft[0] {np.round(s_[0], 4)}")
+            if t.filter == abi.RB_TEXFILTER_NEAREST and not t.srgb:
+                assert np.mean(d < 1e-6) >= 0.99, k
+            elif t.filter == abi.RB_TEXFILTER_NEAREST:
+                # the unit's sRGB decode approximates the curve (the sampler
+                # here evaluates it exactly, in double precision)
+                assert np.mean(d < 5e-3) >= 0.99 and d.mean() < 2e-3, k
+            else:
+                assert d.max() < 1.5e-2 and d.mean() < 3e-3, k
